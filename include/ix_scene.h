@@ -1,0 +1,135 @@
+/*
+ * ix_scene.h -- plain-old-data scene description shared by the CUDA backend
+ * (libix_cuda.so) and every caller of its C ABI.
+ *
+ * This is the C-ABI encoding of the reference's `GpuSceneRef`
+ * (crates/indicatrix/src/renderer/gpu_backend/mod.rs:218-237): camera, image size,
+ * facet half-space planes, per-facet finish, material, bounce cap and environment.
+ * Field meanings follow the reference's GPU buffer layouts
+ * (renderer/buffers/camera.rs:72-88, renderer/buffers/material.rs:93-243,
+ * renderer/buffers/transport.rs:42-101) but the layout is this library's own:
+ * everything a kernel needs per scene is resolved on the host into floats here, so a
+ * device never evaluates a trig function of a light pose or camera pose.
+ *
+ * Units: model units for geometry (girdle diameter 1.0 for the generated cuts),
+ * nanometres for wavelengths, and absorption coefficients in 1/length where
+ * length = model units * absorption_path_scale.
+ */
+#ifndef IX_SCENE_H
+#define IX_SCENE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IX_NUM_CHANNELS 8   /* hero-wavelength channels per path (transport/mod.rs:58) */
+#define IX_MAX_PLANES 128   /* planes per stone the shared-memory cache holds          */
+#define IX_MAX_BANDS 8      /* Gaussian bands per eigenmode (buffers/material.rs:93)     */
+#define IX_SPLINE_KNOTS 16  /* knots of the tabulated absorption spline (new form)      */
+#define IX_RING_LIGHTS 16   /* studio ring emitters (optics/studio_rig.rs:21)           */
+
+/* Pinhole camera, the four vectors of `Camera` (optics/raytracer/camera.rs:89-101). */
+typedef struct ix_camera {
+    float origin[3];
+    float forward[3];
+    float right[3];
+    float up[3];
+    float fov_tan;
+} ix_camera;
+
+/* n(lambda) model (optics/dispersion.rs:4-9).
+ *   IX_DISP_SELLMEIER1: b[0]=B1, c[0]=C1 (um^2)
+ *   IX_DISP_SELLMEIER3: b[0..2], c[0..2]
+ *   IX_DISP_CAUCHY:     b[0]=A, b[1]=B (um^2), b[2]=C (um^4)                        */
+enum { IX_DISP_SELLMEIER1 = 0, IX_DISP_SELLMEIER3 = 1, IX_DISP_CAUCHY = 2 };
+typedef struct ix_dispersion {
+    uint32_t kind;
+    float b[3];
+    float c[3];
+} ix_dispersion;
+
+/* One absorption band (optics/absorption.rs:9-14). */
+enum { IX_BAND_GAUSS_WAVELENGTH = 0, IX_BAND_GAUSS_ENERGY = 1 };
+typedef struct ix_band {
+    float center_nm;
+    float width_nm;
+    float peak;
+    uint32_t shape;
+} ix_band;
+
+/* alpha(lambda) of one eigenmode: the sum of up to IX_MAX_BANDS Gaussian bands plus,
+ * when has_spline != 0, a uniform Catmull-Rom spline through IX_SPLINE_KNOTS knots
+ * spaced evenly over [380, 780] nm, floored at zero.  The spline is this library's
+ * encoding of a smooth tabulated absorption curve; it has no reference counterpart. */
+typedef struct ix_absorption {
+    uint32_t n_bands;
+    ix_band bands[IX_MAX_BANDS];
+    uint32_t has_spline;
+    float spline[IX_SPLINE_KNOTS];
+} ix_absorption;
+
+/* Material (GemMaterial, optics/materials/mod.rs:116-236, the fields the transport
+ * reads).  `anisotropic` is the reference's `is_anisotropic`
+ * (transport/inner.rs:191-193): crystal system not cubic and |birefringence_delta| > 1e-4. */
+typedef struct ix_material {
+    ix_dispersion dispersion;           /* ordinary index                            */
+    uint32_t anisotropic;
+    float birefringence_delta;          /* n_e - n_o for the walk-off approximation   */
+    float c_axis[3];                    /* optic axis, unit length                    */
+    uint32_t has_e_dispersion;          /* independent e-ray dispersion curve present */
+    ix_dispersion e_dispersion;
+    ix_absorption abs_o;                /* ordinary (isotropic: the only) absorption  */
+    ix_absorption abs_e;                /* extraordinary absorption                   */
+    float absorption_path_scale;        /* path length units per model unit           */
+    float edge_rounding_radius;         /* 0 = sharp facet edges                      */
+    float scattering_sigma_s;           /* interior scattering; 0 on the CUDA path     */
+} ix_material;
+
+/* Lighting model ids: the reference's LightingModel::gpu_id for the two it shares
+ * (environment/mod.rs:218-229) plus a uniform furnace dome. */
+enum { IX_ENV_STUDIO = 0, IX_ENV_ISO_HEMISPHERE = 1, IX_ENV_UNIFORM = 100 };
+/* Illuminant spectral power (environment/spectral.rs:89-113). */
+enum { IX_SPEC_D65 = 0, IX_SPEC_BLACKBODY = 1, IX_SPEC_FLAT = 2 };
+
+typedef struct ix_environment {
+    uint32_t model;
+    uint32_t spectrum;
+    float exposure;
+    float spot_mult;            /* studio rig key/ring multiplier                       */
+    uint32_t ambient_fill;      /* studio rig charcoal backdrop term present            */
+    float backdrop;             /* lit tray below the horizon; 0 = none                 */
+    float surface_glare;        /* first-bounce specular scale, clamped to [0, 1]        */
+    float shadow_cos[2];        /* head-shadow smoothstep edges (environment/mod.rs:128) */
+    float bb_t_k;               /* blackbody temperature (max(T, 1000))                  */
+    float bb_denom_560;         /* blackbody normalisation at 560 nm                    */
+    float key_dir[3];           /* StudioRig (optics/studio_rig.rs:33-70)                */
+    float fill_dir[3];
+    float ring_dirs[IX_RING_LIGHTS][3];
+    uint32_t white_balance;     /* apply the Bradford von Kries round trip at finish     */
+    float wb_lms[3];            /* LMS scale of the white balance                       */
+    float uniform_radiance;     /* IX_ENV_UNIFORM dome radiance                         */
+} ix_environment;
+
+/* The scene.  `planes` is n_planes x {nx, ny, nz, d} with the convention n.x + d <= 0
+ * inside (geometry/plane.rs:34-41).  `facet_finishes` may be NULL (all polished);
+ * a nonzero entry marks a frosted facet, which the CUDA backend declines. */
+typedef struct ix_scene {
+    ix_camera camera;
+    uint32_t width;
+    uint32_t height;
+    const float* planes;
+    uint32_t n_planes;
+    const uint8_t* facet_finishes;
+    uint32_t n_finishes;
+    ix_material material;
+    uint32_t max_bounces;
+    ix_environment environment;
+} ix_scene;
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IX_SCENE_H */

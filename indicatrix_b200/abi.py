@@ -1,0 +1,160 @@
+"""ctypes mirror of ``include/ix_scene.h`` and ``include/ix_cuda.h``.
+
+These structures are the C-ABI encoding of the reference's ``GpuSceneRef``
+(crates/indicatrix/src/renderer/gpu_backend/mod.rs:218-237) and of the backend's
+options, batch items and status codes.  Every field matches the C header one for one;
+``tests/test_abi.py`` checks sizes and offsets against the compiled library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+NUM_CHANNELS = 8
+MAX_PLANES = 128
+MAX_BANDS = 8
+SPLINE_KNOTS = 16
+RING_LIGHTS = 16
+
+DISP_SELLMEIER1, DISP_SELLMEIER3, DISP_CAUCHY = 0, 1, 2
+BAND_GAUSS_WAVELENGTH, BAND_GAUSS_ENERGY = 0, 1
+ENV_STUDIO, ENV_ISO_HEMISPHERE, ENV_UNIFORM = 0, 1, 100
+SPEC_D65, SPEC_BLACKBODY, SPEC_FLAT = 0, 1, 2
+
+# GpuAccumulate (gpu_backend/mod.rs:308-326) plus the internal error the C ABI maps to
+# a decline.
+IX_DONE, IX_DECLINED, IX_CANCELLED = 0, 1, 2
+
+# GpuPipelineKind (gpu_backend/mod.rs:347-353).
+PIPELINE_MEGAKERNEL, PIPELINE_WAVEFRONT = 0, 1
+# Rounding modes of the transport kernels.
+PRECISION_FAST, PRECISION_EXACT = 0, 1
+
+
+class Camera(C.Structure):
+    _fields_ = [
+        ("origin", C.c_float * 3),
+        ("forward", C.c_float * 3),
+        ("right", C.c_float * 3),
+        ("up", C.c_float * 3),
+        ("fov_tan", C.c_float),
+    ]
+
+
+class Dispersion(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("b", C.c_float * 3), ("c", C.c_float * 3)]
+
+
+class Band(C.Structure):
+    _fields_ = [
+        ("center_nm", C.c_float),
+        ("width_nm", C.c_float),
+        ("peak", C.c_float),
+        ("shape", C.c_uint32),
+    ]
+
+
+class Absorption(C.Structure):
+    _fields_ = [
+        ("n_bands", C.c_uint32),
+        ("bands", Band * MAX_BANDS),
+        ("has_spline", C.c_uint32),
+        ("spline", C.c_float * SPLINE_KNOTS),
+    ]
+
+
+class Material(C.Structure):
+    _fields_ = [
+        ("dispersion", Dispersion),
+        ("anisotropic", C.c_uint32),
+        ("birefringence_delta", C.c_float),
+        ("c_axis", C.c_float * 3),
+        ("has_e_dispersion", C.c_uint32),
+        ("e_dispersion", Dispersion),
+        ("abs_o", Absorption),
+        ("abs_e", Absorption),
+        ("absorption_path_scale", C.c_float),
+        ("edge_rounding_radius", C.c_float),
+        ("scattering_sigma_s", C.c_float),
+    ]
+
+
+class Environment(C.Structure):
+    _fields_ = [
+        ("model", C.c_uint32),
+        ("spectrum", C.c_uint32),
+        ("exposure", C.c_float),
+        ("spot_mult", C.c_float),
+        ("ambient_fill", C.c_uint32),
+        ("backdrop", C.c_float),
+        ("surface_glare", C.c_float),
+        ("shadow_cos", C.c_float * 2),
+        ("bb_t_k", C.c_float),
+        ("bb_denom_560", C.c_float),
+        ("key_dir", C.c_float * 3),
+        ("fill_dir", C.c_float * 3),
+        ("ring_dirs", (C.c_float * 3) * RING_LIGHTS),
+        ("white_balance", C.c_uint32),
+        ("wb_lms", C.c_float * 3),
+        ("uniform_radiance", C.c_float),
+    ]
+
+
+class Scene(C.Structure):
+    _fields_ = [
+        ("camera", Camera),
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("planes", C.POINTER(C.c_float)),
+        ("n_planes", C.c_uint32),
+        ("facet_finishes", C.POINTER(C.c_uint8)),
+        ("n_finishes", C.c_uint32),
+        ("material", Material),
+        ("max_bounces", C.c_uint32),
+        ("environment", Environment),
+    ]
+
+
+class BackendOptions(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("pipeline", C.c_uint32),
+        ("precision", C.c_uint32),
+        ("threads_per_block", C.c_uint32),
+        ("chunk_paths", C.c_uint64),
+    ]
+
+
+class WorkLimits(C.Structure):
+    _fields_ = [
+        ("max_pixels", C.c_uint64),
+        ("max_paths_per_call", C.c_uint64),
+        ("max_spp", C.c_uint32),
+    ]
+
+
+class BatchItem(C.Structure):
+    """One stone of a batched launch (GpuBatchItem, gpu_backend/mod.rs:246)."""
+
+    _fields_ = [
+        ("scene", C.POINTER(Scene)),
+        ("sample_offset", C.c_uint32),
+        ("spp", C.c_uint32),
+        ("accum_xyz", C.POINTER(C.c_double)),
+        ("status", C.c_int32),
+    ]
+
+
+class TimingInfo(C.Structure):
+    _fields_ = [
+        ("kernel_ms", C.c_float),
+        ("reduce_ms", C.c_float),
+        ("paths", C.c_uint64),
+        ("launches", C.c_uint32),
+    ]
+
+
+def floats(values) -> C.Array:
+    arr = (C.c_float * len(values))()
+    for i, v in enumerate(values):
+        arr[i] = float(v)
+    return arr

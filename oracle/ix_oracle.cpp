@@ -1,0 +1,1441 @@
+// ix_oracle.cpp -- TEST INFRASTRUCTURE ONLY: the CPU oracle.
+//
+// A C++ restatement of the reference's CPU spectral tracer, used by the test suite as
+// the parity checker and by the benchmark as the reported CPU baseline.  It is never
+// linked into, loaded by or called from the CUDA backend.
+//
+// Rounding discipline (the reference's determinism contract, simd/mod.rs:1-27):
+//   * built with -ffp-contract=off, so `a * b + c` rounds twice exactly like the Rust
+//     source; std::fma is used exactly where the reference calls `mul_add`;
+//   * glam's scalar operation order (glam =0.34.1, not vendored): left-associated dot
+//     products `(x*x' + y*y') + z*z'`, cross `(y*z' - y'*z, ...)`, normalize as
+//     `v * (1 / sqrt(dot(v, v)))`, Mat4 * Vec4 as `((c0*x + c1*y) + c2*z) + c3*w`;
+//   * the same libm calls (sinf, cosf, atan2f, atanf, acosf, tanf, expf) that Rust's
+//     std makes on Linux;  f32::midpoint through f64 as Rust's core does on x86_64.
+// Every function names the reference file:line it restates.
+//
+// Built twice: normally (F = float) and with -DIX_COUNT_FLOPS, where F is a wrapper
+// that tallies every floating-point operation so the algorithmic FLOPs per path can be
+// counted on the same inputs the GPU runs.
+
+#include "ix_oracle.h"
+#include "../include/ix_cie_tables.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace ixo {
+
+// ------------------------------------------------------------------------------------
+// The scalar type.
+// ------------------------------------------------------------------------------------
+#ifdef IX_COUNT_FLOPS
+struct Counters {
+    uint64_t add = 0, mul = 0, fma = 0, div = 0, sqrt = 0, transc = 0;
+};
+thread_local Counters g_cnt;
+struct F {
+    float v;
+    F() = default;
+    F(float x) : v(x) {}  // NOLINT: implicit by design so literals mix freely
+};
+static inline F operator+(F a, F b) { g_cnt.add++; return F(a.v + b.v); }
+static inline F operator-(F a, F b) { g_cnt.add++; return F(a.v - b.v); }
+static inline F operator*(F a, F b) { g_cnt.mul++; return F(a.v * b.v); }
+static inline F operator/(F a, F b) { g_cnt.div++; return F(a.v / b.v); }
+static inline F operator-(F a) { return F(-a.v); }
+static inline F& operator+=(F& a, F b) { a = a + b; return a; }
+static inline F& operator*=(F& a, F b) { a = a * b; return a; }
+static inline F& operator/=(F& a, F b) { a = a / b; return a; }
+static inline bool operator<(F a, F b) { return a.v < b.v; }
+static inline bool operator>(F a, F b) { return a.v > b.v; }
+static inline bool operator<=(F a, F b) { return a.v <= b.v; }
+static inline bool operator>=(F a, F b) { return a.v >= b.v; }
+static inline float raw(F x) { return x.v; }
+static inline F fma_(F a, F b, F c) { g_cnt.fma++; return F(std::fma(a.v, b.v, c.v)); }
+static inline F sqrt_(F a) { g_cnt.sqrt++; return F(std::sqrt(a.v)); }
+static inline F sin_(F a) { g_cnt.transc++; return F(sinf(a.v)); }
+static inline F cos_(F a) { g_cnt.transc++; return F(cosf(a.v)); }
+static inline F tan_(F a) { g_cnt.transc++; return F(tanf(a.v)); }
+static inline F atan_(F a) { g_cnt.transc++; return F(atanf(a.v)); }
+static inline F atan2_(F a, F b) { g_cnt.transc++; return F(atan2f(a.v, b.v)); }
+static inline F acos_(F a) { g_cnt.transc++; return F(acosf(a.v)); }
+static inline F exp_(F a) { g_cnt.transc++; return F(expf(a.v)); }
+static inline F midpoint_(F a, F b) {
+    g_cnt.add++; g_cnt.mul++;
+    return F((float)(((double)a.v + (double)b.v) / 2.0));
+}
+#else
+using F = float;
+static inline float raw(F x) { return x; }
+static inline F fma_(F a, F b, F c) { return std::fma(a, b, c); }
+static inline F sqrt_(F a) { return std::sqrt(a); }
+static inline F sin_(F a) { return sinf(a); }
+static inline F cos_(F a) { return cosf(a); }
+static inline F tan_(F a) { return tanf(a); }
+static inline F atan_(F a) { return atanf(a); }
+static inline F atan2_(F a, F b) { return atan2f(a, b); }
+static inline F acos_(F a) { return acosf(a); }
+static inline F exp_(F a) { return expf(a); }
+// f32::midpoint on x86_64: ((a as f64 + b as f64) / 2.0) as f32.
+static inline F midpoint_(F a, F b) { return (float)(((double)a + (double)b) / 2.0); }
+#endif
+
+// f32::max / f32::min are IEEE maxNum/minNum (a NaN operand yields the other one).
+static inline F max_(F a, F b) { return F(fmaxf(raw(a), raw(b))); }
+static inline F min_(F a, F b) { return F(fminf(raw(a), raw(b))); }
+static inline F abs_(F a) { return F(fabsf(raw(a))); }
+static inline F floor_(F a) { return F(floorf(raw(a))); }
+// f32::clamp: `if x < lo { lo }` then `if x > hi { hi }` (NaN passes through).
+static inline F clamp_(F x, F lo, F hi) {
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
+}
+static inline bool is_finite_(F x) { return std::isfinite(raw(x)); }
+static inline F fromu(uint32_t u) { return F((float)u); }
+
+// ------------------------------------------------------------------------------------
+// glam Vec3 (scalar operation order).
+// ------------------------------------------------------------------------------------
+struct V3 {
+    F x, y, z;
+};
+static inline V3 v3(F x, F y, F z) { return V3{x, y, z}; }
+static inline V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
+static inline V3 operator*(V3 a, F s) { return v3(a.x * s, a.y * s, a.z * s); }
+static inline V3 operator*(F s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
+static inline V3 mulv(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline F dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+static inline V3 cross(V3 a, V3 b) {
+    return v3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+static inline F length_squared(V3 a) { return dot(a, a); }
+static inline V3 normalize(V3 a) {
+    F rcp = F(1.0f) / sqrt_(dot(a, a));
+    return a * rcp;
+}
+static inline V3 normalize_or_zero(V3 a) {
+    F rcp = F(1.0f) / sqrt_(dot(a, a));
+    if (is_finite_(rcp) && rcp > F(0.0f)) return a * rcp;
+    return v3(0.0f, 0.0f, 0.0f);
+}
+static inline V3 vmax0(V3 a) {
+    return v3(max_(a.x, 0.0f), max_(a.y, 0.0f), max_(a.z, 0.0f));
+}
+static inline V3 load3(const float* p) { return v3(p[0], p[1], p[2]); }
+static inline void store3(float* p, V3 v) {
+    p[0] = raw(v.x);
+    p[1] = raw(v.y);
+    p[2] = raw(v.z);
+}
+
+// ------------------------------------------------------------------------------------
+// Stokes vector and the Mueller matrices (optics/polarization.rs:9-191).
+// A 4x4 is stored column-major as glam's Mat4 (from_cols_array).
+// ------------------------------------------------------------------------------------
+struct Stokes {
+    F i, q, u, v;
+};
+struct M4 {
+    F c[16];
+};
+static inline Stokes unpolarized(F i) { return Stokes{i, 0.0f, 0.0f, 0.0f}; }
+static inline F intensity(const Stokes& s) { return max_(s.i, 0.0f); }
+static inline Stokes scale(const Stokes& s, F k) {
+    return Stokes{s.i * k, s.q * k, s.u * k, s.v * k};
+}
+// glam Mat4::mul_vec4: ((col0*x + col1*y) + col2*z) + col3*w, element-wise.
+static inline Stokes apply(const M4& m, const Stokes& s) {
+    Stokes o;
+    o.i = ((m.c[0] * s.i + m.c[4] * s.q) + m.c[8] * s.u) + m.c[12] * s.v;
+    o.q = ((m.c[1] * s.i + m.c[5] * s.q) + m.c[9] * s.u) + m.c[13] * s.v;
+    o.u = ((m.c[2] * s.i + m.c[6] * s.q) + m.c[10] * s.u) + m.c[14] * s.v;
+    o.v = ((m.c[3] * s.i + m.c[7] * s.q) + m.c[11] * s.u) + m.c[15] * s.v;
+    return o;
+}
+// MuellerMatrix::frame_rotation (polarization.rs:138).
+static M4 frame_rotation(F psi) {
+    F c2 = cos_(F(2.0f) * psi);
+    F s2 = sin_(F(2.0f) * psi);
+    return M4{{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, c2, -s2, 0.0f, 0.0f, s2, c2, 0.0f, 0.0f, 0.0f,
+               0.0f, 1.0f}};
+}
+// MuellerMatrix::fresnel_reflection (polarization.rs:148).
+static M4 fresnel_reflection(F r_s, F r_p) {
+    F rs2 = r_s * r_s;
+    F rp2 = r_p * r_p;
+    F a = midpoint_(rs2, rp2);
+    F b = F(0.5f) * (rs2 - rp2);
+    F c = r_s * r_p;
+    return M4{{a, b, 0.0f, 0.0f, b, a, 0.0f, 0.0f, 0.0f, 0.0f, c, 0.0f, 0.0f, 0.0f, 0.0f, c}};
+}
+// MuellerMatrix::fresnel_transmission (polarization.rs:162).
+static M4 fresnel_transmission(F n1, F n2, F cos_i, F cos_t, F t_s, F t_p) {
+    F factor = (n2 * cos_t) / max_(n1 * cos_i, 1e-6f);
+    F ts2 = t_s * t_s * factor;
+    F tp2 = t_p * t_p * factor;
+    F a = midpoint_(ts2, tp2);
+    F b = F(0.5f) * (ts2 - tp2);
+    F c = t_s * t_p * factor;
+    return M4{{a, b, 0.0f, 0.0f, b, a, 0.0f, 0.0f, 0.0f, 0.0f, c, 0.0f, 0.0f, 0.0f, 0.0f, c}};
+}
+// MuellerMatrix::tir_retardation (polarization.rs:184).
+static M4 tir_retardation(F delta) {
+    F cd = cos_(delta);
+    F sd = sin_(delta);
+    return M4{{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, cd, -sd, 0.0f, 0.0f,
+               sd, cd}};
+}
+
+// ------------------------------------------------------------------------------------
+// sampling.rs
+// ------------------------------------------------------------------------------------
+static const uint32_t FRESNEL_BRANCH_STREAM = 0x9E3779B1u;     // sampling.rs:13
+static const uint32_t RUSSIAN_ROULETTE_STREAM = 0x517CC1B7u;   // sampling.rs:14
+static const uint32_t PIXEL_JITTER_X_ROTATION_STREAM = 0xA511E9B3u;  // sampling.rs:95
+static const uint32_t PIXEL_JITTER_Y_ROTATION_STREAM = 0x63D81B23u;  // sampling.rs:97
+static const uint32_t HERO_WAVELENGTH_ROTATION_STREAM = 0x1B873593u; // sampling.rs:99
+
+// hash_u32 (sampling.rs:66).
+static inline uint32_t hash_u32(uint32_t x) {
+    x *= 0x85EBCA6Bu;
+    x ^= x >> 13;
+    x *= 0xC2B2AE35u;
+    x ^= x >> 16;
+    return x;
+}
+static inline uint32_t reverse_bits(uint32_t v) {
+    uint32_t r = 0;
+    for (int i = 0; i < 32; ++i) {
+        r = (r << 1) | (v & 1u);
+        v >>= 1;
+    }
+    return r;
+}
+// `(x as f32) / 4_294_967_295.0`: the literal rounds to 2^32 in f32.
+static inline F unit_from_hash(uint32_t h) { return fromu(h) / F(4294967296.0f); }
+// unit_draw (transport/inner/bounce_body.rs:71-73), the per-bounce stream draw.
+static inline F unit_draw(uint32_t seed, uint32_t bounce, uint32_t stream) {
+    return unit_from_hash(hash_u32(seed ^ hash_u32(bounce ^ stream)));
+}
+// low_discrepancy_base2 (sampling.rs:110).
+static inline F low_discrepancy_base2(uint32_t n) {
+    return fromu(reverse_bits(n)) / F(4294967296.0f);
+}
+// radical_inverse_base (sampling.rs:127).
+static inline F radical_inverse_base(uint32_t n, uint32_t base) {
+    uint32_t remaining = n;
+    F val = 0.0f;
+    F inv_base = F(1.0f) / fromu(base);
+    while (remaining > 0) {
+        uint32_t digit = remaining % base;
+        val = fma_(fromu(digit), inv_base, val);
+        inv_base = inv_base / fromu(base);
+        remaining /= base;
+    }
+    return val;
+}
+// cranley_patterson_rotate (sampling.rs:148).
+static inline F cranley_patterson_rotate(F x, F offset) {
+    F sum = x + offset;
+    return sum - floor_(sum);
+}
+struct Rot {
+    F jx, jy, hero;
+};
+// pixel_rotations (sampling.rs:176).
+static inline Rot pixel_rotations(uint32_t pixel) {
+    return Rot{low_discrepancy_base2(hash_u32(pixel ^ PIXEL_JITTER_X_ROTATION_STREAM)),
+               low_discrepancy_base2(hash_u32(pixel ^ PIXEL_JITTER_Y_ROTATION_STREAM)),
+               low_discrepancy_base2(hash_u32(pixel ^ HERO_WAVELENGTH_ROTATION_STREAM))};
+}
+struct Draws {
+    uint32_t seed;
+    F jx, jy, hero;
+};
+// sample_draws (sampling.rs:206).
+static inline Draws sample_draws(uint32_t pixel, uint32_t sample, const Rot& rot) {
+    Draws d;
+    d.seed = hash_u32((pixel * 0x9E3779B9u) ^ (sample * 0x85EBCA6Bu));
+    d.jx = cranley_patterson_rotate(low_discrepancy_base2(sample), rot.jx) - F(0.5f);
+    d.jy = cranley_patterson_rotate(radical_inverse_base(sample, 3), rot.jy) - F(0.5f);
+    d.hero = cranley_patterson_rotate(radical_inverse_base(sample, 5), rot.hero);
+    return d;
+}
+
+// ------------------------------------------------------------------------------------
+// camera.rs
+// ------------------------------------------------------------------------------------
+struct Ray {
+    V3 origin, dir;
+};
+// f32::to_radians: self * (PI / 180.0) with the constant rounded to f32.
+static inline F to_radians(F deg) {
+    return deg * (F(3.14159265358979323846f) / F(180.0f));
+}
+
+// Camera::new (camera.rs:108).
+static void camera_new(F yaw, F pitch, F distance, F fov_deg, ix_camera* out) {
+    F cos_p = cos_(pitch), sin_p = sin_(pitch), cos_y = cos_(yaw), sin_y = sin_(yaw);
+    V3 origin = v3(distance * cos_p * sin_y, distance * sin_p, distance * cos_p * cos_y);
+    V3 forward = normalize(-origin);
+    V3 world_up;
+    if (abs_(cos_p) < F(1e-4f))
+        world_up = v3(0.0f, 0.0f, -1.0f);
+    else if (cos_p < F(0.0f))
+        world_up = v3(0.0f, -1.0f, 0.0f);
+    else
+        world_up = v3(0.0f, 1.0f, 0.0f);
+    V3 right = normalize(cross(forward, world_up));
+    V3 up = normalize(cross(right, forward));
+    F fov_tan = tan_(to_radians(fov_deg) * F(0.5f));
+    store3(out->origin, origin);
+    store3(out->forward, forward);
+    store3(out->right, right);
+    store3(out->up, up);
+    out->fov_tan = raw(fov_tan);
+}
+// Camera::generate_ray (camera.rs:149).
+static inline Ray generate_ray(const ix_camera& c, F sx, F sy, F w, F h, F jx, F jy) {
+    F aspect = w / h;
+    F fov_tan = c.fov_tan;
+    F u = ((sx + jx) / w - F(0.5f)) * F(2.0f) * aspect * fov_tan;
+    F v = (F(0.5f) - (sy + jy) / h) * F(2.0f) * fov_tan;
+    V3 dir = normalize(load3(c.forward) + load3(c.right) * u + load3(c.up) * v);
+    return Ray{load3(c.origin), dir};
+}
+
+// ------------------------------------------------------------------------------------
+// transport/mod.rs:58 -- the wrapped hero comb.
+// ------------------------------------------------------------------------------------
+static inline F rem_euclid(F a, F b) {
+    F r = F(fmodf(raw(a), raw(b)));
+    return (r < F(0.0f)) ? r + abs_(b) : r;
+}
+static inline void hero_wavelengths(F hero_rand, F out[8]) {
+    const F span = 400.0f;
+    const F width = 50.0f;  // 400 / 8
+    F lambda_hero = fma_(hero_rand, span, 380.0f);
+    for (int k = 0; k < 8; ++k) {
+        F offset = fma_(F((float)k), width, lambda_hero - F(380.0f));
+        out[k] = F(380.0f) + rem_euclid(offset, span);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// dispersion.rs:170-210
+// ------------------------------------------------------------------------------------
+static F dispersion_unclamped(const ix_dispersion& d, F lambda_nm) {
+    F um = lambda_nm * F(1e-3f);
+    F l2 = um * um;
+    switch (d.kind) {
+        case IX_DISP_SELLMEIER1: {
+            F n2 = F(1.0f) + (F(d.b[0]) * l2) / (l2 - F(d.c[0]));
+            return sqrt_(max_(n2, 1.0f));
+        }
+        case IX_DISP_SELLMEIER3: {
+            F n2 = 1.0f;
+            n2 += (F(d.b[0]) * l2) / (l2 - F(d.c[0]));
+            n2 += (F(d.b[1]) * l2) / (l2 - F(d.c[1]));
+            n2 += (F(d.b[2]) * l2) / (l2 - F(d.c[2]));
+            return sqrt_(max_(n2, 1.0f));
+        }
+        default: {
+            F l4 = l2 * l2;
+            return max_((F(d.b[0]) + F(d.b[1]) / l2) + F(d.b[2]) / l4, 1.0f);
+        }
+    }
+}
+// DispersionModel::min_valid_nm (dispersion.rs:149).
+static F dispersion_min_valid_nm(const ix_dispersion& d) {
+    if (d.kind == IX_DISP_CAUCHY) return 380.0f;
+    int n = (d.kind == IX_DISP_SELLMEIER1) ? 1 : 3;
+    F floor_nm = 300.0f;
+    for (int i = 0; i < n; ++i) {
+        F c = d.c[i];
+        if (c > F(0.0f)) {
+            F pole_nm = sqrt_(c) * F(1e3f);
+            if (pole_nm < F(380.0f)) floor_nm = max_(floor_nm, pole_nm * F(1.05f));
+        }
+    }
+    return min_(floor_nm, 380.0f);
+}
+static F dispersion_eval(const ix_dispersion& d, F lambda_nm) {
+    if (lambda_nm < F(380.0f))
+        return dispersion_unclamped(d, max_(lambda_nm, dispersion_min_valid_nm(d)));
+    return dispersion_unclamped(d, lambda_nm);
+}
+
+// ------------------------------------------------------------------------------------
+// Absorption alpha(lambda) (optics/absorption.rs:108; raytracer/absorption.rs:32) plus
+// the tabulated spline this library adds (ix_scene.h, ix_absorption).
+// ------------------------------------------------------------------------------------
+static F band_eval(const ix_band& b, F lambda_nm) {
+    if (b.shape == IX_BAND_GAUSS_WAVELENGTH) {
+        F t = (lambda_nm - F(b.center_nm)) / F(b.width_nm);
+        return F(b.peak) * exp_(F(-0.5f) * t * t);
+    }
+    F delta_nm = F(b.center_nm) - lambda_nm;
+    F nu_diff = F(1.0e7f) * delta_nm / (lambda_nm * F(b.center_nm));
+    F t = nu_diff / F(b.width_nm);
+    return F(b.peak) * exp_(F(-0.5f) * t * t);
+}
+// Uniform Catmull-Rom through IX_SPLINE_KNOTS knots over [380, 780] nm, end knots
+// repeated, floored at zero.  Segment s covers [380 + s*h, 380 + (s+1)*h], h = 400/15.
+static F spline_eval(const float* knots, F lambda_nm) {
+    const int n = IX_SPLINE_KNOTS;
+    F pos = (clamp_(lambda_nm, 380.0f, 780.0f) - F(380.0f)) * F((float)(n - 1) / 400.0f);
+    int s = (int)raw(floor_(pos));
+    if (s > n - 2) s = n - 2;
+    if (s < 0) s = 0;
+    F t = pos - F((float)s);
+    F p0 = knots[s > 0 ? s - 1 : 0];
+    F p1 = knots[s];
+    F p2 = knots[s + 1];
+    F p3 = knots[s + 2 < n ? s + 2 : n - 1];
+    // 0.5 * (2 p1 + (p2 - p0) t + (2 p0 - 5 p1 + 4 p2 - p3) t^2 + (3 p1 - p0 - 3 p2 + p3) t^3)
+    F a = F(3.0f) * p1 - p0 - F(3.0f) * p2 + p3;
+    F b = F(2.0f) * p0 - F(5.0f) * p1 + F(4.0f) * p2 - p3;
+    F c = p2 - p0;
+    F poly = fma_(fma_(fma_(a, t, b), t, c), t, F(2.0f) * p1);
+    return max_(F(0.5f) * poly, 0.0f);
+}
+static F spectral_absorption(const ix_absorption& a, F lambda_nm) {
+    F sum = 0.0f;
+    bool first = true;
+    for (uint32_t i = 0; i < a.n_bands && i < IX_MAX_BANDS; ++i) {
+        F v = band_eval(a.bands[i], lambda_nm);
+        sum = first ? v : sum + v;
+        first = false;
+    }
+    if (a.has_spline) sum = first ? spline_eval(a.spline, lambda_nm) : sum + spline_eval(a.spline, lambda_nm);
+    return sum;
+}
+static bool absorption_present(const ix_absorption& a) {
+    if (a.has_spline) return true;
+    for (uint32_t i = 0; i < a.n_bands && i < IX_MAX_BANDS; ++i)
+        if (a.bands[i].peak != 0.0f) return true;
+    return false;
+}
+
+// simd/exp_poly.rs:37 -- the Cephes-style polynomial exponential (Moshier), with the
+// reference's own constants and its AVX2 min/max clamp semantics.
+static F exp_lane(F x) {
+    const F LOG2E = 1.44269504088896340736f;
+    uint32_t c1bits = 0x3F318000u;
+    float c1f;
+    std::memcpy(&c1f, &c1bits, 4);
+    const F C1 = c1f;
+    const F C2 = -2.1219444e-4f;
+    const F P0 = 1.9875691e-4f, P1 = 1.3981999e-3f, P2 = 8.333452e-3f, P3 = 4.1665796e-2f,
+            P4 = 1.6666665e-1f, P5 = 5.0000003e-1f;
+    const F HI = 88.02875f, LO = -87.33654f;
+    F upper = (x < HI) ? x : HI;
+    x = (upper > LO) ? upper : LO;
+    F n = floor_(fma_(x, LOG2E, 0.5f));
+    x = fma_(n, -C1, x);
+    x = fma_(n, -C2, x);
+    F z = x * x;
+    F p = P0;
+    p = fma_(p, x, P1);
+    p = fma_(p, x, P2);
+    p = fma_(p, x, P3);
+    p = fma_(p, x, P4);
+    p = fma_(p, x, P5);
+    p = fma_(p, z, x) + F(1.0f);
+    int32_t e = (int32_t)raw(n);
+    uint32_t bits = (uint32_t)((e + 127) << 23);
+    float pow2n;
+    std::memcpy(&pow2n, &bits, 4);
+    return p * F(pow2n);
+}
+
+// ------------------------------------------------------------------------------------
+// Colour (color/cie1931.rs:157-199; optics/raytracer/color.rs:85-180, 219-329).
+// ------------------------------------------------------------------------------------
+static const float CMF[81][3] = IX_CIE1931_CMF_INIT;
+static const float D65[41] = IX_CIE_D65_SPD_INIT;
+static const float D65_UV[9] = IX_CIE_D65_UV_SPD_INIT;
+
+static V3 cmf(F lambda_nm) {
+    if (!(lambda_nm >= F(380.0f) && lambda_nm <= F(780.0f))) return v3(0.0f, 0.0f, 0.0f);
+    F position = (lambda_nm - F(380.0f)) / F(5.0f);
+    int i0 = (int)raw(floor_(position));
+    if (i0 > 79) i0 = 79;
+    F t = position - F((float)i0);
+    const float* lo = CMF[i0];
+    const float* hi = CMF[i0 + 1];
+    return v3(F(lo[0]) + (F(hi[0]) - F(lo[0])) * t, F(lo[1]) + (F(hi[1]) - F(lo[1])) * t,
+              F(lo[2]) + (F(hi[2]) - F(lo[2])) * t);
+}
+// d65_relative_spectral_power (environment/spectral.rs:28).
+static F d65(F lambda_nm) {
+    if (lambda_nm < F(380.0f)) {
+        F clamped = max_(lambda_nm, 300.0f);
+        F position = (clamped - F(300.0f)) / F(10.0f);
+        int i0 = (int)raw(floor_(position));
+        if (i0 > 7) i0 = 7;
+        F frac = position - F((float)i0);
+        F v0 = D65_UV[i0], v1 = D65_UV[i0 + 1];
+        return fma_(frac, v1 - v0, v0) / F(100.0f);
+    }
+    F clamped = clamp_(lambda_nm, 380.0f, fma_(10.0f, 40.0f, 380.0f));
+    F position = (clamped - F(380.0f)) / F(10.0f);
+    int i0 = (int)raw(floor_(position));
+    if (i0 > 39) i0 = 39;
+    F frac = position - F((float)i0);
+    F v0 = D65[i0], v1 = D65[i0 + 1];
+    return fma_(frac, v1 - v0, v0) / F(100.0f);
+}
+// powi with a constant exponent: LLVM's binary decomposition (and compiler-rt's
+// __powisf2), `res *= x^(2^i)` for the set bits in ascending order.
+static F powi_(F x, unsigned n) {
+    bool have = false;
+    F res = 1.0f;
+    F sq = x;
+    while (n) {
+        if (n & 1u) {
+            res = have ? res * sq : sq;
+            have = true;
+        }
+        n >>= 1;
+        if (n) sq = sq * sq;
+    }
+    return res;
+}
+// blackbody_spectrum_with (environment/spectral.rs:62-82).
+static F blackbody(F t_k, F denom_560, F lambda_nm) {
+    F exp_val = exp_(min_(F(14388000.0f) / (lambda_nm * t_k), 80.0f));
+    F denom = max_(exp_val - F(1.0f), 1e-6f);
+    F ratio = denom_560 / denom;
+    return clamp_(powi_(F(560.0f) / lambda_nm, 5) * ratio, 0.01f, 20.0f);
+}
+static void blackbody_norm(F temp_k, F* t_k, F* denom_560) {
+    *t_k = max_(temp_k, 1000.0f);
+    F exp_560 = exp_(min_(F(14388000.0f) / (F(560.0f) * *t_k), 80.0f));
+    *denom_560 = max_(exp_560 - F(1.0f), 1e-6f);
+}
+static const float BRADFORD_XYZ_TO_LMS[3][3] = {
+    {0.8951f, 0.2664f, -0.1614f}, {-0.7502f, 1.7135f, 0.0367f}, {0.0389f, -0.0685f, 1.0296f}};
+static const float BRADFORD_LMS_TO_XYZ[3][3] = {{0.986993f, -0.147054f, 0.159963f},
+                                                {0.432305f, 0.518360f, 0.049291f},
+                                                {-0.008529f, 0.040043f, 0.968487f}};
+static V3 mat3_fma(const float m[3][3], V3 v) {
+    return v3(fma_(m[0][0], v.x, fma_(m[0][1], v.y, F(m[0][2]) * v.z)),
+              fma_(m[1][0], v.x, fma_(m[1][1], v.y, F(m[1][2]) * v.z)),
+              fma_(m[2][0], v.x, fma_(m[2][1], v.y, F(m[2][2]) * v.z)));
+}
+// compute_illuminant_white_balance (color.rs:277).
+static V3 illuminant_white_balance(F temp_k) {
+    F t_k, den;
+    blackbody_norm(temp_k, &t_k, &den);
+    V3 xyz_w = v3(0.0f, 0.0f, 0.0f);
+    for (int step = 0; step <= 400; ++step) {
+        F lambda = F(380.0f) + F((float)step);
+        xyz_w = xyz_w + cmf(lambda) * blackbody(t_k, den, lambda);
+    }
+    F target_y = max_(xyz_w.y, 1e-6f);
+    const F wx = 0.3127f, wy = 0.3290f;
+    V3 target = v3((wx / wy) * target_y, target_y, ((F(1.0f) - wx - wy) / wy) * target_y);
+    V3 src = mat3_fma(BRADFORD_XYZ_TO_LMS, xyz_w);
+    V3 tgt = mat3_fma(BRADFORD_XYZ_TO_LMS, target);
+    return v3(src.x > F(1e-6f) ? tgt.x / src.x : F(1.0f),
+              src.y > F(1e-6f) ? tgt.y / src.y : F(1.0f),
+              src.z > F(1e-6f) ? tgt.z / src.z : F(1.0f));
+}
+
+// ------------------------------------------------------------------------------------
+// Environment (environment/rig.rs, environment/mod.rs:128-143, optics/studio_rig.rs).
+// ------------------------------------------------------------------------------------
+static inline F smoothstep(F e0, F e1, F x) {
+    F t = clamp_((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * fma_(-2.0f, t, 3.0f);
+}
+static F spectral_power(const ix_environment& env, F lambda_nm) {
+    switch (env.spectrum) {
+        case IX_SPEC_D65: return d65(lambda_nm);
+        case IX_SPEC_BLACKBODY: return blackbody(env.bb_t_k, env.bb_denom_560, lambda_nm);
+        default: return 1.0f;
+    }
+}
+// The direction-only part of the lighting (rig.rs:67-96, 157-170, 320-377), reduced to
+// how radiance(spec_power) is formed from it.
+struct Lighting {
+    int kind;  // 0 scaled, 1 rig, 2 uniform
+    F factor;
+    F bg, softbox, fill;
+    bool has_softbox, has_fill;
+    F ring[IX_RING_LIGHTS];
+    int ring_len;
+    bool has_ground;
+    F horizon, ground;
+};
+static Lighting direction_lighting(const ix_environment& env, V3 dir, V3 observer) {
+    Lighting L;
+    L.kind = 0;
+    L.has_softbox = L.has_fill = L.has_ground = false;
+    L.ring_len = 0;
+    if (env.model == IX_ENV_UNIFORM) {
+        L.kind = 2;
+        return L;
+    }
+    V3 d = normalize(dir);
+    F tray = env.backdrop;
+    if (env.model == IX_ENV_ISO_HEMISPHERE) {
+        F horizon = smoothstep(-0.05f, 0.05f, d.y);
+        F vis = F(1.0f) - smoothstep(env.shadow_cos[0], env.shadow_cos[1], dot(d, observer));
+        if (tray > F(0.0f))
+            L.factor = fma_((F(1.0f) - horizon) * vis, tray, horizon * vis);
+        else
+            L.factor = horizon * vis;
+        return L;
+    }
+    // Studio rig (rig.rs:320-377).
+    L.kind = 1;
+    F exposure = env.exposure;
+    F spot = env.spot_mult;
+    L.bg = env.ambient_fill
+               ? max_(fma_(0.012f, fma_(d.y, 0.5f, 0.5f), 0.015f), 0.005f) * exposure
+               : F(0.0f);
+    F key_dot = max_(dot(d, load3(env.key_dir)), 0.0f);
+    if (key_dot > F(0.0f)) {
+        L.has_softbox = true;
+        L.softbox = powi_(key_dot, 28) * F(12.0f) * spot * exposure;
+    }
+    F fill_dot = max_(dot(d, load3(env.fill_dir)), 0.0f);
+    if (fill_dot > F(0.0f)) {
+        L.has_fill = true;
+        L.fill = powi_(fill_dot, 18) * F(4.5f) * exposure;
+    }
+    for (int i = 0; i < IX_RING_LIGHTS; ++i) {
+        F ring_dot = max_(dot(d, load3(env.ring_dirs[i])), 0.0f);
+        if (ring_dot > F(0.96f)) {
+            F spark = (ring_dot - F(0.96f)) / F(0.04f);
+            L.ring[L.ring_len++] = powi_(spark, 6) * F(22.0f) * spot * exposure;
+        }
+    }
+    if (tray > F(0.0f)) {
+        L.has_ground = true;
+        L.horizon = smoothstep(-0.05f, 0.05f, d.y);
+        L.ground = ((F(1.0f) - L.horizon) * tray) * exposure;
+    }
+    return L;
+}
+// DirectionLighting::radiance (rig.rs:112-155).
+static F lighting_radiance(const Lighting& L, const ix_environment& env, F spec) {
+    if (L.kind == 2) return F(env.uniform_radiance) * spec;
+    if (L.kind == 0) return L.factor * (spec * F(env.exposure));
+    F r = L.bg * spec;
+    if (L.has_softbox) r = fma_(L.softbox, spec, r);
+    if (L.has_fill) r = fma_(L.fill, spec, r);
+    for (int i = 0; i < L.ring_len; ++i) r = fma_(L.ring[i], spec, r);
+    if (L.has_ground) return fma_(L.horizon, r, L.ground * spec);
+    return r;
+}
+static void environment_channels(const ix_environment& env, V3 dir, const F lambdas[8],
+                                 V3 observer, F out[8]) {
+    Lighting L = direction_lighting(env, dir, observer);
+    for (int k = 0; k < 8; ++k) out[k] = lighting_radiance(L, env, spectral_power(env, lambdas[k]));
+}
+static F environment_channel(const ix_environment& env, V3 dir, F lambda, V3 observer) {
+    Lighting L = direction_lighting(env, dir, observer);
+    return lighting_radiance(L, env, spectral_power(env, lambda));
+}
+
+// ------------------------------------------------------------------------------------
+// Intersection (simd/slab.rs:120-160, intersect.rs:101-127).
+// ------------------------------------------------------------------------------------
+struct Hit {
+    F t;
+    V3 normal;
+    int facet;
+};
+static bool intersect(const float* planes, uint32_t n, const Ray& ray, Hit* hit) {
+    F t_near = -1e30f, t_far = 1e30f;
+    int near_idx = -1, far_idx = -1;
+    for (uint32_t i = 0; i < n; ++i) {
+        V3 nrm = load3(planes + 4 * i);
+        F denom = dot(nrm, ray.dir);
+        F side = F(planes[4 * i + 3]) + dot(nrm, ray.origin);
+        F t = (-side) / denom;
+        if (abs_(denom) > F(1e-7f)) {
+            if (denom < F(0.0f)) {
+                if (t > t_near) {
+                    t_near = t;
+                    near_idx = (int)i;
+                }
+            } else if (t < t_far) {
+                t_far = t;
+                far_idx = (int)i;
+            }
+        } else if (side > F(0.0f)) {
+            return false;
+        }
+    }
+    if (t_near > t_far) return false;
+    if (t_near > F(1e-4f)) {
+        hit->t = t_near;
+        hit->normal = near_idx >= 0 ? load3(planes + 4 * near_idx) : v3(0.0f, 0.0f, 0.0f);
+        hit->facet = near_idx >= 0 ? near_idx : 0;
+        return true;
+    }
+    if (t_far > F(1e-4f)) {
+        hit->t = t_far;
+        hit->normal = far_idx >= 0 ? load3(planes + 4 * far_idx) : v3(0.0f, 0.0f, 0.0f);
+        hit->facet = far_idx >= 0 ? far_idx : 0;
+        return true;
+    }
+    return false;
+}
+
+// shading_normal_near_edge (intersect.rs:196).
+static V3 shading_normal_near_edge(const float* planes, uint32_t n, V3 hit_point, int facet,
+                                   V3 hit_normal, F radius) {
+    if (radius <= F(0.0f)) return hit_normal;
+    F nearest = INFINITY;
+    V3 nearest_normal = hit_normal;
+    for (uint32_t i = 0; i < n; ++i) {
+        if ((int)i == facet) continue;
+        V3 nrm = load3(planes + 4 * i);
+        F dist = -(F(planes[4 * i + 3]) + dot(nrm, hit_point));
+        if (dist < nearest) {
+            nearest = dist;
+            nearest_normal = nrm;
+        }
+    }
+    if (nearest >= radius) return hit_normal;
+    F t = clamp_(F(1.0f) - nearest / radius, 0.0f, 1.0f);
+    F smooth_t = t * t * fma_(2.0f, -t, 3.0f);
+    V3 bis = normalize_or_zero(hit_normal + nearest_normal);
+    return normalize_or_zero(hit_normal * (F(1.0f) - smooth_t) + bis * smooth_t);
+}
+
+// ------------------------------------------------------------------------------------
+// Refraction helpers (refraction/{tir,dispatch,reflect_refract,exit_split}.rs).
+// ------------------------------------------------------------------------------------
+static const F DIRECTION_MATCH_COS_TOL = 1.0f - 1e-6f;  // refraction/mod.rs:137
+static const F R_UNPOL_PDF_MIN = 1e-4f;                  // refraction/mod.rs:143
+static const F R_UNPOL_PDF_MAX = 1.0f - 1e-4f;           // refraction/mod.rs:146
+static const F R_UNPOL_SELECT_MIN = 0.02f;               // refraction/mod.rs:153
+static const F R_UNPOL_SELECT_MAX = 0.98f;               // refraction/mod.rs:156
+
+// tir_phase_delta (refraction/tir.rs:33).
+static inline F tir_phase_delta(F n1k, F cos_i, F sin_i) {
+    F tan_half = (cos_i * sqrt_(max_(fma_(n1k * n1k * sin_i, sin_i, -1.0f), 0.0f))) /
+                 max_(n1k * sin_i * sin_i, 1e-6f);
+    return F(2.0f) * atan_(tan_half);
+}
+static inline void fresnel_rs_rp(F n1, F n2, F cos_i, F cos_t, F* r_s, F* r_p) {
+    *r_s = fma_(n2, -cos_t, n1 * cos_i) / fma_(n2, cos_t, n1 * cos_i);
+    *r_p = fma_(n1, -cos_t, n2 * cos_i) / fma_(n1, cos_t, n2 * cos_i);
+}
+static inline F r_unpol_of(F r_s, F r_p) { return F(0.5f) * fma_(r_p, r_p, r_s * r_s); }
+static inline V3 reflect(V3 k, V3 n) { return k - F(2.0f) * dot(k, n) * n; }
+
+// ------------------------------------------------------------------------------------
+// One traced path (transport/inner/bounce_body.rs:216-764, isotropic material).
+// ------------------------------------------------------------------------------------
+struct Path {
+    const ix_scene* sc;
+    uint32_t seed;
+    F lambdas[8];
+    F n_ch[8];
+    F alpha_ch_o[8];
+    bool absorbing;
+    Stokes stokes[8];
+    F radiance[8];
+    F path_pdf[8];
+    F split[8];
+    uint8_t compat[8];
+    Ray ray;
+    V3 k;
+    bool inside;
+    bool has_prev;
+    V3 prev_pn;
+    bool escaped;
+    V3 observer;
+    uint32_t splits;
+};
+
+// try_split_exit_channel (refraction/exit_split.rs:128).
+static void try_split_exit_channel(Path& P, V3 hit_point, int k, V3 dir_k, F transmitted_i) {
+    Ray probe{hit_point + dir_k * F(1e-4f), dir_k};
+    Hit h;
+    if (intersect(P.sc->planes, P.sc->n_planes, probe, &h)) return;
+    F env = environment_channel(P.sc->environment, dir_k, P.lambdas[k], P.observer);
+    P.split[k] = fma_(max_(transmitted_i, 0.0f) * F(1.0f), env, P.split[k]);
+    P.splits++;
+}
+
+// apply_refract_bounce + apply_refract_channel (refraction/reflect_refract.rs:121-591) for
+// an isotropic medium.  Returns the new direction.
+static V3 apply_refract_bounce(Path& P, F r_unpol, F cos_i, F n1, F n2, const F n1_ch[8],
+                               const F n2_ch[8], V3 k_hat, V3 normal, V3 hit_point) {
+    F eta_dir = n1 / n2;
+    F sin2_t_dir = min_(eta_dir * eta_dir * fma_(cos_i, -cos_i, 1.0f), 1.0f);
+    F cos_t_dir = sqrt_(max_(F(1.0f) - sin2_t_dir, 0.0f));
+    V3 final_refr = normalize(eta_dir * k_hat + fma_(eta_dir, cos_i, -cos_t_dir) * normal);
+    V3 dirs[8];
+    bool have_dir[8];
+    bool hero_match[8];
+    for (int c = 0; c < 8; ++c) {
+        Stokes original = P.stokes[c];
+        F n1k = n1_ch[c], n2k = n2_ch[c];
+        F ratio = n1k / n2k;
+        F sin2_t_k = (ratio * ratio) * fma_(cos_i, -cos_i, 1.0f);
+        if (sin2_t_k > F(1.0f)) {
+            P.stokes[c] = scale(P.stokes[c], 0.0f);
+            P.path_pdf[c] = 0.0f;
+            have_dir[c] = false;
+            hero_match[c] = false;
+            continue;
+        }
+        F cos_t_k = sqrt_(max_(F(1.0f) - sin2_t_k, 0.0f));
+        F eta_k = n1k / n2k;
+        V3 refr_k = normalize(eta_k * k_hat + fma_(eta_k, cos_i, -cos_t_k) * normal);
+        bool matches = dot(refr_k, final_refr) >= DIRECTION_MATCH_COS_TOL;
+        // Transmission at this channel's own index (exit_split.rs:69 / reflect_refract.rs:362).
+        F two_n1_cos = F(2.0f) * n1k * cos_i;
+        F t_s = two_n1_cos / fma_(n2k, cos_t_k, n1k * cos_i);
+        F t_p = two_n1_cos / fma_(n1k, cos_t_k, n2k * cos_i);
+        M4 tm = fresnel_transmission(n1k, n2k, cos_i, cos_t_k, t_s, t_p);
+        Stokes transmitted = scale(apply(tm, original), F(1.0f) / (F(1.0f) - r_unpol));
+        F r_s, r_p;
+        fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, &r_s, &r_p);
+        F r_unpol_k = clamp_(r_unpol_of(r_s, r_p), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+        if (matches) {
+            P.stokes[c] = transmitted;
+            P.path_pdf[c] = P.path_pdf[c] * (F(1.0f) - r_unpol_k);
+        } else {
+            // apply_channel_chromatic_termination (reflect_refract.rs:444).
+            F prefix = P.path_pdf[c];
+            P.stokes[c] = scale(P.stokes[c], 0.0f);
+            P.path_pdf[c] = prefix * (F(1.0f) - r_unpol_k);
+            bool is_exit = P.inside;
+            if (is_exit && intensity(original) > F(0.0f))
+                try_split_exit_channel(P, hit_point, c, refr_k, intensity(transmitted));
+        }
+        dirs[c] = refr_k;
+        have_dir[c] = true;
+        hero_match[c] = matches;
+    }
+    if (!P.inside) {
+        // narrow_compat (refraction/context.rs:219), hero = 0.
+        for (int a = 0; a < 8; ++a)
+            for (int b = a + 1; b < 8; ++b) {
+                bool m;
+                if (a == 0)
+                    m = hero_match[b];
+                else if (have_dir[a] && have_dir[b])
+                    m = dot(dirs[a], dirs[b]) >= DIRECTION_MATCH_COS_TOL;
+                else
+                    m = true;
+                if (!m) {
+                    P.compat[a] &= (uint8_t)~(1u << b);
+                    P.compat[b] &= (uint8_t)~(1u << a);
+                }
+            }
+    }
+    return final_refr;
+}
+
+// apply_absorption for an isotropic material (raytracer/absorption.rs:99, :197).
+static void apply_isotropic_absorption(Path& P, V3 k_hat, F path_len) {
+    const ix_material& m = P.sc->material;
+    V3 c_axis = normalize_or_zero(load3(m.c_axis));
+    // AbsorptionTensor3::uniaxial (birefringence/absorption_tensor.rs:39) basis.
+    V3 ax = (abs_(c_axis.x) > F(0.9f)) ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
+    V3 a1 = normalize_or_zero(ax - c_axis * dot(c_axis, ax));
+    V3 a2 = cross(c_axis, a1);
+    // Eigen polarisations (birefringence/uniaxial.rs:121-140).
+    V3 raw_c = load3(m.c_axis);
+    V3 cr = cross(k_hat, raw_c);
+    V3 ea;
+    if (length_squared(cr) > F(1e-8f)) {
+        ea = normalize(cr);
+    } else {
+        V3 nk = normalize_or_zero(k_hat);
+        V3 ax2 = (abs_(nk.x) > F(0.9f)) ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
+        ea = normalize_or_zero(ax2 - nk * dot(nk, ax2));
+    }
+    V3 eb = normalize_or_zero(cross(k_hat, ea));
+    F la0 = dot(a1, ea), la1 = dot(a2, ea), la2 = dot(c_axis, ea);
+    F lb0 = dot(a1, eb), lb1 = dot(a2, eb), lb2 = dot(c_axis, eb);
+    F scaled_len = path_len * F(m.absorption_path_scale);
+    for (int c = 0; c < 8; ++c) {
+        F ao = P.alpha_ch_o[c];
+        // quadratic_form: alpha.dot(local * local) with alpha = (ao, ao, ae), ae == ao.
+        F qa = (ao * (la0 * la0) + ao * (la1 * la1)) + ao * (la2 * la2);
+        F qb = (ao * (lb0 * lb0) + ao * (lb1 * lb1)) + ao * (lb2 * lb2);
+        F alpha = midpoint_(qa, qb);
+        F trans = exp_lane(-alpha * scaled_len);
+        P.stokes[c] = scale(P.stokes[c], trans);
+    }
+}
+
+enum { TERM_ESCAPED = 0, TERM_RR = 1, TERM_CAP = 2 };
+
+static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand,
+                     ixo_path_info* info) {
+    Path P;
+    P.sc = sc;
+    P.seed = seed;
+    P.splits = 0;
+    hero_wavelengths(hero_rand, P.lambdas);
+    const ix_material& m = sc->material;
+    P.absorbing = absorption_present(m.abs_o);
+    for (int c = 0; c < 8; ++c) {
+        P.n_ch[c] = dispersion_eval(m.dispersion, P.lambdas[c]);
+        P.alpha_ch_o[c] = P.absorbing ? spectral_absorption(m.abs_o, P.lambdas[c]) : F(0.0f);
+        P.stokes[c] = unpolarized(1.0f);
+        P.radiance[c] = 0.0f;
+        P.path_pdf[c] = 1.0f;
+        P.split[c] = 0.0f;
+        P.compat[c] = 0xFF;
+    }
+    P.ray = initial;
+    P.k = initial.dir;
+    P.inside = false;
+    P.has_prev = false;
+    P.escaped = false;
+    P.observer = -initial.dir;
+    F glare = clamp_(sc->environment.surface_glare, 0.0f, 1.0f);
+    uint32_t term = TERM_CAP;
+    uint32_t bounce = 0;
+    uint32_t iterations = 0;
+    for (bounce = 0; bounce < sc->max_bounces; ++bounce) {
+        iterations = bounce + 1;
+        Hit hit;
+        if (!intersect(sc->planes, sc->n_planes, P.ray, &hit)) {
+            // handle_miss (bounce_body/miss.rs:33) + accumulate_miss_radiance (bounce.rs:40).
+            F env[8];
+            environment_channels(sc->environment, P.ray.dir, P.lambdas, P.observer, env);
+            for (int c = 0; c < 8; ++c)
+                P.radiance[c] = fma_(intensity(P.stokes[c]) * F(1.0f), env[c], P.radiance[c]);
+            P.escaped = true;
+            term = TERM_ESCAPED;
+            break;
+        }
+        // facet_event (bounce_body.rs:611).
+        V3 hit_point = P.ray.origin + hit.t * P.ray.dir;
+        V3 normal = shading_normal_near_edge(sc->planes, sc->n_planes, hit_point, hit.facet,
+                                             hit.normal, m.edge_rounding_radius);
+        // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:69).
+        V3 cpn = normalize_or_zero(cross(P.k, normal));
+        if (P.has_prev && length_squared(cpn) > F(1e-6f) && length_squared(P.prev_pn) > F(1e-6f)) {
+            F cos_psi = clamp_(dot(P.prev_pn, cpn), -1.0f, 1.0f);
+            F sin_psi = dot(cross(P.prev_pn, cpn), normalize_or_zero(P.k));
+            F psi = atan2_(sin_psi, cos_psi);
+            M4 rot = frame_rotation(psi);
+            for (int c = 0; c < 8; ++c) P.stokes[c] = apply(rot, P.stokes[c]);
+        }
+        P.has_prev = true;
+        P.prev_pn = cpn;
+        // apply_interior_segment (transport/inner.rs:170).
+        if (P.inside) {
+            normal = -normal;
+            if (P.absorbing && m.scattering_sigma_s <= 0.0f)
+                apply_isotropic_absorption(P, P.k, hit.t);
+        }
+        // compute_bounce_refraction_geometry (refraction/geometry.rs:306), isotropic.
+        F cos_i = clamp_(dot(-P.k, normal), 0.0f, 1.0f);
+        F sin_i = sqrt_(max_(fma_(cos_i, -cos_i, 1.0f), 0.0f));
+        F n_hero = P.n_ch[0];
+        F n1 = P.inside ? n_hero : F(1.0f);
+        F n2 = P.inside ? F(1.0f) : n_hero;
+        F eta = n1 / n2;
+        F one_minus_c2 = fma_(cos_i, -cos_i, 1.0f);
+        F sin2_t = eta * eta * one_minus_c2;
+        F n1_ch[8], n2_ch[8], sin2_t_ch[8];
+        for (int c = 0; c < 8; ++c) {
+            n1_ch[c] = P.inside ? P.n_ch[c] : F(1.0f);
+            n2_ch[c] = P.inside ? F(1.0f) : P.n_ch[c];
+            F etak = n1_ch[c] / n2_ch[c];
+            sin2_t_ch[c] = etak * etak * fma_(cos_i, -cos_i, 1.0f);
+        }
+        // dispatch_bounce (transport/bounce.rs:108).
+        V3 new_dir;
+        bool new_inside = P.inside;
+        if (sin2_t > F(1.0f)) {
+            // apply_tir_bounce, isotropic arm (refraction/tir.rs:98-116).
+            for (int c = 0; c < 8; ++c) {
+                F n1k = n1_ch[c], n2k = n2_ch[c];
+                if (sin2_t_ch[c] > F(1.0f)) {
+                    P.stokes[c] = apply(tir_retardation(tir_phase_delta(n1k, cos_i, sin_i)), P.stokes[c]);
+                } else {
+                    F cos_t_k = sqrt_(max_(F(1.0f) - sin2_t_ch[c], 0.0f));
+                    F r_s, r_p;
+                    fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, &r_s, &r_p);
+                    P.stokes[c] = apply(fresnel_reflection(r_s, r_p), P.stokes[c]);
+                    P.path_pdf[c] = P.path_pdf[c] *
+                                    clamp_(r_unpol_of(r_s, r_p), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+                }
+            }
+            new_dir = reflect(P.k, normal);
+        } else {
+            // apply_partial_fresnel_bounce (refraction/dispatch.rs:307).
+            F cos_t = sqrt_(max_(F(1.0f) - sin2_t, 0.0f));
+            F r_s, r_p;
+            fresnel_rs_rp(n1, n2, cos_i, cos_t, &r_s, &r_p);
+            F r_unpol = clamp_(r_unpol_of(r_s, r_p), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
+            F rng = unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM);
+            if (rng < r_unpol) {
+                // apply_partial_reflect_bounce (reflect_refract.rs:33).
+                for (int c = 0; c < 8; ++c) {
+                    F n1k = n1_ch[c], n2k = n2_ch[c];
+                    M4 mm;
+                    if (sin2_t_ch[c] > F(1.0f)) {
+                        mm = tir_retardation(tir_phase_delta(n1k, cos_i, sin_i));
+                    } else {
+                        F cos_t_k = sqrt_(max_(F(1.0f) - sin2_t_ch[c], 0.0f));
+                        F rs, rp;
+                        fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, &rs, &rp);
+                        F r_unpol_k = clamp_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+                        P.path_pdf[c] = P.path_pdf[c] * r_unpol_k;
+                        mm = fresnel_reflection(rs, rp);
+                    }
+                    P.stokes[c] = scale(apply(mm, P.stokes[c]), F(1.0f) / r_unpol);
+                }
+                new_dir = reflect(P.k, normal);
+            } else {
+                new_dir = apply_refract_bounce(P, r_unpol, cos_i, n1, n2, n1_ch, n2_ch, P.k,
+                                               normal, hit_point);
+                new_inside = !P.inside;
+            }
+        }
+        P.ray.dir = new_dir;
+        P.ray.origin = hit_point + new_dir * F(1e-4f);
+        P.k = new_dir;
+        P.inside = new_inside;
+        // Surface glare (bounce_body.rs:691-697).
+        if (bounce == 0 && !P.inside && glare < F(1.0f)) {
+            for (int c = 0; c < 8; ++c) P.stokes[c] = scale(P.stokes[c], glare);
+        }
+        // apply_russian_roulette (transport/bounce.rs:355).
+        if (bounce > 4) {
+            F max_i = 0.0f;
+            for (int c = 0; c < 8; ++c) max_i = max_(max_i, intensity(P.stokes[c]));
+            F q = clamp_(max_i, 0.05f, 1.0f);
+            F rr = unit_draw(P.seed, bounce, RUSSIAN_ROULETTE_STREAM);
+            if (rr > q) {
+                term = TERM_RR;
+                break;
+            }
+            for (int c = 0; c < 8; ++c) P.stokes[c] = scale(P.stokes[c], F(1.0f) / q);
+            for (int c = 0; c < 8; ++c) P.split[c] = P.split[c] / q;
+        }
+    }
+    // finish (bounce_body.rs:724).
+    if (P.escaped)
+        for (int c = 0; c < 8; ++c) P.radiance[c] = P.radiance[c] + P.split[c];
+    const F norm_factor = F(50.0f) / F(106.856f);
+    V3 xyz = v3(0.0f, 0.0f, 0.0f);
+    for (int c = 0; c < 8; ++c) {
+        F family = 0.0f;
+        bool first = true;
+        for (int j = 0; j < 8; ++j)
+            if (P.compat[c] & (1u << j)) {
+                family = first ? P.path_pdf[j] : family + P.path_pdf[j];
+                first = false;
+            }
+        F w = (family <= F(1e-12f)) ? F(1.0f) : (F(8.0f) * P.path_pdf[0]) / family;
+        F weighted = P.radiance[c] * w;
+        xyz = xyz + cmf(P.lambdas[c]) * (weighted * norm_factor);
+    }
+    xyz = xyz + v3(0.0f, 0.0f, 0.0f);  // + nee_xyz (always zero without NEE)
+    if (sc->environment.model != IX_ENV_UNIFORM) {
+        // apply_von_kries_white_balance (color.rs:252), run for every Studio environment.
+        V3 lms = mat3_fma(BRADFORD_XYZ_TO_LMS, xyz);
+        V3 wb = sc->environment.white_balance ? load3(sc->environment.wb_lms) : v3(1.0f, 1.0f, 1.0f);
+        xyz = mat3_fma(BRADFORD_LMS_TO_XYZ, mulv(lms, wb));
+    }
+    xyz = vmax0(xyz);
+    if (info) {
+        info->bounces = iterations;
+        info->termination = term;
+        info->escaped = P.escaped ? 1u : 0u;
+        info->exit_splits = P.splits;
+    }
+    return xyz;
+}
+
+static bool scene_supported(const ix_scene* sc) {
+    if (!sc || sc->material.anisotropic) return false;
+    if (sc->n_planes > 0 && !sc->planes) return false;
+    if (sc->material.scattering_sigma_s > 0.0f) return false;
+    for (uint32_t i = 0; i < sc->n_finishes && sc->facet_finishes; ++i)
+        if (sc->facet_finishes[i] != 0) return false;
+    return true;
+}
+
+// cpu_sample_xyz (renderer/cpu_frame.rs:45).
+static V3 sample_xyz(const ix_scene* sc, uint32_t pixel, const Rot& rot, uint32_t sample,
+                     ixo_path_info* info) {
+    uint32_t width = sc->width;
+    uint32_t x = pixel % width, y = pixel / width;
+    Draws d = sample_draws(pixel, sample, rot);
+    Ray ray = generate_ray(sc->camera, F((float)x), F((float)y), F((float)width),
+                           F((float)sc->height), d.jx, d.jy);
+    return trace_path(sc, ray, d.seed, d.hero, info);
+}
+
+static inline bool xyz_finite(V3 v) { return is_finite_(v.x) && is_finite_(v.y) && is_finite_(v.z); }
+
+}  // namespace ixo
+
+using namespace ixo;
+
+extern "C" {
+
+uint32_t ixo_hash_u32(uint32_t x) { return hash_u32(x); }
+float ixo_low_discrepancy_base2(uint32_t n) { return raw(low_discrepancy_base2(n)); }
+float ixo_radical_inverse_base(uint32_t n, uint32_t base) {
+    return raw(radical_inverse_base(n, base));
+}
+void ixo_pixel_rotations(uint32_t pixel, float out[3]) {
+    Rot r = pixel_rotations(pixel);
+    out[0] = raw(r.jx);
+    out[1] = raw(r.jy);
+    out[2] = raw(r.hero);
+}
+void ixo_sample_draws(uint32_t pixel, uint32_t sample, const float rot[3], uint32_t* seed,
+                      float out[3]) {
+    Rot r = rot ? Rot{rot[0], rot[1], rot[2]} : pixel_rotations(pixel);
+    Draws d = sample_draws(pixel, sample, r);
+    *seed = d.seed;
+    out[0] = raw(d.jx);
+    out[1] = raw(d.jy);
+    out[2] = raw(d.hero);
+}
+void ixo_camera_new(float yaw, float pitch, float distance, float fov_deg, ix_camera* out) {
+    camera_new(yaw, pitch, distance, fov_deg, out);
+}
+void ixo_generate_ray(const ix_camera* cam, float sx, float sy, float w, float h, float jx,
+                      float jy, float origin[3], float dir[3]) {
+    Ray r = generate_ray(*cam, sx, sy, w, h, jx, jy);
+    store3(origin, r.origin);
+    store3(dir, r.dir);
+}
+void ixo_hero_wavelengths(float hero_rand, float out[8]) {
+    F l[8];
+    hero_wavelengths(hero_rand, l);
+    for (int k = 0; k < 8; ++k) out[k] = raw(l[k]);
+}
+float ixo_dispersion_eval(const ix_dispersion* d, float lambda_nm) {
+    return raw(dispersion_eval(*d, lambda_nm));
+}
+void ixo_cmf(float lambda_nm, float out[3]) { store3(out, cmf(lambda_nm)); }
+float ixo_d65(float lambda_nm) { return raw(d65(lambda_nm)); }
+float ixo_exp_lane(float x) { return raw(exp_lane(x)); }
+float ixo_tir_phase_delta(float n1, float cos_i, float sin_i) {
+    return raw(tir_phase_delta(n1, cos_i, sin_i));
+}
+void ixo_fresnel_reflect_apply(float r_s, float r_p, const float s_in[4], float s_out[4]) {
+    Stokes s{s_in[0], s_in[1], s_in[2], s_in[3]};
+    Stokes o = apply(fresnel_reflection(r_s, r_p), s);
+    s_out[0] = raw(o.i);
+    s_out[1] = raw(o.q);
+    s_out[2] = raw(o.u);
+    s_out[3] = raw(o.v);
+}
+int ixo_intersect(const float* planes, uint32_t n_planes, const float origin[3],
+                  const float dir[3], float* t, int32_t* facet) {
+    Ray r{load3(origin), load3(dir)};
+    Hit h;
+    if (!intersect(planes, n_planes, r, &h)) return 0;
+    *t = raw(h.t);
+    *facet = h.facet;
+    return 1;
+}
+
+// Lighting presets by the reference's LightingPreset::index (environment/mod.rs:475-493):
+// 1 IsoHemisphere, 7 Daylight, 8 Incandescent, 9 IlluminantA, 10 RingLights,
+// 11 DarkSpotlight.  Parameters from LightingPreset::params (environment/mod.rs:318-411).
+int ixo_environment_preset(int32_t preset, float exposure, float light_yaw, float light_pitch,
+                           float backdrop, float surface_glare, float head_shadow_deg,
+                           ix_environment* out) {
+    std::memset(out, 0, sizeof(*out));
+    float temp_k, spot;
+    bool d65_spec;
+    uint32_t model;
+    switch (preset) {
+        case 1: model = IX_ENV_ISO_HEMISPHERE; temp_k = 6500.0f; spot = 1.0f; d65_spec = true; break;
+        case 7: model = IX_ENV_STUDIO; temp_k = 6500.0f; spot = 1.0f; d65_spec = true; break;
+        case 8: model = IX_ENV_STUDIO; temp_k = 3200.0f; spot = 1.2f; d65_spec = false; break;
+        case 9: model = IX_ENV_STUDIO; temp_k = 2856.0f; spot = 1.2f; d65_spec = false; break;
+        case 10: model = IX_ENV_STUDIO; temp_k = 5000.0f; spot = 1.6f; d65_spec = false; break;
+        case 11: model = IX_ENV_STUDIO; temp_k = 6000.0f; spot = 2.4f; d65_spec = false; break;
+        default: return -1;
+    }
+    out->model = model;
+    out->spectrum = d65_spec ? IX_SPEC_D65 : IX_SPEC_BLACKBODY;
+    out->exposure = exposure;
+    out->spot_mult = spot;
+    out->ambient_fill = 1;
+    out->backdrop = backdrop;
+    // clamp_surface_glare (environment/source.rs:170).
+    out->surface_glare = (surface_glare >= 1.0f || std::isnan(surface_glare)) ? 1.0f
+                         : (surface_glare > 0.0f ? surface_glare : 0.0f);
+    // head_shadow_cosines (environment/mod.rs:128) after clamp_head_shadow_deg (:146).
+    float deg = head_shadow_deg;
+    if (std::isnan(deg)) deg = 16.0f;
+    else if (deg <= 0.0f) deg = 0.0f;
+    else if (deg < 3.0f) deg = 3.0f;
+    else if (deg > 88.0f) deg = 88.0f;
+    if (deg == 16.0f) {
+        out->shadow_cos[0] = 0.9510565f;
+        out->shadow_cos[1] = 0.9702957f;
+    } else if (deg <= 0.0f) {
+        out->shadow_cos[0] = 2.0f;
+        out->shadow_cos[1] = 3.0f;
+    } else {
+        float dd = deg < 3.0f ? 3.0f : (deg > 88.0f ? 88.0f : deg);
+        out->shadow_cos[0] = raw(cos_(to_radians(F(dd) + F(2.0f))));
+        out->shadow_cos[1] = raw(cos_(to_radians(F(dd) - F(2.0f))));
+    }
+    F t_k, den;
+    blackbody_norm(temp_k, &t_k, &den);
+    out->bb_t_k = raw(t_k);
+    out->bb_denom_560 = raw(den);
+    // StudioRig::new (optics/studio_rig.rs:33).
+    F cos_pitch = cos_(light_pitch), sin_pitch = sin_(light_pitch);
+    F cos_yaw = cos_(light_yaw), sin_yaw = sin_(light_yaw);
+    store3(out->key_dir, normalize(v3(cos_pitch * sin_yaw, sin_pitch, cos_pitch * cos_yaw)));
+    const F PI = 3.14159265358979323846f;
+    F fill_yaw = fma_(PI, 0.78f, light_yaw);
+    F fill_pitch = clamp_(F(light_pitch) * F(0.65f), 0.15f, 1.2f);
+    store3(out->fill_dir, normalize(v3(cos_(fill_pitch) * sin_(fill_yaw), sin_(fill_pitch),
+                                       cos_(fill_pitch) * cos_(fill_yaw))));
+    F step = PI * F(2.0f) / F(16.0f);
+    for (int i = 0; i < IX_RING_LIGHTS; ++i) {
+        F angle = fma_(F((float)i), step, light_yaw);
+        store3(out->ring_dirs[i],
+               normalize(v3(sin_(angle) * F(0.75f), sin_pitch * F(0.8f), cos_(angle) * F(0.75f))));
+    }
+    // illuminant_white_balance (color.rs:328): identity unless the preset uses one.
+    if (!d65_spec) {
+        out->white_balance = 1;
+        store3(out->wb_lms, illuminant_white_balance(temp_k));
+    } else {
+        out->white_balance = 0;
+        out->wb_lms[0] = out->wb_lms[1] = out->wb_lms[2] = 1.0f;
+    }
+    out->uniform_radiance = 0.0f;
+    return 0;
+}
+
+void ixo_environment_uniform(float radiance, ix_environment* out) {
+    std::memset(out, 0, sizeof(*out));
+    out->model = IX_ENV_UNIFORM;
+    out->spectrum = IX_SPEC_FLAT;
+    out->exposure = 1.0f;
+    out->surface_glare = 1.0f;
+    out->wb_lms[0] = out->wb_lms[1] = out->wb_lms[2] = 1.0f;
+    out->uniform_radiance = radiance;
+}
+
+float ixo_environment_channel(const ix_environment* env, const float dir[3], float lambda_nm,
+                              const float observer[3]) {
+    return raw(environment_channel(*env, load3(dir), lambda_nm,
+                                   observer ? load3(observer) : v3(0.0f, 0.0f, 0.0f)));
+}
+
+int ixo_trace_ray(const ix_scene* scene, const float origin[3], const float dir[3],
+                  uint32_t seed, float hero_rand, float xyz[3], ixo_path_info* info) {
+    if (!scene_supported(scene)) return -1;
+    Ray r{load3(origin), load3(dir)};
+    store3(xyz, trace_path(scene, r, seed, hero_rand, info));
+    return 0;
+}
+
+int ixo_trace_sample(const ix_scene* scene, uint32_t pixel, uint32_t sample, float xyz[3],
+                     ixo_path_info* info) {
+    if (!scene_supported(scene)) return -1;
+    store3(xyz, sample_xyz(scene, pixel, pixel_rotations(pixel), sample, info));
+    return 0;
+}
+
+int64_t ixo_trace_frame(const ix_scene* scene, uint32_t sample_offset, uint32_t spp,
+                        uint32_t threads, float* sums_f32, double* sums_f64) {
+    if (!scene_supported(scene)) return -1;
+    uint32_t num_pixels = scene->width * scene->height;
+    if (threads == 0) threads = 1;
+    std::vector<int64_t> dropped(threads, 0);
+    auto worker = [&](uint32_t first) {
+        // trace_pixels_interleaved (cpu_frame.rs:104): pixel = first, first + stride, ...
+        for (uint32_t pixel = first; pixel < num_pixels; pixel += threads) {
+            Rot rot = pixel_rotations(pixel);
+            V3 sum = v3(0.0f, 0.0f, 0.0f);
+            double sd[3] = {0.0, 0.0, 0.0};
+            for (uint32_t s = 0; s < spp; ++s) {
+                V3 xyz = sample_xyz(scene, pixel, rot, sample_offset + s, nullptr);
+                // add_finite_sample (sampling.rs:237).
+                if (xyz_finite(xyz)) {
+                    sum = sum + xyz;
+                    sd[0] += (double)raw(xyz.x);
+                    sd[1] += (double)raw(xyz.y);
+                    sd[2] += (double)raw(xyz.z);
+                } else {
+                    dropped[first]++;
+                }
+            }
+            if (sums_f32) store3(sums_f32 + 3 * (size_t)pixel, sum);
+            if (sums_f64) {
+                sums_f64[3 * (size_t)pixel] = sd[0];
+                sums_f64[3 * (size_t)pixel + 1] = sd[1];
+                sums_f64[3 * (size_t)pixel + 2] = sd[2];
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < threads; ++t) pool.emplace_back(worker, t);
+    worker(0);
+    for (auto& th : pool) th.join();
+    int64_t total = 0;
+    for (auto d : dropped) total += d;
+    return total;
+}
+
+int64_t ixo_trace_pixels(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_end,
+                         uint32_t sample_offset, uint32_t spp, uint32_t threads,
+                         double* sums_f64) {
+    if (!scene_supported(scene)) return -1;
+    if (threads == 0) threads = 1;
+    std::vector<int64_t> dropped(threads, 0);
+    auto worker = [&](uint32_t t) {
+        for (uint32_t pixel = pixel_begin + t; pixel < pixel_end; pixel += threads) {
+            Rot rot = pixel_rotations(pixel);
+            double sd[3] = {0.0, 0.0, 0.0};
+            for (uint32_t s = 0; s < spp; ++s) {
+                V3 xyz = sample_xyz(scene, pixel, rot, sample_offset + s, nullptr);
+                if (xyz_finite(xyz)) {
+                    sd[0] += (double)raw(xyz.x);
+                    sd[1] += (double)raw(xyz.y);
+                    sd[2] += (double)raw(xyz.z);
+                } else {
+                    dropped[t]++;
+                }
+            }
+            size_t o = 3 * (size_t)(pixel - pixel_begin);
+            sums_f64[o] = sd[0];
+            sums_f64[o + 1] = sd[1];
+            sums_f64[o + 2] = sd[2];
+        }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < threads; ++t) pool.emplace_back(worker, t);
+    worker(0);
+    for (auto& th : pool) th.join();
+    int64_t total = 0;
+    for (auto d : dropped) total += d;
+    return total;
+}
+
+int ixo_trace_samples(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_end,
+                      uint32_t sample_offset, uint32_t spp, uint32_t threads, float* xyz,
+                      uint32_t* bounces) {
+    if (!scene_supported(scene)) return -1;
+    if (threads == 0) threads = 1;
+    auto worker = [&](uint32_t t) {
+        for (uint32_t pixel = pixel_begin + t; pixel < pixel_end; pixel += threads) {
+            Rot rot = pixel_rotations(pixel);
+            for (uint32_t s = 0; s < spp; ++s) {
+                ixo_path_info info;
+                V3 v = sample_xyz(scene, pixel, rot, sample_offset + s, &info);
+                size_t o = (size_t)(pixel - pixel_begin) * spp + s;
+                store3(xyz + 3 * o, v);
+                if (bounces) bounces[o] = info.bounces;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < threads; ++t) pool.emplace_back(worker, t);
+    worker(0);
+    for (auto& th : pool) th.join();
+    return 0;
+}
+
+uint32_t ixo_standard_round_brilliant(float* out) {
+    const F PI = 3.14159265358979323846f;
+    const F gear = 96.0f;
+    uint32_t n = 0;
+    auto push = [&](V3 nrm, F d) {
+        V3 u = normalize(nrm);  // GpuFacetPlane::new (geometry/plane.rs:44)
+        out[4 * n] = raw(u.x);
+        out[4 * n + 1] = raw(u.y);
+        out[4 * n + 2] = raw(u.z);
+        out[4 * n + 3] = raw(d);
+        ++n;
+    };
+    auto azimuth = [&](F g) { return F(2.0f) * PI * (g + F(0.0f)) / gear; };
+    auto tier = [&](const float* idx, int count, F angle_deg, bool crown, F d) {
+        F a = to_radians(angle_deg);
+        for (int i = 0; i < count; ++i) {
+            F phi = azimuth(idx[i]);
+            V3 nrm = v3(sin_(a) * cos_(phi), crown ? cos_(a) : -cos_(a), sin_(a) * sin_(phi));
+            push(nrm, d);
+        }
+    };
+    static const float stars[8] = {6, 18, 30, 42, 54, 66, 78, 90};
+    static const float mains[8] = {0, 12, 24, 36, 48, 60, 72, 84};
+    static const float halves[16] = {95, 1, 11, 13, 23, 25, 35, 37, 47, 49, 59, 61, 71, 73, 83, 85};
+    push(v3(0.0f, 1.0f, 0.0f), -0.32f);
+    tier(stars, 8, 15.0f, true, -0.45f);
+    tier(mains, 8, 34.5f, true, -0.59f);
+    tier(halves, 16, 41.0f, true, -0.67f);
+    for (int i = 0; i < 16; ++i) {
+        F phi = F(2.0f) * PI * F((float)i) / F(16.0f);
+        push(v3(cos_(phi), 0.0f, sin_(phi)), -1.0f);
+    }
+    tier(mains, 8, 41.0f, false, -0.67f);
+    tier(halves, 16, 42.5f, false, -0.68f);
+    push(v3(0.0f, -1.0f, 0.0f), -0.88f);
+    return n;
+}
+
+int ixo_counting_build(void) {
+#ifdef IX_COUNT_FLOPS
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+int ixo_count_flops(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_end,
+                    uint32_t pixel_step, uint32_t sample_offset, uint32_t spp,
+                    ixo_flop_counts* out) {
+#ifdef IX_COUNT_FLOPS
+    if (!scene_supported(scene)) return -1;
+    g_cnt = Counters();
+    uint64_t paths = 0;
+    if (pixel_step == 0) pixel_step = 1;
+    for (uint32_t pixel = pixel_begin; pixel < pixel_end; pixel += pixel_step) {
+        Rot rot = pixel_rotations(pixel);
+        for (uint32_t s = 0; s < spp; ++s) {
+            (void)sample_xyz(scene, pixel, rot, sample_offset + s, nullptr);
+            ++paths;
+        }
+    }
+    out->add = g_cnt.add;
+    out->mul = g_cnt.mul;
+    out->fma = g_cnt.fma;
+    out->div = g_cnt.div;
+    out->sqrt = g_cnt.sqrt;
+    out->transcendental = g_cnt.transc;
+    out->paths = paths;
+    return 0;
+#else
+    (void)scene; (void)pixel_begin; (void)pixel_end; (void)pixel_step; (void)sample_offset;
+    (void)spp; (void)out;
+    return -1;
+#endif
+}
+
+}  // extern "C"

@@ -1,0 +1,103 @@
+/*
+ * ix_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * The C entry points of the CPU oracle: a restatement, in C++, of the reference's CPU
+ * spectral tracer (crates/indicatrix/src/optics/raytracer, renderer/cpu_frame.rs).
+ * Only the test suite, the smoke check and the benchmark's CPU-baseline leg load this
+ * library, and only as the checker / reported baseline; the CUDA backend never links it.
+ */
+#ifndef IX_ORACLE_H
+#define IX_ORACLE_H
+
+#include <stdint.h>
+#include "../include/ix_scene.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Per-path bookkeeping a test can read beside the XYZ result. */
+typedef struct ixo_path_info {
+    uint32_t bounces;       /* loop iterations run                                   */
+    uint32_t termination;   /* 0 escaped, 1 russian roulette, 2 hit the bounce cap     */
+    uint32_t escaped;       /* the path's own environment lookup ran                   */
+    uint32_t exit_splits;   /* exit-split probes that reached the environment          */
+} ixo_path_info;
+
+typedef struct ixo_flop_counts {
+    uint64_t add, mul, fma, div, sqrt, transcendental, paths;
+} ixo_flop_counts;
+
+/* sampling.rs */
+uint32_t ixo_hash_u32(uint32_t x);
+float ixo_low_discrepancy_base2(uint32_t n);
+float ixo_radical_inverse_base(uint32_t n, uint32_t base);
+void ixo_pixel_rotations(uint32_t pixel, float out[3]);
+void ixo_sample_draws(uint32_t pixel, uint32_t sample, const float rot[3], uint32_t* seed,
+                      float out[3]);
+/* camera.rs */
+void ixo_camera_new(float yaw, float pitch, float distance, float fov_deg, ix_camera* out);
+void ixo_generate_ray(const ix_camera* cam, float sx, float sy, float w, float h, float jx,
+                      float jy, float origin[3], float dir[3]);
+/* transport/mod.rs:58 */
+void ixo_hero_wavelengths(float hero_rand, float out[8]);
+/* dispersion.rs:170 */
+float ixo_dispersion_eval(const ix_dispersion* d, float lambda_nm);
+/* color/cie1931.rs:157, environment/spectral.rs:28 */
+void ixo_cmf(float lambda_nm, float out[3]);
+float ixo_d65(float lambda_nm);
+/* simd/exp_poly.rs:37 */
+float ixo_exp_lane(float x);
+/* polarization.rs + refraction/tir.rs: Fresnel amplitude coefficients and TIR phase */
+float ixo_tir_phase_delta(float n1, float cos_i, float sin_i);
+void ixo_fresnel_reflect_apply(float r_s, float r_p, const float s_in[4], float s_out[4]);
+/* simd/slab.rs:147 + intersect.rs:101: returns 1 and fills t/idx on a hit */
+int ixo_intersect(const float* planes, uint32_t n_planes, const float origin[3],
+                  const float dir[3], float* t, int32_t* facet);
+/* Environment construction (environment/mod.rs, optics/studio_rig.rs, color.rs) for the
+ * reference's LightingPreset index (environment/mod.rs:475-493).  Returns 0 on success,
+ * -1 for a preset this oracle does not model. */
+int ixo_environment_preset(int32_t preset_index, float exposure, float light_yaw,
+                           float light_pitch, float backdrop, float surface_glare,
+                           float head_shadow_deg, ix_environment* out);
+void ixo_environment_uniform(float radiance, ix_environment* out);
+/* Escape radiance of one channel (environment/rig.rs:18-49). */
+float ixo_environment_channel(const ix_environment* env, const float dir[3], float lambda_nm,
+                              const float observer[3]);
+/* trace_spectral_ray (transport/mod.rs:118): one path from an explicit ray. */
+int ixo_trace_ray(const ix_scene* scene, const float origin[3], const float dir[3],
+                  uint32_t seed, float hero_rand, float xyz[3], ixo_path_info* info);
+/* One (pixel, absolute sample) exactly as renderer/cpu_frame.rs:45 traces it. */
+int ixo_trace_sample(const ix_scene* scene, uint32_t pixel, uint32_t sample, float xyz[3],
+                     ixo_path_info* info);
+/* trace_pixels_interleaved (renderer/cpu_frame.rs:104) for every pixel of the frame,
+ * partitioned over `threads` host threads by the same interleaved stride.  Writes the
+ * reference's f32 per-pixel sums (ascending sample order, non-finite samples dropped)
+ * into sums_f32 and the same samples summed in f64 into sums_f64 (either may be NULL).
+ * Returns the number of dropped non-finite samples, or -1 on an unsupported scene. */
+int64_t ixo_trace_frame(const ix_scene* scene, uint32_t sample_offset, uint32_t spp,
+                        uint32_t threads, float* sums_f32, double* sums_f64);
+/* Like ixo_trace_frame but only for the pixels [pixel_begin, pixel_end). */
+int64_t ixo_trace_pixels(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_end,
+                         uint32_t sample_offset, uint32_t spp, uint32_t threads,
+                         double* sums_f64);
+/* Per-sample XYZ of the pixels [pixel_begin, pixel_end) x samples, row-major
+ * [pixel][sample][3], for path-level comparisons. */
+int ixo_trace_samples(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_end,
+                      uint32_t sample_offset, uint32_t spp, uint32_t threads, float* xyz,
+                      uint32_t* bounces);
+/* StandardGemCuts::standard_round_brilliant (geometry/cuts/round_brilliant.rs:71-155),
+ * the reference's fixed test stone, restated in f32 exactly as built there.
+ * Writes 74 x {nx, ny, nz, d} (57 facets plus 16 girdle planes and the culet). */
+uint32_t ixo_standard_round_brilliant(float* out);
+/* 1 when this build counts floating-point operations. */
+int ixo_counting_build(void);
+/* Counting build only: trace the given pixels x samples and return the operation tally. */
+int ixo_count_flops(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_end,
+                    uint32_t pixel_step, uint32_t sample_offset, uint32_t spp,
+                    ixo_flop_counts* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,238 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the CPU oracle (``libix_oracle.so``).
+
+The oracle restates the reference's CPU spectral tracer in C++ (``ix_oracle.cpp``).  The
+test suite, the smoke check and the benchmark's CPU-baseline leg load it as the checker
+and as the reported CPU baseline; nothing in ``indicatrix_b200`` imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from indicatrix_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+class PathInfo(C.Structure):
+    _fields_ = [
+        ("bounces", C.c_uint32),
+        ("termination", C.c_uint32),
+        ("escaped", C.c_uint32),
+        ("exit_splits", C.c_uint32),
+    ]
+
+
+class FlopCounts(C.Structure):
+    _fields_ = [
+        ("add", C.c_uint64),
+        ("mul", C.c_uint64),
+        ("fma", C.c_uint64),
+        ("div", C.c_uint64),
+        ("sqrt", C.c_uint64),
+        ("transcendental", C.c_uint64),
+        ("paths", C.c_uint64),
+    ]
+
+    def flops(self) -> int:
+        """Floating-point operations: add/sub, mul, div and sqrt count one, FMA two."""
+        return int(self.add + self.mul + 2 * self.fma + self.div + self.sqrt)
+
+
+def build() -> None:
+    """Compile both oracle builds (plain and operation-counting) with make."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_LIBS: dict[str, C.CDLL] = {}
+
+
+def _load(name: str) -> C.CDLL:
+    if name in _LIBS:
+        return _LIBS[name]
+    path = os.path.join(HERE, name)
+    if not os.path.exists(path):
+        build()
+    lib = C.CDLL(path)
+    P = C.POINTER
+    f32p = P(C.c_float)
+    lib.ixo_hash_u32.restype = C.c_uint32
+    lib.ixo_hash_u32.argtypes = [C.c_uint32]
+    lib.ixo_low_discrepancy_base2.restype = C.c_float
+    lib.ixo_low_discrepancy_base2.argtypes = [C.c_uint32]
+    lib.ixo_radical_inverse_base.restype = C.c_float
+    lib.ixo_radical_inverse_base.argtypes = [C.c_uint32, C.c_uint32]
+    lib.ixo_pixel_rotations.argtypes = [C.c_uint32, f32p]
+    lib.ixo_sample_draws.argtypes = [C.c_uint32, C.c_uint32, f32p, P(C.c_uint32), f32p]
+    lib.ixo_camera_new.argtypes = [C.c_float] * 4 + [P(abi.Camera)]
+    lib.ixo_generate_ray.argtypes = [P(abi.Camera)] + [C.c_float] * 6 + [f32p, f32p]
+    lib.ixo_hero_wavelengths.argtypes = [C.c_float, f32p]
+    lib.ixo_dispersion_eval.restype = C.c_float
+    lib.ixo_dispersion_eval.argtypes = [P(abi.Dispersion), C.c_float]
+    lib.ixo_cmf.argtypes = [C.c_float, f32p]
+    lib.ixo_d65.restype = C.c_float
+    lib.ixo_d65.argtypes = [C.c_float]
+    lib.ixo_exp_lane.restype = C.c_float
+    lib.ixo_exp_lane.argtypes = [C.c_float]
+    lib.ixo_tir_phase_delta.restype = C.c_float
+    lib.ixo_tir_phase_delta.argtypes = [C.c_float] * 3
+    lib.ixo_fresnel_reflect_apply.argtypes = [C.c_float, C.c_float, f32p, f32p]
+    lib.ixo_intersect.restype = C.c_int
+    lib.ixo_intersect.argtypes = [f32p, C.c_uint32, f32p, f32p, f32p, P(C.c_int32)]
+    lib.ixo_environment_preset.restype = C.c_int
+    lib.ixo_environment_preset.argtypes = [C.c_int32] + [C.c_float] * 6 + [P(abi.Environment)]
+    lib.ixo_environment_uniform.argtypes = [C.c_float, P(abi.Environment)]
+    lib.ixo_environment_channel.restype = C.c_float
+    lib.ixo_environment_channel.argtypes = [P(abi.Environment), f32p, C.c_float, f32p]
+    lib.ixo_trace_ray.restype = C.c_int
+    lib.ixo_trace_ray.argtypes = [P(abi.Scene), f32p, f32p, C.c_uint32, C.c_float, f32p, P(PathInfo)]
+    lib.ixo_trace_sample.restype = C.c_int
+    lib.ixo_trace_sample.argtypes = [P(abi.Scene), C.c_uint32, C.c_uint32, f32p, P(PathInfo)]
+    lib.ixo_trace_frame.restype = C.c_int64
+    lib.ixo_trace_frame.argtypes = [P(abi.Scene), C.c_uint32, C.c_uint32, C.c_uint32, f32p,
+                                    P(C.c_double)]
+    lib.ixo_trace_pixels.restype = C.c_int64
+    lib.ixo_trace_pixels.argtypes = [P(abi.Scene), C.c_uint32, C.c_uint32, C.c_uint32,
+                                     C.c_uint32, C.c_uint32, P(C.c_double)]
+    lib.ixo_trace_samples.restype = C.c_int
+    lib.ixo_trace_samples.argtypes = [P(abi.Scene), C.c_uint32, C.c_uint32, C.c_uint32,
+                                      C.c_uint32, C.c_uint32, f32p, P(C.c_uint32)]
+    lib.ixo_standard_round_brilliant.restype = C.c_uint32
+    lib.ixo_standard_round_brilliant.argtypes = [f32p]
+    lib.ixo_counting_build.restype = C.c_int
+    lib.ixo_count_flops.restype = C.c_int
+    lib.ixo_count_flops.argtypes = [P(abi.Scene), C.c_uint32, C.c_uint32, C.c_uint32,
+                                    C.c_uint32, C.c_uint32, P(FlopCounts)]
+    _LIBS[name] = lib
+    return lib
+
+
+def lib() -> C.CDLL:
+    return _load("libix_oracle.so")
+
+
+def counting_lib() -> C.CDLL:
+    return _load("libix_oracle_count.so")
+
+
+def _f32p(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def sample_draws(pixel: int, sample: int, rot=None):
+    out = np.zeros(3, np.float32)
+    seed = C.c_uint32()
+    r = None if rot is None else _f32p(np.asarray(rot, np.float32))
+    lib().ixo_sample_draws(pixel, sample, r, C.byref(seed), _f32p(out))
+    return int(seed.value), out
+
+
+def pixel_rotations(pixel: int) -> np.ndarray:
+    out = np.zeros(3, np.float32)
+    lib().ixo_pixel_rotations(pixel, _f32p(out))
+    return out
+
+
+def camera_new(yaw: float, pitch: float, distance: float, fov_deg: float) -> abi.Camera:
+    cam = abi.Camera()
+    lib().ixo_camera_new(yaw, pitch, distance, fov_deg, C.byref(cam))
+    return cam
+
+
+def environment_preset(preset: int, exposure=1.0, yaw=0.0, pitch=0.0, backdrop=0.0,
+                       glare=1.0, head_shadow_deg=16.0) -> abi.Environment:
+    env = abi.Environment()
+    rc = lib().ixo_environment_preset(preset, exposure, yaw, pitch, backdrop, glare,
+                                      head_shadow_deg, C.byref(env))
+    if rc != 0:
+        raise ValueError(f"preset {preset} not modelled by the oracle")
+    return env
+
+
+def environment_uniform(radiance: float) -> abi.Environment:
+    env = abi.Environment()
+    lib().ixo_environment_uniform(radiance, C.byref(env))
+    return env
+
+
+def standard_round_brilliant() -> np.ndarray:
+    out = np.zeros((74, 4), np.float32)
+    n = lib().ixo_standard_round_brilliant(_f32p(out))
+    assert n == 74
+    return out
+
+
+def trace_ray(scene: abi.Scene, origin, direction, seed: int, hero_rand: float):
+    o = np.asarray(origin, np.float32)
+    d = np.asarray(direction, np.float32)
+    xyz = np.zeros(3, np.float32)
+    info = PathInfo()
+    rc = lib().ixo_trace_ray(C.byref(scene), _f32p(o), _f32p(d), seed, hero_rand, _f32p(xyz),
+                             C.byref(info))
+    if rc != 0:
+        raise ValueError("scene not supported by the oracle")
+    return xyz, info
+
+
+def trace_sample(scene: abi.Scene, pixel: int, sample: int):
+    xyz = np.zeros(3, np.float32)
+    info = PathInfo()
+    rc = lib().ixo_trace_sample(C.byref(scene), pixel, sample, _f32p(xyz), C.byref(info))
+    if rc != 0:
+        raise ValueError("scene not supported by the oracle")
+    return xyz, info
+
+
+def trace_frame(scene: abi.Scene, sample_offset: int, spp: int, threads: int = 0):
+    """Returns (f32 sums [h, w, 3] in the reference's order, f64 sums, dropped count)."""
+    if threads <= 0:
+        threads = os.cpu_count() or 1
+    n = scene.width * scene.height
+    s32 = np.zeros((n, 3), np.float32)
+    s64 = np.zeros((n, 3), np.float64)
+    dropped = lib().ixo_trace_frame(C.byref(scene), sample_offset, spp, threads, _f32p(s32),
+                                    s64.ctypes.data_as(C.POINTER(C.c_double)))
+    if dropped < 0:
+        raise ValueError("scene not supported by the oracle")
+    return (s32.reshape(scene.height, scene.width, 3), s64.reshape(scene.height, scene.width, 3),
+            int(dropped))
+
+
+def trace_pixels(scene: abi.Scene, pixel_begin: int, pixel_end: int, sample_offset: int,
+                 spp: int, threads: int = 0) -> np.ndarray:
+    if threads <= 0:
+        threads = os.cpu_count() or 1
+    out = np.zeros((pixel_end - pixel_begin, 3), np.float64)
+    rc = lib().ixo_trace_pixels(C.byref(scene), pixel_begin, pixel_end, sample_offset, spp,
+                                threads, out.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc < 0:
+        raise ValueError("scene not supported by the oracle")
+    return out
+
+
+def trace_samples(scene: abi.Scene, pixel_begin: int, pixel_end: int, sample_offset: int,
+                  spp: int, threads: int = 0):
+    if threads <= 0:
+        threads = os.cpu_count() or 1
+    n = pixel_end - pixel_begin
+    xyz = np.zeros((n, spp, 3), np.float32)
+    bounces = np.zeros((n, spp), np.uint32)
+    rc = lib().ixo_trace_samples(C.byref(scene), pixel_begin, pixel_end, sample_offset, spp,
+                                 threads, _f32p(xyz),
+                                 bounces.ctypes.data_as(C.POINTER(C.c_uint32)))
+    if rc != 0:
+        raise ValueError("scene not supported by the oracle")
+    return xyz, bounces
+
+
+def count_flops(scene: abi.Scene, pixel_begin: int, pixel_end: int, pixel_step: int,
+                sample_offset: int, spp: int) -> FlopCounts:
+    out = FlopCounts()
+    rc = counting_lib().ixo_count_flops(C.byref(scene), pixel_begin, pixel_end, pixel_step,
+                                        sample_offset, spp, C.byref(out))
+    if rc != 0:
+        raise ValueError("flop counting failed")
+    return out
