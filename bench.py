@@ -1,0 +1,382 @@
+"""Benchmark: spectral paths/s of the CUDA Path-Traced sample loop on B200.
+
+One "step" is one pass of the hot path over one batch of synthetic input:
+
+* ``--workload frame`` (default): the 256x256, 64 spp round-brilliant frame
+  (4,194,304 paths; Diamond, D65 hemisphere with a 20-degree head shadow, depth 32);
+* ``--workload batch``: 64 seeded random stones x 9 tilts at 128x128 with spp drawn from
+  {32, 64, 128, 256} -- one persistent launch per step.
+
+Under torchrun (N > 1) every rank traces its own disjoint absolute sample range of the
+same workload (weak scaling), and the per-pixel f64 sums are gathered to rank 0 over
+NCCL and folded in ascending first-sample order (the deterministic merge of the
+reference's indicatrix-dispatch).
+
+Printed on rank 0: one JSON line with the contract's keys, plus ``roofline`` (FP32 FMA
+pipe, measured by a probe kernel) and ``cpu_baseline`` (the CPU oracle on the host
+cores).  ``--impl reference`` times the reference's CPU implementation of the path (the
+oracle restatement, all host threads) on the same workload instead.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "spectral paths/s"
+UNIT = "paths/s"
+L2_FLUSH_BYTES = 512 << 20  # > the 126 MB L2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="frame", choices=["frame", "batch"])
+    ap.add_argument("--precision", default="fast", choices=["fast", "exact"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------
+# Workloads
+# ----------------------------------------------------------------------------------
+def frame_workload():
+    from indicatrix_b200 import workloads
+
+    fs = workloads.round_brilliant_frame(256, 256, 32)
+    return [(fs, 64)], {"workload": "round brilliant frame 256x256 x 64 spp", "pixels": 65536,
+                        "spp": 64, "planes": int(fs.planes.shape[0]), "material": "diamond",
+                        "environment": "D65 hemisphere, 20 deg head shadow", "max_depth": 32}
+
+
+def batch_workload():
+    from indicatrix_b200 import workloads
+
+    stones = workloads.random_stones(64)
+    items = []
+    for st in stones:
+        for tilt in workloads.TILTS_DEG:
+            items.append((workloads.tilted_scene(st, tilt, 128, 128, 32), st.spp))
+    paths = sum(fs.width * fs.height * spp for fs, spp in items)
+    return items, {"workload": "64 random stones x 9 tilts x 128x128, spp in {32,64,128,256}",
+                   "stones": 64, "tilts": 9, "paths": paths, "max_depth": 32}
+
+
+# ----------------------------------------------------------------------------------
+# CPU baseline: the oracle on the host cores, on a bounded sample of the workload.
+# ----------------------------------------------------------------------------------
+def cpu_baseline(items, seconds: float):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ix_oracle
+
+    ix_oracle.build()
+    threads = os.cpu_count() or 1
+    fs, spp = items[0]
+    sc = fs.to_abi()
+    n_pix = fs.width * fs.height
+    # Calibrate on a small pixel slice, then trace a slice sized for ~`seconds`.
+    t0 = time.perf_counter()
+    probe = min(n_pix, 256)
+    ix_oracle.trace_pixels(sc, 0, probe, 0, spp, threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    rate = probe * spp / dt
+    want = int(rate * seconds / spp)
+    # a band of rows through the middle of the frame
+    start = max(0, n_pix // 2 - want // 2)
+    end = min(n_pix, start + max(want, 1))
+    t0 = time.perf_counter()
+    ix_oracle.trace_pixels(sc, start, end, 0, spp, threads)
+    dt = time.perf_counter() - t0
+    paths = (end - start) * spp
+    return {"value": paths / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"pixels [{start},{end}) of the first scene x {spp} spp = {paths} paths, "
+                      f"{dt:.1f} s, C++ oracle -O3 on {threads} host threads"}
+
+
+def count_flops(items):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ix_oracle
+
+    ix_oracle.build()
+    total_f, total_p = 0, 0
+    details = {}
+    step = max(1, len(items) // 8)
+    for fs, spp in items[::step]:
+        sc = fs.to_abi()
+        n_pix = fs.width * fs.height
+        stride = max(1, n_pix // 512)
+        c = ix_oracle.count_flops(sc, 0, n_pix, stride, 0, spp)
+        total_f += c.flops()
+        total_p += c.paths
+        details = {"div_per_path": c.div / c.paths, "sqrt_per_path": c.sqrt / c.paths,
+                   "transcendental_per_path": c.transcendental / c.paths}
+    return total_f / total_p, {"sample_paths": total_p, **details}
+
+
+# ----------------------------------------------------------------------------------
+# Reference arm
+# ----------------------------------------------------------------------------------
+def run_reference(args, items, cfg):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ix_oracle
+
+    ix_oracle.build()
+    threads = os.cpu_count() or 1
+    fs, spp = items[0]
+    sc = fs.to_abi()
+    n_pix = fs.width * fs.height
+    per_step_pixels = max(1, min(n_pix, 4096))
+    for w in range(args.warmup):
+        ix_oracle.trace_pixels(sc, 0, min(256, n_pix), 0, spp, threads)
+    times = []
+    for k in range(args.steps):
+        start = (k * per_step_pixels) % max(1, n_pix - per_step_pixels + 1)
+        t0 = time.perf_counter()
+        ix_oracle.trace_pixels(sc, start, start + per_step_pixels, 0, spp, threads)
+        times.append(time.perf_counter() - t0)
+    paths = per_step_pixels * spp
+    value = paths * len(times) / sum(times)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{per_step_pixels} pixels x {spp} spp per step of the first scene; "
+                                   "the reference (Rust) cannot be built here, its CPU tracer "
+                                   "restated in C++ is timed"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ----------------------------------------------------------------------------------
+# Our arm
+# ----------------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    items, cfg = frame_workload() if args.workload == "frame" else batch_workload()
+    cfg["parallelism"] = f"sample-range shards x{world}" if world > 1 else "single GPU"
+    if args.impl == "reference":
+        run_reference(args, items, cfg)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from indicatrix_b200 import abi
+    from indicatrix_b200.backend import GpuBackend
+
+    precision = abi.PRECISION_EXACT if args.precision == "exact" else abi.PRECISION_FAST
+    backend = GpuBackend.acquire(device=local, precision=precision)
+    if not backend.available:
+        raise RuntimeError("libix_cuda.so could not create a backend")
+
+    # Device-resident inputs and outputs.
+    dev_items = []
+    for fs, spp in items:
+        sc = fs.to_abi()
+        planes = torch.from_numpy(np.ascontiguousarray(fs.planes, np.float32)).to(dev)
+        sc.planes = C.cast(C.c_void_p(planes.data_ptr()), C.POINTER(C.c_float))
+        out = torch.zeros(fs.width * fs.height * 3, dtype=torch.float64, device=dev)
+        dev_items.append((sc, planes, out, spp, fs))
+    total_paths = sum(fs.width * fs.height * spp for fs, spp in items)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sample_base = rank * 1_000_000  # disjoint absolute sample ranges per rank
+
+    def step(k):
+        for sc, _planes, out, spp, _fs in dev_items:
+            rc = backend.accumulate_device(sc, sample_base + 0, spp, out.data_ptr(), False,
+                                           stream.cuda_stream)
+            if rc != 0:
+                raise RuntimeError(f"device trace declined: {backend.last_lost_reason()}")
+        if world > 1:
+            gathered = [torch.empty_like(dev_items[0][2]) for _ in range(world)]
+            torch.distributed.all_gather(gathered, dev_items[0][2])
+            # fold in ascending first-sample order (rank order == first-sample order)
+            acc = gathered[0].clone()
+            for g in gathered[1:]:
+                acc += g
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.zero_()  # L2 flush between timed iterations (outside the step events)
+        starts[k].record(stream)
+        step(k)
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    mean_ms = sum(step_ms) / len(step_ms)
+    if world > 1:
+        t = torch.tensor([mean_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        mean_ms = float(t.item())
+    value = world * total_paths / (mean_ms * 1e-3)
+    launches_per_step = 0
+    for fs, spp in items:
+        n = fs.width * fs.height * spp
+        launches_per_step += 1 + (1 if n > (1 << 20) else 0)
+
+    # End-to-end through the public API with host buffers (H2D planes, D2H sums).
+    e2e_ms = []
+    accs = [np.zeros((fs.height, fs.width, 3), np.float64) for fs, _ in items]
+    for k in range(max(1, args.warmup // 2) + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for (fs, spp), acc in zip(items, accs):
+            if not backend.try_accumulate(fs, sample_base, spp, acc):
+                raise RuntimeError(f"e2e trace declined: {backend.last_lost_reason()}")
+        t1 = time.perf_counter()
+        if k >= max(1, args.warmup // 2):
+            e2e_ms.append((t1 - t0) * 1e3)
+    e2e_mean = sum(e2e_ms) / len(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_mean], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_mean = float(t.item())
+    h2d = sum(int(fs.planes.shape[0]) * 16 for fs, _ in items)
+    d2h = sum(fs.width * fs.height * 3 * 8 + 8 for fs, _ in items)
+
+    if rank == 0:
+        peak = backend.probe_fp32_peak()
+        flops_per_path, flop_info = count_flops(items)
+        # dominant kernel: the trace megakernel; per-launch algorithmic FLOPs / duration
+        achieved = flops_per_path * total_paths / (mean_ms * 1e-3)
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(prof):
+            try:
+                with open(prof) as f:
+                    tr = json.load(f).get(args.workload)
+                if tr:
+                    traffic = tr["bytes_per_path"] * total_paths / launches_per_step
+            except (OSError, ValueError, KeyError):
+                traffic = None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {**cfg, "precision": args.precision,
+                       "l2": "512 MB buffer written between timed steps (outside the step events)",
+                       "spectral_samples_per_s": 8.0 * value},
+            "e2e": {"value": world * total_paths / (e2e_mean * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_mean},
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak / 1e12,
+                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                         "traffic": traffic,
+                         "peak_source": "measured by the FP32 FMA-chain probe kernel (FMA = 2 FLOP) "
+                                        "in this run; MEASURED_PEAKS.json has no non-tensor FP32 figure",
+                         "flops_per_path": flops_per_path, "flop_count": flop_info},
+            "clocks": clk,
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(items, args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    backend.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

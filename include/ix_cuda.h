@@ -1,0 +1,147 @@
+/*
+ * ix_cuda.h -- C ABI of libix_cuda.so, the B200 (sm_100a) backend for indicatrix's
+ * Path-Traced spectral sample loop.
+ *
+ * The entry points are what a host binding of the reference's `GpuBackend`
+ * (crates/indicatrix/src/renderer/gpu_backend/backend.rs, stub.rs) would call: plain
+ * pointers and sizes, no CUDA or torch types except an opaque stream handle on the
+ * device-resident entry.  Each declaration cites the reference interface it replaces.
+ *
+ * Contract shared by every accumulate entry (gpu_backend/mod.rs:24-31, :122-164):
+ *   - `accum_xyz` is caller-owned, row-major, width * height * 3; the backend ADDS the
+ *     per-pixel sums of samples [sample_offset, sample_offset + spp) into it, and only
+ *     when it returns IX_DONE;
+ *   - IX_DECLINED leaves `accum_xyz` untouched and means "trace the full spp on the
+ *     CPU"; device errors are reported as a decline and mark the backend lost;
+ *   - IX_CANCELLED leaves `accum_xyz` untouched;
+ *   - a sample whose XYZ has a NaN/Inf component is dropped but still counted
+ *     (optics/raytracer/sampling.rs:237).
+ * Per-pixel sums are formed on the device in f64 and are bit-identical for any chunking
+ * and any run.
+ */
+#ifndef IX_CUDA_H
+#define IX_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "ix_scene.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* GpuAccumulate (gpu_backend/mod.rs:308-326). */
+enum { IX_DONE = 0, IX_DECLINED = 1, IX_CANCELLED = 2 };
+/* GpuPipelineKind (gpu_backend/mod.rs:347-353). */
+enum { IX_PIPELINE_MEGAKERNEL = 0, IX_PIPELINE_WAVEFRONT = 1 };
+/* Rounding of the transport kernels: FAST lets the compiler fuse multiply-adds;
+ * EXACT rounds every step as the reference's CPU code does (no contraction). */
+enum { IX_PRECISION_FAST = 0, IX_PRECISION_EXACT = 1 };
+
+typedef struct ix_backend ix_backend;
+
+typedef struct ix_backend_options {
+    int32_t device;              /* CUDA device ordinal                                  */
+    uint32_t pipeline;           /* IX_PIPELINE_*                                        */
+    uint32_t precision;          /* IX_PRECISION_*                                       */
+    uint32_t threads_per_block;  /* 0 = autotuned                                        */
+    uint64_t chunk_paths;        /* paths per launch; 0 = default (TDR-safe first chunk)  */
+} ix_backend_options;
+
+/* GpuWorkLimits (gpu_backend/limits.rs:6-27): a request above a limit is declined. */
+typedef struct ix_work_limits {
+    uint64_t max_pixels;
+    uint64_t max_paths_per_call;
+    uint32_t max_spp;
+} ix_work_limits;
+
+/* One stone of a batched request (GpuBatchItem, gpu_backend/mod.rs:246). */
+typedef struct ix_batch_item {
+    const ix_scene* scene;
+    uint32_t sample_offset;
+    uint32_t spp;
+    double* accum_xyz;           /* width * height * 3, added into on IX_DONE           */
+    int32_t status;              /* written by ix_accumulate_batch                      */
+} ix_batch_item;
+
+/* Device timing of the last accumulate call on this backend. */
+typedef struct ix_timing {
+    float kernel_ms;             /* trace kernel(s), CUDA events on the backend stream   */
+    float reduce_ms;             /* host-visible copy and fold                           */
+    uint64_t paths;
+    uint32_t launches;           /* kernels this library launched for the call           */
+} ix_timing;
+
+/* GpuBackend::acquire / acquire_with_diagnostics (gpu_backend/limits.rs:50-71).
+ * `opts` may be NULL (device 0, megakernel, fast rounding).  Returns NULL when no
+ * usable device is present. */
+ix_backend* ix_backend_create(const ix_backend_options* opts);
+/* Drop of GpuBackend. */
+void ix_backend_destroy(ix_backend* b);
+/* GpuBackend::adapter_label (backend.rs:165): device name, NUL-terminated. */
+int ix_backend_label(const ix_backend* b, char* buf, size_t len);
+/* GpuBackend::set_pipeline_kind (backend.rs:165). */
+void ix_set_pipeline_kind(ix_backend* b, uint32_t kind);
+/* GpuBackend::set_work_limits (gpu_backend/limits.rs:75). */
+void ix_set_work_limits(ix_backend* b, const ix_work_limits* limits);
+/* Rounding mode of later calls (IX_PRECISION_*). */
+void ix_set_precision(ix_backend* b, uint32_t precision);
+/* scene_routes_to_gpu (gpu_backend/mod.rs:288): 1 when this backend can trace `scene`
+ * (convex, all facets polished, no scattering, isotropic material, <= IX_MAX_PLANES). */
+int ix_scene_routes_to_gpu(const ix_scene* scene);
+/* GpuBackend::try_accumulate_geom_cancellable (backend.rs:272) with an f32 accumulator:
+ * adds (float)(f64 pixel sum) into accum_xyz.  `cancel` may be NULL; it is polled
+ * between chunks. */
+int ix_accumulate(ix_backend* b, const ix_scene* scene, uint32_t sample_offset, uint32_t spp,
+                  float* accum_xyz, const volatile int32_t* cancel);
+/* The same with an f64 accumulator (no rounding of the pixel sums). */
+int ix_accumulate_f64(ix_backend* b, const ix_scene* scene, uint32_t sample_offset,
+                      uint32_t spp, double* accum_xyz, const volatile int32_t* cancel);
+/* GpuBackend::try_accumulate_batch_cancellable (backend.rs:451): every item traced,
+ * each item's status written to item->status; returns IX_DONE when all items are done. */
+int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items,
+                        const volatile int32_t* cancel);
+/* Device-resident form for callers that keep the scene and the sums in GPU memory:
+ * `scene->planes` and `d_accum_xyz` are device pointers; the launch is enqueued on
+ * `stream` (a cudaStream_t, or NULL for the backend's own stream) and not synchronised.
+ * `accumulate` = 1 adds into d_accum_xyz, 0 overwrites it. */
+int ix_accumulate_device(ix_backend* b, const ix_scene* scene, uint32_t sample_offset,
+                         uint32_t spp, double* d_accum_xyz, int accumulate, void* stream);
+/* GpuBackend::is_lost / try_recover / last_lost_reason (backend.rs:704). */
+int ix_is_lost(const ix_backend* b);
+int ix_try_recover(ix_backend* b);
+int ix_last_error(const ix_backend* b, char* buf, size_t len);
+/* Timing of the last call (device events on the backend's stream). */
+int ix_last_timing(const ix_backend* b, ix_timing* out);
+/* Non-finite samples dropped by the last call. */
+uint64_t ix_last_dropped(const ix_backend* b);
+/* Measured FP32 FMA-pipe throughput of the device in FLOP/s (FMA = 2), the roofline
+ * denominator of the FP32-bound transport kernels.  No reference counterpart. */
+int ix_probe_fp32_peak(ix_backend* b, double* flops);
+
+/* Host-side scene construction, the reference's own host formulas:
+ * Camera::new (optics/raytracer/camera.rs:108). */
+void ix_camera_new(float yaw, float pitch, float distance, float fov_deg, ix_camera* out);
+/* EnvironmentSource::Studio for a LightingPreset index (environment/mod.rs:475-493,
+ * params :318-411, studio_rig.rs:33, color.rs:277-340): 1 IsoHemisphere, 7 Daylight,
+ * 8 Incandescent, 9 IlluminantA, 10 RingLights, 11 DarkSpotlight.  Returns 0, or -1 for
+ * a preset this backend does not model. */
+int ix_environment_preset(int32_t preset_index, float exposure, float light_yaw,
+                          float light_pitch, float backdrop, float surface_glare,
+                          float head_shadow_deg, ix_environment* out);
+/* A uniform dome of constant spectral radiance (white-furnace environment). */
+void ix_environment_uniform(float radiance, ix_environment* out);
+
+/* Per-function check kernels (the GPU equivalence harness's Tier-1/Tier-2 units,
+ * renderer/gpu/ulp.rs): evaluates function `fn` (ix::CheckFn numbering) for `n` input
+ * rows of `in_stride` 32-bit words on the device, writing `out_stride` words per row.
+ * `scene` supplies the material, environment and planes.  Host buffers. */
+int ix_debug_check(ix_backend* b, const ix_scene* scene, int32_t fn, uint32_t n,
+                   const uint32_t* in, uint32_t in_stride, uint32_t* out, uint32_t out_stride);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IX_CUDA_H */

@@ -1,0 +1,383 @@
+"""Host-side mirror of the reference's ``GpuBackend`` over ``libix_cuda.so``.
+
+Same operation names, argument meaning and outcomes as
+crates/indicatrix/src/renderer/gpu_backend/backend.rs (and its always-decline stub,
+gpu_backend/stub.rs:12-138):
+
+* ``GpuBackend.acquire()`` / ``GpuBackend.disabled()`` -- a usable backend or one that
+  declines everything;
+* ``try_accumulate(scene, sample_offset, spp, accum) -> bool`` -- adds the per-pixel sums
+  of samples ``[sample_offset, sample_offset + spp)`` into ``accum`` (row-major
+  ``height x width x 3``) and returns True, or returns False with ``accum`` untouched;
+* ``try_accumulate_cancellable(...) -> GpuAccumulate`` -- DONE / DECLINED / CANCELLED;
+* ``try_accumulate_batch_cancellable(items, cancel, on_done)``;
+* ``is_lost`` / ``try_recover`` / ``adapter_label`` / ``set_pipeline_kind`` /
+  ``set_work_limits``.
+
+The CUDA library is the only compute path: if it is missing or fails to load, the
+import raises; nothing here falls back to a CPU tracer.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import os
+import threading
+from dataclasses import dataclass, field
+from typing import Callable, Optional, Sequence
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libix_cuda.so")
+
+_lib: Optional[C.CDLL] = None
+_lib_lock = threading.Lock()
+
+
+def load_library() -> C.CDLL:
+    """Load ``libix_cuda.so`` (building it first if it is absent).  Raises on failure."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            from .build import build
+
+            build()
+        lib = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        lib.ix_backend_create.restype = C.c_void_p
+        lib.ix_backend_create.argtypes = [P(abi.BackendOptions)]
+        lib.ix_backend_destroy.argtypes = [C.c_void_p]
+        lib.ix_backend_label.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+        lib.ix_set_pipeline_kind.argtypes = [C.c_void_p, C.c_uint32]
+        lib.ix_set_work_limits.argtypes = [C.c_void_p, P(abi.WorkLimits)]
+        lib.ix_set_precision.argtypes = [C.c_void_p, C.c_uint32]
+        lib.ix_scene_routes_to_gpu.argtypes = [P(abi.Scene)]
+        lib.ix_accumulate.argtypes = [C.c_void_p, P(abi.Scene), C.c_uint32, C.c_uint32,
+                                      P(C.c_float), P(C.c_int32)]
+        lib.ix_accumulate_f64.argtypes = [C.c_void_p, P(abi.Scene), C.c_uint32, C.c_uint32,
+                                          P(C.c_double), P(C.c_int32)]
+        lib.ix_accumulate_batch.argtypes = [C.c_void_p, P(abi.BatchItem), C.c_uint32, P(C.c_int32)]
+        lib.ix_accumulate_device.argtypes = [C.c_void_p, P(abi.Scene), C.c_uint32, C.c_uint32,
+                                             C.c_void_p, C.c_int, C.c_void_p]
+        lib.ix_is_lost.argtypes = [C.c_void_p]
+        lib.ix_try_recover.argtypes = [C.c_void_p]
+        lib.ix_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+        lib.ix_last_timing.argtypes = [C.c_void_p, P(abi.TimingInfo)]
+        lib.ix_last_dropped.restype = C.c_uint64
+        lib.ix_last_dropped.argtypes = [C.c_void_p]
+        lib.ix_probe_fp32_peak.argtypes = [C.c_void_p, P(C.c_double)]
+        lib.ix_camera_new.argtypes = [C.c_float] * 4 + [P(abi.Camera)]
+        lib.ix_environment_preset.argtypes = [C.c_int32] + [C.c_float] * 6 + [P(abi.Environment)]
+        lib.ix_environment_uniform.argtypes = [C.c_float, P(abi.Environment)]
+        lib.ix_debug_check.argtypes = [C.c_void_p, P(abi.Scene), C.c_int32, C.c_uint32,
+                                       P(C.c_uint32), C.c_uint32, P(C.c_uint32), C.c_uint32]
+        _lib = lib
+        return lib
+
+
+class GpuAccumulate(enum.IntEnum):
+    """Outcome of an accumulate call (gpu_backend/mod.rs:308-326)."""
+
+    DONE = abi.IX_DONE
+    DECLINED = abi.IX_DECLINED
+    CANCELLED = abi.IX_CANCELLED
+
+
+class GpuPipelineKind(enum.IntEnum):
+    """gpu_backend/mod.rs:347-353."""
+
+    MEGAKERNEL = abi.PIPELINE_MEGAKERNEL
+    WAVEFRONT = abi.PIPELINE_WAVEFRONT
+
+
+@dataclass
+class GpuWorkLimits:
+    """gpu_backend/limits.rs:6-27; zero means unlimited."""
+
+    max_pixels: int = 0
+    max_paths_per_call: int = 0
+    max_spp: int = 0
+
+
+class CancelFlag:
+    """An ``AtomicBool``-like cancel word the library polls between chunks."""
+
+    def __init__(self) -> None:
+        self._word = C.c_int32(0)
+
+    def set(self) -> None:
+        self._word.value = 1
+
+    def clear(self) -> None:
+        self._word.value = 0
+
+    def is_set(self) -> bool:
+        return bool(self._word.value)
+
+    def pointer(self):
+        return C.pointer(self._word)
+
+
+@dataclass
+class FrameScene:
+    """What a frame tracer needs (renderer/frame_scene.rs:22 / GpuSceneRef): the camera,
+    image size, facet planes (n.x + d <= 0 inside), per-facet finishes, material, bounce
+    cap and environment.  ``to_abi`` produces the C POD, keeping the arrays alive."""
+
+    camera: abi.Camera
+    width: int
+    height: int
+    planes: np.ndarray
+    material: abi.Material
+    max_bounces: int
+    environment: abi.Environment
+    facet_finishes: Optional[np.ndarray] = None
+    _keep: list = field(default_factory=list, repr=False)
+
+    def to_abi(self) -> abi.Scene:
+        planes = np.ascontiguousarray(self.planes, dtype=np.float32).reshape(-1, 4)
+        sc = abi.Scene()
+        sc.camera = self.camera
+        sc.width = int(self.width)
+        sc.height = int(self.height)
+        sc.planes = planes.ctypes.data_as(C.POINTER(C.c_float))
+        sc.n_planes = planes.shape[0]
+        if self.facet_finishes is not None:
+            fin = np.ascontiguousarray(self.facet_finishes, dtype=np.uint8)
+            sc.facet_finishes = fin.ctypes.data_as(C.POINTER(C.c_uint8))
+            sc.n_finishes = fin.shape[0]
+            self._keep.append(fin)
+        sc.material = self.material
+        sc.max_bounces = int(self.max_bounces)
+        sc.environment = self.environment
+        self._keep.append(planes)
+        return sc
+
+
+def camera_new(yaw: float, pitch: float, distance: float, fov_deg: float = 42.0) -> abi.Camera:
+    """Camera::new (optics/raytracer/camera.rs:108); DEFAULT_FOV_DEG is 42 (:66)."""
+    cam = abi.Camera()
+    load_library().ix_camera_new(yaw, pitch, distance, fov_deg, C.byref(cam))
+    return cam
+
+
+# LightingPreset::index (environment/mod.rs:475-493) for the presets this backend models.
+PRESET_ISO_HEMISPHERE = 1
+PRESET_DAYLIGHT = 7
+PRESET_INCANDESCENT = 8
+PRESET_ILLUMINANT_A = 9
+PRESET_RING_LIGHTS = 10
+PRESET_DARK_SPOTLIGHT = 11
+
+
+def environment_preset(preset: int, exposure: float = 1.0, light_yaw: float = 0.0,
+                       light_pitch: float = 0.0, backdrop: float = 0.0,
+                       surface_glare: float = 1.0, head_shadow_deg: float = 16.0) -> abi.Environment:
+    """EnvironmentSource::Studio { preset, .. } with its host-side derived fields."""
+    env = abi.Environment()
+    rc = load_library().ix_environment_preset(preset, exposure, light_yaw, light_pitch, backdrop,
+                                              surface_glare, head_shadow_deg, C.byref(env))
+    if rc != 0:
+        raise ValueError(f"lighting preset {preset} is not modelled by this backend")
+    return env
+
+
+def environment_uniform(radiance: float) -> abi.Environment:
+    env = abi.Environment()
+    load_library().ix_environment_uniform(radiance, C.byref(env))
+    return env
+
+
+def scene_routes_to_gpu(scene: FrameScene) -> bool:
+    """scene_routes_to_gpu (gpu_backend/mod.rs:288)."""
+    return bool(load_library().ix_scene_routes_to_gpu(C.byref(scene.to_abi())))
+
+
+@dataclass
+class GpuBatchItem:
+    """One stone of a batch (gpu_backend/mod.rs:246): its scene, absolute sample range and
+    an f64 accumulator the batch adds into."""
+
+    scene: FrameScene
+    sample_offset: int
+    spp: int
+    accum: np.ndarray
+
+
+class GpuBackend:
+    """The CUDA backend.  Thread-safe: calls from several threads are served in FIFO order
+    by the library's turnstile."""
+
+    def __init__(self, handle: Optional[int]) -> None:
+        self._h = handle
+        self._lib = load_library() if handle else None
+
+    @classmethod
+    def acquire(cls, device: int = 0, precision: int = abi.PRECISION_FAST,
+                pipeline: GpuPipelineKind = GpuPipelineKind.MEGAKERNEL,
+                threads_per_block: int = 0, chunk_paths: int = 0) -> "GpuBackend":
+        lib = load_library()
+        opts = abi.BackendOptions(device, int(pipeline), precision, threads_per_block, chunk_paths)
+        h = lib.ix_backend_create(C.byref(opts))
+        return cls(h if h else None)
+
+    @classmethod
+    def disabled(cls) -> "GpuBackend":
+        return cls(None)
+
+    def __del__(self) -> None:
+        self.close()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ix_backend_destroy(self._h)
+            self._h = None
+
+    @property
+    def available(self) -> bool:
+        return self._h is not None
+
+    def adapter_label(self) -> Optional[str]:
+        if not self._h:
+            return None
+        buf = C.create_string_buffer(256)
+        self._lib.ix_backend_label(self._h, buf, 256)
+        return buf.value.decode()
+
+    def set_pipeline_kind(self, kind: GpuPipelineKind) -> None:
+        if self._h:
+            self._lib.ix_set_pipeline_kind(self._h, int(kind))
+
+    def set_precision(self, precision: int) -> None:
+        if self._h:
+            self._lib.ix_set_precision(self._h, precision)
+
+    def set_work_limits(self, limits: GpuWorkLimits) -> None:
+        if self._h:
+            wl = abi.WorkLimits(limits.max_pixels, limits.max_paths_per_call, limits.max_spp)
+            self._lib.ix_set_work_limits(self._h, C.byref(wl))
+
+    def is_lost(self) -> bool:
+        return bool(self._lib.ix_is_lost(self._h)) if self._h else False
+
+    def try_recover(self) -> bool:
+        return bool(self._lib.ix_try_recover(self._h)) if self._h else True
+
+    def last_lost_reason(self) -> Optional[str]:
+        if not self._h:
+            return None
+        buf = C.create_string_buffer(512)
+        n = self._lib.ix_last_error(self._h, buf, 512)
+        return buf.value.decode() if n > 0 else None
+
+    def last_timing(self) -> abi.TimingInfo:
+        t = abi.TimingInfo()
+        if self._h:
+            self._lib.ix_last_timing(self._h, C.byref(t))
+        return t
+
+    def probe_fp32_peak(self) -> float:
+        """Measured FP32 FMA-pipe FLOP/s of this device (FMA counted as 2)."""
+        v = C.c_double(0.0)
+        if not self._h or self._lib.ix_probe_fp32_peak(self._h, C.byref(v)) != 0:
+            return 0.0
+        return float(v.value)
+
+    def last_dropped(self) -> int:
+        return int(self._lib.ix_last_dropped(self._h)) if self._h else 0
+
+    @staticmethod
+    def _check_accum(scene: FrameScene, accum: np.ndarray) -> None:
+        # GpuBackend panics on a mis-sized accumulator (gpu_backend/mod.rs:122-130).
+        if accum.size != scene.width * scene.height * 3 or not accum.flags.c_contiguous:
+            raise ValueError("accum must be a contiguous width*height*3 array")
+
+    def try_accumulate_cancellable(self, scene: FrameScene, sample_offset: int, spp: int,
+                                   accum: np.ndarray,
+                                   cancel: Optional[CancelFlag] = None) -> GpuAccumulate:
+        """try_accumulate_geom_cancellable (backend.rs:272).  ``accum`` is float32 or
+        float64 and is added into only on DONE."""
+        self._check_accum(scene, accum)
+        if not self._h:
+            return GpuAccumulate.DECLINED
+        sc = scene.to_abi()
+        cp = cancel.pointer() if cancel is not None else None
+        if accum.dtype == np.float32:
+            rc = self._lib.ix_accumulate(self._h, C.byref(sc), sample_offset, spp,
+                                         accum.ctypes.data_as(C.POINTER(C.c_float)), cp)
+        elif accum.dtype == np.float64:
+            rc = self._lib.ix_accumulate_f64(self._h, C.byref(sc), sample_offset, spp,
+                                             accum.ctypes.data_as(C.POINTER(C.c_double)), cp)
+        else:
+            raise TypeError("accum must be float32 or float64")
+        return GpuAccumulate(rc)
+
+    def try_accumulate(self, scene: FrameScene, sample_offset: int, spp: int,
+                       accum: np.ndarray) -> bool:
+        """try_accumulate (backend.rs:182): True when every sample was added."""
+        return self.try_accumulate_cancellable(scene, sample_offset, spp, accum) == GpuAccumulate.DONE
+
+    def try_accumulate_batch_cancellable(self, items: Sequence[GpuBatchItem],
+                                         cancel: Optional[CancelFlag] = None,
+                                         on_done: Optional[Callable[[int, GpuAccumulate], None]] = None
+                                         ) -> GpuAccumulate:
+        """try_accumulate_batch_cancellable (backend.rs:451): each item's outcome is
+        reported through ``on_done(index, outcome)``."""
+        if not self._h:
+            for i in range(len(items)):
+                if on_done:
+                    on_done(i, GpuAccumulate.DECLINED)
+            return GpuAccumulate.DECLINED
+        arr = (abi.BatchItem * len(items))()
+        scenes = []
+        for i, it in enumerate(items):
+            if it.accum.dtype != np.float64:
+                raise TypeError("batch accumulators are float64")
+            self._check_accum(it.scene, it.accum)
+            sc = it.scene.to_abi()
+            scenes.append(sc)
+            arr[i].scene = C.pointer(sc)
+            arr[i].sample_offset = it.sample_offset
+            arr[i].spp = it.spp
+            arr[i].accum_xyz = it.accum.ctypes.data_as(C.POINTER(C.c_double))
+            arr[i].status = abi.IX_DECLINED
+        cp = cancel.pointer() if cancel is not None else None
+        rc = self._lib.ix_accumulate_batch(self._h, arr, len(items), cp)
+        if on_done:
+            for i in range(len(items)):
+                on_done(i, GpuAccumulate(arr[i].status))
+        return GpuAccumulate(rc)
+
+    def accumulate_device(self, scene_abi: abi.Scene, sample_offset: int, spp: int,
+                          d_accum_ptr: int, accumulate: bool = True,
+                          stream_ptr: Optional[int] = None) -> GpuAccumulate:
+        """Device-resident form: ``scene_abi.planes`` and ``d_accum_ptr`` are device
+        pointers; the launch is enqueued on ``stream_ptr`` and not synchronised."""
+        if not self._h:
+            return GpuAccumulate.DECLINED
+        rc = self._lib.ix_accumulate_device(self._h, C.byref(scene_abi), sample_offset, spp,
+                                            C.c_void_p(d_accum_ptr), 1 if accumulate else 0,
+                                            C.c_void_p(stream_ptr) if stream_ptr else None)
+        return GpuAccumulate(rc)
+
+    def debug_check(self, scene: FrameScene, fn: int, inputs: np.ndarray, out_words: int) -> np.ndarray:
+        """Runs per-function check kernel ``fn`` over the rows of ``inputs`` (32-bit words)."""
+        if not self._h:
+            raise RuntimeError("no CUDA device")
+        inp = np.ascontiguousarray(inputs).view(np.uint32)
+        if inp.ndim == 1:
+            inp = inp.reshape(-1, 1)
+        n, stride = inp.shape
+        out = np.zeros((n, out_words), np.uint32)
+        sc = scene.to_abi()
+        rc = self._lib.ix_debug_check(self._h, C.byref(sc), fn, n,
+                                      inp.ctypes.data_as(C.POINTER(C.c_uint32)), stride,
+                                      out.ctypes.data_as(C.POINTER(C.c_uint32)), out_words)
+        if rc != 0:
+            raise RuntimeError(f"check kernel failed: {self.last_lost_reason()}")
+        return out

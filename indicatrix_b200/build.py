@@ -1,0 +1,95 @@
+"""Builds ``libix_cuda.so`` in-tree for sm_100a.
+
+The kernel translation unit is compiled twice -- reference-exact rounding
+(``-DIX_EXACT=1 -fmad=false``) and fused rounding (``-DIX_EXACT=0``) -- and linked with
+the C-ABI host code into one shared library beside this file.
+Run ``python -m indicatrix_b200.build`` or call :func:`build`.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.normpath(os.path.join(HERE, "..", "include"))
+OUT = os.path.join(HERE, "libix_cuda.so")
+BUILD_DIR = os.path.join(HERE, "_build")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _cuda_home(nvcc: str) -> str:
+    return os.path.dirname(os.path.dirname(os.path.realpath(nvcc)))
+
+
+def _sources():
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))] + [
+        os.path.join(INCLUDE, f) for f in sorted(os.listdir(INCLUDE))
+    ]
+
+
+def _up_to_date() -> bool:
+    if not os.path.exists(OUT):
+        return False
+    t = os.path.getmtime(OUT)
+    return all(os.path.getmtime(s) <= t for s in _sources() + [__file__])
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile the CUDA extension if any source is newer than the library."""
+    if not force and _up_to_date():
+        return OUT
+    nvcc = _nvcc()
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    common = [nvcc, "-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC",
+              "--expt-relaxed-constexpr", "-Xptxas", "-v", f"-I{INCLUDE}"]
+    objs = []
+    logs = []
+    for variant, flags in (("exact", ["-DIX_EXACT=1", "-fmad=false"]),
+                           ("fast", ["-DIX_EXACT=0", "-fmad=true"])):
+        obj = os.path.join(BUILD_DIR, f"ix_kernels_{variant}.o")
+        cmd = common + flags + ["-c", os.path.join(CSRC, "ix_kernels.cu"), "-o", obj]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        logs.append(r.stderr)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + r.stderr)
+        objs.append(obj)
+    probe_obj = os.path.join(BUILD_DIR, "ix_probe.o")
+    r = subprocess.run(common + ["-c", os.path.join(CSRC, "ix_probe.cu"), "-o", probe_obj],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + r.stderr)
+    objs.append(probe_obj)
+    host_obj = os.path.join(BUILD_DIR, "ix_backend.o")
+    cuda_inc = os.path.join(_cuda_home(nvcc), "include")
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
+           f"-I{INCLUDE}", f"-I{cuda_inc}", "-c", os.path.join(CSRC, "ix_backend.cpp"), "-o", host_obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("g++ failed:\n" + r.stderr)
+    objs.append(host_obj)
+    tmp = OUT + ".tmp"
+    cmd = [nvcc, "-shared", *ARCH, "-o", tmp, *objs, "-cudart", "static", "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("link failed:\n" + r.stderr)
+    os.replace(tmp, OUT)
+    with open(os.path.join(BUILD_DIR, "ptxas.log"), "w") as f:
+        f.write("\n".join(logs))
+    if verbose:
+        print("\n".join(logs))
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,616 @@
+// ix_backend.cpp -- host side of the C ABI declared in include/ix_cuda.h.
+//
+// The reference's GpuBackend (crates/indicatrix/src/renderer/gpu_backend/backend.rs)
+// re-designed for one CUDA device: a backend owns a stream, pooled device buffers and
+// pinned host staging; requests take a FIFO ticket (gpu_backend/turnstile.rs:24-115) so
+// concurrent callers are served in arrival order; a device error marks the backend lost
+// and turns the request into a decline (gpu_backend/mod.rs:151-164, recovery.rs:13-79).
+//
+// Host scene construction (camera, environment presets) follows the reference's own
+// host formulas; this file is compiled with -ffp-contract=off so those round exactly as
+// the reference does.
+
+#include "../../include/ix_cuda.h"
+#include "../../include/ix_cie_tables.h"
+#include "ix_launch.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+struct ix_backend {
+    int device = 0;
+    uint32_t pipeline = IX_PIPELINE_MEGAKERNEL;
+    uint32_t precision = IX_PRECISION_FAST;
+    uint32_t threads = 128;
+    uint64_t chunk_paths = 0;
+    ix_work_limits limits{0, 0, 0};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Pooled buffers.
+    float* d_planes = nullptr;
+    size_t planes_cap = 0;
+    double* d_sums = nullptr;
+    size_t sums_cap = 0;
+    double* h_sums = nullptr;
+    size_t hsums_cap = 0;
+    uint32_t* d_counter = nullptr;
+    unsigned long long* d_dropped = nullptr;
+    uint32_t* d_check = nullptr;
+    size_t check_cap = 0;
+    int sm_count = 0;
+    int bps_exact = 1, bps_fast = 1;
+    std::string label;
+    // State.
+    bool lost = false;
+    std::string last_error;
+    ix_timing timing{0.0f, 0.0f, 0, 0};
+    uint64_t dropped = 0;
+    // FIFO turnstile.
+    std::mutex mu;
+    std::condition_variable cv;
+    uint64_t next_ticket = 0, serving = 0;
+};
+
+namespace {
+
+struct Turn {
+    ix_backend* b;
+    explicit Turn(ix_backend* be) : b(be) {
+        std::unique_lock<std::mutex> lk(b->mu);
+        uint64_t mine = b->next_ticket++;
+        b->cv.wait(lk, [&] { return b->serving == mine; });
+    }
+    ~Turn() {
+        std::lock_guard<std::mutex> lk(b->mu);
+        b->serving++;
+        b->cv.notify_all();
+    }
+};
+
+bool fail(ix_backend* b, cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return false;
+    b->lost = true;
+    b->last_error = std::string(where) + ": " + cudaGetErrorString(e);
+    (void)cudaGetLastError();
+    return true;
+}
+
+template <typename T>
+cudaError_t grow_device(T** p, size_t* cap, size_t need) {
+    if (*cap >= need && *p) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    size_t n = std::max(need, (size_t)1);
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    if (e == cudaSuccess) *cap = n;
+    return e;
+}
+
+template <typename T>
+cudaError_t grow_pinned(T** p, size_t* cap, size_t need) {
+    if (*cap >= need && *p) return cudaSuccess;
+    if (*p) cudaFreeHost(*p);
+    *p = nullptr;
+    *cap = 0;
+    size_t n = std::max(need, (size_t)1);
+    cudaError_t e = cudaMallocHost((void**)p, n * sizeof(T));
+    if (e == cudaSuccess) *cap = n;
+    return e;
+}
+
+bool material_has_absorption(const ix_absorption& a) {
+    if (a.has_spline) return true;
+    for (uint32_t i = 0; i < a.n_bands && i < IX_MAX_BANDS; ++i)
+        if (a.bands[i].peak != 0.0f) return true;
+    return false;
+}
+
+uint32_t pixels_per_task(uint32_t spp) {
+    uint32_t ppt = spp ? 256u / spp : 1u;
+    return std::max(1u, std::min(4u, ppt));
+}
+
+// Enqueue the trace launches for pixels [0, n_pixels) of `sc` (device planes) into
+// d_out; chunked so no single launch exceeds the path budget.  Returns the launch count
+// or -1 on a CUDA error (b->last_error set).
+int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uint32_t spp,
+                  double* d_out, int accumulate, cudaStream_t stream,
+                  const volatile int32_t* cancel, bool* cancelled) {
+    const uint32_t n_pixels = sc.width * sc.height;
+    const bool exact = b->precision == IX_PRECISION_EXACT;
+    ix::TraceLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.scene = sc;
+    L.absorbing = material_has_absorption(sc.material.abs_o) ? 1u : 0u;
+    L.sample_offset = sample_offset;
+    L.spp = spp;
+    L.pixels_per_task = pixels_per_task(spp);
+    L.accumulate = accumulate;
+    L.task_counter = b->d_counter;
+    L.dropped = b->d_dropped;
+    L.threads = (int)b->threads;
+    L.blocks = b->sm_count * (exact ? b->bps_exact : b->bps_fast);
+    if (L.blocks <= 0) L.blocks = b->sm_count > 0 ? b->sm_count : 1;
+    // Chunking: a TDR-safe first launch of at most 1M paths (gpu/frame/mod.rs:355-361),
+    // then launches of `chunk_paths` (default 64M paths), whole pixels each.
+    const uint64_t first_budget = 1u << 20;
+    const uint64_t budget = b->chunk_paths ? b->chunk_paths : (64ull << 20);
+    uint32_t begin = 0;
+    int launches = 0;
+    while (begin < n_pixels) {
+        if (cancel && *cancel) {
+            *cancelled = true;
+            return launches;
+        }
+        uint64_t paths = launches == 0 ? std::min(first_budget, budget) : budget;
+        uint64_t px = std::max<uint64_t>(1, paths / std::max<uint32_t>(spp, 1));
+        uint32_t n = (uint32_t)std::min<uint64_t>(px, n_pixels - begin);
+        L.pixel_begin = begin;
+        L.n_pixels = n;
+        L.out = d_out + (size_t)begin * 3;
+        cudaError_t e = exact ? ix::launch_trace_exact(L, stream) : ix::launch_trace_fast(L, stream);
+        if (fail(b, e, "trace launch")) return -1;
+        ++launches;
+        begin += n;
+    }
+    return launches;
+}
+
+template <typename AccT>
+int accumulate_impl(ix_backend* b, const ix_scene* scene, uint32_t sample_offset, uint32_t spp,
+                    AccT* accum, const volatile int32_t* cancel) {
+    if (!b || !scene || !accum) return IX_DECLINED;
+    if (b->lost) return IX_DECLINED;
+    if (!ix_scene_routes_to_gpu(scene)) return IX_DECLINED;
+    const uint64_t n_pixels = (uint64_t)scene->width * scene->height;
+    if (b->limits.max_pixels && n_pixels > b->limits.max_pixels) return IX_DECLINED;
+    if (b->limits.max_spp && spp > b->limits.max_spp) return IX_DECLINED;
+    if (b->limits.max_paths_per_call && n_pixels * spp > b->limits.max_paths_per_call) return IX_DECLINED;
+    if (cancel && *cancel) return IX_CANCELLED;
+    if (n_pixels == 0 || spp == 0) return IX_DONE;
+    Turn turn(b);
+    if (fail(b, cudaSetDevice(b->device), "set device")) return IX_DECLINED;
+    if (fail(b, grow_device(&b->d_planes, &b->planes_cap, (size_t)scene->n_planes * 4), "planes alloc"))
+        return IX_DECLINED;
+    if (fail(b, grow_device(&b->d_sums, &b->sums_cap, (size_t)n_pixels * 3), "sums alloc"))
+        return IX_DECLINED;
+    if (fail(b, grow_pinned(&b->h_sums, &b->hsums_cap, (size_t)n_pixels * 3), "host alloc"))
+        return IX_DECLINED;
+    if (scene->n_planes &&
+        fail(b, cudaMemcpyAsync(b->d_planes, scene->planes, (size_t)scene->n_planes * 16,
+                                cudaMemcpyHostToDevice, b->stream), "planes upload"))
+        return IX_DECLINED;
+    if (fail(b, cudaMemsetAsync(b->d_dropped, 0, sizeof(unsigned long long), b->stream), "reset"))
+        return IX_DECLINED;
+    ix_scene sc = *scene;
+    sc.planes = b->d_planes;
+    sc.facet_finishes = nullptr;
+    sc.n_finishes = 0;
+    bool cancelled = false;
+    if (fail(b, cudaEventRecord(b->ev0, b->stream), "event")) return IX_DECLINED;
+    int launches = enqueue_frame(b, sc, sample_offset, spp, b->d_sums, 0, b->stream, cancel, &cancelled);
+    if (launches < 0) return IX_DECLINED;
+    if (fail(b, cudaEventRecord(b->ev1, b->stream), "event")) return IX_DECLINED;
+    if (cancelled) {
+        cudaStreamSynchronize(b->stream);
+        return IX_CANCELLED;
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    if (fail(b, cudaMemcpyAsync(b->h_sums, b->d_sums, (size_t)n_pixels * 3 * sizeof(double),
+                                cudaMemcpyDeviceToHost, b->stream), "sums download"))
+        return IX_DECLINED;
+    unsigned long long dropped = 0;
+    if (fail(b, cudaMemcpyAsync(&dropped, b->d_dropped, sizeof(dropped), cudaMemcpyDeviceToHost,
+                                b->stream), "dropped download"))
+        return IX_DECLINED;
+    if (fail(b, cudaStreamSynchronize(b->stream), "trace")) return IX_DECLINED;
+    if (cancel && *cancel) return IX_CANCELLED;
+    for (size_t i = 0; i < (size_t)n_pixels * 3; ++i) accum[i] += (AccT)b->h_sums[i];
+    auto t1 = std::chrono::steady_clock::now();
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->timing.kernel_ms = ms;
+    b->timing.reduce_ms = std::chrono::duration<float, std::milli>(t1 - t0).count();
+    b->timing.paths = n_pixels * spp;
+    b->timing.launches = (uint32_t)launches;
+    b->dropped = dropped;
+    return IX_DONE;
+}
+
+// ------------------------------------------------------------------------------------
+// Host scene construction: the reference's host formulas, rounded as it rounds them.
+// ------------------------------------------------------------------------------------
+struct H3 {
+    float x, y, z;
+};
+inline H3 h3(float x, float y, float z) { return H3{x, y, z}; }
+inline float hdot(H3 a, H3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline H3 hcross(H3 a, H3 b) {
+    return h3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+inline H3 hnormalize(H3 a) {
+    float r = 1.0f / std::sqrt(hdot(a, a));
+    return h3(a.x * r, a.y * r, a.z * r);
+}
+inline void hstore(float* p, H3 v) {
+    p[0] = v.x;
+    p[1] = v.y;
+    p[2] = v.z;
+}
+inline float to_radians(float deg) { return deg * (3.14159265358979323846f / 180.0f); }
+
+const float kCmf[81][3] = IX_CIE1931_CMF_INIT;
+
+H3 cmf_host(float lambda) {
+    if (!(lambda >= 380.0f && lambda <= 780.0f)) return h3(0.0f, 0.0f, 0.0f);
+    float position = (lambda - 380.0f) / 5.0f;
+    int i0 = std::min((int)std::floor(position), 79);
+    float t = position - (float)i0;
+    const float* lo = kCmf[i0];
+    const float* hi = kCmf[i0 + 1];
+    return h3(lo[0] + (hi[0] - lo[0]) * t, lo[1] + (hi[1] - lo[1]) * t, lo[2] + (hi[2] - lo[2]) * t);
+}
+inline float powi5(float x) {
+    float x2 = x * x;
+    return x * (x2 * x2);
+}
+void blackbody_norm(float temp_k, float* t_k, float* den) {
+    *t_k = std::fmax(temp_k, 1000.0f);
+    float e = std::exp(std::fmin(14388000.0f / (560.0f * *t_k), 80.0f));
+    *den = std::fmax(e - 1.0f, 1e-6f);
+}
+float blackbody(float t_k, float den, float lambda) {
+    float e = std::exp(std::fmin(14388000.0f / (lambda * t_k), 80.0f));
+    float d = std::fmax(e - 1.0f, 1e-6f);
+    float v = powi5(560.0f / lambda) * (den / d);
+    return v < 0.01f ? 0.01f : (v > 20.0f ? 20.0f : v);
+}
+H3 bradford_xyz_to_lms(H3 v) {
+    return h3(std::fma(0.8951f, v.x, std::fma(0.2664f, v.y, -0.1614f * v.z)),
+              std::fma(-0.7502f, v.x, std::fma(1.7135f, v.y, 0.0367f * v.z)),
+              std::fma(0.0389f, v.x, std::fma(-0.0685f, v.y, 1.0296f * v.z)));
+}
+// compute_illuminant_white_balance (optics/raytracer/color.rs:277).
+H3 white_balance(float temp_k) {
+    float t_k, den;
+    blackbody_norm(temp_k, &t_k, &den);
+    H3 w = h3(0.0f, 0.0f, 0.0f);
+    for (int step = 0; step <= 400; ++step) {
+        float lambda = 380.0f + (float)step;
+        H3 c = cmf_host(lambda);
+        float p = blackbody(t_k, den, lambda);
+        w = h3(w.x + c.x * p, w.y + c.y * p, w.z + c.z * p);
+    }
+    float ty = std::fmax(w.y, 1e-6f);
+    const float wx = 0.3127f, wy = 0.3290f;
+    H3 target = h3((wx / wy) * ty, ty, ((1.0f - wx - wy) / wy) * ty);
+    H3 s = bradford_xyz_to_lms(w), t = bradford_xyz_to_lms(target);
+    return h3(s.x > 1e-6f ? t.x / s.x : 1.0f, s.y > 1e-6f ? t.y / s.y : 1.0f,
+              s.z > 1e-6f ? t.z / s.z : 1.0f);
+}
+
+}  // namespace
+
+extern "C" {
+
+ix_backend* ix_backend_create(const ix_backend_options* opts) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        (void)cudaGetLastError();
+        return nullptr;
+    }
+    ix_backend* b = new ix_backend();
+    if (opts) {
+        b->device = opts->device;
+        b->pipeline = opts->pipeline;
+        b->precision = opts->precision;
+        if (opts->threads_per_block) b->threads = opts->threads_per_block;
+        b->chunk_paths = opts->chunk_paths;
+    }
+    if (b->device < 0 || b->device >= n || b->threads % 32 || b->threads > 128 || b->threads == 0) {
+        delete b;
+        return nullptr;
+    }
+    cudaDeviceProp prop;
+    if (cudaSetDevice(b->device) != cudaSuccess ||
+        cudaGetDeviceProperties(&prop, b->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaMalloc((void**)&b->d_counter, sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc((void**)&b->d_dropped, sizeof(unsigned long long)) != cudaSuccess) {
+        (void)cudaGetLastError();
+        ix_backend_destroy(b);
+        return nullptr;
+    }
+    b->sm_count = prop.multiProcessorCount;
+    b->label = prop.name;
+    b->bps_exact = std::max(1, ix::trace_blocks_per_sm_exact((int)b->threads, nullptr));
+    b->bps_fast = std::max(1, ix::trace_blocks_per_sm_fast((int)b->threads, nullptr));
+    return b;
+}
+
+void ix_backend_destroy(ix_backend* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    cudaFree(b->d_planes);
+    cudaFree(b->d_sums);
+    cudaFree(b->d_counter);
+    cudaFree(b->d_dropped);
+    cudaFree(b->d_check);
+    if (b->h_sums) cudaFreeHost(b->h_sums);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    (void)cudaGetLastError();
+    delete b;
+}
+
+int ix_backend_label(const ix_backend* b, char* buf, size_t len) {
+    if (!b || !buf || len == 0) return -1;
+    std::snprintf(buf, len, "%s", b->label.c_str());
+    return 0;
+}
+
+void ix_set_pipeline_kind(ix_backend* b, uint32_t kind) {
+    if (b) b->pipeline = kind;
+}
+
+void ix_set_work_limits(ix_backend* b, const ix_work_limits* limits) {
+    if (b && limits) b->limits = *limits;
+}
+
+void ix_set_precision(ix_backend* b, uint32_t precision) {
+    if (b) b->precision = precision ? IX_PRECISION_EXACT : IX_PRECISION_FAST;
+}
+
+int ix_scene_routes_to_gpu(const ix_scene* s) {
+    if (!s) return 0;
+    if (s->n_planes > IX_MAX_PLANES || (s->n_planes && !s->planes)) return 0;
+    if (s->width == 0 || s->height == 0) return 0;
+    const ix_material& m = s->material;
+    if (m.anisotropic || m.scattering_sigma_s > 0.0f || m.edge_rounding_radius > 0.0f) return 0;
+    if (s->facet_finishes)
+        for (uint32_t i = 0; i < s->n_finishes; ++i)
+            if (s->facet_finishes[i] != 0) return 0;
+    const ix_environment& e = s->environment;
+    if (e.model != IX_ENV_STUDIO && e.model != IX_ENV_ISO_HEMISPHERE && e.model != IX_ENV_UNIFORM) return 0;
+    if (m.dispersion.kind > IX_DISP_CAUCHY) return 0;
+    return 1;
+}
+
+int ix_accumulate(ix_backend* b, const ix_scene* scene, uint32_t sample_offset, uint32_t spp,
+                  float* accum_xyz, const volatile int32_t* cancel) {
+    return accumulate_impl<float>(b, scene, sample_offset, spp, accum_xyz, cancel);
+}
+
+int ix_accumulate_f64(ix_backend* b, const ix_scene* scene, uint32_t sample_offset,
+                      uint32_t spp, double* accum_xyz, const volatile int32_t* cancel) {
+    return accumulate_impl<double>(b, scene, sample_offset, spp, accum_xyz, cancel);
+}
+
+int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items,
+                        const volatile int32_t* cancel) {
+    if (!b || (!items && n_items)) return IX_DECLINED;
+    int overall = IX_DONE;
+    for (uint32_t i = 0; i < n_items; ++i) {
+        if (cancel && *cancel) {
+            for (uint32_t j = i; j < n_items; ++j) items[j].status = IX_CANCELLED;
+            return IX_CANCELLED;
+        }
+        int st = accumulate_impl<double>(b, items[i].scene, items[i].sample_offset, items[i].spp,
+                                         items[i].accum_xyz, cancel);
+        items[i].status = st;
+        if (st != IX_DONE && overall == IX_DONE) overall = st;
+    }
+    return overall;
+}
+
+int ix_accumulate_device(ix_backend* b, const ix_scene* scene, uint32_t sample_offset,
+                         uint32_t spp, double* d_accum_xyz, int accumulate, void* stream) {
+    if (!b || !scene || !d_accum_xyz) return IX_DECLINED;
+    if (b->lost || !ix_scene_routes_to_gpu(scene)) return IX_DECLINED;
+    if ((uint64_t)scene->width * scene->height == 0 || spp == 0) return IX_DONE;
+    Turn turn(b);
+    cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+    if (fail(b, cudaSetDevice(b->device), "set device")) return IX_DECLINED;
+    bool cancelled = false;
+    if (fail(b, cudaEventRecord(b->ev0, st), "event")) return IX_DECLINED;
+    int launches = enqueue_frame(b, *scene, sample_offset, spp, d_accum_xyz, accumulate, st, nullptr, &cancelled);
+    if (launches < 0) return IX_DECLINED;
+    if (fail(b, cudaEventRecord(b->ev1, st), "event")) return IX_DECLINED;
+    b->timing.paths = (uint64_t)scene->width * scene->height * spp;
+    b->timing.launches = (uint32_t)launches;
+    return IX_DONE;
+}
+
+int ix_is_lost(const ix_backend* b) { return b ? (b->lost ? 1 : 0) : 1; }
+
+int ix_try_recover(ix_backend* b) {
+    if (!b) return 0;
+    if (!b->lost) return 1;
+    // A sticky device error needs a fresh context; probe with a synchronize.
+    cudaSetDevice(b->device);
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    (void)cudaGetLastError();
+    if (e == cudaSuccess) {
+        b->lost = false;
+        b->last_error.clear();
+        return 1;
+    }
+    return 0;
+}
+
+int ix_last_error(const ix_backend* b, char* buf, size_t len) {
+    if (!b || !buf || len == 0) return -1;
+    std::snprintf(buf, len, "%s", b->last_error.c_str());
+    return (int)b->last_error.size();
+}
+
+int ix_last_timing(const ix_backend* b, ix_timing* out) {
+    if (!b || !out) return -1;
+    ix_timing t = b->timing;
+    if (t.launches && b->ev1) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, b->ev0, b->ev1) == cudaSuccess) t.kernel_ms = ms;
+        (void)cudaGetLastError();
+    }
+    *out = t;
+    return 0;
+}
+
+uint64_t ix_last_dropped(const ix_backend* b) { return b ? b->dropped : 0; }
+
+int ix_probe_fp32_peak(ix_backend* b, double* flops) {
+    if (!b || !flops) return -1;
+    Turn turn(b);
+    if (fail(b, cudaSetDevice(b->device), "set device")) return -1;
+    if (fail(b, ix::fp32_probe(b->sm_count, 5, b->stream, flops), "fp32 probe")) return -1;
+    return 0;
+}
+
+void ix_camera_new(float yaw, float pitch, float distance, float fov_deg, ix_camera* out) {
+    float cos_p = std::cos(pitch), sin_p = std::sin(pitch), cos_y = std::cos(yaw), sin_y = std::sin(yaw);
+    H3 origin = h3(distance * cos_p * sin_y, distance * sin_p, distance * cos_p * cos_y);
+    H3 forward = hnormalize(h3(-origin.x, -origin.y, -origin.z));
+    H3 world_up = std::fabs(cos_p) < 1e-4f ? h3(0.0f, 0.0f, -1.0f)
+                  : (cos_p < 0.0f ? h3(0.0f, -1.0f, 0.0f) : h3(0.0f, 1.0f, 0.0f));
+    H3 right = hnormalize(hcross(forward, world_up));
+    H3 up = hnormalize(hcross(right, forward));
+    hstore(out->origin, origin);
+    hstore(out->forward, forward);
+    hstore(out->right, right);
+    hstore(out->up, up);
+    out->fov_tan = std::tan(to_radians(fov_deg) * 0.5f);
+}
+
+int ix_environment_preset(int32_t preset, float exposure, float light_yaw, float light_pitch,
+                          float backdrop, float surface_glare, float head_shadow_deg,
+                          ix_environment* out) {
+    if (!out) return -1;
+    std::memset(out, 0, sizeof(*out));
+    float temp_k, spot;
+    bool d65;
+    uint32_t model;
+    switch (preset) {
+        case 1: model = IX_ENV_ISO_HEMISPHERE; temp_k = 6500.0f; spot = 1.0f; d65 = true; break;
+        case 7: model = IX_ENV_STUDIO; temp_k = 6500.0f; spot = 1.0f; d65 = true; break;
+        case 8: model = IX_ENV_STUDIO; temp_k = 3200.0f; spot = 1.2f; d65 = false; break;
+        case 9: model = IX_ENV_STUDIO; temp_k = 2856.0f; spot = 1.2f; d65 = false; break;
+        case 10: model = IX_ENV_STUDIO; temp_k = 5000.0f; spot = 1.6f; d65 = false; break;
+        case 11: model = IX_ENV_STUDIO; temp_k = 6000.0f; spot = 2.4f; d65 = false; break;
+        default: return -1;
+    }
+    out->model = model;
+    out->spectrum = d65 ? IX_SPEC_D65 : IX_SPEC_BLACKBODY;
+    out->exposure = exposure;
+    out->spot_mult = spot;
+    out->ambient_fill = 1;
+    out->backdrop = backdrop;
+    out->surface_glare = (surface_glare >= 1.0f || std::isnan(surface_glare)) ? 1.0f
+                         : (surface_glare > 0.0f ? surface_glare : 0.0f);
+    float deg = head_shadow_deg;
+    if (std::isnan(deg)) deg = 16.0f;
+    else if (deg <= 0.0f) deg = 0.0f;
+    else if (deg < 3.0f) deg = 3.0f;
+    else if (deg > 88.0f) deg = 88.0f;
+    if (deg == 16.0f) {
+        out->shadow_cos[0] = 0.9510565f;
+        out->shadow_cos[1] = 0.9702957f;
+    } else if (deg <= 0.0f) {
+        out->shadow_cos[0] = 2.0f;
+        out->shadow_cos[1] = 3.0f;
+    } else {
+        out->shadow_cos[0] = std::cos(to_radians(deg + 2.0f));
+        out->shadow_cos[1] = std::cos(to_radians(deg - 2.0f));
+    }
+    float t_k, den;
+    blackbody_norm(temp_k, &t_k, &den);
+    out->bb_t_k = t_k;
+    out->bb_denom_560 = den;
+    float cp = std::cos(light_pitch), sp = std::sin(light_pitch);
+    float cy = std::cos(light_yaw), sy = std::sin(light_yaw);
+    hstore(out->key_dir, hnormalize(h3(cp * sy, sp, cp * cy)));
+    const float PI = 3.14159265358979323846f;
+    float fill_yaw = std::fma(PI, 0.78f, light_yaw);
+    float fp = light_pitch * 0.65f;
+    fp = fp < 0.15f ? 0.15f : (fp > 1.2f ? 1.2f : fp);
+    hstore(out->fill_dir, hnormalize(h3(std::cos(fp) * std::sin(fill_yaw), std::sin(fp),
+                                        std::cos(fp) * std::cos(fill_yaw))));
+    float step = PI * 2.0f / 16.0f;
+    for (int i = 0; i < IX_RING_LIGHTS; ++i) {
+        float a = std::fma((float)i, step, light_yaw);
+        hstore(out->ring_dirs[i], hnormalize(h3(std::sin(a) * 0.75f, sp * 0.8f, std::cos(a) * 0.75f)));
+    }
+    if (!d65) {
+        out->white_balance = 1;
+        hstore(out->wb_lms, white_balance(temp_k));
+    } else {
+        out->white_balance = 0;
+        out->wb_lms[0] = out->wb_lms[1] = out->wb_lms[2] = 1.0f;
+    }
+    return 0;
+}
+
+void ix_environment_uniform(float radiance, ix_environment* out) {
+    if (!out) return;
+    std::memset(out, 0, sizeof(*out));
+    out->model = IX_ENV_UNIFORM;
+    out->spectrum = IX_SPEC_FLAT;
+    out->exposure = 1.0f;
+    out->surface_glare = 1.0f;
+    out->wb_lms[0] = out->wb_lms[1] = out->wb_lms[2] = 1.0f;
+    out->uniform_radiance = radiance;
+}
+
+int ix_debug_check(ix_backend* b, const ix_scene* scene, int32_t fn, uint32_t n,
+                   const uint32_t* in, uint32_t in_stride, uint32_t* out, uint32_t out_stride) {
+    if (!b || !scene || (n && (!in || !out))) return -1;
+    if (scene->n_planes > IX_MAX_PLANES) return -1;
+    Turn turn(b);
+    if (fail(b, cudaSetDevice(b->device), "set device")) return -1;
+    size_t in_words = (size_t)n * in_stride, out_words = (size_t)n * out_stride;
+    if (fail(b, grow_device(&b->d_check, &b->check_cap, in_words + out_words + 1), "check alloc")) return -1;
+    if (fail(b, grow_device(&b->d_planes, &b->planes_cap, (size_t)scene->n_planes * 4 + 4), "planes alloc"))
+        return -1;
+    if (scene->n_planes &&
+        fail(b, cudaMemcpyAsync(b->d_planes, scene->planes, (size_t)scene->n_planes * 16,
+                                cudaMemcpyHostToDevice, b->stream), "planes upload"))
+        return -1;
+    if (in_words && fail(b, cudaMemcpyAsync(b->d_check, in, in_words * 4, cudaMemcpyHostToDevice, b->stream),
+                         "check upload"))
+        return -1;
+    ix::CheckLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.scene = *scene;
+    L.scene.planes = b->d_planes;
+    L.scene.facet_finishes = nullptr;
+    L.absorbing = material_has_absorption(scene->material.abs_o) ? 1u : 0u;
+    L.fn = fn;
+    L.n = n;
+    L.in_stride = in_stride;
+    L.out_stride = out_stride;
+    L.in = b->d_check;
+    L.out = b->d_check + in_words;
+    cudaError_t e = b->precision == IX_PRECISION_EXACT ? ix::launch_check_exact(L, b->stream)
+                                                        : ix::launch_check_fast(L, b->stream);
+    if (fail(b, e, "check launch")) return -1;
+    if (out_words && fail(b, cudaMemcpyAsync(out, L.out, out_words * 4, cudaMemcpyDeviceToHost, b->stream),
+                          "check download"))
+        return -1;
+    if (fail(b, cudaStreamSynchronize(b->stream), "check")) return -1;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,492 @@
+// ix_device.cuh -- device-side building blocks of the spectral transport (sm_100a).
+//
+// Every function here is the GPU form of one step of the reference's per-sample
+// estimator; the comment on each names the reference file:line whose arithmetic it
+// reproduces.  The operation order follows the reference's scalar code (glam's
+// left-associated dot products, separate multiply and add, `fmaf` exactly where the
+// reference calls `mul_add`).  The library builds this code twice:
+//   * IX_EXACT=1 with -fmad=false: no multiply-add contraction, so every step that has
+//     no transcendental rounds exactly as the CPU tracer does;
+//   * IX_EXACT=0 with contraction: the compiler may fuse a*b+c (faster, and each fused
+//     step is at least as accurate).
+// Division and square root are IEEE round-to-nearest in both builds.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/ix_cie_tables.h"
+#include "../../include/ix_scene.h"
+
+#ifndef IX_EXACT
+#define IX_EXACT 0
+#endif
+
+#define IX_DEV __device__ __forceinline__
+
+namespace ix {
+
+// ------------------------------------------------------------------------------------
+// Vector type (glam Vec3 scalar order).
+// ------------------------------------------------------------------------------------
+struct V3 {
+    float x, y, z;
+};
+IX_DEV V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+IX_DEV V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+IX_DEV V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+IX_DEV V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
+IX_DEV V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+IX_DEV V3 operator*(float s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
+IX_DEV float dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+IX_DEV V3 cross(V3 a, V3 b) {
+    return v3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+IX_DEV float length_squared(V3 a) { return dot(a, a); }
+// glam normalize: v * (1 / sqrt(dot(v, v))), IEEE divide and sqrt.
+IX_DEV V3 normalize(V3 a) {
+    float rcp = 1.0f / sqrtf(dot(a, a));
+    return a * rcp;
+}
+IX_DEV V3 normalize_or_zero(V3 a) {
+    float rcp = 1.0f / sqrtf(dot(a, a));
+    if (isfinite(rcp) && rcp > 0.0f) return a * rcp;
+    return v3(0.0f, 0.0f, 0.0f);
+}
+IX_DEV V3 load3(const float* p) { return v3(p[0], p[1], p[2]); }
+// f32::clamp: `if x < lo {lo}`, then `if x > hi {hi}`.
+IX_DEV float clampf_(float x, float lo, float hi) {
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
+}
+// f32::midpoint on x86_64 rounds (a + b) / 2 once; for finite operands whose sum is a
+// normal number (every use here: squared amplitudes in [0, 4]) halving a correctly
+// rounded sum is that same value.
+IX_DEV float midpointf_(float a, float b) { return (a + b) * 0.5f; }
+
+// ------------------------------------------------------------------------------------
+// Stokes vectors and the Mueller matrices the transport applies
+// (optics/polarization.rs:117-191).  The matrices are sparse; only their non-zero
+// entries are multiplied, in glam's Mat4 * Vec4 column order.
+// ------------------------------------------------------------------------------------
+struct Stokes {
+    float i, q, u, v;
+};
+IX_DEV float intensity(const Stokes& s) { return fmaxf(s.i, 0.0f); }
+IX_DEV Stokes scale(const Stokes& s, float k) {
+    return Stokes{s.i * k, s.q * k, s.u * k, s.v * k};
+}
+// frame_rotation(psi): cols (1,0,0,0), (0,c2,-s2,0), (0,s2,c2,0), (0,0,0,1).
+IX_DEV Stokes rotate(const Stokes& s, float c2, float s2) {
+    return Stokes{s.i, c2 * s.q + s2 * s.u, (-s2) * s.q + c2 * s.u, s.v};
+}
+// fresnel_reflection / fresnel_transmission share the (a, b, c) form
+// cols (a,b,0,0), (b,a,0,0), (0,0,c,0), (0,0,0,c).
+IX_DEV Stokes apply_abc(const Stokes& s, float a, float b, float c) {
+    return Stokes{a * s.i + b * s.q, b * s.i + a * s.q, c * s.u, c * s.v};
+}
+// MuellerMatrix::fresnel_reflection (polarization.rs:148).
+IX_DEV Stokes fresnel_reflect_apply(const Stokes& s, float r_s, float r_p) {
+    float rs2 = r_s * r_s;
+    float rp2 = r_p * r_p;
+    float a = midpointf_(rs2, rp2);
+    float b = 0.5f * (rs2 - rp2);
+    float c = r_s * r_p;
+    return apply_abc(s, a, b, c);
+}
+// MuellerMatrix::fresnel_transmission (polarization.rs:162).
+IX_DEV Stokes fresnel_transmit_apply(const Stokes& s, float n1, float n2, float cos_i,
+                                     float cos_t, float t_s, float t_p) {
+    float factor = (n2 * cos_t) / fmaxf(n1 * cos_i, 1e-6f);
+    float ts2 = t_s * t_s * factor;
+    float tp2 = t_p * t_p * factor;
+    float a = midpointf_(ts2, tp2);
+    float b = 0.5f * (ts2 - tp2);
+    float c = t_s * t_p * factor;
+    return apply_abc(s, a, b, c);
+}
+// MuellerMatrix::tir_retardation (polarization.rs:184):
+// cols (1,0,0,0), (0,1,0,0), (0,0,cd,-sd), (0,0,sd,cd).
+IX_DEV Stokes tir_retard_apply(const Stokes& s, float delta) {
+    float sd, cd;
+    sincosf(delta, &sd, &cd);
+    return Stokes{s.i, s.q, cd * s.u + sd * s.v, (-sd) * s.u + cd * s.v};
+}
+
+// ------------------------------------------------------------------------------------
+// Sampler (optics/raytracer/sampling.rs).
+// ------------------------------------------------------------------------------------
+constexpr uint32_t FRESNEL_BRANCH_STREAM = 0x9E3779B1u;            // sampling.rs:13
+constexpr uint32_t RUSSIAN_ROULETTE_STREAM = 0x517CC1B7u;          // sampling.rs:14
+constexpr uint32_t PIXEL_JITTER_X_ROTATION_STREAM = 0xA511E9B3u;   // sampling.rs:95
+constexpr uint32_t PIXEL_JITTER_Y_ROTATION_STREAM = 0x63D81B23u;   // sampling.rs:97
+constexpr uint32_t HERO_WAVELENGTH_ROTATION_STREAM = 0x1B873593u;  // sampling.rs:99
+
+// hash_u32 (sampling.rs:66).
+IX_DEV uint32_t hash_u32(uint32_t x) {
+    x *= 0x85EBCA6Bu;
+    x ^= x >> 13;
+    x *= 0xC2B2AE35u;
+    x ^= x >> 16;
+    return x;
+}
+// `(h as f32) / 4_294_967_295.0` -- the divisor rounds to 2^32, so the quotient is the
+// exact scaling of the round-to-nearest conversion.
+IX_DEV float unit_from_hash(uint32_t h) { return __uint2float_rn(h) * 2.3283064365386963e-10f; }
+IX_DEV float unit_draw(uint32_t seed, uint32_t bounce, uint32_t stream) {
+    return unit_from_hash(hash_u32(seed ^ hash_u32(bounce ^ stream)));
+}
+// low_discrepancy_base2 (sampling.rs:110).
+IX_DEV float low_discrepancy_base2(uint32_t n) {
+    return __uint2float_rn(__brev(n)) * 2.3283064365386963e-10f;
+}
+// radical_inverse_base (sampling.rs:127): fused digit accumulation, IEEE divides.
+IX_DEV float radical_inverse_base(uint32_t n, uint32_t base) {
+    uint32_t remaining = n;
+    float val = 0.0f;
+    float fb = __uint2float_rn(base);
+    float inv_base = 1.0f / fb;
+    while (remaining > 0) {
+        uint32_t digit = remaining % base;
+        val = fmaf(__uint2float_rn(digit), inv_base, val);
+        inv_base = inv_base / fb;
+        remaining /= base;
+    }
+    return val;
+}
+// cranley_patterson_rotate (sampling.rs:148).
+IX_DEV float cranley_patterson_rotate(float x, float offset) {
+    float sum = x + offset;
+    return sum - floorf(sum);
+}
+struct Draws {
+    uint32_t seed;
+    float jx, jy, hero;
+};
+// pixel_rotations (sampling.rs:176) + sample_draws (sampling.rs:206).
+IX_DEV Draws sample_draws(uint32_t pixel, uint32_t sample) {
+    float rx = low_discrepancy_base2(hash_u32(pixel ^ PIXEL_JITTER_X_ROTATION_STREAM));
+    float ry = low_discrepancy_base2(hash_u32(pixel ^ PIXEL_JITTER_Y_ROTATION_STREAM));
+    float rh = low_discrepancy_base2(hash_u32(pixel ^ HERO_WAVELENGTH_ROTATION_STREAM));
+    Draws d;
+    d.seed = hash_u32((pixel * 0x9E3779B9u) ^ (sample * 0x85EBCA6Bu));
+    d.jx = cranley_patterson_rotate(low_discrepancy_base2(sample), rx) - 0.5f;
+    d.jy = cranley_patterson_rotate(radical_inverse_base(sample, 3), ry) - 0.5f;
+    d.hero = cranley_patterson_rotate(radical_inverse_base(sample, 5), rh);
+    return d;
+}
+
+// ------------------------------------------------------------------------------------
+// Camera (camera.rs:149) and the hero comb (transport/mod.rs:58).
+// ------------------------------------------------------------------------------------
+struct Ray {
+    V3 origin, dir;
+};
+IX_DEV Ray generate_ray(const ix_camera& c, float sx, float sy, float w, float h, float jx,
+                        float jy) {
+    float aspect = w / h;
+    float u = ((sx + jx) / w - 0.5f) * 2.0f * aspect * c.fov_tan;
+    float v = (0.5f - (sy + jy) / h) * 2.0f * c.fov_tan;
+    V3 dir = normalize(load3(c.forward) + load3(c.right) * u + load3(c.up) * v);
+    return Ray{load3(c.origin), dir};
+}
+IX_DEV float rem_euclid_400(float a) {
+    float r = fmodf(a, 400.0f);
+    return (r < 0.0f) ? r + 400.0f : r;
+}
+IX_DEV void hero_wavelengths(float hero_rand, float out[8]) {
+    float lambda_hero = fmaf(hero_rand, 400.0f, 380.0f);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        float offset = fmaf((float)k, 50.0f, lambda_hero - 380.0f);
+        out[k] = 380.0f + rem_euclid_400(offset);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Dispersion (optics/dispersion.rs:149-210).
+// ------------------------------------------------------------------------------------
+IX_DEV float dispersion_unclamped(const ix_dispersion& d, float lambda_nm) {
+    float um = lambda_nm * 1e-3f;
+    float l2 = um * um;
+    if (d.kind == IX_DISP_SELLMEIER1) {
+        float n2 = 1.0f + (d.b[0] * l2) / (l2 - d.c[0]);
+        return sqrtf(fmaxf(n2, 1.0f));
+    }
+    if (d.kind == IX_DISP_SELLMEIER3) {
+        float n2 = 1.0f;
+        n2 += (d.b[0] * l2) / (l2 - d.c[0]);
+        n2 += (d.b[1] * l2) / (l2 - d.c[1]);
+        n2 += (d.b[2] * l2) / (l2 - d.c[2]);
+        return sqrtf(fmaxf(n2, 1.0f));
+    }
+    float l4 = l2 * l2;
+    return fmaxf((d.b[0] + d.b[1] / l2) + d.b[2] / l4, 1.0f);
+}
+IX_DEV float dispersion_min_valid_nm(const ix_dispersion& d) {
+    if (d.kind == IX_DISP_CAUCHY) return 380.0f;
+    int n = (d.kind == IX_DISP_SELLMEIER1) ? 1 : 3;
+    float floor_nm = 300.0f;
+    for (int i = 0; i < n; ++i) {
+        float c = d.c[i];
+        if (c > 0.0f) {
+            float pole = sqrtf(c) * 1e3f;
+            if (pole < 380.0f) floor_nm = fmaxf(floor_nm, pole * 1.05f);
+        }
+    }
+    return fminf(floor_nm, 380.0f);
+}
+IX_DEV float dispersion_eval(const ix_dispersion& d, float lambda_nm) {
+    if (lambda_nm < 380.0f)
+        return dispersion_unclamped(d, fmaxf(lambda_nm, dispersion_min_valid_nm(d)));
+    return dispersion_unclamped(d, lambda_nm);
+}
+
+// ------------------------------------------------------------------------------------
+// Absorption alpha(lambda): Gaussian bands (optics/absorption.rs:108) plus the uniform
+// Catmull-Rom knot table (ix_scene.h), and the Cephes-style exponential the reference
+// applies per channel (simd/exp_poly.rs:37, its own constants).
+// ------------------------------------------------------------------------------------
+IX_DEV float band_eval(const ix_band& b, float lambda_nm) {
+    if (b.shape == IX_BAND_GAUSS_WAVELENGTH) {
+        float t = (lambda_nm - b.center_nm) / b.width_nm;
+        return b.peak * expf(-0.5f * t * t);
+    }
+    float delta_nm = b.center_nm - lambda_nm;
+    float nu_diff = 1.0e7f * delta_nm / (lambda_nm * b.center_nm);
+    float t = nu_diff / b.width_nm;
+    return b.peak * expf(-0.5f * t * t);
+}
+IX_DEV float spline_eval(const float* knots, float lambda_nm) {
+    const int n = IX_SPLINE_KNOTS;
+    float pos = (clampf_(lambda_nm, 380.0f, 780.0f) - 380.0f) * ((float)(n - 1) / 400.0f);
+    int s = (int)floorf(pos);
+    s = s > n - 2 ? n - 2 : (s < 0 ? 0 : s);
+    float t = pos - (float)s;
+    float p0 = knots[s > 0 ? s - 1 : 0];
+    float p1 = knots[s];
+    float p2 = knots[s + 1];
+    float p3 = knots[s + 2 < n ? s + 2 : n - 1];
+    float a = 3.0f * p1 - p0 - 3.0f * p2 + p3;
+    float b = 2.0f * p0 - 5.0f * p1 + 4.0f * p2 - p3;
+    float c = p2 - p0;
+    float poly = fmaf(fmaf(fmaf(a, t, b), t, c), t, 2.0f * p1);
+    return fmaxf(0.5f * poly, 0.0f);
+}
+IX_DEV float spectral_absorption(const ix_absorption& a, float lambda_nm) {
+    float sum = 0.0f;
+    bool first = true;
+    for (uint32_t i = 0; i < a.n_bands && i < IX_MAX_BANDS; ++i) {
+        float v = band_eval(a.bands[i], lambda_nm);
+        sum = first ? v : sum + v;
+        first = false;
+    }
+    if (a.has_spline) {
+        float v = spline_eval(a.spline, lambda_nm);
+        sum = first ? v : sum + v;
+    }
+    return sum;
+}
+IX_DEV float exp_lane(float x) {
+    const float LOG2E = 1.44269504088896340736f;
+    const float C1 = __uint_as_float(0x3F318000u);
+    const float C2 = -2.1219444e-4f;
+    float upper = (x < 88.02875f) ? x : 88.02875f;
+    x = (upper > -87.33654f) ? upper : -87.33654f;
+    float n = floorf(fmaf(x, LOG2E, 0.5f));
+    x = fmaf(n, -C1, x);
+    x = fmaf(n, -C2, x);
+    float z = x * x;
+    float p = 1.9875691e-4f;
+    p = fmaf(p, x, 1.3981999e-3f);
+    p = fmaf(p, x, 8.333452e-3f);
+    p = fmaf(p, x, 4.1665796e-2f);
+    p = fmaf(p, x, 1.6666665e-1f);
+    p = fmaf(p, x, 5.0000003e-1f);
+    p = fmaf(p, z, x) + 1.0f;
+    int e = (int)n;
+    return p * __int_as_float((e + 127) << 23);
+}
+
+// ------------------------------------------------------------------------------------
+// Colour tables and spectral integration (color/cie1931.rs:157; environment/spectral.rs:28).
+// ------------------------------------------------------------------------------------
+__constant__ float c_cmf[81][3] = IX_CIE1931_CMF_INIT;
+__constant__ float c_d65[41] = IX_CIE_D65_SPD_INIT;
+__constant__ float c_d65_uv[9] = IX_CIE_D65_UV_SPD_INIT;
+
+IX_DEV V3 cmf(float lambda_nm) {
+    if (!(lambda_nm >= 380.0f && lambda_nm <= 780.0f)) return v3(0.0f, 0.0f, 0.0f);
+    float position = (lambda_nm - 380.0f) / 5.0f;
+    int i0 = (int)floorf(position);
+    i0 = i0 > 79 ? 79 : i0;
+    float t = position - (float)i0;
+    float l0 = c_cmf[i0][0], l1 = c_cmf[i0][1], l2 = c_cmf[i0][2];
+    float h0 = c_cmf[i0 + 1][0], h1 = c_cmf[i0 + 1][1], h2 = c_cmf[i0 + 1][2];
+    return v3(l0 + (h0 - l0) * t, l1 + (h1 - l1) * t, l2 + (h2 - l2) * t);
+}
+IX_DEV float d65(float lambda_nm) {
+    if (lambda_nm < 380.0f) {
+        float clamped = fmaxf(lambda_nm, 300.0f);
+        float position = (clamped - 300.0f) / 10.0f;
+        int i0 = (int)floorf(position);
+        i0 = i0 > 7 ? 7 : i0;
+        float frac = position - (float)i0;
+        float v0 = c_d65_uv[i0], v1 = c_d65_uv[i0 + 1];
+        return fmaf(frac, v1 - v0, v0) / 100.0f;
+    }
+    float clamped = clampf_(lambda_nm, 380.0f, 780.0f);
+    float position = (clamped - 380.0f) / 10.0f;
+    int i0 = (int)floorf(position);
+    i0 = i0 > 39 ? 39 : i0;
+    float frac = position - (float)i0;
+    float v0 = c_d65[i0], v1 = c_d65[i0 + 1];
+    return fmaf(frac, v1 - v0, v0) / 100.0f;
+}
+// powi with a constant exponent: x^(2^i) factors multiplied in ascending bit order.
+IX_DEV float powi5(float x) {
+    float x2 = x * x;
+    return x * (x2 * x2);
+}
+IX_DEV float powi6(float x) {
+    float x2 = x * x;
+    return x2 * (x2 * x2);
+}
+IX_DEV float powi18(float x) {
+    float x2 = x * x, x4 = x2 * x2, x8 = x4 * x4, x16 = x8 * x8;
+    return x2 * x16;
+}
+IX_DEV float powi28(float x) {
+    float x2 = x * x, x4 = x2 * x2, x8 = x4 * x4, x16 = x8 * x8;
+    return (x4 * x8) * x16;
+}
+// blackbody_spectrum_with (environment/spectral.rs:62).
+IX_DEV float blackbody(float t_k, float denom_560, float lambda_nm) {
+    float exp_val = expf(fminf(14388000.0f / (lambda_nm * t_k), 80.0f));
+    float denom = fmaxf(exp_val - 1.0f, 1e-6f);
+    float ratio = denom_560 / denom;
+    return clampf_(powi5(560.0f / lambda_nm) * ratio, 0.01f, 20.0f);
+}
+IX_DEV float spectral_power(const ix_environment& env, float lambda_nm) {
+    if (env.spectrum == IX_SPEC_D65) return d65(lambda_nm);
+    if (env.spectrum == IX_SPEC_BLACKBODY) return blackbody(env.bb_t_k, env.bb_denom_560, lambda_nm);
+    return 1.0f;
+}
+
+// ------------------------------------------------------------------------------------
+// Environment (environment/rig.rs:67-377): the direction-only lighting, then the
+// per-wavelength radiance built from it.
+// ------------------------------------------------------------------------------------
+IX_DEV float smoothstep_(float e0, float e1, float x) {
+    float t = clampf_((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * fmaf(-2.0f, t, 3.0f);
+}
+struct Lighting {
+    float factor;  // scaled models: radiance = factor * (spec * exposure)
+    float bg, softbox, fill, ground, horizon;
+    float ring[4];
+    int ring_len;  // ring emitters lit for this direction (at most 4 overlap)
+    bool has_softbox, has_fill, has_ground;
+};
+IX_DEV Lighting direction_lighting(const ix_environment& env, V3 dir, V3 observer) {
+    Lighting L;
+    L.factor = 0.0f;
+    L.ring_len = 0;
+    L.has_softbox = L.has_fill = L.has_ground = false;
+    L.bg = L.softbox = L.fill = L.ground = L.horizon = 0.0f;
+    if (env.model == IX_ENV_UNIFORM) return L;
+    V3 d = normalize(dir);
+    float tray = env.backdrop;
+    if (env.model == IX_ENV_ISO_HEMISPHERE) {
+        float horizon = smoothstep_(-0.05f, 0.05f, d.y);
+        float vis = 1.0f - smoothstep_(env.shadow_cos[0], env.shadow_cos[1], dot(d, observer));
+        L.factor = (tray > 0.0f) ? fmaf((1.0f - horizon) * vis, tray, horizon * vis) : horizon * vis;
+        return L;
+    }
+    float exposure = env.exposure;
+    float spot = env.spot_mult;
+    L.bg = env.ambient_fill ? fmaxf(fmaf(0.012f, fmaf(d.y, 0.5f, 0.5f), 0.015f), 0.005f) * exposure
+                            : 0.0f;
+    float key_dot = fmaxf(dot(d, load3(env.key_dir)), 0.0f);
+    if (key_dot > 0.0f) {
+        L.has_softbox = true;
+        L.softbox = powi28(key_dot) * 12.0f * spot * exposure;
+    }
+    float fill_dot = fmaxf(dot(d, load3(env.fill_dir)), 0.0f);
+    if (fill_dot > 0.0f) {
+        L.has_fill = true;
+        L.fill = powi18(fill_dot) * 4.5f * exposure;
+    }
+    for (int i = 0; i < IX_RING_LIGHTS; ++i) {
+        float ring_dot = fmaxf(dot(d, load3(env.ring_dirs[i])), 0.0f);
+        if (ring_dot > 0.96f && L.ring_len < 4) {
+            float spark = (ring_dot - 0.96f) / 0.04f;
+            L.ring[L.ring_len++] = powi6(spark) * 22.0f * spot * exposure;
+        }
+    }
+    if (tray > 0.0f) {
+        L.has_ground = true;
+        L.horizon = smoothstep_(-0.05f, 0.05f, d.y);
+        L.ground = ((1.0f - L.horizon) * tray) * exposure;
+    }
+    return L;
+}
+IX_DEV float lighting_radiance(const Lighting& L, const ix_environment& env, float spec) {
+    if (env.model == IX_ENV_UNIFORM) return env.uniform_radiance * spec;
+    if (env.model != IX_ENV_STUDIO) return L.factor * (spec * env.exposure);
+    float r = L.bg * spec;
+    if (L.has_softbox) r = fmaf(L.softbox, spec, r);
+    if (L.has_fill) r = fmaf(L.fill, spec, r);
+    for (int i = 0; i < L.ring_len; ++i) r = fmaf(L.ring[i], spec, r);
+    if (L.has_ground) return fmaf(L.horizon, r, L.ground * spec);
+    return r;
+}
+
+// ------------------------------------------------------------------------------------
+// Convex slab intersection over the CTA's shared-memory plane cache
+// (simd/slab.rs:120-160; intersect.rs:101-127).
+// ------------------------------------------------------------------------------------
+struct Hit {
+    float t;
+    int facet;  // -1: no hit
+};
+IX_DEV Hit intersect_planes(const float4* __restrict__ planes, int n, V3 o, V3 d) {
+    float t_near = -1e30f, t_far = 1e30f;
+    int near_idx = -1, far_idx = -1;
+    bool outside = false;
+    for (int i = 0; i < n; ++i) {
+        float4 p = planes[i];
+        float denom = (p.x * d.x + p.y * d.y) + p.z * d.z;
+        float side = p.w + ((p.x * o.x + p.y * o.y) + p.z * o.z);
+        float t = (-side) / denom;
+        if (fabsf(denom) > 1e-7f) {
+            if (denom < 0.0f) {
+                if (t > t_near) {
+                    t_near = t;
+                    near_idx = i;
+                }
+            } else if (t < t_far) {
+                t_far = t;
+                far_idx = i;
+            }
+        } else if (side > 0.0f) {
+            outside = true;
+            break;
+        }
+    }
+    Hit h;
+    h.facet = -1;
+    h.t = 0.0f;
+    if (outside || t_near > t_far) return h;
+    if (t_near > 1e-4f) {
+        h.t = t_near;
+        h.facet = near_idx >= 0 ? near_idx : 0;
+    } else if (t_far > 1e-4f) {
+        h.t = t_far;
+        h.facet = far_idx >= 0 ? far_idx : 0;
+    }
+    return h;
+}
+
+}  // namespace ix

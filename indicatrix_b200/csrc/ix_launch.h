@@ -1,0 +1,70 @@
+// ix_launch.h -- internal interface between the C-ABI host code (ix_backend.cpp) and the
+// kernel translation unit, which is compiled twice (reference-exact rounding and fused
+// rounding).  Not part of the public ABI.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/ix_scene.h"
+
+namespace ix {
+
+// One frame-tracing launch over the pixels [pixel_begin, pixel_begin + n_pixels).
+struct TraceLaunch {
+    ix_scene scene;            // `planes` is a device pointer here
+    uint32_t absorbing;
+    uint32_t pixel_begin;
+    uint32_t n_pixels;
+    uint32_t sample_offset;
+    uint32_t spp;
+    uint32_t pixels_per_task;  // consecutive pixels one warp task covers
+    double* out;               // device, n_pixels * 3 per-pixel sums
+    int accumulate;            // 1: out += sums, 0: out = sums
+    uint32_t* task_counter;    // device, zeroed by the launcher
+    unsigned long long* dropped;  // device, non-finite samples dropped (may be null)
+    int blocks;                // persistent grid size
+    int threads;               // threads per block (multiple of 32)
+};
+
+// Per-function check kernels: evaluate one reference function per input row on the
+// device so the host can compare against the CPU oracle value by value.
+enum CheckFn {
+    CHECK_SAMPLE_DRAWS = 0,   // in: pixel, sample (u32)  out: seed (u32 bits), jx, jy, hero
+    CHECK_HERO_LAMBDAS = 1,   // in: hero_rand           out: 8 wavelengths
+    CHECK_DISPERSION = 2,     // in: lambda               out: n (scene material)
+    CHECK_CMF = 3,            // in: lambda               out: x, y, z
+    CHECK_D65 = 4,            // in: lambda               out: power
+    CHECK_EXP_LANE = 5,       // in: x                    out: exp
+    CHECK_TIR_DELTA = 6,      // in: n1, cos_i, sin_i     out: delta
+    CHECK_FRESNEL = 7,        // in: n1, n2, cos_i, I,Q,U,V  out: reflected I,Q,U,V, rs, rp
+    CHECK_ENV = 8,            // in: dir xyz, lambda, observer xyz  out: radiance
+    CHECK_INTERSECT = 9,      // in: origin xyz, dir xyz  out: t, facet (as float)
+    CHECK_TRACE = 10,         // in: pixel, sample (u32)  out: x, y, z, bounces
+    CHECK_CAMERA_RAY = 11,    // in: pixel, sample (u32)  out: origin xyz, dir xyz
+    CHECK_ABSORPTION = 12,    // in: lambda               out: alpha (abs_o)
+    CHECK_TRACE_RAY = 13,     // in: origin xyz, dir xyz, seed (u32), hero  out: x, y, z, bounces
+};
+
+struct CheckLaunch {
+    ix_scene scene;    // device planes
+    uint32_t absorbing;
+    int fn;
+    uint32_t n;
+    uint32_t in_stride;   // 32-bit words per input row
+    uint32_t out_stride;  // 32-bit words per output row
+    const uint32_t* in;   // device
+    uint32_t* out;        // device
+};
+
+cudaError_t launch_trace_exact(const TraceLaunch& l, cudaStream_t stream);
+cudaError_t launch_trace_fast(const TraceLaunch& l, cudaStream_t stream);
+cudaError_t launch_check_exact(const CheckLaunch& l, cudaStream_t stream);
+cudaError_t launch_check_fast(const CheckLaunch& l, cudaStream_t stream);
+// Occupancy-derived resident blocks per SM for the trace kernel at `threads` per block.
+int trace_blocks_per_sm_exact(int threads, size_t* smem_bytes);
+int trace_blocks_per_sm_fast(int threads, size_t* smem_bytes);
+// FP32 FMA-pipe throughput probe (ix_probe.cu): best FLOP/s of `reps` timed runs.
+cudaError_t fp32_probe(int sm_count, int reps, cudaStream_t stream, double* flops);
+
+}  // namespace ix

@@ -1,0 +1,114 @@
+"""The benchmark workloads as concrete, seeded synthetic scenes.
+
+* ``round_brilliant_frame``: a 121-plane round brilliant (table 57 %, crown 34.5 deg,
+  pavilion 40.75 deg, 8 + 8 + 16 crown, 8 + 16 pavilion, 64-segment girdle 2 % thick,
+  girdle diameter 1.0) in Diamond (Peter 1923 Sellmeier), face up under a D65 uniform
+  hemisphere with a 20-degree head shadow, 42-degree pinhole camera, max depth 32.
+* ``random_stones``: seeded random convex round stones, 33-121 facets, crown 25-45 deg,
+  pavilion 37-45 deg, table 45-70 %, Cauchy or Sellmeier materials with n_D in
+  [1.45, 2.60] and dispersion in [0.01, 0.07], half of them with a smooth 16-knot
+  absorption spline of 0-5 /cm, each at 9 tilts 0-40 deg.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import List
+
+import numpy as np
+
+from . import abi, geometry, materials
+from .backend import FrameScene, camera_new, environment_preset, PRESET_ISO_HEMISPHERE
+
+FACE_UP_PITCH = np.float32(math.pi / 2.0)
+DEFAULT_FOV_DEG = 42.0
+FACE_UP_DISTANCE = 1.6
+# Model units per centimetre of a 1.0-diameter stone: a 6.5 mm girdle.
+CM_PER_MODEL_UNIT = 0.65
+
+
+def iso_hemisphere(head_shadow_deg: float = 20.0) -> abi.Environment:
+    return environment_preset(PRESET_ISO_HEMISPHERE, 1.0, 0.0, 0.0, 0.0, 1.0, head_shadow_deg)
+
+
+def round_brilliant_frame(width: int = 256, height: int = 256, max_bounces: int = 32) -> FrameScene:
+    planes = geometry.to_f32(geometry.round_brilliant())
+    cam = camera_new(0.0, float(FACE_UP_PITCH), FACE_UP_DISTANCE, DEFAULT_FOV_DEG)
+    return FrameScene(camera=cam, width=width, height=height, planes=planes,
+                      material=materials.diamond(), max_bounces=max_bounces,
+                      environment=iso_hemisphere())
+
+
+@dataclass
+class StoneSpec:
+    planes: np.ndarray
+    material: abi.Material
+    spp: int
+    info: dict
+
+
+def random_material(rng: np.random.Generator, absorbing: bool) -> abi.Material:
+    """Cauchy or Sellmeier-1 with n_D ~ U(1.45, 2.60) and an Abbe-like dispersion
+    n_F - n_C ~ U(0.01, 0.07); optional smooth absorption spline in 1/cm."""
+    n_d = float(rng.uniform(1.45, 2.60))
+    disp = float(rng.uniform(0.01, 0.07))
+    lf, lc, ld = 0.4861, 0.6563, 0.5893  # um
+    if rng.uniform() < 0.5:
+        # Cauchy n = A + B / l^2 : n_F - n_C = B (1/lf^2 - 1/lc^2).
+        b = disp / (1.0 / lf ** 2 - 1.0 / lc ** 2)
+        a = n_d - b / ld ** 2
+        d = materials.cauchy(a, b, 0.0)
+    else:
+        # Sellmeier-1 n^2 = 1 + B l^2 / (l^2 - C): solve C from the dispersion, then B.
+        def n_of(B, C, l):
+            return math.sqrt(1.0 + B * l * l / (l * l - C))
+
+        def fit(C):
+            B = (n_d ** 2 - 1.0) * (ld ** 2 - C) / ld ** 2
+            return n_of(B, C, lf) - n_of(B, C, lc) - disp, B
+
+        lo, hi = 1e-5, 0.12
+        for _ in range(80):
+            mid = 0.5 * (lo + hi)
+            if fit(mid)[0] > 0:
+                hi = mid
+            else:
+                lo = mid
+        C = 0.5 * (lo + hi)
+        B = fit(C)[1]
+        d = abi.Dispersion()
+        d.kind = abi.DISP_SELLMEIER1
+        d.b[:] = [B, 0.0, 0.0]
+        d.c[:] = [C, 0.0, 0.0]
+    spline = None
+    if absorbing:
+        knots = rng.uniform(0.0, 1.0, abi.SPLINE_KNOTS)
+        # smooth: average neighbours, scale to a random peak in [0, 5] /cm
+        knots = np.convolve(np.pad(knots, 2, mode="edge"), np.ones(5) / 5.0, mode="valid")
+        knots = knots / max(knots.max(), 1e-6) * rng.uniform(0.0, 5.0)
+        spline = knots.astype(np.float32)
+    return materials.isotropic(d, spline, path_scale=CM_PER_MODEL_UNIT)
+
+
+def random_stones(n: int, seed: int = 20251203) -> List[StoneSpec]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        planes, info = geometry.random_stone(rng)
+        mat = random_material(rng, absorbing=(i % 2 == 1))
+        spp = int(rng.choice([32, 64, 128, 256]))
+        out.append(StoneSpec(geometry.to_f32(planes), mat, spp, info))
+    return out
+
+
+TILTS_DEG = [0.0, 5.0, 10.0, 15.0, 20.0, 25.0, 30.0, 35.0, 40.0]
+
+
+def tilted_scene(stone: StoneSpec, tilt_deg: float, width: int = 128, height: int = 128,
+                 max_bounces: int = 32) -> FrameScene:
+    """The stone seen face-up with the camera tilted `tilt_deg` from the table normal."""
+    pitch = float(np.float32(math.pi / 2.0 - math.radians(tilt_deg)))
+    cam = camera_new(0.0, pitch, FACE_UP_DISTANCE, DEFAULT_FOV_DEG)
+    return FrameScene(camera=cam, width=width, height=height, planes=stone.planes,
+                      material=stone.material, max_bounces=max_bounces,
+                      environment=iso_hemisphere())
