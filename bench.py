@@ -2,10 +2,10 @@
 
 One "step" is one pass of the hot path over one batch of synthetic input:
 
-* ``--workload frame`` (default): the 256x256, 64 spp round-brilliant frame
-  (4,194,304 paths; Diamond, D65 hemisphere with a 20-degree head shadow, depth 32);
-* ``--workload batch``: 64 seeded random stones x 9 tilts at 128x128 with spp drawn from
-  {32, 64, 128, 256} -- one persistent launch per step.
+* ``--workload batch`` (default): 64 seeded random stones x 9 tilts at 128x128 with spp
+  drawn from {32, 64, 128, 256} -- one persistent launch per step (about 1.1e9 paths);
+* ``--workload frame``: the 256x256, 64 spp round-brilliant frame (4,194,304 paths;
+  Diamond, D65 hemisphere with a 20-degree head shadow, depth 32).
 
 Under torchrun (N > 1) every rank traces its own disjoint absolute sample range of the
 same workload (weak scaling), and the per-pixel f64 sums are gathered to rank 0 over
@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="frame", choices=["frame", "batch"])
+    ap.add_argument("--workload", default="batch", choices=["frame", "batch"])
     ap.add_argument("--precision", default="fast", choices=["fast", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -180,7 +180,7 @@ def count_flops(items):
     for fs, spp in items[::step]:
         sc = fs.to_abi()
         n_pix = fs.width * fs.height
-        stride = max(1, n_pix // 512)
+        stride = max(1, n_pix // (8192 // max(1, spp // 16)))
         c = ix_oracle.count_flops(sc, 0, n_pix, stride, 0, spp)
         total_f += c.flops()
         total_p += c.paths
@@ -259,27 +259,42 @@ def main():
         raise RuntimeError("libix_cuda.so could not create a backend")
 
     # Device-resident inputs and outputs.
-    dev_items = []
-    for fs, spp in items:
-        sc = fs.to_abi()
-        planes = torch.from_numpy(np.ascontiguousarray(fs.planes, np.float32)).to(dev)
-        sc.planes = C.cast(C.c_void_p(planes.data_ptr()), C.POINTER(C.c_float))
-        out = torch.zeros(fs.width * fs.height * 3, dtype=torch.float64, device=dev)
-        dev_items.append((sc, planes, out, spp, fs))
     total_paths = sum(fs.width * fs.height * spp for fs, spp in items)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    # A dedicated (non-default) stream: the library enqueues on exactly this stream and
+    # the step events are recorded on it.
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     sample_base = rank * 1_000_000  # disjoint absolute sample ranges per rank
+    dev_items = []
+    plan = None
+    if args.workload == "batch":
+        from indicatrix_b200.backend import BatchPlan
+
+        plan = BatchPlan(backend, [(fs, sample_base, spp) for fs, spp in items])
+        cfg["autotuned_variant"] = plan.autotune(reps=1)
+        n_out = sum(fs.width * fs.height * 3 for fs, _ in items)
+        result = torch.empty(0)
+    else:
+        for fs, spp in items:
+            sc = fs.to_abi()
+            planes = torch.from_numpy(np.ascontiguousarray(fs.planes, np.float32)).to(dev)
+            sc.planes = C.cast(C.c_void_p(planes.data_ptr()), C.POINTER(C.c_float))
+            out = torch.zeros(fs.width * fs.height * 3, dtype=torch.float64, device=dev)
+            dev_items.append((sc, planes, out, spp, fs))
+        result = dev_items[0][2]
 
     def step(k):
+        if plan is not None:
+            plan.run(stream.cuda_stream)
         for sc, _planes, out, spp, _fs in dev_items:
             rc = backend.accumulate_device(sc, sample_base + 0, spp, out.data_ptr(), False,
                                            stream.cuda_stream)
             if rc != 0:
                 raise RuntimeError(f"device trace declined: {backend.last_lost_reason()}")
-        if world > 1:
-            gathered = [torch.empty_like(dev_items[0][2]) for _ in range(world)]
-            torch.distributed.all_gather(gathered, dev_items[0][2])
+        if world > 1 and plan is None:
+            gathered = [torch.empty_like(result) for _ in range(world)]
+            torch.distributed.all_gather(gathered, result)
             # fold in ascending first-sample order (rank order == first-sample order)
             acc = gathered[0].clone()
             for g in gathered[1:]:
@@ -311,20 +326,31 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         mean_ms = float(t.item())
     value = world * total_paths / (mean_ms * 1e-3)
-    launches_per_step = 0
-    for fs, spp in items:
-        n = fs.width * fs.height * spp
-        launches_per_step += 1 + (1 if n > (1 << 20) else 0)
+    if plan is not None:
+        launches_per_step = 1
+    else:
+        launches_per_step = 0
+        for fs, spp in items:
+            n = fs.width * fs.height * spp
+            launches_per_step += 1 + (1 if n > (1 << 20) else 0)
 
-    # End-to-end through the public API with host buffers (H2D planes, D2H sums).
+    # End-to-end through the public API with host buffers (H2D scenes and planes, D2H
+    # per-pixel sums): try_accumulate for the frame, try_accumulate_batch for the batch.
+    from indicatrix_b200.backend import GpuBatchItem
+
     e2e_ms = []
     accs = [np.zeros((fs.height, fs.width, 3), np.float64) for fs, _ in items]
     for k in range(max(1, args.warmup // 2) + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for (fs, spp), acc in zip(items, accs):
-            if not backend.try_accumulate(fs, sample_base, spp, acc):
-                raise RuntimeError(f"e2e trace declined: {backend.last_lost_reason()}")
+        if plan is not None:
+            batch = [GpuBatchItem(fs, sample_base, spp, acc) for (fs, spp), acc in zip(items, accs)]
+            if backend.try_accumulate_batch_cancellable(batch) != 0:
+                raise RuntimeError(f"e2e batch declined: {backend.last_lost_reason()}")
+        else:
+            for (fs, spp), acc in zip(items, accs):
+                if not backend.try_accumulate(fs, sample_base, spp, acc):
+                    raise RuntimeError(f"e2e trace declined: {backend.last_lost_reason()}")
         t1 = time.perf_counter()
         if k >= max(1, args.warmup // 2):
             e2e_ms.append((t1 - t0) * 1e3)

@@ -47,6 +47,8 @@ typedef struct ix_backend_options {
     uint32_t precision;          /* IX_PRECISION_*                                       */
     uint32_t threads_per_block;  /* 0 = autotuned                                        */
     uint64_t chunk_paths;        /* paths per launch; 0 = default (TDR-safe first chunk)  */
+    uint32_t kernel_variant;     /* register budget of the megakernel: 0 unconstrained,    */
+                                 /* 1 six CTAs per SM, 2 eight CTAs per SM                 */
 } ix_backend_options;
 
 /* GpuWorkLimits (gpu_backend/limits.rs:6-27): a request above a limit is declined. */
@@ -102,6 +104,34 @@ int ix_accumulate_f64(ix_backend* b, const ix_scene* scene, uint32_t sample_offs
  * each item's status written to item->status; returns IX_DONE when all items are done. */
 int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items,
                         const volatile int32_t* cancel);
+/* Batched plans (the reference's batch path, backend.rs:451, as ONE persistent launch
+ * over many stones and tilts, replayed from a CUDA graph).  A job is a whole frame of
+ * scene `scene` over samples [sample_offset, sample_offset + spp).  Scenes, planes and
+ * the job table are uploaded once by ix_batch_plan_create; each ix_batch_plan_run
+ * overwrites the plan's device sums (job-major, each job width * height * 3 f64, job j
+ * starting at ix_batch_plan_job_offset(j)).  Returns NULL when a scene does not route
+ * to the GPU or the device fails. */
+typedef struct ix_batch_job {
+    uint32_t scene;
+    uint32_t sample_offset;
+    uint32_t spp;
+} ix_batch_job;
+typedef struct ix_batch_plan ix_batch_plan;
+ix_batch_plan* ix_batch_plan_create(ix_backend* b, const ix_scene* scenes, uint32_t n_scenes,
+                                    const ix_batch_job* jobs, uint32_t n_jobs);
+/* One persistent launch of every job on `stream` (NULL: the backend's stream); not
+ * synchronised.  IX_DONE or IX_DECLINED. */
+int ix_batch_plan_run(ix_batch_plan* p, void* stream);
+/* Times each megakernel register variant `reps` times and keeps the fastest. */
+int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen);
+/* Copies the plan's sums to host memory (ix_batch_plan_output_size doubles). */
+int ix_batch_plan_download(ix_batch_plan* p, double* host_out);
+uint64_t ix_batch_plan_output_size(const ix_batch_plan* p);
+const double* ix_batch_plan_device_output(const ix_batch_plan* p);
+uint64_t ix_batch_plan_paths(const ix_batch_plan* p);
+uint32_t ix_batch_plan_variant(const ix_batch_plan* p);
+uint64_t ix_batch_plan_job_offset(const ix_batch_plan* p, uint32_t job);
+void ix_batch_plan_destroy(ix_batch_plan* p);
 /* Device-resident form for callers that keep the scene and the sums in GPU memory:
  * `scene->planes` and `d_accum_xyz` are device pointers; the launch is enqueued on
  * `stream` (a cudaStream_t, or NULL for the backend's own stream) and not synchronised.

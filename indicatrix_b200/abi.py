@@ -121,6 +121,7 @@ class BackendOptions(C.Structure):
         ("precision", C.c_uint32),
         ("threads_per_block", C.c_uint32),
         ("chunk_paths", C.c_uint64),
+        ("kernel_variant", C.c_uint32),
     ]
 
 
@@ -141,6 +142,16 @@ class BatchItem(C.Structure):
         ("spp", C.c_uint32),
         ("accum_xyz", C.POINTER(C.c_double)),
         ("status", C.c_int32),
+    ]
+
+
+class BatchJob(C.Structure):
+    """One job of a batch plan: a whole frame of one scene over an absolute sample range."""
+
+    _fields_ = [
+        ("scene", C.c_uint32),
+        ("sample_offset", C.c_uint32),
+        ("spp", C.c_uint32),
     ]
 
 

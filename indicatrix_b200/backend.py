@@ -71,6 +71,23 @@ def load_library() -> C.CDLL:
         lib.ix_last_dropped.restype = C.c_uint64
         lib.ix_last_dropped.argtypes = [C.c_void_p]
         lib.ix_probe_fp32_peak.argtypes = [C.c_void_p, P(C.c_double)]
+        lib.ix_batch_plan_create.restype = C.c_void_p
+        lib.ix_batch_plan_create.argtypes = [C.c_void_p, P(abi.Scene), C.c_uint32, P(abi.BatchJob),
+                                             C.c_uint32]
+        lib.ix_batch_plan_run.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ix_batch_plan_autotune.argtypes = [C.c_void_p, C.c_int, P(C.c_uint32)]
+        lib.ix_batch_plan_download.argtypes = [C.c_void_p, P(C.c_double)]
+        lib.ix_batch_plan_output_size.restype = C.c_uint64
+        lib.ix_batch_plan_output_size.argtypes = [C.c_void_p]
+        lib.ix_batch_plan_device_output.restype = C.c_void_p
+        lib.ix_batch_plan_device_output.argtypes = [C.c_void_p]
+        lib.ix_batch_plan_paths.restype = C.c_uint64
+        lib.ix_batch_plan_paths.argtypes = [C.c_void_p]
+        lib.ix_batch_plan_variant.restype = C.c_uint32
+        lib.ix_batch_plan_variant.argtypes = [C.c_void_p]
+        lib.ix_batch_plan_job_offset.restype = C.c_uint64
+        lib.ix_batch_plan_job_offset.argtypes = [C.c_void_p, C.c_uint32]
+        lib.ix_batch_plan_destroy.argtypes = [C.c_void_p]
         lib.ix_camera_new.argtypes = [C.c_float] * 4 + [P(abi.Camera)]
         lib.ix_environment_preset.argtypes = [C.c_int32] + [C.c_float] * 6 + [P(abi.Environment)]
         lib.ix_environment_uniform.argtypes = [C.c_float, P(abi.Environment)]
@@ -220,9 +237,11 @@ class GpuBackend:
     @classmethod
     def acquire(cls, device: int = 0, precision: int = abi.PRECISION_FAST,
                 pipeline: GpuPipelineKind = GpuPipelineKind.MEGAKERNEL,
-                threads_per_block: int = 0, chunk_paths: int = 0) -> "GpuBackend":
+                threads_per_block: int = 0, chunk_paths: int = 0,
+                kernel_variant: int = 0) -> "GpuBackend":
         lib = load_library()
-        opts = abi.BackendOptions(device, int(pipeline), precision, threads_per_block, chunk_paths)
+        opts = abi.BackendOptions(device, int(pipeline), precision, threads_per_block, chunk_paths,
+                                  kernel_variant)
         h = lib.ix_backend_create(C.byref(opts))
         return cls(h if h else None)
 
@@ -381,3 +400,76 @@ class GpuBackend:
         if rc != 0:
             raise RuntimeError(f"check kernel failed: {self.last_lost_reason()}")
         return out
+
+
+class BatchPlan:
+    """Many scenes (stones x tilts) traced by one persistent launch, replayed from a CUDA
+    graph: ``run()`` enqueues every job; ``sums(j)`` is job j's per-pixel f64 sums
+    (``height x width x 3``) after ``download()``."""
+
+    def __init__(self, backend: GpuBackend, jobs: Sequence[tuple]):
+        """``jobs``: (FrameScene, sample_offset, spp) per job; identical scene objects are
+        uploaded once."""
+        if not backend.available:
+            raise RuntimeError("no CUDA backend")
+        self._b = backend
+        self._lib = backend._lib
+        uniq, index = [], {}
+        job_arr = (abi.BatchJob * len(jobs))()
+        for j, (fs, off, spp) in enumerate(jobs):
+            if id(fs) not in index:
+                index[id(fs)] = len(uniq)
+                uniq.append(fs)
+            job_arr[j] = abi.BatchJob(index[id(fs)], off, spp)
+        scenes = (abi.Scene * len(uniq))()
+        for i, fs in enumerate(uniq):
+            scenes[i] = fs.to_abi()
+        self.scenes = uniq
+        self.jobs = list(jobs)
+        self._h = self._lib.ix_batch_plan_create(backend._h, scenes, len(uniq), job_arr, len(jobs))
+        if not self._h:
+            raise RuntimeError(f"batch plan declined: {backend.last_lost_reason()}")
+        self.paths = int(self._lib.ix_batch_plan_paths(self._h))
+        self._host = None
+
+    def run(self, stream_ptr: Optional[int] = None) -> None:
+        rc = self._lib.ix_batch_plan_run(self._h, C.c_void_p(stream_ptr) if stream_ptr else None)
+        if rc != abi.IX_DONE:
+            raise RuntimeError(f"batch launch declined: {self._b.last_lost_reason()}")
+
+    def autotune(self, reps: int = 2) -> int:
+        v = C.c_uint32(0)
+        if self._lib.ix_batch_plan_autotune(self._h, reps, C.byref(v)) != 0:
+            raise RuntimeError(f"autotune failed: {self._b.last_lost_reason()}")
+        return int(v.value)
+
+    @property
+    def variant(self) -> int:
+        return int(self._lib.ix_batch_plan_variant(self._h))
+
+    def device_output(self) -> int:
+        return int(self._lib.ix_batch_plan_device_output(self._h))
+
+    def download(self) -> np.ndarray:
+        n = int(self._lib.ix_batch_plan_output_size(self._h))
+        host = np.zeros(n, np.float64)
+        if self._lib.ix_batch_plan_download(self._h, host.ctypes.data_as(C.POINTER(C.c_double))) != 0:
+            raise RuntimeError(f"download failed: {self._b.last_lost_reason()}")
+        self._host = host
+        return host
+
+    def sums(self, job: int) -> np.ndarray:
+        if self._host is None:
+            self.download()
+        fs = self.jobs[job][0]
+        off = int(self._lib.ix_batch_plan_job_offset(self._h, job))
+        n = fs.width * fs.height * 3
+        return self._host[off:off + n].reshape(fs.height, fs.width, 3)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ix_batch_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self) -> None:
+        self.close()

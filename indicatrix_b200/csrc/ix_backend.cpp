@@ -48,7 +48,8 @@ struct ix_backend {
     uint32_t* d_check = nullptr;
     size_t check_cap = 0;
     int sm_count = 0;
-    int bps_exact = 1, bps_fast = 1;
+    uint32_t variant = 0;
+    int bps_exact[3] = {1, 1, 1}, bps_fast[3] = {1, 1, 1};
     std::string label;
     // State.
     bool lost = false;
@@ -117,8 +118,9 @@ bool material_has_absorption(const ix_absorption& a) {
 }
 
 uint32_t pixels_per_task(uint32_t spp) {
+    // About 256 paths per warp task (64 per 8-lane group), at most 8 pixels.
     uint32_t ppt = spp ? 256u / spp : 1u;
-    return std::max(1u, std::min(4u, ppt));
+    return std::max(1u, std::min(8u, ppt));
 }
 
 // Enqueue the trace launches for pixels [0, n_pixels) of `sc` (device planes) into
@@ -140,7 +142,8 @@ int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uin
     L.task_counter = b->d_counter;
     L.dropped = b->d_dropped;
     L.threads = (int)b->threads;
-    L.blocks = b->sm_count * (exact ? b->bps_exact : b->bps_fast);
+    L.variant = (int)b->variant;
+    L.blocks = b->sm_count * (exact ? b->bps_exact[b->variant] : b->bps_fast[b->variant]);
     if (L.blocks <= 0) L.blocks = b->sm_count > 0 ? b->sm_count : 1;
     // Chunking: a TDR-safe first launch of at most 1M paths (gpu/frame/mod.rs:355-361),
     // then launches of `chunk_paths` (default 64M paths), whole pixels each.
@@ -335,8 +338,11 @@ ix_backend* ix_backend_create(const ix_backend_options* opts) {
     }
     b->sm_count = prop.multiProcessorCount;
     b->label = prop.name;
-    b->bps_exact = std::max(1, ix::trace_blocks_per_sm_exact((int)b->threads, nullptr));
-    b->bps_fast = std::max(1, ix::trace_blocks_per_sm_fast((int)b->threads, nullptr));
+    for (int v = 0; v < 3; ++v) {
+        b->bps_exact[v] = std::max(1, ix::trace_blocks_per_sm_exact((int)b->threads, v, nullptr));
+        b->bps_fast[v] = std::max(1, ix::trace_blocks_per_sm_fast((int)b->threads, v, nullptr));
+    }
+    if (opts && opts->kernel_variant < 3) b->variant = opts->kernel_variant;
     return b;
 }
 
@@ -400,20 +406,281 @@ int ix_accumulate_f64(ix_backend* b, const ix_scene* scene, uint32_t sample_offs
     return accumulate_impl<double>(b, scene, sample_offset, spp, accum_xyz, cancel);
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------
+// Batched plans: many scenes (stones x tilts) traced by one persistent launch.
+// ------------------------------------------------------------------------------------
+struct ix_batch_plan {
+    ix_backend* b = nullptr;
+    uint32_t n_scenes = 0, n_jobs = 0, total_tasks = 0;
+    uint64_t out_doubles = 0, paths = 0;
+    ix_scene* d_scenes = nullptr;
+    uint32_t* d_absorbing = nullptr;
+    ix::BatchJob* d_jobs = nullptr;
+    float* d_planes = nullptr;
+    double* d_out = nullptr;
+    uint32_t* d_counter = nullptr;
+    unsigned long long* d_dropped = nullptr;
+    std::vector<ix::BatchJob> jobs;
+    std::vector<uint64_t> job_out;  // first double of each job's sums
+    // CUDA graph of [counter reset, batch kernel], rebuilt when the stream or the variant
+    // changes.
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+    int graph_variant = -1;
+    uint32_t variant = 0;
+    bool tuned = false;
+};
+
+namespace {
+
+void plan_free_graph(ix_batch_plan* p) {
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    p->exec = nullptr;
+    p->graph = nullptr;
+    p->graph_variant = -1;
+}
+
+cudaError_t plan_enqueue(ix_batch_plan* p, cudaStream_t st, uint32_t variant) {
+    ix_backend* b = p->b;
+    const bool exact = b->precision == IX_PRECISION_EXACT;
+    ix::BatchLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.scenes = p->d_scenes;
+    L.absorbing = p->d_absorbing;
+    L.jobs = p->d_jobs;
+    L.n_jobs = p->n_jobs;
+    L.total_tasks = p->total_tasks;
+    L.out = p->d_out;
+    L.accumulate = 0;
+    L.task_counter = p->d_counter;
+    L.dropped = p->d_dropped;
+    L.threads = 128;
+    L.variant = (int)variant;
+    int bps = exact ? ix::batch_blocks_per_sm_exact(128, (int)variant)
+                    : ix::batch_blocks_per_sm_fast(128, (int)variant);
+    L.blocks = b->sm_count * std::max(1, bps);
+    return exact ? ix::launch_batch_exact(L, st) : ix::launch_batch_fast(L, st);
+}
+
+}  // namespace
+
+extern "C" {
+
+ix_batch_plan* ix_batch_plan_create(ix_backend* b, const ix_scene* scenes, uint32_t n_scenes,
+                                    const ix_batch_job* jobs, uint32_t n_jobs) {
+    if (!b || !scenes || !jobs || n_scenes == 0 || n_jobs == 0 || b->lost) return nullptr;
+    for (uint32_t i = 0; i < n_scenes; ++i)
+        if (!ix_scene_routes_to_gpu(&scenes[i])) return nullptr;
+    Turn turn(b);
+    if (fail(b, cudaSetDevice(b->device), "set device")) return nullptr;
+    ix_batch_plan* p = new ix_batch_plan();
+    p->b = b;
+    p->n_scenes = n_scenes;
+    p->n_jobs = n_jobs;
+    // Job table: tasks of ~256 paths, jobs laid out back to back.
+    uint64_t task = 0, out = 0;
+    p->jobs.resize(n_jobs);
+    p->job_out.resize(n_jobs);
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+        const ix_batch_job& in = jobs[j];
+        if (in.scene >= n_scenes || in.spp == 0) {
+            delete p;
+            return nullptr;
+        }
+        const ix_scene& sc = scenes[in.scene];
+        ix::BatchJob& bj = p->jobs[j];
+        bj.scene = in.scene;
+        bj.n_pixels = sc.width * sc.height;
+        bj.spp = in.spp;
+        bj.ppt = pixels_per_task(in.spp);
+        bj.task_begin = (uint32_t)task;
+        bj.sample_offset = in.sample_offset;
+        bj.out_offset = out;
+        p->job_out[j] = out;
+        task += (bj.n_pixels + bj.ppt - 1) / bj.ppt;
+        out += (uint64_t)bj.n_pixels * 3;
+        p->paths += (uint64_t)bj.n_pixels * in.spp;
+    }
+    if (task >= 0xFFFFFFFFull) {
+        delete p;
+        return nullptr;
+    }
+    p->total_tasks = (uint32_t)task;
+    p->out_doubles = out;
+    uint64_t plane_floats = 0;
+    for (uint32_t i = 0; i < n_scenes; ++i) plane_floats += (uint64_t)scenes[i].n_planes * 4;
+    std::vector<ix_scene> dev_scenes(scenes, scenes + n_scenes);
+    std::vector<uint32_t> absorbing(n_scenes);
+    std::vector<float> planes(std::max<uint64_t>(plane_floats, 4));
+    uint64_t off = 0;
+    bool ok = cudaMalloc((void**)&p->d_planes, planes.size() * sizeof(float)) == cudaSuccess;
+    for (uint32_t i = 0; ok && i < n_scenes; ++i) {
+        std::memcpy(planes.data() + off, scenes[i].planes, (size_t)scenes[i].n_planes * 16);
+        dev_scenes[i].planes = p->d_planes + off;
+        dev_scenes[i].facet_finishes = nullptr;
+        dev_scenes[i].n_finishes = 0;
+        absorbing[i] = material_has_absorption(scenes[i].material.abs_o) ? 1u : 0u;
+        off += (uint64_t)scenes[i].n_planes * 4;
+    }
+    ok = ok && cudaMalloc((void**)&p->d_scenes, n_scenes * sizeof(ix_scene)) == cudaSuccess &&
+         cudaMalloc((void**)&p->d_absorbing, n_scenes * sizeof(uint32_t)) == cudaSuccess &&
+         cudaMalloc((void**)&p->d_jobs, n_jobs * sizeof(ix::BatchJob)) == cudaSuccess &&
+         cudaMalloc((void**)&p->d_out, std::max<uint64_t>(out, 1) * sizeof(double)) == cudaSuccess &&
+         cudaMalloc((void**)&p->d_counter, sizeof(uint32_t)) == cudaSuccess &&
+         cudaMalloc((void**)&p->d_dropped, sizeof(unsigned long long)) == cudaSuccess;
+    ok = ok && cudaMemcpy(p->d_planes, planes.data(), planes.size() * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(p->d_scenes, dev_scenes.data(), n_scenes * sizeof(ix_scene), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(p->d_absorbing, absorbing.data(), n_scenes * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(p->d_jobs, p->jobs.data(), n_jobs * sizeof(ix::BatchJob), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemset(p->d_dropped, 0, sizeof(unsigned long long)) == cudaSuccess;
+    p->variant = b->variant;
+    if (!ok) {
+        fail(b, cudaGetLastError(), "batch plan");
+        ix_batch_plan_destroy(p);
+        return nullptr;
+    }
+    return p;
+}
+
+int ix_batch_plan_run(ix_batch_plan* p, void* stream) {
+    if (!p || p->b->lost) return IX_DECLINED;
+    ix_backend* b = p->b;
+    Turn turn(b);
+    cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+    if (fail(b, cudaSetDevice(b->device), "set device")) return IX_DECLINED;
+    if (!p->exec || p->graph_stream != st || p->graph_variant != (int)p->variant) {
+        plan_free_graph(p);
+        if (fail(b, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture")) return IX_DECLINED;
+        cudaError_t e = plan_enqueue(p, st, p->variant);
+        cudaError_t e2 = cudaStreamEndCapture(st, &p->graph);
+        if (fail(b, e, "batch launch") || fail(b, e2, "graph capture")) return IX_DECLINED;
+        if (fail(b, cudaGraphInstantiate(&p->exec, p->graph, 0), "graph instantiate")) return IX_DECLINED;
+        p->graph_stream = st;
+        p->graph_variant = (int)p->variant;
+    }
+    if (fail(b, cudaEventRecord(b->ev0, st), "event")) return IX_DECLINED;
+    if (fail(b, cudaGraphLaunch(p->exec, st), "graph launch")) return IX_DECLINED;
+    if (fail(b, cudaEventRecord(b->ev1, st), "event")) return IX_DECLINED;
+    b->timing.paths = p->paths;
+    b->timing.launches = 1;
+    return IX_DONE;
+}
+
+int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen) {
+    if (!p || p->b->lost) return -1;
+    ix_backend* b = p->b;
+    float best = 1e30f;
+    uint32_t best_v = p->variant;
+    for (uint32_t v = 0; v < 3; ++v) {
+        p->variant = v;
+        float total = 0.0f;
+        for (int r = 0; r < std::max(1, reps) + 1; ++r) {
+            if (ix_batch_plan_run(p, nullptr) != IX_DONE) return -1;
+            if (fail(b, cudaStreamSynchronize(b->stream), "autotune")) return -1;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+            if (r > 0) total += ms;  // first run of a variant builds its graph
+        }
+        if (total < best) {
+            best = total;
+            best_v = v;
+        }
+    }
+    p->variant = best_v;
+    p->tuned = true;
+    if (chosen) *chosen = best_v;
+    return 0;
+}
+
+int ix_batch_plan_download(ix_batch_plan* p, double* host_out) {
+    if (!p || !host_out || p->b->lost) return -1;
+    ix_backend* b = p->b;
+    Turn turn(b);
+    if (fail(b, cudaMemcpyAsync(host_out, p->d_out, p->out_doubles * sizeof(double), cudaMemcpyDeviceToHost,
+                                b->stream), "batch download"))
+        return -1;
+    if (fail(b, cudaStreamSynchronize(b->stream), "batch download")) return -1;
+    return 0;
+}
+
+uint64_t ix_batch_plan_output_size(const ix_batch_plan* p) { return p ? p->out_doubles : 0; }
+const double* ix_batch_plan_device_output(const ix_batch_plan* p) { return p ? p->d_out : nullptr; }
+uint64_t ix_batch_plan_paths(const ix_batch_plan* p) { return p ? p->paths : 0; }
+uint32_t ix_batch_plan_variant(const ix_batch_plan* p) { return p ? p->variant : 0; }
+
+uint64_t ix_batch_plan_job_offset(const ix_batch_plan* p, uint32_t job) {
+    return (p && job < p->n_jobs) ? p->job_out[job] : 0;
+}
+
+void ix_batch_plan_destroy(ix_batch_plan* p) {
+    if (!p) return;
+    cudaSetDevice(p->b->device);
+    cudaStreamSynchronize(p->b->stream);
+    plan_free_graph(p);
+    cudaFree(p->d_scenes);
+    cudaFree(p->d_absorbing);
+    cudaFree(p->d_jobs);
+    cudaFree(p->d_planes);
+    cudaFree(p->d_out);
+    cudaFree(p->d_counter);
+    cudaFree(p->d_dropped);
+    (void)cudaGetLastError();
+    delete p;
+}
+
 int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items,
                         const volatile int32_t* cancel) {
     if (!b || (!items && n_items)) return IX_DECLINED;
-    int overall = IX_DONE;
-    for (uint32_t i = 0; i < n_items; ++i) {
-        if (cancel && *cancel) {
-            for (uint32_t j = i; j < n_items; ++j) items[j].status = IX_CANCELLED;
-            return IX_CANCELLED;
-        }
-        int st = accumulate_impl<double>(b, items[i].scene, items[i].sample_offset, items[i].spp,
-                                         items[i].accum_xyz, cancel);
-        items[i].status = st;
-        if (st != IX_DONE && overall == IX_DONE) overall = st;
+    if (n_items == 0) return IX_DONE;
+    if (cancel && *cancel) {
+        for (uint32_t j = 0; j < n_items; ++j) items[j].status = IX_CANCELLED;
+        return IX_CANCELLED;
     }
+    // Items the CUDA path cannot trace are declined individually; the rest run in one
+    // persistent launch.
+    std::vector<ix_scene> scenes;
+    std::vector<ix_batch_job> jobs;
+    std::vector<uint32_t> which;
+    for (uint32_t i = 0; i < n_items; ++i) {
+        items[i].status = IX_DECLINED;
+        if (!items[i].scene || !items[i].accum_xyz || !ix_scene_routes_to_gpu(items[i].scene)) continue;
+        if (items[i].spp == 0 || items[i].scene->width * items[i].scene->height == 0) {
+            items[i].status = IX_DONE;
+            continue;
+        }
+        jobs.push_back(ix_batch_job{(uint32_t)scenes.size(), items[i].sample_offset, items[i].spp});
+        scenes.push_back(*items[i].scene);
+        which.push_back(i);
+    }
+    if (!jobs.empty()) {
+        ix_batch_plan* p = ix_batch_plan_create(b, scenes.data(), (uint32_t)scenes.size(), jobs.data(),
+                                                (uint32_t)jobs.size());
+        if (!p) return IX_DECLINED;
+        std::vector<double> host(p->out_doubles);
+        bool ok = ix_batch_plan_run(p, nullptr) == IX_DONE && ix_batch_plan_download(p, host.data()) == 0;
+        if (ok && !(cancel && *cancel)) {
+            for (size_t k = 0; k < which.size(); ++k) {
+                ix_batch_item& it = items[which[k]];
+                const double* src = host.data() + p->job_out[k];
+                const size_t n = (size_t)it.scene->width * it.scene->height * 3;
+                for (size_t e = 0; e < n; ++e) it.accum_xyz[e] += src[e];
+                it.status = IX_DONE;
+            }
+        } else if (ok) {
+            for (uint32_t k : which) items[k].status = IX_CANCELLED;
+        }
+        ix_batch_plan_destroy(p);
+    }
+    int overall = IX_DONE;
+    for (uint32_t i = 0; i < n_items; ++i)
+        if (items[i].status != IX_DONE) {
+            overall = items[i].status;
+            break;
+        }
     return overall;
 }
 

@@ -451,24 +451,38 @@ struct Hit {
     float t;
     int facet;  // -1: no hit
 };
+//
+// The reference divides t = -side / denom for every plane.  Here the IEEE quotient is
+// formed only for candidate planes, with no change to any result: for an entering
+// plane (denom < 0) the update `RN(q) > t_near` (q = -side / denom exactly) needs
+// q > t_near, i.e. t_near * denom + side > 0; for an exiting plane (denom > 0)
+// `RN(q) < t_far` needs t_far * denom + side > 0.  One fused multiply-add rounds that
+// expression once, which keeps its sign (a positive value can only round to +0, so the
+// test is `>= 0`), so every plane the reference would select passes the filter, and the
+// exact division and comparison then decide exactly as the reference does.
 IX_DEV Hit intersect_planes(const float4* __restrict__ planes, int n, V3 o, V3 d) {
     float t_near = -1e30f, t_far = 1e30f;
     int near_idx = -1, far_idx = -1;
     bool outside = false;
+#pragma unroll 4
     for (int i = 0; i < n; ++i) {
         float4 p = planes[i];
         float denom = (p.x * d.x + p.y * d.y) + p.z * d.z;
         float side = p.w + ((p.x * o.x + p.y * o.y) + p.z * o.z);
-        float t = (-side) / denom;
         if (fabsf(denom) > 1e-7f) {
-            if (denom < 0.0f) {
-                if (t > t_near) {
-                    t_near = t;
-                    near_idx = i;
+            const bool entering = denom < 0.0f;
+            const float bound = entering ? t_near : t_far;
+            if (fmaf(bound, denom, side) >= 0.0f) {
+                float t = __fdiv_rn(-side, denom);
+                if (entering) {
+                    if (t > t_near) {
+                        t_near = t;
+                        near_idx = i;
+                    }
+                } else if (t < t_far) {
+                    t_far = t;
+                    far_idx = i;
                 }
-            } else if (t < t_far) {
-                t_far = t;
-                far_idx = i;
             }
         } else if (side > 0.0f) {
             outside = true;

@@ -1,23 +1,25 @@
-// ix_kernels.cu -- the frame-tracing megakernel and the per-function check kernels.
+// ix_kernels.cu -- the frame-tracing megakernels and the per-function check kernels.
 //
 // Compiled twice by the build (IX_EXACT=1 with -fmad=false, IX_EXACT=0 with
 // contraction); every symbol is suffixed accordingly.
 //
-// Megakernel layout (GPU-first, not a translation of the reference's one-thread-per-tuple
-// WGSL kernel):
-//   * persistent CTAs; each CTA stages the stone's half-space planes (<= 128 x 16 B) in
-//     shared memory once, and every slab scan reads them as warp-wide broadcasts;
-//   * work is claimed a warp at a time from a global counter: one task is a run of
-//     `pixels_per_task` consecutive pixels x all their samples, flattened pixel-major;
-//     lane l takes flattened indices l, l+32, ... so a warp's 32 paths start in the same
-//     pixel neighbourhood;
-//   * a lane whose path finishes regenerates with its next sample while the other lanes
-//     keep bouncing, so the bounce body (nearly all the arithmetic) stays converged
-//     across lanes that are on different paths;
-//   * per-pixel sums are accumulated in f64: each lane sums its own samples of a pixel
-//     in ascending sample order into a shared-memory slot, then the warp folds the 32
-//     slots in a fixed tree order.  The result depends only on (pixel, samples), never
-//     on scheduling, so every run and every chunking of a frame gives the same bits.
+// Megakernel layout (GPU-first; the reference's WGSL kernel runs one thread per
+// (pixel, sample) tuple):
+//   * a path is traced by an 8-lane group, one lane per hero-wavelength channel
+//     (ix_transport.cuh); a warp holds 4 independent paths;
+//   * persistent CTAs claim work a warp at a time from a global counter: one task is a
+//     run of consecutive pixels x all their samples, flattened pixel-major; group gi of
+//     the warp takes flattened paths gi, gi + 4, ...; a group whose path finishes starts
+//     its next path while the other groups keep bouncing;
+//   * the stone's half-space planes (<= 128 x 16 B) sit in shared memory and every slab
+//     scan reads them as broadcasts;
+//   * per-pixel sums are accumulated in f64, each group over its own samples of a pixel
+//     in ascending order, then the 4 group partials are folded in a fixed order.  The
+//     sums depend only on (pixel, samples), never on scheduling: every run and every
+//     chunking of a frame gives the same bits.
+// The batch kernel runs the same task loop over many scenes (stones x tilts) in one
+// launch; each warp keeps the planes of the scene it is working on in its own
+// shared-memory slot.
 #include "ix_launch.h"
 #include "ix_transport.cuh"
 
@@ -29,25 +31,105 @@
 
 namespace ix {
 
-constexpr int TRACE_MAX_PPT = 4;  // pixels per warp task held in the partial-sum table
+constexpr int TRACE_MAX_PPT = 8;     // pixels per warp task held in the partial-sum table
+constexpr int GROUPS_PER_WARP = 4;   // paths in flight per warp (8 lanes each)
+constexpr int WARPS_PER_CTA = 4;     // 128 threads
 
-__global__ void __launch_bounds__(128) IX_SFX(trace_kernel)(const __grid_constant__ TraceLaunch L) {
+typedef double PartSlot[TRACE_MAX_PPT][GROUPS_PER_WARP][3];
+
+// One warp task: pixels [pixel0, pixel0 + npix) x samples [sample_offset, +spp), written
+// to out[0 .. 3 npix).  Returns the number of non-finite samples this lane dropped.
+IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const float4* __restrict__ planes,
+                                     uint32_t pixel0, uint32_t npix, uint32_t spp,
+                                     uint32_t sample_offset, PartSlot& part, double* out, int accumulate) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gi = lane >> 3;
+    const uint32_t total = npix * spp;
+    const uint32_t max_bounces = S.s.max_bounces;
+    unsigned long long drops = 0;
+    if (g.c == 0)
+        for (uint32_t j = 0; j < npix; ++j) {
+            part[j][gi][0] = 0.0;
+            part[j][gi][1] = 0.0;
+            part[j][gi][2] = 0.0;
+        }
+    uint32_t q = gi;
+    bool active = q < total;
+    uint32_t cur_j = active ? q / spp : 0;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    LanePath P;
+    if (active) group_init(g, P, S, pixel0 + cur_j, sample_offset + (q - cur_j * spp));
+    while (__any_sync(0xFFFFFFFFu, active)) {
+        if (!active) continue;
+        float esc = 0.0f;
+        const int r = (P.bounce >= max_bounces) ? (int)BOUNCE_KILLED : group_bounce(g, P, S, planes, esc);
+        if (r == BOUNCE_CONTINUE && P.bounce < max_bounces) continue;
+        // The path finished (escaped, roulette, or reached the bounce cap).
+        const V3 xyz = group_finish(g, P, S, r == BOUNCE_ESCAPED, esc);
+        if (isfinite(xyz.x) && isfinite(xyz.y) && isfinite(xyz.z)) {
+            ax += (double)xyz.x;
+            ay += (double)xyz.y;
+            az += (double)xyz.z;
+        } else if (g.c == 0) {
+            ++drops;
+        }
+        q += GROUPS_PER_WARP;
+        const uint32_t j = (q < total) ? q / spp : 0xFFFFFFFFu;
+        if (j != cur_j) {
+            if (g.c == 0) {
+                part[cur_j][gi][0] = ax;
+                part[cur_j][gi][1] = ay;
+                part[cur_j][gi][2] = az;
+            }
+            ax = ay = az = 0.0;
+            cur_j = j;
+        }
+        if (q < total)
+            group_init(g, P, S, pixel0 + cur_j, sample_offset + (q - cur_j * spp));
+        else
+            active = false;
+    }
+    __syncwarp();
+    // Fold each pixel's 4 group partials in a fixed order.
+    if (lane < npix) {
+        const uint32_t j = lane;
+        double x = part[j][0][0], y = part[j][0][1], z = part[j][0][2];
+#pragma unroll
+        for (int k = 1; k < GROUPS_PER_WARP; ++k) {
+            x += part[j][k][0];
+            y += part[j][k][1];
+            z += part[j][k][2];
+        }
+        double* o = out + (size_t)j * 3;
+        if (accumulate) {
+            o[0] += x;
+            o[1] += y;
+            o[2] += z;
+        } else {
+            o[0] = x;
+            o[1] = y;
+            o[2] = z;
+        }
+    }
+    __syncwarp();
+    return drops;
+}
+
+// Single scene: MINB is the resident CTAs per SM the register allocation must allow
+// (1 = unconstrained).
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_constant__ TraceLaunch L) {
     __shared__ float4 s_planes[IX_MAX_PLANES];
-    extern __shared__ double s_part[];  // [warps][TRACE_MAX_PPT][32][3]
+    __shared__ PartSlot s_part[WARPS_PER_CTA];
     const float4* gplanes = reinterpret_cast<const float4*>(L.scene.planes);
     for (uint32_t i = threadIdx.x; i < L.scene.n_planes; i += blockDim.x) s_planes[i] = gplanes[i];
     __syncthreads();
-
     const DevScene S{L.scene, L.absorbing};
+    const Group g = make_group();
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warp = threadIdx.x >> 5;
-    double* part = s_part + (size_t)warp * TRACE_MAX_PPT * 32 * 3;
     const uint32_t ppt = L.pixels_per_task;
-    const uint32_t spp = L.spp;
     const uint32_t n_tasks = (L.n_pixels + ppt - 1) / ppt;
-    const uint32_t max_bounces = L.scene.max_bounces;
     unsigned long long drops = 0;
-
     for (;;) {
         uint32_t task = 0;
         if (lane == 0) task = atomicAdd(L.task_counter, 1u);
@@ -55,74 +137,84 @@ __global__ void __launch_bounds__(128) IX_SFX(trace_kernel)(const __grid_constan
         if (task >= n_tasks) break;
         const uint32_t local0 = task * ppt;
         const uint32_t npix = min(ppt, L.n_pixels - local0);
-        const uint32_t total = npix * spp;
-        for (uint32_t j = 0; j < npix; ++j) {
-            double* slot = part + ((size_t)j * 32 + lane) * 3;
-            slot[0] = 0.0;
-            slot[1] = 0.0;
-            slot[2] = 0.0;
-        }
-        uint32_t q = lane;
-        bool active = q < total;
-        uint32_t cur_j = active ? q / spp : 0;
-        double ax = 0.0, ay = 0.0, az = 0.0;
-        PathState P;
-        if (active) path_init(P, S, L.pixel_begin + local0 + cur_j, L.sample_offset + (q - cur_j * spp));
-        while (__any_sync(0xFFFFFFFFu, active)) {
-            if (!active) continue;
-            float env[8];
-            int r = (P.bounce >= max_bounces) ? (int)BOUNCE_KILLED : path_bounce(P, S, s_planes, env);
-            if (r == BOUNCE_CONTINUE && P.bounce < max_bounces) continue;
-            // The path finished (escaped, roulette, or reached the bounce cap).
-            V3 xyz = path_finish(P, S, r == BOUNCE_ESCAPED, env);
-            if (isfinite(xyz.x) && isfinite(xyz.y) && isfinite(xyz.z)) {
-                ax += (double)xyz.x;
-                ay += (double)xyz.y;
-                az += (double)xyz.z;
-            } else {
-                ++drops;
-            }
-            q += 32;
-            uint32_t j = (q < total) ? q / spp : 0xFFFFFFFFu;
-            if (j != cur_j) {
-                double* slot = part + ((size_t)cur_j * 32 + lane) * 3;
-                slot[0] = ax;
-                slot[1] = ay;
-                slot[2] = az;
-                ax = ay = az = 0.0;
-                cur_j = j;
-            }
-            if (q < total)
-                path_init(P, S, L.pixel_begin + local0 + cur_j, L.sample_offset + (q - cur_j * spp));
-            else
-                active = false;
-        }
-        __syncwarp();
-        for (uint32_t j = 0; j < npix; ++j) {
-            const double* slot = part + ((size_t)j * 32 + lane) * 3;
-            double x = slot[0], y = slot[1], z = slot[2];
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                x += __shfl_down_sync(0xFFFFFFFFu, x, off);
-                y += __shfl_down_sync(0xFFFFFFFFu, y, off);
-                z += __shfl_down_sync(0xFFFFFFFFu, z, off);
-            }
-            if (lane == 0) {
-                double* o = L.out + (size_t)(local0 + j) * 3;
-                if (L.accumulate) {
-                    o[0] += x;
-                    o[1] += y;
-                    o[2] += z;
-                } else {
-                    o[0] = x;
-                    o[1] = y;
-                    o[2] = z;
-                }
-            }
-        }
-        __syncwarp();
+        drops += trace_task(g, S, s_planes, L.pixel_begin + local0, npix, L.spp, L.sample_offset,
+                            s_part[threadIdx.x >> 5], L.out + (size_t)local0 * 3, L.accumulate);
     }
     if (drops && L.dropped) atomicAdd(L.dropped, drops);
+}
+
+// Many scenes in one persistent launch (BatchLaunch): the task space is the
+// concatenation of every job's tasks; a warp finds its job by binary search over the
+// jobs' first-task offsets and reloads its plane slot only when the job's scene changes.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) IX_SFX(batch_kernel)(const __grid_constant__ BatchLaunch L) {
+    __shared__ float4 s_planes[WARPS_PER_CTA][IX_MAX_PLANES];
+    __shared__ PartSlot s_part[WARPS_PER_CTA];
+    const Group g = make_group();
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = threadIdx.x >> 5;
+    uint32_t cached = 0xFFFFFFFFu;
+    unsigned long long drops = 0;
+    for (;;) {
+        uint32_t task = 0;
+        if (lane == 0) task = atomicAdd(L.task_counter, 1u);
+        task = __shfl_sync(0xFFFFFFFFu, task, 0);
+        if (task >= L.total_tasks) break;
+        uint32_t lo = 0, hi = L.n_jobs;  // last job with task_begin <= task
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (L.jobs[mid].task_begin <= task)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const BatchJob job = L.jobs[lo];
+        const ix_scene& sc = L.scenes[job.scene];
+        if (job.scene != cached) {
+            __syncwarp();
+            const float4* gp = reinterpret_cast<const float4*>(sc.planes);
+            for (uint32_t i = lane; i < sc.n_planes; i += 32) s_planes[warp][i] = gp[i];
+            __syncwarp();
+            cached = job.scene;
+        }
+        const DevScene S{sc, L.absorbing[job.scene]};
+        const uint32_t local0 = (task - job.task_begin) * job.ppt;
+        const uint32_t npix = min(job.ppt, job.n_pixels - local0);
+        drops += trace_task(g, S, s_planes[warp], local0, npix, job.spp, job.sample_offset, s_part[warp],
+                            L.out + job.out_offset + (size_t)local0 * 3, L.accumulate);
+    }
+    if (drops && L.dropped) atomicAdd(L.dropped, drops);
+}
+
+// Per-path checks: each 8-lane group traces one input row, exactly as the megakernel
+// traces a path.
+__global__ void __launch_bounds__(128) IX_SFX(check_trace_kernel)(const __grid_constant__ CheckLaunch L) {
+    __shared__ float4 s_planes[IX_MAX_PLANES];
+    const float4* gplanes = reinterpret_cast<const float4*>(L.scene.planes);
+    for (uint32_t i = threadIdx.x; i < L.scene.n_planes; i += blockDim.x) s_planes[i] = gplanes[i];
+    __syncthreads();
+    const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+    if (row >= L.n) return;  // whole groups leave together (rows are group-aligned)
+    const DevScene S{L.scene, L.absorbing};
+    const Group g = make_group();
+    const uint32_t* in = L.in + (size_t)row * L.in_stride;
+    uint32_t* out = L.out + (size_t)row * L.out_stride;
+    LanePath P;
+    if (L.fn == CHECK_TRACE) {
+        group_init(g, P, S, in[0], in[1]);
+    } else {
+        Ray r{v3(__uint_as_float(in[0]), __uint_as_float(in[1]), __uint_as_float(in[2])),
+              v3(__uint_as_float(in[3]), __uint_as_float(in[4]), __uint_as_float(in[5]))};
+        group_init_ray(g, P, S, r, in[6], __uint_as_float(in[7]));
+    }
+    uint32_t it = 0;
+    const V3 xyz = group_trace(g, P, S, s_planes, &it);
+    if (g.c == 0) {
+        out[0] = __float_as_uint(xyz.x);
+        out[1] = __float_as_uint(xyz.y);
+        out[2] = __float_as_uint(xyz.z);
+        out[3] = it;
+    }
 }
 
 // One reference function per thread, for the per-function parity checks.
@@ -193,29 +285,6 @@ __global__ void IX_SFX(check_kernel)(const __grid_constant__ CheckLaunch L) {
             put(1, (float)h.facet);
             break;
         }
-        case CHECK_TRACE:
-        case CHECK_TRACE_RAY: {
-            PathState P;
-            if (L.fn == CHECK_TRACE)
-                path_init(P, S, in[0], in[1]);
-            else
-                path_init_ray(P, S, Ray{v3(inf(0), inf(1), inf(2)), v3(inf(3), inf(4), inf(5))}, in[6],
-                              inf(7));
-            float env[8];
-            int r = BOUNCE_CONTINUE;
-            uint32_t iterations = 0;
-            while (P.bounce < S.s.max_bounces) {
-                r = path_bounce(P, S, s_planes, env);
-                ++iterations;
-                if (r != BOUNCE_CONTINUE) break;
-            }
-            V3 xyz = path_finish(P, S, r == BOUNCE_ESCAPED, env);
-            put(0, xyz.x);
-            put(1, xyz.y);
-            put(2, xyz.z);
-            out[3] = iterations;
-            break;
-        }
         case CHECK_CAMERA_RAY: {
             Draws d = sample_draws(in[0], in[1]);
             uint32_t x = in[0] % S.s.width, y = in[0] / S.s.width;
@@ -234,17 +303,31 @@ __global__ void IX_SFX(check_kernel)(const __grid_constant__ CheckLaunch L) {
     }
 }
 
-static size_t trace_smem_bytes(int threads) {
-    return (size_t)(threads / 32) * TRACE_MAX_PPT * 32 * 3 * sizeof(double);
-}
+static bool launch_shape_ok(int threads) { return threads == 128; }
 
 cudaError_t IX_SFX(launch_trace)(const TraceLaunch& l, cudaStream_t stream) {
     if (l.pixels_per_task == 0 || l.pixels_per_task > (uint32_t)TRACE_MAX_PPT) return cudaErrorInvalidValue;
-    if (l.threads % 32 != 0 || l.threads > 128 || l.threads <= 0) return cudaErrorInvalidValue;
+    if (!launch_shape_ok(l.threads)) return cudaErrorInvalidValue;
     if (l.scene.n_planes > IX_MAX_PLANES) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
-    IX_SFX(trace_kernel)<<<l.blocks, l.threads, trace_smem_bytes(l.threads), stream>>>(l);
+    switch (l.variant) {
+        case 1: IX_SFX(trace_kernel)<6><<<l.blocks, l.threads, 0, stream>>>(l); break;
+        case 2: IX_SFX(trace_kernel)<8><<<l.blocks, l.threads, 0, stream>>>(l); break;
+        default: IX_SFX(trace_kernel)<1><<<l.blocks, l.threads, 0, stream>>>(l); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t IX_SFX(launch_batch)(const BatchLaunch& l, cudaStream_t stream) {
+    if (!launch_shape_ok(l.threads) || l.n_jobs == 0) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    switch (l.variant) {
+        case 1: IX_SFX(batch_kernel)<6><<<l.blocks, l.threads, 0, stream>>>(l); break;
+        case 2: IX_SFX(batch_kernel)<8><<<l.blocks, l.threads, 0, stream>>>(l); break;
+        default: IX_SFX(batch_kernel)<1><<<l.blocks, l.threads, 0, stream>>>(l); break;
+    }
     return cudaGetLastError();
 }
 
@@ -252,18 +335,34 @@ cudaError_t IX_SFX(launch_check)(const CheckLaunch& l, cudaStream_t stream) {
     if (l.scene.n_planes > IX_MAX_PLANES) return cudaErrorInvalidValue;
     if (l.n == 0) return cudaSuccess;
     const int threads = 128;
-    const int blocks = (int)((l.n + threads - 1) / threads);
-    IX_SFX(check_kernel)<<<blocks, threads, 0, stream>>>(l);
+    if (l.fn == CHECK_TRACE || l.fn == CHECK_TRACE_RAY) {
+        const int blocks = (int)((l.n * 8ull + threads - 1) / threads);
+        IX_SFX(check_trace_kernel)<<<blocks, threads, 0, stream>>>(l);
+    } else {
+        const int blocks = (int)((l.n + threads - 1) / threads);
+        IX_SFX(check_kernel)<<<blocks, threads, 0, stream>>>(l);
+    }
     return cudaGetLastError();
 }
 
-int IX_SFX(trace_blocks_per_sm)(int threads, size_t* smem_bytes) {
+template <typename K>
+static int occupancy(K kernel, int threads) {
     int blocks = 0;
-    size_t smem = trace_smem_bytes(threads);
-    if (smem_bytes) *smem_bytes = smem;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, IX_SFX(trace_kernel), threads, smem) != cudaSuccess)
-        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, 0) != cudaSuccess) return 0;
     return blocks;
+}
+
+int IX_SFX(trace_blocks_per_sm)(int threads, int variant, size_t* smem_bytes) {
+    if (smem_bytes) *smem_bytes = 0;
+    if (variant == 1) return occupancy(IX_SFX(trace_kernel)<6>, threads);
+    if (variant == 2) return occupancy(IX_SFX(trace_kernel)<8>, threads);
+    return occupancy(IX_SFX(trace_kernel)<1>, threads);
+}
+
+int IX_SFX(batch_blocks_per_sm)(int threads, int variant) {
+    if (variant == 1) return occupancy(IX_SFX(batch_kernel)<6>, threads);
+    if (variant == 2) return occupancy(IX_SFX(batch_kernel)<8>, threads);
+    return occupancy(IX_SFX(batch_kernel)<1>, threads);
 }
 
 }  // namespace ix

@@ -25,6 +25,35 @@ struct TraceLaunch {
     unsigned long long* dropped;  // device, non-finite samples dropped (may be null)
     int blocks;                // persistent grid size
     int threads;               // threads per block (multiple of 32)
+    int variant;               // register/occupancy variant: 0 unconstrained, 1 six blocks/SM, 2 eight
+};
+
+// One job of a batched launch: `n_pixels` pixels of scene `scene` x `spp` samples from
+// `sample_offset`, split into tasks of `ppt` pixels starting at global task `task_begin`;
+// its per-pixel sums go to out + out_offset.
+struct BatchJob {
+    uint32_t scene;
+    uint32_t n_pixels;
+    uint32_t spp;
+    uint32_t ppt;
+    uint32_t task_begin;
+    uint32_t sample_offset;
+    uint64_t out_offset;
+};
+
+struct BatchLaunch {
+    const ix_scene* scenes;      // device array; each scene's `planes` is a device pointer
+    const uint32_t* absorbing;   // device, per scene
+    const BatchJob* jobs;        // device, ascending task_begin
+    uint32_t n_jobs;
+    uint32_t total_tasks;
+    double* out;
+    int accumulate;
+    uint32_t* task_counter;
+    unsigned long long* dropped;
+    int blocks;
+    int threads;
+    int variant;
 };
 
 // Per-function check kernels: evaluate one reference function per input row on the
@@ -59,11 +88,15 @@ struct CheckLaunch {
 
 cudaError_t launch_trace_exact(const TraceLaunch& l, cudaStream_t stream);
 cudaError_t launch_trace_fast(const TraceLaunch& l, cudaStream_t stream);
+cudaError_t launch_batch_exact(const BatchLaunch& l, cudaStream_t stream);
+cudaError_t launch_batch_fast(const BatchLaunch& l, cudaStream_t stream);
+int batch_blocks_per_sm_exact(int threads, int variant);
+int batch_blocks_per_sm_fast(int threads, int variant);
 cudaError_t launch_check_exact(const CheckLaunch& l, cudaStream_t stream);
 cudaError_t launch_check_fast(const CheckLaunch& l, cudaStream_t stream);
 // Occupancy-derived resident blocks per SM for the trace kernel at `threads` per block.
-int trace_blocks_per_sm_exact(int threads, size_t* smem_bytes);
-int trace_blocks_per_sm_fast(int threads, size_t* smem_bytes);
+int trace_blocks_per_sm_exact(int threads, int variant, size_t* smem_bytes);
+int trace_blocks_per_sm_fast(int threads, int variant, size_t* smem_bytes);
 // FP32 FMA-pipe throughput probe (ix_probe.cu): best FLOP/s of `reps` timed runs.
 cudaError_t fp32_probe(int sm_count, int reps, cudaStream_t stream, double* flops);
 

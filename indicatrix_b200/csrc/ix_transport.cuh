@@ -1,13 +1,18 @@
-// ix_transport.cuh -- one spectral path on the GPU: setup, one bounce, finish.
+// ix_transport.cuh -- one spectral path traced by an 8-lane group (sm_100a).
 //
-// The path is split into three device functions so the megakernel can regenerate a
-// finished lane with its next sample while the warp's other lanes keep bouncing (the
-// bounce body, where nearly all the work is, then runs converged across lanes that are
-// on different paths).  Together they compute what the reference's
-// trace_spectral_ray_core computes for one (pixel, absolute sample)
-// (optics/raytracer/transport/inner/bounce_body.rs:216-764) for a convex, polished,
-// non-scattering, non-fluorescent stone with an isotropic material -- the scenes
-// `ix_scene_routes_to_gpu` admits.
+// GPU-first layout of the reference's per-sample estimator
+// (optics/raytracer/transport/inner/bounce_body.rs:216-764): a path carries 8
+// hero-wavelength channels, so a path is traced by 8 lanes of a warp, lane c holding
+// channel c (its wavelength, index, absorption, Stokes vector, path pdf, exit-split
+// radiance and MIS family mask).  What the reference computes once per path (the ray,
+// the hero's decisions, the lighting direction) every lane of the group computes from
+// identical inputs; what it loops over channels for, each lane does for its own channel.
+// The slab intersection is split across the group (lane c scans planes c, c+8, ...) and
+// reduced with shuffles to the first plane attaining the extremum, which is exactly the
+// plane the reference's sequential scan keeps.  A warp holds 4 independent paths.
+//
+// Every group-level branch condition is computed from bit-identical inputs in the 8
+// lanes, so a group never diverges internally and all shuffles use the group's mask.
 #pragma once
 
 #include "ix_device.cuh"
@@ -20,58 +25,130 @@ constexpr float R_UNPOL_PDF_MAX = 1.0f - 1e-4f;          // refraction/mod.rs:14
 constexpr float R_UNPOL_SELECT_MIN = 0.02f;              // refraction/mod.rs:153
 constexpr float R_UNPOL_SELECT_MAX = 0.98f;              // refraction/mod.rs:156
 
-// Scene as the kernels see it: the host POD with `planes` pointing at device memory and
-// a few per-scene flags resolved on the host.
+// Scene as the kernels see it: the host POD (in kernel parameter space) with `planes`
+// pointing at device memory, plus per-scene flags resolved on the host.
 struct DevScene {
-    const ix_scene& s;   // lives in kernel parameter space (__grid_constant__)
+    const ix_scene& s;
     uint32_t absorbing;  // the material has any absorption term
 };
 
-struct PathState {
+// The 8 lanes of one path: `mask` selects them in the warp, `c` is this lane's channel.
+struct Group {
+    unsigned mask;
+    int c;
+};
+IX_DEV Group make_group() {
+    const int lane = (int)(threadIdx.x & 31u);
+    return Group{0xFFu << (lane & ~7), lane & 7};
+}
+IX_DEV float gshfl(const Group& g, float v, int src) { return __shfl_sync(g.mask, v, src, 8); }
+IX_DEV int gshfl(const Group& g, int v, int src) { return __shfl_sync(g.mask, v, src, 8); }
+IX_DEV float gxor(const Group& g, float v, int m) { return __shfl_xor_sync(g.mask, v, m, 8); }
+IX_DEV int gxor(const Group& g, int v, int m) { return __shfl_xor_sync(g.mask, v, m, 8); }
+
+// Per-lane path state.  The first block is identical in the group's 8 lanes.
+struct LanePath {
     uint32_t seed;
     uint32_t bounce;
-    float lambdas[8];
-    float n_ch[8];
-    float alpha[8];
-    Stokes st[8];
-    float pdf[8];
-    float split[8];
-    uint32_t compat_lo, compat_hi;  // compat[k] as bytes: k<4 in lo, k>=4 in hi
     V3 o, d;
     V3 prev_pn;
     V3 observer;
+    float n_hero;
     bool inside;
     bool has_prev;
+    // channel c of the path
+    float lambda;
+    float n;
+    float alpha;
+    Stokes st;
+    float pdf;
+    float split;
+    uint32_t compat;  // MIS family of this channel (refraction/context.rs:219)
 };
 
-IX_DEV uint32_t compat_get(const PathState& P, int k) {
-    uint32_t w = (k < 4) ? P.compat_lo : P.compat_hi;
-    return (w >> (8 * (k & 3))) & 0xFFu;
-}
-IX_DEV void compat_clear_bit(PathState& P, int k, int bit) {
-    uint32_t m = ~(1u << (8 * (k & 3) + bit));
-    if (k < 4)
-        P.compat_lo &= m;
-    else
-        P.compat_hi &= m;
+// ------------------------------------------------------------------------------------
+// Cooperative slab intersection (simd/slab.rs:120-160; intersect.rs:101-127), with the
+// division-free candidate filter of intersect_planes (ix_device.cuh).
+// ------------------------------------------------------------------------------------
+IX_DEV Hit group_intersect(const Group& g, const float4* __restrict__ planes, int n, V3 o, V3 d) {
+    float t_near = -1e30f, t_far = 1e30f;
+    int near_idx = -1, far_idx = -1;
+    int outside = 0;
+    for (int i = g.c; i < n; i += 8) {
+        float4 p = planes[i];
+        float denom = (p.x * d.x + p.y * d.y) + p.z * d.z;
+        float side = p.w + ((p.x * o.x + p.y * o.y) + p.z * o.z);
+        if (fabsf(denom) > 1e-7f) {
+            const bool entering = denom < 0.0f;
+            const float bound = entering ? t_near : t_far;
+            if (fmaf(bound, denom, side) >= 0.0f) {
+                float t = __fdiv_rn(-side, denom);
+                if (entering) {
+                    if (t > t_near) {
+                        t_near = t;
+                        near_idx = i;
+                    }
+                } else if (t < t_far) {
+                    t_far = t;
+                    far_idx = i;
+                }
+            }
+        } else if (side > 0.0f) {
+            outside = 1;
+            break;
+        }
+    }
+    // Reduce to the first plane attaining the max t_near / min t_far (sequential-scan
+    // semantics: a later plane replaces the running extremum only when strictly better).
+#pragma unroll
+    for (int m = 4; m > 0; m >>= 1) {
+        float tn = gxor(g, t_near, m);
+        int ni = gxor(g, near_idx, m);
+        float tf = gxor(g, t_far, m);
+        int fi = gxor(g, far_idx, m);
+        outside |= gxor(g, outside, m);
+        if (tn > t_near || (tn == t_near && ni >= 0 && (near_idx < 0 || ni < near_idx))) {
+            t_near = tn;
+            near_idx = ni;
+        }
+        if (tf < t_far || (tf == t_far && fi >= 0 && (far_idx < 0 || fi < far_idx))) {
+            t_far = tf;
+            far_idx = fi;
+        }
+    }
+    Hit h;
+    h.facet = -1;
+    h.t = 0.0f;
+    if (outside || t_near > t_far) return h;
+    if (t_near > 1e-4f) {
+        h.t = t_near;
+        h.facet = near_idx >= 0 ? near_idx : 0;
+    } else if (t_far > 1e-4f) {
+        h.t = t_far;
+        h.facet = far_idx >= 0 ? far_idx : 0;
+    }
+    return h;
 }
 
-// PathState::new (bounce_body.rs:260-356) for an explicit ray, seed and hero draw
-// (trace_spectral_ray, transport/mod.rs:118).
-IX_DEV void path_init_ray(PathState& P, const DevScene& S, Ray r, uint32_t seed, float hero) {
+// ------------------------------------------------------------------------------------
+// Path setup: PathState::new (bounce_body.rs:260-356).
+// ------------------------------------------------------------------------------------
+IX_DEV void group_init_ray(const Group& g, LanePath& P, const DevScene& S, Ray r, uint32_t seed,
+                           float hero_rand) {
     const ix_scene& sc = S.s;
     P.seed = seed;
     P.bounce = 0;
-    hero_wavelengths(hero, P.lambdas);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        P.n_ch[k] = dispersion_eval(sc.material.dispersion, P.lambdas[k]);
-        P.alpha[k] = S.absorbing ? spectral_absorption(sc.material.abs_o, P.lambdas[k]) : 0.0f;
-        P.st[k] = Stokes{1.0f, 0.0f, 0.0f, 0.0f};
-        P.pdf[k] = 1.0f;
-        P.split[k] = 0.0f;
-    }
-    P.compat_lo = P.compat_hi = 0xFFFFFFFFu;
+    // wrapped_hero_wavelengths (transport/mod.rs:58): channel c of the comb.
+    float lambda_hero = fmaf(hero_rand, 400.0f, 380.0f);
+    float offset = fmaf((float)g.c, 50.0f, lambda_hero - 380.0f);
+    P.lambda = 380.0f + rem_euclid_400(offset);
+    P.n = dispersion_eval(sc.material.dispersion, P.lambda);
+    P.n_hero = gshfl(g, P.n, 0);
+    P.alpha = S.absorbing ? spectral_absorption(sc.material.abs_o, P.lambda) : 0.0f;
+    P.st = Stokes{1.0f, 0.0f, 0.0f, 0.0f};
+    P.pdf = 1.0f;
+    P.split = 0.0f;
+    P.compat = 0xFFu;
     P.o = r.origin;
     P.d = r.dir;
     P.observer = -r.dir;
@@ -81,32 +158,35 @@ IX_DEV void path_init_ray(PathState& P, const DevScene& S, Ray r, uint32_t seed,
 }
 
 // One (pixel, absolute sample) as renderer/cpu_frame.rs:45-70 traces it.
-IX_DEV void path_init(PathState& P, const DevScene& S, uint32_t pixel, uint32_t sample) {
+IX_DEV void group_init(const Group& g, LanePath& P, const DevScene& S, uint32_t pixel,
+                       uint32_t sample) {
     const ix_scene& sc = S.s;
     Draws dr = sample_draws(pixel, sample);
     uint32_t x = pixel % sc.width, y = pixel / sc.width;
     Ray r = generate_ray(sc.camera, (float)x, (float)y, (float)sc.width, (float)sc.height,
                          dr.jx, dr.jy);
-    path_init_ray(P, S, r, dr.seed, dr.hero);
+    group_init_ray(g, P, S, r, dr.seed, dr.hero);
 }
 
-// try_split_exit_channel (refraction/exit_split.rs:128): one extra intersection, then an
-// environment lookup at the channel's own wavelength if the probe escapes.
-IX_DEV void split_exit_channel(PathState& P, const DevScene& S, const float4* planes, V3 hit,
-                               int k, V3 dir_k, float transmitted_i) {
-    V3 o = hit + dir_k * 1e-4f;
-    Hit h = intersect_planes(planes, (int)S.s.n_planes, o, dir_k);
-    if (h.facet >= 0) return;
-    const ix_environment& env = S.s.environment;
-    Lighting L = direction_lighting(env, dir_k, P.observer);
-    float e = lighting_radiance(L, env, spectral_power(env, P.lambdas[k]));
-    P.split[k] = fmaf(fmaxf(transmitted_i, 0.0f), e, P.split[k]);
+// ------------------------------------------------------------------------------------
+// Per-channel physics.
+// ------------------------------------------------------------------------------------
+// tir_phase_delta (refraction/tir.rs:33).
+IX_DEV float tir_phase_delta(float n1k, float cos_i, float sin_i) {
+    float tan_half = (cos_i * sqrtf(fmaxf(fmaf(n1k * n1k * sin_i, sin_i, -1.0f), 0.0f))) /
+                     fmaxf(n1k * sin_i * sin_i, 1e-6f);
+    return 2.0f * atanf(tan_half);
 }
+IX_DEV void fresnel_rs_rp(float n1, float n2, float cos_i, float cos_t, float& r_s, float& r_p) {
+    r_s = fmaf(n2, -cos_t, n1 * cos_i) / fmaf(n2, cos_t, n1 * cos_i);
+    r_p = fmaf(n1, -cos_t, n2 * cos_i) / fmaf(n1, cos_t, n2 * cos_i);
+}
+IX_DEV float r_unpol_of(float r_s, float r_p) { return 0.5f * fmaf(r_p, r_p, r_s * r_s); }
 
 // Beer-Lambert for an isotropic material (raytracer/absorption.rs:99, :197): the channel
 // alpha is the midpoint of the absorption tensor's quadratic form over the two
 // eigen-polarisations of the wave normal.
-IX_DEV void isotropic_absorption(PathState& P, const DevScene& S, V3 k_hat, float len) {
+IX_DEV void lane_absorption(LanePath& P, const DevScene& S, V3 k_hat, float len) {
     const ix_material& m = S.s.material;
     V3 raw_c = load3(m.c_axis);
     V3 c_axis = normalize_or_zero(raw_c);
@@ -125,66 +205,48 @@ IX_DEV void isotropic_absorption(PathState& P, const DevScene& S, V3 k_hat, floa
     V3 eb = normalize_or_zero(cross(k_hat, ea));
     float la0 = dot(a1, ea), la1 = dot(a2, ea), la2 = dot(c_axis, ea);
     float lb0 = dot(a1, eb), lb1 = dot(a2, eb), lb2 = dot(c_axis, eb);
-    float qa0 = la0 * la0, qa1 = la1 * la1, qa2 = la2 * la2;
-    float qb0 = lb0 * lb0, qb1 = lb1 * lb1, qb2 = lb2 * lb2;
-    float scaled = len * m.absorption_path_scale;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        float ao = P.alpha[k];
-        float qa = (ao * qa0 + ao * qa1) + ao * qa2;
-        float qb = (ao * qb0 + ao * qb1) + ao * qb2;
-        float alpha = midpointf_(qa, qb);
-        P.st[k] = scale(P.st[k], exp_lane(-alpha * scaled));
-    }
+    float ao = P.alpha;
+    float qa = (ao * (la0 * la0) + ao * (la1 * la1)) + ao * (la2 * la2);
+    float qb = (ao * (lb0 * lb0) + ao * (lb1 * lb1)) + ao * (lb2 * lb2);
+    float alpha = midpointf_(qa, qb);
+    P.st = scale(P.st, exp_lane(-alpha * (len * m.absorption_path_scale)));
 }
 
-// tir_phase_delta (refraction/tir.rs:33).
-IX_DEV float tir_phase_delta(float n1k, float cos_i, float sin_i) {
-    float tan_half = (cos_i * sqrtf(fmaxf(fmaf(n1k * n1k * sin_i, sin_i, -1.0f), 0.0f))) /
-                     fmaxf(n1k * sin_i * sin_i, 1e-6f);
-    return 2.0f * atanf(tan_half);
+// Escape radiance of channel c along `dir` (environment/rig.rs:18-49, :728).
+IX_DEV float lane_environment(const ix_environment& env, V3 dir, V3 observer, float lambda) {
+    Lighting L = direction_lighting(env, dir, observer);
+    return lighting_radiance(L, env, spectral_power(env, lambda));
 }
-IX_DEV void fresnel_rs_rp(float n1, float n2, float cos_i, float cos_t, float& r_s, float& r_p) {
-    r_s = fmaf(n2, -cos_t, n1 * cos_i) / fmaf(n2, cos_t, n1 * cos_i);
-    r_p = fmaf(n1, -cos_t, n2 * cos_i) / fmaf(n1, cos_t, n2 * cos_i);
-}
-IX_DEV float r_unpol_of(float r_s, float r_p) { return 0.5f * fmaf(r_p, r_p, r_s * r_s); }
 
 enum BounceResult { BOUNCE_CONTINUE = 0, BOUNCE_ESCAPED = 1, BOUNCE_KILLED = 2 };
 
 // One iteration of the bounce loop (bounce_body.rs:361-423 and facet_event :611-707).
-// On BOUNCE_ESCAPED, `env_out` holds the escape radiance per channel already weighted by
-// the channel's Stokes intensity (accumulate_miss_radiance, transport/bounce.rs:40).
-IX_DEV int path_bounce(PathState& P, const DevScene& S, const float4* __restrict__ planes,
-                       float env_out[8]) {
+// On BOUNCE_ESCAPED `esc` is this channel's escape radiance already weighted by its
+// Stokes intensity (accumulate_miss_radiance, transport/bounce.rs:40).
+IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
+                        const float4* __restrict__ planes, float& esc) {
     const ix_scene& sc = S.s;
     const uint32_t bounce = P.bounce;
-    Hit hit = intersect_planes(planes, (int)sc.n_planes, P.o, P.d);
+    const int n_planes = (int)sc.n_planes;
+    Hit hit = group_intersect(g, planes, n_planes, P.o, P.d);
     if (hit.facet < 0) {
-        const ix_environment& env = sc.environment;
-        Lighting L = direction_lighting(env, P.d, P.observer);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            float e = lighting_radiance(L, env, spectral_power(env, P.lambdas[k]));
-            env_out[k] = fmaf(intensity(P.st[k]), e, 0.0f);
-        }
+        esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         return BOUNCE_ESCAPED;
     }
-    float4 pl = planes[hit.facet];
+    const float4 pl = planes[hit.facet];
     V3 normal = v3(pl.x, pl.y, pl.z);
-    V3 hit_point = P.o + hit.t * P.d;
+    const V3 hit_point = P.o + hit.t * P.d;
     const V3 k_hat = P.d;  // isotropic: wave normal == ray direction
 
     // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:69).
-    V3 cpn = normalize_or_zero(cross(k_hat, normal));
+    const V3 cpn = normalize_or_zero(cross(k_hat, normal));
     if (P.has_prev && length_squared(cpn) > 1e-6f && length_squared(P.prev_pn) > 1e-6f) {
         float cos_psi = clampf_(dot(P.prev_pn, cpn), -1.0f, 1.0f);
         float sin_psi = dot(cross(P.prev_pn, cpn), normalize_or_zero(k_hat));
         float psi = atan2f(sin_psi, cos_psi);
         float s2, c2;
         sincosf(2.0f * psi, &s2, &c2);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) P.st[k] = rotate(P.st[k], c2, s2);
+        P.st = rotate(P.st, c2, s2);
     }
     P.has_prev = true;
     P.prev_pn = cpn;
@@ -192,135 +254,122 @@ IX_DEV int path_bounce(PathState& P, const DevScene& S, const float4* __restrict
     // apply_interior_segment (transport/inner.rs:170).
     if (P.inside) {
         normal = -normal;
-        if (S.absorbing) isotropic_absorption(P, S, k_hat, hit.t);
+        if (S.absorbing) lane_absorption(P, S, k_hat, hit.t);
     }
 
     // compute_bounce_refraction_geometry (refraction/geometry.rs:306), isotropic.
     const float cos_i = clampf_(dot(-k_hat, normal), 0.0f, 1.0f);
     const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
     const float sin_i = sqrtf(fmaxf(one_m_c2, 0.0f));
-    const float n1 = P.inside ? P.n_ch[0] : 1.0f;
-    const float n2 = P.inside ? 1.0f : P.n_ch[0];
+    const float n1 = P.inside ? P.n_hero : 1.0f;
+    const float n2 = P.inside ? 1.0f : P.n_hero;
     const float eta = n1 / n2;
     const float sin2_t = eta * eta * one_m_c2;
+    const float n1k = P.inside ? P.n : 1.0f;
+    const float n2k = P.inside ? 1.0f : P.n;
 
-    V3 new_dir;
-    bool new_inside = P.inside;
-    if (sin2_t > 1.0f) {
-        // apply_tir_bounce, isotropic arm (refraction/tir.rs:98-116).
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            float n1k = P.inside ? P.n_ch[k] : 1.0f;
-            float n2k = P.inside ? 1.0f : P.n_ch[k];
-            float etak = n1k / n2k;
-            float s2k = etak * etak * one_m_c2;
-            if (s2k > 1.0f) {
-                P.st[k] = tir_retard_apply(P.st[k], tir_phase_delta(n1k, cos_i, sin_i));
-            } else {
-                float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
-                float r_s, r_p;
-                fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, r_s, r_p);
-                P.st[k] = fresnel_reflect_apply(P.st[k], r_s, r_p);
-                P.pdf[k] = P.pdf[k] * clampf_(r_unpol_of(r_s, r_p), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
-            }
-        }
-        new_dir = k_hat - 2.0f * dot(k_hat, normal) * normal;
-    } else {
-        // apply_partial_fresnel_bounce (refraction/dispatch.rs:307).
+    // dispatch_bounce (transport/bounce.rs:108): the hero decides TIR (sin2_t > 1), else
+    // apply_partial_fresnel_bounce (refraction/dispatch.rs:307) draws reflect vs refract.
+    const bool tir = sin2_t > 1.0f;
+    float r_unpol = 1.0f;
+    bool reflect = tir;
+    if (!tir) {
         float cos_t = sqrtf(fmaxf(1.0f - sin2_t, 0.0f));
         float r_s, r_p;
         fresnel_rs_rp(n1, n2, cos_i, cos_t, r_s, r_p);
-        const float r_unpol = clampf_(r_unpol_of(r_s, r_p), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
-        const float rng = unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM);
-        if (rng < r_unpol) {
-            // apply_partial_reflect_bounce (reflect_refract.rs:33).
-            const float inv = 1.0f / r_unpol;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                float n1k = P.inside ? P.n_ch[k] : 1.0f;
-                float n2k = P.inside ? 1.0f : P.n_ch[k];
-                float etak = n1k / n2k;
-                float s2k = etak * etak * one_m_c2;
-                Stokes s;
-                if (s2k > 1.0f) {
-                    s = tir_retard_apply(P.st[k], tir_phase_delta(n1k, cos_i, sin_i));
-                } else {
-                    float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
-                    float rs, rp;
-                    fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, rs, rp);
-                    P.pdf[k] = P.pdf[k] * clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
-                    s = fresnel_reflect_apply(P.st[k], rs, rp);
-                }
-                P.st[k] = scale(s, inv);
-            }
-            new_dir = k_hat - 2.0f * dot(k_hat, normal) * normal;
+        r_unpol = clampf_(r_unpol_of(r_s, r_p), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
+        reflect = unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM) < r_unpol;
+    }
+    V3 new_dir;
+    bool new_inside = P.inside;
+    if (reflect) {
+        // apply_tir_bounce (tir.rs:98-116) / apply_partial_reflect_bounce
+        // (reflect_refract.rs:33): the channel's TIR retarder or Fresnel reflection; a
+        // partial reflection divides by the selection probability (TIR scales by 1).
+        const float etak = n1k / n2k;
+        const float s2k = etak * etak * one_m_c2;
+        Stokes s;
+        if (s2k > 1.0f) {
+            s = tir_retard_apply(P.st, tir_phase_delta(n1k, cos_i, sin_i));
         } else {
-            // apply_refract_bounce + apply_refract_channel (reflect_refract.rs:121-591).
-            float sin2_t_dir = fminf(eta * eta * one_m_c2, 1.0f);
-            float cos_t_dir = sqrtf(fmaxf(1.0f - sin2_t_dir, 0.0f));
-            V3 final_refr = normalize(eta * k_hat + fmaf(eta, cos_i, -cos_t_dir) * normal);
-            const float inv_t = 1.0f / (1.0f - r_unpol);
-            V3 dirs[8];
-            uint32_t have_dir = 0, hero_match = 0;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                float n1k = P.inside ? P.n_ch[k] : 1.0f;
-                float n2k = P.inside ? 1.0f : P.n_ch[k];
-                float ratio = n1k / n2k;
-                float s2k = (ratio * ratio) * one_m_c2;
-                dirs[k] = v3(0.0f, 0.0f, 0.0f);
-                if (s2k > 1.0f) {
-                    P.st[k] = scale(P.st[k], 0.0f);
-                    P.pdf[k] = 0.0f;
-                    continue;
-                }
-                float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
-                V3 refr_k = normalize(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
-                bool match = dot(refr_k, final_refr) >= DIRECTION_MATCH_COS_TOL;
-                float two = 2.0f * n1k * cos_i;
-                float t_s = two / fmaf(n2k, cos_t_k, n1k * cos_i);
-                float t_p = two / fmaf(n1k, cos_t_k, n2k * cos_i);
-                Stokes original = P.st[k];
-                Stokes transmitted =
-                    scale(fresnel_transmit_apply(original, n1k, n2k, cos_i, cos_t_k, t_s, t_p), inv_t);
-                float rs, rp;
-                fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, rs, rp);
-                float r_unpol_k = clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
-                P.pdf[k] = P.pdf[k] * (1.0f - r_unpol_k);
-                if (match) {
-                    P.st[k] = transmitted;
-                } else {
-                    // apply_channel_chromatic_termination (reflect_refract.rs:444).
-                    P.st[k] = scale(P.st[k], 0.0f);
-                    if (P.inside && intensity(original) > 0.0f)
-                        split_exit_channel(P, S, planes, hit_point, k, refr_k, intensity(transmitted));
-                }
-                dirs[k] = refr_k;
-                have_dir |= 1u << k;
-                hero_match |= (match ? 1u : 0u) << k;
-            }
-            if (!P.inside) {
-                // narrow_compat (refraction/context.rs:219), hero channel 0.
-#pragma unroll
-                for (int a = 0; a < 8; ++a)
-#pragma unroll
-                    for (int b = a + 1; b < 8; ++b) {
-                        bool m;
-                        if (a == 0)
-                            m = (hero_match >> b) & 1u;
-                        else if (((have_dir >> a) & 1u) && ((have_dir >> b) & 1u))
-                            m = dot(dirs[a], dirs[b]) >= DIRECTION_MATCH_COS_TOL;
-                        else
-                            m = true;
-                        if (!m) {
-                            compat_clear_bit(P, a, b);
-                            compat_clear_bit(P, b, a);
-                        }
-                    }
-            }
-            new_dir = final_refr;
-            new_inside = !P.inside;
+            float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
+            float rs, rp;
+            fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, rs, rp);
+            s = fresnel_reflect_apply(P.st, rs, rp);
+            P.pdf = P.pdf * clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
         }
+        P.st = scale(s, tir ? 1.0f : 1.0f / r_unpol);
+        new_dir = k_hat - 2.0f * dot(k_hat, normal) * normal;
+    } else {
+        // apply_refract_bounce (reflect_refract.rs:121): the hero's direction, then each
+        // channel's own Snell direction, transmission and direction match
+        // (apply_refract_channel :517, compute_channel_refraction_geometry :255).
+        const float sin2_t_dir = fminf(eta * eta * one_m_c2, 1.0f);
+        const float cos_t_dir = sqrtf(fmaxf(1.0f - sin2_t_dir, 0.0f));
+        const V3 final_refr = normalize(eta * k_hat + fmaf(eta, cos_i, -cos_t_dir) * normal);
+        const float ratio = n1k / n2k;
+        const float s2k = (ratio * ratio) * one_m_c2;
+        int status = 0;  // 0 channel TIR, 1 direction matches the hero, 2 diverges
+        V3 dir_k = v3(0.0f, 0.0f, 0.0f);
+        float t_intensity = 0.0f;
+        const Stokes original = P.st;
+        if (s2k > 1.0f) {
+            P.st = scale(P.st, 0.0f);
+            P.pdf = 0.0f;
+        } else {
+            const float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
+            dir_k = normalize(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
+            status = dot(dir_k, final_refr) >= DIRECTION_MATCH_COS_TOL ? 1 : 2;
+            const float two = 2.0f * n1k * cos_i;
+            const float t_s = two / fmaf(n2k, cos_t_k, n1k * cos_i);
+            const float t_p = two / fmaf(n1k, cos_t_k, n2k * cos_i);
+            const Stokes transmitted =
+                scale(fresnel_transmit_apply(original, n1k, n2k, cos_i, cos_t_k, t_s, t_p),
+                      1.0f / (1.0f - r_unpol));
+            float rs, rp;
+            fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, rs, rp);
+            P.pdf = P.pdf * (1.0f - clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX));
+            // apply_channel_chromatic_termination (reflect_refract.rs:444): a diverging
+            // channel's radiance is zeroed (its pdf keeps accumulating).
+            P.st = status == 1 ? transmitted : scale(original, 0.0f);
+            t_intensity = intensity(transmitted);
+        }
+        // try_split_exit_channel (refraction/exit_split.rs:128): at an exit, each diverging
+        // live channel probes its own direction; the group scans each probe together.
+        const bool want_probe = status == 2 && P.inside && intensity(original) > 0.0f;
+        unsigned probes = (__ballot_sync(g.mask, want_probe) >> (threadIdx.x & 24u)) & 0xFFu;
+        while (probes) {
+            const int j = __ffs(probes) - 1;
+            probes &= probes - 1;
+            const V3 dj = v3(gshfl(g, dir_k.x, j), gshfl(g, dir_k.y, j), gshfl(g, dir_k.z, j));
+            const Hit ph = group_intersect(g, planes, n_planes, hit_point + dj * 1e-4f, dj);
+            if (ph.facet < 0 && g.c == j) {
+                const float e = lane_environment(sc.environment, dj, P.observer, P.lambda);
+                P.split = fmaf(fmaxf(t_intensity, 0.0f), e, P.split);
+            }
+        }
+        if (!P.inside) {
+            // narrow_compat (refraction/context.rs:219), hero channel 0: channel pairs whose
+            // directions differ leave each other's MIS family.
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const float dx = gshfl(g, dir_k.x, j), dy = gshfl(g, dir_k.y, j), dz = gshfl(g, dir_k.z, j);
+                const int sj = gshfl(g, status, j);
+                if (j == g.c) continue;
+                bool m;
+                if (g.c == 0)
+                    m = sj == 1;
+                else if (j == 0)
+                    m = status == 1;
+                else if (status != 0 && sj != 0)
+                    m = dot(dir_k, v3(dx, dy, dz)) >= DIRECTION_MATCH_COS_TOL;
+                else
+                    m = true;
+                if (!m) P.compat &= ~(1u << j);
+            }
+        }
+        new_dir = final_refr;
+        new_inside = !P.inside;
     }
     P.d = new_dir;
     P.o = hit_point + new_dir * 1e-4f;
@@ -328,24 +377,16 @@ IX_DEV int path_bounce(PathState& P, const DevScene& S, const float4* __restrict
 
     // Surface glare (bounce_body.rs:691-697).
     const float glare = clampf_(sc.environment.surface_glare, 0.0f, 1.0f);
-    if (bounce == 0 && !P.inside && glare < 1.0f) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) P.st[k] = scale(P.st[k], glare);
-    }
-    // apply_russian_roulette (transport/bounce.rs:355).
+    if (bounce == 0 && !P.inside && glare < 1.0f) P.st = scale(P.st, glare);
+    // apply_russian_roulette (transport/bounce.rs:355): q from the brightest channel.
     if (bounce > 4) {
-        float max_i = 0.0f;
+        float max_i = intensity(P.st);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) max_i = fmaxf(max_i, intensity(P.st[k]));
-        float q = clampf_(max_i, 0.05f, 1.0f);
-        float rr = unit_draw(P.seed, bounce, RUSSIAN_ROULETTE_STREAM);
-        if (rr > q) return BOUNCE_KILLED;
-        float inv_q = 1.0f / q;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            P.st[k] = scale(P.st[k], inv_q);
-            P.split[k] = P.split[k] / q;
-        }
+        for (int m = 4; m > 0; m >>= 1) max_i = fmaxf(max_i, gxor(g, max_i, m));
+        const float q = clampf_(fmaxf(0.0f, max_i), 0.05f, 1.0f);
+        if (unit_draw(P.seed, bounce, RUSSIAN_ROULETTE_STREAM) > q) return BOUNCE_KILLED;
+        P.st = scale(P.st, 1.0f / q);
+        P.split = P.split / q;
     }
     P.bounce = bounce + 1;
     return BOUNCE_CONTINUE;
@@ -353,29 +394,33 @@ IX_DEV int path_bounce(PathState& P, const DevScene& S, const float4* __restrict
 
 // finish (bounce_body.rs:724-764): commit the exit splits of an escaped path, integrate
 // each channel over its MIS family (optics/raytracer/color.rs:145), apply the Bradford
-// round trip for studio environments (color.rs:252) and floor at zero.
-IX_DEV V3 path_finish(const PathState& P, const DevScene& S, bool escaped, const float env_i[8]) {
-    const float norm_factor = 50.0f / 106.856f;
+// round trip for studio environments (color.rs:252) and floor at zero.  Every lane of
+// the group returns the path's XYZ.
+IX_DEV V3 group_finish(const Group& g, const LanePath& P, const DevScene& S, bool escaped, float esc) {
+    // family pdf: the sum, in ascending channel order, over this channel's family.
+    float family = 0.0f;
+    bool first = true;
+    const float pdf0 = gshfl(g, P.pdf, 0);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const float pj = gshfl(g, P.pdf, j);
+        if (P.compat & (1u << j)) {
+            family = first ? pj : family + pj;
+            first = false;
+        }
+    }
+    const float w = (family <= 1e-12f) ? 1.0f : (8.0f * pdf0) / family;
+    const float rad = escaped ? esc + P.split : 0.0f;
+    const float s = (rad * w) * (50.0f / 106.856f);
+    const V3 c = cmf(P.lambda);
+    const float cx = c.x * s, cy = c.y * s, cz = c.z * s;
+    // xyz += cmf_k * (...), folded in channel order as the reference folds it.
     float x = 0.0f, y = 0.0f, z = 0.0f;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        uint32_t ck = compat_get(P, k);
-        float family = 0.0f;
-        bool first = true;
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-            if (ck & (1u << j)) {
-                family = first ? P.pdf[j] : family + P.pdf[j];
-                first = false;
-            }
-        float w = (family <= 1e-12f) ? 1.0f : (8.0f * P.pdf[0]) / family;
-        float rad = escaped ? env_i[k] + P.split[k] : 0.0f;
-        float weighted = rad * w;
-        V3 c = cmf(P.lambdas[k]);
-        float s = weighted * norm_factor;
-        x = x + c.x * s;
-        y = y + c.y * s;
-        z = z + c.z * s;
+    for (int j = 0; j < 8; ++j) {
+        x = x + gshfl(g, cx, j);
+        y = y + gshfl(g, cy, j);
+        z = z + gshfl(g, cz, j);
     }
     x = x + 0.0f;
     y = y + 0.0f;
@@ -384,21 +429,30 @@ IX_DEV V3 path_finish(const PathState& P, const DevScene& S, bool escaped, const
     if (env.model != IX_ENV_UNIFORM) {
         float l = fmaf(0.8951f, x, fmaf(0.2664f, y, -0.1614f * z));
         float m = fmaf(-0.7502f, x, fmaf(1.7135f, y, 0.0367f * z));
-        float s = fmaf(0.0389f, x, fmaf(-0.0685f, y, 1.0296f * z));
-        if (env.white_balance) {
-            l = l * env.wb_lms[0];
-            m = m * env.wb_lms[1];
-            s = s * env.wb_lms[2];
-        } else {
-            l = l * 1.0f;
-            m = m * 1.0f;
-            s = s * 1.0f;
-        }
-        x = fmaf(0.986993f, l, fmaf(-0.147054f, m, 0.159963f * s));
-        y = fmaf(0.432305f, l, fmaf(0.518360f, m, 0.049291f * s));
-        z = fmaf(-0.008529f, l, fmaf(0.040043f, m, 0.968487f * s));
+        float q = fmaf(0.0389f, x, fmaf(-0.0685f, y, 1.0296f * z));
+        l = l * env.wb_lms[0];
+        m = m * env.wb_lms[1];
+        q = q * env.wb_lms[2];
+        x = fmaf(0.986993f, l, fmaf(-0.147054f, m, 0.159963f * q));
+        y = fmaf(0.432305f, l, fmaf(0.518360f, m, 0.049291f * q));
+        z = fmaf(-0.008529f, l, fmaf(0.040043f, m, 0.968487f * q));
     }
     return v3(fmaxf(x, 0.0f), fmaxf(y, 0.0f), fmaxf(z, 0.0f));
+}
+
+// A whole path by one group (the check kernels' per-path entry).
+IX_DEV V3 group_trace(const Group& g, LanePath& P, const DevScene& S, const float4* planes,
+                      uint32_t* iterations) {
+    float esc = 0.0f;
+    int r = BOUNCE_CONTINUE;
+    uint32_t it = 0;
+    while (P.bounce < S.s.max_bounces) {
+        r = group_bounce(g, P, S, planes, esc);
+        ++it;
+        if (r != BOUNCE_CONTINUE) break;
+    }
+    if (iterations) *iterations = it;
+    return group_finish(g, P, S, r == BOUNCE_ESCAPED, esc);
 }
 
 }  // namespace ix
