@@ -47,8 +47,8 @@ typedef struct ix_backend_options {
     uint32_t precision;          /* IX_PRECISION_*                                       */
     uint32_t threads_per_block;  /* 0 = autotuned                                        */
     uint64_t chunk_paths;        /* paths per launch; 0 = default (TDR-safe first chunk)  */
-    uint32_t kernel_variant;     /* register budget of the megakernel: 0 unconstrained,    */
-                                 /* 1 six CTAs per SM, 2 eight CTAs per SM                 */
+    uint32_t kernel_variant;     /* register budget of the megakernel: 0 default (eight    */
+                                 /* CTAs per SM), 1 unconstrained, 2 six, 3 eight CTAs/SM   */
 } ix_backend_options;
 
 /* GpuWorkLimits (gpu_backend/limits.rs:6-27): a request above a limit is declined. */

@@ -342,7 +342,9 @@ ix_backend* ix_backend_create(const ix_backend_options* opts) {
         b->bps_exact[v] = std::max(1, ix::trace_blocks_per_sm_exact((int)b->threads, v, nullptr));
         b->bps_fast[v] = std::max(1, ix::trace_blocks_per_sm_fast((int)b->threads, v, nullptr));
     }
-    if (opts && opts->kernel_variant < 3) b->variant = opts->kernel_variant;
+    // Option 0 = the measured default (8 CTAs per SM); 1/2/3 = unconstrained / 6 / 8.
+    b->variant = 2;
+    if (opts && opts->kernel_variant >= 1 && opts->kernel_variant <= 3) b->variant = opts->kernel_variant - 1;
     return b;
 }
 
