@@ -55,12 +55,18 @@ IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const fl
         }
     uint32_t q = gi;
     bool active = q < total;
+    bool fresh = active;  // the group's next path still needs its setup
     uint32_t cur_j = active ? q / spp : 0;
     double ax = 0.0, ay = 0.0, az = 0.0;
     LanePath P;
-    if (active) group_init(g, P, S, pixel0 + cur_j, sample_offset + (q - cur_j * spp));
     while (__any_sync(0xFFFFFFFFu, active)) {
         if (!active) continue;
+        // One setup site for the first path and every regenerated one keeps a single
+        // copy of the setup code in the loop.
+        if (fresh) {
+            group_init(g, P, S, pixel0 + cur_j, sample_offset + (q - cur_j * spp));
+            fresh = false;
+        }
         float esc = 0.0f;
         const int r = (P.bounce >= max_bounces) ? (int)BOUNCE_KILLED : group_bounce(g, P, S, planes, esc);
         if (r == BOUNCE_CONTINUE && P.bounce < max_bounces) continue;
@@ -85,7 +91,7 @@ IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const fl
             cur_j = j;
         }
         if (q < total)
-            group_init(g, P, S, pixel0 + cur_j, sample_offset + (q - cur_j * spp));
+            fresh = true;
         else
             active = false;
     }

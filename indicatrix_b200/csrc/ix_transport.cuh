@@ -130,6 +130,12 @@ IX_DEV Hit group_intersect(const Group& g, const float4* __restrict__ planes, in
     return h;
 }
 
+// The exit-split probes' copy of the scan, out of line (probes are rare next to bounces).
+static __device__ __noinline__ Hit probe_intersect(Group g, const float4* __restrict__ planes, int n, V3 o,
+                                                   V3 d) {
+    return group_intersect(g, planes, n, o, d);
+}
+
 // ------------------------------------------------------------------------------------
 // Path setup: PathState::new (bounce_body.rs:260-356).
 // ------------------------------------------------------------------------------------
@@ -213,7 +219,10 @@ IX_DEV void lane_absorption(LanePath& P, const DevScene& S, V3 k_hat, float len)
 }
 
 // Escape radiance of channel c along `dir` (environment/rig.rs:18-49, :728).
-IX_DEV float lane_environment(const ix_environment& env, V3 dir, V3 observer, float lambda) {
+// Out of line: it runs once per path (the escape) and per exit-split probe, so one copy
+// of the lighting models keeps the bounce loop's instruction footprint small.
+static __device__ __noinline__ float lane_environment(const ix_environment& env, V3 dir, V3 observer,
+                                                     float lambda) {
     Lighting L = direction_lighting(env, dir, observer);
     return lighting_radiance(L, env, spectral_power(env, lambda));
 }
@@ -342,7 +351,7 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
             const int j = __ffs(probes) - 1;
             probes &= probes - 1;
             const V3 dj = v3(gshfl(g, dir_k.x, j), gshfl(g, dir_k.y, j), gshfl(g, dir_k.z, j));
-            const Hit ph = group_intersect(g, planes, n_planes, hit_point + dj * 1e-4f, dj);
+            const Hit ph = probe_intersect(g, planes, n_planes, hit_point + dj * 1e-4f, dj);
             if (ph.facet < 0 && g.c == j) {
                 const float e = lane_environment(sc.environment, dj, P.observer, P.lambda);
                 P.split = fmaf(fmaxf(t_intensity, 0.0f), e, P.split);
