@@ -138,6 +138,33 @@ void ix_batch_plan_destroy(ix_batch_plan* p);
  * `accumulate` = 1 adds into d_accum_xyz, 0 overwrites it. */
 int ix_accumulate_device(ix_backend* b, const ix_scene* scene, uint32_t sample_offset,
                          uint32_t spp, double* d_accum_xyz, int accumulate, void* stream);
+/* Allocation-free form of ix_accumulate_device.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc (a host whose own pool or arena owns all
+ * device memory, a sandboxed plug-in, a runtime with a fixed memory budget): they pass
+ * a scene whose `planes` is a device pointer and a device output `d_accum_xyz`
+ * (width * height * 3 doubles, added into when `accumulate` is 1, overwritten when 0),
+ * and the call needs no backend object and makes no cudaMalloc, cudaFree or other
+ * allocating call.  The kernel's work counters live in a 264-byte array in device
+ * memory that every GPU loading this library holds until the process exits.
+ *
+ * Limits and rules:
+ *   - at most IX_NOALLOC_MAX_LAUNCHES launches of 2^26 paths each, i.e. width * height
+ *     rounded up to whole pixels per launch must fit in 2^32 paths; larger requests
+ *     return IX_NOALLOC_ERR_TOO_LARGE without touching the device;
+ *   - the first call on a device (the current device) looks up the array's device
+ *     address and the launch shape; make that first call before any stream capture;
+ *   - every call shares the one array and clears it on `stream` before its launches, so
+ *     calls whose work overlaps on the GPU (different streams, or other threads) race:
+ *     serialise them on one stream;
+ *   - the work is enqueued on `stream` (NULL: the legacy default stream) and not
+ *     synchronised.
+ * Returns IX_DONE, IX_DECLINED (the scene does not route to the GPU) or an
+ * IX_NOALLOC_ERR_* code. */
+#define IX_NOALLOC_MAX_LAUNCHES 64
+enum { IX_NOALLOC_ERR_ARGS = -1, IX_NOALLOC_ERR_TOO_LARGE = -2, IX_NOALLOC_ERR_CUDA = -3 };
+int ix_accumulate_device_noalloc(const ix_scene* scene, uint32_t sample_offset, uint32_t spp,
+                                 double* d_accum_xyz, int accumulate, void* stream);
 /* GpuBackend::is_lost / try_recover / last_lost_reason (backend.rs:704). */
 int ix_is_lost(const ix_backend* b);
 int ix_try_recover(ix_backend* b);

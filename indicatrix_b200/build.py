@@ -64,12 +64,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if r.returncode != 0:
             raise RuntimeError("nvcc failed:\n" + r.stderr)
         objs.append(obj)
-    probe_obj = os.path.join(BUILD_DIR, "ix_probe.o")
-    r = subprocess.run(common + ["-c", os.path.join(CSRC, "ix_probe.cu"), "-o", probe_obj],
-                       capture_output=True, text=True)
-    if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stderr)
-    objs.append(probe_obj)
+    for unit in ("ix_probe", "ix_noalloc"):
+        obj = os.path.join(BUILD_DIR, unit + ".o")
+        r = subprocess.run(common + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + r.stderr)
+        objs.append(obj)
     host_obj = os.path.join(BUILD_DIR, "ix_backend.o")
     cuda_inc = os.path.join(_cuda_home(nvcc), "include")
     cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
