@@ -71,14 +71,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if r.returncode != 0:
             raise RuntimeError("nvcc failed:\n" + r.stderr)
         objs.append(obj)
-    host_obj = os.path.join(BUILD_DIR, "ix_backend.o")
     cuda_inc = os.path.join(_cuda_home(nvcc), "include")
-    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
-           f"-I{INCLUDE}", f"-I{cuda_inc}", "-c", os.path.join(CSRC, "ix_backend.cpp"), "-o", host_obj]
-    r = subprocess.run(cmd, capture_output=True, text=True)
-    if r.returncode != 0:
-        raise RuntimeError("g++ failed:\n" + r.stderr)
-    objs.append(host_obj)
+    for unit in ("ix_backend", "ix_dispatch"):
+        host_obj = os.path.join(BUILD_DIR, unit + ".o")
+        cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
+               f"-I{INCLUDE}", f"-I{cuda_inc}", "-c", os.path.join(CSRC, unit + ".cpp"), "-o", host_obj]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("g++ failed:\n" + r.stderr)
+        objs.append(host_obj)
     tmp = OUT + ".tmp"
     cmd = [nvcc, "-shared", *ARCH, "-o", tmp, *objs, "-cudart", "static", "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -1,0 +1,166 @@
+"""Sample-range dispatch and the deterministic merge (include/ix_dispatch.h), plus the
+multi-process plumbing that uses them.
+
+The reference's indicatrix-dispatch hands disjoint absolute sample ranges to lanes and
+folds their per-pixel sums in ascending first-sample order
+(crates/indicatrix-dispatch/src/sample_cursor/mod.rs, merge/mod.rs).  Here a lane is a
+rank of a ``torch.distributed`` group (one per GPU, or gloo ranks on CPU): ranks claim
+chunks from a cursor shared through the process group's store, trace them, and rank 0
+merges every rank's (first_sample, done, sums) in sample order.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Callable, List, Optional, Tuple
+
+import numpy as np
+
+from .backend import load_library
+
+_bound = False
+
+
+def _lib():
+    global _bound
+    lib = load_library()
+    if not _bound:
+        P = C.POINTER
+        lib.ix_sample_cursor_new.restype = C.c_void_p
+        lib.ix_sample_cursor_new.argtypes = [C.c_uint32, C.c_uint32]
+        lib.ix_sample_cursor_free.argtypes = [C.c_void_p]
+        lib.ix_sample_cursor_claim.argtypes = [C.c_void_p, C.c_uint32, P(C.c_uint32), P(C.c_uint32)]
+        lib.ix_sample_cursor_requeue.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
+        lib.ix_sample_cursor_fully_claimed.argtypes = [C.c_void_p]
+        lib.ix_merger_new.restype = C.c_void_p
+        lib.ix_merger_new.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64]
+        lib.ix_merger_free.argtypes = [C.c_void_p]
+        lib.ix_merger_add.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, P(C.c_double), C.c_uint64,
+                                      P(C.c_uint32)]
+        lib.ix_merger_frontier.restype = C.c_uint32
+        lib.ix_merger_frontier.argtypes = [C.c_void_p]
+        lib.ix_merger_total.restype = C.c_uint32
+        lib.ix_merger_total.argtypes = [C.c_void_p]
+        lib.ix_merger_dropped_pixels.restype = C.c_uint64
+        lib.ix_merger_dropped_pixels.argtypes = [C.c_void_p]
+        lib.ix_merger_snapshot.restype = C.c_uint32
+        lib.ix_merger_snapshot.argtypes = [C.c_void_p, P(C.c_double), C.c_uint64]
+        lib.ix_merger_finish.restype = C.c_uint32
+        lib.ix_merger_finish.argtypes = [C.c_void_p, P(C.c_double), C.c_uint64]
+        _bound = True
+    return lib
+
+
+MERGE_OK, MERGE_WRONG_LENGTH, MERGE_OVERLAP, MERGE_BUDGET = 0, -1, -2, -3
+
+
+class MergeError(RuntimeError):
+    pass
+
+
+class SampleCursor:
+    """SampleCursor (sample_cursor/mod.rs:64): disjoint absolute ranges in order."""
+
+    def __init__(self, start: int, end: int):
+        self._lib = _lib()
+        self._h = self._lib.ix_sample_cursor_new(start, end)
+
+    def claim(self, want: int) -> Optional[Tuple[int, int]]:
+        s, n = C.c_uint32(), C.c_uint32()
+        if self._lib.ix_sample_cursor_claim(self._h, want, C.byref(s), C.byref(n)):
+            return int(s.value), int(n.value)
+        return None
+
+    def requeue(self, start: int, count: int) -> None:
+        self._lib.ix_sample_cursor_requeue(self._h, start, count)
+
+    def fully_claimed(self) -> bool:
+        return bool(self._lib.ix_sample_cursor_fully_claimed(self._h))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.ix_sample_cursor_free(self._h)
+            self._h = None
+
+
+class Merger:
+    """Merger (merge/mod.rs:155): left fold of chunk sums in ascending first-sample
+    order; chunks ahead of the frontier are parked."""
+
+    def __init__(self, pixels: int, first_sample: int = 0, parked_budget_bytes: int = 0):
+        self._lib = _lib()
+        self.pixels = pixels
+        self._h = self._lib.ix_merger_new(pixels, first_sample, parked_budget_bytes)
+
+    def add(self, first_sample: int, done: int, sums: np.ndarray) -> int:
+        s = np.ascontiguousarray(sums, np.float64).reshape(-1)
+        total = C.c_uint32()
+        rc = self._lib.ix_merger_add(self._h, first_sample, done, s.ctypes.data_as(C.POINTER(C.c_double)),
+                                     s.size, C.byref(total))
+        if rc != MERGE_OK:
+            raise MergeError({MERGE_WRONG_LENGTH: "wrong length", MERGE_OVERLAP: "overlap",
+                              MERGE_BUDGET: "parked budget exceeded"}.get(rc, str(rc)))
+        return int(total.value)
+
+    @property
+    def frontier(self) -> int:
+        return int(self._lib.ix_merger_frontier(self._h))
+
+    @property
+    def total(self) -> int:
+        return int(self._lib.ix_merger_total(self._h))
+
+    @property
+    def dropped_pixels(self) -> int:
+        return int(self._lib.ix_merger_dropped_pixels(self._h))
+
+    def snapshot(self) -> Tuple[np.ndarray, int]:
+        dst = np.zeros(self.pixels * 3)
+        n = self._lib.ix_merger_snapshot(self._h, dst.ctypes.data_as(C.POINTER(C.c_double)), dst.size)
+        return dst, int(n)
+
+    def finish(self) -> Tuple[np.ndarray, int]:
+        dst = np.zeros(self.pixels * 3)
+        n = self._lib.ix_merger_finish(self._h, dst.ctypes.data_as(C.POINTER(C.c_double)), dst.size)
+        return dst, int(n)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.ix_merger_free(self._h)
+            self._h = None
+
+
+def store_claim(store, key: str, start: int, end: int, want: int) -> Optional[Tuple[int, int]]:
+    """A SampleCursor shared by every rank through a torch.distributed store: the store's
+    atomic add hands out disjoint ranges of `want` samples."""
+    hi = int(store.add(key, want))
+    lo = hi - want
+    s = start + lo
+    if s >= end:
+        return None
+    return s, min(want, end - s)
+
+
+def distributed_accumulate(trace: Callable[[int, int], np.ndarray], pixels: int, start: int, end: int,
+                           chunk: int, key: str = "ix_cursor") -> Optional[Tuple[np.ndarray, int]]:
+    """Every rank claims chunks of `chunk` samples from [start, end) through the process
+    group's store, traces each with ``trace(first_sample, count) -> sums``, and rank 0
+    merges all ranks' chunks in ascending first-sample order.  Returns (sums, samples)
+    on rank 0, None elsewhere.  Every rank takes the same collective steps."""
+    import torch.distributed as dist
+
+    store = dist.distributed_c10d._get_default_store()
+    mine: List[Tuple[int, int, np.ndarray]] = []
+    while True:
+        c = store_claim(store, key, start, end, chunk)
+        if c is None:
+            break
+        mine.append((c[0], c[1], np.ascontiguousarray(trace(c[0], c[1]), np.float64).reshape(-1)))
+    gathered: List = [None] * dist.get_world_size()
+    dist.all_gather_object(gathered, mine)
+    if dist.get_rank() != 0:
+        return None
+    m = Merger(pixels, start)
+    for chunks in gathered:
+        for first, done, sums in chunks:
+            m.add(first, done, sums)
+    return m.finish()

@@ -1,0 +1,155 @@
+"""Sample-range dispatch and deterministic merge (include/ix_dispatch.h) on the CPU,
+including a 2-rank gloo run of the multi-process path.
+
+Modelled on the reference's dispatch tests (crates/indicatrix-dispatch/src/merge,
+pool/tests/fake.rs): lanes produce deterministic per-pixel sums, and the merged result
+must not depend on which lane traced which chunk or in which order chunks arrive.
+"""
+import os
+import pickle
+import socket
+import tempfile
+
+import numpy as np
+import pytest
+
+from indicatrix_b200.dispatch import MergeError, Merger, SampleCursor
+
+
+def test_sample_cursor_hands_out_disjoint_ranges_and_requeues():
+    c = SampleCursor(10, 33)
+    got = []
+    while True:
+        r = c.claim(5)
+        if r is None:
+            break
+        got.append(r)
+    assert got == [(10, 5), (15, 5), (20, 5), (25, 5), (30, 3)]
+    assert c.fully_claimed()
+    c.requeue(20, 5)
+    assert not c.fully_claimed()
+    assert c.claim(3) == (20, 3) and c.claim(3) == (23, 2) and c.claim(3) is None
+
+
+def fake_chunk(pixels, first, done, salt=0):
+    """A lane's chunk sum: a deterministic function of (pixel, sample), small integers
+    plus a non-dyadic part so the fold order shows in the bits."""
+    s = np.arange(first, first + done, dtype=np.float64)
+    p = np.arange(pixels, dtype=np.float64)[:, None]
+    v = (p * 0.1 + s[None, :] * 0.3 + salt) % 7.0 + 0.013
+    return np.repeat(v.sum(axis=1)[:, None], 3, axis=1) * np.array([1.0, 1.1, 0.9])
+
+
+def test_merger_fold_is_order_independent_and_exact():
+    pixels = 37
+    chunks = [(0, 4), (4, 7), (11, 1), (12, 9), (21, 3)]
+    sums = {c: fake_chunk(pixels, *c) for c in chunks}
+    ref = Merger(pixels, 0)
+    for c in chunks:
+        ref.add(c[0], c[1], sums[c])
+    want, n = ref.finish()
+    assert n == 24
+    rng = np.random.default_rng(3)
+    for _ in range(6):
+        order = list(rng.permutation(len(chunks)))
+        m = Merger(pixels, 0)
+        for i in order:
+            m.add(chunks[i][0], chunks[i][1], sums[chunks[i]])
+        got, n2 = m.finish()
+        assert n2 == 24 and np.array_equal(got.view(np.uint64), want.view(np.uint64))
+    # the fold is ((0 + a) + b) + ... in sample order
+    fold = np.zeros((pixels, 3))
+    for c in chunks:
+        fold = fold + sums[c]
+    assert np.array_equal(want.reshape(pixels, 3), fold)
+
+
+def test_merger_rejects_overlaps_and_bad_lengths_and_drops_invalid_pixels():
+    m = Merger(4, 10)
+    m.add(12, 2, np.ones((4, 3)))
+    assert m.frontier == 10 and m.total == 2
+    with pytest.raises(MergeError):
+        m.add(13, 1, np.ones((4, 3)))
+    with pytest.raises(MergeError):
+        m.add(10, 1, np.ones((3, 3)))
+    bad = np.ones((4, 3))
+    bad[1, 2] = np.nan
+    bad[3, 0] = -1.0
+    m.add(10, 2, bad)
+    assert m.frontier == 14 and m.dropped_pixels == 2
+    snap, n = m.snapshot()
+    out, n2 = m.finish()
+    assert n == n2 == 4 and np.array_equal(snap, out)
+    assert out.reshape(4, 3)[1].tolist() == [1.0, 1.0, 1.0] and out.reshape(4, 3)[0].tolist() == [2.0] * 3
+
+
+def test_merger_parked_budget_refuses_instead_of_growing():
+    m = Merger(2, 0, parked_budget_bytes=2 * 3 * 8)  # room for one parked chunk
+    m.add(5, 1, np.ones((2, 3)))
+    with pytest.raises(MergeError):
+        m.add(7, 1, np.ones((2, 3)))
+    m.add(0, 5, np.ones((2, 3)))  # folds itself and the parked chunk
+    assert m.frontier == 6
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank_main(rank, world, port, out_path):
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    sys.path.insert(0, os.path.join(root, "oracle"))
+    import datetime
+
+    import torch.distributed as dist
+
+    import ix_oracle
+    from indicatrix_b200 import workloads
+    from indicatrix_b200.dispatch import distributed_accumulate
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    fs = workloads.round_brilliant_frame(8, 6)
+    sc = fs.to_abi()
+
+    def trace(first, count):  # a CPU lane: the oracle traces the chunk's samples
+        _, s64, _ = ix_oracle.trace_frame(sc, first, count, threads=1)
+        return s64
+
+    res = distributed_accumulate(trace, 48, 0, 23, 5)
+    if rank == 0:
+        with open(out_path, "wb") as f:
+            pickle.dump(res, f)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_gloo_sample_sharding_merges_deterministically(oracle):
+    """2 gloo ranks claim 5-sample chunks of [0, 23) through the store, trace them on the
+    CPU, and rank 0 folds every chunk in sample order: the result equals a single
+    process folding the same partition, bit for bit."""
+    import torch.multiprocessing as mp
+
+    from indicatrix_b200 import workloads
+
+    port = _free_port()
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "res.pkl")
+        mp.start_processes(_rank_main, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+        with open(out, "rb") as f:
+            sums, n = pickle.load(f)
+    assert n == 23
+    fs = workloads.round_brilliant_frame(8, 6)
+    sc = fs.to_abi()
+    want = np.zeros(48 * 3)
+    for first in range(0, 23, 5):
+        _, s64, _ = oracle.trace_frame(sc, first, min(5, 23 - first), threads=1)
+        want = want + s64.reshape(-1)
+    assert np.array_equal(sums.view(np.uint64), want.view(np.uint64))
