@@ -56,3 +56,50 @@ def isotropic(dispersion: abi.Dispersion, spline_alpha=None, path_scale: float =
             ab.spline[:] = [float(x) for x in knots]
     m.absorption_path_scale = float(path_scale)
     return m
+
+
+def energy_band(center_nm: float, fwhm_cm_inv: float, peak: float) -> abi.Band:
+    """AbsorptionBand::energy (optics/absorption.rs:95): a Gaussian in wavenumber whose
+    width field holds sigma = FWHM / 2.35482, rounded in f32."""
+    b = abi.Band()
+    b.center_nm = float(center_nm)
+    b.width_nm = float(np.float32(fwhm_cm_inv) / np.float32(2.35482))
+    b.peak = float(peak)
+    b.shape = abi.BAND_GAUSS_ENERGY
+    return b
+
+
+def _set_bands(ab: abi.Absorption, bands) -> None:
+    assert len(bands) <= abi.MAX_BANDS
+    ab.n_bands = len(bands)
+    for i, b in enumerate(bands):
+        ab.bands[i] = b
+
+
+def uniaxial(dispersion: abi.Dispersion, delta: float, c_axis=(0.0, 1.0, 0.0), o_bands=(), e_bands=(),
+             e_dispersion: abi.Dispersion | None = None) -> abi.Material:
+    """A uniaxial material (GemMaterial with crystal_system != Cubic and
+    |birefringence_delta| > 1e-4, transport/inner.rs:183): ordinary dispersion, the
+    constant-offset or separate extraordinary index, the optic axis as stored, and the
+    o-ray / e-ray absorption bands."""
+    m = _base(dispersion)
+    m.anisotropic = 1 if abs(float(np.float32(delta))) > 1e-4 else 0
+    m.birefringence_delta = float(delta)
+    m.c_axis[:] = [float(x) for x in c_axis]
+    if e_dispersion is not None:
+        m.has_e_dispersion = 1
+        m.e_dispersion = e_dispersion
+    _set_bands(m.abs_o, list(o_bands))
+    _set_bands(m.abs_e, list(e_bands))
+    return m
+
+
+def sapphire(c_axis=(0.0, 1.0, 0.0)) -> abi.Material:
+    """Sapphire (materials/diamond_through_emerald.rs:74-140): Malitson-o three-term
+    Sellmeier, birefringence -0.0081, optic axis +Y, Fe-Ti pleochroic o/e energy bands."""
+    return uniaxial(
+        sellmeier3([1.431349, 0.650547, 5.341402], [0.00528, 0.01424, 325.015]), -0.0081, c_axis,
+        o_bands=[energy_band(585.0, 4878.0, 2.01), energy_band(744.0, 3142.0, 0.887),
+                 energy_band(457.0, 12000.0, 0.433)],
+        e_bands=[energy_band(612.0, 7466.0, 0.371), energy_band(729.0, 4955.0, 1.03),
+                 energy_band(467.0, 11169.0, 0.524)])

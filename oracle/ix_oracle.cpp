@@ -740,15 +740,438 @@ static inline F r_unpol_of(F r_s, F r_p) { return F(0.5f) * fma_(r_p, r_p, r_s *
 static inline V3 reflect(V3 k, V3 n) { return k - F(2.0f) * dot(k, n) * n; }
 
 // ------------------------------------------------------------------------------------
-// One traced path (transport/inner/bounce_body.rs:216-764, isotropic material).
+// Uniaxial birefringence helpers (optics/birefringence/uniaxial.rs, helpers.rs,
+// absorption_tensor.rs; materials/optics.rs:42).
+// ------------------------------------------------------------------------------------
+static const uint32_t BIREFRINGENT_SPLIT_STREAM = 0x2545F491u;  // sampling.rs:17
+static const uint32_t MODE_COUPLING_STREAM = 0xCC9E2D51u;       // sampling.rs:21
+
+// extraordinary_index_at (materials/optics.rs:42).
+static F extraordinary_index_at(const ix_material& m, F lambda_nm, F n_o) {
+    if (m.has_e_dispersion) return dispersion_eval(m.e_dispersion, lambda_nm);
+    return n_o + F(m.birefringence_delta);
+}
+// stable_orthonormal_basis (birefringence/helpers.rs:13).
+static void stable_orthonormal_basis(V3 n, V3* t_out, V3* b_out) {
+    V3 a = (abs_(n.x) > F(0.9f)) ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
+    V3 t = normalize_or_zero(a - n * dot(n, a));
+    *t_out = t;
+    if (b_out) *b_out = cross(n, t);
+}
+// effective_extraordinary_index (birefringence/uniaxial.rs:33).
+static F effective_extraordinary_index(F n_o, F n_e, F theta) {
+    if (abs_(n_o - n_e) < F(1e-5f)) return n_o;
+    F sin_t = sin_(theta);
+    F cos_t = cos_(theta);
+    F ns = n_o * sin_t;
+    F denom_sq = fma_(n_e * cos_t, n_e * cos_t, ns * ns);
+    if (denom_sq <= F(1e-8f)) return n_o;
+    return (n_o * n_e) / sqrt_(denom_sq);
+}
+// walk_off_from_sin_cos (birefringence/uniaxial.rs:56).
+static F walk_off_from_sin_cos(F n_o, F n_e, F sin_t, F cos_t) {
+    if (abs_(n_o - n_e) < F(1e-5f)) return 0.0f;
+    F n_o2 = n_o * n_o;
+    F n_e2 = n_e * n_e;
+    F tan_rho = (((n_o2 - n_e2) * sin_t) * cos_t) /
+                max_(fma_(n_e2 * cos_t, cos_t, (n_o2 * sin_t) * sin_t), 1e-6f);
+    return atan_(tan_rho);
+}
+// extraordinary_poynting_dir (birefringence/uniaxial.rs:72).
+static V3 extraordinary_poynting_dir(V3 w, V3 c, F n_o, F n_e) {
+    F cos_theta = clamp_(dot(w, c), -1.0f, 1.0f);
+    F abs_cos = abs_(cos_theta);
+    F sin_t = sqrt_(max_((F(1.0f) - abs_cos) * (F(1.0f) + abs_cos), 0.0f));
+    F delta = walk_off_from_sin_cos(n_o, n_e, sin_t, abs_cos);
+    if (abs_(delta) < F(1e-5f)) return w;
+    V3 c_proj = normalize_or_zero(c - cos_theta * w);
+    if (length_squared(c_proj) < F(1e-6f)) return w;
+    F sign = (cos_theta >= F(0.0f)) ? F(1.0f) : F(-1.0f);
+    return normalize(w * cos_(delta) - (sign * c_proj) * sin_(delta));
+}
+// ordinary_eigen_polarization / extraordinary_eigen_polarization (uniaxial.rs:95-110).
+static V3 ordinary_eigen_polarization(V3 w, V3 c) {
+    V3 cr = cross(w, c);
+    if (length_squared(cr) > F(1e-8f)) return normalize(cr);
+    V3 t;
+    stable_orthonormal_basis(normalize_or_zero(w), &t, nullptr);
+    return t;
+}
+static V3 extraordinary_eigen_polarization(V3 w, V3 c) {
+    return normalize_or_zero(cross(w, ordinary_eigen_polarization(w, c)));
+}
+// assigned_mode_e_field_uniaxial (birefringence/absorption_tensor.rs:144).
+static V3 assigned_mode_e_field_uniaxial(V3 k, V3 c, bool is_e, F n_o_hero, F n_e_hero) {
+    if (!is_e) return ordinary_eigen_polarization(k, c);
+    V3 kc = cross(k, c);
+    if (length_squared(kc) < F(1e-8f)) return extraordinary_eigen_polarization(k, c);
+    V3 s = extraordinary_poynting_dir(k, c, n_o_hero, n_e_hero);
+    return normalize(cross(kc, s));
+}
+// AbsorptionTensor3::uniaxial(..).quadratic_form (absorption_tensor.rs:39, :80): the
+// tensor's local frame (a1, a2, c_hat) projected onto a unit field direction.
+struct TensorFrame {
+    V3 a1, a2, c;
+};
+static TensorFrame tensor_frame(V3 c_axis) {
+    TensorFrame f;
+    f.c = normalize_or_zero(c_axis);
+    stable_orthonormal_basis(f.c, &f.a1, &f.a2);
+    return f;
+}
+static F quadratic_form(const TensorFrame& f, F ao, F ae, V3 e) {
+    F l0 = dot(f.a1, e), l1 = dot(f.a2, e), l2 = dot(f.c, e);
+    return (ao * (l0 * l0) + ao * (l1 * l1)) + ae * (l2 * l2);
+}
+
+// ------------------------------------------------------------------------------------
+// Closed-form uniaxial interface solves (raytracer/uniaxial_fresnel/*.rs, after Lekner,
+// J. Phys.: Condens. Matter 3 (1991) 6121).
+// ------------------------------------------------------------------------------------
+struct Cx {
+    F re, im;
+};
+static inline Cx cx(F re, F im) { return Cx{re, im}; }
+static inline Cx cadd(Cx a, Cx b) { return cx(a.re + b.re, a.im + b.im); }
+static inline Cx csub(Cx a, Cx b) { return cx(a.re - b.re, a.im - b.im); }
+static inline Cx cmul(Cx a, Cx b) { return cx(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+static inline Cx cscale(Cx a, F s) { return cx(a.re * s, a.im * s); }
+static inline Cx cconj(Cx a) { return cx(a.re, -a.im); }
+static inline Cx cneg(Cx a) { return csub(cx(0.0f, 0.0f), a); }  // Cplx::ZERO.sub(a)
+static inline F cnorm2(Cx a) { return fma_(a.im, a.im, a.re * a.re); }
+// Cplx::div (complex.rs:79).
+static inline Cx cdiv(Cx a, Cx o) {
+    F denom = max_(fma_(o.im, o.im, o.re * o.re), 1e-20f);
+    return cx(fma_(a.im, o.im, a.re * o.re) / denom, fma_(a.re, -o.im, a.im * o.re) / denom);
+}
+// Cplx::sqrt_forward_branch (complex.rs:109).
+static Cx csqrt_fwd(Cx a) {
+    if (raw(a.im) == 0.0f && a.re < F(0.0f)) return cx(0.0f, sqrt_(-a.re));
+    F r = sqrt_(sqrt_(cnorm2(a)));
+    F theta = atan2_(a.im, a.re) * F(0.5f);
+    Cx out = cx(r * cos_(theta), r * sin_(theta));
+    if (out.re < F(0.0f)) out = cx(-out.re, -out.im);
+    if (abs_(out.re) < F(1e-9f) && out.im < F(0.0f)) out = cx(-out.re, -out.im);
+    return out;
+}
+struct CV3 {
+    V3 re, im;
+};
+static inline CV3 cv_real(V3 v) { return CV3{v, v3(0.0f, 0.0f, 0.0f)}; }
+static inline CV3 cv_wavevector(V3 that, V3 zhat, F tangential, Cx q) {
+    return CV3{that * tangential + zhat * q.re, zhat * q.im};
+}
+static inline CV3 cv_add(CV3 a, CV3 b) { return CV3{a.re + b.re, a.im + b.im}; }
+static inline CV3 cv_scale_real(CV3 a, F s) { return CV3{a.re * s, a.im * s}; }
+static inline CV3 cv_scale(CV3 a, Cx s) {
+    return CV3{a.re * s.re - a.im * s.im, a.re * s.im + a.im * s.re};
+}
+static inline CV3 cv_cross_real(CV3 a, V3 r) { return CV3{cross(a.re, r), cross(a.im, r)}; }
+static inline CV3 cv_cross(CV3 a, CV3 b) {
+    return CV3{cross(a.re, b.re) - cross(a.im, b.im), cross(a.re, b.im) + cross(a.im, b.re)};
+}
+static inline Cx cv_dot_real(CV3 a, V3 r) { return cx(dot(a.re, r), dot(a.im, r)); }
+static inline CV3 cv_conj(CV3 a) { return CV3{a.re, -a.im}; }
+
+// UniaxialFrame::build (uniaxial_fresnel/frame.rs:55).
+struct UFrame {
+    V3 that, zhat, s_axis;
+    F cos_i, sin_i, alpha, beta, gamma;
+};
+static UFrame uframe_build(V3 k, V3 normal, V3 c, F cos_i, F sin_i) {
+    UFrame f;
+    f.zhat = -normal;
+    if (sin_i > F(1e-5f)) {
+        V3 t = k + normal * cos_i;
+        f.that = normalize_or_zero(v3(t.x / sin_i, t.y / sin_i, t.z / sin_i));
+    } else {
+        V3 fb = (abs_(f.zhat.x) < F(0.9f)) ? v3(1.0f, 0.0f, 0.0f) : v3(0.0f, 1.0f, 0.0f);
+        f.that = normalize_or_zero(fb - f.zhat * dot(f.zhat, fb));
+    }
+    V3 s = normalize_or_zero(cross(k, normal));
+    f.s_axis = (length_squared(s) > F(1e-8f)) ? s : normalize_or_zero(cross(f.zhat, f.that));
+    f.cos_i = cos_i;
+    f.sin_i = sin_i;
+    f.alpha = dot(c, f.that);
+    f.beta = dot(c, f.s_axis);
+    f.gamma = dot(c, f.zhat);
+    return f;
+}
+// uniaxial_q_roots (frame.rs:111).
+struct QRoots {
+    Cx qo_plus, qo_minus, qe_plus, qe_minus;
+};
+static QRoots uniaxial_q_roots(F n_o, F n_e, const UFrame& f, F tangential) {
+    QRoots r;
+    F n_o2 = n_o * n_o;
+    F k2 = tangential * tangential;
+    r.qo_plus = csqrt_fwd(cx(n_o2 - k2, 0.0f));
+    r.qo_minus = cneg(r.qo_plus);
+    if (raw(n_o) == raw(n_e)) {
+        r.qe_plus = r.qo_plus;
+        r.qe_minus = r.qo_minus;
+        return r;
+    }
+    F n_e2 = n_e * n_e;
+    F deleps = n_e2 - n_o2;
+    F denom = fma_(f.gamma * f.gamma, deleps, n_o2);
+    F d_val = n_o2 * fma_(fma_(f.beta * f.beta, -deleps, n_e2), -k2,
+                          n_e2 * fma_(f.gamma * f.gamma, deleps, n_o2));
+    Cx sqrt_d = csqrt_fwd(cx(d_val, 0.0f));
+    Cx shift = cx(((f.alpha * f.gamma) * tangential) * deleps, 0.0f);
+    Cx denom_c = cx(max_(denom, 1e-12f), 0.0f);
+    r.qe_plus = cdiv(csub(sqrt_d, shift), denom_c);
+    r.qe_minus = cdiv(csub(cneg(sqrt_d), shift), denom_c);
+    return r;
+}
+// ModeFields (frame.rs:176-232): E and H of one eigenmode at amplitude 1.
+struct Mode {
+    CV3 e, h;
+};
+static Mode ordinary_mode(F n_o, V3 c, const UFrame& f, F tangential, Cx q) {
+    CV3 k = cv_wavevector(f.that, f.zhat, tangential, q);
+    CV3 d_o = cv_cross_real(k, c);
+    Mode m;
+    m.e = cv_scale_real(d_o, F(1.0f) / (n_o * n_o));
+    m.h = cv_cross(k, m.e);
+    return m;
+}
+static Mode extraordinary_mode(F n_o, F n_e, V3 c, const UFrame& f, F tangential, Cx q) {
+    F n_o2 = n_o * n_o;
+    F n_e2 = n_e * n_e;
+    F deleps = n_e2 - n_o2;
+    CV3 k = cv_wavevector(f.that, f.zhat, tangential, q);
+    CV3 d_o = cv_cross_real(k, c);
+    CV3 d_e = cv_cross(k, d_o);
+    Cx c_dot_de = cv_dot_real(d_e, c);
+    Mode m;
+    m.e = cv_add(cv_scale_real(d_e, F(1.0f) / n_o2),
+                 cv_scale(cv_real(c), cscale(c_dot_de, -(deleps / (n_o2 * n_e2)))));
+    m.h = cv_cross(k, m.e);
+    return m;
+}
+static Mode iso_mode(CV3 k, CV3 e) { return Mode{e, cv_cross(k, e)}; }
+// poynting_z (frame.rs:237) at amplitude 1.
+static F poynting_z(const Mode& m, V3 zhat) {
+    Cx one = cx(1.0f, 0.0f);
+    CV3 e = cv_scale(m.e, one);
+    CV3 h = cv_scale(m.h, one);
+    CV3 s = cv_cross(e, cv_conj(h));
+    return F(0.5f) * cv_dot_real(s, zhat).re;
+}
+// tangential_components (linalg.rs:264).
+static void tangential(const Mode& m, const UFrame& f, Cx out[4]) {
+    out[0] = cv_dot_real(m.e, f.that);
+    out[1] = cv_dot_real(m.e, f.s_axis);
+    out[2] = cv_dot_real(m.h, f.that);
+    out[3] = cv_dot_real(m.h, f.s_axis);
+}
+// solve4 / solve4_two_rhs (linalg.rs:172, :217): Gauss-Jordan with partial pivoting
+// (strictly larger |.|^2 wins), applied to nrhs right-hand sides in lockstep.
+static void solve4(Cx a[4][4], Cx* b[], int nrhs) {
+    for (int col = 0; col < 4; ++col) {
+        int piv = col;
+        F piv_mag = cnorm2(a[col][col]);
+        for (int row = col + 1; row < 4; ++row) {
+            F mag = cnorm2(a[row][col]);
+            if (mag > piv_mag) {
+                piv = row;
+                piv_mag = mag;
+            }
+        }
+        for (int j = 0; j < 4; ++j) std::swap(a[col][j], a[piv][j]);
+        for (int r = 0; r < nrhs; ++r) std::swap(b[r][col], b[r][piv]);
+        Cx pivot = a[col][col];
+        for (int j = col; j < 4; ++j) a[col][j] = cdiv(a[col][j], pivot);
+        for (int r = 0; r < nrhs; ++r) b[r][col] = cdiv(b[r][col], pivot);
+        for (int row = 0; row < 4; ++row) {
+            if (row == col) continue;
+            Cx factor = a[row][col];
+            if (raw(cnorm2(factor)) == 0.0f) continue;
+            for (int j = col; j < 4; ++j) a[row][j] = csub(a[row][j], cmul(factor, a[col][j]));
+            for (int r = 0; r < nrhs; ++r) b[r][row] = csub(b[r][row], cmul(factor, b[r][col]));
+        }
+    }
+}
+// EntryIncidenceFrame / entry_incidence_frame (entry.rs:95-147).
+struct EntryInc {
+    Cx inc_s[4], inc_p[4], refl_s[4], refl_p[4];
+};
+static EntryInc entry_incidence_frame(F n1, const UFrame& f) {
+    F k_tan = n1 * f.sin_i;
+    CV3 k_fwd = cv_wavevector(f.that, f.zhat, k_tan, cx(n1 * f.cos_i, 0.0f));
+    CV3 k_bwd = cv_wavevector(f.that, f.zhat, k_tan, cx(-n1 * f.cos_i, 0.0f));
+    CV3 s_c = cv_real(f.s_axis);
+    CV3 ep_bwd = cv_scale_real(cv_cross(k_bwd, s_c), F(-1.0f) / (n1 * n1));
+    CV3 ep_fwd = cv_scale_real(cv_cross(k_fwd, s_c), F(-1.0f) / (n1 * n1));
+    EntryInc e;
+    tangential(iso_mode(k_fwd, s_c), f, e.inc_s);
+    tangential(iso_mode(k_fwd, ep_fwd), f, e.inc_p);
+    tangential(iso_mode(k_bwd, s_c), f, e.refl_s);
+    tangential(iso_mode(k_bwd, ep_bwd), f, e.refl_p);
+    return e;
+}
+// EntryPolarizationSolution (entry.rs:23) for s and p incidence.
+struct EntrySol {
+    Cx r_s[2], r_p[2], t_o[2], t_e[2];  // [0] = s incidence, [1] = p incidence
+    F flux_o, flux_e;
+    V3 o_hat, e_hat;
+};
+// entry_solve_pair_with_incidence (entry.rs:173).
+static EntrySol entry_solve(const EntryInc& inc, F n1, F n_o, F n_e, V3 c, const UFrame& f) {
+    F k_tan = n1 * f.sin_i;
+    QRoots q = uniaxial_q_roots(n_o, n_e, f, k_tan);
+    Mode fo = ordinary_mode(n_o, c, f, k_tan, q.qo_plus);
+    Mode fe = extraordinary_mode(n_o, n_e, c, f, k_tan, q.qe_plus);
+    Cx oc[4], ec[4];
+    tangential(fo, f, oc);
+    tangential(fe, f, ec);
+    Cx a[4][4], bs[4], bp[4];
+    for (int i = 0; i < 4; ++i) {
+        a[i][0] = inc.refl_s[i];
+        a[i][1] = inc.refl_p[i];
+        a[i][2] = cneg(oc[i]);
+        a[i][3] = cneg(ec[i]);
+        bs[i] = cneg(inc.inc_s[i]);
+        bp[i] = cneg(inc.inc_p[i]);
+    }
+    Cx* rhs[2] = {bs, bp};
+    solve4(a, rhs, 2);
+    EntrySol s;
+    for (int p = 0; p < 2; ++p) {
+        s.r_s[p] = rhs[p][0];
+        s.r_p[p] = rhs[p][1];
+        s.t_o[p] = rhs[p][2];
+        s.t_e[p] = rhs[p][3];
+    }
+    s.flux_o = abs_(poynting_z(fo, f.zhat));
+    s.flux_e = abs_(poynting_z(fe, f.zhat));
+    s.o_hat = normalize_or_zero(fo.e.re);
+    s.e_hat = normalize_or_zero(fe.e.re);
+    return s;
+}
+// InternalPolarizationSolution / internal_solve (internal.rs:265, :334).
+struct IntSol {
+    Cx r_o, r_e, t_s, t_p;
+    F flux_ro, flux_re, flux_ts, flux_tp, flux_inc;
+};
+static IntSol internal_solve(F n_mode_inc, F n_o, F n_e, V3 c, const UFrame& f, bool inc_ordinary) {
+    F k_tan = n_mode_inc * f.sin_i;
+    QRoots q = uniaxial_q_roots(n_o, n_e, f, k_tan);
+    Mode f_inc = inc_ordinary ? ordinary_mode(n_o, c, f, k_tan, q.qo_plus)
+                              : extraordinary_mode(n_o, n_e, c, f, k_tan, q.qe_plus);
+    Mode f_o_bwd = ordinary_mode(n_o, c, f, k_tan, q.qo_minus);
+    Mode f_e_bwd = extraordinary_mode(n_o, n_e, c, f, k_tan, q.qe_minus);
+    const F n2 = 1.0f;
+    F zeta = k_tan / n2;
+    Cx cos_t = (abs_(zeta) <= F(1.0f)) ? cx(sqrt_(max_(fma_(zeta, -zeta, 1.0f), 0.0f)), 0.0f)
+                                       : cx(0.0f, sqrt_(fma_(zeta, zeta, -1.0f)));
+    CV3 k_iso = cv_wavevector(f.that, f.zhat, k_tan, cscale(cos_t, n2));
+    CV3 s_c = cv_real(f.s_axis);
+    CV3 ep_t = cv_scale_real(cv_cross(k_iso, s_c), F(-1.0f) / (n2 * n2));
+    Mode f_s_t = iso_mode(k_iso, s_c);
+    Mode f_p_t = iso_mode(k_iso, ep_t);
+    Cx inc_c[4], eo_c[4], ee_c[4], es_c[4], ep_c[4];
+    tangential(f_inc, f, inc_c);
+    tangential(f_o_bwd, f, eo_c);
+    tangential(f_e_bwd, f, ee_c);
+    tangential(f_s_t, f, es_c);
+    tangential(f_p_t, f, ep_c);
+    Cx a[4][4], b[4];
+    for (int i = 0; i < 4; ++i) {
+        a[i][0] = eo_c[i];
+        a[i][1] = ee_c[i];
+        a[i][2] = cneg(es_c[i]);
+        a[i][3] = cneg(ep_c[i]);
+        b[i] = cneg(inc_c[i]);
+    }
+    Cx* rhs[1] = {b};
+    solve4(a, rhs, 1);
+    IntSol s;
+    s.r_o = b[0];
+    s.r_e = b[1];
+    s.t_s = b[2];
+    s.t_p = b[3];
+    s.flux_ro = abs_(poynting_z(f_o_bwd, f.zhat));
+    s.flux_re = abs_(poynting_z(f_e_bwd, f.zhat));
+    s.flux_ts = abs_(poynting_z(f_s_t, f.zhat));
+    s.flux_tp = abs_(poynting_z(f_p_t, f.zhat));
+    s.flux_inc = abs_(poynting_z(f_inc, f.zhat));
+    return s;
+}
+// azimuth2_in_frame (mueller.rs:455).
+static void azimuth2_in_frame(V3 dir, V3 s_axis, V3 p_axis, F* cos2, F* sin2) {
+    F s = dot(dir, s_axis);
+    F p = dot(dir, p_axis);
+    F norm = max_(fma_(p, p, s * s), 1e-12f);
+    *cos2 = fma_(p, -p, s * s) / norm;
+    *sin2 = ((F(2.0f) * s) * p) / norm;
+}
+// jones_to_mueller (mueller.rs:478), column-major like glam's Mat4.
+static M4 jones_to_mueller(Cx j_ss, Cx j_sp, Cx j_ps, Cx j_pp) {
+    F m_ss = cnorm2(j_ss), m_sp = cnorm2(j_sp), m_ps = cnorm2(j_ps), m_pp = cnorm2(j_pp);
+    Cx a_ssp = cmul(j_ss, cconj(j_sp));
+    Cx a_pep = cmul(j_ps, cconj(j_pp));
+    Cx a_plus = cadd(a_ssp, a_pep);
+    Cx a_minus = csub(a_ssp, a_pep);
+    Cx b_sp = cmul(j_ss, cconj(j_ps));
+    Cx b_pp = cmul(j_sp, cconj(j_pp));
+    Cx c_sspp = cmul(j_ss, cconj(j_pp));
+    Cx c_spps = cmul(j_sp, cconj(j_ps));
+    F i_i = F(0.5f) * (((m_ss + m_ps) + m_sp) + m_pp);
+    F i_q = F(0.5f) * (((m_ss + m_ps) - m_sp) - m_pp);
+    F i_u = a_plus.re, i_v = a_plus.im;
+    F q_i = F(0.5f) * (((m_ss - m_ps) + m_sp) - m_pp);
+    F q_q = midpoint_((m_ss - m_ps) - m_sp, m_pp);
+    F q_u = a_minus.re, q_v = a_minus.im;
+    F u_i = b_sp.re + b_pp.re;
+    F u_q = b_sp.re - b_pp.re;
+    F u_u = c_sspp.re + c_spps.re;
+    F u_v = c_sspp.im - c_spps.im;
+    F v_i = -(b_sp.im + b_pp.im);
+    F v_q = -(b_sp.im) + b_pp.im;
+    F v_u = -(c_sspp.im + c_spps.im);
+    F v_v = c_sspp.re - c_spps.re;
+    return M4{{i_i, q_i, u_i, v_i, i_q, q_q, u_q, v_q, i_u, q_u, u_u, v_u, i_v, q_v, u_v, v_v}};
+}
+// mode_power (mueller.rs:541).
+static F mode_power(Cx t_s, Cx t_p, F mode_flux, F inc_flux, const Stokes& st) {
+    F m_s = cnorm2(t_s);
+    F m_p = cnorm2(t_p);
+    Cx cr = cmul(t_s, cconj(t_p));
+    F rawv = fma_(cr.im, st.v, fma_(cr.re, st.u, F(0.5f) * fma_(m_s, st.i + st.q, m_p * (st.i - st.q))));
+    return (mode_flux / max_(inc_flux, 1e-12f)) * rawv;
+}
+// entry_eigenmode_selection (refraction/uniaxial_entry.rs:50): returns false for None.
+static bool entry_eigenmode_selection(V3 c, V3 cpn, V3 k, const Stokes& hs, F* p_o, F* cos2,
+                                      F* sin2) {
+    if (hs.i <= F(1e-7f) || length_squared(cpn) <= F(1e-6f)) return false;
+    if (fma_(hs.q, hs.q, hs.u * hs.u) <= F(1e-12f)) return false;
+    V3 o_hat = ordinary_eigen_polarization(k, c);
+    V3 p_hat = cross(k, cpn);
+    F s_comp = dot(o_hat, cpn);
+    F p_comp = dot(o_hat, p_hat);
+    *cos2 = fma_(s_comp, s_comp, -(p_comp * p_comp));
+    *sin2 = (F(2.0f) * s_comp) * p_comp;
+    *p_o = clamp_(F(0.5f) + (F(0.5f) * fma_(hs.q, *cos2, hs.u * *sin2)) / hs.i, 0.0f, 1.0f);
+    return true;
+}
+
+// ------------------------------------------------------------------------------------
+// One traced path (transport/inner/bounce_body.rs:216-764).
 // ------------------------------------------------------------------------------------
 struct Path {
     const ix_scene* sc;
     uint32_t seed;
     F lambdas[8];
-    F n_ch[8];
+    F n_ch[8];     // ordinary (or isotropic) index per channel
+    F n_e_at[8];   // extraordinary_index_at per channel (uniaxial only)
     F alpha_ch_o[8];
+    F alpha_ch_e[8];
     bool absorbing;
+    bool aniso;
+    bool is_e;  // the eigenmode assigned at the last entry (or by internal coupling)
+    V3 c_axis;  // the material's optic axis as stored (RayMaterialContext::c_axis)
     Stokes stokes[8];
     F radiance[8];
     F path_pdf[8];
@@ -774,20 +1197,184 @@ static void try_split_exit_channel(Path& P, V3 hit_point, int k, V3 dir_k, F tra
     P.splits++;
 }
 
-// apply_refract_bounce + apply_refract_channel (refraction/reflect_refract.rs:121-591) for
-// an isotropic medium.  Returns the new direction.
-static V3 apply_refract_bounce(Path& P, F r_unpol, F cos_i, F n1, F n2, const F n1_ch[8],
-                               const F n2_ch[8], V3 k_hat, V3 normal, V3 hit_point) {
-    F eta_dir = n1 / n2;
-    F sin2_t_dir = min_(eta_dir * eta_dir * fma_(cos_i, -cos_i, 1.0f), 1.0f);
-    F cos_t_dir = sqrt_(max_(F(1.0f) - sin2_t_dir, 0.0f));
-    V3 final_refr = normalize(eta_dir * k_hat + fma_(eta_dir, cos_i, -cos_t_dir) * normal);
+// narrow_compat (refraction/context.rs:219) with the hero at channel 0.
+static void narrow_compat(Path& P, const V3 dirs[8], const bool have_dir[8], const bool hero_match[8]) {
+    for (int a = 0; a < 8; ++a)
+        for (int b = a + 1; b < 8; ++b) {
+            bool m;
+            if (a == 0)
+                m = hero_match[b];
+            else if (have_dir[a] && have_dir[b])
+                m = dot(dirs[a], dirs[b]) >= DIRECTION_MATCH_COS_TOL;
+            else
+                m = true;
+            if (!m) {
+                P.compat[a] &= (uint8_t)~(1u << b);
+                P.compat[b] &= (uint8_t)~(1u << a);
+            }
+        }
+}
+
+// Snell-refracted wave normal at index ratio eta (reflect_refract.rs:192-197).
+static inline V3 snell_dir(F eta, F cos_i, V3 k, V3 normal) {
+    F sin2_t = min_(eta * eta * fma_(cos_i, -cos_i, 1.0f), 1.0f);
+    F cos_t = sqrt_(max_(F(1.0f) - sin2_t, 0.0f));
+    return normalize(eta * k + fma_(eta, cos_i, -cos_t) * normal);
+}
+
+// BounceRefractionGeometry (refraction/geometry.rs:24, :306) for an isotropic or a
+// uniaxial material.
+struct Geo {
+    F cos_i, sin_i;
+    F n_o_hero, n_e_hero;  // n_e_hero: the constant-offset form, used for walk-off only
+    F n1, n2, sin2_t;
+    F n1_ch[8], n2_ch[8], sin2_t_ch[8];
+    bool has_frame;
+    UFrame frame;
+};
+
+// theta_c_for_bounce (refraction/geometry.rs:75), uniaxial only.
+static F theta_c_for_bounce(const Path& P, V3 normal, V3 k, F cos_i) {
+    if (!P.inside) {
+        F n_o_seed = P.n_ch[0];
+        F n_e_seed = P.n_e_at[0];
+        F n_guess = n_o_seed;
+        F theta = 0.0f;
+        for (int it = 0; it < 2; ++it) {
+            F eta = F(1.0f) / n_guess;
+            F s2 = eta * eta * fma_(cos_i, -cos_i, 1.0f);
+            if (s2 > F(1.0f)) break;
+            F ct = sqrt_(max_(F(1.0f) - s2, 0.0f));
+            V3 w = normalize(eta * k + fma_(eta, cos_i, -ct) * normal);
+            theta = acos_(abs_(clamp_(dot(w, P.c_axis), -1.0f, 1.0f)));
+            n_guess = effective_extraordinary_index(n_o_seed, n_e_seed, theta);
+        }
+        return theta;
+    }
+    return acos_(abs_(clamp_(dot(k, P.c_axis), -1.0f, 1.0f)));
+}
+
+static Geo compute_geo(const Path& P, V3 normal) {
+    Geo g;
+    V3 k = P.k;
+    g.cos_i = clamp_(dot(-k, normal), 0.0f, 1.0f);
+    g.sin_i = sqrt_(max_(fma_(g.cos_i, -g.cos_i, 1.0f), 0.0f));
+    F n_eff[8];
+    if (P.aniso) {
+        F theta = theta_c_for_bounce(P, normal, k, g.cos_i);
+        for (int c = 0; c < 8; ++c) n_eff[c] = effective_extraordinary_index(P.n_ch[c], P.n_e_at[c], theta);
+    } else {
+        for (int c = 0; c < 8; ++c) n_eff[c] = P.n_ch[c];
+    }
+    g.n_o_hero = P.n_ch[0];
+    g.n_e_hero = g.n_o_hero + F(P.sc->material.birefringence_delta);
+    // n_medium_ch: the ordinary indices while inside in the ordinary mode, else n_eff.
+    const bool ordinary_medium = P.aniso && P.inside && !P.is_e;
+    F n_med[8];
+    for (int c = 0; c < 8; ++c) n_med[c] = ordinary_medium ? P.n_ch[c] : n_eff[c];
+    g.n1 = P.inside ? n_med[0] : F(1.0f);
+    g.n2 = P.inside ? F(1.0f) : n_med[0];
+    F eta = g.n1 / g.n2;
+    g.sin2_t = eta * eta * fma_(g.cos_i, -g.cos_i, 1.0f);
+    for (int c = 0; c < 8; ++c) {
+        g.n1_ch[c] = P.inside ? n_med[c] : F(1.0f);
+        g.n2_ch[c] = P.inside ? F(1.0f) : n_med[c];
+        F etak = g.n1_ch[c] / g.n2_ch[c];
+        g.sin2_t_ch[c] = etak * etak * fma_(g.cos_i, -g.cos_i, 1.0f);
+    }
+    g.has_frame = P.aniso;
+    if (P.aniso) g.frame = uframe_build(k, normal, P.c_axis, g.cos_i, g.sin_i);
+    return g;
+}
+
+// poynting_dir_for_mode (refraction/geometry.rs:440).
+static V3 poynting_dir_for_mode(const Path& P, const Geo& g, V3 k, bool inside, bool is_e) {
+    if (!inside || !P.aniso || !is_e) return k;
+    return extraordinary_poynting_dir(k, P.c_axis, g.n_o_hero, g.n_e_hero);
+}
+
+// What one bounce dispatch decides (transport/bounce.rs:108-160).
+struct Outcome {
+    V3 new_k, new_s;
+    bool new_inside;
+    int update;  // -1: is_extraordinary unchanged, else its new value
+    bool has_p_o;
+    F p_o;  // the closed-form R_o / (R_o + R_e) for internal mode coupling
+};
+
+// apply_tir_bounce (refraction/tir.rs:41-116).
+static void apply_tir_bounce(Path& P, const Geo& g, V3 k, V3 normal, Outcome* o) {
+    if (g.has_frame && length_squared(cross(k, P.c_axis)) > F(1e-6f)) {
+        for (int c = 0; c < 8; ++c) {
+            IntSol sol = internal_solve(g.n1_ch[c], P.n_ch[c], P.n_e_at[c], P.c_axis, g.frame, !P.is_e);
+            F flux_inc = max_(sol.flux_inc, 1e-12f);
+            F ro_pow = cnorm2(sol.r_o) * sol.flux_ro;
+            F re_pow = cnorm2(sol.r_e) * sol.flux_re;
+            F r_total = min_((ro_pow + re_pow) / flux_inc, 1.0f);
+            P.stokes[c] = scale(P.stokes[c], r_total);
+            if (g.sin2_t_ch[c] <= F(1.0f))
+                P.path_pdf[c] = P.path_pdf[c] * clamp_(r_total, R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+            if (c == 0) {
+                o->has_p_o = true;
+                o->p_o = ro_pow / max_(ro_pow + re_pow, 1e-12f);
+            }
+        }
+    } else {
+        for (int c = 0; c < 8; ++c) {
+            F n1k = g.n1_ch[c], n2k = g.n2_ch[c];
+            if (g.sin2_t_ch[c] > F(1.0f)) {
+                P.stokes[c] = apply(tir_retardation(tir_phase_delta(n1k, g.cos_i, g.sin_i)), P.stokes[c]);
+            } else {
+                F cos_t_k = sqrt_(max_(F(1.0f) - g.sin2_t_ch[c], 0.0f));
+                F r_s, r_p;
+                fresnel_rs_rp(n1k, n2k, g.cos_i, cos_t_k, &r_s, &r_p);
+                P.stokes[c] = apply(fresnel_reflection(r_s, r_p), P.stokes[c]);
+                P.path_pdf[c] =
+                    P.path_pdf[c] * clamp_(r_unpol_of(r_s, r_p), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+            }
+        }
+    }
+    o->new_k = reflect(k, normal);
+    o->new_s = poynting_dir_for_mode(P, g, o->new_k, P.inside, P.is_e);
+    o->new_inside = P.inside;
+}
+
+// apply_partial_reflect_bounce (refraction/reflect_refract.rs:33).
+static void apply_partial_reflect(Path& P, const Geo& g, F r_unpol) {
+    for (int c = 0; c < 8; ++c) {
+        F n1k = g.n1_ch[c], n2k = g.n2_ch[c];
+        M4 mm;
+        if (g.sin2_t_ch[c] > F(1.0f)) {
+            mm = tir_retardation(tir_phase_delta(n1k, g.cos_i, g.sin_i));
+        } else {
+            F cos_t_k = sqrt_(max_(F(1.0f) - g.sin2_t_ch[c], 0.0f));
+            F rs, rp;
+            fresnel_rs_rp(n1k, n2k, g.cos_i, cos_t_k, &rs, &rp);
+            P.path_pdf[c] = P.path_pdf[c] * clamp_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+            mm = fresnel_reflection(rs, rp);
+        }
+        P.stokes[c] = scale(apply(mm, P.stokes[c]), F(1.0f) / r_unpol);
+    }
+}
+
+// apply_refract_bounce + apply_refract_channel + compute_channel_transmission
+// (refraction/reflect_refract.rs:121-591, exit_split.rs:51): the scalar-Fresnel refract
+// branch of an isotropic material or of the degenerate uniaxial case.
+static void apply_refract_bounce(Path& P, const Geo& g, F r_unpol, V3 k, V3 normal, V3 hit_point,
+                                 bool use_e, bool has_az, F az_c, F az_s, Outcome* o) {
+    const bool entering = !P.inside && P.aniso;
+    const F cos_i = g.cos_i;
+    F n2_hero_dir = (entering && !use_e) ? g.n_o_hero : g.n2;
+    V3 refr = snell_dir(g.n1 / n2_hero_dir, cos_i, k, normal);
+    V3 final_refr = (entering && use_e) ? extraordinary_poynting_dir(refr, P.c_axis, g.n_o_hero, g.n_e_hero)
+                                        : refr;
     V3 dirs[8];
     bool have_dir[8];
     bool hero_match[8];
     for (int c = 0; c < 8; ++c) {
         Stokes original = P.stokes[c];
-        F n1k = n1_ch[c], n2k = n2_ch[c];
+        F n1k = g.n1_ch[c];
+        F n2k = (entering && !use_e) ? P.n_ch[c] : g.n2_ch[c];
         F ratio = n1k / n2k;
         F sin2_t_k = (ratio * ratio) * fma_(cos_i, -cos_i, 1.0f);
         if (sin2_t_k > F(1.0f)) {
@@ -799,14 +1386,21 @@ static V3 apply_refract_bounce(Path& P, F r_unpol, F cos_i, F n1, F n2, const F 
         }
         F cos_t_k = sqrt_(max_(F(1.0f) - sin2_t_k, 0.0f));
         F eta_k = n1k / n2k;
-        V3 refr_k = normalize(eta_k * k_hat + fma_(eta_k, cos_i, -cos_t_k) * normal);
-        bool matches = dot(refr_k, final_refr) >= DIRECTION_MATCH_COS_TOL;
-        // Transmission at this channel's own index (exit_split.rs:69 / reflect_refract.rs:362).
+        V3 refr_k = normalize(eta_k * k + fma_(eta_k, cos_i, -cos_t_k) * normal);
+        V3 final_k = (entering && use_e)
+                         ? extraordinary_poynting_dir(refr_k, P.c_axis, P.n_ch[c],
+                                                      P.n_ch[c] + F(P.sc->material.birefringence_delta))
+                         : refr_k;
+        bool matches = dot(final_k, final_refr) >= DIRECTION_MATCH_COS_TOL;
+        // Transmission at this channel's own index, projected onto the selected
+        // eigenmode at an anisotropic entry (reflect_refract.rs:362, exit_split.rs:69).
         F two_n1_cos = F(2.0f) * n1k * cos_i;
         F t_s = two_n1_cos / fma_(n2k, cos_t_k, n1k * cos_i);
         F t_p = two_n1_cos / fma_(n1k, cos_t_k, n2k * cos_i);
         M4 tm = fresnel_transmission(n1k, n2k, cos_i, cos_t_k, t_s, t_p);
-        Stokes transmitted = scale(apply(tm, original), F(1.0f) / (F(1.0f) - r_unpol));
+        Stokes incident = original;
+        if (entering && has_az) incident = Stokes{original.i, original.i * az_c, original.i * az_s, 0.0f};
+        Stokes transmitted = scale(apply(tm, incident), F(1.0f) / (F(1.0f) - r_unpol));
         F r_s, r_p;
         fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, &r_s, &r_p);
         F r_unpol_k = clamp_(r_unpol_of(r_s, r_p), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
@@ -818,66 +1412,232 @@ static V3 apply_refract_bounce(Path& P, F r_unpol, F cos_i, F n1, F n2, const F 
             F prefix = P.path_pdf[c];
             P.stokes[c] = scale(P.stokes[c], 0.0f);
             P.path_pdf[c] = prefix * (F(1.0f) - r_unpol_k);
-            bool is_exit = P.inside;
+            bool is_exit = P.inside && !entering;
             if (is_exit && intensity(original) > F(0.0f))
                 try_split_exit_channel(P, hit_point, c, refr_k, intensity(transmitted));
         }
-        dirs[c] = refr_k;
+        dirs[c] = final_k;
         have_dir[c] = true;
         hero_match[c] = matches;
     }
-    if (!P.inside) {
-        // narrow_compat (refraction/context.rs:219), hero = 0.
-        for (int a = 0; a < 8; ++a)
-            for (int b = a + 1; b < 8; ++b) {
-                bool m;
-                if (a == 0)
-                    m = hero_match[b];
-                else if (have_dir[a] && have_dir[b])
-                    m = dot(dirs[a], dirs[b]) >= DIRECTION_MATCH_COS_TOL;
-                else
-                    m = true;
-                if (!m) {
-                    P.compat[a] &= (uint8_t)~(1u << b);
-                    P.compat[b] &= (uint8_t)~(1u << a);
-                }
-            }
-    }
-    return final_refr;
+    if (!P.inside) narrow_compat(P, dirs, have_dir, hero_match);
+    o->new_k = refr;
+    o->new_s = final_refr;
+    o->new_inside = !P.inside;
+    o->update = entering ? (use_e ? 1 : 0) : -1;
 }
 
-// apply_absorption for an isotropic material (raytracer/absorption.rs:99, :197).
-static void apply_isotropic_absorption(Path& P, V3 k_hat, F path_len) {
-    const ix_material& m = P.sc->material;
-    V3 c_axis = normalize_or_zero(load3(m.c_axis));
-    // AbsorptionTensor3::uniaxial (birefringence/absorption_tensor.rs:39) basis.
-    V3 ax = (abs_(c_axis.x) > F(0.9f)) ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
-    V3 a1 = normalize_or_zero(ax - c_axis * dot(c_axis, ax));
-    V3 a2 = cross(c_axis, a1);
-    // Eigen polarisations (birefringence/uniaxial.rs:121-140).
-    V3 raw_c = load3(m.c_axis);
-    V3 cr = cross(k_hat, raw_c);
-    V3 ea;
-    if (length_squared(cr) > F(1e-8f)) {
-        ea = normalize(cr);
+// apply_partial_fresnel_bounce's scalar-Fresnel path (refraction/dispatch.rs:162-380):
+// mode selection at an anisotropic entry, the reflect/transmit draw, then the branch.
+static void apply_scalar_fresnel(Path& P, const Geo& g, V3 k, V3 normal, V3 cpn, V3 hit_point,
+                                 uint32_t bounce, Outcome* o) {
+    const bool entering = !P.inside && P.aniso;
+    // resolve_entry_mode_selection (dispatch.rs:162).
+    F p_o = 0.5f, cos2 = 0.0f, sin2 = 0.0f;
+    bool has_sel = entering && entry_eigenmode_selection(P.c_axis, cpn, k, P.stokes[0], &p_o, &cos2, &sin2);
+    if (!has_sel) p_o = 0.5f;
+    F msr = unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM);
+    bool use_e = entering ? (msr < F(1.0f) - p_o) : P.is_e;
+    F az_c = use_e ? -cos2 : cos2;
+    F az_s = use_e ? -sin2 : sin2;
+    // compute_entry_reflect_probability (dispatch.rs:230).
+    bool ord_sel = entering && !use_e;
+    F n2 = ord_sel ? g.n_o_hero : g.n2;
+    F sin2_t = g.sin2_t;
+    if (ord_sel) {
+        F eta = g.n1 / n2;
+        sin2_t = eta * eta * fma_(g.cos_i, -g.cos_i, 1.0f);
+    }
+    F cos_t = sqrt_(max_(F(1.0f) - sin2_t, 0.0f));
+    F r_s, r_p;
+    fresnel_rs_rp(g.n1, n2, g.cos_i, cos_t, &r_s, &r_p);
+    F r_unpol = clamp_(r_unpol_of(r_s, r_p), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
+    F rng = unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM);
+    if (rng < r_unpol) {
+        apply_partial_reflect(P, g, r_unpol);
+        o->new_k = reflect(k, normal);
+        o->new_s = poynting_dir_for_mode(P, g, o->new_k, P.inside, P.is_e);
+        o->new_inside = P.inside;
     } else {
-        V3 nk = normalize_or_zero(k_hat);
-        V3 ax2 = (abs_(nk.x) > F(0.9f)) ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
-        ea = normalize_or_zero(ax2 - nk * dot(nk, ax2));
+        apply_refract_bounce(P, g, r_unpol, k, normal, hit_point, use_e, has_sel, az_c, az_s, o);
     }
-    V3 eb = normalize_or_zero(cross(k_hat, ea));
-    F la0 = dot(a1, ea), la1 = dot(a2, ea), la2 = dot(c_axis, ea);
-    F lb0 = dot(a1, eb), lb1 = dot(a2, eb), lb2 = dot(c_axis, eb);
-    F scaled_len = path_len * F(m.absorption_path_scale);
+}
+
+// apply_uniaxial_entry_bounce (refraction/uniaxial_entry.rs:108-412).
+static void apply_uniaxial_entry(Path& P, const Geo& g, V3 k, V3 normal, uint32_t bounce, Outcome* o) {
+    const UFrame& f = g.frame;
+    const V3 c_axis = P.c_axis;
+    const F delta_n = F(P.sc->material.birefringence_delta);
+    EntryInc inc = entry_incidence_frame(1.0f, f);
+    EntrySol sh = entry_solve(inc, 1.0f, P.n_ch[0], P.n_e_at[0], c_axis, f);
+    M4 mh = jones_to_mueller(sh.r_s[0], sh.r_s[1], sh.r_p[0], sh.r_p[1]);
+    F r_branch = clamp_(mh.c[0], R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
+    F inc_flux = F(0.5f) * f.cos_i;
+    F p_o_raw = mode_power(sh.t_o[0], sh.t_o[1], sh.flux_o, inc_flux, P.stokes[0]);
+    F p_e_raw = mode_power(sh.t_e[0], sh.t_e[1], sh.flux_e, inc_flux, P.stokes[0]);
+    F p_o_hero = clamp_(p_o_raw / max_(p_o_raw + p_e_raw, 1e-12f), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
+    F msr = unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM);
+    bool use_e = msr < F(1.0f) - p_o_hero;
+    F p_frac = use_e ? F(1.0f) - p_o_hero : p_o_hero;
+    F n2_hero_dir = use_e ? g.n2 : g.n_o_hero;
+    V3 refr = snell_dir(g.n1 / n2_hero_dir, g.cos_i, k, normal);
+    V3 final_refr = use_e ? extraordinary_poynting_dir(refr, c_axis, g.n_o_hero, g.n_e_hero) : refr;
+    V3 p_axis_t = cross(refr, f.s_axis);
+    F rng = unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM);
+    if (rng < r_branch) {
+        for (int c = 0; c < 8; ++c) {
+            EntrySol s = entry_solve(inc, 1.0f, P.n_ch[c], P.n_e_at[c], c_axis, f);
+            M4 mk = jones_to_mueller(s.r_s[0], s.r_s[1], s.r_p[0], s.r_p[1]);
+            F r_unpol_k = clamp_(mk.c[0], R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+            P.stokes[c] = scale(apply(mk, P.stokes[c]), F(1.0f) / r_branch);
+            P.path_pdf[c] = P.path_pdf[c] * r_unpol_k;
+        }
+        o->new_k = o->new_s = reflect(k, normal);
+        o->new_inside = false;
+        return;
+    }
+    V3 dirs[8];
+    bool have_dir[8];
+    bool hero_match[8];
     for (int c = 0; c < 8; ++c) {
-        F ao = P.alpha_ch_o[c];
-        // quadratic_form: alpha.dot(local * local) with alpha = (ao, ao, ae), ae == ao.
-        F qa = (ao * (la0 * la0) + ao * (la1 * la1)) + ao * (la2 * la2);
-        F qb = (ao * (lb0 * lb0) + ao * (lb1 * lb1)) + ao * (lb2 * lb2);
-        F alpha = midpoint_(qa, qb);
-        F trans = exp_lane(-alpha * scaled_len);
-        P.stokes[c] = scale(P.stokes[c], trans);
+        F n_o_k = P.n_ch[c];
+        F n2k_dir = use_e ? g.n2_ch[c] : n_o_k;
+        F ratio = g.n1 / n2k_dir;
+        F sin2_t_k = (ratio * ratio) * fma_(g.cos_i, -g.cos_i, 1.0f);
+        if (sin2_t_k > F(1.0f)) {
+            P.stokes[c] = scale(P.stokes[c], 0.0f);
+            P.path_pdf[c] = 0.0f;
+            have_dir[c] = false;
+            hero_match[c] = false;
+            continue;
+        }
+        F cos_t_k = sqrt_(max_(F(1.0f) - sin2_t_k, 0.0f));
+        F eta_k = g.n1 / n2k_dir;
+        V3 refr_k = normalize(eta_k * k + fma_(eta_k, g.cos_i, -cos_t_k) * normal);
+        V3 final_k = use_e ? extraordinary_poynting_dir(refr_k, c_axis, n_o_k, n_o_k + delta_n) : refr_k;
+        dirs[c] = final_k;
+        have_dir[c] = true;
+        bool matches = dot(final_k, final_refr) >= DIRECTION_MATCH_COS_TOL;
+        hero_match[c] = matches;
+        EntrySol s = entry_solve(inc, 1.0f, n_o_k, P.n_e_at[c], c_axis, f);
+        M4 mk = jones_to_mueller(s.r_s[0], s.r_s[1], s.r_p[0], s.r_p[1]);
+        F t_unpol_k = clamp_(F(1.0f) - mk.c[0], R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+        if (!matches) {
+            P.stokes[c] = scale(P.stokes[c], 0.0f);
+            P.path_pdf[c] = P.path_pdf[c] * t_unpol_k;
+            continue;
+        }
+        Cx t_s_row = use_e ? s.t_e[0] : s.t_o[0];
+        Cx t_p_row = use_e ? s.t_e[1] : s.t_o[1];
+        F flux_k = use_e ? s.flux_e : s.flux_o;
+        V3 mode_dir = use_e ? s.e_hat : s.o_hat;
+        F deposit = mode_power(t_s_row, t_p_row, flux_k, inc_flux, P.stokes[c]) / p_frac;
+        F c2, s2;
+        azimuth2_in_frame(mode_dir, f.s_axis, p_axis_t, &c2, &s2);
+        P.stokes[c] = scale(Stokes{deposit, deposit * c2, deposit * s2, 0.0f}, F(1.0f) / (F(1.0f) - r_branch));
+        P.path_pdf[c] = P.path_pdf[c] * t_unpol_k;
     }
+    narrow_compat(P, dirs, have_dir, hero_match);
+    o->new_k = refr;
+    o->new_s = final_refr;
+    o->new_inside = true;
+    o->update = use_e ? 1 : 0;
+}
+
+// compute_uniaxial_exit_transmission (refraction/uniaxial_internal.rs:212).
+static Stokes uniaxial_exit_transmission(const IntSol& sol, F r_branch, F incident_i, F* i_unit_out) {
+    F flux_inc = max_(sol.flux_inc, 1e-12f);
+    Cx ts_n = cscale(sol.t_s, sqrt_(sol.flux_ts / flux_inc));
+    Cx tp_n = cscale(sol.t_p, sqrt_(sol.flux_tp / flux_inc));
+    F i_unit = cnorm2(ts_n) + cnorm2(tp_n);
+    F q_unit = cnorm2(ts_n) - cnorm2(tp_n);
+    Cx cr = cmul(ts_n, cconj(tp_n));
+    F u_unit = F(2.0f) * cr.re;
+    F v_unit = F(-2.0f) * cr.im;
+    *i_unit_out = i_unit;
+    return scale(Stokes{incident_i * i_unit, incident_i * q_unit, incident_i * u_unit, incident_i * v_unit},
+                 F(1.0f) / (F(1.0f) - r_branch));
+}
+
+// apply_uniaxial_internal_bounce (refraction/uniaxial_internal.rs:68-353).
+static void apply_uniaxial_internal(Path& P, const Geo& g, V3 k, V3 normal, V3 hit_point, uint32_t bounce,
+                                    Outcome* o) {
+    const UFrame& f = g.frame;
+    const bool inc_o = !P.is_e;
+    IntSol sh = internal_solve(g.n1_ch[0], P.n_ch[0], P.n_e_at[0], P.c_axis, f, inc_o);
+    F flux_inc_hero = max_(sh.flux_inc, 1e-12f);
+    F ro_pow = cnorm2(sh.r_o) * sh.flux_ro;
+    F re_pow = cnorm2(sh.r_e) * sh.flux_re;
+    F r_branch = clamp_((ro_pow + re_pow) / flux_inc_hero, R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
+    F p_o_exact = ro_pow / max_(ro_pow + re_pow, 1e-12f);
+    F rng = unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM);
+    if (rng < r_branch) {
+        for (int c = 0; c < 8; ++c) {
+            IntSol sol = (c == 0) ? sh : internal_solve(g.n1_ch[c], P.n_ch[c], P.n_e_at[c], P.c_axis, f, inc_o);
+            F flux_inc = max_(sol.flux_inc, 1e-12f);
+            F r_total_k = min_(fma_(cnorm2(sol.r_e), sol.flux_re, cnorm2(sol.r_o) * sol.flux_ro) / flux_inc, 1.0f);
+            P.stokes[c] = scale(P.stokes[c], r_total_k / r_branch);
+            P.path_pdf[c] = P.path_pdf[c] * clamp_(r_total_k, R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+        }
+        o->new_k = o->new_s = reflect(k, normal);
+        o->new_inside = true;
+        o->has_p_o = true;
+        o->p_o = p_o_exact;
+        return;
+    }
+    V3 hero_refr = snell_dir(g.n1 / g.n2, g.cos_i, k, normal);
+    for (int c = 0; c < 8; ++c) {
+        F original_i = P.stokes[c].i;
+        F n_inc_k = g.n1_ch[c];
+        F n2k = g.n2_ch[c];
+        F ratio = n_inc_k / n2k;
+        F sin2_t_k = (ratio * ratio) * fma_(g.cos_i, -g.cos_i, 1.0f);
+        if (sin2_t_k > F(1.0f)) {
+            P.stokes[c] = scale(P.stokes[c], 0.0f);
+            P.path_pdf[c] = 0.0f;
+            continue;
+        }
+        F cos_t_k = sqrt_(max_(F(1.0f) - sin2_t_k, 0.0f));
+        F eta_k = n_inc_k / n2k;
+        V3 refr_k = normalize(eta_k * k + fma_(eta_k, g.cos_i, -cos_t_k) * normal);
+        bool matches = dot(refr_k, hero_refr) >= DIRECTION_MATCH_COS_TOL;
+        IntSol sol = (c == 0) ? sh : internal_solve(n_inc_k, P.n_ch[c], P.n_e_at[c], P.c_axis, f, inc_o);
+        F i_unit;
+        Stokes transmitted = uniaxial_exit_transmission(sol, r_branch, original_i, &i_unit);
+        F t_unpol_k = clamp_(i_unit, R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+        if (!matches) {
+            F prefix = P.path_pdf[c];
+            P.stokes[c] = scale(P.stokes[c], 0.0f);
+            P.path_pdf[c] = prefix * t_unpol_k;
+            if (original_i > F(0.0f))
+                try_split_exit_channel(P, hit_point, c, refr_k, intensity(transmitted));
+            continue;
+        }
+        P.stokes[c] = transmitted;
+        P.path_pdf[c] = P.path_pdf[c] * t_unpol_k;
+    }
+    o->new_k = o->new_s = hero_refr;
+    o->new_inside = false;
+}
+
+// apply_absorption (raytracer/absorption.rs:99-197): the mean over the two eigenmodes
+// for an isotropic material, the assigned eigenmode's field for a uniaxial one.
+static void apply_absorption(Path& P, F path_len) {
+    const ix_material& m = P.sc->material;
+    TensorFrame tf = tensor_frame(P.c_axis);
+    F alpha[8];
+    if (!P.aniso) {
+        V3 ea = ordinary_eigen_polarization(P.k, P.c_axis);
+        V3 eb = normalize_or_zero(cross(P.k, ea));
+        for (int c = 0; c < 8; ++c)
+            alpha[c] = midpoint_(quadratic_form(tf, P.alpha_ch_o[c], P.alpha_ch_e[c], ea),
+                                 quadratic_form(tf, P.alpha_ch_o[c], P.alpha_ch_e[c], eb));
+    } else {
+        V3 e_mode = assigned_mode_e_field_uniaxial(P.k, P.c_axis, P.is_e, P.n_ch[0], P.n_e_at[0]);
+        for (int c = 0; c < 8; ++c) alpha[c] = quadratic_form(tf, P.alpha_ch_o[c], P.alpha_ch_e[c], e_mode);
+    }
+    F scaled_len = path_len * F(m.absorption_path_scale);
+    for (int c = 0; c < 8; ++c) P.stokes[c] = scale(P.stokes[c], exp_lane(-alpha[c] * scaled_len));
 }
 
 enum { TERM_ESCAPED = 0, TERM_RR = 1, TERM_CAP = 2 };
@@ -890,10 +1650,15 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
     P.splits = 0;
     hero_wavelengths(hero_rand, P.lambdas);
     const ix_material& m = sc->material;
-    P.absorbing = absorption_present(m.abs_o);
+    P.absorbing = absorption_present(m.abs_o) || absorption_present(m.abs_e);
+    P.aniso = m.anisotropic != 0;
+    P.is_e = false;
+    P.c_axis = load3(m.c_axis);
     for (int c = 0; c < 8; ++c) {
         P.n_ch[c] = dispersion_eval(m.dispersion, P.lambdas[c]);
+        P.n_e_at[c] = P.aniso ? extraordinary_index_at(m, P.lambdas[c], P.n_ch[c]) : P.n_ch[c];
         P.alpha_ch_o[c] = P.absorbing ? spectral_absorption(m.abs_o, P.lambdas[c]) : F(0.0f);
+        P.alpha_ch_e[c] = P.absorbing ? spectral_absorption(m.abs_e, P.lambdas[c]) : F(0.0f);
         P.stokes[c] = unpolarized(1.0f);
         P.radiance[c] = 0.0f;
         P.path_pdf[c] = 1.0f;
@@ -941,79 +1706,43 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
         // apply_interior_segment (transport/inner.rs:170).
         if (P.inside) {
             normal = -normal;
-            if (P.absorbing && m.scattering_sigma_s <= 0.0f)
-                apply_isotropic_absorption(P, P.k, hit.t);
+            if (P.absorbing && m.scattering_sigma_s <= 0.0f) apply_absorption(P, hit.t);
         }
-        // compute_bounce_refraction_geometry (refraction/geometry.rs:306), isotropic.
-        F cos_i = clamp_(dot(-P.k, normal), 0.0f, 1.0f);
-        F sin_i = sqrt_(max_(fma_(cos_i, -cos_i, 1.0f), 0.0f));
-        F n_hero = P.n_ch[0];
-        F n1 = P.inside ? n_hero : F(1.0f);
-        F n2 = P.inside ? F(1.0f) : n_hero;
-        F eta = n1 / n2;
-        F one_minus_c2 = fma_(cos_i, -cos_i, 1.0f);
-        F sin2_t = eta * eta * one_minus_c2;
-        F n1_ch[8], n2_ch[8], sin2_t_ch[8];
-        for (int c = 0; c < 8; ++c) {
-            n1_ch[c] = P.inside ? P.n_ch[c] : F(1.0f);
-            n2_ch[c] = P.inside ? F(1.0f) : P.n_ch[c];
-            F etak = n1_ch[c] / n2_ch[c];
-            sin2_t_ch[c] = etak * etak * fma_(cos_i, -cos_i, 1.0f);
-        }
-        // dispatch_bounce (transport/bounce.rs:108).
-        V3 new_dir;
-        bool new_inside = P.inside;
-        if (sin2_t > F(1.0f)) {
-            // apply_tir_bounce, isotropic arm (refraction/tir.rs:98-116).
-            for (int c = 0; c < 8; ++c) {
-                F n1k = n1_ch[c], n2k = n2_ch[c];
-                if (sin2_t_ch[c] > F(1.0f)) {
-                    P.stokes[c] = apply(tir_retardation(tir_phase_delta(n1k, cos_i, sin_i)), P.stokes[c]);
-                } else {
-                    F cos_t_k = sqrt_(max_(F(1.0f) - sin2_t_ch[c], 0.0f));
-                    F r_s, r_p;
-                    fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, &r_s, &r_p);
-                    P.stokes[c] = apply(fresnel_reflection(r_s, r_p), P.stokes[c]);
-                    P.path_pdf[c] = P.path_pdf[c] *
-                                    clamp_(r_unpol_of(r_s, r_p), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
-                }
-            }
-            new_dir = reflect(P.k, normal);
+        Geo g = compute_geo(P, normal);
+        // dispatch_bounce (transport/bounce.rs:108) + try_dispatch_uniaxial_bounce
+        // (refraction/dispatch.rs:67).
+        Outcome o;
+        o.update = -1;
+        o.has_p_o = false;
+        o.p_o = 0.0f;
+        if (g.sin2_t > F(1.0f)) {
+            apply_tir_bounce(P, g, P.k, normal, &o);
         } else {
-            // apply_partial_fresnel_bounce (refraction/dispatch.rs:307).
-            F cos_t = sqrt_(max_(F(1.0f) - sin2_t, 0.0f));
-            F r_s, r_p;
-            fresnel_rs_rp(n1, n2, cos_i, cos_t, &r_s, &r_p);
-            F r_unpol = clamp_(r_unpol_of(r_s, r_p), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
-            F rng = unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM);
-            if (rng < r_unpol) {
-                // apply_partial_reflect_bounce (reflect_refract.rs:33).
-                for (int c = 0; c < 8; ++c) {
-                    F n1k = n1_ch[c], n2k = n2_ch[c];
-                    M4 mm;
-                    if (sin2_t_ch[c] > F(1.0f)) {
-                        mm = tir_retardation(tir_phase_delta(n1k, cos_i, sin_i));
-                    } else {
-                        F cos_t_k = sqrt_(max_(F(1.0f) - sin2_t_ch[c], 0.0f));
-                        F rs, rp;
-                        fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, &rs, &rp);
-                        F r_unpol_k = clamp_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
-                        P.path_pdf[c] = P.path_pdf[c] * r_unpol_k;
-                        mm = fresnel_reflection(rs, rp);
-                    }
-                    P.stokes[c] = scale(apply(mm, P.stokes[c]), F(1.0f) / r_unpol);
-                }
-                new_dir = reflect(P.k, normal);
-            } else {
-                new_dir = apply_refract_bounce(P, r_unpol, cos_i, n1, n2, n1_ch, n2_ch, P.k,
-                                               normal, hit_point);
-                new_inside = !P.inside;
-            }
+            const bool nondegenerate = g.has_frame && length_squared(cross(P.k, P.c_axis)) > F(1e-6f);
+            if (!P.inside && P.aniso && nondegenerate)
+                apply_uniaxial_entry(P, g, P.k, normal, bounce, &o);
+            else if (P.inside && nondegenerate)
+                apply_uniaxial_internal(P, g, P.k, normal, hit_point, bounce, &o);
+            else
+                apply_scalar_fresnel(P, g, P.k, normal, cpn, hit_point, bounce, &o);
         }
-        P.ray.dir = new_dir;
-        P.ray.origin = hit_point + new_dir * F(1e-4f);
-        P.k = new_dir;
-        P.inside = new_inside;
+        const bool was_internal_reflection = P.inside && o.update < 0 && o.new_inside == P.inside;
+        P.ray.dir = o.new_s;
+        P.ray.origin = hit_point + o.new_s * F(1e-4f);
+        P.k = o.new_k;
+        P.inside = o.new_inside;
+        if (o.update >= 0) P.is_e = o.update != 0;
+        // maybe_apply_internal_mode_coupling (transport/bounce.rs:470).
+        if (P.aniso && was_internal_reflection) {
+            F p_o = 0.5f;
+            if (o.has_p_o) {
+                p_o = o.p_o;
+            } else {
+                F po, c2, s2;
+                if (entry_eigenmode_selection(P.c_axis, cpn, P.k, P.stokes[0], &po, &c2, &s2)) p_o = po;
+            }
+            P.is_e = unit_draw(P.seed, bounce, MODE_COUPLING_STREAM) >= p_o;
+        }
         // Surface glare (bounce_body.rs:691-697).
         if (bounce == 0 && !P.inside && glare < F(1.0f)) {
             for (int c = 0; c < 8; ++c) P.stokes[c] = scale(P.stokes[c], glare);
@@ -1067,7 +1796,7 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
 }
 
 static bool scene_supported(const ix_scene* sc) {
-    if (!sc || sc->material.anisotropic) return false;
+    if (!sc) return false;
     if (sc->n_planes > 0 && !sc->planes) return false;
     if (sc->material.scattering_sigma_s > 0.0f) return false;
     for (uint32_t i = 0; i < sc->n_finishes && sc->facet_finishes; ++i)

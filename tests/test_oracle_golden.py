@@ -67,6 +67,28 @@ def test_golden_diamond_trace_bits(oracle, case):
     assert tuple(bits(v) for v in xyz) == want
 
 
+# golden_regression.rs:47-135 -- the same four rays traced through Sapphire (uniaxial,
+# optic axis +Y).  Rows 1, 2 and 4 enter along the optic axis (the degenerate k || c case,
+# scalar-Fresnel entry, then closed-form internal solves); row 3 draws the extraordinary
+# mode at a closed-form entry and exits through a dispersive split.
+GOLDEN_SAPPHIRE = [(0x3B1B2CF1, 0x3ADEBEE5, 0x3C0B3654), (0x3DDCDDC6, 0x3D386677, 0x3F13264C),
+                   (0x3ACBDC76, 0x3A2C6F2F, 0x3BF35083), (0x3AA6A762, 0x3A1781A5, 0x3BD5BA42)]
+
+
+@pytest.mark.parametrize("idx", range(4), ids=[str(c[2]) for c in GOLDEN_DIAMOND])
+def test_golden_sapphire_trace_bits(oracle, idx):
+    """golden_regression.rs:35-170, the sapphire column: uniaxial entry (closed-form Lekner
+    solve and the degenerate scalar path), internal o/e-coupled reflection and exit,
+    walk-off, assigned-mode pleochroic absorption and mode coupling, bit for bit."""
+    case = GOLDEN_DIAMOND[idx]
+    o, d = golden_ray(case)
+    seed, preset, yaw, pitch = case[2], case[3], case[4], case[5]
+    sc, _planes = srb_scene(oracle, materials.sapphire(), preset, yaw, pitch)
+    hero = f32(np.float32(oracle.lib().ixo_hash_u32(seed)) / np.float32(4294967296.0))
+    xyz, info = oracle.trace_ray(sc, o, d, seed, hero)
+    assert tuple(bits(v) for v in xyz) == GOLDEN_SAPPHIRE[idx]
+
+
 def test_golden_studio_environment_bits(oracle):
     """golden_regression.rs:172-207: sample_studio_environment(RingLights, exposure 1,
     yaw 0.85, pitch 0.95) at 450/550/650 nm across four directions."""
