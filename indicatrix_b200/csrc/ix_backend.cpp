@@ -49,7 +49,8 @@ struct ix_backend {
     size_t check_cap = 0;
     int sm_count = 0;
     uint32_t variant = 0;
-    int bps_exact[3] = {1, 1, 1}, bps_fast[3] = {1, 1, 1};
+    // Resident CTAs per SM by [uniaxial instantiation][variant].
+    int bps_exact[2][3] = {{1, 1, 1}, {1, 1, 1}}, bps_fast[2][3] = {{1, 1, 1}, {1, 1, 1}};
     std::string label;
     // State.
     bool lost = false;
@@ -134,7 +135,7 @@ int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uin
     ix::TraceLaunch L;
     std::memset(&L, 0, sizeof(L));
     L.scene = sc;
-    L.absorbing = material_has_absorption(sc.material.abs_o) ? 1u : 0u;
+    L.flags = ix::scene_flags(sc.material);
     L.sample_offset = sample_offset;
     L.spp = spp;
     L.pixels_per_task = pixels_per_task(spp);
@@ -143,7 +144,8 @@ int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uin
     L.dropped = b->d_dropped;
     L.threads = (int)b->threads;
     L.variant = (int)b->variant;
-    L.blocks = b->sm_count * (exact ? b->bps_exact[b->variant] : b->bps_fast[b->variant]);
+    const int uni = ix::needs_uniaxial_kernel(L.flags) ? 1 : 0;
+    L.blocks = b->sm_count * (exact ? b->bps_exact[uni][b->variant] : b->bps_fast[uni][b->variant]);
     if (L.blocks <= 0) L.blocks = b->sm_count > 0 ? b->sm_count : 1;
     // Chunking: a TDR-safe first launch of at most 1M paths (gpu/frame/mod.rs:355-361),
     // then launches of `chunk_paths` (default 64M paths), whole pixels each.
@@ -338,10 +340,11 @@ ix_backend* ix_backend_create(const ix_backend_options* opts) {
     }
     b->sm_count = prop.multiProcessorCount;
     b->label = prop.name;
-    for (int v = 0; v < 3; ++v) {
-        b->bps_exact[v] = std::max(1, ix::trace_blocks_per_sm_exact((int)b->threads, v, nullptr));
-        b->bps_fast[v] = std::max(1, ix::trace_blocks_per_sm_fast((int)b->threads, v, nullptr));
-    }
+    for (int u = 0; u < 2; ++u)
+        for (int v = 0; v < 3; ++v) {
+            b->bps_exact[u][v] = std::max(1, ix::trace_blocks_per_sm_exact((int)b->threads, v, u, nullptr));
+            b->bps_fast[u][v] = std::max(1, ix::trace_blocks_per_sm_fast((int)b->threads, v, u, nullptr));
+        }
     // Option 0 = the measured default (8 CTAs per SM); 1/2/3 = unconstrained / 6 / 8.
     b->variant = 2;
     if (opts && opts->kernel_variant >= 1 && opts->kernel_variant <= 3) b->variant = opts->kernel_variant - 1;
@@ -388,7 +391,8 @@ int ix_scene_routes_to_gpu(const ix_scene* s) {
     if (s->n_planes > IX_MAX_PLANES || (s->n_planes && !s->planes)) return 0;
     if (s->width == 0 || s->height == 0) return 0;
     const ix_material& m = s->material;
-    if (m.anisotropic || m.scattering_sigma_s > 0.0f || m.edge_rounding_radius > 0.0f) return 0;
+    if (m.scattering_sigma_s > 0.0f || m.edge_rounding_radius > 0.0f) return 0;
+    if (m.has_e_dispersion && m.e_dispersion.kind > IX_DISP_CAUCHY) return 0;
     if (s->facet_finishes)
         for (uint32_t i = 0; i < s->n_finishes; ++i)
             if (s->facet_finishes[i] != 0) return 0;
@@ -418,7 +422,8 @@ struct ix_batch_plan {
     uint32_t n_scenes = 0, n_jobs = 0, total_tasks = 0;
     uint64_t out_doubles = 0, paths = 0;
     ix_scene* d_scenes = nullptr;
-    uint32_t* d_absorbing = nullptr;
+    uint32_t* d_flags = nullptr;
+    uint32_t uniaxial = 0;  // some scene needs the uniaxial transport instantiation
     ix::BatchJob* d_jobs = nullptr;
     float* d_planes = nullptr;
     double* d_out = nullptr;
@@ -452,7 +457,8 @@ cudaError_t plan_enqueue(ix_batch_plan* p, cudaStream_t st, uint32_t variant) {
     ix::BatchLaunch L;
     std::memset(&L, 0, sizeof(L));
     L.scenes = p->d_scenes;
-    L.absorbing = p->d_absorbing;
+    L.flags = p->d_flags;
+    L.uniaxial = p->uniaxial;
     L.jobs = p->d_jobs;
     L.n_jobs = p->n_jobs;
     L.total_tasks = p->total_tasks;
@@ -462,8 +468,8 @@ cudaError_t plan_enqueue(ix_batch_plan* p, cudaStream_t st, uint32_t variant) {
     L.dropped = p->d_dropped;
     L.threads = 128;
     L.variant = (int)variant;
-    int bps = exact ? ix::batch_blocks_per_sm_exact(128, (int)variant)
-                    : ix::batch_blocks_per_sm_fast(128, (int)variant);
+    int bps = exact ? ix::batch_blocks_per_sm_exact(128, (int)variant, (int)p->uniaxial)
+                    : ix::batch_blocks_per_sm_fast(128, (int)variant, (int)p->uniaxial);
     L.blocks = b->sm_count * std::max(1, bps);
     return exact ? ix::launch_batch_exact(L, st) : ix::launch_batch_fast(L, st);
 }
@@ -516,7 +522,7 @@ ix_batch_plan* ix_batch_plan_create(ix_backend* b, const ix_scene* scenes, uint3
     uint64_t plane_floats = 0;
     for (uint32_t i = 0; i < n_scenes; ++i) plane_floats += (uint64_t)scenes[i].n_planes * 4;
     std::vector<ix_scene> dev_scenes(scenes, scenes + n_scenes);
-    std::vector<uint32_t> absorbing(n_scenes);
+    std::vector<uint32_t> flags(n_scenes);
     std::vector<float> planes(std::max<uint64_t>(plane_floats, 4));
     uint64_t off = 0;
     bool ok = cudaMalloc((void**)&p->d_planes, planes.size() * sizeof(float)) == cudaSuccess;
@@ -525,18 +531,19 @@ ix_batch_plan* ix_batch_plan_create(ix_backend* b, const ix_scene* scenes, uint3
         dev_scenes[i].planes = p->d_planes + off;
         dev_scenes[i].facet_finishes = nullptr;
         dev_scenes[i].n_finishes = 0;
-        absorbing[i] = material_has_absorption(scenes[i].material.abs_o) ? 1u : 0u;
+        flags[i] = ix::scene_flags(scenes[i].material);
+        if (ix::needs_uniaxial_kernel(flags[i])) p->uniaxial = 1;
         off += (uint64_t)scenes[i].n_planes * 4;
     }
     ok = ok && cudaMalloc((void**)&p->d_scenes, n_scenes * sizeof(ix_scene)) == cudaSuccess &&
-         cudaMalloc((void**)&p->d_absorbing, n_scenes * sizeof(uint32_t)) == cudaSuccess &&
+         cudaMalloc((void**)&p->d_flags, n_scenes * sizeof(uint32_t)) == cudaSuccess &&
          cudaMalloc((void**)&p->d_jobs, n_jobs * sizeof(ix::BatchJob)) == cudaSuccess &&
          cudaMalloc((void**)&p->d_out, std::max<uint64_t>(out, 1) * sizeof(double)) == cudaSuccess &&
          cudaMalloc((void**)&p->d_counter, sizeof(uint32_t)) == cudaSuccess &&
          cudaMalloc((void**)&p->d_dropped, sizeof(unsigned long long)) == cudaSuccess;
     ok = ok && cudaMemcpy(p->d_planes, planes.data(), planes.size() * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(p->d_scenes, dev_scenes.data(), n_scenes * sizeof(ix_scene), cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(p->d_absorbing, absorbing.data(), n_scenes * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(p->d_flags, flags.data(), n_scenes * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(p->d_jobs, p->jobs.data(), n_jobs * sizeof(ix::BatchJob), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemset(p->d_dropped, 0, sizeof(unsigned long long)) == cudaSuccess;
     p->variant = b->variant;
@@ -624,7 +631,7 @@ void ix_batch_plan_destroy(ix_batch_plan* p) {
     cudaStreamSynchronize(p->b->stream);
     plan_free_graph(p);
     cudaFree(p->d_scenes);
-    cudaFree(p->d_absorbing);
+    cudaFree(p->d_flags);
     cudaFree(p->d_jobs);
     cudaFree(p->d_planes);
     cudaFree(p->d_out);
@@ -865,7 +872,7 @@ int ix_debug_check(ix_backend* b, const ix_scene* scene, int32_t fn, uint32_t n,
     L.scene = *scene;
     L.scene.planes = b->d_planes;
     L.scene.facet_finishes = nullptr;
-    L.absorbing = material_has_absorption(scene->material.abs_o) ? 1u : 0u;
+    L.flags = ix::scene_flags(scene->material);
     L.fn = fn;
     L.n = n;
     L.in_stride = in_stride;

@@ -35,10 +35,18 @@ constexpr int TRACE_MAX_PPT = 8;     // pixels per warp task held in the partial
 constexpr int GROUPS_PER_WARP = 4;   // paths in flight per warp (8 lanes each)
 constexpr int WARPS_PER_CTA = 4;     // 128 threads
 
+// Resident-CTA targets of the register variants 1 and 2.  The isotropic megakernel fits
+// 6 or 8 CTAs per SM; the uniaxial one carries the per-lane 4x4 complex solves (about
+// 200 registers unconstrained) and spills heavily below ~160, so its variants ask 3 or 4.
+constexpr int UNI_MINB_1 = 3;
+constexpr int UNI_MINB_2 = 4;
+
 typedef double PartSlot[TRACE_MAX_PPT][GROUPS_PER_WARP][3];
 
 // One warp task: pixels [pixel0, pixel0 + npix) x samples [sample_offset, +spp), written
 // to out[0 .. 3 npix).  Returns the number of non-finite samples this lane dropped.
+// UNI selects the transport instantiation (isotropic megakernel, or the uniaxial one).
+template <bool UNI>
 IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const float4* __restrict__ planes,
                                      uint32_t pixel0, uint32_t npix, uint32_t spp,
                                      uint32_t sample_offset, PartSlot& part, double* out, int accumulate) {
@@ -64,11 +72,11 @@ IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const fl
         // One setup site for the first path and every regenerated one keeps a single
         // copy of the setup code in the loop.
         if (fresh) {
-            group_init(g, P, S, pixel0 + cur_j, sample_offset + (q - cur_j * spp));
+            group_init<UNI>(g, P, S, pixel0 + cur_j, sample_offset + (q - cur_j * spp));
             fresh = false;
         }
         float esc = 0.0f;
-        const int r = (P.bounce >= max_bounces) ? (int)BOUNCE_KILLED : group_bounce(g, P, S, planes, esc);
+        const int r = (P.bounce >= max_bounces) ? (int)BOUNCE_KILLED : group_step<UNI>(g, P, S, planes, esc);
         if (r == BOUNCE_CONTINUE && P.bounce < max_bounces) continue;
         // The path finished (escaped, roulette, or reached the bounce cap).
         const V3 xyz = group_finish(g, P, S, r == BOUNCE_ESCAPED, esc);
@@ -123,14 +131,14 @@ IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const fl
 
 // Single scene: MINB is the resident CTAs per SM the register allocation must allow
 // (1 = unconstrained).
-template <int MINB>
+template <int MINB, bool UNI>
 __global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_constant__ TraceLaunch L) {
     __shared__ float4 s_planes[IX_MAX_PLANES];
     __shared__ PartSlot s_part[WARPS_PER_CTA];
     const float4* gplanes = reinterpret_cast<const float4*>(L.scene.planes);
     for (uint32_t i = threadIdx.x; i < L.scene.n_planes; i += blockDim.x) s_planes[i] = gplanes[i];
     __syncthreads();
-    const DevScene S{L.scene, L.absorbing};
+    const DevScene S = make_scene(L.scene, L.flags);
     const Group g = make_group();
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t ppt = L.pixels_per_task;
@@ -143,8 +151,8 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_c
         if (task >= n_tasks) break;
         const uint32_t local0 = task * ppt;
         const uint32_t npix = min(ppt, L.n_pixels - local0);
-        drops += trace_task(g, S, s_planes, L.pixel_begin + local0, npix, L.spp, L.sample_offset,
-                            s_part[threadIdx.x >> 5], L.out + (size_t)local0 * 3, L.accumulate);
+        drops += trace_task<UNI>(g, S, s_planes, L.pixel_begin + local0, npix, L.spp, L.sample_offset,
+                                 s_part[threadIdx.x >> 5], L.out + (size_t)local0 * 3, L.accumulate);
     }
     if (drops && L.dropped) atomicAdd(L.dropped, drops);
 }
@@ -152,7 +160,7 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_c
 // Many scenes in one persistent launch (BatchLaunch): the task space is the
 // concatenation of every job's tasks; a warp finds its job by binary search over the
 // jobs' first-task offsets and reloads its plane slot only when the job's scene changes.
-template <int MINB>
+template <int MINB, bool UNI>
 __global__ void __launch_bounds__(128, MINB) IX_SFX(batch_kernel)(const __grid_constant__ BatchLaunch L) {
     __shared__ float4 s_planes[WARPS_PER_CTA][IX_MAX_PLANES];
     __shared__ PartSlot s_part[WARPS_PER_CTA];
@@ -183,17 +191,18 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(batch_kernel)(const __grid_c
             __syncwarp();
             cached = job.scene;
         }
-        const DevScene S{sc, L.absorbing[job.scene]};
+        const DevScene S = make_scene(sc, L.flags[job.scene]);
         const uint32_t local0 = (task - job.task_begin) * job.ppt;
         const uint32_t npix = min(job.ppt, job.n_pixels - local0);
-        drops += trace_task(g, S, s_planes[warp], local0, npix, job.spp, job.sample_offset, s_part[warp],
-                            L.out + job.out_offset + (size_t)local0 * 3, L.accumulate);
+        drops += trace_task<UNI>(g, S, s_planes[warp], local0, npix, job.spp, job.sample_offset, s_part[warp],
+                                 L.out + job.out_offset + (size_t)local0 * 3, L.accumulate);
     }
     if (drops && L.dropped) atomicAdd(L.dropped, drops);
 }
 
 // Per-path checks: each 8-lane group traces one input row, exactly as the megakernel
 // traces a path.
+template <bool UNI>
 __global__ void __launch_bounds__(128) IX_SFX(check_trace_kernel)(const __grid_constant__ CheckLaunch L) {
     __shared__ float4 s_planes[IX_MAX_PLANES];
     const float4* gplanes = reinterpret_cast<const float4*>(L.scene.planes);
@@ -201,20 +210,20 @@ __global__ void __launch_bounds__(128) IX_SFX(check_trace_kernel)(const __grid_c
     __syncthreads();
     const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
     if (row >= L.n) return;  // whole groups leave together (rows are group-aligned)
-    const DevScene S{L.scene, L.absorbing};
+    const DevScene S = make_scene(L.scene, L.flags);
     const Group g = make_group();
     const uint32_t* in = L.in + (size_t)row * L.in_stride;
     uint32_t* out = L.out + (size_t)row * L.out_stride;
     LanePath P;
     if (L.fn == CHECK_TRACE) {
-        group_init(g, P, S, in[0], in[1]);
+        group_init<UNI>(g, P, S, in[0], in[1]);
     } else {
         Ray r{v3(__uint_as_float(in[0]), __uint_as_float(in[1]), __uint_as_float(in[2])),
               v3(__uint_as_float(in[3]), __uint_as_float(in[4]), __uint_as_float(in[5]))};
-        group_init_ray(g, P, S, r, in[6], __uint_as_float(in[7]));
+        group_init_ray<UNI>(g, P, S, r, in[6], __uint_as_float(in[7]));
     }
     uint32_t it = 0;
-    const V3 xyz = group_trace(g, P, S, s_planes, &it);
+    const V3 xyz = group_trace<UNI>(g, P, S, s_planes, &it);
     if (g.c == 0) {
         out[0] = __float_as_uint(xyz.x);
         out[1] = __float_as_uint(xyz.y);
@@ -231,7 +240,7 @@ __global__ void IX_SFX(check_kernel)(const __grid_constant__ CheckLaunch L) {
     __syncthreads();
     const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= L.n) return;
-    const DevScene S{L.scene, L.absorbing};
+    const DevScene S = make_scene(L.scene, L.flags);
     const uint32_t* in = L.in + (size_t)row * L.in_stride;
     uint32_t* out = L.out + (size_t)row * L.out_stride;
     auto inf = [&](int i) { return __uint_as_float(in[i]); };
@@ -317,10 +326,18 @@ cudaError_t IX_SFX(launch_trace)(const TraceLaunch& l, cudaStream_t stream) {
     if (l.scene.n_planes > IX_MAX_PLANES) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
-    switch (l.variant) {
-        case 1: IX_SFX(trace_kernel)<6><<<l.blocks, l.threads, 0, stream>>>(l); break;
-        case 2: IX_SFX(trace_kernel)<8><<<l.blocks, l.threads, 0, stream>>>(l); break;
-        default: IX_SFX(trace_kernel)<1><<<l.blocks, l.threads, 0, stream>>>(l); break;
+    if (needs_uniaxial_kernel(l.flags)) {
+        switch (l.variant) {
+            case 1: IX_SFX(trace_kernel)<UNI_MINB_1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
+            case 2: IX_SFX(trace_kernel)<UNI_MINB_2, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
+            default: IX_SFX(trace_kernel)<1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
+        }
+    } else {
+        switch (l.variant) {
+            case 1: IX_SFX(trace_kernel)<6, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
+            case 2: IX_SFX(trace_kernel)<8, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
+            default: IX_SFX(trace_kernel)<1, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
+        }
     }
     return cudaGetLastError();
 }
@@ -329,10 +346,18 @@ cudaError_t IX_SFX(launch_batch)(const BatchLaunch& l, cudaStream_t stream) {
     if (!launch_shape_ok(l.threads) || l.n_jobs == 0) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
-    switch (l.variant) {
-        case 1: IX_SFX(batch_kernel)<6><<<l.blocks, l.threads, 0, stream>>>(l); break;
-        case 2: IX_SFX(batch_kernel)<8><<<l.blocks, l.threads, 0, stream>>>(l); break;
-        default: IX_SFX(batch_kernel)<1><<<l.blocks, l.threads, 0, stream>>>(l); break;
+    if (l.uniaxial) {
+        switch (l.variant) {
+            case 1: IX_SFX(batch_kernel)<UNI_MINB_1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
+            case 2: IX_SFX(batch_kernel)<UNI_MINB_2, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
+            default: IX_SFX(batch_kernel)<1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
+        }
+    } else {
+        switch (l.variant) {
+            case 1: IX_SFX(batch_kernel)<6, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
+            case 2: IX_SFX(batch_kernel)<8, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
+            default: IX_SFX(batch_kernel)<1, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
+        }
     }
     return cudaGetLastError();
 }
@@ -343,7 +368,10 @@ cudaError_t IX_SFX(launch_check)(const CheckLaunch& l, cudaStream_t stream) {
     const int threads = 128;
     if (l.fn == CHECK_TRACE || l.fn == CHECK_TRACE_RAY) {
         const int blocks = (int)((l.n * 8ull + threads - 1) / threads);
-        IX_SFX(check_trace_kernel)<<<blocks, threads, 0, stream>>>(l);
+        if (needs_uniaxial_kernel(l.flags))
+            IX_SFX(check_trace_kernel)<true><<<blocks, threads, 0, stream>>>(l);
+        else
+            IX_SFX(check_trace_kernel)<false><<<blocks, threads, 0, stream>>>(l);
     } else {
         const int blocks = (int)((l.n + threads - 1) / threads);
         IX_SFX(check_kernel)<<<blocks, threads, 0, stream>>>(l);
@@ -358,17 +386,27 @@ static int occupancy(K kernel, int threads) {
     return blocks;
 }
 
-int IX_SFX(trace_blocks_per_sm)(int threads, int variant, size_t* smem_bytes) {
+int IX_SFX(trace_blocks_per_sm)(int threads, int variant, int uniaxial, size_t* smem_bytes) {
     if (smem_bytes) *smem_bytes = 0;
-    if (variant == 1) return occupancy(IX_SFX(trace_kernel)<6>, threads);
-    if (variant == 2) return occupancy(IX_SFX(trace_kernel)<8>, threads);
-    return occupancy(IX_SFX(trace_kernel)<1>, threads);
+    if (uniaxial) {
+        if (variant == 1) return occupancy(IX_SFX(trace_kernel)<UNI_MINB_1, true>, threads);
+        if (variant == 2) return occupancy(IX_SFX(trace_kernel)<UNI_MINB_2, true>, threads);
+        return occupancy(IX_SFX(trace_kernel)<1, true>, threads);
+    }
+    if (variant == 1) return occupancy(IX_SFX(trace_kernel)<6, false>, threads);
+    if (variant == 2) return occupancy(IX_SFX(trace_kernel)<8, false>, threads);
+    return occupancy(IX_SFX(trace_kernel)<1, false>, threads);
 }
 
-int IX_SFX(batch_blocks_per_sm)(int threads, int variant) {
-    if (variant == 1) return occupancy(IX_SFX(batch_kernel)<6>, threads);
-    if (variant == 2) return occupancy(IX_SFX(batch_kernel)<8>, threads);
-    return occupancy(IX_SFX(batch_kernel)<1>, threads);
+int IX_SFX(batch_blocks_per_sm)(int threads, int variant, int uniaxial) {
+    if (uniaxial) {
+        if (variant == 1) return occupancy(IX_SFX(batch_kernel)<UNI_MINB_1, true>, threads);
+        if (variant == 2) return occupancy(IX_SFX(batch_kernel)<UNI_MINB_2, true>, threads);
+        return occupancy(IX_SFX(batch_kernel)<1, true>, threads);
+    }
+    if (variant == 1) return occupancy(IX_SFX(batch_kernel)<6, false>, threads);
+    if (variant == 2) return occupancy(IX_SFX(batch_kernel)<8, false>, threads);
+    return occupancy(IX_SFX(batch_kernel)<1, false>, threads);
 }
 
 }  // namespace ix

@@ -10,10 +10,45 @@
 
 namespace ix {
 
+// Per-scene transport flags, resolved on the host from the material.
+enum : uint32_t {
+    SCENE_ABSORBING = 1u,   // the o-ray or e-ray absorption has a non-zero term
+    SCENE_UNIAXIAL = 2u,    // uniaxial birefringence (ix_material::anisotropic)
+    SCENE_PLEOCHROIC = 4u,  // the o-ray and e-ray absorption differ
+};
+inline bool absorption_present(const ix_absorption& a) {
+    if (a.has_spline) return true;
+    for (uint32_t i = 0; i < a.n_bands && i < IX_MAX_BANDS; ++i)
+        if (a.bands[i].peak != 0.0f) return true;
+    return false;
+}
+inline bool absorption_equal(const ix_absorption& a, const ix_absorption& b) {
+    if (a.n_bands != b.n_bands || a.has_spline != b.has_spline) return false;
+    for (uint32_t i = 0; i < a.n_bands && i < IX_MAX_BANDS; ++i) {
+        const ix_band &x = a.bands[i], &y = b.bands[i];
+        if (x.center_nm != y.center_nm || x.width_nm != y.width_nm || x.peak != y.peak || x.shape != y.shape)
+            return false;
+    }
+    if (a.has_spline)
+        for (int i = 0; i < IX_SPLINE_KNOTS; ++i)
+            if (a.spline[i] != b.spline[i]) return false;
+    return true;
+}
+inline uint32_t scene_flags(const ix_material& m) {
+    uint32_t f = 0;
+    if (absorption_present(m.abs_o) || absorption_present(m.abs_e)) f |= SCENE_ABSORBING;
+    if (m.anisotropic) f |= SCENE_UNIAXIAL;
+    if (!absorption_equal(m.abs_o, m.abs_e)) f |= SCENE_PLEOCHROIC;
+    return f;
+}
+// The isotropic megakernel assumes equal o/e absorption and no birefringence; any other
+// scene runs the uniaxial instantiation of the transport.
+inline bool needs_uniaxial_kernel(uint32_t flags) { return (flags & (SCENE_UNIAXIAL | SCENE_PLEOCHROIC)) != 0; }
+
 // One frame-tracing launch over the pixels [pixel_begin, pixel_begin + n_pixels).
 struct TraceLaunch {
     ix_scene scene;            // `planes` is a device pointer here
-    uint32_t absorbing;
+    uint32_t flags;            // scene_flags(scene.material)
     uint32_t pixel_begin;
     uint32_t n_pixels;
     uint32_t sample_offset;
@@ -43,7 +78,8 @@ struct BatchJob {
 
 struct BatchLaunch {
     const ix_scene* scenes;      // device array; each scene's `planes` is a device pointer
-    const uint32_t* absorbing;   // device, per scene
+    const uint32_t* flags;       // device, scene_flags per scene
+    uint32_t uniaxial;           // any scene needs the uniaxial transport
     const BatchJob* jobs;        // device, ascending task_begin
     uint32_t n_jobs;
     uint32_t total_tasks;
@@ -77,7 +113,7 @@ enum CheckFn {
 
 struct CheckLaunch {
     ix_scene scene;    // device planes
-    uint32_t absorbing;
+    uint32_t flags;    // scene_flags(scene.material)
     int fn;
     uint32_t n;
     uint32_t in_stride;   // 32-bit words per input row
@@ -90,13 +126,14 @@ cudaError_t launch_trace_exact(const TraceLaunch& l, cudaStream_t stream);
 cudaError_t launch_trace_fast(const TraceLaunch& l, cudaStream_t stream);
 cudaError_t launch_batch_exact(const BatchLaunch& l, cudaStream_t stream);
 cudaError_t launch_batch_fast(const BatchLaunch& l, cudaStream_t stream);
-int batch_blocks_per_sm_exact(int threads, int variant);
-int batch_blocks_per_sm_fast(int threads, int variant);
+int batch_blocks_per_sm_exact(int threads, int variant, int uniaxial);
+int batch_blocks_per_sm_fast(int threads, int variant, int uniaxial);
 cudaError_t launch_check_exact(const CheckLaunch& l, cudaStream_t stream);
 cudaError_t launch_check_fast(const CheckLaunch& l, cudaStream_t stream);
-// Occupancy-derived resident blocks per SM for the trace kernel at `threads` per block.
-int trace_blocks_per_sm_exact(int threads, int variant, size_t* smem_bytes);
-int trace_blocks_per_sm_fast(int threads, int variant, size_t* smem_bytes);
+// Occupancy-derived resident blocks per SM for the trace kernel at `threads` per block
+// (the uniaxial instantiation when `uniaxial` != 0).
+int trace_blocks_per_sm_exact(int threads, int variant, int uniaxial, size_t* smem_bytes);
+int trace_blocks_per_sm_fast(int threads, int variant, int uniaxial, size_t* smem_bytes);
 // FP32 FMA-pipe throughput probe (ix_probe.cu): best FLOP/s of `reps` timed runs.
 cudaError_t fp32_probe(int sm_count, int reps, cudaStream_t stream, double* flops);
 

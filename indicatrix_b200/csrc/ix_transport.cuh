@@ -16,6 +16,8 @@
 #pragma once
 
 #include "ix_device.cuh"
+#include "ix_launch.h"
+#include "ix_uniaxial.cuh"
 
 namespace ix {
 
@@ -30,7 +32,11 @@ constexpr float R_UNPOL_SELECT_MAX = 0.98f;              // refraction/mod.rs:15
 struct DevScene {
     const ix_scene& s;
     uint32_t absorbing;  // the material has any absorption term
+    uint32_t aniso;      // uniaxial birefringence
 };
+IX_DEV DevScene make_scene(const ix_scene& s, uint32_t flags) {
+    return DevScene{s, (flags & SCENE_ABSORBING) ? 1u : 0u, (flags & SCENE_UNIAXIAL) ? 1u : 0u};
+}
 
 // The 8 lanes of one path: `mask` selects them in the warp, `c` is this lane's channel.
 struct Group {
@@ -64,6 +70,12 @@ struct LanePath {
     float pdf;
     float split;
     uint32_t compat;  // MIS family of this channel (refraction/context.rs:219)
+    // Uniaxial transport only (the isotropic kernels never touch these).
+    V3 k;              // wave normal; the ray direction `d` is the Poynting direction
+    bool is_e;         // eigenmode assigned at the last entry or internal coupling
+    float n_e;         // extraordinary_index_at for channel c
+    float n_e_hero;    // channel 0's
+    float alpha_e;     // e-ray absorption of channel c
 };
 
 // ------------------------------------------------------------------------------------
@@ -139,6 +151,7 @@ static __device__ __noinline__ Hit probe_intersect(Group g, const float4* __rest
 // ------------------------------------------------------------------------------------
 // Path setup: PathState::new (bounce_body.rs:260-356).
 // ------------------------------------------------------------------------------------
+template <bool UNI>
 IX_DEV void group_init_ray(const Group& g, LanePath& P, const DevScene& S, Ray r, uint32_t seed,
                            float hero_rand) {
     const ix_scene& sc = S.s;
@@ -161,9 +174,17 @@ IX_DEV void group_init_ray(const Group& g, LanePath& P, const DevScene& S, Ray r
     P.inside = false;
     P.has_prev = false;
     P.prev_pn = v3(0.0f, 0.0f, 0.0f);
+    if constexpr (UNI) {
+        P.k = r.dir;
+        P.is_e = false;
+        P.n_e = S.aniso ? extraordinary_index_at(sc.material, P.lambda, P.n) : P.n;
+        P.n_e_hero = gshfl(g, P.n_e, 0);
+        P.alpha_e = S.absorbing ? spectral_absorption(sc.material.abs_e, P.lambda) : 0.0f;
+    }
 }
 
 // One (pixel, absolute sample) as renderer/cpu_frame.rs:45-70 traces it.
+template <bool UNI>
 IX_DEV void group_init(const Group& g, LanePath& P, const DevScene& S, uint32_t pixel,
                        uint32_t sample) {
     const ix_scene& sc = S.s;
@@ -171,7 +192,7 @@ IX_DEV void group_init(const Group& g, LanePath& P, const DevScene& S, uint32_t 
     uint32_t x = pixel % sc.width, y = pixel / sc.width;
     Ray r = generate_ray(sc.camera, (float)x, (float)y, (float)sc.width, (float)sc.height,
                          dr.jx, dr.jy);
-    group_init_ray(g, P, S, r, dr.seed, dr.hero);
+    group_init_ray<UNI>(g, P, S, r, dr.seed, dr.hero);
 }
 
 // ------------------------------------------------------------------------------------
@@ -228,6 +249,59 @@ static __device__ __noinline__ float lane_environment(const ix_environment& env,
 }
 
 enum BounceResult { BOUNCE_CONTINUE = 0, BOUNCE_ESCAPED = 1, BOUNCE_KILLED = 2 };
+
+// try_split_exit_channel (refraction/exit_split.rs:128): at an exit, each diverging live
+// channel probes its own refracted direction `dir_k`; the group scans each probe
+// together and the probing lane adds its transmitted intensity times the radiance found.
+IX_DEV void group_exit_probes(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes,
+                              V3 hit_point, bool want_probe, V3 dir_k, float t_intensity) {
+    unsigned probes = (__ballot_sync(g.mask, want_probe) >> (threadIdx.x & 24u)) & 0xFFu;
+    while (probes) {
+        const int j = __ffs(probes) - 1;
+        probes &= probes - 1;
+        const V3 dj = v3(gshfl(g, dir_k.x, j), gshfl(g, dir_k.y, j), gshfl(g, dir_k.z, j));
+        const Hit ph = probe_intersect(g, planes, (int)S.s.n_planes, hit_point + dj * 1e-4f, dj);
+        if (ph.facet < 0 && g.c == j) {
+            const float e = lane_environment(S.s.environment, dj, P.observer, P.lambda);
+            P.split = fmaf(fmaxf(t_intensity, 0.0f), e, P.split);
+        }
+    }
+}
+
+// narrow_compat (refraction/context.rs:219) with the hero at channel 0: channel pairs
+// whose directions differ leave each other's MIS family.  `status` is 0 for a channel
+// with no transmitted direction, 1 when its direction matches the hero's, 2 otherwise.
+IX_DEV void group_narrow_compat(const Group& g, LanePath& P, int status, V3 dir_k) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const float dx = gshfl(g, dir_k.x, j), dy = gshfl(g, dir_k.y, j), dz = gshfl(g, dir_k.z, j);
+        const int sj = gshfl(g, status, j);
+        if (j == g.c) continue;
+        bool m;
+        if (g.c == 0)
+            m = sj == 1;
+        else if (j == 0)
+            m = status == 1;
+        else if (status != 0 && sj != 0)
+            m = dot(dir_k, v3(dx, dy, dz)) >= DIRECTION_MATCH_COS_TOL;
+        else
+            m = true;
+        if (!m) P.compat &= ~(1u << j);
+    }
+}
+
+// The channel's scalar-Fresnel reflection (apply_tir_bounce's isotropic arm,
+// refraction/tir.rs:98-116, and apply_partial_reflect_bounce, reflect_refract.rs:33):
+// the TIR retarder past the channel's own critical angle, else the Fresnel reflection
+// with its reflectance folded into the channel pdf.
+IX_DEV Stokes lane_scalar_reflect(LanePath& P, float n1k, float n2k, float s2k, float cos_i, float sin_i) {
+    if (s2k > 1.0f) return tir_retard_apply(P.st, tir_phase_delta(n1k, cos_i, sin_i));
+    const float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
+    float rs, rp;
+    fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, rs, rp);
+    P.pdf = P.pdf * clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+    return fresnel_reflect_apply(P.st, rs, rp);
+}
 
 // One iteration of the bounce loop (bounce_body.rs:361-423 and facet_event :611-707).
 // On BOUNCE_ESCAPED `esc` is this channel's escape radiance already weighted by its
@@ -343,40 +417,9 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
             P.st = status == 1 ? transmitted : scale(original, 0.0f);
             t_intensity = intensity(transmitted);
         }
-        // try_split_exit_channel (refraction/exit_split.rs:128): at an exit, each diverging
-        // live channel probes its own direction; the group scans each probe together.
-        const bool want_probe = status == 2 && P.inside && intensity(original) > 0.0f;
-        unsigned probes = (__ballot_sync(g.mask, want_probe) >> (threadIdx.x & 24u)) & 0xFFu;
-        while (probes) {
-            const int j = __ffs(probes) - 1;
-            probes &= probes - 1;
-            const V3 dj = v3(gshfl(g, dir_k.x, j), gshfl(g, dir_k.y, j), gshfl(g, dir_k.z, j));
-            const Hit ph = probe_intersect(g, planes, n_planes, hit_point + dj * 1e-4f, dj);
-            if (ph.facet < 0 && g.c == j) {
-                const float e = lane_environment(sc.environment, dj, P.observer, P.lambda);
-                P.split = fmaf(fmaxf(t_intensity, 0.0f), e, P.split);
-            }
-        }
-        if (!P.inside) {
-            // narrow_compat (refraction/context.rs:219), hero channel 0: channel pairs whose
-            // directions differ leave each other's MIS family.
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const float dx = gshfl(g, dir_k.x, j), dy = gshfl(g, dir_k.y, j), dz = gshfl(g, dir_k.z, j);
-                const int sj = gshfl(g, status, j);
-                if (j == g.c) continue;
-                bool m;
-                if (g.c == 0)
-                    m = sj == 1;
-                else if (j == 0)
-                    m = status == 1;
-                else if (status != 0 && sj != 0)
-                    m = dot(dir_k, v3(dx, dy, dz)) >= DIRECTION_MATCH_COS_TOL;
-                else
-                    m = true;
-                if (!m) P.compat &= ~(1u << j);
-            }
-        }
+        group_exit_probes(g, P, S, planes, hit_point, status == 2 && P.inside && intensity(original) > 0.0f,
+                          dir_k, t_intensity);
+        if (!P.inside) group_narrow_compat(g, P, status, dir_k);
         new_dir = final_refr;
         new_inside = !P.inside;
     }
@@ -399,6 +442,351 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
     }
     P.bounce = bounce + 1;
     return BOUNCE_CONTINUE;
+}
+
+// ------------------------------------------------------------------------------------
+// The bounce of the uniaxial transport instantiation: an isotropic material, a
+// pleochroic one, or a uniaxial crystal (transport/bounce.rs:108-160,
+// refraction/dispatch.rs:67-380, uniaxial_entry.rs, uniaxial_internal.rs, tir.rs:41).
+// Group-level decisions come from the hero (lane 0): its closed-form solve sets the
+// reflect probability and the eigenmode draw; every lane solves its own channel.
+// The path carries the wave normal `k` beside the (walked-off) ray direction `d`.
+// ------------------------------------------------------------------------------------
+IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
+                                 const float4* __restrict__ planes, float& esc) {
+    const ix_scene& sc = S.s;
+    const ix_material& mat = sc.material;
+    const uint32_t bounce = P.bounce;
+    Hit hit = group_intersect(g, planes, (int)sc.n_planes, P.o, P.d);
+    if (hit.facet < 0) {
+        esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
+        return BOUNCE_ESCAPED;
+    }
+    const float4 pl = planes[hit.facet];
+    V3 normal = v3(pl.x, pl.y, pl.z);
+    const V3 hit_point = P.o + hit.t * P.d;
+    const V3 k_hat = P.k;
+    const V3 c_axis = load3(mat.c_axis);
+    const bool aniso = S.aniso != 0;
+
+    // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:69), about k.
+    const V3 cpn = normalize_or_zero(cross(k_hat, normal));
+    if (P.has_prev && length_squared(cpn) > 1e-6f && length_squared(P.prev_pn) > 1e-6f) {
+        float cos_psi = clampf_(dot(P.prev_pn, cpn), -1.0f, 1.0f);
+        float sin_psi = dot(cross(P.prev_pn, cpn), normalize_or_zero(k_hat));
+        float psi = atan2f(sin_psi, cos_psi);
+        float s2, c2;
+        sincosf(2.0f * psi, &s2, &c2);
+        P.st = rotate(P.st, c2, s2);
+    }
+    P.has_prev = true;
+    P.prev_pn = cpn;
+
+    // apply_interior_segment + apply_absorption (transport/inner.rs:170,
+    // raytracer/absorption.rs:99-197): the assigned eigenmode's field for a crystal, the
+    // mean over both eigen-polarisations otherwise.
+    if (P.inside) {
+        normal = -normal;
+        if (S.absorbing) {
+            float alpha;
+            if (aniso) {
+                const V3 e = assigned_mode_e_field(k_hat, c_axis, P.is_e, P.n_hero, P.n_e_hero);
+                alpha = absorption_quadratic_form(c_axis, P.alpha, P.alpha_e, e);
+            } else {
+                const V3 ea = ordinary_eigen_polarization(k_hat, c_axis);
+                const V3 eb = normalize_or_zero(cross(k_hat, ea));
+                alpha = midpointf_(absorption_quadratic_form(c_axis, P.alpha, P.alpha_e, ea),
+                                   absorption_quadratic_form(c_axis, P.alpha, P.alpha_e, eb));
+            }
+            P.st = scale(P.st, exp_lane(-alpha * (hit.t * mat.absorption_path_scale)));
+        }
+    }
+
+    // compute_bounce_refraction_geometry (refraction/geometry.rs:306).
+    const float cos_i = clampf_(dot(-k_hat, normal), 0.0f, 1.0f);
+    const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
+    const float sin_i = sqrtf(fmaxf(one_m_c2, 0.0f));
+    float n_eff = P.n, n_eff_hero = P.n_hero;
+    if (aniso) {
+        // theta_c_for_bounce (geometry.rs:75): two fixed-point steps on entry.
+        float theta;
+        if (!P.inside) {
+            float n_guess = P.n_hero;
+            theta = 0.0f;
+#pragma unroll
+            for (int it = 0; it < 2; ++it) {
+                const float e = 1.0f / n_guess;
+                const float s2 = e * e * one_m_c2;
+                if (s2 > 1.0f) break;
+                const float ct = sqrtf(fmaxf(1.0f - s2, 0.0f));
+                const V3 w = normalize(e * k_hat + fmaf(e, cos_i, -ct) * normal);
+                theta = acosf(fabsf(clampf_(dot(w, c_axis), -1.0f, 1.0f)));
+                n_guess = effective_extraordinary_index(P.n_hero, P.n_e_hero, theta);
+            }
+        } else {
+            theta = acosf(fabsf(clampf_(dot(k_hat, c_axis), -1.0f, 1.0f)));
+        }
+        n_eff = effective_extraordinary_index(P.n, P.n_e, theta);
+        n_eff_hero = gshfl(g, n_eff, 0);
+    }
+    const bool inside0 = P.inside;
+    const bool ord_medium = aniso && inside0 && !P.is_e;
+    const float n_med = ord_medium ? P.n : n_eff;
+    const float n_med_hero = ord_medium ? P.n_hero : n_eff_hero;
+    const float n1 = inside0 ? n_med_hero : 1.0f;
+    const float n2 = inside0 ? 1.0f : n_med_hero;
+    const float eta = n1 / n2;
+    const float sin2_t = eta * eta * one_m_c2;
+    const float n1k = inside0 ? n_med : 1.0f;
+    const float n2k = inside0 ? 1.0f : n_med;
+    const float etak = n1k / n2k;
+    const float s2k = etak * etak * one_m_c2;
+    const float n_o_hero = P.n_hero;
+    const float n_e_hero_c = n_o_hero + mat.birefringence_delta;  // walk-off directions only
+    const float delta_n = mat.birefringence_delta;
+    const bool nondeg = aniso && length_squared(cross(k_hat, c_axis)) > 1e-6f;
+
+    V3 new_k, new_s;
+    bool new_inside = inside0;
+    int update = -1;
+    bool has_p_o = false;
+    float p_o_exact = 0.0f;
+    int status = 0;
+    bool narrow = false, want_probe = false;
+    V3 dir_k = v3(0.0f, 0.0f, 0.0f);
+    float t_int = 0.0f;
+
+    if (sin2_t > 1.0f) {
+        // apply_tir_bounce (tir.rs:41): forced reflection.
+        if (nondeg) {
+            const UFrame f = uframe_build(k_hat, normal, c_axis, cos_i, sin_i);
+            const IntSol sol = internal_solve(n1k, P.n, P.n_e, c_axis, f, !P.is_e);
+            const float ro = cnorm2(sol.r_o) * sol.flux_ro;
+            const float re = cnorm2(sol.r_e) * sol.flux_re;
+            const float r_total = fminf((ro + re) / fmaxf(sol.flux_inc, 1e-12f), 1.0f);
+            P.st = scale(P.st, r_total);
+            if (s2k <= 1.0f) P.pdf = P.pdf * clampf_(r_total, R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+            p_o_exact = gshfl(g, ro / fmaxf(ro + re, 1e-12f), 0);
+            has_p_o = true;
+        } else {
+            P.st = lane_scalar_reflect(P, n1k, n2k, s2k, cos_i, sin_i);
+        }
+        new_k = k_hat - 2.0f * dot(k_hat, normal) * normal;
+        new_s = (aniso && inside0 && P.is_e) ? extraordinary_poynting_dir(new_k, c_axis, n_o_hero, n_e_hero_c) : new_k;
+    } else if (nondeg && !inside0) {
+        // apply_uniaxial_entry_bounce (uniaxial_entry.rs:108).
+        const UFrame f = uframe_build(k_hat, normal, c_axis, cos_i, sin_i);
+        const EntryInc inc = entry_incidence_frame(1.0f, f);
+        const EntrySol s = entry_solve(inc, 1.0f, P.n, P.n_e, c_axis, f);
+        const float r_unpol_k = jones_r_unpol(s.r_s[0], s.r_s[1], s.r_p[0], s.r_p[1]);
+        const float r_branch = clampf_(gshfl(g, r_unpol_k, 0), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
+        const float inc_flux = 0.5f * f.cos_i;
+        const float p_o_raw = mode_power(s.t_o[0], s.t_o[1], s.flux_o, inc_flux, P.st);
+        const float p_e_raw = mode_power(s.t_e[0], s.t_e[1], s.flux_e, inc_flux, P.st);
+        const float p_o_hero = gshfl(
+            g, clampf_(p_o_raw / fmaxf(p_o_raw + p_e_raw, 1e-12f), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX), 0);
+        const bool use_e = unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 1.0f - p_o_hero;
+        const float p_frac = use_e ? 1.0f - p_o_hero : p_o_hero;
+        const float e_dir = n1 / (use_e ? n2 : n_o_hero);
+        const float c_dir = sqrtf(fmaxf(1.0f - fminf(e_dir * e_dir * one_m_c2, 1.0f), 0.0f));
+        const V3 refr = normalize(e_dir * k_hat + fmaf(e_dir, cos_i, -c_dir) * normal);
+        const V3 final_refr = use_e ? extraordinary_poynting_dir(refr, c_axis, n_o_hero, n_e_hero_c) : refr;
+        if (unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM) < r_branch) {
+            const M4 mk = jones_to_mueller(s.r_s[0], s.r_s[1], s.r_p[0], s.r_p[1]);
+            P.st = scale(apply_m4(mk, P.st), 1.0f / r_branch);
+            P.pdf = P.pdf * clampf_(mk.c[0], R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+            new_k = new_s = k_hat - 2.0f * dot(k_hat, normal) * normal;
+            new_inside = false;
+        } else {
+            const float n2k_dir = use_e ? n2k : P.n;
+            const float ratio = n1 / n2k_dir;
+            const float s2 = (ratio * ratio) * one_m_c2;
+            if (s2 > 1.0f) {
+                P.st = scale(P.st, 0.0f);
+                P.pdf = 0.0f;
+            } else {
+                const float cos_t_k = sqrtf(fmaxf(1.0f - s2, 0.0f));
+                const V3 refr_k = normalize(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
+                dir_k = use_e ? extraordinary_poynting_dir(refr_k, c_axis, P.n, P.n + delta_n) : refr_k;
+                status = dot(dir_k, final_refr) >= DIRECTION_MATCH_COS_TOL ? 1 : 2;
+                const float t_unpol = clampf_(1.0f - r_unpol_k, R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+                if (status == 1) {
+                    const float deposit =
+                        mode_power(use_e ? s.t_e[0] : s.t_o[0], use_e ? s.t_e[1] : s.t_o[1],
+                                   use_e ? s.flux_e : s.flux_o, inc_flux, P.st) / p_frac;
+                    float c2, s2a;
+                    azimuth2_in_frame(use_e ? s.e_hat : s.o_hat, f.s_axis, cross(refr, f.s_axis), c2, s2a);
+                    P.st = scale(Stokes{deposit, deposit * c2, deposit * s2a, 0.0f}, 1.0f / (1.0f - r_branch));
+                } else {
+                    P.st = scale(P.st, 0.0f);
+                }
+                P.pdf = P.pdf * t_unpol;
+            }
+            narrow = true;
+            new_k = refr;
+            new_s = final_refr;
+            new_inside = true;
+            update = use_e ? 1 : 0;
+        }
+    } else if (nondeg) {
+        // apply_uniaxial_internal_bounce (uniaxial_internal.rs:68).
+        const UFrame f = uframe_build(k_hat, normal, c_axis, cos_i, sin_i);
+        const IntSol sol = internal_solve(n1k, P.n, P.n_e, c_axis, f, !P.is_e);
+        const float flux_inc = fmaxf(sol.flux_inc, 1e-12f);
+        const float ro = cnorm2(sol.r_o) * sol.flux_ro;
+        const float re = cnorm2(sol.r_e) * sol.flux_re;
+        const float r_branch =
+            gshfl(g, clampf_((ro + re) / flux_inc, R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX), 0);
+        const float p_o_h = gshfl(g, ro / fmaxf(ro + re, 1e-12f), 0);
+        if (unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM) < r_branch) {
+            const float r_total_k =
+                fminf(fmaf(cnorm2(sol.r_e), sol.flux_re, cnorm2(sol.r_o) * sol.flux_ro) / flux_inc, 1.0f);
+            P.st = scale(P.st, r_total_k / r_branch);
+            P.pdf = P.pdf * clampf_(r_total_k, R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+            new_k = new_s = k_hat - 2.0f * dot(k_hat, normal) * normal;
+            has_p_o = true;
+            p_o_exact = p_o_h;
+        } else {
+            const float c_dir = sqrtf(fmaxf(1.0f - fminf(eta * eta * one_m_c2, 1.0f), 0.0f));
+            const V3 hero_refr = normalize(eta * k_hat + fmaf(eta, cos_i, -c_dir) * normal);
+            const float original_i = P.st.i;
+            if (s2k > 1.0f) {
+                P.st = scale(P.st, 0.0f);
+                P.pdf = 0.0f;
+            } else {
+                const float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
+                dir_k = normalize(etak * k_hat + fmaf(etak, cos_i, -cos_t_k) * normal);
+                status = dot(dir_k, hero_refr) >= DIRECTION_MATCH_COS_TOL ? 1 : 2;
+                float i_unit;
+                const Stokes tr = uniaxial_exit_transmission(sol, r_branch, original_i, i_unit);
+                P.pdf = P.pdf * clampf_(i_unit, R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+                P.st = status == 1 ? tr : scale(P.st, 0.0f);
+                want_probe = status == 2 && original_i > 0.0f;
+                t_int = intensity(tr);
+            }
+            new_k = new_s = hero_refr;
+            new_inside = false;
+        }
+    } else {
+        // apply_partial_fresnel_bounce's scalar path (dispatch.rs:162-380): an isotropic
+        // material, or a uniaxial one with k along the optic axis.
+        const bool entering = aniso && !inside0;
+        bool has_sel = false;
+        float p_o = 0.5f, c2 = 0.0f, s2 = 0.0f;
+        if (entering) {
+            // resolve_entry_mode_selection (dispatch.rs:162): the hero's Stokes state.
+            float po_l = 0.5f, c2_l = 0.0f, s2_l = 0.0f;
+            const bool sel_l = entry_eigenmode_selection(c_axis, cpn, k_hat, P.st, po_l, c2_l, s2_l);
+            has_sel = gshfl(g, sel_l ? 1 : 0, 0) != 0;
+            p_o = has_sel ? gshfl(g, po_l, 0) : 0.5f;
+            c2 = gshfl(g, c2_l, 0);
+            s2 = gshfl(g, s2_l, 0);
+        }
+        const bool use_e = entering ? unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 1.0f - p_o : P.is_e;
+        const bool ord_sel = entering && !use_e;
+        // compute_entry_reflect_probability (dispatch.rs:230).
+        const float n2s = ord_sel ? n_o_hero : n2;
+        float sin2_ts = sin2_t;
+        if (ord_sel) {
+            const float e2 = n1 / n2s;
+            sin2_ts = e2 * e2 * one_m_c2;
+        }
+        float r_s, r_p;
+        fresnel_rs_rp(n1, n2s, cos_i, sqrtf(fmaxf(1.0f - sin2_ts, 0.0f)), r_s, r_p);
+        const float r_unpol = clampf_(r_unpol_of(r_s, r_p), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
+        if (unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM) < r_unpol) {
+            P.st = scale(lane_scalar_reflect(P, n1k, n2k, s2k, cos_i, sin_i), 1.0f / r_unpol);
+            new_k = k_hat - 2.0f * dot(k_hat, normal) * normal;
+            new_s = (aniso && inside0 && P.is_e) ? extraordinary_poynting_dir(new_k, c_axis, n_o_hero, n_e_hero_c)
+                                                 : new_k;
+        } else {
+            // apply_refract_bounce / apply_refract_channel (reflect_refract.rs:121-591).
+            const float e_dir = n1 / n2s;
+            const float c_dir = sqrtf(fmaxf(1.0f - fminf(e_dir * e_dir * one_m_c2, 1.0f), 0.0f));
+            const V3 refr = normalize(e_dir * k_hat + fmaf(e_dir, cos_i, -c_dir) * normal);
+            const bool walk = entering && use_e;
+            const V3 final_refr = walk ? extraordinary_poynting_dir(refr, c_axis, n_o_hero, n_e_hero_c) : refr;
+            const float n2k_r = ord_sel ? P.n : n2k;
+            const float ratio = n1k / n2k_r;
+            const float s2r = (ratio * ratio) * one_m_c2;
+            const Stokes original = P.st;
+            if (s2r > 1.0f) {
+                P.st = scale(P.st, 0.0f);
+                P.pdf = 0.0f;
+            } else {
+                const float cos_t_k = sqrtf(fmaxf(1.0f - s2r, 0.0f));
+                const V3 refr_k = normalize(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
+                dir_k = walk ? extraordinary_poynting_dir(refr_k, c_axis, P.n, P.n + delta_n) : refr_k;
+                status = dot(dir_k, final_refr) >= DIRECTION_MATCH_COS_TOL ? 1 : 2;
+                const float two = 2.0f * n1k * cos_i;
+                const float t_s = two / fmaf(n2k_r, cos_t_k, n1k * cos_i);
+                const float t_p = two / fmaf(n1k, cos_t_k, n2k_r * cos_i);
+                // The selected eigenmode's projection at an anisotropic entry.
+                const float az_c = use_e ? -c2 : c2, az_s = use_e ? -s2 : s2;
+                const Stokes incident = (entering && has_sel)
+                                            ? Stokes{original.i, original.i * az_c, original.i * az_s, 0.0f}
+                                            : original;
+                const Stokes transmitted =
+                    scale(fresnel_transmit_apply(incident, n1k, n2k_r, cos_i, cos_t_k, t_s, t_p),
+                          1.0f / (1.0f - r_unpol));
+                float rs, rp;
+                fresnel_rs_rp(n1k, n2k_r, cos_i, cos_t_k, rs, rp);
+                P.pdf = P.pdf * (1.0f - clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX));
+                P.st = status == 1 ? transmitted : scale(original, 0.0f);
+                t_int = intensity(transmitted);
+                want_probe = status == 2 && inside0 && intensity(original) > 0.0f;
+            }
+            narrow = !inside0;
+            new_k = refr;
+            new_s = final_refr;
+            new_inside = !inside0;
+            update = entering ? (use_e ? 1 : 0) : -1;
+        }
+    }
+    group_exit_probes(g, P, S, planes, hit_point, want_probe, dir_k, t_int);
+    if (narrow) group_narrow_compat(g, P, status, dir_k);
+
+    const bool was_internal_reflection = inside0 && update < 0 && new_inside == inside0;
+    P.d = new_s;
+    P.o = hit_point + new_s * 1e-4f;
+    P.k = new_k;
+    P.inside = new_inside;
+    if (update >= 0) P.is_e = update != 0;
+    // maybe_apply_internal_mode_coupling (transport/bounce.rs:470): an internal
+    // reflection relabels the eigenmode with the closed-form R_o / (R_o + R_e), else the
+    // hero's polarisation weight.
+    if (aniso && was_internal_reflection) {
+        float p_o = p_o_exact;
+        if (!has_p_o) {
+            float po_l = 0.5f, a, b;
+            if (!entry_eigenmode_selection(c_axis, cpn, P.k, P.st, po_l, a, b)) po_l = 0.5f;
+            p_o = gshfl(g, po_l, 0);
+        }
+        P.is_e = unit_draw(P.seed, bounce, MODE_COUPLING_STREAM) >= p_o;
+    }
+
+    // Surface glare (bounce_body.rs:691-697) and Russian roulette (transport/bounce.rs:355).
+    const float glare = clampf_(sc.environment.surface_glare, 0.0f, 1.0f);
+    if (bounce == 0 && !P.inside && glare < 1.0f) P.st = scale(P.st, glare);
+    if (bounce > 4) {
+        float max_i = intensity(P.st);
+#pragma unroll
+        for (int m = 4; m > 0; m >>= 1) max_i = fmaxf(max_i, gxor(g, max_i, m));
+        const float q = clampf_(fmaxf(0.0f, max_i), 0.05f, 1.0f);
+        if (unit_draw(P.seed, bounce, RUSSIAN_ROULETTE_STREAM) > q) return BOUNCE_KILLED;
+        P.st = scale(P.st, 1.0f / q);
+        P.split = P.split / q;
+    }
+    P.bounce = bounce + 1;
+    return BOUNCE_CONTINUE;
+}
+
+template <bool UNI>
+IX_DEV int group_step(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes, float& esc) {
+    if constexpr (UNI)
+        return group_bounce_uniaxial(g, P, S, planes, esc);
+    else
+        return group_bounce(g, P, S, planes, esc);
 }
 
 // finish (bounce_body.rs:724-764): commit the exit splits of an escaped path, integrate
@@ -450,13 +838,14 @@ IX_DEV V3 group_finish(const Group& g, const LanePath& P, const DevScene& S, boo
 }
 
 // A whole path by one group (the check kernels' per-path entry).
+template <bool UNI>
 IX_DEV V3 group_trace(const Group& g, LanePath& P, const DevScene& S, const float4* planes,
                       uint32_t* iterations) {
     float esc = 0.0f;
     int r = BOUNCE_CONTINUE;
     uint32_t it = 0;
     while (P.bounce < S.s.max_bounces) {
-        r = group_bounce(g, P, S, planes, esc);
+        r = group_step<UNI>(g, P, S, planes, esc);
         ++it;
         if (r != BOUNCE_CONTINUE) break;
     }

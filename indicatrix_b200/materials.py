@@ -103,3 +103,27 @@ def sapphire(c_axis=(0.0, 1.0, 0.0)) -> abi.Material:
                  energy_band(457.0, 12000.0, 0.433)],
         e_bands=[energy_band(612.0, 7466.0, 0.371), energy_band(729.0, 4955.0, 1.03),
                  energy_band(467.0, 11169.0, 0.524)])
+
+
+def wavelength_band(center_nm: float, width_nm: float, peak: float) -> abi.Band:
+    """AbsorptionBand::new (optics/absorption.rs): a Gaussian in wavelength."""
+    b = abi.Band()
+    b.center_nm, b.width_nm, b.peak = float(center_nm), float(width_nm), float(peak)
+    b.shape = abi.BAND_GAUSS_WAVELENGTH
+    return b
+
+
+def quartz(c_axis=(0.0, 1.0, 0.0)) -> abi.Material:
+    """Quartz (materials/spinel_through_tourmaline.rs:76-118): Ghosh o-ray Sellmeier and
+    its own e-ray Sellmeier (a separate extraordinary dispersion curve), colourless."""
+    return uniaxial(sellmeier3([0.2860414, 1.0704408, 1.1020224], [0.0, 0.0100586, 100.0]), 0.0091, c_axis,
+                    e_dispersion=sellmeier3([0.28851804, 1.0950992, 1.1566248], [0.0, 0.010210186, 100.0]))
+
+
+def rutile(c_axis=(0.0, 1.0, 0.0)) -> abi.Material:
+    """Rutile (materials/rutile.rs:54-80): extreme positive birefringence (0.2957) with
+    o- and e-ray Sellmeier fits and a UV band on both rays."""
+    band = [wavelength_band(350.0, 40.0, 8.0)]
+    return uniaxial(sellmeier3([3.039851, 1.873149, 0.0], [0.0803, 0.0, 0.0]), 0.2957, c_axis,
+                    o_bands=band, e_bands=band,
+                    e_dispersion=sellmeier3([3.940688, 2.256312, 0.0], [0.0843, 0.0, 0.0]))

@@ -101,6 +101,43 @@ def random_stones(n: int, seed: int = 20251203) -> List[StoneSpec]:
     return out
 
 
+def smooth_spline(rng: np.random.Generator, peak_max: float) -> np.ndarray:
+    """A seeded smooth 16-knot absorption curve with a random peak in [0, peak_max]."""
+    knots = rng.uniform(0.0, 1.0, abi.SPLINE_KNOTS)
+    knots = np.convolve(np.pad(knots, 2, mode="edge"), np.ones(5) / 5.0, mode="valid")
+    return (knots / max(knots.max(), 1e-6) * rng.uniform(0.0, peak_max)).astype(np.float32)
+
+
+def stress_material(seed: int = 7, tilt_deg: float = 30.0) -> abi.Material:
+    """The anisotropic stress material: corundum o-ray and e-ray Sellmeier fits
+    (Malitson & Dodge 1972; n_o = 1.768, n_e = 1.760 at the D line), optic axis tilted
+    `tilt_deg` from the table normal toward +x, and a pleochroic absorption tensor whose
+    o-ray and e-ray coefficients are two seeded smooth 16-knot splines of 0-8 /cm."""
+    rng = np.random.default_rng(seed)
+    t = math.radians(tilt_deg)
+    m = materials.uniaxial(
+        materials.sellmeier3([1.4313493, 0.65054713, 5.3414021], [0.0726631 ** 2, 0.1193242 ** 2, 18.028251 ** 2]),
+        -0.0081, (math.sin(t), math.cos(t), 0.0),
+        e_dispersion=materials.sellmeier3([1.5039759, 0.55069141, 6.5927379],
+                                          [0.0740288 ** 2, 0.1216529 ** 2, 20.072248 ** 2]))
+    for ab in (m.abs_o, m.abs_e):
+        ab.has_spline = 1
+        ab.spline[:] = [float(x) for x in smooth_spline(rng, 8.0)]
+    m.absorption_path_scale = CM_PER_MODEL_UNIT
+    return m
+
+
+def anisotropic_stress_frame(width: int = 512, height: int = 512, max_bounces: int = 64,
+                             seed: int = 7) -> FrameScene:
+    """The emerald step cut (3 crown + 3 pavilion tiers, 49 facets) in the stress
+    material, face up under the D65 hemisphere with the 20-degree head shadow, max depth 64."""
+    planes = geometry.to_f32(geometry.step_cut())
+    cam = camera_new(0.0, float(FACE_UP_PITCH), FACE_UP_DISTANCE, DEFAULT_FOV_DEG)
+    return FrameScene(camera=cam, width=width, height=height, planes=planes,
+                      material=stress_material(seed), max_bounces=max_bounces,
+                      environment=iso_hemisphere())
+
+
 TILTS_DEG = [0.0, 5.0, 10.0, 15.0, 20.0, 25.0, 30.0, 35.0, 40.0]
 
 

@@ -84,8 +84,10 @@ def test_host_builders_match_oracle_bits(oracle):
 def test_routing_predicate():
     fs = workloads.round_brilliant_frame(8, 8)
     assert scene_routes_to_gpu(fs)
-    m = materials.diamond()
-    m.anisotropic = 1
+    for m in (materials.sapphire(), materials.quartz(), materials.rutile((0.6, 0.8, 0.0))):
+        assert scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, fs.planes, m, 32, fs.environment))
+    m = materials.quartz()
+    m.e_dispersion.kind = 7
     assert not scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, fs.planes, m, 32, fs.environment))
     m = materials.diamond()
     m.scattering_sigma_s = 0.5
