@@ -5,7 +5,10 @@ One "step" is one pass of the hot path over one batch of synthetic input:
 * ``--workload batch`` (default): 64 seeded random stones x 9 tilts at 128x128 with spp
   drawn from {32, 64, 128, 256} -- one persistent launch per step (about 1.1e9 paths);
 * ``--workload frame``: the 256x256, 64 spp round-brilliant frame (4,194,304 paths;
-  Diamond, D65 hemisphere with a 20-degree head shadow, depth 32).
+  Diamond, D65 hemisphere with a 20-degree head shadow, depth 32);
+* ``--workload stress``: the anisotropic stress frame, 512x512 x 256 spp (67,108,864
+  paths) of a uniaxial pleochroic emerald-cut stone with its optic axis tilted 30
+  degrees, depth 64.
 
 Under torchrun (N > 1) every rank traces its own disjoint absolute sample range of the
 same workload (weak scaling), and the per-pixel f64 sums are gathered to rank 0 over
@@ -46,7 +49,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["frame", "batch"])
+    ap.add_argument("--workload", default="batch", choices=["frame", "batch", "stress"])
     ap.add_argument("--precision", default="fast", choices=["fast", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -125,6 +128,18 @@ def frame_workload():
                         "environment": "D65 hemisphere, 20 deg head shadow", "max_depth": 32}
 
 
+def stress_workload():
+    from indicatrix_b200 import workloads
+
+    fs = workloads.anisotropic_stress_frame(512, 512, 64)
+    return [(fs, 256)], {"workload": "anisotropic stress frame 512x512 x 256 spp", "pixels": 512 * 512,
+                         "spp": 256, "planes": int(fs.planes.shape[0]),
+                         "material": "uniaxial corundum (n_o 1.768, n_e 1.760, Sellmeier o/e), optic axis "
+                                     "tilted 30 deg, o/e spline absorption 0-8 /cm",
+                         "stone": "emerald step cut, 3+3 tiers, 49 facets",
+                         "environment": "D65 hemisphere, 20 deg head shadow", "max_depth": 64}
+
+
 def batch_workload():
     from indicatrix_b200 import workloads
 
@@ -150,10 +165,12 @@ def cpu_baseline(items, seconds: float):
     fs, spp = items[0]
     sc = fs.to_abi()
     n_pix = fs.width * fs.height
-    # Calibrate on a small pixel slice, then trace a slice sized for ~`seconds`.
+    # Calibrate on a small slice through the middle of the frame (where the stone is),
+    # then trace a band of rows there sized for ~`seconds`.
     t0 = time.perf_counter()
     probe = min(n_pix, 256)
-    ix_oracle.trace_pixels(sc, 0, probe, 0, spp, threads)
+    p0 = max(0, n_pix // 2 - probe // 2)
+    ix_oracle.trace_pixels(sc, p0, p0 + probe, 0, spp, threads)
     dt = max(time.perf_counter() - t0, 1e-3)
     rate = probe * spp / dt
     want = int(rate * seconds / spp)
@@ -175,18 +192,21 @@ def count_flops(items):
 
     ix_oracle.build()
     total_f, total_p = 0, 0
-    details = {}
+    div = sqrt = transc = 0
     step = max(1, len(items) // 8)
     for fs, spp in items[::step]:
         sc = fs.to_abi()
         n_pix = fs.width * fs.height
+        # A pixel stride coprime with the width, so the sample spreads over every column.
         stride = max(1, n_pix // (8192 // max(1, spp // 16)))
+        while math.gcd(stride, fs.width) != 1:
+            stride += 1
         c = ix_oracle.count_flops(sc, 0, n_pix, stride, 0, spp)
         total_f += c.flops()
         total_p += c.paths
-        details = {"div_per_path": c.div / c.paths, "sqrt_per_path": c.sqrt / c.paths,
-                   "transcendental_per_path": c.transcendental / c.paths}
-    return total_f / total_p, {"sample_paths": total_p, **details}
+        div, sqrt, transc = div + c.div, sqrt + c.sqrt, transc + c.transcendental
+    return total_f / total_p, {"sample_paths": total_p, "div_per_path": div / total_p,
+                               "sqrt_per_path": sqrt / total_p, "transcendental_per_path": transc / total_p}
 
 
 # ----------------------------------------------------------------------------------
@@ -234,7 +254,7 @@ def run_reference(args, items, cfg):
 def main():
     args = parse()
     rank, world, local = dist_env()
-    items, cfg = frame_workload() if args.workload == "frame" else batch_workload()
+    items, cfg = {"frame": frame_workload, "stress": stress_workload, "batch": batch_workload}[args.workload]()
     cfg["parallelism"] = f"sample-range shards x{world}" if world > 1 else "single GPU"
     if args.impl == "reference":
         run_reference(args, items, cfg)

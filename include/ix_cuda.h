@@ -190,6 +190,60 @@ int ix_environment_preset(int32_t preset_index, float exposure, float light_yaw,
 /* A uniform dome of constant spectral radiance (white-furnace environment). */
 void ix_environment_uniform(float radiance, ix_environment* out);
 
+/* ---- Analytic optical metrics (color/metrics/evaluate.rs:158-392) -----------------
+ * evaluate_gem_optical_metrics on the device: for each camera pose, an 18 x 18 fan of
+ * grid cells inside the stone's outline disc, 5 aperture rays per cell traced through
+ * the stone at n_D (with n_F / n_C companions for fire) and 5 yaw-jittered rays for the
+ * temporal scintillation term, each classified against the exit lighting.  Output is
+ * the reference's GemOpticalMetrics, in its order. */
+typedef struct ix_gem_metrics {
+    float brilliance_pct;
+    float fire_index;
+    float scintillation_pct;
+    float windowing_pct;
+    float extinction_pct;
+} ix_gem_metrics;
+
+/* The lighting a call scores against: a LightingPreset index (as ix_environment_preset),
+ * the rig's light yaw / pitch and the environment's head-shadow size in degrees
+ * (16 = the default). */
+typedef struct ix_metrics_lighting {
+    int32_t preset;
+    float light_yaw;
+    float light_pitch;
+    float head_shadow_deg;
+} ix_metrics_lighting;
+
+/* One stone of a batched call: its half-spaces (host, n x {nx, ny, nz, d}) and its
+ * ordinary dispersion (n_D, n_F, n_C are evaluated from it). */
+typedef struct ix_metrics_stone {
+    const float* planes;
+    uint32_t n_planes;
+    ix_dispersion dispersion;
+} ix_metrics_stone;
+
+/* One camera pose (Camera::new yaw / pitch) of stone `stone`. */
+typedef struct ix_metrics_pose {
+    uint32_t stone;
+    float cam_yaw;
+    float cam_pitch;
+} ix_metrics_pose;
+
+/* evaluate_gem_optical_metrics(planes, material, cam_yaw, cam_pitch, environment)
+ * (color/metrics/evaluate.rs:158): one pose.  Returns IX_DONE, or IX_DECLINED (no
+ * device, an empty or oversized plane set, an unmodelled preset; `out` untouched). */
+int ix_evaluate_gem_optical_metrics(ix_backend* b, const float* planes, uint32_t n_planes,
+                                    const ix_material* material, float cam_yaw, float cam_pitch,
+                                    const ix_metrics_lighting* lighting, ix_gem_metrics* out);
+/* Many poses of many stones under one lighting in one launch (one CTA per pose), the
+ * batched form of the reference's pose runs (color/metrics/pose_batch.rs, profile.rs,
+ * sweep.rs).  want_fire_and_scintillation = 0 is MetricsWanted::CONSUMED_ONLY (fire and
+ * scintillation report the placeholders 25 and 75, their rays are not traced). */
+int ix_evaluate_gem_optical_metrics_batch(ix_backend* b, const ix_metrics_stone* stones, uint32_t n_stones,
+                                          const ix_metrics_lighting* lighting, const ix_metrics_pose* poses,
+                                          uint32_t n_poses, uint32_t want_fire_and_scintillation,
+                                          ix_gem_metrics* out);
+
 /* Per-function check kernels (the GPU equivalence harness's Tier-1/Tier-2 units,
  * renderer/gpu/ulp.rs): evaluates function `fn` (ix::CheckFn numbering) for `n` input
  * rows of `in_stride` 32-bit words on the device, writing `out_stride` words per row.

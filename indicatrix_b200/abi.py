@@ -164,6 +164,43 @@ class TimingInfo(C.Structure):
     ]
 
 
+class GemMetrics(C.Structure):
+    """GemOpticalMetrics (color/metrics/types.rs)."""
+
+    _fields_ = [
+        ("brilliance_pct", C.c_float),
+        ("fire_index", C.c_float),
+        ("scintillation_pct", C.c_float),
+        ("windowing_pct", C.c_float),
+        ("extinction_pct", C.c_float),
+    ]
+
+
+class MetricsLighting(C.Structure):
+    _fields_ = [
+        ("preset", C.c_int32),
+        ("light_yaw", C.c_float),
+        ("light_pitch", C.c_float),
+        ("head_shadow_deg", C.c_float),
+    ]
+
+
+class MetricsStone(C.Structure):
+    _fields_ = [
+        ("planes", C.POINTER(C.c_float)),
+        ("n_planes", C.c_uint32),
+        ("dispersion", Dispersion),
+    ]
+
+
+class MetricsPose(C.Structure):
+    _fields_ = [
+        ("stone", C.c_uint32),
+        ("cam_yaw", C.c_float),
+        ("cam_pitch", C.c_float),
+    ]
+
+
 def floats(values) -> C.Array:
     arr = (C.c_float * len(values))()
     for i, v in enumerate(values):

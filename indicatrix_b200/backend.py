@@ -93,6 +93,12 @@ def load_library() -> C.CDLL:
         lib.ix_environment_uniform.argtypes = [C.c_float, P(abi.Environment)]
         lib.ix_debug_check.argtypes = [C.c_void_p, P(abi.Scene), C.c_int32, C.c_uint32,
                                        P(C.c_uint32), C.c_uint32, P(C.c_uint32), C.c_uint32]
+        lib.ix_evaluate_gem_optical_metrics.argtypes = [C.c_void_p, P(C.c_float), C.c_uint32, P(abi.Material),
+                                                        C.c_float, C.c_float, P(abi.MetricsLighting),
+                                                        P(abi.GemMetrics)]
+        lib.ix_evaluate_gem_optical_metrics_batch.argtypes = [C.c_void_p, P(abi.MetricsStone), C.c_uint32,
+                                                              P(abi.MetricsLighting), P(abi.MetricsPose),
+                                                              C.c_uint32, C.c_uint32, P(abi.GemMetrics)]
         _lib = lib
         return lib
 
@@ -213,6 +219,22 @@ def environment_uniform(radiance: float) -> abi.Environment:
 def scene_routes_to_gpu(scene: FrameScene) -> bool:
     """scene_routes_to_gpu (gpu_backend/mod.rs:288)."""
     return bool(load_library().ix_scene_routes_to_gpu(C.byref(scene.to_abi())))
+
+
+@dataclass
+class MetricsLighting:
+    """The environment the metrics score against (EnvironmentSource::Studio): a
+    LightingPreset index, the rig's light yaw / pitch and the head-shadow size in
+    degrees."""
+
+    preset: int = PRESET_RING_LIGHTS
+    light_yaw: float = 0.0
+    light_pitch: float = 0.0
+    head_shadow_deg: float = 16.0
+
+    def to_abi(self) -> abi.MetricsLighting:
+        return abi.MetricsLighting(int(self.preset), float(self.light_yaw), float(self.light_pitch),
+                                   float(self.head_shadow_deg))
 
 
 @dataclass
@@ -383,6 +405,47 @@ class GpuBackend:
                                             C.c_void_p(d_accum_ptr), 1 if accumulate else 0,
                                             C.c_void_p(stream_ptr) if stream_ptr else None)
         return GpuAccumulate(rc)
+
+    def evaluate_gem_optical_metrics(self, planes: np.ndarray, material: abi.Material, cam_yaw: float,
+                                     cam_pitch: float, lighting: "MetricsLighting") -> Optional[np.ndarray]:
+        """evaluate_gem_optical_metrics (color/metrics/evaluate.rs:158): [brilliance %,
+        fire index, scintillation %, windowing %, extinction %] as float32, or None when
+        the call is declined."""
+        if not self._h:
+            return None
+        p = np.ascontiguousarray(planes, np.float32)
+        out = abi.GemMetrics()
+        rc = self._lib.ix_evaluate_gem_optical_metrics(self._h, p.ctypes.data_as(C.POINTER(C.c_float)),
+                                                       p.shape[0], C.byref(material), cam_yaw, cam_pitch,
+                                                       C.byref(lighting.to_abi()), C.byref(out))
+        if rc != abi.IX_DONE:
+            return None
+        return np.array([out.brilliance_pct, out.fire_index, out.scintillation_pct, out.windowing_pct,
+                         out.extinction_pct], np.float32)
+
+    def evaluate_metrics_batch(self, stones: Sequence[tuple], poses: Sequence[tuple], lighting: "MetricsLighting",
+                               want_fire_and_scintillation: bool = True) -> Optional[np.ndarray]:
+        """Many poses in one launch.  ``stones``: (planes, dispersion) pairs; ``poses``:
+        (stone index, cam_yaw, cam_pitch).  Returns an (n_poses, 5) float32 array in the
+        GemOpticalMetrics order, or None when declined."""
+        if not self._h:
+            return None
+        keep = [np.ascontiguousarray(p, np.float32) for p, _ in stones]
+        st = (abi.MetricsStone * len(stones))()
+        for i, (p, (_, disp)) in enumerate(zip(keep, stones)):
+            st[i].planes = p.ctypes.data_as(C.POINTER(C.c_float))
+            st[i].n_planes = p.shape[0]
+            st[i].dispersion = disp
+        ps = (abi.MetricsPose * len(poses))()
+        for i, (s, yaw, pitch) in enumerate(poses):
+            ps[i].stone, ps[i].cam_yaw, ps[i].cam_pitch = int(s), float(yaw), float(pitch)
+        out = (abi.GemMetrics * len(poses))()
+        rc = self._lib.ix_evaluate_gem_optical_metrics_batch(self._h, st, len(stones), C.byref(lighting.to_abi()),
+                                                             ps, len(poses), 1 if want_fire_and_scintillation else 0,
+                                                             out)
+        if rc != abi.IX_DONE:
+            return None
+        return np.frombuffer(bytes(out), np.float32).reshape(len(poses), 5).copy()
 
     def debug_check(self, scene: FrameScene, fn: int, inputs: np.ndarray, out_words: int) -> np.ndarray:
         """Runs per-function check kernel ``fn`` over the rows of ``inputs`` (32-bit words)."""

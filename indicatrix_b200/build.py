@@ -53,24 +53,26 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD_DIR, exist_ok=True)
     common = [nvcc, "-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC",
               "--expt-relaxed-constexpr", "-Xptxas", "-v", f"-I{INCLUDE}"]
-    objs = []
-    logs = []
-    for variant, flags in (("exact", ["-DIX_EXACT=1", "-fmad=false"]),
-                           ("fast", ["-DIX_EXACT=0", "-fmad=true"])):
-        obj = os.path.join(BUILD_DIR, f"ix_kernels_{variant}.o")
-        cmd = common + flags + ["-c", os.path.join(CSRC, "ix_kernels.cu"), "-o", obj]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        logs.append(r.stderr)
-        if r.returncode != 0:
-            raise RuntimeError("nvcc failed:\n" + r.stderr)
-        objs.append(obj)
+    jobs = []  # (object, command); the device units compile concurrently
+    for unit in ("ix_kernels", "ix_metrics"):
+        for variant, flags in (("exact", ["-DIX_EXACT=1", "-fmad=false"]),
+                               ("fast", ["-DIX_EXACT=0", "-fmad=true"])):
+            obj = os.path.join(BUILD_DIR, f"{unit}_{variant}.o")
+            jobs.append((obj, common + flags + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj]))
     for unit in ("ix_probe", "ix_noalloc"):
         obj = os.path.join(BUILD_DIR, unit + ".o")
-        r = subprocess.run(common + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj],
-                           capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError("nvcc failed:\n" + r.stderr)
+        jobs.append((obj, common + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj]))
+    procs = [(obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+             for obj, cmd in jobs]
+    objs, logs, errors = [], [], []
+    for obj, proc in procs:
+        _, err = proc.communicate()
+        logs.append(err)
+        if proc.returncode != 0:
+            errors.append(err)
         objs.append(obj)
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
     cuda_inc = os.path.join(_cuda_home(nvcc), "include")
     for unit in ("ix_backend", "ix_dispatch"):
         host_obj = os.path.join(BUILD_DIR, unit + ".o")

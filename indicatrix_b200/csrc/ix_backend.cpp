@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -303,6 +304,77 @@ H3 white_balance(float temp_k) {
     H3 s = bradford_xyz_to_lms(w), t = bradford_xyz_to_lms(target);
     return h3(s.x > 1e-6f ? t.x / s.x : 1.0f, s.y > 1e-6f ? t.y / s.y : 1.0f,
               s.z > 1e-6f ? t.z / s.z : 1.0f);
+}
+
+// ------------------------------------------------------------------------------------
+// Host setup of the analytic metrics (color/metrics/prepared.rs, fan.rs, lighting.rs,
+// visibility.rs, camera.rs): per stone and per lighting, computed once per call.
+// ------------------------------------------------------------------------------------
+const float kD65[41] = IX_CIE_D65_SPD_INIT;
+
+// d65_relative_spectral_power (environment/spectral.rs:49) on [380, 780] nm.
+float d65_host(float lambda) {
+    float c = lambda < 380.0f ? 380.0f : (lambda > 780.0f ? 780.0f : lambda);
+    float position = (c - 380.0f) / 10.0f;
+    int i0 = std::min((int)std::floor(position), 39);
+    float frac = position - (float)i0;
+    return std::fma(frac, kD65[i0 + 1] - kD65[i0], kD65[i0]) / 100.0f;
+}
+
+// measure_model_width (render_setup/stone_width.rs:27, geometry/stone_metrics/measure.rs):
+// the narrower horizontal extent (x or z) of the solid's vertices, in f64.  A vertex is
+// any point where three planes meet and no plane is violated by more than 1e-9.
+double solid_width(const float* planes, uint32_t n) {
+    std::vector<std::array<double, 4>> pl;  // n.x <= m with m = -d
+    for (uint32_t i = 0; i < n; ++i) {
+        std::array<double, 4> p{planes[4 * i], planes[4 * i + 1], planes[4 * i + 2], -(double)planes[4 * i + 3]};
+        bool same = false;
+        for (const auto& q : pl)
+            if (p[0] * q[0] + p[1] * q[1] + p[2] * q[2] > 1.0 - 1e-12 && std::fabs(p[3] - q[3]) < 1e-9) same = true;
+        if (!same) pl.push_back(p);
+    }
+    const size_t m = pl.size();
+    double lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
+    size_t found = 0;
+    auto cr = [](const std::array<double, 4>& a, const std::array<double, 4>& b, double o[3]) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    for (size_t i = 0; i < m; ++i)
+        for (size_t j = i + 1; j < m; ++j)
+            for (size_t k = j + 1; k < m; ++k) {
+                double jk[3], ki[3], ij[3];
+                cr(pl[j], pl[k], jk);
+                double det = pl[i][0] * jk[0] + pl[i][1] * jk[1] + pl[i][2] * jk[2];
+                if (std::fabs(det) < 1e-12) continue;
+                cr(pl[k], pl[i], ki);
+                cr(pl[i], pl[j], ij);
+                double v[3];
+                for (int a = 0; a < 3; ++a) v[a] = (pl[i][3] * jk[a] + pl[j][3] * ki[a] + pl[k][3] * ij[a]) / det;
+                if (!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2])) continue;
+                bool inside = true;
+                for (size_t q = 0; inside && q < m; ++q)
+                    inside = pl[q][0] * v[0] + pl[q][1] * v[1] + pl[q][2] * v[2] - pl[q][3] <= 1e-9;
+                if (!inside) continue;
+                ++found;
+                lo[0] = std::min(lo[0], v[0]);
+                hi[0] = std::max(hi[0], v[0]);
+                lo[1] = std::min(lo[1], v[2]);
+                hi[1] = std::max(hi[1], v[2]);
+            }
+    if (found < 4) return NAN;
+    const double dx = hi[0] - lo[0], dz = hi[1] - lo[1];
+    return dx <= dz ? dx : dz;
+}
+
+// head_shadow_cone_cos (visibility.rs:16).
+float metrics_head_shadow_cos(bool studio, float deg) {
+    if (studio || std::isnan(deg) || deg == 16.0f) return 0.96f;
+    if (deg <= 0.0f) return 2.0f;
+    const float offset = std::acos(0.96f) - to_radians(16.0f);
+    const float c = deg < 1.0f ? 1.0f : (deg > 89.0f ? 89.0f : deg);
+    return std::cos(to_radians(c) + offset);
 }
 
 }  // namespace
@@ -837,6 +909,115 @@ int ix_environment_preset(int32_t preset, float exposure, float light_yaw, float
         out->wb_lms[0] = out->wb_lms[1] = out->wb_lms[2] = 1.0f;
     }
     return 0;
+}
+
+int ix_evaluate_gem_optical_metrics_batch(ix_backend* b, const ix_metrics_stone* stones, uint32_t n_stones,
+                                          const ix_metrics_lighting* lighting, const ix_metrics_pose* poses,
+                                          uint32_t n_poses, uint32_t want_fire_and_scintillation,
+                                          ix_gem_metrics* out) {
+    if (!b || b->lost || !stones || !lighting || (!poses && n_poses) || (!out && n_poses) || n_stones == 0)
+        return IX_DECLINED;
+    if (n_poses == 0) return IX_DONE;
+    for (uint32_t s = 0; s < n_stones; ++s)
+        if (!stones[s].planes || stones[s].n_planes == 0 || stones[s].n_planes > IX_MAX_PLANES ||
+            stones[s].dispersion.kind > IX_DISP_CAUCHY)
+            return IX_DECLINED;
+    for (uint32_t p = 0; p < n_poses; ++p)
+        if (poses[p].stone >= n_stones) return IX_DECLINED;
+    ix::MetricsLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    // ExitLighting::new (lighting.rs:137): the preset at exposure 1, no tray, the default
+    // head-shadow cosines; the radiance threshold over the hemisphere median.
+    if (ix_environment_preset(lighting->preset, 1.0f, lighting->light_yaw, lighting->light_pitch, 0.0f, 1.0f,
+                              16.0f, &L.env) != 0)
+        return IX_DECLINED;
+    const bool studio = L.env.model == IX_ENV_STUDIO;
+    L.spec = L.env.spectrum == IX_SPEC_D65 ? d65_host(550.0f) : blackbody(L.env.bb_t_k, L.env.bb_denom_560, 550.0f);
+    L.factor = studio ? 4.0f : 0.5f;
+    L.head_shadow_cos = metrics_head_shadow_cos(studio, lighting->head_shadow_deg);
+    for (int i = 0; i < 96; ++i) {  // hemisphere_direction (lighting.rs:74)
+        const float y = ((float)i + 0.5f) / 96.0f;
+        const float ring = std::sqrt(std::fmax(std::fma(y, -y, 1.0f), 0.0f));
+        const float a = (float)i * 2.3999632f;
+        L.dirs[i][0] = ring * std::cos(a);
+        L.dirs[i][1] = y;
+        L.dirs[i][2] = ring * std::sin(a);
+    }
+    L.want_fire = want_fire_and_scintillation ? 1u : 0u;
+    L.n_poses = n_poses;
+    std::vector<float> planes;
+    std::vector<ix::MetricsStoneDev> dstones(n_stones);
+    for (uint32_t s = 0; s < n_stones; ++s) {
+        dstones[s].plane_offset = (uint32_t)(planes.size() / 4);
+        dstones[s].n_planes = stones[s].n_planes;
+        const double w = solid_width(stones[s].planes, stones[s].n_planes);
+        dstones[s].half_width = (std::isfinite(w) && w > 0.0) ? (float)(w * 0.5) : 1.0f;
+        dstones[s].dispersion = stones[s].dispersion;
+        planes.insert(planes.end(), stones[s].planes, stones[s].planes + 4 * (size_t)stones[s].n_planes);
+    }
+    // camera_view_basis for the pose and its SCINT_TEMPORAL_YAW_OFFSETS_DEG jitters
+    // (camera.rs:15, scintillation.rs:13-40).
+    static const float kOffsets[5] = {-3.0f, -1.5f, 0.0f, 1.5f, 3.0f};
+    std::vector<ix::MetricsPoseDev> dposes(n_poses);
+    for (uint32_t p = 0; p < n_poses; ++p) {
+        dposes[p].stone = poses[p].stone;
+        for (int k = 0; k < 6; ++k) {
+            ix_camera cam;
+            const float yaw = k == 0 ? poses[p].cam_yaw : poses[p].cam_yaw + to_radians(kOffsets[k - 1]);
+            ix_camera_new(yaw, poses[p].cam_pitch, 1.0f, 42.0f, &cam);
+            std::memcpy(dposes[p].basis[k] + 0, cam.forward, 12);
+            std::memcpy(dposes[p].basis[k] + 3, cam.right, 12);
+            std::memcpy(dposes[p].basis[k] + 6, cam.up, 12);
+        }
+    }
+    Turn turn(b);
+    if (fail(b, cudaSetDevice(b->device), "set device")) return IX_DECLINED;
+    float *d_planes = nullptr, *d_out = nullptr;
+    ix::MetricsStoneDev* d_stones = nullptr;
+    ix::MetricsPoseDev* d_poses = nullptr;
+    bool ok = cudaMalloc((void**)&d_planes, planes.size() * sizeof(float)) == cudaSuccess &&
+              cudaMalloc((void**)&d_stones, n_stones * sizeof(ix::MetricsStoneDev)) == cudaSuccess &&
+              cudaMalloc((void**)&d_poses, n_poses * sizeof(ix::MetricsPoseDev)) == cudaSuccess &&
+              cudaMalloc((void**)&d_out, (size_t)n_poses * 5 * sizeof(float)) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(d_planes, planes.data(), planes.size() * sizeof(float), cudaMemcpyHostToDevice,
+                               b->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d_stones, dstones.data(), n_stones * sizeof(ix::MetricsStoneDev), cudaMemcpyHostToDevice,
+                         b->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d_poses, dposes.data(), n_poses * sizeof(ix::MetricsPoseDev), cudaMemcpyHostToDevice,
+                         b->stream) == cudaSuccess;
+    if (ok) {
+        L.planes = reinterpret_cast<const float4*>(d_planes);
+        L.stones = d_stones;
+        L.poses = d_poses;
+        L.out = d_out;
+        cudaError_t e = b->precision == IX_PRECISION_EXACT ? ix::launch_metrics_exact(L, b->stream)
+                                                           : ix::launch_metrics_fast(L, b->stream);
+        ok = !fail(b, e, "metrics launch");
+        std::vector<float> host((size_t)n_poses * 5);
+        ok = ok && !fail(b, cudaMemcpyAsync(host.data(), d_out, host.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                                            b->stream), "metrics download");
+        ok = ok && !fail(b, cudaStreamSynchronize(b->stream), "metrics sync");
+        if (ok)
+            for (uint32_t p = 0; p < n_poses; ++p)
+                out[p] = ix_gem_metrics{host[5 * p], host[5 * p + 1], host[5 * p + 2], host[5 * p + 3],
+                                        host[5 * p + 4]};
+    } else {
+        fail(b, cudaGetLastError(), "metrics buffers");
+    }
+    cudaFree(d_planes);
+    cudaFree(d_stones);
+    cudaFree(d_poses);
+    cudaFree(d_out);
+    return ok ? IX_DONE : IX_DECLINED;
+}
+
+int ix_evaluate_gem_optical_metrics(ix_backend* b, const float* planes, uint32_t n_planes,
+                                    const ix_material* material, float cam_yaw, float cam_pitch,
+                                    const ix_metrics_lighting* lighting, ix_gem_metrics* out) {
+    if (!material) return IX_DECLINED;
+    ix_metrics_stone stone{planes, n_planes, material->dispersion};
+    ix_metrics_pose pose{0, cam_yaw, cam_pitch};
+    return ix_evaluate_gem_optical_metrics_batch(b, &stone, 1, lighting, &pose, 1, 1, out);
 }
 
 void ix_environment_uniform(float radiance, ix_environment* out) {

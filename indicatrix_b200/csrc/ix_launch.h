@@ -122,6 +122,33 @@ struct CheckLaunch {
     uint32_t* out;        // device
 };
 
+// Analytic optical metrics (ix_metrics.cu): one CTA per pose.
+struct MetricsStoneDev {
+    uint32_t plane_offset;  // first float4 of the stone in `planes`
+    uint32_t n_planes;
+    float half_width;       // girdle half-width (fan.rs:34), measured on the host in f64
+    ix_dispersion dispersion;
+};
+struct MetricsPoseDev {
+    uint32_t stone;
+    float basis[6][9];  // forward, right, up of the pose and of its 5 yaw-jittered poses
+};
+struct MetricsLaunch {
+    const float4* planes;          // device
+    const MetricsStoneDev* stones;  // device
+    const MetricsPoseDev* poses;    // device
+    uint32_t n_poses;
+    uint32_t want_fire;             // fire and scintillation rays traced
+    ix_environment env;             // the scoring light: exposure 1, no tray, default shadow
+    float spec;                     // its spectral power at 550 nm
+    float factor;                   // threshold over the median hemisphere radiance
+    float head_shadow_cos;          // observer cone (visibility.rs:16)
+    float dirs[96][3];              // hemisphere probe directions (lighting.rs:74)
+    float* out;                     // device, 5 floats per pose
+};
+cudaError_t launch_metrics_exact(const MetricsLaunch& l, cudaStream_t stream);
+cudaError_t launch_metrics_fast(const MetricsLaunch& l, cudaStream_t stream);
+
 cudaError_t launch_trace_exact(const TraceLaunch& l, cudaStream_t stream);
 cudaError_t launch_trace_fast(const TraceLaunch& l, cudaStream_t stream);
 cudaError_t launch_batch_exact(const BatchLaunch& l, cudaStream_t stream);

@@ -1817,6 +1817,303 @@ static V3 sample_xyz(const ix_scene* sc, uint32_t pixel, const Rot& rot, uint32_
 
 static inline bool xyz_finite(V3 v) { return is_finite_(v.x) && is_finite_(v.y) && is_finite_(v.z); }
 
+// ------------------------------------------------------------------------------------
+// Analytic optical metrics: evaluate_gem_optical_metrics (color/metrics/evaluate.rs:158)
+// and what it calls -- the fan geometry (fan.rs), exit lighting (lighting.rs,
+// visibility.rs), the single-index interior trace (ray_trace.rs), aperture-sample
+// classification and fire (classify.rs), temporal scintillation (scintillation.rs) and
+// the finish (accumulate.rs).  Frosted facets and concave tools are not modelled.
+// ------------------------------------------------------------------------------------
+// f32::to_degrees: a multiply by the f32 rounding of 180/pi.
+static inline F to_degrees(F rad) { return rad * F(57.2957795130823208767981548141051703f); }
+
+// measure_model_width (render_setup/stone_width.rs:27): the narrower of the x and z
+// extents of the solid's vertices, in f64 (planes n.x + d <= 0 as n.x <= -d).
+static double model_width(const float* planes, uint32_t n) {
+    struct P {
+        double x, y, z, m;
+    };
+    std::vector<P> ps;
+    for (uint32_t i = 0; i < n; ++i) {
+        P p{planes[4 * i], planes[4 * i + 1], planes[4 * i + 2], -(double)planes[4 * i + 3]};
+        bool dup = false;
+        for (const P& q : ps) {
+            double c = p.x * q.x + p.y * q.y + p.z * q.z;
+            if (c > 1.0 - 1e-12 && std::fabs(p.m - q.m) < 1e-9) dup = true;
+        }
+        if (!dup) ps.push_back(p);
+    }
+    double x_min = INFINITY, x_max = -INFINITY, z_min = INFINITY, z_max = -INFINITY;
+    size_t count = 0;
+    const size_t m = ps.size();
+    for (size_t a = 0; a < m; ++a)
+        for (size_t b = a + 1; b < m; ++b)
+            for (size_t c = b + 1; c < m; ++c) {
+                const P &A = ps[a], &B = ps[b], &Cc = ps[c];
+                // Cramer: v = (m_a (B x C) + m_b (C x A) + m_c (A x B)) / det.
+                double bcx = B.y * Cc.z - B.z * Cc.y, bcy = B.z * Cc.x - B.x * Cc.z, bcz = B.x * Cc.y - B.y * Cc.x;
+                double det = A.x * bcx + A.y * bcy + A.z * bcz;
+                if (std::fabs(det) < 1e-12) continue;
+                double cax = Cc.y * A.z - Cc.z * A.y, cay = Cc.z * A.x - Cc.x * A.z, caz = Cc.x * A.y - Cc.y * A.x;
+                double abx = A.y * B.z - A.z * B.y, aby = A.z * B.x - A.x * B.z, abz = A.x * B.y - A.y * B.x;
+                double vx = (A.m * bcx + B.m * cax + Cc.m * abx) / det;
+                double vy = (A.m * bcy + B.m * cay + Cc.m * aby) / det;
+                double vz = (A.m * bcz + B.m * caz + Cc.m * abz) / det;
+                bool ok = std::isfinite(vx) && std::isfinite(vy) && std::isfinite(vz);
+                for (size_t k = 0; ok && k < m; ++k)
+                    if (ps[k].x * vx + ps[k].y * vy + ps[k].z * vz - ps[k].m > 1e-9) ok = false;
+                if (!ok) continue;
+                ++count;
+                x_min = std::min(x_min, vx);
+                x_max = std::max(x_max, vx);
+                z_min = std::min(z_min, vz);
+                z_max = std::max(z_max, vz);
+            }
+    if (count < 4) return NAN;
+    double dx = x_max - x_min, dz = z_max - z_min;
+    return dx <= dz ? dx : dz;
+}
+
+// The exit lighting of the metrics (lighting.rs:137-209, visibility.rs:30-58).
+struct MetricLighting {
+    ix_environment env;  // exposure 1, no tray, the default head-shadow cosines
+    F spec;              // spectral power at 550 nm
+    F threshold;
+    F head_shadow_cos;
+};
+static F metric_radiance(const MetricLighting& L, V3 dir) {
+    return lighting_radiance(direction_lighting(L.env, dir, v3(0.0f, 0.0f, 0.0f)), L.env, L.spec);
+}
+// hemisphere_direction (lighting.rs:74).
+static V3 hemisphere_direction(int index) {
+    F y = (F((float)index) + F(0.5f)) / F(96.0f);
+    F ring = sqrt_(max_(fma_(y, -y, 1.0f), 0.0f));
+    F a = F((float)index) * F(2.3999632f);
+    return v3(ring * cos_(a), y, ring * sin_(a));
+}
+static bool metric_lighting(int32_t preset, float light_yaw, float light_pitch, float head_shadow_deg,
+                            MetricLighting* out) {
+    if (ixo_environment_preset(preset, 1.0f, light_yaw, light_pitch, 0.0f, 1.0f, 16.0f, &out->env) != 0)
+        return false;
+    const bool studio = out->env.model == IX_ENV_STUDIO;
+    out->spec = spectral_power(out->env, 550.0f);
+    // head_shadow_cone_cos (visibility.rs:16).
+    if (studio || std::isnan(head_shadow_deg) || head_shadow_deg == 16.0f) {
+        out->head_shadow_cos = 0.96f;
+    } else if (head_shadow_deg <= 0.0f) {
+        out->head_shadow_cos = 2.0f;
+    } else {
+        F offset = acos_(0.96f) - to_radians(16.0f);
+        out->head_shadow_cos = cos_(to_radians(clamp_(head_shadow_deg, 1.0f, 89.0f)) + offset);
+    }
+    // ambient_level: the median of 96 hemisphere radiances (lighting.rs:101).
+    float samples[96];
+    for (int i = 0; i < 96; ++i) samples[i] = raw(metric_radiance(*out, hemisphere_direction(i)));
+    std::sort(samples, samples + 96);
+    F factor = studio ? F(4.0f) : F(0.5f);
+    out->threshold = max_(F(samples[48]) * factor, 1.17549435e-38f);
+    return true;
+}
+
+// The metrics' interior trace at one index (ray_trace.rs:166-352), unfrosted.
+enum { FATE_ENTRY_BLOCKED = 0, FATE_LEAKED = 1, FATE_EXITED_UP = 2, FATE_ABSORBED = 3 };
+struct ExitPath {
+    V3 dir;
+    F transmittance, exit_cos;
+    int facet;
+    uint32_t bounces;
+    F path_len;
+};
+// fresnel_transmittance (ray_trace.rs:35).
+static F fresnel_transmittance(F n1, F n2, F cos_i, F cos_t) {
+    F denom_s = fma_(n2, cos_t, n1 * cos_i);
+    F denom_p = fma_(n2, cos_i, n1 * cos_t);
+    if (abs_(denom_s) < F(1e-6f) || abs_(denom_p) < F(1e-6f)) return 0.0f;
+    F rs = fma_(n2, -cos_t, n1 * cos_i) / denom_s;
+    F rp = fma_(n2, -cos_i, n1 * cos_t) / denom_p;
+    F r = midpoint_(rs * rs, rp * rp);
+    return clamp_(F(1.0f) - r, 0.0f, 1.0f);
+}
+static int trace_entry(const float* planes, uint32_t n, V3 entry_point, V3 incoming, V3 n_entry, F cos_i,
+                       F index, ExitPath* exit) {
+    F inv = F(1.0f) / index;
+    F sin2_t = (F(1.0f) / (index * index)) * fma_(cos_i, -cos_i, 1.0f);
+    if (sin2_t > F(1.0f)) return FATE_ENTRY_BLOCKED;
+    F cos_t = sqrt_(F(1.0f) - sin2_t);
+    V3 dir = normalize(inv * incoming + fma_(inv, cos_i, -cos_t) * n_entry);
+    F entry_t = fresnel_transmittance(1.0f, index, cos_i, cos_t);
+    V3 point = entry_point + dir * F(1e-4f);
+    F sin_crit = F(1.0f) / index;
+    bool leaked = false, up = false;
+    F path_len = 0.0f;
+    for (uint32_t bounce = 0; bounce < 10; ++bounce) {
+        Hit h;
+        if (!intersect(planes, n, Ray{point, dir}, &h)) break;
+        path_len = path_len + h.t;
+        V3 next = point + h.t * dir;
+        V3 n_out = h.normal;
+        F cos_theta = clamp_(dot(dir, n_out), 0.0f, 1.0f);
+        F sin_theta = sqrt_(max_(fma_(cos_theta, -cos_theta, 1.0f), 0.0f));
+        if (sin_theta < sin_crit) {
+            F sin2_out = (index * index) * fma_(cos_theta, -cos_theta, 1.0f);
+            if (sin2_out <= F(1.0f)) {
+                F cos_out = sqrt_(F(1.0f) - sin2_out);
+                V3 out_dir = normalize(index * dir + fma_(index, -cos_theta, cos_out) * n_out);
+                // Escape::record (ray_trace.rs:110).
+                if (n_out.y < F(-0.05f)) {
+                    leaked = true;
+                } else if (out_dir.y > F(0.05f)) {
+                    up = true;
+                    exit->dir = out_dir;
+                    exit->transmittance = fresnel_transmittance(index, 1.0f, cos_theta, cos_out);
+                    exit->exit_cos = cos_out;
+                    exit->facet = h.facet;
+                    exit->bounces = bounce;
+                }
+                break;
+            }
+        }
+        dir = normalize(dir - (F(2.0f) * cos_theta) * n_out);
+        point = next + dir * F(1e-4f);
+    }
+    if (leaked) return FATE_LEAKED;
+    if (up) {
+        exit->transmittance = entry_t * exit->transmittance;
+        exit->path_len = path_len;
+        return FATE_EXITED_UP;
+    }
+    return FATE_ABSORBED;
+}
+
+// The whole-pose evaluation (evaluate.rs:229-392).
+struct MetricStone {
+    const float* planes;
+    uint32_t n;
+    F lateral, standoff;
+    F nd, n_f, n_c;
+};
+static V3 fan_origin(const MetricStone& s, V3 f, V3 r, V3 u, F gu, F gv) {
+    return (-f * s.standoff + (gu * s.lateral) * r) + (gv * s.lateral) * u;
+}
+enum { CLS_NONE = -1, CLS_BLOCKED = 0, CLS_WINDOWED = 1, CLS_EXTINCT = 2, CLS_RETURNED = 3 };
+// classify_aperture_sample + classify_ray + fire_sample (classify.rs:47-190).
+static int classify_aperture(const MetricStone& s, const MetricLighting& L, V3 f, V3 r, V3 u, F gu, F gv,
+                             F sub_r, F sub_u, bool* has_fire, F* fire_angle, F* fire_weight) {
+    *has_fire = false;
+    V3 dir = normalize((f + sub_r * r) + sub_u * u);
+    Ray ray{fan_origin(s, f, r, u, gu, gv), dir};
+    Hit h;
+    if (!intersect(s.planes, s.n, ray, &h)) return CLS_NONE;
+    V3 p = ray.origin + h.t * ray.dir;
+    F cos_i = clamp_(dot(-ray.dir, h.normal), 0.0f, 1.0f);
+    ExitPath ex;
+    int fate = trace_entry(s.planes, s.n, p, ray.dir, h.normal, cos_i, s.nd, &ex);
+    if (fate == FATE_ENTRY_BLOCKED) return CLS_BLOCKED;
+    if (fate == FATE_LEAKED) return CLS_WINDOWED;
+    if (fate == FATE_ABSORBED) return CLS_EXTINCT;
+    // returned_or_reason (visibility.rs:42) with the observer at -forward.
+    if (dot(ex.dir, -f) > L.head_shadow_cos) return CLS_EXTINCT;
+    if (!(metric_radiance(L, ex.dir) > L.threshold)) return CLS_EXTINCT;
+    ExitPath ef, ec;
+    int ff = trace_entry(s.planes, s.n, p, ray.dir, h.normal, cos_i, s.n_f, &ef);
+    int fc = trace_entry(s.planes, s.n, p, ray.dir, h.normal, cos_i, s.n_c, &ec);
+    if (ff == FATE_EXITED_UP && fc == FATE_EXITED_UP && ef.facet == ec.facet && ef.bounces == ec.bounces) {
+        F cos_sep = clamp_(dot(ef.dir, ec.dir), -1.0f, 1.0f);
+        *fire_angle = to_degrees(acos_(cos_sep));
+        F energy = (ex.transmittance * ef.transmittance) * ec.transmittance;
+        F radiance = max_(ef.exit_cos, 0.0f) * max_(ec.exit_cos, 0.0f);
+        *fire_weight = energy * radiance;
+        *has_fire = true;
+    }
+    return CLS_RETURNED;
+}
+// cell_returned_at_yaw_offset (scintillation.rs:85).
+static bool temporal_returned(const MetricStone& s, const MetricLighting& L, const ix_camera& cam, F gu, F gv) {
+    V3 f = load3(cam.forward), r = load3(cam.right), u = load3(cam.up);
+    Ray ray{fan_origin(s, f, r, u, gu, gv), f};
+    Hit h;
+    if (!intersect(s.planes, s.n, ray, &h)) return false;
+    V3 p = ray.origin + h.t * ray.dir;
+    F cos_i = clamp_(dot(-ray.dir, h.normal), 0.0f, 1.0f);
+    ExitPath ex;
+    if (trace_entry(s.planes, s.n, p, ray.dir, h.normal, cos_i, s.nd, &ex) != FATE_EXITED_UP) return false;
+    if (dot(ex.dir, -f) > L.head_shadow_cos) return false;
+    return metric_radiance(L, ex.dir) > L.threshold;
+}
+
+static void evaluate_metrics(const float* planes, uint32_t n, const ix_material& m, F cam_yaw, F cam_pitch,
+                             const MetricLighting& L, float out[5]) {
+    MetricStone s;
+    s.planes = planes;
+    s.n = n;
+    double w = model_width(planes, n);
+    F half_width = (std::isfinite(w) && w > 0.0) ? F((float)(w * 0.5)) : F(1.0f);
+    s.standoff = F(2.5f) * half_width;
+    s.lateral = (F(0.95f) * half_width) / sqrt_(0.70f);
+    s.nd = max_(dispersion_eval(m.dispersion, 589.3f), 1.1f);
+    s.n_f = max_(dispersion_eval(m.dispersion, 486.1f), 1.001f);
+    s.n_c = max_(dispersion_eval(m.dispersion, 656.3f), 1.001f);
+    ix_camera cam;
+    camera_new(cam_yaw, cam_pitch, 1.0f, 42.0f, &cam);
+    const F offsets[5] = {-3.0f, -1.5f, 0.0f, 1.5f, 3.0f};
+    ix_camera tcam[5];
+    for (int k = 0; k < 5; ++k) camera_new(cam_yaw + to_radians(offsets[k]), cam_pitch, 1.0f, 42.0f, &tcam[k]);
+    const F subs[5][2] = {{0.0f, 0.0f}, {0.08f, 0.0f}, {-0.08f, 0.0f}, {0.0f, 0.08f}, {0.0f, -0.08f}};
+    V3 f = load3(cam.forward), r = load3(cam.right), u = load3(cam.up);
+    uint32_t total = 0, windowed = 0, extinct = 0, returned = 0, cells = 0;
+    F fire_sum = 0.0f, frac_sum = 0.0f, frac_sq = 0.0f, tvar_sum = 0.0f;
+    for (int ix = 0; ix < 18; ++ix)
+        for (int iz = 0; iz < 18; ++iz) {
+            F gu = fma_((F((float)ix) + F(0.5f)) / F(18.0f), 2.0f, -1.0f);
+            F gv = fma_((F((float)iz) + F(0.5f)) / F(18.0f), 2.0f, -1.0f);
+            if (fma_(gv, gv, gu * gu) > F(0.70f)) continue;
+            uint32_t cell_total = 0, cell_returned = 0;
+            for (int k = 0; k < 5; ++k) {
+                bool has_fire;
+                F angle, weight;
+                int cls = classify_aperture(s, L, f, r, u, gu, gv, subs[k][0], subs[k][1], &has_fire, &angle, &weight);
+                if (cls == CLS_NONE) continue;
+                ++total;
+                ++cell_total;
+                if (cls == CLS_WINDOWED) ++windowed;
+                else if (cls == CLS_EXTINCT) ++extinct;
+                else if (cls == CLS_RETURNED) {
+                    ++returned;
+                    ++cell_returned;
+                    if (has_fire) fire_sum = fma_(angle, weight, fire_sum);
+                }
+            }
+            if (cell_total > 0) {
+                F frac = F((float)cell_returned) / F((float)cell_total);
+                frac_sum = frac_sum + frac;
+                frac_sq = fma_(frac, frac, frac_sq);
+                ++cells;
+                uint32_t t_ret = 0;
+                for (int k = 0; k < 5; ++k) t_ret += temporal_returned(s, L, tcam[k], gu, gv) ? 1u : 0u;
+                F tp = F((float)t_ret) / F(5.0f);
+                tvar_sum = tvar_sum + fma_(tp, -tp, tp);
+            }
+        }
+    // finish_metrics (accumulate.rs:99).
+    F n_total = F((float)std::max(total, 1u));
+    out[0] = raw(clamp_(F((float)returned) / n_total * F(100.0f), 0.0f, 100.0f));
+    out[1] = raw(max_(fire_sum / n_total * F(275.0f), 0.1f));
+    // spatial / temporal / combined scintillation (scintillation.rs:119-160).
+    F spatial = 0.0f;
+    if (cells > 0) {
+        F mean = frac_sum / F((float)cells);
+        if (mean > F(1e-4f)) {
+            F var = max_(fma_(mean, -mean, frac_sq / F((float)cells)), 0.0f);
+            F cv = sqrt_(var) / mean;
+            spatial = clamp_(cv / (F(1.0f) + cv) * F(100.0f), 0.0f, 100.0f);
+        }
+    }
+    F temporal = cells > 0 ? clamp_(tvar_sum / F((float)cells) / F(0.24f) * F(100.0f), 0.0f, 100.0f) : F(0.0f);
+    out[2] = raw(clamp_(fma_(0.4f, temporal, F(0.6f) * spatial), 0.0f, 100.0f));
+    out[3] = raw(clamp_(F((float)windowed) / n_total * F(100.0f), 0.0f, 100.0f));
+    out[4] = raw(clamp_(F((float)extinct) / n_total * F(100.0f), 0.0f, 100.0f));
+}
+
 }  // namespace ixo
 
 using namespace ixo;
@@ -1957,6 +2254,31 @@ int ixo_environment_preset(int32_t preset, float exposure, float light_yaw, floa
         out->wb_lms[0] = out->wb_lms[1] = out->wb_lms[2] = 1.0f;
     }
     out->uniform_radiance = 0.0f;
+    return 0;
+}
+
+int ixo_metrics(const float* planes, uint32_t n_planes, const ix_material* material, float cam_yaw,
+                float cam_pitch, int32_t preset, float light_yaw, float light_pitch,
+                float head_shadow_deg, float out[5]) {
+    if (!planes || n_planes == 0 || !material) return -1;
+    MetricLighting L;
+    if (!metric_lighting(preset, light_yaw, light_pitch, head_shadow_deg, &L)) return -1;
+    evaluate_metrics(planes, n_planes, *material, cam_yaw, cam_pitch, L, out);
+    return 0;
+}
+
+float ixo_metrics_half_width(const float* planes, uint32_t n_planes) {
+    double w = model_width(planes, n_planes);
+    return (std::isfinite(w) && w > 0.0) ? (float)(w * 0.5) : 1.0f;
+}
+
+int ixo_metrics_lighting(int32_t preset, float light_yaw, float light_pitch, float head_shadow_deg,
+                         float out[3]) {
+    MetricLighting L;
+    if (!metric_lighting(preset, light_yaw, light_pitch, head_shadow_deg, &L)) return -1;
+    out[0] = raw(L.threshold);
+    out[1] = raw(L.head_shadow_cos);
+    out[2] = raw(L.spec);
     return 0;
 }
 

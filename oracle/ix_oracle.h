@@ -90,6 +90,19 @@ int ixo_trace_samples(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixe
  * the reference's fixed test stone, restated in f32 exactly as built there.
  * Writes 74 x {nx, ny, nz, d} (57 facets plus 16 girdle planes and the culet). */
 uint32_t ixo_standard_round_brilliant(float* out);
+/* evaluate_gem_optical_metrics (color/metrics/evaluate.rs:158) for a camera pose and a
+ * lighting preset (LightingPreset index, light yaw/pitch, head-shadow degrees).  Writes
+ * {brilliance_pct, fire_index, scintillation_pct, windowing_pct, extinction_pct}.
+ * Returns 0, or -1 for an unmodelled preset or an empty plane set. */
+int ixo_metrics(const float* planes, uint32_t n_planes, const ix_material* material, float cam_yaw,
+                float cam_pitch, int32_t preset, float light_yaw, float light_pitch,
+                float head_shadow_deg, float out[5]);
+/* Pieces of the metrics setup, for unit checks: the fan's girdle half-width
+ * (fan.rs:34, measure_model_width in f64) and the exit lighting's threshold and
+ * head-shadow cone cosine (lighting.rs:137, visibility.rs:16). */
+float ixo_metrics_half_width(const float* planes, uint32_t n_planes);
+int ixo_metrics_lighting(int32_t preset, float light_yaw, float light_pitch, float head_shadow_deg,
+                         float out[3]);
 /* 1 when this build counts floating-point operations. */
 int ixo_counting_build(void);
 /* Counting build only: trace the given pixels x samples and return the operation tally. */

@@ -102,6 +102,13 @@ def _load(name: str) -> C.CDLL:
                                       C.c_uint32, C.c_uint32, f32p, P(C.c_uint32)]
     lib.ixo_standard_round_brilliant.restype = C.c_uint32
     lib.ixo_standard_round_brilliant.argtypes = [f32p]
+    lib.ixo_metrics.restype = C.c_int
+    lib.ixo_metrics.argtypes = [f32p, C.c_uint32, P(abi.Material), C.c_float, C.c_float, C.c_int32,
+                                C.c_float, C.c_float, C.c_float, f32p]
+    lib.ixo_metrics_half_width.restype = C.c_float
+    lib.ixo_metrics_half_width.argtypes = [f32p, C.c_uint32]
+    lib.ixo_metrics_lighting.restype = C.c_int
+    lib.ixo_metrics_lighting.argtypes = [C.c_int32, C.c_float, C.c_float, C.c_float, f32p]
     lib.ixo_counting_build.restype = C.c_int
     lib.ixo_count_flops.restype = C.c_int
     lib.ixo_count_flops.argtypes = [P(abi.Scene), C.c_uint32, C.c_uint32, C.c_uint32,
@@ -235,4 +242,29 @@ def count_flops(scene: abi.Scene, pixel_begin: int, pixel_end: int, pixel_step: 
                                         sample_offset, spp, C.byref(out))
     if rc != 0:
         raise ValueError("flop counting failed")
+    return out
+
+
+def metrics(planes: np.ndarray, material: abi.Material, cam_yaw: float, cam_pitch: float, preset: int,
+            light_yaw: float, light_pitch: float, head_shadow_deg: float = 16.0) -> np.ndarray:
+    """evaluate_gem_optical_metrics: [brilliance %, fire index, scintillation %,
+    windowing %, extinction %] as float32."""
+    p = np.ascontiguousarray(planes, np.float32)
+    out = np.zeros(5, np.float32)
+    rc = lib().ixo_metrics(_f32p(p), p.shape[0], C.byref(material), cam_yaw, cam_pitch, preset, light_yaw,
+                           light_pitch, head_shadow_deg, _f32p(out))
+    if rc != 0:
+        raise ValueError("metrics: unmodelled preset or empty stone")
+    return out
+
+
+def metrics_half_width(planes: np.ndarray) -> float:
+    p = np.ascontiguousarray(planes, np.float32)
+    return float(lib().ixo_metrics_half_width(_f32p(p), p.shape[0]))
+
+
+def metrics_lighting(preset: int, light_yaw: float, light_pitch: float, head_shadow_deg: float = 16.0):
+    out = np.zeros(3, np.float32)
+    if lib().ixo_metrics_lighting(preset, light_yaw, light_pitch, head_shadow_deg, _f32p(out)) != 0:
+        raise ValueError("unmodelled preset")
     return out

@@ -44,6 +44,8 @@ def test_abi_struct_layout_matches_c():
         "ix_environment": abi.Environment, "ix_scene": abi.Scene,
         "ix_backend_options": abi.BackendOptions, "ix_work_limits": abi.WorkLimits,
         "ix_batch_item": abi.BatchItem, "ix_timing": abi.TimingInfo,
+        "ix_gem_metrics": abi.GemMetrics, "ix_metrics_lighting": abi.MetricsLighting,
+        "ix_metrics_stone": abi.MetricsStone, "ix_metrics_pose": abi.MetricsPose,
     }
     src = ['#include <stdio.h>', '#include <stddef.h>', '#include "ix_cuda.h"', "int main(void){"]
     for cname, py in checks.items():

@@ -89,6 +89,33 @@ def test_golden_sapphire_trace_bits(oracle, idx):
     assert tuple(bits(v) for v in xyz) == GOLDEN_SAPPHIRE[idx]
 
 
+# golden_regression.rs:210-233: evaluate_gem_optical_metrics(standard round brilliant,
+# Diamond, cam yaw 0, cam pitch 0.45, RingLights studio(1.0, 0.85, 0.95)).
+GOLDEN_METRICS = (0x418F4899, 0x40B5EF5A, 0x421FD86A, 0x4213C2DD, 0x423498D6)
+
+
+def test_golden_metrics_bits(oracle):
+    """The analytic metrics (brilliance, fire, scintillation, windowing, extinction) of
+    the reference's golden case, bit for bit: the fan geometry from the f64 girdle width,
+    the exit-lighting median threshold, the 10-bounce single-index traces, fire from the
+    n_F / n_C companions and the spatial + temporal scintillation."""
+    planes = oracle.standard_round_brilliant()
+    assert oracle.metrics_half_width(planes) == 1.0  # girdle radius 1 in this stone
+    m = oracle.metrics(planes, materials.diamond(), 0.0, 0.45, 10, 0.85, 0.95)
+    assert tuple(bits(v) for v in m) == GOLDEN_METRICS
+
+
+def test_metrics_lighting_rules(oracle):
+    """visibility.rs tests: the head-shadow cone is the literal 0.96 for a studio rig or
+    the default size, absent for 0 degrees on a lit (non-rig) model, and follows the size
+    otherwise; the studio threshold is 4x the hemisphere median."""
+    assert bits(oracle.metrics_lighting(10, 0.85, 0.95, 40.0)[1]) == bits(0.96)
+    assert bits(oracle.metrics_lighting(1, 0.85, 0.95, 16.0)[1]) == bits(0.96)
+    assert oracle.metrics_lighting(1, 0.85, 0.95, 0.0)[1] > 1.0
+    off = math.acos(0.96) - math.radians(16.0)
+    assert abs(oracle.metrics_lighting(1, 0.85, 0.95, 30.0)[1] - math.cos(math.radians(30.0) + off)) < 1e-6
+
+
 def test_golden_studio_environment_bits(oracle):
     """golden_regression.rs:172-207: sample_studio_environment(RingLights, exposure 1,
     yaw 0.85, pitch 0.95) at 450/550/650 nm across four directions."""
