@@ -1,8 +1,9 @@
 """Builds ``libix_cuda.so`` in-tree for sm_100a.
 
-The kernel translation unit is compiled twice -- reference-exact rounding
-(``-DIX_EXACT=1 -fmad=false``) and fused rounding (``-DIX_EXACT=0``) -- and linked with
-the C-ABI host code into one shared library beside this file.
+The transport and metrics units are compiled twice -- reference-exact rounding
+(``-DIX_EXACT=1 -fmad=false``) and the fast build (``-DIX_EXACT=0``: contraction,
+approximate divide / square root, denormal flushing) -- and linked with the C-ABI host
+code into one shared library beside this file.
 Run ``python -m indicatrix_b200.build`` or call :func:`build`.
 """
 from __future__ import annotations
@@ -54,9 +55,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
     common = [nvcc, "-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC",
               "--expt-relaxed-constexpr", "-Xptxas", "-v", f"-I{INCLUDE}"]
     jobs = []  # (object, command); the device units compile concurrently
+    # The fused build also takes the approximate divide / square root and flushes
+    # denormals; the slab scan's division stays IEEE (__fdiv_rn) in both builds.
     for unit in ("ix_kernels", "ix_metrics"):
         for variant, flags in (("exact", ["-DIX_EXACT=1", "-fmad=false"]),
-                               ("fast", ["-DIX_EXACT=0", "-fmad=true"])):
+                               ("fast", ["-DIX_EXACT=0", "-fmad=true", "-prec-div=false",
+                                         "-prec-sqrt=false", "-ftz=true"])):
             obj = os.path.join(BUILD_DIR, f"{unit}_{variant}.o")
             jobs.append((obj, common + flags + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj]))
     for unit in ("ix_probe", "ix_noalloc"):

@@ -199,10 +199,26 @@ IX_DEV void group_init(const Group& g, LanePath& P, const DevScene& S, uint32_t 
 // Per-channel physics.
 // ------------------------------------------------------------------------------------
 // tir_phase_delta (refraction/tir.rs:33).
+IX_DEV float tir_tan_half(float n1k, float cos_i, float sin_i) {
+    return (cos_i * sqrtf(fmaxf(fmaf(n1k * n1k * sin_i, sin_i, -1.0f), 0.0f))) /
+           fmaxf(n1k * sin_i * sin_i, 1e-6f);
+}
 IX_DEV float tir_phase_delta(float n1k, float cos_i, float sin_i) {
-    float tan_half = (cos_i * sqrtf(fmaxf(fmaf(n1k * n1k * sin_i, sin_i, -1.0f), 0.0f))) /
-                     fmaxf(n1k * sin_i * sin_i, 1e-6f);
-    return 2.0f * atanf(tan_half);
+    return 2.0f * atanf(tir_tan_half(n1k, cos_i, sin_i));
+}
+// The channel's TIR retarder (tir.rs:98-116, polarization.rs:184).  The fast build forms
+// cos(delta) and sin(delta) of delta = 2 atan(t) without a transcendental:
+// cos = (1 - t^2) / (1 + t^2), sin = 2t / (1 + t^2).
+IX_DEV Stokes tir_retard(const Stokes& s, float n1k, float cos_i, float sin_i) {
+#if IX_EXACT
+    return tir_retard_apply(s, tir_phase_delta(n1k, cos_i, sin_i));
+#else
+    const float t = tir_tan_half(n1k, cos_i, sin_i);
+    const float inv = 1.0f / fmaf(t, t, 1.0f);
+    const float cd = fmaf(-t, t, 1.0f) * inv;
+    const float sd = (2.0f * t) * inv;
+    return Stokes{s.i, s.q, cd * s.u + sd * s.v, (-sd) * s.u + cd * s.v};
+#endif
 }
 IX_DEV void fresnel_rs_rp(float n1, float n2, float cos_i, float cos_t, float& r_s, float& r_p) {
     r_s = fmaf(n2, -cos_t, n1 * cos_i) / fmaf(n2, cos_t, n1 * cos_i);
@@ -271,8 +287,10 @@ IX_DEV void group_exit_probes(const Group& g, LanePath& P, const DevScene& S, co
 // narrow_compat (refraction/context.rs:219) with the hero at channel 0: channel pairs
 // whose directions differ leave each other's MIS family.  `status` is 0 for a channel
 // with no transmitted direction, 1 when its direction matches the hero's, 2 otherwise.
+// The 8-channel shuffle loops here and in group_finish stay rolled: the megakernel is
+// instruction-fetch bound, and rolling them measured 5 % faster than unrolling.
 IX_DEV void group_narrow_compat(const Group& g, LanePath& P, int status, V3 dir_k) {
-#pragma unroll
+#pragma unroll 1
     for (int j = 0; j < 8; ++j) {
         const float dx = gshfl(g, dir_k.x, j), dy = gshfl(g, dir_k.y, j), dz = gshfl(g, dir_k.z, j);
         const int sj = gshfl(g, status, j);
@@ -295,7 +313,7 @@ IX_DEV void group_narrow_compat(const Group& g, LanePath& P, int status, V3 dir_
 // the TIR retarder past the channel's own critical angle, else the Fresnel reflection
 // with its reflectance folded into the channel pdf.
 IX_DEV Stokes lane_scalar_reflect(LanePath& P, float n1k, float n2k, float s2k, float cos_i, float sin_i) {
-    if (s2k > 1.0f) return tir_retard_apply(P.st, tir_phase_delta(n1k, cos_i, sin_i));
+    if (s2k > 1.0f) return tir_retard(P.st, n1k, cos_i, sin_i);
     const float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
     float rs, rp;
     fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, rs, rp);
@@ -326,9 +344,8 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
     if (P.has_prev && length_squared(cpn) > 1e-6f && length_squared(P.prev_pn) > 1e-6f) {
         float cos_psi = clampf_(dot(P.prev_pn, cpn), -1.0f, 1.0f);
         float sin_psi = dot(cross(P.prev_pn, cpn), normalize_or_zero(k_hat));
-        float psi = atan2f(sin_psi, cos_psi);
         float s2, c2;
-        sincosf(2.0f * psi, &s2, &c2);
+        rotation_2psi(sin_psi, cos_psi, c2, s2);
         P.st = rotate(P.st, c2, s2);
     }
     P.has_prev = true;
@@ -346,7 +363,7 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
     const float sin_i = sqrtf(fmaxf(one_m_c2, 0.0f));
     const float n1 = P.inside ? P.n_hero : 1.0f;
     const float n2 = P.inside ? 1.0f : P.n_hero;
-    const float eta = n1 / n2;
+    const float eta = __fdiv_rn(n1, n2);  // IEEE: it decides TIR and the hero's direction
     const float sin2_t = eta * eta * one_m_c2;
     const float n1k = P.inside ? P.n : 1.0f;
     const float n2k = P.inside ? 1.0f : P.n;
@@ -369,11 +386,11 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
         // apply_tir_bounce (tir.rs:98-116) / apply_partial_reflect_bounce
         // (reflect_refract.rs:33): the channel's TIR retarder or Fresnel reflection; a
         // partial reflection divides by the selection probability (TIR scales by 1).
-        const float etak = n1k / n2k;
+        const float etak = __fdiv_rn(n1k, n2k);
         const float s2k = etak * etak * one_m_c2;
         Stokes s;
         if (s2k > 1.0f) {
-            s = tir_retard_apply(P.st, tir_phase_delta(n1k, cos_i, sin_i));
+            s = tir_retard(P.st, n1k, cos_i, sin_i);
         } else {
             float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
             float rs, rp;
@@ -388,9 +405,10 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
         // channel's own Snell direction, transmission and direction match
         // (apply_refract_channel :517, compute_channel_refraction_geometry :255).
         const float sin2_t_dir = fminf(eta * eta * one_m_c2, 1.0f);
-        const float cos_t_dir = sqrtf(fmaxf(1.0f - sin2_t_dir, 0.0f));
-        const V3 final_refr = normalize(eta * k_hat + fmaf(eta, cos_i, -cos_t_dir) * normal);
-        const float ratio = n1k / n2k;
+        // The directions entering the match test take IEEE divide / sqrt (normalize_dir).
+        const float cos_t_dir = __fsqrt_rn(fmaxf(1.0f - sin2_t_dir, 0.0f));
+        const V3 final_refr = normalize_dir(eta * k_hat + fmaf(eta, cos_i, -cos_t_dir) * normal);
+        const float ratio = __fdiv_rn(n1k, n2k);
         const float s2k = (ratio * ratio) * one_m_c2;
         int status = 0;  // 0 channel TIR, 1 direction matches the hero, 2 diverges
         V3 dir_k = v3(0.0f, 0.0f, 0.0f);
@@ -400,8 +418,8 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
             P.st = scale(P.st, 0.0f);
             P.pdf = 0.0f;
         } else {
-            const float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
-            dir_k = normalize(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
+            const float cos_t_k = __fsqrt_rn(fmaxf(1.0f - s2k, 0.0f));
+            dir_k = normalize_dir(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
             status = dot(dir_k, final_refr) >= DIRECTION_MATCH_COS_TOL ? 1 : 2;
             const float two = 2.0f * n1k * cos_i;
             const float t_s = two / fmaf(n2k, cos_t_k, n1k * cos_i);
@@ -474,9 +492,8 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     if (P.has_prev && length_squared(cpn) > 1e-6f && length_squared(P.prev_pn) > 1e-6f) {
         float cos_psi = clampf_(dot(P.prev_pn, cpn), -1.0f, 1.0f);
         float sin_psi = dot(cross(P.prev_pn, cpn), normalize_or_zero(k_hat));
-        float psi = atan2f(sin_psi, cos_psi);
         float s2, c2;
-        sincosf(2.0f * psi, &s2, &c2);
+        rotation_2psi(sin_psi, cos_psi, c2, s2);
         P.st = rotate(P.st, c2, s2);
     }
     P.has_prev = true;
@@ -535,11 +552,11 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     const float n_med_hero = ord_medium ? P.n_hero : n_eff_hero;
     const float n1 = inside0 ? n_med_hero : 1.0f;
     const float n2 = inside0 ? 1.0f : n_med_hero;
-    const float eta = n1 / n2;
+    const float eta = __fdiv_rn(n1, n2);  // IEEE: it decides TIR and the hero's direction
     const float sin2_t = eta * eta * one_m_c2;
     const float n1k = inside0 ? n_med : 1.0f;
     const float n2k = inside0 ? 1.0f : n_med;
-    const float etak = n1k / n2k;
+    const float etak = __fdiv_rn(n1k, n2k);
     const float s2k = etak * etak * one_m_c2;
     const float n_o_hero = P.n_hero;
     const float n_e_hero_c = n_o_hero + mat.birefringence_delta;  // walk-off directions only
@@ -587,9 +604,9 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
             g, clampf_(p_o_raw / fmaxf(p_o_raw + p_e_raw, 1e-12f), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX), 0);
         const bool use_e = unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 1.0f - p_o_hero;
         const float p_frac = use_e ? 1.0f - p_o_hero : p_o_hero;
-        const float e_dir = n1 / (use_e ? n2 : n_o_hero);
-        const float c_dir = sqrtf(fmaxf(1.0f - fminf(e_dir * e_dir * one_m_c2, 1.0f), 0.0f));
-        const V3 refr = normalize(e_dir * k_hat + fmaf(e_dir, cos_i, -c_dir) * normal);
+        const float e_dir = __fdiv_rn(n1, use_e ? n2 : n_o_hero);
+        const float c_dir = __fsqrt_rn(fmaxf(1.0f - fminf(e_dir * e_dir * one_m_c2, 1.0f), 0.0f));
+        const V3 refr = normalize_dir(e_dir * k_hat + fmaf(e_dir, cos_i, -c_dir) * normal);
         const V3 final_refr = use_e ? extraordinary_poynting_dir(refr, c_axis, n_o_hero, n_e_hero_c) : refr;
         if (unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM) < r_branch) {
             const M4 mk = jones_to_mueller(s.r_s[0], s.r_s[1], s.r_p[0], s.r_p[1]);
@@ -599,14 +616,14 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
             new_inside = false;
         } else {
             const float n2k_dir = use_e ? n2k : P.n;
-            const float ratio = n1 / n2k_dir;
+            const float ratio = __fdiv_rn(n1, n2k_dir);
             const float s2 = (ratio * ratio) * one_m_c2;
             if (s2 > 1.0f) {
                 P.st = scale(P.st, 0.0f);
                 P.pdf = 0.0f;
             } else {
-                const float cos_t_k = sqrtf(fmaxf(1.0f - s2, 0.0f));
-                const V3 refr_k = normalize(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
+                const float cos_t_k = __fsqrt_rn(fmaxf(1.0f - s2, 0.0f));
+                const V3 refr_k = normalize_dir(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
                 dir_k = use_e ? extraordinary_poynting_dir(refr_k, c_axis, P.n, P.n + delta_n) : refr_k;
                 status = dot(dir_k, final_refr) >= DIRECTION_MATCH_COS_TOL ? 1 : 2;
                 const float t_unpol = clampf_(1.0f - r_unpol_k, R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
@@ -647,15 +664,15 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
             has_p_o = true;
             p_o_exact = p_o_h;
         } else {
-            const float c_dir = sqrtf(fmaxf(1.0f - fminf(eta * eta * one_m_c2, 1.0f), 0.0f));
-            const V3 hero_refr = normalize(eta * k_hat + fmaf(eta, cos_i, -c_dir) * normal);
+            const float c_dir = __fsqrt_rn(fmaxf(1.0f - fminf(eta * eta * one_m_c2, 1.0f), 0.0f));
+            const V3 hero_refr = normalize_dir(eta * k_hat + fmaf(eta, cos_i, -c_dir) * normal);
             const float original_i = P.st.i;
             if (s2k > 1.0f) {
                 P.st = scale(P.st, 0.0f);
                 P.pdf = 0.0f;
             } else {
-                const float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
-                dir_k = normalize(etak * k_hat + fmaf(etak, cos_i, -cos_t_k) * normal);
+                const float cos_t_k = __fsqrt_rn(fmaxf(1.0f - s2k, 0.0f));
+                dir_k = normalize_dir(etak * k_hat + fmaf(etak, cos_i, -cos_t_k) * normal);
                 status = dot(dir_k, hero_refr) >= DIRECTION_MATCH_COS_TOL ? 1 : 2;
                 float i_unit;
                 const Stokes tr = uniaxial_exit_transmission(sol, r_branch, original_i, i_unit);
@@ -701,21 +718,21 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
                                                  : new_k;
         } else {
             // apply_refract_bounce / apply_refract_channel (reflect_refract.rs:121-591).
-            const float e_dir = n1 / n2s;
-            const float c_dir = sqrtf(fmaxf(1.0f - fminf(e_dir * e_dir * one_m_c2, 1.0f), 0.0f));
-            const V3 refr = normalize(e_dir * k_hat + fmaf(e_dir, cos_i, -c_dir) * normal);
+            const float e_dir = __fdiv_rn(n1, n2s);
+            const float c_dir = __fsqrt_rn(fmaxf(1.0f - fminf(e_dir * e_dir * one_m_c2, 1.0f), 0.0f));
+            const V3 refr = normalize_dir(e_dir * k_hat + fmaf(e_dir, cos_i, -c_dir) * normal);
             const bool walk = entering && use_e;
             const V3 final_refr = walk ? extraordinary_poynting_dir(refr, c_axis, n_o_hero, n_e_hero_c) : refr;
             const float n2k_r = ord_sel ? P.n : n2k;
-            const float ratio = n1k / n2k_r;
+            const float ratio = __fdiv_rn(n1k, n2k_r);
             const float s2r = (ratio * ratio) * one_m_c2;
             const Stokes original = P.st;
             if (s2r > 1.0f) {
                 P.st = scale(P.st, 0.0f);
                 P.pdf = 0.0f;
             } else {
-                const float cos_t_k = sqrtf(fmaxf(1.0f - s2r, 0.0f));
-                const V3 refr_k = normalize(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
+                const float cos_t_k = __fsqrt_rn(fmaxf(1.0f - s2r, 0.0f));
+                const V3 refr_k = normalize_dir(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
                 dir_k = walk ? extraordinary_poynting_dir(refr_k, c_axis, P.n, P.n + delta_n) : refr_k;
                 status = dot(dir_k, final_refr) >= DIRECTION_MATCH_COS_TOL ? 1 : 2;
                 const float two = 2.0f * n1k * cos_i;
@@ -798,7 +815,7 @@ IX_DEV V3 group_finish(const Group& g, const LanePath& P, const DevScene& S, boo
     float family = 0.0f;
     bool first = true;
     const float pdf0 = gshfl(g, P.pdf, 0);
-#pragma unroll
+#pragma unroll 1
     for (int j = 0; j < 8; ++j) {
         const float pj = gshfl(g, P.pdf, j);
         if (P.compat & (1u << j)) {
@@ -813,7 +830,7 @@ IX_DEV V3 group_finish(const Group& g, const LanePath& P, const DevScene& S, boo
     const float cx = c.x * s, cy = c.y * s, cz = c.z * s;
     // xyz += cmf_k * (...), folded in channel order as the reference folds it.
     float x = 0.0f, y = 0.0f, z = 0.0f;
-#pragma unroll
+#pragma unroll 1
     for (int j = 0; j < 8; ++j) {
         x = x + gshfl(g, cx, j);
         y = y + gshfl(g, cy, j);

@@ -63,7 +63,7 @@ IX_DEV V3 extraordinary_poynting_dir(V3 w, V3 c, float n_o, float n_e) {
     float sign = (cos_theta >= 0.0f) ? 1.0f : -1.0f;
     float sd, cd;
     sincosf(delta, &sd, &cd);
-    return normalize(w * cd - (sign * c_proj) * sd);
+    return normalize_dir(w * cd - (sign * c_proj) * sd);  // compared in the match test
 }
 // ordinary_eigen_polarization (uniaxial.rs:95).
 IX_DEV V3 ordinary_eigen_polarization(V3 w, V3 c) {
