@@ -526,10 +526,10 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     float n_eff = P.n, n_eff_hero = P.n_hero;
     if (aniso) {
         // theta_c_for_bounce (geometry.rs:75): two fixed-point steps on entry.
-        float theta;
+        ThetaC theta;
         if (!P.inside) {
             float n_guess = P.n_hero;
-            theta = 0.0f;
+            theta = ThetaC{0.0f, 1.0f};
 #pragma unroll
             for (int it = 0; it < 2; ++it) {
                 const float e = 1.0f / n_guess;
@@ -537,11 +537,11 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
                 if (s2 > 1.0f) break;
                 const float ct = sqrtf(fmaxf(1.0f - s2, 0.0f));
                 const V3 w = normalize(e * k_hat + fmaf(e, cos_i, -ct) * normal);
-                theta = acosf(fabsf(clampf_(dot(w, c_axis), -1.0f, 1.0f)));
+                theta = theta_from_cos(fabsf(clampf_(dot(w, c_axis), -1.0f, 1.0f)));
                 n_guess = effective_extraordinary_index(P.n_hero, P.n_e_hero, theta);
             }
         } else {
-            theta = acosf(fabsf(clampf_(dot(k_hat, c_axis), -1.0f, 1.0f)));
+            theta = theta_from_cos(fabsf(clampf_(dot(k_hat, c_axis), -1.0f, 1.0f)));
         }
         n_eff = effective_extraordinary_index(P.n, P.n_e, theta);
         n_eff_hero = gshfl(g, n_eff, 0);

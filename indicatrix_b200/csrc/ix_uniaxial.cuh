@@ -33,11 +33,30 @@ IX_DEV V3 stable_basis_t(V3 n) {
     V3 a = (fabsf(n.x) > 0.9f) ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
     return normalize_or_zero(a - n * dot(n, a));
 }
+// The angle theta_c between the wave normal and the optic axis, carried as the |cos| it
+// is taken from (geometry.rs:108, :118).  The exact build forms theta = acos(|cos|) and
+// later its sincos as the reference does; the fast build keeps cos and forms
+// sin = sqrt(1 - cos^2) from it (no transcendental).
+struct ThetaC {
+    float theta, cos_abs;
+};
+IX_DEV ThetaC theta_from_cos(float cos_abs) {
+#if IX_EXACT
+    return ThetaC{acosf(cos_abs), cos_abs};
+#else
+    return ThetaC{0.0f, cos_abs};
+#endif
+}
 // effective_extraordinary_index (uniaxial.rs:33).
-IX_DEV float effective_extraordinary_index(float n_o, float n_e, float theta) {
+IX_DEV float effective_extraordinary_index(float n_o, float n_e, ThetaC th) {
     if (fabsf(n_o - n_e) < 1e-5f) return n_o;
     float sin_t, cos_t;
-    sincosf(theta, &sin_t, &cos_t);
+#if IX_EXACT
+    sincosf(th.theta, &sin_t, &cos_t);
+#else
+    cos_t = th.cos_abs;
+    sin_t = sqrtf(fmaxf(fmaf(-cos_t, cos_t, 1.0f), 0.0f));
+#endif
     float ns = n_o * sin_t;
     float denom_sq = fmaf(n_e * cos_t, n_e * cos_t, ns * ns);
     if (denom_sq <= 1e-8f) return n_o;
@@ -101,20 +120,42 @@ IX_DEV Cx cscale(Cx a, float s) { return cx(a.re * s, a.im * s); }
 IX_DEV Cx cconj(Cx a) { return cx(a.re, -a.im); }
 IX_DEV Cx cneg(Cx a) { return csub(cx(0.0f, 0.0f), a); }
 IX_DEV float cnorm2(Cx a) { return fmaf(a.im, a.im, a.re * a.re); }
-// Cplx::div (complex.rs:79).
+// Cplx::div (complex.rs:79).  The fast build takes one reciprocal of the divisor's
+// squared norm for both components.
 IX_DEV Cx cdiv(Cx a, Cx o) {
     float denom = fmaxf(fmaf(o.im, o.im, o.re * o.re), 1e-20f);
+#if IX_EXACT
     return cx(fmaf(a.im, o.im, a.re * o.re) / denom, fmaf(a.re, -o.im, a.im * o.re) / denom);
+#else
+    const float inv = 1.0f / denom;
+    return cx(fmaf(a.im, o.im, a.re * o.re) * inv, fmaf(a.re, -o.im, a.im * o.re) * inv);
+#endif
 }
 // Cplx::sqrt_forward_branch (complex.rs:109): the root with re > 0, or im > 0 when
-// evanescent; a pure negative real takes sqrt(-re) directly.
+// evanescent; a pure negative real takes sqrt(-re) directly.  The exact build forms the
+// polar root as the reference does (|z|^(1/2) at half the atan2 angle); the fast build
+// uses the algebraic principal root, re = sqrt((|z| + x) / 2), im = y / (2 re) (for
+// x < 0 the mirrored form, free of cancellation), which is the same branch: re >= 0 and
+// im with the sign of y.
 IX_DEV Cx csqrt_fwd(Cx a) {
     if (a.im == 0.0f && a.re < 0.0f) return cx(0.0f, sqrtf(-a.re));
+#if IX_EXACT
     float r = sqrtf(sqrtf(cnorm2(a)));
     float theta = atan2f(a.im, a.re) * 0.5f;
     float st, ct;
     sincosf(theta, &st, &ct);
     Cx out = cx(r * ct, r * st);
+#else
+    const float m = sqrtf(cnorm2(a));
+    Cx out;
+    if (a.re >= 0.0f) {
+        const float re = sqrtf(0.5f * (m + a.re));
+        out = cx(re, re > 0.0f ? a.im / (2.0f * re) : 0.0f);
+    } else {
+        const float im = sqrtf(0.5f * (m - a.re));
+        out = cx(fabsf(a.im) / (2.0f * im), copysignf(im, a.im));
+    }
+#endif
     if (out.re < 0.0f) out = cx(-out.re, -out.im);
     if (fabsf(out.re) < 1e-9f && out.im < 0.0f) out = cx(-out.re, -out.im);
     return out;
@@ -261,10 +302,20 @@ IX_DEV void solve4(Cx a[4][4], Cx b[NRHS][4]) {
             }
         }
         const Cx pivot = a[col][col];
+#if IX_EXACT
 #pragma unroll
         for (int j = col; j < 4; ++j) a[col][j] = cdiv(a[col][j], pivot);
 #pragma unroll
         for (int r = 0; r < NRHS; ++r) b[r][col] = cdiv(b[r][col], pivot);
+#else
+        // One complex reciprocal of the pivot scales the whole row.
+        const float inv = 1.0f / fmaxf(cnorm2(pivot), 1e-20f);
+        const Cx rp = cx(pivot.re * inv, -pivot.im * inv);
+#pragma unroll
+        for (int j = col; j < 4; ++j) a[col][j] = cmul(a[col][j], rp);
+#pragma unroll
+        for (int r = 0; r < NRHS; ++r) b[r][col] = cmul(b[r][col], rp);
+#endif
 #pragma unroll
         for (int row = 0; row < 4; ++row) {
             if (row == col) continue;
