@@ -25,6 +25,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "ix_attribution.h"
 #include "ix_scene.h"
 
 #ifdef __cplusplus
@@ -243,6 +244,21 @@ int ix_evaluate_gem_optical_metrics_batch(ix_backend* b, const ix_metrics_stone*
                                           const ix_metrics_lighting* lighting, const ix_metrics_pose* poses,
                                           uint32_t n_poses, uint32_t want_fire_and_scintillation,
                                           ix_gem_metrics* out);
+
+/* ix_accumulate_f64 with spectral attribution: every sample is traced as the plain entry
+ * traces it (the same XYZ bits) with its hero path's events recorded
+ * (trace_spectral_ray_attributed_soa_geom, transport/attributed.rs:28), labelled by
+ * classify_path (color/metrics/attribution.rs:75) under the exit lighting `lighting`
+ * describes -- the preset, light pose and head shadow the scene's environment was built
+ * from -- and added to its pixel's record with AttributionPixel::add
+ * (renderer/attribution_map.rs:105), in ascending sample order.  `attribution` is
+ * caller-owned, width * height records, updated only when the call returns IX_DONE.  A
+ * frame of more than IX_ATTRIBUTION_MAX_PIXELS pixels (or a NULL map) is traced without
+ * attribution (AttributionMap::checked, attribution_map.rs:201).  IX_DECLINED also for a
+ * lighting preset the backend does not model. */
+int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metrics_lighting* lighting,
+                             uint32_t sample_offset, uint32_t spp, double* accum_xyz,
+                             ix_attribution_pixel* attribution, const volatile int32_t* cancel);
 
 /* Per-function check kernels (the GPU equivalence harness's Tier-1/Tier-2 units,
  * renderer/gpu/ulp.rs): evaluates function `fn` (ix::CheckFn numbering) for `n` input

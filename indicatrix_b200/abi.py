@@ -185,6 +185,46 @@ class MetricsLighting(C.Structure):
     ]
 
 
+# Spectral attribution (include/ix_attribution.h): the class slots of
+# renderer/attribution_map.rs:17-36 and the code of a camera ray that missed the stone.
+ATTRIBUTION_CLASSES = 9
+ATTRIBUTION_VERSION = 1
+(CLASS_GLARE, CLASS_WINDOWED, CLASS_RETURNED, CLASS_SHADOW, CLASS_UNLIT, CLASS_SIDE_EXIT,
+ CLASS_NO_INTERSECTION, CLASS_BUDGET, CLASS_KILLED) = range(9)
+CLASS_MISS = 0xFF
+
+
+class AttributionPixel(C.Structure):
+    """AttributionPixel (renderer/attribution_map.rs:80-97), field for field."""
+
+    _fields_ = [
+        ("samples", C.c_uint32),
+        ("hits", C.c_uint32),
+        ("counts", C.c_uint32 * ATTRIBUTION_CLASSES),
+        ("y_sum", C.c_float * ATTRIBUTION_CLASSES),
+        ("y_sq_sum", C.c_float * ATTRIBUTION_CLASSES),
+        ("scattered", C.c_uint32),
+        ("fluoresced", C.c_uint32),
+    ]
+
+
+def attribution_dtype():
+    """The numpy structured dtype of ``ix_attribution_pixel`` (a map is an array of it)."""
+    import numpy as np
+
+    dt = np.dtype([
+        ("samples", "<u4"),
+        ("hits", "<u4"),
+        ("counts", "<u4", (ATTRIBUTION_CLASSES,)),
+        ("y_sum", "<f4", (ATTRIBUTION_CLASSES,)),
+        ("y_sq_sum", "<f4", (ATTRIBUTION_CLASSES,)),
+        ("scattered", "<u4"),
+        ("fluoresced", "<u4"),
+    ])
+    assert dt.itemsize == C.sizeof(AttributionPixel)
+    return dt
+
+
 class MetricsStone(C.Structure):
     _fields_ = [
         ("planes", C.POINTER(C.c_float)),

@@ -99,6 +99,8 @@ def load_library() -> C.CDLL:
         lib.ix_evaluate_gem_optical_metrics_batch.argtypes = [C.c_void_p, P(abi.MetricsStone), C.c_uint32,
                                                               P(abi.MetricsLighting), P(abi.MetricsPose),
                                                               C.c_uint32, C.c_uint32, P(abi.GemMetrics)]
+        lib.ix_accumulate_attributed.argtypes = [C.c_void_p, P(abi.Scene), P(abi.MetricsLighting), C.c_uint32,
+                                                 C.c_uint32, P(C.c_double), C.c_void_p, P(C.c_int32)]
         _lib = lib
         return lib
 
@@ -356,6 +358,32 @@ class GpuBackend:
                                              accum.ctypes.data_as(C.POINTER(C.c_double)), cp)
         else:
             raise TypeError("accum must be float32 or float64")
+        return GpuAccumulate(rc)
+
+    def try_accumulate_attributed(self, scene: FrameScene, lighting: "MetricsLighting", sample_offset: int,
+                                  spp: int, accum: np.ndarray, attribution,
+                                  cancel: Optional[CancelFlag] = None) -> GpuAccumulate:
+        """try_accumulate_cancellable with spectral attribution: ``accum`` (float64) gets
+        the same sums as the plain call and ``attribution`` (an
+        ``attribution.AttributionMap`` of the frame's size) each sample's class and
+        luminance (trace_spectral_ray_attributed_soa_geom + classify_path +
+        AttributionPixel::add).  ``lighting`` is the preset / light pose / head shadow the
+        scene's environment was built from.  Both are added into only on DONE."""
+        self._check_accum(scene, accum)
+        if accum.dtype != np.float64:
+            raise TypeError("accum must be float64")
+        if not self._h:
+            return GpuAccumulate.DECLINED
+        pixels = attribution.pixels if attribution is not None else None
+        if pixels is not None and (pixels.dtype != abi.attribution_dtype() or not pixels.flags.c_contiguous):
+            raise TypeError("attribution pixels must be a contiguous ix_attribution_pixel array")
+        if pixels is not None and pixels.size and pixels.size != scene.width * scene.height:
+            raise ValueError("attribution map must have width * height pixels")
+        sc = scene.to_abi()
+        cp = cancel.pointer() if cancel is not None else None
+        ptr = C.c_void_p(pixels.ctypes.data) if pixels is not None and pixels.size else None
+        rc = self._lib.ix_accumulate_attributed(self._h, C.byref(sc), C.byref(lighting.to_abi()), sample_offset,
+                                                spp, accum.ctypes.data_as(C.POINTER(C.c_double)), ptr, cp)
         return GpuAccumulate(rc)
 
     def try_accumulate(self, scene: FrameScene, sample_offset: int, spp: int,

@@ -48,10 +48,22 @@ struct ix_backend {
     unsigned long long* d_dropped = nullptr;
     uint32_t* d_check = nullptr;
     size_t check_cap = 0;
+    // Spectral attribution: per-sample class / luminance records of one launch and the
+    // frame's attribution map.
+    uint8_t* d_attr_cls = nullptr;
+    size_t attr_cls_cap = 0;
+    float* d_attr_y = nullptr;
+    size_t attr_y_cap = 0;
+    ix_attribution_pixel* d_attr_map = nullptr;
+    size_t attr_map_cap = 0;
+    ix_attribution_pixel* h_attr_map = nullptr;
+    size_t hattr_map_cap = 0;
     int sm_count = 0;
     uint32_t variant = 0;
     // Resident CTAs per SM by [uniaxial instantiation][variant].
     int bps_exact[2][3] = {{1, 1, 1}, {1, 1, 1}}, bps_fast[2][3] = {{1, 1, 1}, {1, 1, 1}};
+    // ... and of the attributed trace kernels by [uniaxial instantiation].
+    int bps_attr_exact[2] = {1, 1}, bps_attr_fast[2] = {1, 1};
     std::string label;
     // State.
     bool lost = false;
@@ -125,12 +137,24 @@ uint32_t pixels_per_task(uint32_t spp) {
     return std::max(1u, std::min(8u, ppt));
 }
 
+// The chunking of enqueue_frame: a TDR-safe first launch of at most 1M paths
+// (gpu/frame/mod.rs:355-361), then launches of `chunk_paths` (default 64M paths), whole
+// pixels each.
+uint64_t chunk_budget(const ix_backend* b, int launch_index) {
+    const uint64_t first_budget = 1u << 20;
+    const uint64_t budget = b->chunk_paths ? b->chunk_paths : (64ull << 20);
+    return launch_index == 0 ? std::min(first_budget, budget) : budget;
+}
+
 // Enqueue the trace launches for pixels [0, n_pixels) of `sc` (device planes) into
-// d_out; chunked so no single launch exceeds the path budget.  Returns the launch count
-// or -1 on a CUDA error (b->last_error set).
+// d_out; chunked so no single launch exceeds the path budget.  With `attr`, every launch
+// is the attributed trace kernel, followed by the fold of its records into d_map (the
+// frame's attribution map on the device).  Returns the launch count or -1 on a CUDA
+// error (b->last_error set).
 int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uint32_t spp,
                   double* d_out, int accumulate, cudaStream_t stream,
-                  const volatile int32_t* cancel, bool* cancelled) {
+                  const volatile int32_t* cancel, bool* cancelled,
+                  const ix::AttrLaunch* attr = nullptr, ix_attribution_pixel* d_map = nullptr) {
     const uint32_t n_pixels = sc.width * sc.height;
     const bool exact = b->precision == IX_PRECISION_EXACT;
     ix::TraceLaunch L;
@@ -147,11 +171,8 @@ int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uin
     L.variant = (int)b->variant;
     const int uni = ix::needs_uniaxial_kernel(L.flags) ? 1 : 0;
     L.blocks = b->sm_count * (exact ? b->bps_exact[uni][b->variant] : b->bps_fast[uni][b->variant]);
+    if (attr) L.blocks = b->sm_count * (exact ? b->bps_attr_exact[uni] : b->bps_attr_fast[uni]);
     if (L.blocks <= 0) L.blocks = b->sm_count > 0 ? b->sm_count : 1;
-    // Chunking: a TDR-safe first launch of at most 1M paths (gpu/frame/mod.rs:355-361),
-    // then launches of `chunk_paths` (default 64M paths), whole pixels each.
-    const uint64_t first_budget = 1u << 20;
-    const uint64_t budget = b->chunk_paths ? b->chunk_paths : (64ull << 20);
     uint32_t begin = 0;
     int launches = 0;
     while (begin < n_pixels) {
@@ -159,14 +180,22 @@ int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uin
             *cancelled = true;
             return launches;
         }
-        uint64_t paths = launches == 0 ? std::min(first_budget, budget) : budget;
-        uint64_t px = std::max<uint64_t>(1, paths / std::max<uint32_t>(spp, 1));
+        uint64_t px = std::max<uint64_t>(1, chunk_budget(b, launches) / std::max<uint32_t>(spp, 1));
         uint32_t n = (uint32_t)std::min<uint64_t>(px, n_pixels - begin);
         L.pixel_begin = begin;
         L.n_pixels = n;
         L.out = d_out + (size_t)begin * 3;
-        cudaError_t e = exact ? ix::launch_trace_exact(L, stream) : ix::launch_trace_fast(L, stream);
-        if (fail(b, e, "trace launch")) return -1;
+        if (attr) {
+            cudaError_t e = exact ? ix::launch_trace_attributed_exact(L, *attr, stream)
+                                  : ix::launch_trace_attributed_fast(L, *attr, stream);
+            if (fail(b, e, "attributed trace launch")) return -1;
+            const ix::AttrFoldLaunch F{attr->cls, attr->y, d_map + begin, n, spp};
+            e = exact ? ix::launch_attribution_fold_exact(F, stream) : ix::launch_attribution_fold_fast(F, stream);
+            if (fail(b, e, "attribution fold")) return -1;
+        } else {
+            cudaError_t e = exact ? ix::launch_trace_exact(L, stream) : ix::launch_trace_fast(L, stream);
+            if (fail(b, e, "trace launch")) return -1;
+        }
         ++launches;
         begin += n;
     }
@@ -377,6 +406,30 @@ float metrics_head_shadow_cos(bool studio, float deg) {
     return std::cos(to_radians(c) + offset);
 }
 
+// ExitLighting::new (lighting.rs:137) for a lighting preset: the preset at exposure 1, no
+// tray and the default head-shadow edges, its spectral power at 550 nm, the threshold
+// factor over the median hemisphere radiance, the observer cone and the 96 hemisphere
+// probe directions (hemisphere_direction, lighting.rs:74).  False for an unmodelled preset.
+bool exit_lighting_setup(const ix_metrics_lighting& lighting, ix_environment* env, float* spec, float* factor,
+                         float* head_shadow_cos, float dirs[96][3]) {
+    if (ix_environment_preset(lighting.preset, 1.0f, lighting.light_yaw, lighting.light_pitch, 0.0f, 1.0f, 16.0f,
+                              env) != 0)
+        return false;
+    const bool studio = env->model == IX_ENV_STUDIO;
+    *spec = env->spectrum == IX_SPEC_D65 ? d65_host(550.0f) : blackbody(env->bb_t_k, env->bb_denom_560, 550.0f);
+    *factor = studio ? 4.0f : 0.5f;
+    *head_shadow_cos = metrics_head_shadow_cos(studio, lighting.head_shadow_deg);
+    for (int i = 0; i < 96; ++i) {
+        const float y = ((float)i + 0.5f) / 96.0f;
+        const float ring = std::sqrt(std::fmax(std::fma(y, -y, 1.0f), 0.0f));
+        const float a = (float)i * 2.3999632f;
+        dirs[i][0] = ring * std::cos(a);
+        dirs[i][1] = y;
+        dirs[i][2] = ring * std::sin(a);
+    }
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -417,6 +470,10 @@ ix_backend* ix_backend_create(const ix_backend_options* opts) {
             b->bps_exact[u][v] = std::max(1, ix::trace_blocks_per_sm_exact((int)b->threads, v, u, nullptr));
             b->bps_fast[u][v] = std::max(1, ix::trace_blocks_per_sm_fast((int)b->threads, v, u, nullptr));
         }
+    for (int u = 0; u < 2; ++u) {
+        b->bps_attr_exact[u] = std::max(1, ix::trace_attributed_blocks_per_sm_exact((int)b->threads, u));
+        b->bps_attr_fast[u] = std::max(1, ix::trace_attributed_blocks_per_sm_fast((int)b->threads, u));
+    }
     // Option 0 = the measured default (8 CTAs per SM); 1/2/3 = unconstrained / 6 / 8.
     b->variant = 2;
     if (opts && opts->kernel_variant >= 1 && opts->kernel_variant <= 3) b->variant = opts->kernel_variant - 1;
@@ -432,6 +489,10 @@ void ix_backend_destroy(ix_backend* b) {
     cudaFree(b->d_counter);
     cudaFree(b->d_dropped);
     cudaFree(b->d_check);
+    cudaFree(b->d_attr_cls);
+    cudaFree(b->d_attr_y);
+    cudaFree(b->d_attr_map);
+    if (b->h_attr_map) cudaFreeHost(b->h_attr_map);
     if (b->h_sums) cudaFreeHost(b->h_sums);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -482,6 +543,88 @@ int ix_accumulate(ix_backend* b, const ix_scene* scene, uint32_t sample_offset, 
 int ix_accumulate_f64(ix_backend* b, const ix_scene* scene, uint32_t sample_offset,
                       uint32_t spp, double* accum_xyz, const volatile int32_t* cancel) {
     return accumulate_impl<double>(b, scene, sample_offset, spp, accum_xyz, cancel);
+}
+
+int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metrics_lighting* lighting,
+                             uint32_t sample_offset, uint32_t spp, double* accum_xyz,
+                             ix_attribution_pixel* attribution, const volatile int32_t* cancel) {
+    if (!b || !scene || !accum_xyz || !lighting) return IX_DECLINED;
+    const uint64_t n_pixels = (uint64_t)scene->width * scene->height;
+    // AttributionMap::checked (attribution_map.rs:201): a map of more than
+    // MAX_DIAGNOSTIC_PIXELS pixels accepts no sample; the frame is still traced.
+    if (!attribution || n_pixels > IX_ATTRIBUTION_MAX_PIXELS)
+        return accumulate_impl<double>(b, scene, sample_offset, spp, accum_xyz, cancel);
+    if (b->lost) return IX_DECLINED;
+    if (!ix_scene_routes_to_gpu(scene)) return IX_DECLINED;
+    if (b->limits.max_pixels && n_pixels > b->limits.max_pixels) return IX_DECLINED;
+    if (b->limits.max_spp && spp > b->limits.max_spp) return IX_DECLINED;
+    if (b->limits.max_paths_per_call && n_pixels * spp > b->limits.max_paths_per_call) return IX_DECLINED;
+    ix::AttrLaunch A;
+    std::memset(&A, 0, sizeof(A));
+    if (!exit_lighting_setup(*lighting, &A.env, &A.spec, &A.factor, &A.head_shadow_cos, A.dirs)) return IX_DECLINED;
+    if (cancel && *cancel) return IX_CANCELLED;
+    if (n_pixels == 0 || spp == 0) return IX_DONE;
+    // The records of the largest launch: whole pixels of at most max(budget, spp) paths.
+    const uint64_t max_budget = std::max(chunk_budget(b, 0), chunk_budget(b, 1));
+    const size_t records = (size_t)std::min<uint64_t>(n_pixels * spp, std::max<uint64_t>(max_budget, spp));
+    Turn turn(b);
+    if (fail(b, cudaSetDevice(b->device), "set device")) return IX_DECLINED;
+    if (fail(b, grow_device(&b->d_planes, &b->planes_cap, (size_t)scene->n_planes * 4), "planes alloc") ||
+        fail(b, grow_device(&b->d_sums, &b->sums_cap, (size_t)n_pixels * 3), "sums alloc") ||
+        fail(b, grow_pinned(&b->h_sums, &b->hsums_cap, (size_t)n_pixels * 3), "host alloc") ||
+        fail(b, grow_device(&b->d_attr_cls, &b->attr_cls_cap, records), "attribution alloc") ||
+        fail(b, grow_device(&b->d_attr_y, &b->attr_y_cap, records), "attribution alloc") ||
+        fail(b, grow_device(&b->d_attr_map, &b->attr_map_cap, (size_t)n_pixels), "attribution alloc") ||
+        fail(b, grow_pinned(&b->h_attr_map, &b->hattr_map_cap, (size_t)n_pixels), "attribution host alloc"))
+        return IX_DECLINED;
+    const size_t map_bytes = (size_t)n_pixels * sizeof(ix_attribution_pixel);
+    std::memcpy(b->h_attr_map, attribution, map_bytes);
+    if (scene->n_planes &&
+        fail(b, cudaMemcpyAsync(b->d_planes, scene->planes, (size_t)scene->n_planes * 16,
+                                cudaMemcpyHostToDevice, b->stream), "planes upload"))
+        return IX_DECLINED;
+    if (fail(b, cudaMemcpyAsync(b->d_attr_map, b->h_attr_map, map_bytes, cudaMemcpyHostToDevice, b->stream),
+             "attribution upload") ||
+        fail(b, cudaMemsetAsync(b->d_dropped, 0, sizeof(unsigned long long), b->stream), "reset"))
+        return IX_DECLINED;
+    ix_scene sc = *scene;
+    sc.planes = b->d_planes;
+    sc.facet_finishes = nullptr;
+    sc.n_finishes = 0;
+    A.cls = b->d_attr_cls;
+    A.y = b->d_attr_y;
+    bool cancelled = false;
+    if (fail(b, cudaEventRecord(b->ev0, b->stream), "event")) return IX_DECLINED;
+    const int launches =
+        enqueue_frame(b, sc, sample_offset, spp, b->d_sums, 0, b->stream, cancel, &cancelled, &A, b->d_attr_map);
+    if (launches < 0) return IX_DECLINED;
+    if (fail(b, cudaEventRecord(b->ev1, b->stream), "event")) return IX_DECLINED;
+    if (cancelled) {
+        cudaStreamSynchronize(b->stream);
+        return IX_CANCELLED;
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    unsigned long long dropped = 0;
+    if (fail(b, cudaMemcpyAsync(b->h_sums, b->d_sums, (size_t)n_pixels * 3 * sizeof(double),
+                                cudaMemcpyDeviceToHost, b->stream), "sums download") ||
+        fail(b, cudaMemcpyAsync(b->h_attr_map, b->d_attr_map, map_bytes, cudaMemcpyDeviceToHost, b->stream),
+             "attribution download") ||
+        fail(b, cudaMemcpyAsync(&dropped, b->d_dropped, sizeof(dropped), cudaMemcpyDeviceToHost, b->stream),
+             "dropped download"))
+        return IX_DECLINED;
+    if (fail(b, cudaStreamSynchronize(b->stream), "attributed trace")) return IX_DECLINED;
+    if (cancel && *cancel) return IX_CANCELLED;
+    for (size_t i = 0; i < (size_t)n_pixels * 3; ++i) accum_xyz[i] += b->h_sums[i];
+    std::memcpy(attribution, b->h_attr_map, map_bytes);
+    auto t1 = std::chrono::steady_clock::now();
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->timing.kernel_ms = ms;
+    b->timing.reduce_ms = std::chrono::duration<float, std::milli>(t1 - t0).count();
+    b->timing.paths = n_pixels * spp;
+    b->timing.launches = (uint32_t)launches;
+    b->dropped = dropped;
+    return IX_DONE;
 }
 
 }  // extern "C"
@@ -926,23 +1069,7 @@ int ix_evaluate_gem_optical_metrics_batch(ix_backend* b, const ix_metrics_stone*
         if (poses[p].stone >= n_stones) return IX_DECLINED;
     ix::MetricsLaunch L;
     std::memset(&L, 0, sizeof(L));
-    // ExitLighting::new (lighting.rs:137): the preset at exposure 1, no tray, the default
-    // head-shadow cosines; the radiance threshold over the hemisphere median.
-    if (ix_environment_preset(lighting->preset, 1.0f, lighting->light_yaw, lighting->light_pitch, 0.0f, 1.0f,
-                              16.0f, &L.env) != 0)
-        return IX_DECLINED;
-    const bool studio = L.env.model == IX_ENV_STUDIO;
-    L.spec = L.env.spectrum == IX_SPEC_D65 ? d65_host(550.0f) : blackbody(L.env.bb_t_k, L.env.bb_denom_560, 550.0f);
-    L.factor = studio ? 4.0f : 0.5f;
-    L.head_shadow_cos = metrics_head_shadow_cos(studio, lighting->head_shadow_deg);
-    for (int i = 0; i < 96; ++i) {  // hemisphere_direction (lighting.rs:74)
-        const float y = ((float)i + 0.5f) / 96.0f;
-        const float ring = std::sqrt(std::fmax(std::fma(y, -y, 1.0f), 0.0f));
-        const float a = (float)i * 2.3999632f;
-        L.dirs[i][0] = ring * std::cos(a);
-        L.dirs[i][1] = y;
-        L.dirs[i][2] = ring * std::sin(a);
-    }
+    if (!exit_lighting_setup(*lighting, &L.env, &L.spec, &L.factor, &L.head_shadow_cos, L.dirs)) return IX_DECLINED;
     L.want_fire = want_fire_and_scintillation ? 1u : 0u;
     L.n_poses = n_poses;
     std::vector<float> planes;

@@ -480,6 +480,52 @@ IX_DEV float lighting_radiance(const Lighting& L, const ix_environment& env, flo
     return r;
 }
 
+// ExitLighting (color/metrics/lighting.rs:137-209) and returned_or_reason
+// (visibility.rs:55): the metrics' verdict on a direction leaving the stone.  `env` is the
+// scoring environment (the preset at exposure 1, no tray), `spec` its 550 nm power.
+struct ExitScorer {
+    const ix_environment& env;
+    float spec, threshold, head_shadow_cos;
+    // is_illuminated (lighting.rs:207): the scoring light's radiance along `dir`.
+    IX_DEV bool lit(V3 dir) const {
+        return lighting_radiance(direction_lighting(env, dir, v3(0.0f, 0.0f, 0.0f)), env, spec) > threshold;
+    }
+    // Exits closer to the eye than the head-shadow cone are lost to the observer.
+    IX_DEV bool shadowed(V3 exit_dir, V3 observer) const { return dot(exit_dir, observer) > head_shadow_cos; }
+    // ray_is_visibly_returned (visibility.rs:78) for an observer at -forward.
+    IX_DEV bool returned(V3 exit_dir, V3 forward) const {
+        if (shadowed(exit_dir, -forward)) return false;
+        return lit(exit_dir);
+    }
+};
+
+// ambient_level (lighting.rs:101) scaled by SOURCE_OVER_AMBIENT or
+// UNIFORM_FRACTION_OF_AMBIENT (`factor`) and floored at the least positive normal
+// (lighting.rs:186): the median of the radiances along the 96 hemisphere directions.
+// Block-wide: every thread of the block calls it; `s_rad` is 96 floats of shared memory.
+IX_DEV float exit_lighting_threshold(const ix_environment& env, float spec, float factor, const float (*dirs)[3],
+                                     float* s_rad, float* s_threshold) {
+    for (int i = threadIdx.x; i < 96; i += blockDim.x) {
+        const V3 d = v3(dirs[i][0], dirs[i][1], dirs[i][2]);
+        s_rad[i] = lighting_radiance(direction_lighting(env, d, v3(0.0f, 0.0f, 0.0f)), env, spec);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < 96; ++i) {  // insertion sort, ascending
+            const float v = s_rad[i];
+            int j = i - 1;
+            while (j >= 0 && s_rad[j] > v) {
+                s_rad[j + 1] = s_rad[j];
+                --j;
+            }
+            s_rad[j + 1] = v;
+        }
+        *s_threshold = fmaxf(s_rad[48] * factor, 1.17549435e-38f);
+    }
+    __syncthreads();
+    return *s_threshold;
+}
+
 // ------------------------------------------------------------------------------------
 // Convex slab intersection over the CTA's shared-memory plane cache
 // (simd/slab.rs:120-160; intersect.rs:101-127).

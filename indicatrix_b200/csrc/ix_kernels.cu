@@ -43,13 +43,55 @@ constexpr int UNI_MINB_2 = 4;
 
 typedef double PartSlot[TRACE_MAX_PPT][GROUPS_PER_WARP][3];
 
+// What the attributed kernels record of a path (PathEvents, transport/path_events.rs:27),
+// reduced to what classify_path reads: group-uniform bits plus the first exit direction.
+enum : uint32_t {
+    EV_FACET = 1u,      // a facet event happened (first_facet is Some)
+    EV_ENTERED = 2u,    // ... and the first one left the ray inside the stone
+    EV_EXITED = 4u,     // an inside-to-outside transition happened (first_exit is Some)
+    EV_WINDOWED = 8u,   // ... through a facet whose outward normal has y < -0.05
+    EV_ROULETTE = 16u,  // the loop stopped by Russian roulette
+    EV_ESCAPED = 32u,   // the loop stopped because the ray met no facet
+};
+
+// Where a task's attribution records go: record (s, pixel0 + j) of the launch is at
+// s * stride + pixel0 + j.
+struct AttrTask {
+    const ExitScorer* scorer;
+    uint8_t* cls;
+    float* y;
+    uint32_t stride;  // the launch's pixel count
+    uint32_t pixel0;  // the task's first pixel within the launch
+};
+
+// classify_path (color/metrics/attribution.rs:75-98) through class_index
+// (renderer/attribution_map.rs:39-58).  A path that never exited is labelled by how it
+// stopped (unexited_reason, attribution.rs:57): roulette, the bounce cap, or an escape.
+IX_DEV uint32_t classify_path(uint32_t ev, V3 exit_dir, V3 observer, const ExitScorer& sc) {
+    if (!(ev & EV_FACET)) return IX_CLASS_MISS;
+    if (!(ev & EV_ENTERED)) return IX_CLASS_GLARE;
+    if (!(ev & EV_EXITED)) {
+        if (ev & EV_ROULETTE) return IX_CLASS_KILLED;
+        return (ev & EV_ESCAPED) ? IX_CLASS_NO_INTERSECTION : IX_CLASS_BUDGET;
+    }
+    if (ev & EV_WINDOWED) return IX_CLASS_WINDOWED;
+    if (exit_dir.y > 0.05f) {
+        if (sc.shadowed(exit_dir, observer)) return IX_CLASS_SHADOW;
+        return sc.lit(exit_dir) ? IX_CLASS_RETURNED : IX_CLASS_UNLIT;
+    }
+    return IX_CLASS_SIDE_EXIT;
+}
+
 // One warp task: pixels [pixel0, pixel0 + npix) x samples [sample_offset, +spp), written
 // to out[0 .. 3 npix).  Returns the number of non-finite samples this lane dropped.
-// UNI selects the transport instantiation (isotropic megakernel, or the uniaxial one).
-template <bool UNI>
+// UNI selects the transport instantiation (isotropic megakernel, or the uniaxial one);
+// ATTR adds the event record of each path and writes its class and luminance to `at`
+// (the traced arithmetic is the same: the record only reads the path state).
+template <bool UNI, bool ATTR = false>
 IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const float4* __restrict__ planes,
                                      uint32_t pixel0, uint32_t npix, uint32_t spp,
-                                     uint32_t sample_offset, PartSlot& part, double* out, int accumulate) {
+                                     uint32_t sample_offset, PartSlot& part, double* out, int accumulate,
+                                     const AttrTask* at = nullptr) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t gi = lane >> 3;
     const uint32_t total = npix * spp;
@@ -67,6 +109,8 @@ IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const fl
     uint32_t cur_j = active ? q / spp : 0;
     double ax = 0.0, ay = 0.0, az = 0.0;
     LanePath P;
+    uint32_t ev = 0;  // ATTR: the path's event bits
+    V3 exit_dir = v3(0.0f, 0.0f, 0.0f);
     while (__any_sync(0xFFFFFFFFu, active)) {
         if (!active) continue;
         // One setup site for the first path and every regenerated one keeps a single
@@ -74,12 +118,35 @@ IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const fl
         if (fresh) {
             group_init<UNI>(g, P, S, pixel0 + cur_j, sample_offset + (q - cur_j * spp));
             fresh = false;
+            ev = 0;
         }
         float esc = 0.0f;
-        const int r = (P.bounce >= max_bounces) ? (int)BOUNCE_KILLED : group_step<UNI>(g, P, S, planes, esc);
+        const bool capped = P.bounce >= max_bounces;
+        const bool inside_before = P.inside;
+        const int r = capped ? (int)BOUNCE_KILLED : group_step<UNI>(g, P, S, planes, esc);
+        if constexpr (ATTR) {
+            // record_facet (bounce_body.rs:680) runs after every facet dispatch, before
+            // the roulette that may end the path; a miss records no facet event.
+            if (!capped && r != BOUNCE_ESCAPED) {
+                if (!(ev & EV_FACET)) ev |= EV_FACET | (P.inside ? EV_ENTERED : 0u);
+                if (inside_before && !P.inside && !(ev & EV_EXITED)) {
+                    ev |= EV_EXITED | (planes[P.facet].y < -0.05f ? EV_WINDOWED : 0u);
+                    exit_dir = P.d;
+                }
+            }
+            if (r == BOUNCE_ESCAPED) ev |= EV_ESCAPED;
+            if (r == BOUNCE_KILLED && !capped) ev |= EV_ROULETTE;
+        }
         if (r == BOUNCE_CONTINUE && P.bounce < max_bounces) continue;
         // The path finished (escaped, roulette, or reached the bounce cap).
         const V3 xyz = group_finish(g, P, S, r == BOUNCE_ESCAPED, esc);
+        if constexpr (ATTR) {
+            if (g.c == 0) {
+                const size_t rec = (size_t)(q - cur_j * spp) * at->stride + at->pixel0 + cur_j;
+                at->cls[rec] = (uint8_t)classify_path(ev, exit_dir, P.observer, *at->scorer);
+                at->y[rec] = xyz.y;
+            }
+        }
         if (isfinite(xyz.x) && isfinite(xyz.y) && isfinite(xyz.z)) {
             ax += (double)xyz.x;
             ay += (double)xyz.y;
@@ -155,6 +222,70 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_c
                                  s_part[threadIdx.x >> 5], L.out + (size_t)local0 * 3, L.accumulate);
     }
     if (drops && L.dropped) atomicAdd(L.dropped, drops);
+}
+
+// The trace kernel with spectral attribution: the same task loop, and each path's
+// class code and luminance recorded for the fold.  Each CTA first derives the exit
+// lighting's threshold (96 radiances and their median), which the classes are judged by.
+template <int MINB, bool UNI>
+__global__ void __launch_bounds__(128, MINB)
+    IX_SFX(trace_attributed_kernel)(const __grid_constant__ TraceLaunch L, const __grid_constant__ AttrLaunch A) {
+    __shared__ float4 s_planes[IX_MAX_PLANES];
+    __shared__ PartSlot s_part[WARPS_PER_CTA];
+    __shared__ float s_rad[96];
+    __shared__ float s_threshold;
+    const float4* gplanes = reinterpret_cast<const float4*>(L.scene.planes);
+    for (uint32_t i = threadIdx.x; i < L.scene.n_planes; i += blockDim.x) s_planes[i] = gplanes[i];
+    // Its barriers also publish the plane cache.
+    const float threshold = exit_lighting_threshold(A.env, A.spec, A.factor, A.dirs, s_rad, &s_threshold);
+    const ExitScorer scorer{A.env, A.spec, threshold, A.head_shadow_cos};
+    const DevScene S = make_scene(L.scene, L.flags);
+    const Group g = make_group();
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t ppt = L.pixels_per_task;
+    const uint32_t n_tasks = (L.n_pixels + ppt - 1) / ppt;
+    unsigned long long drops = 0;
+    for (;;) {
+        uint32_t task = 0;
+        if (lane == 0) task = atomicAdd(L.task_counter, 1u);
+        task = __shfl_sync(0xFFFFFFFFu, task, 0);
+        if (task >= n_tasks) break;
+        const uint32_t local0 = task * ppt;
+        const uint32_t npix = min(ppt, L.n_pixels - local0);
+        const AttrTask at{&scorer, A.cls, A.y, L.n_pixels, local0};
+        drops += trace_task<UNI, true>(g, S, s_planes, L.pixel_begin + local0, npix, L.spp, L.sample_offset,
+                                       s_part[threadIdx.x >> 5], L.out + (size_t)local0 * 3, L.accumulate, &at);
+    }
+    if (drops && L.dropped) atomicAdd(L.dropped, drops);
+}
+
+// AttributionPixel::add (renderer/attribution_map.rs:105-120), one thread per pixel, the
+// launch's samples in ascending order: the f32 sums are formed exactly as the reference
+// forms them (rounded adds and multiplies, no contraction), and the counts saturate.
+__global__ void __launch_bounds__(128) IX_SFX(attribution_fold_kernel)(const __grid_constant__ AttrFoldLaunch L) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= L.n_pixels) return;
+    ix_attribution_pixel a = L.map[p];
+    auto sat = [](uint32_t v) { return v == 0xFFFFFFFFu ? v : v + 1u; };
+    for (uint32_t s = 0; s < L.spp; ++s) {
+        const size_t rec = (size_t)s * L.n_pixels + p;
+        const uint32_t c = L.cls[rec];
+        const float y = L.y[rec];
+        a.samples = sat(a.samples);
+        if (c >= IX_ATTRIBUTION_CLASSES) continue;
+        a.hits = sat(a.hits);
+        const bool finite = isfinite(y);
+#pragma unroll
+        for (uint32_t k = 0; k < IX_ATTRIBUTION_CLASSES; ++k) {
+            if (k != c) continue;
+            a.counts[k] = sat(a.counts[k]);
+            if (finite) {
+                a.y_sum[k] = __fadd_rn(a.y_sum[k], y);
+                a.y_sq_sum[k] = __fadd_rn(a.y_sq_sum[k], __fmul_rn(y, y));
+            }
+        }
+    }
+    L.map[p] = a;
 }
 
 // Many scenes in one persistent launch (BatchLaunch): the task space is the
@@ -342,6 +473,33 @@ cudaError_t IX_SFX(launch_trace)(const TraceLaunch& l, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
+// The attributed kernels carry one register budget each: the trace kernels' 6-CTA/SM
+// variant (isotropic) and 3-CTA/SM variant (uniaxial).
+constexpr int ATTR_MINB_ISO = 6;
+constexpr int ATTR_MINB_UNI = UNI_MINB_1;
+
+cudaError_t IX_SFX(launch_trace_attributed)(const TraceLaunch& l, const AttrLaunch& a, cudaStream_t stream) {
+    if (l.pixels_per_task == 0 || l.pixels_per_task > (uint32_t)TRACE_MAX_PPT) return cudaErrorInvalidValue;
+    if (!launch_shape_ok(l.threads)) return cudaErrorInvalidValue;
+    if (l.scene.n_planes > IX_MAX_PLANES || !a.cls || !a.y) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    if (needs_uniaxial_kernel(l.flags))
+        IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, true><<<l.blocks, l.threads, 0, stream>>>(l, a);
+    else
+        IX_SFX(trace_attributed_kernel)<ATTR_MINB_ISO, false><<<l.blocks, l.threads, 0, stream>>>(l, a);
+    return cudaGetLastError();
+}
+
+cudaError_t IX_SFX(launch_attribution_fold)(const AttrFoldLaunch& l, cudaStream_t stream) {
+    if (l.n_pixels == 0) return cudaSuccess;
+    if (!l.cls || !l.y || !l.map) return cudaErrorInvalidValue;
+    const int threads = 128;
+    const int blocks = (int)((l.n_pixels + threads - 1) / threads);
+    IX_SFX(attribution_fold_kernel)<<<blocks, threads, 0, stream>>>(l);
+    return cudaGetLastError();
+}
+
 cudaError_t IX_SFX(launch_batch)(const BatchLaunch& l, cudaStream_t stream) {
     if (!launch_shape_ok(l.threads) || l.n_jobs == 0) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
@@ -396,6 +554,11 @@ int IX_SFX(trace_blocks_per_sm)(int threads, int variant, int uniaxial, size_t* 
     if (variant == 1) return occupancy(IX_SFX(trace_kernel)<6, false>, threads);
     if (variant == 2) return occupancy(IX_SFX(trace_kernel)<8, false>, threads);
     return occupancy(IX_SFX(trace_kernel)<1, false>, threads);
+}
+
+int IX_SFX(trace_attributed_blocks_per_sm)(int threads, int uniaxial) {
+    if (uniaxial) return occupancy(IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, true>, threads);
+    return occupancy(IX_SFX(trace_attributed_kernel)<ATTR_MINB_ISO, false>, threads);
 }
 
 int IX_SFX(batch_blocks_per_sm)(int threads, int variant, int uniaxial) {

@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/ix_attribution.h"
 #include "../../include/ix_scene.h"
 
 namespace ix {
@@ -148,6 +149,35 @@ struct MetricsLaunch {
 };
 cudaError_t launch_metrics_exact(const MetricsLaunch& l, cudaStream_t stream);
 cudaError_t launch_metrics_fast(const MetricsLaunch& l, cudaStream_t stream);
+
+// Spectral attribution of a trace launch (classify_path, color/metrics/attribution.rs:75):
+// the exit lighting the classes are judged by, and where each sample's class code and
+// luminance go -- [sample][pixel] over the launch's samples [0, spp) and pixels
+// [0, n_pixels), so the fold reads them coalesced.
+struct AttrLaunch {
+    ix_environment env;     // the scoring light: exposure 1, no tray, default shadow
+    float spec;             // its spectral power at 550 nm
+    float factor;           // threshold over the median hemisphere radiance
+    float head_shadow_cos;  // observer cone (visibility.rs:16)
+    float dirs[96][3];      // hemisphere probe directions (lighting.rs:74)
+    uint8_t* cls;           // device, spp * n_pixels class codes (IX_CLASS_*, IX_CLASS_MISS)
+    float* y;               // device, spp * n_pixels luminances (the sample's XYZ.y)
+};
+// AttributionPixel::add (renderer/attribution_map.rs:105) of a launch's records, in
+// ascending sample order, into `map` (device, n_pixels records of the launch's pixels).
+struct AttrFoldLaunch {
+    const uint8_t* cls;
+    const float* y;
+    ix_attribution_pixel* map;
+    uint32_t n_pixels;
+    uint32_t spp;
+};
+cudaError_t launch_trace_attributed_exact(const TraceLaunch& l, const AttrLaunch& a, cudaStream_t stream);
+cudaError_t launch_trace_attributed_fast(const TraceLaunch& l, const AttrLaunch& a, cudaStream_t stream);
+int trace_attributed_blocks_per_sm_exact(int threads, int uniaxial);
+int trace_attributed_blocks_per_sm_fast(int threads, int uniaxial);
+cudaError_t launch_attribution_fold_exact(const AttrFoldLaunch& l, cudaStream_t stream);
+cudaError_t launch_attribution_fold_fast(const AttrFoldLaunch& l, cudaStream_t stream);
 
 cudaError_t launch_trace_exact(const TraceLaunch& l, cudaStream_t stream);
 cudaError_t launch_trace_fast(const TraceLaunch& l, cudaStream_t stream);

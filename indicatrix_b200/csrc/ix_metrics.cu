@@ -104,20 +104,6 @@ IX_DEV int trace_entry(const float4* __restrict__ planes, int n, V3 entry_point,
     return FATE_ABSORBED;
 }
 
-struct Scorer {
-    const ix_environment& env;
-    float spec, threshold, head_shadow_cos;
-    // is_illuminated (lighting.rs:205): the scoring light's radiance along `dir`.
-    IX_DEV bool lit(V3 dir) const {
-        return lighting_radiance(direction_lighting(env, dir, v3(0.0f, 0.0f, 0.0f)), env, spec) > threshold;
-    }
-    // returned_or_reason (visibility.rs:42) for an observer at -forward.
-    IX_DEV bool returned(V3 exit_dir, V3 forward) const {
-        if (dot(exit_dir, -forward) > head_shadow_cos) return false;
-        return lit(exit_dir);
-    }
-};
-
 struct Fan {
     float standoff, lateral;
     // FanGeometry::origin (fan.rs:89).
@@ -150,26 +136,9 @@ __global__ void __launch_bounds__(METRICS_THREADS) IX_SFX(metrics_kernel)(const 
     const MetricsStoneDev stone = L.stones[pose.stone];
     const int n = (int)stone.n_planes;
     for (int i = threadIdx.x; i < n; i += blockDim.x) s_planes[i] = L.planes[stone.plane_offset + i];
-    // ambient_level (lighting.rs:101): the radiances of the 96 hemisphere probes.
-    for (int i = threadIdx.x; i < 96; i += blockDim.x) {
-        const V3 d = v3(L.dirs[i][0], L.dirs[i][1], L.dirs[i][2]);
-        s_rad[i] = lighting_radiance(direction_lighting(L.env, d, v3(0.0f, 0.0f, 0.0f)), L.env, L.spec);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int i = 1; i < 96; ++i) {  // insertion sort, ascending
-            const float v = s_rad[i];
-            int j = i - 1;
-            while (j >= 0 && s_rad[j] > v) {
-                s_rad[j + 1] = s_rad[j];
-                --j;
-            }
-            s_rad[j + 1] = v;
-        }
-        s_threshold = fmaxf(s_rad[48] * L.factor, 1.17549435e-38f);
-    }
-    __syncthreads();
-    const Scorer sc{L.env, L.spec, s_threshold, L.head_shadow_cos};
+    // The exit-lighting threshold; its barriers also publish the plane cache.
+    const float threshold = exit_lighting_threshold(L.env, L.spec, L.factor, L.dirs, s_rad, &s_threshold);
+    const ExitScorer sc{L.env, L.spec, threshold, L.head_shadow_cos};
     const float nd = fmaxf(dispersion_eval(stone.dispersion, 589.3f), 1.1f);
     const float n_f = fmaxf(dispersion_eval(stone.dispersion, 486.1f), 1.001f);
     const float n_c = fmaxf(dispersion_eval(stone.dispersion, 656.3f), 1.001f);

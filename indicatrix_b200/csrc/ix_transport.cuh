@@ -62,6 +62,7 @@ struct LanePath {
     float n_hero;
     bool inside;
     bool has_prev;
+    int facet;  // facet of the last facet event (read only by the attributed kernels)
     // channel c of the path
     float lambda;
     float n;
@@ -334,6 +335,7 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
         esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         return BOUNCE_ESCAPED;
     }
+    P.facet = hit.facet;
     const float4 pl = planes[hit.facet];
     V3 normal = v3(pl.x, pl.y, pl.z);
     const V3 hit_point = P.o + hit.t * P.d;
@@ -480,6 +482,7 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
         esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         return BOUNCE_ESCAPED;
     }
+    P.facet = hit.facet;
     const float4 pl = planes[hit.facet];
     V3 normal = v3(pl.x, pl.y, pl.z);
     const V3 hit_point = P.o + hit.t * P.d;

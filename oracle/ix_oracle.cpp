@@ -1642,8 +1642,34 @@ static void apply_absorption(Path& P, F path_len) {
 
 enum { TERM_ESCAPED = 0, TERM_RR = 1, TERM_CAP = 2 };
 
+// PathEvents::facet (transport/path_events.rs:55-79): the first facet event, the first
+// inside-to-outside transition, internal events before it and a re-entry after it.
+static void record_facet(ixo_path_events* ev, uint32_t bounce, const Hit& hit, bool inside_before,
+                         bool inside_after, V3 dir_after) {
+    if (ev->first_facet < 0) {
+        ev->first_facet = hit.facet;
+        ev->first_entered = inside_after ? 1u : 0u;
+    }
+    const bool exited = ev->exit_facet >= 0;
+    if (inside_before && !inside_after && !exited) {
+        ev->exit_facet = hit.facet;
+        store3(ev->exit_normal, hit.normal);
+        store3(ev->exit_dir, dir_after);
+        ev->exit_bounce = bounce;
+    } else if (inside_before && inside_after && !exited) {
+        ev->bounces_before_exit += 1;
+    } else if (!inside_before && inside_after && exited) {
+        ev->reentered = 1;
+    }
+}
+
 static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand,
-                     ixo_path_info* info) {
+                     ixo_path_info* info, ixo_path_events* ev = nullptr) {
+    if (ev) {
+        std::memset(ev, 0, sizeof(*ev));
+        ev->first_facet = -1;
+        ev->exit_facet = -1;
+    }
     Path P;
     P.sc = sc;
     P.seed = seed;
@@ -1686,6 +1712,10 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
                 P.radiance[c] = fma_(intensity(P.stokes[c]) * F(1.0f), env[c], P.radiance[c]);
             P.escaped = true;
             term = TERM_ESCAPED;
+            if (ev) {  // PathEvents::miss (path_events.rs:88)
+                ev->has_escaped_dir = 1;
+                store3(ev->escaped_dir, P.ray.dir);
+            }
             break;
         }
         // facet_event (bounce_body.rs:611).
@@ -1727,10 +1757,13 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
                 apply_scalar_fresnel(P, g, P.k, normal, cpn, hit_point, bounce, &o);
         }
         const bool was_internal_reflection = P.inside && o.update < 0 && o.new_inside == P.inside;
+        const bool inside_before = P.inside;
         P.ray.dir = o.new_s;
         P.ray.origin = hit_point + o.new_s * F(1e-4f);
         P.k = o.new_k;
         P.inside = o.new_inside;
+        // record_facet (bounce_body.rs:680), after the dispatch and before glare / roulette.
+        if (ev) record_facet(ev, bounce, hit, inside_before, P.inside, P.ray.dir);
         if (o.update >= 0) P.is_e = o.update != 0;
         // maybe_apply_internal_mode_coupling (transport/bounce.rs:470).
         if (P.aniso && was_internal_reflection) {
@@ -1786,6 +1819,7 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
         xyz = mat3_fma(BRADFORD_LMS_TO_XYZ, mulv(lms, wb));
     }
     xyz = vmax0(xyz);
+    if (ev) ev->termination = term;  // attributed.rs:61
     if (info) {
         info->bounces = iterations;
         info->termination = term;
@@ -1806,13 +1840,14 @@ static bool scene_supported(const ix_scene* sc) {
 
 // cpu_sample_xyz (renderer/cpu_frame.rs:45).
 static V3 sample_xyz(const ix_scene* sc, uint32_t pixel, const Rot& rot, uint32_t sample,
-                     ixo_path_info* info) {
+                     ixo_path_info* info, ixo_path_events* ev = nullptr, V3* camera_dir = nullptr) {
     uint32_t width = sc->width;
     uint32_t x = pixel % width, y = pixel / width;
     Draws d = sample_draws(pixel, sample, rot);
     Ray ray = generate_ray(sc->camera, F((float)x), F((float)y), F((float)width),
                            F((float)sc->height), d.jx, d.jy);
-    return trace_path(sc, ray, d.seed, d.hero, info);
+    if (camera_dir) *camera_dir = ray.dir;
+    return trace_path(sc, ray, d.seed, d.hero, info, ev);
 }
 
 static inline bool xyz_finite(V3 v) { return is_finite_(v.x) && is_finite_(v.y) && is_finite_(v.z); }
@@ -2114,6 +2149,46 @@ static void evaluate_metrics(const float* planes, uint32_t n, const ix_material&
     out[4] = raw(clamp_(F((float)extinct) / n_total * F(100.0f), 0.0f, 100.0f));
 }
 
+// ------------------------------------------------------------------------------------
+// Spectral attribution: classify_path (color/metrics/attribution.rs:75-98) through
+// class_index (renderer/attribution_map.rs:39-58), and AttributionPixel::add
+// (attribution_map.rs:105-120).
+// ------------------------------------------------------------------------------------
+static uint32_t classify_events(const ixo_path_events& ev, V3 observer, const MetricLighting& L) {
+    if (ev.first_facet < 0) return IX_CLASS_MISS;
+    if (!ev.first_entered) return IX_CLASS_GLARE;
+    if (ev.exit_facet < 0) {
+        // unexited_reason (attribution.rs:57): roulette, the bounce cap, or an escape
+        // without an exit event (the analytical map's "no intersection").
+        if (ev.termination == TERM_RR) return IX_CLASS_KILLED;
+        if (ev.termination == TERM_CAP) return IX_CLASS_BUDGET;
+        return IX_CLASS_NO_INTERSECTION;
+    }
+    if (F(ev.exit_normal[1]) < F(-0.05f)) return IX_CLASS_WINDOWED;  // WINDOW_NORMAL_Y
+    const V3 dir = load3(ev.exit_dir);
+    if (dir.y > F(0.05f)) {  // UPWARD_DIR_Y
+        // returned_or_reason (visibility.rs:55) and is_illuminated (lighting.rs:207).
+        if (dot(dir, observer) > L.head_shadow_cos) return IX_CLASS_SHADOW;
+        return metric_radiance(L, dir) > L.threshold ? IX_CLASS_RETURNED : IX_CLASS_UNLIT;
+    }
+    return IX_CLASS_SIDE_EXIT;
+}
+
+static void attribution_add(ix_attribution_pixel* p, uint32_t cls, uint32_t scattered, uint32_t fluoresced,
+                            float y) {
+    auto sat = [](uint32_t a) { return a == UINT32_MAX ? a : a + 1u; };
+    p->samples = sat(p->samples);
+    if (cls >= IX_ATTRIBUTION_CLASSES) return;
+    p->hits = sat(p->hits);
+    p->counts[cls] = sat(p->counts[cls]);
+    if (std::isfinite(y)) {
+        p->y_sum[cls] = raw(F(p->y_sum[cls]) + F(y));
+        p->y_sq_sum[cls] = raw(F(p->y_sq_sum[cls]) + F(y) * F(y));
+    }
+    p->scattered += scattered ? 1u : 0u;
+    p->fluoresced += fluoresced ? 1u : 0u;
+}
+
 }  // namespace ixo
 
 using namespace ixo;
@@ -2280,6 +2355,87 @@ int ixo_metrics_lighting(int32_t preset, float light_yaw, float light_pitch, flo
     out[1] = raw(L.head_shadow_cos);
     out[2] = raw(L.spec);
     return 0;
+}
+
+int ixo_trace_ray_events(const ix_scene* scene, const float origin[3], const float dir[3],
+                         uint32_t seed, float hero_rand, float xyz[3], ixo_path_events* events) {
+    if (!scene_supported(scene) || !events) return -1;
+    Ray r{load3(origin), load3(dir)};
+    store3(xyz, trace_path(scene, r, seed, hero_rand, nullptr, events));
+    return 0;
+}
+
+void ixo_path_events_reset(ixo_path_events* events) {
+    std::memset(events, 0, sizeof(*events));
+    events->first_facet = -1;
+    events->exit_facet = -1;
+}
+
+void ixo_path_events_facet(ixo_path_events* events, uint32_t bounce, int32_t facet, const float normal[3],
+                           uint32_t inside_before, uint32_t inside_after, const float dir_after[3]) {
+    Hit h;
+    h.t = 1.0f;
+    h.normal = load3(normal);
+    h.facet = facet;
+    record_facet(events, bounce, h, inside_before != 0, inside_after != 0, load3(dir_after));
+}
+
+int ixo_classify_path(const ixo_path_events* events, const float observer[3], int32_t preset,
+                      float light_yaw, float light_pitch, float head_shadow_deg) {
+    MetricLighting L;
+    if (!events || !metric_lighting(preset, light_yaw, light_pitch, head_shadow_deg, &L)) return -1;
+    return (int)classify_events(*events, load3(observer), L);
+}
+
+void ixo_attribution_add(ix_attribution_pixel* pixel, uint32_t class_code, uint32_t scattered,
+                         uint32_t fluoresced, float y) {
+    attribution_add(pixel, class_code, scattered, fluoresced, y);
+}
+
+int64_t ixo_attribute_pixels(const ix_scene* scene, int32_t preset, float light_yaw,
+                             float light_pitch, float head_shadow_deg, uint32_t pixel_begin,
+                             uint32_t pixel_end, uint32_t sample_offset, uint32_t spp,
+                             uint32_t threads, ix_attribution_pixel* map, double* sums_f64) {
+    if (!scene_supported(scene) || !map) return -1;
+    MetricLighting L;
+    if (!metric_lighting(preset, light_yaw, light_pitch, head_shadow_deg, &L)) return -1;
+    if (threads == 0) threads = 1;
+    std::vector<int64_t> dropped(threads, 0);
+    auto worker = [&](uint32_t t) {
+        for (uint32_t pixel = pixel_begin + t; pixel < pixel_end; pixel += threads) {
+            Rot rot = pixel_rotations(pixel);
+            ix_attribution_pixel& ap = map[pixel - pixel_begin];
+            double sd[3] = {0.0, 0.0, 0.0};
+            for (uint32_t s = 0; s < spp; ++s) {
+                ixo_path_events ev;
+                V3 cam_dir;
+                V3 xyz = sample_xyz(scene, pixel, rot, sample_offset + s, nullptr, &ev, &cam_dir);
+                // The observer is the reverse of the camera ray (attribution_tests.rs:129).
+                const uint32_t cls = classify_events(ev, -cam_dir, L);
+                attribution_add(&ap, cls, 0, 0, raw(xyz.y));
+                if (xyz_finite(xyz)) {
+                    sd[0] += (double)raw(xyz.x);
+                    sd[1] += (double)raw(xyz.y);
+                    sd[2] += (double)raw(xyz.z);
+                } else {
+                    dropped[t]++;
+                }
+            }
+            if (sums_f64) {
+                size_t o = 3 * (size_t)(pixel - pixel_begin);
+                sums_f64[o] += sd[0];
+                sums_f64[o + 1] += sd[1];
+                sums_f64[o + 2] += sd[2];
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < threads; ++t) pool.emplace_back(worker, t);
+    worker(0);
+    for (auto& th : pool) th.join();
+    int64_t total = 0;
+    for (auto d : dropped) total += d;
+    return total;
 }
 
 void ixo_environment_uniform(float radiance, ix_environment* out) {

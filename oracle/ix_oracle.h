@@ -11,6 +11,7 @@
 
 #include <stdint.h>
 #include "../include/ix_scene.h"
+#include "../include/ix_attribution.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -24,6 +25,22 @@ typedef struct ixo_path_info {
     uint32_t exit_splits;   /* exit-split probes that reached the environment          */
 } ixo_path_info;
 
+/* What one traced path did (PathEvents, transport/path_events.rs:27-49): filled by the
+ * same hook points the reference's recorder uses (bounce_body.rs:388, :680 and
+ * attributed.rs:61).  first_facet / exit_facet are -1 when absent. */
+typedef struct ixo_path_events {
+    int32_t first_facet;
+    uint32_t first_entered;      /* the first facet event left the ray inside the stone */
+    int32_t exit_facet;          /* the first inside-to-outside transition              */
+    float exit_normal[3];        /* its facet's outward normal                           */
+    float exit_dir[3];           /* the ray direction after it                           */
+    uint32_t exit_bounce;
+    uint32_t bounces_before_exit;
+    uint32_t reentered;
+    uint32_t termination;        /* ixo_path_info numbering                              */
+    uint32_t has_escaped_dir;
+    float escaped_dir[3];
+} ixo_path_events;
 typedef struct ixo_flop_counts {
     uint64_t add, mul, fma, div, sqrt, transcendental, paths;
 } ixo_flop_counts;
@@ -103,6 +120,36 @@ int ixo_metrics(const float* planes, uint32_t n_planes, const ix_material* mater
 float ixo_metrics_half_width(const float* planes, uint32_t n_planes);
 int ixo_metrics_lighting(int32_t preset, float light_yaw, float light_pitch, float head_shadow_deg,
                          float out[3]);
+/* trace_spectral_ray_attributed_soa_geom (transport/attributed.rs:28): ixo_trace_ray plus
+ * the path's events. */
+int ixo_trace_ray_events(const ix_scene* scene, const float origin[3], const float dir[3],
+                         uint32_t seed, float hero_rand, float xyz[3], ixo_path_events* events);
+/* The recorder alone, for its unit checks: PathEvents::default and PathEvents::facet
+ * (path_events.rs:55) for a facet event of `facet` with outward `normal`. */
+void ixo_path_events_reset(ixo_path_events* events);
+void ixo_path_events_facet(ixo_path_events* events, uint32_t bounce, int32_t facet, const float normal[3],
+                           uint32_t inside_before, uint32_t inside_after, const float dir_after[3]);
+/* classify_path (color/metrics/attribution.rs:75) through class_index
+ * (renderer/attribution_map.rs:39) under the exit lighting of a LightingPreset index,
+ * light yaw / pitch and head-shadow degrees (lighting.rs:137): the class slot
+ * (IX_CLASS_*), IX_CLASS_MISS for a path with no facet event, or -1 for an unmodelled
+ * preset.  `observer` is the unit direction from the stone to the eye. */
+int ixo_classify_path(const ixo_path_events* events, const float observer[3], int32_t preset,
+                      float light_yaw, float light_pitch, float head_shadow_deg);
+/* AttributionPixel::add (attribution_map.rs:105) for one sample (class IX_CLASS_MISS for a
+ * miss; scattered / fluoresced flags). */
+void ixo_attribution_add(ix_attribution_pixel* pixel, uint32_t class_code, uint32_t scattered,
+                         uint32_t fluoresced, float y);
+/* The attributed frame loop: for the pixels [pixel_begin, pixel_end) and samples
+ * [sample_offset, sample_offset + spp), each sample traced as renderer/cpu_frame.rs:45
+ * traces it with its events recorded, classified under the given lighting and added to
+ * map[pixel - pixel_begin] in ascending sample order.  Per-pixel XYZ sums (f64, finite
+ * samples) are added into sums_f64 when it is not NULL.  Returns the number of dropped
+ * non-finite samples, or -1 on an unsupported scene or an unmodelled preset. */
+int64_t ixo_attribute_pixels(const ix_scene* scene, int32_t preset, float light_yaw,
+                             float light_pitch, float head_shadow_deg, uint32_t pixel_begin,
+                             uint32_t pixel_end, uint32_t sample_offset, uint32_t spp,
+                             uint32_t threads, ix_attribution_pixel* map, double* sums_f64);
 /* 1 when this build counts floating-point operations. */
 int ixo_counting_build(void);
 /* Counting build only: trace the given pixels x samples and return the operation tally. */

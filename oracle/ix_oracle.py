@@ -26,6 +26,27 @@ class PathInfo(C.Structure):
     ]
 
 
+class PathEvents(C.Structure):
+    """ixo_path_events: what one traced path did (transport/path_events.rs:27)."""
+
+    _fields_ = [
+        ("first_facet", C.c_int32),
+        ("first_entered", C.c_uint32),
+        ("exit_facet", C.c_int32),
+        ("exit_normal", C.c_float * 3),
+        ("exit_dir", C.c_float * 3),
+        ("exit_bounce", C.c_uint32),
+        ("bounces_before_exit", C.c_uint32),
+        ("reentered", C.c_uint32),
+        ("termination", C.c_uint32),
+        ("has_escaped_dir", C.c_uint32),
+        ("escaped_dir", C.c_float * 3),
+    ]
+
+
+TERM_ESCAPED, TERM_RR, TERM_CAP = 0, 1, 2
+
+
 class FlopCounts(C.Structure):
     _fields_ = [
         ("add", C.c_uint64),
@@ -109,6 +130,19 @@ def _load(name: str) -> C.CDLL:
     lib.ixo_metrics_half_width.argtypes = [f32p, C.c_uint32]
     lib.ixo_metrics_lighting.restype = C.c_int
     lib.ixo_metrics_lighting.argtypes = [C.c_int32, C.c_float, C.c_float, C.c_float, f32p]
+    lib.ixo_trace_ray_events.restype = C.c_int
+    lib.ixo_trace_ray_events.argtypes = [P(abi.Scene), f32p, f32p, C.c_uint32, C.c_float, f32p,
+                                         P(PathEvents)]
+    lib.ixo_path_events_reset.argtypes = [P(PathEvents)]
+    lib.ixo_path_events_facet.argtypes = [P(PathEvents), C.c_uint32, C.c_int32, f32p, C.c_uint32, C.c_uint32,
+                                          f32p]
+    lib.ixo_classify_path.restype = C.c_int
+    lib.ixo_classify_path.argtypes = [P(PathEvents), f32p, C.c_int32, C.c_float, C.c_float, C.c_float]
+    lib.ixo_attribution_add.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float]
+    lib.ixo_attribute_pixels.restype = C.c_int64
+    lib.ixo_attribute_pixels.argtypes = [P(abi.Scene), C.c_int32, C.c_float, C.c_float, C.c_float,
+                                         C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                         C.c_void_p, P(C.c_double)]
     lib.ixo_counting_build.restype = C.c_int
     lib.ixo_count_flops.restype = C.c_int
     lib.ixo_count_flops.argtypes = [P(abi.Scene), C.c_uint32, C.c_uint32, C.c_uint32,
@@ -268,3 +302,72 @@ def metrics_lighting(preset: int, light_yaw: float, light_pitch: float, head_sha
     if lib().ixo_metrics_lighting(preset, light_yaw, light_pitch, head_shadow_deg, _f32p(out)) != 0:
         raise ValueError("unmodelled preset")
     return out
+
+
+def trace_ray_events(scene: abi.Scene, origin, direction, seed: int, hero_rand: float):
+    """trace_spectral_ray_attributed_soa_geom: (xyz, PathEvents)."""
+    o = np.asarray(origin, np.float32)
+    d = np.asarray(direction, np.float32)
+    xyz = np.zeros(3, np.float32)
+    ev = PathEvents()
+    rc = lib().ixo_trace_ray_events(C.byref(scene), _f32p(o), _f32p(d), seed, hero_rand, _f32p(xyz),
+                                    C.byref(ev))
+    if rc != 0:
+        raise ValueError("scene not supported by the oracle")
+    return xyz, ev
+
+
+def classify_path(events: PathEvents, observer, preset: int, light_yaw: float, light_pitch: float,
+                  head_shadow_deg: float = 16.0) -> int:
+    """classify_path + class_index: the class slot, or abi.CLASS_MISS."""
+    ob = np.asarray(observer, np.float32)
+    r = lib().ixo_classify_path(C.byref(events), _f32p(ob), preset, light_yaw, light_pitch,
+                                head_shadow_deg)
+    if r < 0:
+        raise ValueError("unmodelled preset")
+    return int(r)
+
+
+def attribution_add(pixel_map: np.ndarray, index: int, class_code: int, y: float,
+                    scattered: bool = False, fluoresced: bool = False) -> None:
+    """AttributionPixel::add on element `index` of a map (abi.attribution_dtype())."""
+    assert pixel_map.dtype == abi.attribution_dtype() and pixel_map.flags.c_contiguous
+    addr = pixel_map.ctypes.data + index * pixel_map.dtype.itemsize
+    lib().ixo_attribution_add(C.c_void_p(addr), class_code, int(scattered), int(fluoresced), y)
+
+
+def attribute_pixels(scene: abi.Scene, lighting: abi.MetricsLighting, pixel_begin: int, pixel_end: int,
+                     sample_offset: int, spp: int, threads: int = 0, pixel_map=None, sums=None):
+    """The attributed frame loop over pixels [pixel_begin, pixel_end): returns
+    (map, f64 XYZ sums, dropped).  `pixel_map` / `sums` are accumulated when given."""
+    if threads <= 0:
+        threads = os.cpu_count() or 1
+    n = pixel_end - pixel_begin
+    if pixel_map is None:
+        pixel_map = np.zeros(n, abi.attribution_dtype())
+    if sums is None:
+        sums = np.zeros((n, 3), np.float64)
+    dropped = lib().ixo_attribute_pixels(C.byref(scene), lighting.preset, lighting.light_yaw,
+                                         lighting.light_pitch, lighting.head_shadow_deg, pixel_begin,
+                                         pixel_end, sample_offset, spp, threads,
+                                         C.c_void_p(pixel_map.ctypes.data),
+                                         sums.ctypes.data_as(C.POINTER(C.c_double)))
+    if dropped < 0:
+        raise ValueError("scene or lighting not supported by the oracle")
+    return pixel_map, sums, int(dropped)
+
+
+def path_events() -> PathEvents:
+    """PathEvents::default."""
+    ev = PathEvents()
+    lib().ixo_path_events_reset(C.byref(ev))
+    return ev
+
+
+def path_events_facet(events: PathEvents, bounce: int, facet: int, normal, inside_before: bool,
+                      inside_after: bool, dir_after) -> None:
+    """PathEvents::facet for one facet event."""
+    n = np.asarray(normal, np.float32)
+    d = np.asarray(dir_after, np.float32)
+    lib().ixo_path_events_facet(C.byref(events), bounce, facet, _f32p(n), int(inside_before), int(inside_after),
+                                _f32p(d))

@@ -46,6 +46,7 @@ def test_abi_struct_layout_matches_c():
         "ix_batch_item": abi.BatchItem, "ix_timing": abi.TimingInfo,
         "ix_gem_metrics": abi.GemMetrics, "ix_metrics_lighting": abi.MetricsLighting,
         "ix_metrics_stone": abi.MetricsStone, "ix_metrics_pose": abi.MetricsPose,
+        "ix_attribution_pixel": abi.AttributionPixel,
     }
     src = ['#include <stdio.h>', '#include <stddef.h>', '#include "ix_cuda.h"', "int main(void){"]
     for cname, py in checks.items():
