@@ -52,21 +52,25 @@ def test_per_sample_classes_match_oracle(backend, exact_backend, oracle, exact):
     """One sample per call: the device's class of every (pixel, sample) against the
     oracle's.  The exact build follows the oracle path for path except where a
     transcendental's last bit flips a branch; the fast build also where its rounding
-    does (its per-path drift is bounded in the path tests)."""
+    does (its per-path drift is bounded in the path tests).  Observed on a B200 (64 x 64
+    x 8 samples): every class identical in both builds; luminance bit-identical for
+    99.3 % (exact) / 76.7 % (fast) of the samples, within 1e-4 for 100 % / 97.8 %."""
     b = exact_backend if exact else backend
     fs = workloads.round_brilliant_frame(48, 48, max_bounces=32)
     got, want, gy, wy = per_sample(b, oracle, fs, ISO, 6)
     agree = np.mean(got == want)
-    assert agree >= (0.995 if exact else 0.97), agree
+    assert agree >= (0.999 if exact else 0.99), agree
     same = got == want
     close = np.abs(gy[same] - wy[same]) <= 1e-4 * np.maximum(np.abs(wy[same]), 1e-2)
-    assert np.mean(close) >= (0.98 if exact else 0.9)
+    assert np.mean(close) >= (0.995 if exact else 0.95)
     # Every class the oracle produces here also comes out of the device.
     assert set(np.unique(want)) == set(np.unique(got))
 
 
 def test_frame_map_matches_oracle(exact_backend, oracle):
-    """A whole frame at 16 samples per pixel: counts per pixel and class totals."""
+    """A whole frame at 16 samples per pixel: counts per pixel and class totals
+    (observed: every pixel's counts identical, 93.6 % of the records bit-identical
+    including their f32 luminance sums)."""
     fs = workloads.round_brilliant_frame(40, 40, max_bounces=32)
     n = 40 * 40
     g, acc = gpu_map(exact_backend, fs, ISO, 0, 16)
@@ -75,7 +79,8 @@ def test_frame_map_matches_oracle(exact_backend, oracle):
     assert (g["counts"].sum(axis=1) == g["hits"]).all()
     assert np.array_equal(g["hits"], o["hits"])  # camera-ray hits do not depend on the path
     same = np.all(g["counts"] == o["counts"], axis=1)
-    assert np.mean(same) >= 0.95, np.mean(same)
+    assert np.mean(same) >= 0.99, np.mean(same)
+    assert np.mean([g[i].tobytes() == o[i].tobytes() for i in range(n)]) >= 0.85
     gt, ot = g["counts"].sum(axis=0).astype(np.int64), o["counts"].sum(axis=0).astype(np.int64)
     assert np.all(np.abs(gt - ot) <= np.maximum(3, 0.01 * ot)), (gt, ot)
     gy = g["y_sum"].astype(np.float64).sum(axis=0)
@@ -115,7 +120,7 @@ def test_uniaxial_stress_frame_attribution(exact_backend, oracle):
     stress workload (tilted optic axis, o/e absorption, depth 64) against the oracle."""
     fs = workloads.anisotropic_stress_frame(32, 32)
     got, want, _, _ = per_sample(exact_backend, oracle, fs, ISO, 4)
-    assert np.mean(got == want) >= 0.98, np.mean(got == want)
+    assert np.mean(got == want) >= 0.995, np.mean(got == want)  # observed 100 %
 
 
 def test_studio_lighting_classes(exact_backend, oracle):
@@ -127,7 +132,7 @@ def test_studio_lighting_classes(exact_backend, oracle):
     fs.environment = environment_preset(10, 1.0, 0.85, 0.95, 0.0, 1.0, 16.0)
     light = MetricsLighting(preset=10, light_yaw=0.85, light_pitch=0.95, head_shadow_deg=16.0)
     got, want, _, _ = per_sample(exact_backend, oracle, fs, light, 4)
-    assert np.mean(got == want) >= 0.995, np.mean(got == want)
+    assert np.mean(got == want) >= 0.999, np.mean(got == want)  # observed 100 %
     for cls in (abi.CLASS_RETURNED, abi.CLASS_UNLIT, abi.CLASS_WINDOWED):
         assert np.sum(want == cls) > 0, cls
 
