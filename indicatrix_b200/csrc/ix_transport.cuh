@@ -149,6 +149,31 @@ static __device__ __noinline__ Hit probe_intersect(Group g, const float4* __rest
     return group_intersect(g, planes, n, o, d);
 }
 
+// A ray that starts strictly outside the half-space of facet `f` and moves away from it
+// meets no facet of the stone (an intersection of half-spaces): every point of the ray
+// stays outside f.  The slab scan reports the same miss -- f's update leaves its t_far at
+// most f's negative distance, below the 1e-4 every hit needs -- so a caller may skip the
+// scan.  The 1e-6 margins keep the test inside the region where the scan's own rounding
+// also sees |denom| > 1e-7 and side > 0.
+IX_DEV bool leaves_stone_through(const float4* __restrict__ planes, int f, V3 o, V3 d) {
+    const float4 p = planes[f];
+    const float denom = (p.x * d.x + p.y * d.y) + p.z * d.z;
+    const float side = p.w + ((p.x * o.x + p.y * o.y) + p.z * o.z);
+    return denom > 1e-6f && side > 1e-6f;
+}
+
+// The bounce's intersection: after an exit (or an outside reflection) through facet
+// P.facet the ray has left the stone and the scan is skipped.
+IX_DEV Hit group_next_hit(const Group& g, const LanePath& P, const float4* __restrict__ planes, int n) {
+    if (!P.inside && P.has_prev && leaves_stone_through(planes, P.facet, P.o, P.d)) {
+        Hit h;
+        h.facet = -1;
+        h.t = 0.0f;
+        return h;
+    }
+    return group_intersect(g, planes, n, P.o, P.d);
+}
+
 // ------------------------------------------------------------------------------------
 // Path setup: PathState::new (bounce_body.rs:260-356).
 // ------------------------------------------------------------------------------------
@@ -272,7 +297,14 @@ enum BounceResult { BOUNCE_CONTINUE = 0, BOUNCE_ESCAPED = 1, BOUNCE_KILLED = 2 }
 // together and the probing lane adds its transmitted intensity times the radiance found.
 IX_DEV void group_exit_probes(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes,
                               V3 hit_point, bool want_probe, V3 dir_k, float t_intensity) {
-    unsigned probes = (__ballot_sync(g.mask, want_probe) >> (threadIdx.x & 24u)) & 0xFFu;
+    // A probe leaving through the exit facet itself cannot meet the stone: its channel
+    // goes straight to the environment, every such lane at once.
+    const bool clear = want_probe && leaves_stone_through(planes, P.facet, hit_point + dir_k * 1e-4f, dir_k);
+    if (clear) {
+        const float e = lane_environment(S.s.environment, dir_k, P.observer, P.lambda);
+        P.split = fmaf(fmaxf(t_intensity, 0.0f), e, P.split);
+    }
+    unsigned probes = (__ballot_sync(g.mask, want_probe && !clear) >> (threadIdx.x & 24u)) & 0xFFu;
     while (probes) {
         const int j = __ffs(probes) - 1;
         probes &= probes - 1;
@@ -330,7 +362,7 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
     const ix_scene& sc = S.s;
     const uint32_t bounce = P.bounce;
     const int n_planes = (int)sc.n_planes;
-    Hit hit = group_intersect(g, planes, n_planes, P.o, P.d);
+    Hit hit = group_next_hit(g, P, planes, n_planes);
     if (hit.facet < 0) {
         esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         return BOUNCE_ESCAPED;
@@ -477,7 +509,7 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     const ix_scene& sc = S.s;
     const ix_material& mat = sc.material;
     const uint32_t bounce = P.bounce;
-    Hit hit = group_intersect(g, planes, (int)sc.n_planes, P.o, P.d);
+    Hit hit = group_next_hit(g, P, planes, (int)sc.n_planes);
     if (hit.facet < 0) {
         esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         return BOUNCE_ESCAPED;

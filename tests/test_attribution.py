@@ -327,3 +327,57 @@ def test_attributed_frame_matches_the_plain_frame(oracle):
     m2, _, _ = oracle.attribute_pixels(sc, light, 0, n, 0, 4, threads=4)
     m2, _, _ = oracle.attribute_pixels(sc, light, 0, n, 4, 4, threads=4, pixel_map=m2)
     assert m2.tobytes() == m.tobytes()
+
+
+# --- the convex-exit shortcut of the device's bounce loop ----------------------------
+
+def test_a_ray_leaving_through_a_facet_misses_the_stone(oracle):
+    """The device skips the plane scan for a ray that starts more than 1e-6 outside the
+    half-space of the facet it left and moves away from it (denom > 1e-6).  The oracle's
+    scan (the reference's slab arithmetic) must report a miss for every such ray: exit
+    points of rays from inside the round brilliant, the step cut and random stones, with
+    outward directions down to grazing, restarted 1e-4 along the direction as the
+    bounce loop restarts them."""
+    import ctypes as C
+
+    from indicatrix_b200 import geometry
+
+    lib = oracle.lib()
+    t, f = C.c_float(), C.c_int32()
+    stones = [np.ascontiguousarray(oracle.standard_round_brilliant()), geometry.to_f32(geometry.step_cut())]
+    from indicatrix_b200 import workloads
+
+    stones += [np.ascontiguousarray(s.planes, np.float32) for s in workloads.random_stones(3, seed=11)]
+    rng = np.random.default_rng(3)
+    f32 = np.float32
+    checked = skipped = 0
+    for planes in stones:
+        planes = np.ascontiguousarray(planes, np.float32)
+        centre = np.array([0.0, -0.1, 0.0], np.float32)
+        for _ in range(600):
+            d_in = glam_normalize(rng.normal(size=3))
+            if not lib.ixo_intersect(oracle._f32p(planes), planes.shape[0], oracle._f32p(centre),
+                                     oracle._f32p(d_in), C.byref(t), C.byref(f)):
+                continue
+            fi = f.value
+            h = (centre + f32(t.value) * d_in).astype(np.float32)
+            n = planes[fi, :3]
+            # An outward direction: a random unit vector flipped to the facet's side, some
+            # of them nearly grazing.
+            d = glam_normalize(rng.normal(size=3))
+            if f32(np.dot(n, d)) < 0:
+                d = -d
+            if rng.random() < 0.3:
+                d = glam_normalize(d - n * f32(np.dot(n, d) * f32(0.999)))
+            o = (h + d * f32(1e-4)).astype(np.float32)
+            p = planes[fi]
+            denom = f32(f32(f32(p[0] * d[0]) + f32(p[1] * d[1])) + f32(p[2] * d[2]))
+            side = f32(p[3] + f32(f32(f32(p[0] * o[0]) + f32(p[1] * o[1])) + f32(p[2] * o[2])))
+            if not (denom > 1e-6 and side > 1e-6):
+                skipped += 1
+                continue
+            checked += 1
+            hit = lib.ixo_intersect(oracle._f32p(planes), planes.shape[0], oracle._f32p(o), oracle._f32p(d),
+                                    C.byref(t), C.byref(f))
+            assert hit == 0, (fi, o, d, t.value, f.value)
+    assert checked > 2000 and skipped > 0
