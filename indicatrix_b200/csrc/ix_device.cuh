@@ -174,18 +174,36 @@ IX_DEV float unit_draw(uint32_t seed, uint32_t bounce, uint32_t stream) {
 IX_DEV float low_discrepancy_base2(uint32_t n) {
     return __uint2float_rn(__brev(n)) * 2.3283064365386963e-10f;
 }
-// radical_inverse_base (sampling.rs:127): fused digit accumulation, IEEE divides (explicit
-// __fdiv_rn: the sampler is bit-exact in both builds).
-IX_DEV float radical_inverse_base(uint32_t n, uint32_t base) {
+// radical_inverse_base (sampling.rs:127) accumulates digit * inv_base with a fused
+// multiply-add and divides inv_base by the base after every digit.  Those weights,
+// w_0 = 1/B and w_{k+1} = w_k / B, each an IEEE round-to-nearest quotient, depend on the
+// base alone: they are evaluated once, at compile time, for the bases the sampler uses
+// (N covers every digit of a u32: 21 in base 3, 14 in base 5).
+template <uint32_t B, int N>
+struct DigitWeights {
+    float w[N];
+    constexpr DigitWeights() : w() {
+        float x = 1.0f / (float)B;
+        for (int k = 0; k < N; ++k) {
+            w[k] = x;
+            x = x / (float)B;
+        }
+    }
+};
+static __constant__ DigitWeights<3, 21> c_weights3;
+static __constant__ DigitWeights<5, 14> c_weights5;
+// radical_inverse_base for base 3 or 5: the same fused accumulation with the weights read
+// from the table instead of a division per digit (bit-identical).  The digit index
+// advances in step across a warp, so the constant-cache reads broadcast.
+template <uint32_t B>
+IX_DEV float radical_inverse_table(uint32_t n) {
+    const float* w = (B == 3) ? c_weights3.w : c_weights5.w;
     uint32_t remaining = n;
     float val = 0.0f;
-    float fb = __uint2float_rn(base);
-    float inv_base = __fdiv_rn(1.0f, fb);
-    while (remaining > 0) {
-        uint32_t digit = remaining % base;
-        val = fmaf(__uint2float_rn(digit), inv_base, val);
-        inv_base = __fdiv_rn(inv_base, fb);
-        remaining /= base;
+    for (int k = 0; remaining > 0; ++k) {
+        const uint32_t digit = remaining % B;
+        val = fmaf(__uint2float_rn(digit), w[k], val);
+        remaining /= B;
     }
     return val;
 }
@@ -206,8 +224,8 @@ IX_DEV Draws sample_draws(uint32_t pixel, uint32_t sample) {
     Draws d;
     d.seed = hash_u32((pixel * 0x9E3779B9u) ^ (sample * 0x85EBCA6Bu));
     d.jx = cranley_patterson_rotate(low_discrepancy_base2(sample), rx) - 0.5f;
-    d.jy = cranley_patterson_rotate(radical_inverse_base(sample, 3), ry) - 0.5f;
-    d.hero = cranley_patterson_rotate(radical_inverse_base(sample, 5), rh);
+    d.jy = cranley_patterson_rotate(radical_inverse_table<3>(sample), ry) - 0.5f;
+    d.hero = cranley_patterson_rotate(radical_inverse_table<5>(sample), rh);
     return d;
 }
 
@@ -228,7 +246,11 @@ IX_DEV Ray generate_ray(const ix_camera& c, float sx, float sy, float w, float h
     V3 dir = d * __fdiv_rn(1.0f, __fsqrt_rn(dot(d, d)));
     return Ray{load3(c.origin), dir};
 }
+// f32::rem_euclid(a, 400).  The remainder is exact; for 0 <= a < 800 it is a or a - 400
+// (exact by Sterbenz's lemma), which covers every offset of the hero comb, so fmodf runs
+// only for inputs outside that range.
 IX_DEV float rem_euclid_400(float a) {
+    if (a >= 0.0f && a < 800.0f) return a < 400.0f ? a : a - 400.0f;
     float r = fmodf(a, 400.0f);
     return (r < 0.0f) ? r + 400.0f : r;
 }
@@ -349,9 +371,11 @@ IX_DEV float exp_lane(float x) {
 // ------------------------------------------------------------------------------------
 // Colour tables and spectral integration (color/cie1931.rs:157; environment/spectral.rs:28).
 // ------------------------------------------------------------------------------------
-__constant__ float c_cmf[81][3] = IX_CIE1931_CMF_INIT;
-__constant__ float c_d65[41] = IX_CIE_D65_SPD_INIT;
-__constant__ float c_d65_uv[9] = IX_CIE_D65_UV_SPD_INIT;
+// In global memory, read through the read-only data cache: the 8 channels of a path look
+// up 8 different wavelengths, which the constant cache would serialise.
+static __device__ const float c_cmf[81][3] = IX_CIE1931_CMF_INIT;
+static __device__ const float c_d65[41] = IX_CIE_D65_SPD_INIT;
+static __device__ const float c_d65_uv[9] = IX_CIE_D65_UV_SPD_INIT;
 
 IX_DEV V3 cmf(float lambda_nm) {
     if (!(lambda_nm >= 380.0f && lambda_nm <= 780.0f)) return v3(0.0f, 0.0f, 0.0f);
@@ -359,8 +383,8 @@ IX_DEV V3 cmf(float lambda_nm) {
     int i0 = (int)floorf(position);
     i0 = i0 > 79 ? 79 : i0;
     float t = position - (float)i0;
-    float l0 = c_cmf[i0][0], l1 = c_cmf[i0][1], l2 = c_cmf[i0][2];
-    float h0 = c_cmf[i0 + 1][0], h1 = c_cmf[i0 + 1][1], h2 = c_cmf[i0 + 1][2];
+    float l0 = __ldg(&c_cmf[i0][0]), l1 = __ldg(&c_cmf[i0][1]), l2 = __ldg(&c_cmf[i0][2]);
+    float h0 = __ldg(&c_cmf[i0 + 1][0]), h1 = __ldg(&c_cmf[i0 + 1][1]), h2 = __ldg(&c_cmf[i0 + 1][2]);
     return v3(l0 + (h0 - l0) * t, l1 + (h1 - l1) * t, l2 + (h2 - l2) * t);
 }
 IX_DEV float d65(float lambda_nm) {
@@ -370,7 +394,7 @@ IX_DEV float d65(float lambda_nm) {
         int i0 = (int)floorf(position);
         i0 = i0 > 7 ? 7 : i0;
         float frac = position - (float)i0;
-        float v0 = c_d65_uv[i0], v1 = c_d65_uv[i0 + 1];
+        float v0 = __ldg(&c_d65_uv[i0]), v1 = __ldg(&c_d65_uv[i0 + 1]);
         return fmaf(frac, v1 - v0, v0) / 100.0f;
     }
     float clamped = clampf_(lambda_nm, 380.0f, 780.0f);
@@ -378,7 +402,7 @@ IX_DEV float d65(float lambda_nm) {
     int i0 = (int)floorf(position);
     i0 = i0 > 39 ? 39 : i0;
     float frac = position - (float)i0;
-    float v0 = c_d65[i0], v1 = c_d65[i0 + 1];
+    float v0 = __ldg(&c_d65[i0]), v1 = __ldg(&c_d65[i0 + 1]);
     return fmaf(frac, v1 - v0, v0) / 100.0f;
 }
 // powi with a constant exponent: x^(2^i) factors multiplied in ascending bit order.
@@ -553,10 +577,17 @@ IX_DEV Hit intersect_planes(const float4* __restrict__ planes, int n, V3 o, V3 d
         float denom = (p.x * d.x + p.y * d.y) + p.z * d.z;
         float side = p.w + ((p.x * o.x + p.y * o.y) + p.z * o.z);
         if (fabsf(denom) > 1e-7f) {
+            // An entering plane the origin is not outside of cannot make the entry (t <= 0)
+            // and an exiting plane the origin is outside of makes the scan a miss: neither
+            // needs its division (the argument is spelled out at group_intersect).
             const bool entering = denom < 0.0f;
+            if (!entering && side > 0.0f) {
+                outside = true;
+                break;
+            }
             const float bound = entering ? t_near : t_far;
-            if (fmaf(bound, denom, side) >= 0.0f) {
-                float t = __fdiv_rn(-side, denom);
+            if ((side > 0.0f || !entering) && fmaf(bound, denom, side) >= 0.0f) {
+                const float t = __fdiv_rn(-side, denom);
                 if (entering) {
                     if (t > t_near) {
                         t_near = t;

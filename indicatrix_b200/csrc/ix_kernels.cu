@@ -88,15 +88,14 @@ IX_DEV uint32_t classify_path(uint32_t ev, V3 exit_dir, V3 observer, const ExitS
 // ATTR adds the event record of each path and writes its class and luminance to `at`
 // (the traced arithmetic is the same: the record only reads the path state).
 template <bool UNI, bool ATTR = false>
-IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const float4* __restrict__ planes,
-                                     uint32_t pixel0, uint32_t npix, uint32_t spp,
-                                     uint32_t sample_offset, PartSlot& part, double* out, int accumulate,
-                                     const AttrTask* at = nullptr) {
+IX_DEV uint32_t trace_task(const Group& g, const DevScene& S, const float4* __restrict__ planes,
+                           uint32_t pixel0, uint32_t npix, uint32_t spp, uint32_t sample_offset,
+                           PartSlot& part, double* out, int accumulate, const AttrTask* at = nullptr) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t gi = lane >> 3;
     const uint32_t total = npix * spp;
     const uint32_t max_bounces = S.s.max_bounces;
-    unsigned long long drops = 0;
+    uint32_t drops = 0;  // non-finite samples this lane dropped
     if (g.c == 0)
         for (uint32_t j = 0; j < npix; ++j) {
             part[j][gi][0] = 0.0;
@@ -107,7 +106,6 @@ IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const fl
     bool active = q < total;
     bool fresh = active;  // the group's next path still needs its setup
     uint32_t cur_j = active ? q / spp : 0;
-    double ax = 0.0, ay = 0.0, az = 0.0;
     LanePath P;
     uint32_t ev = 0;  // ATTR: the path's event bits
     V3 exit_dir = v3(0.0f, 0.0f, 0.0f);
@@ -147,24 +145,19 @@ IX_DEV unsigned long long trace_task(const Group& g, const DevScene& S, const fl
                 at->y[rec] = xyz.y;
             }
         }
-        if (isfinite(xyz.x) && isfinite(xyz.y) && isfinite(xyz.z)) {
-            ax += (double)xyz.x;
-            ay += (double)xyz.y;
-            az += (double)xyz.z;
-        } else if (g.c == 0) {
-            ++drops;
+        // The group's f64 sums of this pixel live in its shared-memory slot (zeroed
+        // above), added in the group's sample order.
+        if (g.c == 0) {
+            if (isfinite(xyz.x) && isfinite(xyz.y) && isfinite(xyz.z)) {
+                part[cur_j][gi][0] += (double)xyz.x;
+                part[cur_j][gi][1] += (double)xyz.y;
+                part[cur_j][gi][2] += (double)xyz.z;
+            } else {
+                ++drops;
+            }
         }
         q += GROUPS_PER_WARP;
-        const uint32_t j = (q < total) ? q / spp : 0xFFFFFFFFu;
-        if (j != cur_j) {
-            if (g.c == 0) {
-                part[cur_j][gi][0] = ax;
-                part[cur_j][gi][1] = ay;
-                part[cur_j][gi][2] = az;
-            }
-            ax = ay = az = 0.0;
-            cur_j = j;
-        }
+        cur_j = (q < total) ? q / spp : 0;
         if (q < total)
             fresh = true;
         else
@@ -210,7 +203,7 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_c
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t ppt = L.pixels_per_task;
     const uint32_t n_tasks = (L.n_pixels + ppt - 1) / ppt;
-    unsigned long long drops = 0;
+    uint32_t drops = 0;  // non-finite samples this lane dropped
     for (;;) {
         uint32_t task = 0;
         if (lane == 0) task = atomicAdd(L.task_counter, 1u);
@@ -221,7 +214,7 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_c
         drops += trace_task<UNI>(g, S, s_planes, L.pixel_begin + local0, npix, L.spp, L.sample_offset,
                                  s_part[threadIdx.x >> 5], L.out + (size_t)local0 * 3, L.accumulate);
     }
-    if (drops && L.dropped) atomicAdd(L.dropped, drops);
+    if (drops && L.dropped) atomicAdd(L.dropped, (unsigned long long)drops);
 }
 
 // The trace kernel with spectral attribution: the same task loop, and each path's
@@ -244,7 +237,7 @@ __global__ void __launch_bounds__(128, MINB)
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t ppt = L.pixels_per_task;
     const uint32_t n_tasks = (L.n_pixels + ppt - 1) / ppt;
-    unsigned long long drops = 0;
+    uint32_t drops = 0;  // non-finite samples this lane dropped
     for (;;) {
         uint32_t task = 0;
         if (lane == 0) task = atomicAdd(L.task_counter, 1u);
@@ -256,7 +249,7 @@ __global__ void __launch_bounds__(128, MINB)
         drops += trace_task<UNI, true>(g, S, s_planes, L.pixel_begin + local0, npix, L.spp, L.sample_offset,
                                        s_part[threadIdx.x >> 5], L.out + (size_t)local0 * 3, L.accumulate, &at);
     }
-    if (drops && L.dropped) atomicAdd(L.dropped, drops);
+    if (drops && L.dropped) atomicAdd(L.dropped, (unsigned long long)drops);
 }
 
 // AttributionPixel::add (renderer/attribution_map.rs:105-120), one thread per pixel, the
@@ -299,7 +292,7 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(batch_kernel)(const __grid_c
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = threadIdx.x >> 5;
     uint32_t cached = 0xFFFFFFFFu;
-    unsigned long long drops = 0;
+    uint32_t drops = 0;  // non-finite samples this lane dropped
     for (;;) {
         uint32_t task = 0;
         if (lane == 0) task = atomicAdd(L.task_counter, 1u);
@@ -328,7 +321,7 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(batch_kernel)(const __grid_c
         drops += trace_task<UNI>(g, S, s_planes[warp], local0, npix, job.spp, job.sample_offset, s_part[warp],
                                  L.out + job.out_offset + (size_t)local0 * 3, L.accumulate);
     }
-    if (drops && L.dropped) atomicAdd(L.dropped, drops);
+    if (drops && L.dropped) atomicAdd(L.dropped, (unsigned long long)drops);
 }
 
 // Per-path checks: each 8-lane group traces one input row, exactly as the megakernel

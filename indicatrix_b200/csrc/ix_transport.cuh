@@ -82,6 +82,17 @@ struct LanePath {
 // ------------------------------------------------------------------------------------
 // Cooperative slab intersection (simd/slab.rs:120-160; intersect.rs:101-127), with the
 // division-free candidate filter of intersect_planes (ix_device.cuh).
+//
+// Two kinds of plane are passed over without a division; neither can change the hit the
+// full scan returns:
+//  * an entering plane (denom < 0) the origin is not outside of (side <= 0): its t <= 0.
+//    If every entering plane is of this kind the scan's t_near stays <= 0, below both
+//    the 1e-4 an entry needs and t_far (>= 0 unless the scan misses anyway); otherwise
+//    the first plane with side > 0 takes t_near past every such t, and after it they
+//    fail the filter.  So t_near, and near_idx whenever it is used, come out the same.
+//  * an exiting plane (denom > 0) the origin is outside of (side > 0): the ray leaves
+//    that half-space for good, the scan's t_far ends at most at this plane's negative t,
+//    and it reports a miss -- returned at once, as for a parallel plane outside.
 // ------------------------------------------------------------------------------------
 IX_DEV Hit group_intersect(const Group& g, const float4* __restrict__ planes, int n, V3 o, V3 d) {
     float t_near = -1e30f, t_far = 1e30f;
@@ -93,9 +104,14 @@ IX_DEV Hit group_intersect(const Group& g, const float4* __restrict__ planes, in
         float side = p.w + ((p.x * o.x + p.y * o.y) + p.z * o.z);
         if (fabsf(denom) > 1e-7f) {
             const bool entering = denom < 0.0f;
+            if (!entering && side > 0.0f) {
+                outside = 1;
+                break;
+            }
+            // One division site for both kinds keeps the lanes of a group together.
             const float bound = entering ? t_near : t_far;
-            if (fmaf(bound, denom, side) >= 0.0f) {
-                float t = __fdiv_rn(-side, denom);
+            if ((side > 0.0f || !entering) && fmaf(bound, denom, side) >= 0.0f) {
+                const float t = __fdiv_rn(-side, denom);
                 if (entering) {
                     if (t > t_near) {
                         t_near = t;

@@ -183,9 +183,25 @@ def test_environment_and_intersection(exact_backend, oracle):
     o = rng.uniform(-2, 2, (3000, 3)).astype(np.float32)
     d = rng.normal(size=(3000, 3)).astype(np.float32)
     d /= np.linalg.norm(d, axis=1, keepdims=True)
-    out = exact_backend.debug_check(fs, CHECK_INTERSECT, np.concatenate([o, d], 1), 2).view(np.float32)
     t = C.c_float()
     f = C.c_int32()
+    # Plus rays restarted 1e-4 past a facet, as the bounce loop restarts them: reflected
+    # back inside, refracted-like onward, and leaving outward (the regime where the scan
+    # passes over planes without dividing).
+    extra_o, extra_d = [], []
+    for oo, dd in zip(o[:1500], d[:1500]):
+        if not oracle.lib().ixo_intersect(oracle._f32p(planes), planes.shape[0], oracle._f32p(oo.copy()),
+                                          oracle._f32p(dd.copy()), C.byref(t), C.byref(f)):
+            continue
+        hp = (oo + np.float32(t.value) * dd).astype(np.float32)
+        n = planes[f.value, :3]
+        refl = (dd - np.float32(2.0) * np.float32(np.dot(dd, n)) * n).astype(np.float32)
+        for nd in (refl, dd, -refl):
+            extra_o.append((hp + nd * np.float32(1e-4)).astype(np.float32))
+            extra_d.append(nd)
+    o = np.concatenate([o, np.array(extra_o, np.float32)])
+    d = np.concatenate([d, np.array(extra_d, np.float32)])
+    out = exact_backend.debug_check(fs, CHECK_INTERSECT, np.concatenate([o, d], 1), 2).view(np.float32)
     for oo, dd, r in zip(o, d, out):
         h = oracle.lib().ixo_intersect(oracle._f32p(planes), planes.shape[0], oracle._f32p(oo.copy()),
                                        oracle._f32p(dd.copy()), C.byref(t), C.byref(f))
