@@ -410,7 +410,7 @@ def main():
         # DRAM bytes (read + write) per pixel from one ncu capture of a small case of the
         # same kernel, scaled to a full launch by its pixels (the per-pixel f64 sums are the
         # only DRAM traffic; planes and paths live on chip): profiles/*.md.
-        dram_bytes_per_pixel = {"batch": 12.9, "stress": 20.2}.get(args.workload)
+        dram_bytes_per_pixel = {"batch": 11.75, "stress": 19.7}.get(args.workload)
         total_pixels = sum(fs.width * fs.height for fs, _ in items)
         traffic = (dram_bytes_per_pixel * total_pixels / launches_per_step
                    if dram_bytes_per_pixel is not None else None)
