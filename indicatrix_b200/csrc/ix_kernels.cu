@@ -41,7 +41,19 @@ constexpr int WARPS_PER_CTA = 4;     // 128 threads
 constexpr int UNI_MINB_1 = 3;
 constexpr int UNI_MINB_2 = 4;
 
-typedef double PartSlot[TRACE_MAX_PPT][GROUPS_PER_WARP][3];
+// A path's camera sample: its seed and hero draw and its camera ray.
+struct PathSetup {
+    uint32_t seed;
+    float hero;
+    float o[3], d[3];
+};
+// A warp's shared scratch: each group's f64 partial sums per task pixel, and each
+// group's next PATH_PREP path setups.
+constexpr int PATH_PREP = 8;
+struct WarpScratch {
+    double part[TRACE_MAX_PPT][GROUPS_PER_WARP][3];
+    PathSetup setup[GROUPS_PER_WARP][PATH_PREP];
+};
 
 // What the attributed kernels record of a path (PathEvents, transport/path_events.rs:27),
 // reduced to what classify_path reads: group-uniform bits plus the first exit direction.
@@ -90,12 +102,14 @@ IX_DEV uint32_t classify_path(uint32_t ev, V3 exit_dir, V3 observer, const ExitS
 template <bool UNI, bool ATTR = false>
 IX_DEV uint32_t trace_task(const Group& g, const DevScene& S, const float4* __restrict__ planes,
                            uint32_t pixel0, uint32_t npix, uint32_t spp, uint32_t sample_offset,
-                           PartSlot& part, double* out, int accumulate, const AttrTask* at = nullptr) {
+                           WarpScratch& ws, double* out, int accumulate, const AttrTask* at = nullptr) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t gi = lane >> 3;
     const uint32_t total = npix * spp;
     const uint32_t max_bounces = S.s.max_bounces;
     uint32_t drops = 0;  // non-finite samples this lane dropped
+    auto& part = ws.part;
+    PathSetup* const setup = ws.setup[gi];
     if (g.c == 0)
         for (uint32_t j = 0; j < npix; ++j) {
             part[j][gi][0] = 0.0;
@@ -103,6 +117,7 @@ IX_DEV uint32_t trace_task(const Group& g, const DevScene& S, const float4* __re
             part[j][gi][2] = 0.0;
         }
     uint32_t q = gi;
+    uint32_t m = 0;  // the group's paths started so far: path m is q = gi + 4 m
     bool active = q < total;
     bool fresh = active;  // the group's next path still needs its setup
     uint32_t cur_j = active ? q / spp : 0;
@@ -114,7 +129,30 @@ IX_DEV uint32_t trace_task(const Group& g, const DevScene& S, const float4* __re
         // One setup site for the first path and every regenerated one keeps a single
         // copy of the setup code in the loop.
         if (fresh) {
-            group_init<UNI>(g, P, S, pixel0 + cur_j, sample_offset + (q - cur_j * spp));
+            // Camera samples are prepared PATH_PREP paths at a time, lane c taking the
+            // group's path m + c: one draw and camera ray per lane instead of the same
+            // one on all 8 lanes.  The path then starts from its prepared slot.
+            if (m % PATH_PREP == 0) {
+                const uint32_t qc = gi + GROUPS_PER_WARP * (m + (uint32_t)g.c);
+                if (qc < total) {
+                    const uint32_t jc = qc / spp;
+                    const uint32_t pixel = pixel0 + jc;
+                    const Draws dr = sample_draws(pixel, sample_offset + (qc - jc * spp));
+                    const ix_scene& sc = S.s;
+                    const Ray r = generate_ray(sc.camera, (float)(pixel % sc.width), (float)(pixel / sc.width),
+                                               (float)sc.width, (float)sc.height, dr.jx, dr.jy);
+                    PathSetup& ps = setup[g.c];
+                    ps.seed = dr.seed;
+                    ps.hero = dr.hero;
+                    ps.o[0] = r.origin.x, ps.o[1] = r.origin.y, ps.o[2] = r.origin.z;
+                    ps.d[0] = r.dir.x, ps.d[1] = r.dir.y, ps.d[2] = r.dir.z;
+                }
+                __syncwarp(g.mask);
+            }
+            const PathSetup& ps = setup[m % PATH_PREP];
+            const Ray r{v3(ps.o[0], ps.o[1], ps.o[2]), v3(ps.d[0], ps.d[1], ps.d[2])};
+            group_init_ray<UNI>(g, P, S, r, ps.seed, ps.hero);
+            ++m;
             fresh = false;
             ev = 0;
         }
@@ -194,7 +232,7 @@ IX_DEV uint32_t trace_task(const Group& g, const DevScene& S, const float4* __re
 template <int MINB, bool UNI>
 __global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_constant__ TraceLaunch L) {
     __shared__ float4 s_planes[IX_MAX_PLANES];
-    __shared__ PartSlot s_part[WARPS_PER_CTA];
+    __shared__ WarpScratch s_scratch[WARPS_PER_CTA];
     const float4* gplanes = reinterpret_cast<const float4*>(L.scene.planes);
     for (uint32_t i = threadIdx.x; i < L.scene.n_planes; i += blockDim.x) s_planes[i] = gplanes[i];
     __syncthreads();
@@ -212,7 +250,7 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_c
         const uint32_t local0 = task * ppt;
         const uint32_t npix = min(ppt, L.n_pixels - local0);
         drops += trace_task<UNI>(g, S, s_planes, L.pixel_begin + local0, npix, L.spp, L.sample_offset,
-                                 s_part[threadIdx.x >> 5], L.out + (size_t)local0 * 3, L.accumulate);
+                                 s_scratch[threadIdx.x >> 5], L.out + (size_t)local0 * 3, L.accumulate);
     }
     if (drops && L.dropped) atomicAdd(L.dropped, (unsigned long long)drops);
 }
@@ -224,7 +262,7 @@ template <int MINB, bool UNI>
 __global__ void __launch_bounds__(128, MINB)
     IX_SFX(trace_attributed_kernel)(const __grid_constant__ TraceLaunch L, const __grid_constant__ AttrLaunch A) {
     __shared__ float4 s_planes[IX_MAX_PLANES];
-    __shared__ PartSlot s_part[WARPS_PER_CTA];
+    __shared__ WarpScratch s_scratch[WARPS_PER_CTA];
     __shared__ float s_rad[96];
     __shared__ float s_threshold;
     const float4* gplanes = reinterpret_cast<const float4*>(L.scene.planes);
@@ -247,7 +285,7 @@ __global__ void __launch_bounds__(128, MINB)
         const uint32_t npix = min(ppt, L.n_pixels - local0);
         const AttrTask at{&scorer, A.cls, A.y, L.n_pixels, local0};
         drops += trace_task<UNI, true>(g, S, s_planes, L.pixel_begin + local0, npix, L.spp, L.sample_offset,
-                                       s_part[threadIdx.x >> 5], L.out + (size_t)local0 * 3, L.accumulate, &at);
+                                       s_scratch[threadIdx.x >> 5], L.out + (size_t)local0 * 3, L.accumulate, &at);
     }
     if (drops && L.dropped) atomicAdd(L.dropped, (unsigned long long)drops);
 }
@@ -287,7 +325,7 @@ __global__ void __launch_bounds__(128) IX_SFX(attribution_fold_kernel)(const __g
 template <int MINB, bool UNI>
 __global__ void __launch_bounds__(128, MINB) IX_SFX(batch_kernel)(const __grid_constant__ BatchLaunch L) {
     __shared__ float4 s_planes[WARPS_PER_CTA][IX_MAX_PLANES];
-    __shared__ PartSlot s_part[WARPS_PER_CTA];
+    __shared__ WarpScratch s_scratch[WARPS_PER_CTA];
     const Group g = make_group();
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = threadIdx.x >> 5;
@@ -318,7 +356,7 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(batch_kernel)(const __grid_c
         const DevScene S = make_scene(sc, L.flags[job.scene]);
         const uint32_t local0 = (task - job.task_begin) * job.ppt;
         const uint32_t npix = min(job.ppt, job.n_pixels - local0);
-        drops += trace_task<UNI>(g, S, s_planes[warp], local0, npix, job.spp, job.sample_offset, s_part[warp],
+        drops += trace_task<UNI>(g, S, s_planes[warp], local0, npix, job.spp, job.sample_offset, s_scratch[warp],
                                  L.out + job.out_offset + (size_t)local0 * 3, L.accumulate);
     }
     if (drops && L.dropped) atomicAdd(L.dropped, (unsigned long long)drops);
