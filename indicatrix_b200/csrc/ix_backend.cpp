@@ -26,6 +26,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 struct ix_backend {
@@ -60,6 +61,8 @@ struct ix_backend {
     size_t hattr_map_cap = 0;
     int sm_count = 0;
     uint32_t variant = 0;
+    // Register variant new batch plans start from: the last autotuner pick (or `variant`).
+    uint32_t batch_variant = 0;
     // Resident CTAs per SM by [uniaxial instantiation][variant].
     int bps_exact[2][3] = {{1, 1, 1}, {1, 1, 1}}, bps_fast[2][3] = {{1, 1, 1}, {1, 1, 1}};
     // ... and of the attributed trace kernels by [uniaxial instantiation].
@@ -477,6 +480,7 @@ ix_backend* ix_backend_create(const ix_backend_options* opts) {
     // Option 0 = the measured default (8 CTAs per SM); 1/2/3 = unconstrained / 6 / 8.
     b->variant = 2;
     if (opts && opts->kernel_variant >= 1 && opts->kernel_variant <= 3) b->variant = opts->kernel_variant - 1;
+    b->batch_variant = b->variant;
     return b;
 }
 
@@ -689,6 +693,37 @@ cudaError_t plan_enqueue(ix_batch_plan* p, cudaStream_t st, uint32_t variant) {
     return exact ? ix::launch_batch_exact(L, st) : ix::launch_batch_fast(L, st);
 }
 
+// ix_batch_plan_run / ix_batch_plan_download for a caller that already holds the
+// backend's turn.
+int plan_run_locked(ix_batch_plan* p, cudaStream_t st) {
+    ix_backend* b = p->b;
+    if (fail(b, cudaSetDevice(b->device), "set device")) return IX_DECLINED;
+    if (!p->exec || p->graph_stream != st || p->graph_variant != (int)p->variant) {
+        plan_free_graph(p);
+        if (fail(b, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture")) return IX_DECLINED;
+        cudaError_t e = plan_enqueue(p, st, p->variant);
+        cudaError_t e2 = cudaStreamEndCapture(st, &p->graph);
+        if (fail(b, e, "batch launch") || fail(b, e2, "graph capture")) return IX_DECLINED;
+        if (fail(b, cudaGraphInstantiate(&p->exec, p->graph, 0), "graph instantiate")) return IX_DECLINED;
+        p->graph_stream = st;
+        p->graph_variant = (int)p->variant;
+    }
+    if (fail(b, cudaEventRecord(b->ev0, st), "event")) return IX_DECLINED;
+    if (fail(b, cudaGraphLaunch(p->exec, st), "graph launch")) return IX_DECLINED;
+    if (fail(b, cudaEventRecord(b->ev1, st), "event")) return IX_DECLINED;
+    b->timing.paths = p->paths;
+    b->timing.launches = 1;
+    return IX_DONE;
+}
+int plan_download_locked(ix_batch_plan* p, double* host_out) {
+    ix_backend* b = p->b;
+    if (fail(b, cudaMemcpyAsync(host_out, p->d_out, p->out_doubles * sizeof(double), cudaMemcpyDeviceToHost,
+                                b->stream), "batch download"))
+        return -1;
+    if (fail(b, cudaStreamSynchronize(b->stream), "batch download")) return -1;
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -761,7 +796,7 @@ ix_batch_plan* ix_batch_plan_create(ix_backend* b, const ix_scene* scenes, uint3
          cudaMemcpy(p->d_flags, flags.data(), n_scenes * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(p->d_jobs, p->jobs.data(), n_jobs * sizeof(ix::BatchJob), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemset(p->d_dropped, 0, sizeof(unsigned long long)) == cudaSuccess;
-    p->variant = b->variant;
+    p->variant = b->batch_variant;
     if (!ok) {
         fail(b, cudaGetLastError(), "batch plan");
         ix_batch_plan_destroy(p);
@@ -772,26 +807,8 @@ ix_batch_plan* ix_batch_plan_create(ix_backend* b, const ix_scene* scenes, uint3
 
 int ix_batch_plan_run(ix_batch_plan* p, void* stream) {
     if (!p || p->b->lost) return IX_DECLINED;
-    ix_backend* b = p->b;
-    Turn turn(b);
-    cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
-    if (fail(b, cudaSetDevice(b->device), "set device")) return IX_DECLINED;
-    if (!p->exec || p->graph_stream != st || p->graph_variant != (int)p->variant) {
-        plan_free_graph(p);
-        if (fail(b, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture")) return IX_DECLINED;
-        cudaError_t e = plan_enqueue(p, st, p->variant);
-        cudaError_t e2 = cudaStreamEndCapture(st, &p->graph);
-        if (fail(b, e, "batch launch") || fail(b, e2, "graph capture")) return IX_DECLINED;
-        if (fail(b, cudaGraphInstantiate(&p->exec, p->graph, 0), "graph instantiate")) return IX_DECLINED;
-        p->graph_stream = st;
-        p->graph_variant = (int)p->variant;
-    }
-    if (fail(b, cudaEventRecord(b->ev0, st), "event")) return IX_DECLINED;
-    if (fail(b, cudaGraphLaunch(p->exec, st), "graph launch")) return IX_DECLINED;
-    if (fail(b, cudaEventRecord(b->ev1, st), "event")) return IX_DECLINED;
-    b->timing.paths = p->paths;
-    b->timing.launches = 1;
-    return IX_DONE;
+    Turn turn(p->b);
+    return plan_run_locked(p, stream ? (cudaStream_t)stream : p->b->stream);
 }
 
 int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen) {
@@ -816,19 +833,15 @@ int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen) {
     }
     p->variant = best_v;
     p->tuned = true;
+    b->batch_variant = best_v;  // later plans of this backend start from the pick
     if (chosen) *chosen = best_v;
     return 0;
 }
 
 int ix_batch_plan_download(ix_batch_plan* p, double* host_out) {
     if (!p || !host_out || p->b->lost) return -1;
-    ix_backend* b = p->b;
-    Turn turn(b);
-    if (fail(b, cudaMemcpyAsync(host_out, p->d_out, p->out_doubles * sizeof(double), cudaMemcpyDeviceToHost,
-                                b->stream), "batch download"))
-        return -1;
-    if (fail(b, cudaStreamSynchronize(b->stream), "batch download")) return -1;
-    return 0;
+    Turn turn(p->b);
+    return plan_download_locked(p, host_out);
 }
 
 uint64_t ix_batch_plan_output_size(const ix_batch_plan* p) { return p ? p->out_doubles : 0; }
@@ -884,16 +897,27 @@ int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items,
         ix_batch_plan* p = ix_batch_plan_create(b, scenes.data(), (uint32_t)scenes.size(), jobs.data(),
                                                 (uint32_t)jobs.size());
         if (!p) return IX_DECLINED;
-        std::vector<double> host(p->out_doubles);
-        bool ok = ix_batch_plan_run(p, nullptr) == IX_DONE && ix_batch_plan_download(p, host.data()) == 0;
+        // The sums come back through the backend's pinned staging buffer, all under one
+        // turn so no other call reuses it meanwhile.
+        Turn turn(b);
+        bool ok = !fail(b, grow_pinned(&b->h_sums, &b->hsums_cap, (size_t)p->out_doubles), "host alloc") &&
+                  plan_run_locked(p, b->stream) == IX_DONE && plan_download_locked(p, b->h_sums) == 0;
         if (ok && !(cancel && *cancel)) {
-            for (size_t k = 0; k < which.size(); ++k) {
-                ix_batch_item& it = items[which[k]];
-                const double* src = host.data() + p->job_out[k];
-                const size_t n = (size_t)it.scene->width * it.scene->height * 3;
-                for (size_t e = 0; e < n; ++e) it.accum_xyz[e] += src[e];
-                it.status = IX_DONE;
-            }
+            // Add into the callers' accumulators, items split over a few host threads.
+            const unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+            auto add = [&](unsigned t) {
+                for (size_t k = t; k < which.size(); k += nt) {
+                    ix_batch_item& it = items[which[k]];
+                    const double* src = b->h_sums + p->job_out[k];
+                    const size_t n = (size_t)it.scene->width * it.scene->height * 3;
+                    for (size_t e = 0; e < n; ++e) it.accum_xyz[e] += src[e];
+                }
+            };
+            std::vector<std::thread> pool;
+            for (unsigned t = 1; t < nt && t < which.size(); ++t) pool.emplace_back(add, t);
+            add(0);
+            for (auto& th : pool) th.join();
+            for (uint32_t k : which) items[k].status = IX_DONE;
         } else if (ok) {
             for (uint32_t k : which) items[k].status = IX_CANCELLED;
         }
