@@ -245,6 +245,25 @@ int ix_evaluate_gem_optical_metrics_batch(ix_backend* b, const ix_metrics_stone*
                                           uint32_t n_poses, uint32_t want_fire_and_scintillation,
                                           ix_gem_metrics* out);
 
+/* Tilt-performance sweeps over the batched metrics kernel, fire-less
+ * (MetricsWanted::CONSUMED_ONLY), all poses of a call in one launch. */
+#define IX_PROFILE_ANGLES 19   /* PROFILE_ANGLES_DEG (color/metrics/types.rs:27): 0, 5, ..., 90 */
+#define IX_AXIS_TILTS 181      /* TILT_ANGLES_DEG (profile.rs:146): -90, ..., 90 */
+/* evaluate_angular_profile_at_azimuth (color/metrics/profile.rs:37): brilliance,
+ * extinction and windowing at the 19 camera elevations of PROFILE_ANGLES_DEG, azimuth
+ * cam_yaw (radians).  `out`: 3 x 19 floats, the three curves in that order. */
+int ix_evaluate_angular_profile_at_azimuth(ix_backend* b, const float* planes, uint32_t n_planes,
+                                           const ix_material* material, float cam_yaw,
+                                           const ix_metrics_lighting* lighting, float* out);
+/* evaluate_full_axis_profile_at_azimuth (profile.rs:200) for each of n_axes positive
+ * azimuths (degrees): `out` is n_axes x 3 x 181 floats, the brilliance, extinction and
+ * windowing curves indexed by tilt away from table-up + 90 degrees.  With the azimuths
+ * {0, 45, 90, 135} (PROFILE_AZIMUTHS_DEG) this is evaluate_all_axes_profiles
+ * (sweep.rs:74): 724 poses. */
+int ix_evaluate_axis_profiles(ix_backend* b, const float* planes, uint32_t n_planes, const ix_material* material,
+                              const float* azimuths_deg, uint32_t n_axes, const ix_metrics_lighting* lighting,
+                              float* out);
+
 /* ix_accumulate_f64 with spectral attribution: every sample is traced as the plain entry
  * traces it (the same XYZ bits) with its hero path's events recorded
  * (trace_spectral_ray_attributed_soa_geom, transport/attributed.rs:28), labelled by

@@ -3,7 +3,7 @@
 These structures are the C-ABI encoding of the reference's ``GpuSceneRef``
 (crates/indicatrix/src/renderer/gpu_backend/mod.rs:218-237) and of the backend's
 options, batch items and status codes.  Every field matches the C header one for one;
-``tests/test_abi.py`` checks sizes and offsets against the compiled library.
+``tests/test_host.py`` checks sizes and offsets against the C headers.
 """
 from __future__ import annotations
 
@@ -184,6 +184,14 @@ class MetricsLighting(C.Structure):
         ("head_shadow_deg", C.c_float),
     ]
 
+
+# Tilt-performance sweeps (include/ix_cuda.h): PROFILE_ANGLES_DEG (color/metrics/types.rs:27),
+# TILT_ANGLES_DEG (profile.rs:146) and PROFILE_AZIMUTHS_DEG (profile.rs:26).
+PROFILE_ANGLES = 19
+AXIS_TILTS = 181
+PROFILE_ANGLES_DEG = [5.0 * i for i in range(PROFILE_ANGLES)]
+TILT_ANGLES_DEG = [float(i - 90) for i in range(AXIS_TILTS)]
+PROFILE_AZIMUTHS_DEG = [0.0, 45.0, 90.0, 135.0]
 
 # Spectral attribution (include/ix_attribution.h): the class slots of
 # renderer/attribution_map.rs:17-36 and the code of a camera ray that missed the stone.

@@ -24,7 +24,7 @@ import enum
 import os
 import threading
 from dataclasses import dataclass, field
-from typing import Callable, Optional, Sequence
+from typing import Callable, List, Optional, Sequence
 
 import numpy as np
 
@@ -99,6 +99,12 @@ def load_library() -> C.CDLL:
         lib.ix_evaluate_gem_optical_metrics_batch.argtypes = [C.c_void_p, P(abi.MetricsStone), C.c_uint32,
                                                               P(abi.MetricsLighting), P(abi.MetricsPose),
                                                               C.c_uint32, C.c_uint32, P(abi.GemMetrics)]
+        lib.ix_evaluate_angular_profile_at_azimuth.argtypes = [C.c_void_p, P(C.c_float), C.c_uint32,
+                                                               P(abi.Material), C.c_float,
+                                                               P(abi.MetricsLighting), P(C.c_float)]
+        lib.ix_evaluate_axis_profiles.argtypes = [C.c_void_p, P(C.c_float), C.c_uint32, P(abi.Material),
+                                                  P(C.c_float), C.c_uint32, P(abi.MetricsLighting),
+                                                  P(C.c_float)]
         lib.ix_accumulate_attributed.argtypes = [C.c_void_p, P(abi.Scene), P(abi.MetricsLighting), C.c_uint32,
                                                  C.c_uint32, P(C.c_double), C.c_void_p, P(C.c_int32)]
         _lib = lib
@@ -237,6 +243,16 @@ class MetricsLighting:
     def to_abi(self) -> abi.MetricsLighting:
         return abi.MetricsLighting(int(self.preset), float(self.light_yaw), float(self.light_pitch),
                                    float(self.head_shadow_deg))
+
+
+@dataclass
+class AxisProfile:
+    """AxisProfile (color/metrics/sweep.rs:20): the three 181-point curves of one axis,
+    indexed by tilt away from table-up + 90 degrees (TILT_ANGLES_DEG)."""
+
+    brilliance: np.ndarray
+    extinction: np.ndarray
+    windowing: np.ndarray
 
 
 @dataclass
@@ -450,6 +466,57 @@ class GpuBackend:
             return None
         return np.array([out.brilliance_pct, out.fire_index, out.scintillation_pct, out.windowing_pct,
                          out.extinction_pct], np.float32)
+
+    def evaluate_angular_profile_at_azimuth(self, planes: np.ndarray, material: abi.Material, cam_yaw: float,
+                                            lighting: "MetricsLighting"):
+        """evaluate_angular_profile_at_azimuth (color/metrics/profile.rs:37): (brilliance,
+        extinction, windowing) float32 curves over PROFILE_ANGLES_DEG, or None when
+        declined."""
+        if not self._h:
+            return None
+        p = np.ascontiguousarray(planes, np.float32)
+        out = np.zeros(3 * abi.PROFILE_ANGLES, np.float32)
+        rc = self._lib.ix_evaluate_angular_profile_at_azimuth(
+            self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.shape[0], C.byref(material), cam_yaw,
+            C.byref(lighting.to_abi()), out.ctypes.data_as(C.POINTER(C.c_float)))
+        if rc != abi.IX_DONE:
+            return None
+        b, e, w = out.reshape(3, abi.PROFILE_ANGLES)
+        return b.copy(), e.copy(), w.copy()
+
+    def evaluate_angular_profile(self, planes: np.ndarray, material: abi.Material, lighting: "MetricsLighting"):
+        """evaluate_angular_profile (profile.rs:379): the profile at azimuth 0."""
+        return self.evaluate_angular_profile_at_azimuth(planes, material, 0.0, lighting)
+
+    def evaluate_axis_profiles(self, planes: np.ndarray, material: abi.Material, azimuths_deg: Sequence[float],
+                               lighting: "MetricsLighting") -> Optional[List["AxisProfile"]]:
+        """evaluate_full_axis_profile_at_azimuth (profile.rs:200) for each positive azimuth
+        (degrees), all poses in one launch; None when declined."""
+        if not self._h:
+            return None
+        p = np.ascontiguousarray(planes, np.float32)
+        az = np.ascontiguousarray(azimuths_deg, np.float32)
+        out = np.zeros((len(az), 3, abi.AXIS_TILTS), np.float32)
+        rc = self._lib.ix_evaluate_axis_profiles(
+            self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.shape[0], C.byref(material),
+            az.ctypes.data_as(C.POINTER(C.c_float)), len(az), C.byref(lighting.to_abi()),
+            out.ctypes.data_as(C.POINTER(C.c_float)))
+        if rc != abi.IX_DONE:
+            return None
+        return [AxisProfile(o[0].copy(), o[1].copy(), o[2].copy()) for o in out]
+
+    def evaluate_full_axis_profile_at_azimuth(self, planes: np.ndarray, material: abi.Material,
+                                              positive_azimuth_deg: float, lighting: "MetricsLighting"):
+        """evaluate_full_axis_profile_at_azimuth (profile.rs:200): (brilliance, extinction,
+        windowing) over TILT_ANGLES_DEG, or None when declined."""
+        r = self.evaluate_axis_profiles(planes, material, [positive_azimuth_deg], lighting)
+        return None if r is None else (r[0].brilliance, r[0].extinction, r[0].windowing)
+
+    def evaluate_all_axes_profiles(self, planes: np.ndarray, material: abi.Material,
+                                   lighting: "MetricsLighting") -> Optional[List["AxisProfile"]]:
+        """evaluate_all_axes_profiles (sweep.rs:74): one AxisProfile per
+        PROFILE_AZIMUTHS_DEG entry (724 poses, one launch)."""
+        return self.evaluate_axis_profiles(planes, material, abi.PROFILE_AZIMUTHS_DEG, lighting)
 
     def evaluate_metrics_batch(self, stones: Sequence[tuple], poses: Sequence[tuple], lighting: "MetricsLighting",
                                want_fire_and_scintillation: bool = True) -> Optional[np.ndarray]:

