@@ -59,6 +59,9 @@ struct ix_backend {
     size_t attr_map_cap = 0;
     ix_attribution_pixel* h_attr_map = nullptr;
     size_t hattr_map_cap = 0;
+    // The one-shot batch entry's device sums.
+    double* d_batch_out = nullptr;
+    size_t batch_out_cap = 0;
     int sm_count = 0;
     uint32_t variant = 0;
     // Register variant new batch plans start from: the last autotuner pick (or `variant`).
@@ -498,6 +501,7 @@ void ix_backend_destroy(ix_backend* b) {
     cudaFree(b->d_attr_cls);
     cudaFree(b->d_attr_y);
     cudaFree(b->d_attr_map);
+    cudaFree(b->d_batch_out);
     if (b->h_attr_map) cudaFreeHost(b->h_attr_map);
     if (b->h_sums) cudaFreeHost(b->h_sums);
     if (b->ev0) cudaEventDestroy(b->ev0);
@@ -660,6 +664,7 @@ struct ix_batch_plan {
     int graph_variant = -1;
     uint32_t variant = 0;
     bool tuned = false;
+    bool out_pooled = false;  // d_out is the backend's pooled buffer
 };
 
 namespace {
@@ -730,12 +735,11 @@ int plan_download_locked(ix_batch_plan* p, double* host_out) {
 
 extern "C" {
 
-ix_batch_plan* ix_batch_plan_create(ix_backend* b, const ix_scene* scenes, uint32_t n_scenes,
-                                    const ix_batch_job* jobs, uint32_t n_jobs) {
-    if (!b || !scenes || !jobs || n_scenes == 0 || n_jobs == 0 || b->lost) return nullptr;
-    for (uint32_t i = 0; i < n_scenes; ++i)
-        if (!ix_scene_routes_to_gpu(&scenes[i])) return nullptr;
-    Turn turn(b);
+// ix_batch_plan_create for a caller that holds the backend's turn.  With `pooled_out` the
+// plan's sums live in the backend's pooled device buffer (the one-shot batch entry, which
+// destroys its plan within the same turn).
+static ix_batch_plan* plan_create_locked(ix_backend* b, const ix_scene* scenes, uint32_t n_scenes,
+                                         const ix_batch_job* jobs, uint32_t n_jobs, bool pooled_out) {
     if (fail(b, cudaSetDevice(b->device), "set device")) return nullptr;
     ix_batch_plan* p = new ix_batch_plan();
     p->b = b;
@@ -790,9 +794,14 @@ ix_batch_plan* ix_batch_plan_create(ix_backend* b, const ix_scene* scenes, uint3
     ok = ok && cudaMalloc((void**)&p->d_scenes, n_scenes * sizeof(ix_scene)) == cudaSuccess &&
          cudaMalloc((void**)&p->d_flags, n_scenes * sizeof(uint32_t)) == cudaSuccess &&
          cudaMalloc((void**)&p->d_jobs, n_jobs * sizeof(ix::BatchJob)) == cudaSuccess &&
-         cudaMalloc((void**)&p->d_out, std::max<uint64_t>(out, 1) * sizeof(double)) == cudaSuccess &&
+         (pooled_out ? grow_device(&b->d_batch_out, &b->batch_out_cap, std::max<uint64_t>(out, 1))
+                     : cudaMalloc((void**)&p->d_out, std::max<uint64_t>(out, 1) * sizeof(double))) == cudaSuccess &&
          cudaMalloc((void**)&p->d_counter, sizeof(uint32_t)) == cudaSuccess &&
          cudaMalloc((void**)&p->d_dropped, sizeof(unsigned long long)) == cudaSuccess;
+    if (ok && pooled_out) {
+        p->d_out = b->d_batch_out;
+        p->out_pooled = true;
+    }
     ok = ok && cudaMemcpy(p->d_planes, planes.data(), planes.size() * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(p->d_scenes, dev_scenes.data(), n_scenes * sizeof(ix_scene), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(p->d_flags, flags.data(), n_scenes * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess &&
@@ -805,6 +814,15 @@ ix_batch_plan* ix_batch_plan_create(ix_backend* b, const ix_scene* scenes, uint3
         return nullptr;
     }
     return p;
+}
+
+ix_batch_plan* ix_batch_plan_create(ix_backend* b, const ix_scene* scenes, uint32_t n_scenes,
+                                    const ix_batch_job* jobs, uint32_t n_jobs) {
+    if (!b || !scenes || !jobs || n_scenes == 0 || n_jobs == 0 || b->lost) return nullptr;
+    for (uint32_t i = 0; i < n_scenes; ++i)
+        if (!ix_scene_routes_to_gpu(&scenes[i])) return nullptr;
+    Turn turn(b);
+    return plan_create_locked(b, scenes, n_scenes, jobs, n_jobs, false);
 }
 
 int ix_batch_plan_run(ix_batch_plan* p, void* stream) {
@@ -864,7 +882,7 @@ void ix_batch_plan_destroy(ix_batch_plan* p) {
     cudaFree(p->d_flags);
     cudaFree(p->d_jobs);
     cudaFree(p->d_planes);
-    cudaFree(p->d_out);
+    if (!p->out_pooled) cudaFree(p->d_out);
     cudaFree(p->d_counter);
     cudaFree(p->d_dropped);
     (void)cudaGetLastError();
@@ -896,12 +914,14 @@ int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items,
         which.push_back(i);
     }
     if (!jobs.empty()) {
-        ix_batch_plan* p = ix_batch_plan_create(b, scenes.data(), (uint32_t)scenes.size(), jobs.data(),
-                                                (uint32_t)jobs.size());
-        if (!p) return IX_DECLINED;
-        // The sums come back through the backend's pinned staging buffer, all under one
-        // turn so no other call reuses it meanwhile.
+        if (b->lost) return IX_DECLINED;
+        // One turn for the whole call: the plan's sums sit in the backend's pooled device
+        // buffer and come back through its pinned staging buffer, which no other call may
+        // touch meanwhile.
         Turn turn(b);
+        ix_batch_plan* p = plan_create_locked(b, scenes.data(), (uint32_t)scenes.size(), jobs.data(),
+                                              (uint32_t)jobs.size(), true);
+        if (!p) return IX_DECLINED;
         bool ok = !fail(b, grow_pinned(&b->h_sums, &b->hsums_cap, (size_t)p->out_doubles), "host alloc") &&
                   plan_run_locked(p, b->stream) == IX_DONE && plan_download_locked(p, b->h_sums) == 0;
         if (ok && !(cancel && *cancel)) {
