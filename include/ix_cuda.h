@@ -47,7 +47,7 @@ typedef struct ix_backend_options {
     uint32_t pipeline;           /* IX_PIPELINE_*                                        */
     uint32_t precision;          /* IX_PRECISION_*                                       */
     uint32_t threads_per_block;  /* 0 = autotuned                                        */
-    uint64_t chunk_paths;        /* paths per launch; 0 = default (TDR-safe first chunk)  */
+    uint64_t chunk_paths;        /* paths per launch; 0 = default (2^26)                   */
     uint32_t kernel_variant;     /* register budget of the megakernel: 0 default (eight    */
                                  /* CTAs per SM), 1 unconstrained, 2 six, 3 eight CTAs/SM   */
 } ix_backend_options;
@@ -91,7 +91,9 @@ void ix_set_work_limits(ix_backend* b, const ix_work_limits* limits);
 /* Rounding mode of later calls (IX_PRECISION_*). */
 void ix_set_precision(ix_backend* b, uint32_t precision);
 /* scene_routes_to_gpu (gpu_backend/mod.rs:288): 1 when this backend can trace `scene`
- * (convex, all facets polished, no scattering, isotropic material, <= IX_MAX_PLANES). */
+ * (convex, <= IX_MAX_PLANES, polished or frosted facets, no volume scattering or edge
+ * rounding, an isotropic or uniaxial material with modelled dispersion, a modelled
+ * environment).  The facet finishes are not read here. */
 int ix_scene_routes_to_gpu(const ix_scene* scene);
 /* GpuBackend::try_accumulate_geom_cancellable (backend.rs:272) with an f32 accumulator:
  * adds (float)(f64 pixel sum) into accum_xyz.  `cancel` may be NULL; it is polled
@@ -134,8 +136,9 @@ uint32_t ix_batch_plan_variant(const ix_batch_plan* p);
 uint64_t ix_batch_plan_job_offset(const ix_batch_plan* p, uint32_t job);
 void ix_batch_plan_destroy(ix_batch_plan* p);
 /* Device-resident form for callers that keep the scene and the sums in GPU memory:
- * `scene->planes` and `d_accum_xyz` are device pointers; the launch is enqueued on
- * `stream` (a cudaStream_t, or NULL for the backend's own stream) and not synchronised.
+ * `scene->planes`, `scene->facet_finishes` (if any) and `d_accum_xyz` are device
+ * pointers; the launch is enqueued on `stream` (a cudaStream_t, or NULL for the
+ * backend's own stream) and not synchronised.
  * `accumulate` = 1 adds into d_accum_xyz, 0 overwrites it. */
 int ix_accumulate_device(ix_backend* b, const ix_scene* scene, uint32_t sample_offset,
                          uint32_t spp, double* d_accum_xyz, int accumulate, void* stream);
@@ -143,7 +146,8 @@ int ix_accumulate_device(ix_backend* b, const ix_scene* scene, uint32_t sample_o
  *
  * For callers that cannot call cudaMalloc (a host whose own pool or arena owns all
  * device memory, a sandboxed plug-in, a runtime with a fixed memory budget): they pass
- * a scene whose `planes` is a device pointer and a device output `d_accum_xyz`
+ * a scene whose `planes` (and `facet_finishes`, if any) are device pointers and a device
+ * output `d_accum_xyz`
  * (width * height * 3 doubles, added into when `accumulate` is 1, overwritten when 0),
  * and the call needs no backend object and makes no cudaMalloc, cudaFree or other
  * allocating call.  The kernel's work counters live in a 264-byte array in device

@@ -113,8 +113,9 @@ typedef struct ix_environment {
 } ix_environment;
 
 /* The scene.  `planes` is n_planes x {nx, ny, nz, d} with the convention n.x + d <= 0
- * inside (geometry/plane.rs:34-41).  `facet_finishes` may be NULL (all polished);
- * a nonzero entry marks a frosted facet, which the CUDA backend declines. */
+ * inside (geometry/plane.rs:34-41).  `facet_finishes` may be NULL (all polished); entry
+ * i is facet i's FacetFinish (0 Polished, nonzero Frosted), facets past n_finishes are
+ * polished. */
 typedef struct ix_scene {
     ix_camera camera;
     uint32_t width;

@@ -62,6 +62,9 @@ struct ix_backend {
     // The one-shot batch entry's device sums.
     double* d_batch_out = nullptr;
     size_t batch_out_cap = 0;
+    // A host scene's per-facet finishes, copied for the kernels.
+    uint8_t* d_finishes = nullptr;
+    size_t finishes_cap = 0;
     int sm_count = 0;
     uint32_t variant = 0;
     // Register variant new batch plans start from: the last autotuner pick (or `variant`).
@@ -210,6 +213,22 @@ int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uin
     return launches;
 }
 
+// Points a device copy of host scene `sc` at the backend's copy of its facet finishes
+// (none: all polished).  Caller holds the turn.  False on a CUDA error.
+bool upload_finishes(ix_backend* b, ix_scene& sc, cudaStream_t st) {
+    if (!sc.facet_finishes || sc.n_finishes == 0) {
+        sc.facet_finishes = nullptr;
+        sc.n_finishes = 0;
+        return true;
+    }
+    if (fail(b, grow_device(&b->d_finishes, &b->finishes_cap, (size_t)sc.n_finishes), "finishes alloc") ||
+        fail(b, cudaMemcpyAsync(b->d_finishes, sc.facet_finishes, sc.n_finishes, cudaMemcpyHostToDevice, st),
+             "finishes upload"))
+        return false;
+    sc.facet_finishes = b->d_finishes;
+    return true;
+}
+
 template <typename AccT>
 int accumulate_impl(ix_backend* b, const ix_scene* scene, uint32_t sample_offset, uint32_t spp,
                     AccT* accum, const volatile int32_t* cancel) {
@@ -238,8 +257,7 @@ int accumulate_impl(ix_backend* b, const ix_scene* scene, uint32_t sample_offset
         return IX_DECLINED;
     ix_scene sc = *scene;
     sc.planes = b->d_planes;
-    sc.facet_finishes = nullptr;
-    sc.n_finishes = 0;
+    if (!upload_finishes(b, sc, b->stream)) return IX_DECLINED;
     bool cancelled = false;
     if (fail(b, cudaEventRecord(b->ev0, b->stream), "event")) return IX_DECLINED;
     int launches = enqueue_frame(b, sc, sample_offset, spp, b->d_sums, 0, b->stream, cancel, &cancelled);
@@ -502,6 +520,7 @@ void ix_backend_destroy(ix_backend* b) {
     cudaFree(b->d_attr_y);
     cudaFree(b->d_attr_map);
     cudaFree(b->d_batch_out);
+    cudaFree(b->d_finishes);
     if (b->h_attr_map) cudaFreeHost(b->h_attr_map);
     if (b->h_sums) cudaFreeHost(b->h_sums);
     if (b->ev0) cudaEventDestroy(b->ev0);
@@ -536,9 +555,6 @@ int ix_scene_routes_to_gpu(const ix_scene* s) {
     const ix_material& m = s->material;
     if (m.scattering_sigma_s > 0.0f || m.edge_rounding_radius > 0.0f) return 0;
     if (m.has_e_dispersion && m.e_dispersion.kind > IX_DISP_CAUCHY) return 0;
-    if (s->facet_finishes)
-        for (uint32_t i = 0; i < s->n_finishes; ++i)
-            if (s->facet_finishes[i] != 0) return 0;
     const ix_environment& e = s->environment;
     if (e.model != IX_ENV_STUDIO && e.model != IX_ENV_ISO_HEMISPHERE && e.model != IX_ENV_UNIFORM) return 0;
     if (m.dispersion.kind > IX_DISP_CAUCHY) return 0;
@@ -599,8 +615,7 @@ int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metr
         return IX_DECLINED;
     ix_scene sc = *scene;
     sc.planes = b->d_planes;
-    sc.facet_finishes = nullptr;
-    sc.n_finishes = 0;
+    if (!upload_finishes(b, sc, b->stream)) return IX_DECLINED;
     A.cls = b->d_attr_cls;
     A.y = b->d_attr_y;
     bool cancelled = false;
@@ -665,6 +680,7 @@ struct ix_batch_plan {
     uint32_t variant = 0;
     bool tuned = false;
     bool out_pooled = false;  // d_out is the backend's pooled buffer
+    uint8_t* d_finishes = nullptr;  // every scene's facet finishes, back to back
 };
 
 namespace {
@@ -780,13 +796,25 @@ static ix_batch_plan* plan_create_locked(ix_backend* b, const ix_scene* scenes, 
     std::vector<ix_scene> dev_scenes(scenes, scenes + n_scenes);
     std::vector<uint32_t> flags(n_scenes);
     std::vector<float> planes(std::max<uint64_t>(plane_floats, 4));
+    std::vector<uint8_t> finishes;
+    std::vector<size_t> finish_off(n_scenes, 0);
+    for (uint32_t i = 0; i < n_scenes; ++i)
+        if (scenes[i].facet_finishes && scenes[i].n_finishes) {
+            finish_off[i] = finishes.size();
+            finishes.insert(finishes.end(), scenes[i].facet_finishes,
+                            scenes[i].facet_finishes + scenes[i].n_finishes);
+        }
     uint64_t off = 0;
     bool ok = cudaMalloc((void**)&p->d_planes, planes.size() * sizeof(float)) == cudaSuccess;
+    ok = ok && (finishes.empty() || (cudaMalloc((void**)&p->d_finishes, finishes.size()) == cudaSuccess &&
+                                     cudaMemcpy(p->d_finishes, finishes.data(), finishes.size(),
+                                                cudaMemcpyHostToDevice) == cudaSuccess));
     for (uint32_t i = 0; ok && i < n_scenes; ++i) {
         std::memcpy(planes.data() + off, scenes[i].planes, (size_t)scenes[i].n_planes * 16);
         dev_scenes[i].planes = p->d_planes + off;
-        dev_scenes[i].facet_finishes = nullptr;
-        dev_scenes[i].n_finishes = 0;
+        const bool has_finishes = scenes[i].facet_finishes && scenes[i].n_finishes;
+        dev_scenes[i].facet_finishes = has_finishes ? p->d_finishes + finish_off[i] : nullptr;
+        dev_scenes[i].n_finishes = has_finishes ? scenes[i].n_finishes : 0;
         flags[i] = ix::scene_flags(scenes[i].material);
         if (ix::needs_uniaxial_kernel(flags[i])) p->uniaxial = 1;
         off += (uint64_t)scenes[i].n_planes * 4;
@@ -882,6 +910,7 @@ void ix_batch_plan_destroy(ix_batch_plan* p) {
     cudaFree(p->d_flags);
     cudaFree(p->d_jobs);
     cudaFree(p->d_planes);
+    cudaFree(p->d_finishes);
     if (!p->out_pooled) cudaFree(p->d_out);
     cudaFree(p->d_counter);
     cudaFree(p->d_dropped);
@@ -1281,7 +1310,7 @@ int ix_debug_check(ix_backend* b, const ix_scene* scene, int32_t fn, uint32_t n,
     std::memset(&L, 0, sizeof(L));
     L.scene = *scene;
     L.scene.planes = b->d_planes;
-    L.scene.facet_finishes = nullptr;
+    if (!upload_finishes(b, L.scene, b->stream)) return -1;
     L.flags = ix::scene_flags(scene->material);
     L.fn = fn;
     L.n = n;

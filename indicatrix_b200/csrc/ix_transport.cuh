@@ -372,6 +372,68 @@ IX_DEV Stokes lane_scalar_reflect(LanePath& P, float n1k, float n2k, float s2k, 
     return fresnel_reflect_apply(P.st, rs, rp);
 }
 
+// ------------------------------------------------------------------------------------
+// Frosted (bruted) facets: apply_frosted_bounce (optics/raytracer/scattering/frosted.rs:289)
+// without next-event estimation, which the reference enables only for an HDR map or the
+// DaylightSun model (environment_supports_nee, environment/nee.rs:60), neither of which
+// this path carries.
+// ------------------------------------------------------------------------------------
+constexpr uint32_t FROSTED_DIR_U_STREAM = 0x27D4EB2Fu;  // sampling.rs:24
+constexpr uint32_t FROSTED_DIR_V_STREAM = 0x165667B1u;  // sampling.rs:25
+
+// facet_finish_for (bounce_body.rs:656): Polished past the end of the finish list.
+IX_DEV bool facet_frosted(const DevScene& S, int f) {
+    return S.s.facet_finishes && (uint32_t)f < S.s.n_finishes && S.s.facet_finishes[f] != 0;
+}
+// cosine_weighted_hemisphere (frosted.rs:34) on frosted_orthonormal_basis
+// (scattering/mod.rs:110): the angle is (2 pi) u2, the three scaled basis vectors are
+// summed left to right.
+IX_DEV V3 cosine_weighted_hemisphere(float u1, float u2, V3 n) {
+    const float r = sqrtf(u1);
+    const float theta = (2.0f * 3.14159265358979323846f) * u2;
+    float sin_t, cos_t;
+    sincosf(theta, &sin_t, &cos_t);
+    const V3 a = fabsf(n.x) > 0.9f ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
+    const V3 t = normalize_or_zero(a - n * dot(n, a));
+    const V3 b = cross(n, t);
+    return normalize_or_zero((t * (r * cos_t) + b * (r * sin_t)) + n * sqrtf(fmaxf(1.0f - u1, 0.0f)));
+}
+// The frosted bounce of one channel: a cosine-weighted diffuse reflection or
+// transmission, chosen by the hero's unpolarised Fresnel reflectance (n1, n2, cos_i,
+// sin2_t are the hero's geometry, identical in the 8 lanes), always reflection past the
+// hero's critical angle.  Returns the new direction (the same in every lane), the factor
+// the channel's path pdf takes (the chosen branch's probability) and whether the ray
+// crossed the facet; the caller depolarises the channel.  Out of line and by value, so
+// the polished bounce around the call compiles exactly as it does without it (the fast
+// build's multiply-add contraction, and with it every sum, stays the same in every
+// kernel that inlines the bounce).
+struct FrostedScatter {
+    V3 dir;
+    float pdf_factor;
+    int transmit;
+};
+static __device__ __noinline__ FrostedScatter frosted_scatter(uint32_t seed, uint32_t bounce, V3 normal, float n1,
+                                                       float n2, float cos_i, float sin2_t) {
+    const float u1 = unit_draw(seed, bounce, FROSTED_DIR_U_STREAM);
+    const float u2 = unit_draw(seed, bounce, FROSTED_DIR_V_STREAM);
+    FrostedScatter out{v3(0.0f, 0.0f, 0.0f), 1.0f, 0};
+    if (!(sin2_t > 1.0f)) {
+        const float cos_t = sqrtf(fmaxf(1.0f - sin2_t, 0.0f));
+        float r_s, r_p;
+        fresnel_rs_rp(n1, n2, cos_i, cos_t, r_s, r_p);
+        const float r_unpol = clampf_(r_unpol_of(r_s, r_p), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+        out.transmit = unit_draw(seed, bounce, FRESNEL_BRANCH_STREAM) < r_unpol ? 0 : 1;
+        out.pdf_factor = out.transmit ? 1.0f - r_unpol : r_unpol;
+    }
+    out.dir = cosine_weighted_hemisphere(u1, u2, out.transmit ? -normal : normal);
+    return out;
+}
+// Applies a frosted scatter's pdf factor and depolarisation to this channel.
+IX_DEV void lane_frosted_apply(LanePath& P, const FrostedScatter& f) {
+    P.pdf = P.pdf * f.pdf_factor;
+    P.st = Stokes{intensity(P.st), 0.0f, 0.0f, 0.0f};
+}
+
 // One iteration of the bounce loop (bounce_body.rs:361-423 and facet_event :611-707).
 // On BOUNCE_ESCAPED `esc` is this channel's escape radiance already weighted by its
 // Stokes intensity (accumulate_miss_radiance, transport/bounce.rs:40).
@@ -420,8 +482,9 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
     const float n1k = P.inside ? P.n : 1.0f;
     const float n2k = P.inside ? 1.0f : P.n;
 
-    // dispatch_bounce (transport/bounce.rs:108): the hero decides TIR (sin2_t > 1), else
-    // apply_partial_fresnel_bounce (refraction/dispatch.rs:307) draws reflect vs refract.
+    // dispatch_bounce (transport/bounce.rs:108): a frosted facet scatters diffusely;
+    // otherwise the hero decides TIR (sin2_t > 1), else apply_partial_fresnel_bounce
+    // (refraction/dispatch.rs:307) draws reflect vs refract.
     const bool tir = sin2_t > 1.0f;
     float r_unpol = 1.0f;
     bool reflect = tir;
@@ -432,9 +495,15 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
         r_unpol = clampf_(r_unpol_of(r_s, r_p), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
         reflect = unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM) < r_unpol;
     }
+    const bool frosted = facet_frosted(S, hit.facet);
     V3 new_dir;
     bool new_inside = P.inside;
-    if (reflect) {
+    if (frosted) {
+        const FrostedScatter f = frosted_scatter(P.seed, bounce, normal, n1, n2, cos_i, sin2_t);
+        lane_frosted_apply(P, f);
+        new_dir = f.dir;
+        if (f.transmit) new_inside = !P.inside;
+    } else if (reflect) {
         // apply_tir_bounce (tir.rs:98-116) / apply_partial_reflect_bounce
         // (reflect_refract.rs:33): the channel's TIR retarder or Fresnel reflection; a
         // partial reflection divides by the selection probability (TIR scales by 1).
@@ -497,9 +566,9 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
     P.o = hit_point + new_dir * 1e-4f;
     P.inside = new_inside;
 
-    // Surface glare (bounce_body.rs:691-697).
+    // Surface glare (bounce_body.rs:691-697): the outside reflection of a polished facet.
     const float glare = clampf_(sc.environment.surface_glare, 0.0f, 1.0f);
-    if (bounce == 0 && !P.inside && glare < 1.0f) P.st = scale(P.st, glare);
+    if (bounce == 0 && !P.inside && glare < 1.0f && !frosted) P.st = scale(P.st, glare);
     // apply_russian_roulette (transport/bounce.rs:355): q from the brightest channel.
     if (bounce > 4) {
         float max_i = intensity(P.st);
@@ -626,7 +695,19 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     V3 dir_k = v3(0.0f, 0.0f, 0.0f);
     float t_int = 0.0f;
 
-    if (sin2_t > 1.0f) {
+    const bool frosted = facet_frosted(S, hit.facet);
+    if (frosted) {
+        // apply_frosted_bounce (frosted.rs:289): the diffuse lobe is both the wave normal
+        // and the ray; an anisotropic entry draws its eigenmode with probability 1/2.
+        const FrostedScatter f = frosted_scatter(P.seed, bounce, normal, n1, n2, cos_i, sin2_t);
+        lane_frosted_apply(P, f);
+        new_k = f.dir;
+        new_s = new_k;
+        if (f.transmit) {
+            new_inside = !inside0;
+            if (!inside0 && aniso) update = unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f ? 1 : 0;
+        }
+    } else if (sin2_t > 1.0f) {
         // apply_tir_bounce (tir.rs:41): forced reflection.
         if (nondeg) {
             const UFrame f = uframe_build(k_hat, normal, c_axis, cos_i, sin_i);
@@ -835,9 +916,10 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
         P.is_e = unit_draw(P.seed, bounce, MODE_COUPLING_STREAM) >= p_o;
     }
 
-    // Surface glare (bounce_body.rs:691-697) and Russian roulette (transport/bounce.rs:355).
+    // Surface glare (bounce_body.rs:691-697), polished facets only, and Russian roulette
+    // (transport/bounce.rs:355).
     const float glare = clampf_(sc.environment.surface_glare, 0.0f, 1.0f);
-    if (bounce == 0 && !P.inside && glare < 1.0f) P.st = scale(P.st, glare);
+    if (bounce == 0 && !P.inside && glare < 1.0f && !frosted) P.st = scale(P.st, glare);
     if (bounce > 4) {
         float max_i = intensity(P.st);
 #pragma unroll

@@ -22,6 +22,7 @@
 #include "../include/ix_cie_tables.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -55,6 +56,8 @@ static inline bool operator<(F a, F b) { return a.v < b.v; }
 static inline bool operator>(F a, F b) { return a.v > b.v; }
 static inline bool operator<=(F a, F b) { return a.v <= b.v; }
 static inline bool operator>=(F a, F b) { return a.v >= b.v; }
+static inline bool operator==(F a, F b) { return a.v == b.v; }
+static inline bool operator!=(F a, F b) { return a.v != b.v; }
 static inline float raw(F x) { return x.v; }
 static inline F fma_(F a, F b, F c) { g_cnt.fma++; return F(std::fma(a.v, b.v, c.v)); }
 static inline F sqrt_(F a) { g_cnt.sqrt++; return F(std::sqrt(a.v)); }
@@ -1622,6 +1625,73 @@ static void apply_uniaxial_internal(Path& P, const Geo& g, V3 k, V3 normal, V3 h
 
 // apply_absorption (raytracer/absorption.rs:99-197): the mean over the two eigenmodes
 // for an isotropic material, the assigned eigenmode's field for a uniaxial one.
+// Frosted facets (optics/raytracer/scattering/frosted.rs, scattering/mod.rs:110) without
+// next-event estimation, which the modelled environments do not enable
+// (environment_supports_nee, environment/nee.rs:60: DaylightSun and HDR maps only).
+static const uint32_t FROSTED_DIR_U_STREAM = 0x27D4EB2Fu;  // sampling.rs:24
+static const uint32_t FROSTED_DIR_V_STREAM = 0x165667B1u;  // sampling.rs:25
+
+// frosted_orthonormal_basis (scattering/mod.rs:110).
+static void frosted_orthonormal_basis(V3 n, V3* t, V3* b) {
+    const V3 a = abs_(n.x) > F(0.9f) ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
+    *t = normalize_or_zero(a - n * dot(n, a));
+    *b = cross(n, *t);
+}
+// cosine_weighted_hemisphere (frosted.rs:34): (2 pi) u2 as the angle, glam's left-to-right
+// sum of the three scaled basis vectors.
+static V3 cosine_weighted_hemisphere(F u1, F u2, V3 n) {
+    const F r = sqrt_(u1);
+    const F theta = F(2.0f * 3.14159265358979323846f) * u2;
+    const F sin_t = sin_(theta), cos_t = cos_(theta);
+    V3 t, b;
+    frosted_orthonormal_basis(n, &t, &b);
+    return normalize_or_zero((t * (r * cos_t) + b * (r * sin_t)) + n * sqrt_(max_(F(1.0f) - u1, 0.0f)));
+}
+// apply_frosted_bounce (frosted.rs:289) with NEE off: a cosine-weighted diffuse
+// reflection or transmission chosen by the hero's unpolarised Fresnel reflectance
+// (always reflection past the hero's critical angle); every channel is depolarised and
+// its path pdf takes the chosen branch's probability.  An anisotropic entry draws its
+// eigenmode with probability one half.
+static void apply_frosted_bounce(Path& P, const Geo& g, V3 normal, uint32_t bounce, Outcome* o) {
+    const F u1 = unit_draw(P.seed, bounce, FROSTED_DIR_U_STREAM);
+    const F u2 = unit_draw(P.seed, bounce, FROSTED_DIR_V_STREAM);
+    o->update = -1;
+    o->has_p_o = false;
+    o->p_o = 0.0f;
+    if (g.sin2_t > F(1.0f)) {
+        const V3 d = cosine_weighted_hemisphere(u1, u2, normal);
+        for (int c = 0; c < 8; ++c) P.stokes[c] = unpolarized(intensity(P.stokes[c]));
+        o->new_k = o->new_s = d;
+        o->new_inside = P.inside;
+        return;
+    }
+    const F cos_t = sqrt_(max_(F(1.0f) - g.sin2_t, 0.0f));
+    const F r_s = fma_(g.n2, -cos_t, g.n1 * g.cos_i) / fma_(g.n2, cos_t, g.n1 * g.cos_i);
+    const F r_p = fma_(g.n1, -cos_t, g.n2 * g.cos_i) / fma_(g.n1, cos_t, g.n2 * g.cos_i);
+    const F r_unpol = clamp_(F(0.5f) * fma_(r_p, r_p, r_s * r_s), 1e-4f, 1.0f - 1e-4f);
+    const F rng_bounce = unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM);
+    if (rng_bounce < r_unpol) {
+        const V3 d = cosine_weighted_hemisphere(u1, u2, normal);
+        for (int c = 0; c < 8; ++c) {
+            P.stokes[c] = unpolarized(intensity(P.stokes[c]));
+            P.path_pdf[c] = P.path_pdf[c] * r_unpol;
+        }
+        o->new_k = o->new_s = d;
+        o->new_inside = P.inside;
+        return;
+    }
+    const V3 d = cosine_weighted_hemisphere(u1, u2, -normal);
+    const bool entering_anisotropic = !P.inside && P.aniso;
+    if (entering_anisotropic) o->update = unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM) < F(0.5f) ? 1 : 0;
+    const F t_unpol = F(1.0f) - r_unpol;
+    for (int c = 0; c < 8; ++c) {
+        P.stokes[c] = unpolarized(intensity(P.stokes[c]));
+        P.path_pdf[c] = P.path_pdf[c] * t_unpol;
+    }
+    o->new_k = o->new_s = d;
+    o->new_inside = !P.inside;
+}
+
 static void apply_absorption(Path& P, F path_len) {
     const ix_material& m = P.sc->material;
     TensorFrame tf = tensor_frame(P.c_axis);
@@ -1745,7 +1815,12 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
         o.update = -1;
         o.has_p_o = false;
         o.p_o = 0.0f;
-        if (g.sin2_t > F(1.0f)) {
+        // facet_finish_for (bounce_body.rs:656): Polished past the end of the list.
+        const bool frosted =
+            sc->facet_finishes && (uint32_t)hit.facet < sc->n_finishes && sc->facet_finishes[hit.facet] != 0;
+        if (frosted) {
+            apply_frosted_bounce(P, g, normal, bounce, &o);
+        } else if (g.sin2_t > F(1.0f)) {
             apply_tir_bounce(P, g, P.k, normal, &o);
         } else {
             const bool nondegenerate = g.has_frame && length_squared(cross(P.k, P.c_axis)) > F(1e-6f);
@@ -1777,7 +1852,7 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
             P.is_e = unit_draw(P.seed, bounce, MODE_COUPLING_STREAM) >= p_o;
         }
         // Surface glare (bounce_body.rs:691-697).
-        if (bounce == 0 && !P.inside && glare < F(1.0f)) {
+        if (bounce == 0 && !P.inside && glare < F(1.0f) && !frosted) {
             for (int c = 0; c < 8; ++c) P.stokes[c] = scale(P.stokes[c], glare);
         }
         // apply_russian_roulette (transport/bounce.rs:355).
@@ -1833,8 +1908,6 @@ static bool scene_supported(const ix_scene* sc) {
     if (!sc) return false;
     if (sc->n_planes > 0 && !sc->planes) return false;
     if (sc->material.scattering_sigma_s > 0.0f) return false;
-    for (uint32_t i = 0; i < sc->n_finishes && sc->facet_finishes; ++i)
-        if (sc->facet_finishes[i] != 0) return false;
     return true;
 }
 
@@ -2189,6 +2262,292 @@ static void attribution_add(ix_attribution_pixel* p, uint32_t cls, uint32_t scat
     p->fluoresced += fluoresced ? 1u : 0u;
 }
 
+
+// ------------------------------------------------------------------------------------
+// The display pipeline after the path (renderer/guide_pass.rs, renderer/denoise/,
+// renderer/tonemap.rs, color/space.rs, color/gamut.rs).  Plain f32 arithmetic in the
+// reference's operation order; `mul_add` is std::fma; expf / powf are the libm calls
+// Rust's f32::exp / f32::powf make on Linux.
+// ------------------------------------------------------------------------------------
+static inline F pow_(F a, F b) { return F(powf(raw(a), raw(b))); }
+
+// Guide pass: path_signature (guide_pass.rs:560-625).
+static const uint32_t SIG_EXIT_BIT = 0x8000u, SIG_ESCAPE = 0xFFFFu;
+static inline uint32_t fnv_mix(uint32_t hash, uint32_t word) {
+    for (int shift = 0; shift < 32; shift += 8) {
+        hash ^= (word >> shift) & 0xFFu;
+        hash *= 0x01000193u;
+    }
+    return hash;
+}
+// guide_pass.rs `unit`: v / |v| with an unfused dot (glam's Vec3 / f32 divides each lane).
+static inline V3 unit_div(V3 v) {
+    F len = sqrt_(dot(v, v));
+    if (len > F(0.0f)) return v3(v.x / len, v.y / len, v.z / len);
+    return v;
+}
+static uint32_t path_signature(const Ray& ray, const Hit& first, const float* planes, uint32_t n, F n_d) {
+    if (std::isnan(raw(n_d)) || n_d <= F(1.0f)) return 0;
+    uint32_t hash = fnv_mix(0x811c9dc5u, (uint32_t)first.facet);
+    V3 incident = unit_div(ray.dir);
+    F cos_i = max_(-dot(incident, first.normal), 0.0f);
+    F eta = F(1.0f) / n_d;
+    F k = F(1.0f) - eta * eta * (F(1.0f) - cos_i * cos_i);
+    if (k <= F(0.0f)) return std::max(fnv_mix(hash, SIG_ESCAPE), 1u);
+    V3 dir = unit_div(incident * eta + first.normal * (eta * cos_i - sqrt_(k)));
+    V3 origin = ray.origin + ray.dir * first.t;
+    for (int b = 0; b < 3; ++b) {  // SIGNATURE_BOUNCES
+        Ray probe{origin + dir * F(1.0e-4f), dir};
+        Hit hit;
+        if (!intersect(planes, n, probe, &hit)) {
+            hash = fnv_mix(hash, SIG_ESCAPE);
+            break;
+        }
+        origin = probe.origin + dir * hit.t;
+        const uint32_t facet = (uint32_t)hit.facet & 0x7FFFu;
+        F cos_t = dot(dir, hit.normal);
+        F sin_sq = n_d * n_d * (F(1.0f) - cos_t * cos_t);
+        if (sin_sq > F(1.0f)) {
+            hash = fnv_mix(hash, facet);
+            dir = unit_div(dir - hit.normal * (F(2.0f) * cos_t));
+        } else {
+            hash = fnv_mix(hash, facet | SIG_EXIT_BIT);
+            break;
+        }
+    }
+    return std::max(hash, 1u);
+}
+// fill_rows (guide_pass.rs:640-690) for one pixel.
+static void guide_pixel(const ix_camera& cam, uint32_t x, uint32_t y, uint32_t w, uint32_t h,
+                        const float* planes, uint32_t n, F n_d, float* depth, float* normal,
+                        int32_t* facet, uint32_t* sig) {
+    Ray ray = generate_ray(cam, F((float)x), F((float)y), F((float)w), F((float)h), 0.0f, 0.0f);
+    Hit hit;
+    if (intersect(planes, n, ray, &hit)) {
+        *depth = raw(hit.t);
+        store3(normal, hit.normal);
+        *facet = hit.facet;
+        if (sig) *sig = path_signature(ray, hit, planes, n, n_d);
+    } else {
+        *depth = 1.0e6f;
+        normal[0] = normal[1] = normal[2] = 0.0f;
+        *facet = -1;
+        if (sig) *sig = 0;
+    }
+}
+
+// A-Trous (denoise/pass.rs).
+static const float B3_SPLINE[5] = {1.0f / 16.0f, 1.0f / 4.0f, 3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
+static const float SIGMA_EPS = 1.0e-8f;
+static inline F sanitize(F v) { return is_finite_(v) ? v : F(0.0f); }
+static inline bool finite3(V3 v) { return is_finite_(v.x) && is_finite_(v.y) && is_finite_(v.z); }
+// unit_normal_or_zero (pass.rs:67).
+static inline V3 unit_normal_or_zero(V3 n) {
+    n = v3(sanitize(n.x), sanitize(n.y), sanitize(n.z));
+    F len = sqrt_(dot(n, n));
+    if (len <= F(SIGMA_EPS)) return v3(0.0f, 0.0f, 0.0f);
+    return v3(n.x / len, n.y / len, n.z / len);
+}
+// cos_pow (pass.rs:87): repeated squaring for a power-of-two integer exponent, else powf.
+static inline F cos_pow(F base, F power) {
+    const float p = raw(power);
+    if (p >= 0.0f && p == std::floor(p) && p <= 4294967295.0f) {
+        const uint32_t ip = (uint32_t)p;
+        if (ip != 0 && (ip & (ip - 1)) == 0) {
+            F v = base;
+            for (uint32_t s = ip; s > 1; s >>= 1) v = v * v;
+            return v;
+        }
+    }
+    return pow_(base, power);
+}
+static inline bool is_zero3(V3 v) { return v.x == F(0.0f) && v.y == F(0.0f) && v.z == F(0.0f); }
+struct TapConst {
+    F neg_inv_sigma_depth, neg_inv_two_sigma_color_sq, normal_power;
+};
+// atrous_pixel (pass.rs:330-378) with tap_contribution (pass.rs:283-316).
+static V3 atrous_pixel(const float* src, const float* depth, const float* nrm_n, const int32_t* facet_id,
+                       const uint32_t* sig, uint32_t width, uint32_t height, uint32_t x, uint32_t y,
+                       int64_t stride, const TapConst& tc) {
+    const size_t ci = (size_t)y * width + x;
+    V3 raw_c = load3(src + 3 * ci);
+    V3 color = finite3(raw_c) ? raw_c : v3(0.0f, 0.0f, 0.0f);
+    const int32_t facet = facet_id[ci];
+    if (facet < 0) return color;
+    const uint32_t csig = sig ? sig[ci] : 0u;
+    const F cdepth = depth[ci];
+    const V3 cnormal = load3(nrm_n + 3 * ci);
+    V3 sum = v3(0.0f, 0.0f, 0.0f);
+    F wsum = 0.0f;
+    for (int ky = 0; ky < 5; ++ky) {
+        const int64_t sy = (int64_t)y + (int64_t)(ky - 2) * stride;
+        if (sy < 0 || sy >= (int64_t)height) continue;
+        for (int kx = 0; kx < 5; ++kx) {
+            const int64_t sx = (int64_t)x + (int64_t)(kx - 2) * stride;
+            if (sx < 0 || sx >= (int64_t)width) continue;
+            const size_t idx = (size_t)sy * width + (size_t)sx;
+            const F kernel_w = F(B3_SPLINE[ky]) * F(B3_SPLINE[kx]);
+            if (facet_id[idx] != facet) continue;
+            if (sig && sig[idx] != csig) continue;
+            const V3 texel = load3(src + 3 * idx);
+            if (!finite3(texel)) continue;
+            F wn;
+            const V3 qn = load3(nrm_n + 3 * idx);
+            if (is_zero3(cnormal) || is_zero3(qn)) {
+                wn = 1.0f;
+            } else {
+                F c = max_(clamp_(dot(cnormal, qn), -1.0f, 1.0f), 0.0f);
+                wn = cos_pow(c, max_(tc.normal_power, 0.0f));
+            }
+            if (wn == F(0.0f)) continue;
+            const F gap = abs_(sanitize(cdepth) - sanitize(F(depth[idx])));
+            const F wd = gap == F(0.0f) ? F(1.0f) : exp_(gap * tc.neg_inv_sigma_depth);
+            const V3 d = color - texel;
+            const F dist_sq = dot(d, d);
+            const F wc = dist_sq == F(0.0f) ? F(1.0f) : exp_(dist_sq * tc.neg_inv_two_sigma_color_sq);
+            const F w = kernel_w * F(1.0f) * wn * wd * wc;
+            sum = sum + texel * w;
+            wsum = wsum + w;
+        }
+    }
+    if (wsum > F(SIGMA_EPS)) return v3(sum.x / wsum, sum.y / wsum, sum.z / wsum);
+    return color;
+}
+template <typename Fn>
+static void parallel_rows(uint32_t rows, int threads, Fn fn) {
+    if (threads <= 1 || rows < 2) {
+        for (uint32_t y = 0; y < rows; ++y) fn(y);
+        return;
+    }
+    std::vector<std::thread> pool;
+    std::atomic<uint32_t> next{0};
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&] {
+            for (uint32_t y; (y = next.fetch_add(1)) < rows;) fn(y);
+        });
+    for (auto& th : pool) th.join();
+}
+static int display_threads(int threads) {
+    if (threads > 0) return threads;
+    const unsigned hc = std::thread::hardware_concurrency();
+    return hc ? (int)hc : 8;
+}
+// AtrousDenoiser::denoise_into_with_threads (denoise/mod.rs:280-345).
+static void atrous_denoise(const float* color, const float* depth, const float* normal, const int32_t* facet_id,
+                           const uint32_t* sig, uint32_t width, uint32_t height, uint32_t spp,
+                           const ix_atrous_params& p, float* out, int threads) {
+    const size_t len = (size_t)width * height;
+    if (len == 0) return;
+    const F n0 = max_(p.taper_reference_spp, SIGMA_EPS);
+    const F taper = F(1.0f) / sqrt_(F(1.0f) + F((float)spp) / n0);
+    const uint32_t passes = std::min(std::max(p.num_passes, 1u), 8u);
+    if (taper < F(p.taper_identity_epsilon)) {
+        std::memcpy(out, color, len * 3 * sizeof(float));
+        return;
+    }
+    const F sce = max_(F(p.sigma_color) * taper, 0.0f);
+    std::vector<float> buf[2] = {std::vector<float>(color, color + 3 * len), std::vector<float>(3 * len)};
+    std::vector<float> nrm_n(3 * len);
+    for (size_t i = 0; i < len; ++i) store3(nrm_n.data() + 3 * i, unit_normal_or_zero(load3(normal + 3 * i)));
+    const F sd = max_(p.sigma_depth, SIGMA_EPS);
+    const F scs = max_(sce * sce, SIGMA_EPS);
+    TapConst tc{F(-1.0f) / sd, F(-1.0f) / (F(2.0f) * scs), F(p.normal_power)};
+    const int nt = display_threads(threads);
+    for (uint32_t pass = 0; pass < passes; ++pass) {
+        const float* src = buf[pass & 1].data();
+        float* dst = buf[(pass & 1) ^ 1].data();
+        parallel_rows(height, nt, [&](uint32_t y) {
+            for (uint32_t x = 0; x < width; ++x)
+                store3(dst + 3 * ((size_t)y * width + x),
+                       atrous_pixel(src, depth, nrm_n.data(), facet_id, sig, width, height, x, y,
+                                    (int64_t)1 << pass, tc));
+        });
+    }
+    std::memcpy(out, buf[passes & 1].data(), len * 3 * sizeof(float));
+}
+
+// ColorSpace tables (color/space.rs:159-196).
+static const float XYZ_TO_RGB[4][3][3] = {
+    {{3.2404542f, -1.5371385f, -0.4985314f}, {-0.969266f, 1.8760108f, 0.041556f}, {0.0556434f, -0.2040259f, 1.0572252f}},
+    {{2.493497f, -0.9313836f, -0.40271078f}, {-0.829489f, 1.762664f, 0.023624686f}, {0.03584583f, -0.07617239f, 0.9568845f}},
+    {{1.7166512f, -0.35567078f, -0.2533663f}, {-0.6666843f, 1.6164812f, 0.015768546f}, {0.017639857f, -0.042770613f, 0.9421031f}},
+    {{1.6410234f, -0.3248033f, -0.2364247f}, {-0.66366286f, 1.6153316f, 0.016756348f}, {0.011721894f, -0.008284442f, 0.98839486f}},
+};
+static const float WHITE_XY[4][2] = {{0.3127f, 0.3290f}, {0.3127f, 0.3290f}, {0.3127f, 0.3290f}, {0.32168f, 0.33767f}};
+// ColorSpace::xyz_to_linear (space.rs:210).
+static inline V3 xyz_to_linear(uint32_t sp, V3 c) {
+    const float (*m)[3] = XYZ_TO_RGB[sp];
+    return v3(fma_(m[0][0], c.x, fma_(m[0][1], c.y, F(m[0][2]) * c.z)),
+              fma_(m[1][0], c.x, fma_(m[1][1], c.y, F(m[1][2]) * c.z)),
+              fma_(m[2][0], c.x, fma_(m[2][1], c.y, F(m[2][2]) * c.z)));
+}
+// project_to_gamut_bounded (gamut.rs:43-101).
+static V3 project_to_gamut_bounded(V3 c, uint32_t sp, F mx) {
+    const F sum = c.x + c.y + c.z;
+    if (!is_finite_(sum) || sum <= F(1e-6f)) return v3(0.0f, 0.0f, 0.0f);
+    const F x = c.x / sum, y = c.y / sum;
+    const F lum = max_(c.y, 0.0f);
+    auto in_range = [&](V3 v) {
+        return v.x >= F(0.0f) && v.y >= F(0.0f) && v.z >= F(0.0f) && v.x <= mx && v.y <= mx && v.z <= mx;
+    };
+    const V3 lin = xyz_to_linear(sp, c);
+    if (in_range(lin)) return lin;
+    const F wx = WHITE_XY[sp][0], wy = WHITE_XY[sp][1];
+    auto mapped = [&](F t) {
+        const F xp = fma_(wx - x, t, x);
+        const F yp = fma_(wy - y, t, y);
+        if (yp > F(1e-6f)) return v3((xp / yp) * lum, lum, ((F(1.0f) - xp - yp) / yp) * lum);
+        return v3((wx / wy) * lum, lum, ((F(1.0f) - wx - wy) / wy) * lum);
+    };
+    V3 resolved = vmax0(xyz_to_linear(sp, mapped(1.0f)));
+    for (uint32_t i = 0; i <= 32; ++i) {
+        const F t = F((float)i) / F(32.0f);
+        const V3 cand = xyz_to_linear(sp, mapped(t));
+        if (in_range(cand)) {
+            resolved = cand;
+            break;
+        }
+    }
+    return resolved;
+}
+// TransferFunction::encode (space.rs:54-75).
+static inline F transfer_encode(uint32_t sp, F lin) {
+    if (sp == IX_COLOR_SPACE_SRGB || sp == IX_COLOR_SPACE_DISPLAY_P3) {
+        if (lin <= F(0.0031308f)) return lin * F(12.92f);
+        return fma_(1.055f, pow_(lin, F(1.0f) / F(2.4f)), -0.055f);
+    }
+    if (sp == IX_COLOR_SPACE_REC2020) {
+        const F alpha = 1.0992968f, beta = 0.01805397f;
+        if (lin < beta) return lin * F(4.5f);
+        return fma_(alpha, pow_(lin, 0.45f), -(alpha - F(1.0f)));
+    }
+    return lin;
+}
+// aces_tonemap (optics/raytracer/color.rs:372).
+static inline F aces_tonemap(F y) {
+    return (y * fma_(2.51f, y, 0.03f)) / fma_(y, fma_(2.43f, y, 0.59f), 0.14f);
+}
+// ColorSpace::encode with ToneMap::AcesFilmic { exposure: 1.0 } (space.rs:234-278).
+static void color_encode(V3 c, uint32_t sp, uint8_t out[4]) {
+    out[3] = 255;
+    const F sum = c.x + c.y + c.z;
+    if (!is_finite_(sum) || sum <= F(1e-6f)) {
+        out[0] = out[1] = out[2] = 0;
+        return;
+    }
+    const F exposure = 1.0f;
+    const F lum = max_(c.y, 0.0f);
+    const F exposed = max_(lum * exposure, 0.0f);
+    const F y_tm = aces_tonemap(exposed);
+    const F scale = (y_tm / max_(exposed, 1e-5f)) * exposure;
+    const V3 rgb = project_to_gamut_bounded(c * scale, sp, 1.0f);
+    const F ch[3] = {rgb.x, rgb.y, rgb.z};
+    for (int k = 0; k < 3; ++k) {
+        const F lin = is_finite_(ch[k]) ? clamp_(ch[k], 0.0f, 1.0f) : F(0.0f);
+        const F enc = clamp_(transfer_encode(sp, lin), 0.0f, 1.0f);
+        out[k] = (uint8_t)raw(fma_(enc, 255.0f, 0.5f));
+    }
+}
 }  // namespace ixo
 
 using namespace ixo;
@@ -2643,6 +3002,63 @@ int ixo_count_flops(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_
     (void)spp; (void)out;
     return -1;
 #endif
+}
+
+
+// ---- display pipeline --------------------------------------------------------------
+void ixo_atrous_params_default(ix_atrous_params* p) {
+    // AtrousParams::default (denoise/mod.rs:194).
+    *p = ix_atrous_params{5u, 0.35f, 0.1f, 64.0f, 4.0f, 0.02f};
+}
+void ixo_generate_guide_buffers(uint32_t width, uint32_t height, const ix_camera* cam, const float* planes,
+                                uint32_t n_planes, float n_d, float* depth, float* normal, int32_t* facet_id,
+                                uint32_t* path_sig, int threads) {
+    parallel_rows(height, display_threads(threads), [&](uint32_t y) {
+        for (uint32_t x = 0; x < width; ++x) {
+            const size_t i = (size_t)y * width + x;
+            guide_pixel(*cam, x, y, width, height, planes, n_planes, F(n_d), depth + i, normal + 3 * i,
+                        facet_id + i, path_sig ? path_sig + i : nullptr);
+        }
+    });
+}
+float ixo_n_d(const ix_dispersion* d) {
+    // DispersionModel::n_d (optics/dispersion.rs:264): the index at 589.3 nm.
+    return raw(dispersion_eval(*d, F(589.3f)));
+}
+void ixo_atrous_denoise(const float* color, const float* depth, const float* normal, const int32_t* facet_id,
+                        const uint32_t* path_sig, uint32_t width, uint32_t height, uint32_t spp,
+                        const ix_atrous_params* params, float* out, int threads) {
+    atrous_denoise(color, depth, normal, facet_id, path_sig, width, height, spp, *params, out, threads);
+}
+void ixo_color_encode(const float xyz[3], uint32_t color_space, uint8_t out[4]) {
+    color_encode(load3(xyz), color_space, out);
+}
+void ixo_tonemap_to_rgba(const float* xyz, uint64_t pixels, float scale, uint32_t color_space, uint8_t* rgba,
+                         int threads) {
+    // tonemap_chunk / tonemap_chunk_in (tonemap.rs:85, 165): encode(xyz * scale).
+    const uint64_t rows = (pixels + 4095) / 4096;
+    parallel_rows((uint32_t)rows, display_threads(threads), [&](uint32_t r) {
+        const uint64_t end = std::min<uint64_t>(pixels, (uint64_t)(r + 1) * 4096);
+        for (uint64_t i = (uint64_t)r * 4096; i < end; ++i)
+            color_encode(load3(xyz + 3 * i) * F(scale), color_space, rgba + 4 * i);
+    });
+}
+void ixo_denoise_and_tonemap_frame(uint32_t width, uint32_t height, uint32_t spp, const float* accum,
+                                   const float* depth, const float* normal, const int32_t* facet_id,
+                                   const uint32_t* path_sig, const ix_atrous_params* params, uint8_t* rgba,
+                                   int threads) {
+    // denoise_and_tonemap_frame_with_params_into (frame_denoise.rs:40-80).
+    const size_t len = (size_t)width * height;
+    std::vector<float> avg(3 * len, 0.0f), filtered(3 * len, 0.0f);
+    if (spp == 0) {
+        ixo_tonemap_to_rgba(filtered.data(), len, 1.0f, IX_COLOR_SPACE_SRGB, rgba, threads);
+        return;
+    }
+    const F inv = F(1.0f) / F((float)spp);
+    for (size_t i = 0; i < 3 * len; ++i) avg[i] = raw(F(accum[i]) * inv);
+    atrous_denoise(avg.data(), depth, normal, facet_id, path_sig, width, height, spp, *params, filtered.data(),
+                   threads);
+    ixo_tonemap_to_rgba(filtered.data(), len, 1.0f, IX_COLOR_SPACE_SRGB, rgba, threads);
 }
 
 }  // extern "C"

@@ -12,6 +12,7 @@
 #include <stdint.h>
 #include "../include/ix_scene.h"
 #include "../include/ix_attribution.h"
+#include "../include/ix_display.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -156,6 +157,25 @@ int ixo_counting_build(void);
 int ixo_count_flops(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_end,
                     uint32_t pixel_step, uint32_t sample_offset, uint32_t spp,
                     ixo_flop_counts* out);
+
+/* The display pipeline after the path (renderer/guide_pass.rs, renderer/denoise/,
+ * renderer/tonemap.rs, renderer/frame_denoise.rs); threads 0 = all host threads, the
+ * results do not depend on it. */
+void ixo_atrous_params_default(ix_atrous_params* p);
+void ixo_generate_guide_buffers(uint32_t width, uint32_t height, const ix_camera* cam, const float* planes,
+                                uint32_t n_planes, float n_d, float* depth, float* normal, int32_t* facet_id,
+                                uint32_t* path_sig, int threads);
+float ixo_n_d(const ix_dispersion* d);
+void ixo_atrous_denoise(const float* color, const float* depth, const float* normal, const int32_t* facet_id,
+                        const uint32_t* path_sig, uint32_t width, uint32_t height, uint32_t spp,
+                        const ix_atrous_params* params, float* out, int threads);
+void ixo_color_encode(const float xyz[3], uint32_t color_space, uint8_t out[4]);
+void ixo_tonemap_to_rgba(const float* xyz, uint64_t pixels, float scale, uint32_t color_space, uint8_t* rgba,
+                         int threads);
+void ixo_denoise_and_tonemap_frame(uint32_t width, uint32_t height, uint32_t spp, const float* accum,
+                                   const float* depth, const float* normal, const int32_t* facet_id,
+                                   const uint32_t* path_sig, const ix_atrous_params* params, uint8_t* rgba,
+                                   int threads);
 
 #ifdef __cplusplus
 }

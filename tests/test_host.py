@@ -95,10 +95,11 @@ def test_routing_predicate():
     m = materials.diamond()
     m.scattering_sigma_s = 0.5
     assert not scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, fs.planes, m, 32, fs.environment))
+    # Frosted facets route (apply_frosted_bounce runs on the device).
     fin = np.zeros(fs.planes.shape[0], np.uint8)
     fin[70] = 1
-    assert not scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, fs.planes, materials.diamond(), 32,
-                                              fs.environment, fin))
+    assert scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, fs.planes, materials.diamond(), 32,
+                                          fs.environment, fin))
     too_many = np.zeros((129, 4), np.float32)
     too_many[:, 1] = 1.0
     assert not scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, too_many, materials.diamond(), 32,
