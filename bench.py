@@ -9,6 +9,11 @@ One "step" is one pass of the hot path over one batch of synthetic input:
 * ``--workload stress``: the anisotropic stress frame, 512x512 x 256 spp (67,108,864
   paths) of a uniaxial pleochroic emerald-cut stone with its optic axis tilted 30
   degrees, depth 64.
+* ``--workload display``: the display step after the path on a 1920x1080 frame of 16 spp
+  XYZ sums (the reference's denoise bench: round brilliant at (0.60, 0.45, 2.4, 42 deg),
+  path signature at n_d 1.76, seeded noise in [0, 2) per channel): average, 5 A-Trous
+  passes with the sRGB tone-map fused into the last, guides cached per pose.  The metric
+  is display frames/s; under torchrun every rank displays its own frame (replicas).
 
 Under torchrun (N > 1) every rank traces its own disjoint absolute sample range of the
 same workload (weak scaling), and the per-pixel f64 sums are gathered to rank 0 over
@@ -49,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["frame", "batch", "stress"])
+    ap.add_argument("--workload", default="batch", choices=["frame", "batch", "stress", "display"])
     ap.add_argument("--precision", default="fast", choices=["fast", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -266,10 +271,225 @@ def run_reference(args, items, cfg):
 
 
 # ----------------------------------------------------------------------------------
+# The display step after the path (guide pass, A-Trous denoise, tone-map)
+# ----------------------------------------------------------------------------------
+DISPLAY_METRIC, DISPLAY_UNIT = "display frames/s", "frames/s"
+HBM_PEAK_FALLBACK_GBS = 6650.0
+
+
+def display_workload():
+    from indicatrix_b200 import materials, workloads
+    from indicatrix_b200.backend import FrameScene, camera_new
+
+    w, h, spp = 1920, 1080, 16
+    base = workloads.round_brilliant_frame(8, 8)
+    # n_d exactly 1.76 (the reference bench's signature index): a flat Cauchy index.
+    mat = materials.isotropic(materials.cauchy(1.76, 0.0, 0.0))
+    fs = FrameScene(camera_new(0.60, 0.45, 2.4, 42.0), w, h, base.planes, mat, 32, base.environment)
+    rng = np.random.default_rng(0x9E3779B9)
+    # Per channel a value in [0, 2) on the reference bench's 1/32768 grid, summed over spp.
+    color = (rng.integers(0, 65536, size=(h, w, 3), dtype=np.uint32).astype(np.float32) / np.float32(32768.0))
+    accum = (color * np.float32(spp)).astype(np.float32)
+    cfg = {"workload": "display step 1920x1080 from 16 spp XYZ sums: average, 5 A-Trous passes with path "
+                       "signature, sRGB tone-map", "width": w, "height": h, "spp": spp, "passes": 5,
+           "signature_n_d": 1.76, "stone": "standard round brilliant, 74 facets",
+           "pose": "yaw 0.60, pitch 0.45, distance 2.4, fov 42 deg"}
+    return fs, accum, spp, cfg
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            v = json.load(f).get("hbm_gbs")
+        if v:
+            return float(v), "measured"
+    return HBM_PEAK_FALLBACK_GBS, "fallback"
+
+
+def display_cpu(fs, accum, spp, frames: int):
+    """The oracle's display step (guides at n_d 1.76, denoise, tone-map) on all host
+    threads: seconds per frame, the guides timed once outside."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ix_oracle
+
+    ix_oracle.build()
+    threads = os.cpu_count() or 1
+    d, n, f, s = ix_oracle.generate_guide_buffers(fs.width, fs.height, fs.camera, fs.planes, 1.76, threads)
+    times = []
+    for _ in range(frames):
+        t0 = time.perf_counter()
+        ix_oracle.denoise_and_tonemap_frame(accum, spp, d, n, f, s, threads=threads)
+        times.append(time.perf_counter() - t0)
+    return sum(times) / len(times), threads
+
+
+def display_flops_per_pixel_pass(fs, accum, spp):
+    """Algorithmic FP32 operations per pixel-pass of the A-Trous denoise, counted by the
+    oracle's counting build on a 480x270 crop around the stone of the same frame."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ix_oracle
+
+    ix_oracle.build()
+    cw, ch = 480, 270
+    x0, y0 = (fs.width - cw) // 2, (fs.height - ch) // 2
+    d, n, f, s = ix_oracle.generate_guide_buffers(fs.width, fs.height, fs.camera, fs.planes, 1.76)
+    crop = (slice(y0, y0 + ch), slice(x0, x0 + cw))
+    avg = (accum[crop] * (np.float32(1.0) / np.float32(spp))).astype(np.float32)
+    c = ix_oracle.count_denoise_flops(avg, d[crop], n[crop], f[crop], s[crop], spp)
+    return c.flops() / c.paths, float(np.mean(f[crop] >= 0))
+
+
+def run_display_reference(args, fs, accum, spp, cfg):
+    rank, _, _ = dist_env()
+    if rank != 0:
+        return
+    for _ in range(max(0, min(args.warmup, 1))):
+        display_cpu(fs, accum, spp, 1)
+    sec, threads = display_cpu(fs, accum, spp, args.steps)
+    value = 1.0 / sec
+    print(json.dumps({
+        "impl": "reference", "metric": DISPLAY_METRIC, "value": value, "unit": DISPLAY_UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": DISPLAY_UNIT, "cores": threads, "kind": "port",
+                         "sample": f"the whole 1920x1080 frame per step ({args.steps} frames): the reference's "
+                                   "denoise and tone-map (Rust, not buildable here) restated in C++, all host "
+                                   "threads"},
+        "e2e": {"value": value, "unit": DISPLAY_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main_display(args):
+    rank, world, local = dist_env()
+    fs, accum, spp, cfg = display_workload()
+    cfg["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
+    if args.impl == "reference":
+        run_display_reference(args, fs, accum, spp, cfg)
+        return
+    import torch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from indicatrix_b200 import abi, display
+    from indicatrix_b200.backend import GpuBackend
+
+    precision = abi.PRECISION_EXACT if args.precision == "exact" else abi.PRECISION_FAST
+    backend = GpuBackend.acquire(device=local, precision=precision)
+    if not backend.available:
+        raise RuntimeError("libix_cuda.so could not create a backend")
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    d_acc = torch.from_numpy(accum).to(dev)
+    d_rgba = torch.empty((fs.height, fs.width, 4), dtype=torch.uint8, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    sc = fs.to_abi()
+
+    def step():
+        if not display.display_frame_device(backend, sc, spp, d_acc.data_ptr(), d_rgba.data_ptr(), True,
+                                            stream_ptr=stream.cuda_stream):
+            raise RuntimeError(f"display declined: {backend.last_lost_reason()}")
+
+    for _ in range(args.warmup):  # the first call computes and caches the guides
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    atrous_ms, launches = [], 0
+    for k in range(args.steps):
+        flush.zero_()  # the ~120 MB working set fits L2: flush between timed steps
+        starts[k].record(stream)
+        step()
+        ends[k].record(stream)
+        t = display.last_timing(backend)  # the A-Trous kernels' events on the same stream
+        atrous_ms.append(t.atrous_ms)
+        launches += t.launches
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    mean_ms = sum(step_ms) / len(step_ms)
+    if world > 1:
+        t = torch.tensor([mean_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        mean_ms = float(t.item())
+    value = world / (mean_ms * 1e-3)
+
+    # End to end through the public host API: H2D of the f32 sums, D2H of the RGBA8.
+    e2e_ms = []
+    for k in range(max(1, args.warmup // 2) + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = display.display_frame(backend, fs, spp, accum, True)
+        if out is None:
+            raise RuntimeError(f"display declined: {backend.last_lost_reason()}")
+        if k >= max(1, args.warmup // 2):
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_mean = sum(e2e_ms) / len(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_mean], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_mean = float(t.item())
+        torch.distributed.destroy_process_group()
+    pixels = fs.width * fs.height
+
+    if rank == 0:
+        passes = 5
+        # Algorithmic bytes of one A-Trous launch: per pixel the centre's colour (16 B),
+        # packed guides (16 + 8 B) and the colour written (16 B); the last pass writes
+        # RGBA8 (4 B) instead.  Averaged over the 5 launches of a frame.
+        bytes_per_launch = pixels * (4 * 56 + 44) / passes
+        atrous_launch_ms = statistics.mean(atrous_ms) / passes
+        achieved = bytes_per_launch / (atrous_launch_ms * 1e-3) / 1e9
+        peak, peak_kind = hbm_peak()
+        flops_pp, fg = display_flops_per_pixel_pass(fs, accum, spp)
+        line = {
+            "metric": DISPLAY_METRIC, "value": value, "unit": DISPLAY_UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {**cfg, "precision": args.precision,
+                       "l2": "512 MB buffer written between timed steps (outside the step events)",
+                       "megapixels_per_s": value * pixels / 1e6},
+            "e2e": {"value": world / (e2e_mean * 1e-3), "unit": DISPLAY_UNIT,
+                    "h2d_bytes_per_step": pixels * 12, "d2h_bytes_per_step": pixels * 4, "ms_per_step": e2e_mean},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": f"{peak_kind} HBM copy bandwidth",
+                         "kernel": "atrous_pass_kernel", "launch_ms": atrous_launch_ms,
+                         "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "flops_per_pixel_pass": flops_pp, "foreground_fraction": fg},
+            "clocks": clk,
+        }
+        if not args.no_cpu_baseline:
+            sec, threads = display_cpu(fs, accum, spp, 1)
+            line["cpu_baseline"] = {"value": 1.0 / sec, "unit": DISPLAY_UNIT, "cores": threads, "kind": "port",
+                                    "sample": "one whole 1920x1080 frame: the C++ oracle's denoise + tone-map on "
+                                              f"{threads} host threads ({sec:.2f} s)"}
+        print(json.dumps(line), flush=True)
+    backend.close()
+
+
+# ----------------------------------------------------------------------------------
 # Our arm
 # ----------------------------------------------------------------------------------
 def main():
     args = parse()
+    if args.workload == "display":
+        main_display(args)
+        return
     rank, world, local = dist_env()
     if args.workload == "batch":
         items, cfg = batch_workload(args.stones)

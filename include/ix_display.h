@@ -49,9 +49,21 @@ enum {
     IX_COLOR_SPACE_ACESCG = 3
 };
 
+/* Device time of the last display call's stages (CUDA events on the stream it ran on):
+ * the guide pass (0 when the cache served it), packing, and the A-Trous passes with the
+ * fused tone-map; `atrous_passes` of the `launches` kernels were A-Trous passes. */
+typedef struct ix_display_timing {
+    float guide_ms;
+    float pack_ms;
+    float atrous_ms;
+    uint32_t atrous_passes;
+    uint32_t launches;
+} ix_display_timing;
+
 struct ix_backend;
 
 void ix_atrous_params_default(ix_atrous_params* out);
+int ix_display_last_timing(const struct ix_backend* b, ix_display_timing* out);
 
 /* One un-jittered camera ray per pixel (guide_pass.rs:640-690): first-hit depth t
  * (1e6 on a miss), facet normal (0 on a miss, 3 floats per pixel), facet id (-1 on a
@@ -98,6 +110,14 @@ int ix_denoise_and_tonemap_frame(struct ix_backend* b, uint32_t width, uint32_t 
 int ix_display_frame(struct ix_backend* b, const ix_scene* scene, uint32_t with_signature,
                      uint32_t spp, const float* accum, const ix_atrous_params* params,
                      uint8_t* rgba);
+
+/* Device-resident form of ix_display_frame (no counterpart in the reference): `accum` and
+ * `rgba` are device pointers, scene->planes stays a host pointer (it keys the guide
+ * cache); the kernels are enqueued on `stream` (a cudaStream_t, NULL for the backend's
+ * own) and not synchronised.  With spp == 0 the frame is opaque black. */
+int ix_display_frame_device(struct ix_backend* b, const ix_scene* scene, uint32_t with_signature,
+                            uint32_t spp, const float* accum, const ix_atrous_params* params,
+                            uint8_t* rgba, void* stream);
 
 #ifdef __cplusplus
 }

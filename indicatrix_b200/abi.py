@@ -249,6 +249,27 @@ class MetricsPose(C.Structure):
     ]
 
 
+class AtrousParams(C.Structure):
+    """ix_atrous_params (include/ix_display.h): AtrousParams, denoise/mod.rs:157."""
+
+    _fields_ = [
+        ("num_passes", C.c_uint32),
+        ("sigma_color", C.c_float),
+        ("sigma_depth", C.c_float),
+        ("normal_power", C.c_float),
+        ("taper_reference_spp", C.c_float),
+        ("taper_identity_epsilon", C.c_float),
+    ]
+
+    @classmethod
+    def default(cls) -> "AtrousParams":
+        """AtrousParams::default (denoise/mod.rs:194)."""
+        return cls(5, 0.35, 0.1, 64.0, 4.0, 0.02)
+
+
+COLOR_SPACE_SRGB, COLOR_SPACE_DISPLAY_P3, COLOR_SPACE_REC2020, COLOR_SPACE_ACESCG = 0, 1, 2, 3
+
+
 def floats(values) -> C.Array:
     arr = (C.c_float * len(values))()
     for i, v in enumerate(values):

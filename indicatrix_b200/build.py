@@ -57,7 +57,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     jobs = []  # (object, command); the device units compile concurrently
     # The fused build also takes the approximate divide / square root and flushes
     # denormals; the slab scan's division stays IEEE (__fdiv_rn) in both builds.
-    for unit in ("ix_kernels", "ix_metrics"):
+    for unit in ("ix_kernels", "ix_metrics", "ix_display"):
         for variant, flags in (("exact", ["-DIX_EXACT=1", "-fmad=false"]),
                                ("fast", ["-DIX_EXACT=0", "-fmad=true", "-prec-div=false",
                                          "-prec-sqrt=false", "-ftz=true"])):
@@ -78,7 +78,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if errors:
         raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
     cuda_inc = os.path.join(_cuda_home(nvcc), "include")
-    for unit in ("ix_backend", "ix_dispatch"):
+    for unit in ("ix_backend", "ix_dispatch", "ix_display_host"):
         host_obj = os.path.join(BUILD_DIR, unit + ".o")
         cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
                f"-I{INCLUDE}", f"-I{cuda_inc}", "-c", os.path.join(CSRC, unit + ".cpp"), "-o", host_obj]

@@ -12,6 +12,7 @@
 
 #include "../../include/ix_cuda.h"
 #include "../../include/ix_cie_tables.h"
+#include "ix_backend_state.h"
 #include "ix_launch.h"
 
 #include <cuda_runtime.h>
@@ -29,109 +30,9 @@
 #include <thread>
 #include <vector>
 
-struct ix_backend {
-    int device = 0;
-    uint32_t pipeline = IX_PIPELINE_MEGAKERNEL;
-    uint32_t precision = IX_PRECISION_FAST;
-    uint32_t threads = 128;
-    uint64_t chunk_paths = 0;
-    ix_work_limits limits{0, 0, 0};
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // Pooled buffers.
-    float* d_planes = nullptr;
-    size_t planes_cap = 0;
-    double* d_sums = nullptr;
-    size_t sums_cap = 0;
-    double* h_sums = nullptr;
-    size_t hsums_cap = 0;
-    uint32_t* d_counter = nullptr;
-    unsigned long long* d_dropped = nullptr;
-    uint32_t* d_check = nullptr;
-    size_t check_cap = 0;
-    // Spectral attribution: per-sample class / luminance records of one launch and the
-    // frame's attribution map.
-    uint8_t* d_attr_cls = nullptr;
-    size_t attr_cls_cap = 0;
-    float* d_attr_y = nullptr;
-    size_t attr_y_cap = 0;
-    ix_attribution_pixel* d_attr_map = nullptr;
-    size_t attr_map_cap = 0;
-    ix_attribution_pixel* h_attr_map = nullptr;
-    size_t hattr_map_cap = 0;
-    // The one-shot batch entry's device sums.
-    double* d_batch_out = nullptr;
-    size_t batch_out_cap = 0;
-    // A host scene's per-facet finishes, copied for the kernels.
-    uint8_t* d_finishes = nullptr;
-    size_t finishes_cap = 0;
-    int sm_count = 0;
-    uint32_t variant = 0;
-    // Register variant new batch plans start from: the last autotuner pick (or `variant`).
-    uint32_t batch_variant = 0;
-    // Resident CTAs per SM by [uniaxial instantiation][variant].
-    int bps_exact[2][3] = {{1, 1, 1}, {1, 1, 1}}, bps_fast[2][3] = {{1, 1, 1}, {1, 1, 1}};
-    // ... and of the attributed trace kernels by [uniaxial instantiation].
-    int bps_attr_exact[2] = {1, 1}, bps_attr_fast[2] = {1, 1};
-    std::string label;
-    // State.
-    bool lost = false;
-    std::string last_error;
-    ix_timing timing{0.0f, 0.0f, 0, 0};
-    uint64_t dropped = 0;
-    // FIFO turnstile.
-    std::mutex mu;
-    std::condition_variable cv;
-    uint64_t next_ticket = 0, serving = 0;
-};
+using namespace ixh;
 
 namespace {
-
-struct Turn {
-    ix_backend* b;
-    explicit Turn(ix_backend* be) : b(be) {
-        std::unique_lock<std::mutex> lk(b->mu);
-        uint64_t mine = b->next_ticket++;
-        b->cv.wait(lk, [&] { return b->serving == mine; });
-    }
-    ~Turn() {
-        std::lock_guard<std::mutex> lk(b->mu);
-        b->serving++;
-        b->cv.notify_all();
-    }
-};
-
-bool fail(ix_backend* b, cudaError_t e, const char* where) {
-    if (e == cudaSuccess) return false;
-    b->lost = true;
-    b->last_error = std::string(where) + ": " + cudaGetErrorString(e);
-    (void)cudaGetLastError();
-    return true;
-}
-
-template <typename T>
-cudaError_t grow_device(T** p, size_t* cap, size_t need) {
-    if (*cap >= need && *p) return cudaSuccess;
-    if (*p) cudaFree(*p);
-    *p = nullptr;
-    *cap = 0;
-    size_t n = std::max(need, (size_t)1);
-    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
-    if (e == cudaSuccess) *cap = n;
-    return e;
-}
-
-template <typename T>
-cudaError_t grow_pinned(T** p, size_t* cap, size_t need) {
-    if (*cap >= need && *p) return cudaSuccess;
-    if (*p) cudaFreeHost(*p);
-    *p = nullptr;
-    *cap = 0;
-    size_t n = std::max(need, (size_t)1);
-    cudaError_t e = cudaMallocHost((void**)p, n * sizeof(T));
-    if (e == cudaSuccess) *cap = n;
-    return e;
-}
 
 bool material_has_absorption(const ix_absorption& a) {
     if (a.has_spline) return true;
@@ -521,6 +422,7 @@ void ix_backend_destroy(ix_backend* b) {
     cudaFree(b->d_attr_map);
     cudaFree(b->d_batch_out);
     cudaFree(b->d_finishes);
+    display_state_free(b->display);
     if (b->h_attr_map) cudaFreeHost(b->h_attr_map);
     if (b->h_sums) cudaFreeHost(b->h_sums);
     if (b->ev0) cudaEventDestroy(b->ev0);

@@ -1,0 +1,126 @@
+// ix_backend_state.h -- the backend object behind the C ABI and the host helpers every
+// entry-point file shares: the FIFO turn (gpu_backend/turnstile.rs:24-115), the
+// device-error-to-lost-backend rule (gpu_backend/mod.rs:151-164) and pooled buffers.
+#pragma once
+
+#include "../../include/ix_cuda.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <condition_variable>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+struct DisplayState;  // the display pipeline's pooled buffers (ix_display_host.cpp)
+void display_state_free(DisplayState* d);
+
+struct ix_backend {
+    int device = 0;
+    uint32_t pipeline = IX_PIPELINE_MEGAKERNEL;
+    uint32_t precision = IX_PRECISION_FAST;
+    uint32_t threads = 128;
+    uint64_t chunk_paths = 0;
+    ix_work_limits limits{0, 0, 0};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Pooled buffers.
+    float* d_planes = nullptr;
+    size_t planes_cap = 0;
+    double* d_sums = nullptr;
+    size_t sums_cap = 0;
+    double* h_sums = nullptr;
+    size_t hsums_cap = 0;
+    uint32_t* d_counter = nullptr;
+    unsigned long long* d_dropped = nullptr;
+    uint32_t* d_check = nullptr;
+    size_t check_cap = 0;
+    // Spectral attribution: per-sample class / luminance records of one launch and the
+    // frame's attribution map.
+    uint8_t* d_attr_cls = nullptr;
+    size_t attr_cls_cap = 0;
+    float* d_attr_y = nullptr;
+    size_t attr_y_cap = 0;
+    ix_attribution_pixel* d_attr_map = nullptr;
+    size_t attr_map_cap = 0;
+    ix_attribution_pixel* h_attr_map = nullptr;
+    size_t hattr_map_cap = 0;
+    // The one-shot batch entry's device sums.
+    double* d_batch_out = nullptr;
+    size_t batch_out_cap = 0;
+    // A host scene's per-facet finishes, copied for the kernels.
+    uint8_t* d_finishes = nullptr;
+    size_t finishes_cap = 0;
+    int sm_count = 0;
+    uint32_t variant = 0;
+    // Register variant new batch plans start from: the last autotuner pick (or `variant`).
+    uint32_t batch_variant = 0;
+    // Resident CTAs per SM by [uniaxial instantiation][variant].
+    int bps_exact[2][3] = {{1, 1, 1}, {1, 1, 1}}, bps_fast[2][3] = {{1, 1, 1}, {1, 1, 1}};
+    // ... and of the attributed trace kernels by [uniaxial instantiation].
+    int bps_attr_exact[2] = {1, 1}, bps_attr_fast[2] = {1, 1};
+    std::string label;
+    // State.
+    bool lost = false;
+    std::string last_error;
+    ix_timing timing{0.0f, 0.0f, 0, 0};
+    uint64_t dropped = 0;
+    // FIFO turnstile.
+    std::mutex mu;
+    std::condition_variable cv;
+    uint64_t next_ticket = 0, serving = 0;
+    // Guide buffers, colour ping-pong and output of the display pipeline.
+    DisplayState* display = nullptr;
+};
+
+namespace ixh {
+
+
+struct Turn {
+    ix_backend* b;
+    explicit Turn(ix_backend* be) : b(be) {
+        std::unique_lock<std::mutex> lk(b->mu);
+        uint64_t mine = b->next_ticket++;
+        b->cv.wait(lk, [&] { return b->serving == mine; });
+    }
+    ~Turn() {
+        std::lock_guard<std::mutex> lk(b->mu);
+        b->serving++;
+        b->cv.notify_all();
+    }
+};
+
+inline bool fail(ix_backend* b, cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return false;
+    b->lost = true;
+    b->last_error = std::string(where) + ": " + cudaGetErrorString(e);
+    (void)cudaGetLastError();
+    return true;
+}
+
+template <typename T>
+inline cudaError_t grow_device(T** p, size_t* cap, size_t need) {
+    if (*cap >= need && *p) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    size_t n = std::max(need, (size_t)1);
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    if (e == cudaSuccess) *cap = n;
+    return e;
+}
+
+template <typename T>
+inline cudaError_t grow_pinned(T** p, size_t* cap, size_t need) {
+    if (*cap >= need && *p) return cudaSuccess;
+    if (*p) cudaFreeHost(*p);
+    *p = nullptr;
+    *cap = 0;
+    size_t n = std::max(need, (size_t)1);
+    cudaError_t e = cudaMallocHost((void**)p, n * sizeof(T));
+    if (e == cudaSuccess) *cap = n;
+    return e;
+}
+
+}  // namespace ixh

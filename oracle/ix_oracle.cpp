@@ -3061,4 +3061,29 @@ void ixo_denoise_and_tonemap_frame(uint32_t width, uint32_t height, uint32_t spp
     ixo_tonemap_to_rgba(filtered.data(), len, 1.0f, IX_COLOR_SPACE_SRGB, rgba, threads);
 }
 
+/* Counting build only: the floating-point operations of one A-Trous denoise of the given
+ * frame (all passes), tallied like ixo_count_flops; `paths` holds pixel-passes. */
+int ixo_count_denoise_flops(const float* color, const float* depth, const float* normal, const int32_t* facet_id,
+                            const uint32_t* path_sig, uint32_t width, uint32_t height, uint32_t spp,
+                            const ix_atrous_params* params, ixo_flop_counts* out) {
+#ifdef IX_COUNT_FLOPS
+    const size_t len = (size_t)width * height;
+    std::vector<float> tmp(3 * len);
+    g_cnt = Counters{};
+    atrous_denoise(color, depth, normal, facet_id, path_sig, width, height, spp, *params, tmp.data(), 1);
+    out->add = g_cnt.add;
+    out->mul = g_cnt.mul;
+    out->fma = g_cnt.fma;
+    out->div = g_cnt.div;
+    out->sqrt = g_cnt.sqrt;
+    out->transcendental = g_cnt.transc;
+    out->paths = (uint64_t)len * std::min(std::max(params->num_passes, 1u), 8u);
+    return 0;
+#else
+    (void)color; (void)depth; (void)normal; (void)facet_id; (void)path_sig; (void)width; (void)height;
+    (void)spp; (void)params; (void)out;
+    return -1;
+#endif
+}
+
 }  // extern "C"

@@ -162,6 +162,10 @@ int ixo_count_flops(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_
  * renderer/tonemap.rs, renderer/frame_denoise.rs); threads 0 = all host threads, the
  * results do not depend on it. */
 void ixo_atrous_params_default(ix_atrous_params* p);
+/* Counting build only: the operation tally of one A-Trous denoise (paths = pixel-passes). */
+int ixo_count_denoise_flops(const float* color, const float* depth, const float* normal, const int32_t* facet_id,
+                            const uint32_t* path_sig, uint32_t width, uint32_t height, uint32_t spp,
+                            const ix_atrous_params* params, ixo_flop_counts* out);
 void ixo_generate_guide_buffers(uint32_t width, uint32_t height, const ix_camera* cam, const float* planes,
                                 uint32_t n_planes, float n_d, float* depth, float* normal, int32_t* facet_id,
                                 uint32_t* path_sig, int threads);

@@ -147,6 +147,21 @@ def _load(name: str) -> C.CDLL:
     lib.ixo_count_flops.restype = C.c_int
     lib.ixo_count_flops.argtypes = [P(abi.Scene), C.c_uint32, C.c_uint32, C.c_uint32,
                                     C.c_uint32, C.c_uint32, P(FlopCounts)]
+    i32p, u32p, u8p = P(C.c_int32), P(C.c_uint32), P(C.c_uint8)
+    lib.ixo_atrous_params_default.argtypes = [P(abi.AtrousParams)]
+    lib.ixo_generate_guide_buffers.argtypes = [C.c_uint32, C.c_uint32, P(abi.Camera), f32p, C.c_uint32,
+                                               C.c_float, f32p, f32p, i32p, u32p, C.c_int]
+    lib.ixo_n_d.restype = C.c_float
+    lib.ixo_n_d.argtypes = [P(abi.Dispersion)]
+    lib.ixo_atrous_denoise.argtypes = [f32p, f32p, f32p, i32p, u32p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                       P(abi.AtrousParams), f32p, C.c_int]
+    lib.ixo_color_encode.argtypes = [f32p, C.c_uint32, u8p]
+    lib.ixo_count_denoise_flops.restype = C.c_int
+    lib.ixo_count_denoise_flops.argtypes = [f32p, f32p, f32p, i32p, u32p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                            P(abi.AtrousParams), P(FlopCounts)]
+    lib.ixo_tonemap_to_rgba.argtypes = [f32p, C.c_uint64, C.c_float, C.c_uint32, u8p, C.c_int]
+    lib.ixo_denoise_and_tonemap_frame.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, f32p, f32p, f32p, i32p,
+                                                  u32p, P(abi.AtrousParams), u8p, C.c_int]
     _LIBS[name] = lib
     return lib
 
@@ -371,3 +386,95 @@ def path_events_facet(events: PathEvents, bounce: int, facet: int, normal, insid
     d = np.asarray(dir_after, np.float32)
     lib().ixo_path_events_facet(C.byref(events), bounce, facet, _f32p(n), int(inside_before), int(inside_after),
                                 _f32p(d))
+
+
+# ---- display pipeline (renderer/guide_pass.rs, renderer/denoise/, renderer/tonemap.rs) ----
+def _ptr(a: np.ndarray, ctype):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ctype))
+
+
+def generate_guide_buffers(width: int, height: int, camera: abi.Camera, planes: np.ndarray, n_d: float = 0.0,
+                           threads: int = 0):
+    """generate_guide_buffers_with_index: (depth, normal[h, w, 3], facet_id, path_sig)."""
+    planes = np.ascontiguousarray(planes, np.float32)
+    depth = np.zeros((height, width), np.float32)
+    normal = np.zeros((height, width, 3), np.float32)
+    facet = np.zeros((height, width), np.int32)
+    sig = np.zeros((height, width), np.uint32)
+    lib().ixo_generate_guide_buffers(width, height, C.byref(camera), _f32p(planes), planes.shape[0], n_d,
+                                     _f32p(depth), _f32p(normal), _ptr(facet, C.c_int32),
+                                     _ptr(sig, C.c_uint32), threads)
+    return depth, normal, facet, sig
+
+
+def n_d(dispersion: abi.Dispersion) -> float:
+    return float(lib().ixo_n_d(C.byref(dispersion)))
+
+
+def atrous_denoise(color: np.ndarray, depth: np.ndarray, normal: np.ndarray, facet: np.ndarray, sig, spp: int,
+                   params: abi.AtrousParams = None, threads: int = 0) -> np.ndarray:
+    """AtrousDenoiser::denoise_into on [h, w, 3] float32 colour; `sig` None for no signature."""
+    h, w = facet.shape
+    params = params if params is not None else abi.AtrousParams.default()
+    color = np.ascontiguousarray(color, np.float32)
+    out = np.zeros((h, w, 3), np.float32)
+    sig = None if sig is None else np.ascontiguousarray(sig, np.uint32)
+    lib().ixo_atrous_denoise(_f32p(color), _f32p(np.ascontiguousarray(depth, np.float32)),
+                             _f32p(np.ascontiguousarray(normal, np.float32)),
+                             _ptr(np.ascontiguousarray(facet, np.int32), C.c_int32), _ptr(sig, C.c_uint32),
+                             w, h, spp, C.byref(params), _f32p(out), threads)
+    return out
+
+
+def color_encode(xyz, color_space: int = abi.COLOR_SPACE_SRGB) -> bytes:
+    """ColorSpace::encode with ToneMap::AcesFilmic { exposure: 1.0 }."""
+    v = np.ascontiguousarray(xyz, np.float32)
+    out = np.zeros(4, np.uint8)
+    lib().ixo_color_encode(_f32p(v), color_space, _ptr(out, C.c_uint8))
+    return bytes(out)
+
+
+def tonemap_to_rgba(xyz: np.ndarray, scale: float = 1.0, color_space: int = abi.COLOR_SPACE_SRGB,
+                    threads: int = 0) -> np.ndarray:
+    """tonemap_to_rgba / tonemap_wide_gamut_with_threads: RGBA8 per pixel of `xyz` (..., 3)."""
+    xyz = np.ascontiguousarray(xyz, np.float32)
+    n = xyz.size // 3
+    out = np.zeros(xyz.shape[:-1] + (4,), np.uint8)
+    lib().ixo_tonemap_to_rgba(_f32p(xyz), n, scale, color_space, _ptr(out, C.c_uint8), threads)
+    return out
+
+
+def tonemap_accumulation(accum: np.ndarray, samples_per_pixel: int, color_space: int) -> np.ndarray:
+    """tonemap_accumulation (tonemap.rs:213): encode(accum * (1 / spp)) in `color_space`."""
+    inv = np.float32(1.0) / np.float32(samples_per_pixel)
+    return tonemap_to_rgba(accum, float(inv), color_space)
+
+
+def denoise_and_tonemap_frame(accum: np.ndarray, spp: int, depth, normal, facet, sig=None, params=None,
+                              threads: int = 0) -> np.ndarray:
+    """denoise_and_tonemap_frame_with_params_into: sRGB RGBA8 [h, w, 4]."""
+    h, w = facet.shape
+    params = params if params is not None else abi.AtrousParams.default()
+    accum = np.ascontiguousarray(accum, np.float32)
+    out = np.zeros((h, w, 4), np.uint8)
+    sig = None if sig is None else np.ascontiguousarray(sig, np.uint32)
+    lib().ixo_denoise_and_tonemap_frame(w, h, spp, _f32p(accum), _f32p(np.ascontiguousarray(depth, np.float32)),
+                                        _f32p(np.ascontiguousarray(normal, np.float32)),
+                                        _ptr(np.ascontiguousarray(facet, np.int32), C.c_int32),
+                                        _ptr(sig, C.c_uint32), C.byref(params), _ptr(out, C.c_uint8), threads)
+    return out
+
+
+def count_denoise_flops(color, depth, normal, facet, sig, spp: int, params=None) -> FlopCounts:
+    """Counting build: the operations of one A-Trous denoise; `paths` = pixel-passes."""
+    h, w = facet.shape
+    params = params if params is not None else abi.AtrousParams.default()
+    out = FlopCounts()
+    sig = None if sig is None else np.ascontiguousarray(sig, np.uint32)
+    rc = counting_lib().ixo_count_denoise_flops(
+        _f32p(np.ascontiguousarray(color, np.float32)), _f32p(np.ascontiguousarray(depth, np.float32)),
+        _f32p(np.ascontiguousarray(normal, np.float32)), _ptr(np.ascontiguousarray(facet, np.int32), C.c_int32),
+        _ptr(sig, C.c_uint32), w, h, spp, C.byref(params), C.byref(out))
+    if rc != 0:
+        raise RuntimeError("the counting oracle build is required")
+    return out

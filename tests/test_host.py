@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 from indicatrix_b200 import abi, geometry, materials, workloads
+from indicatrix_b200.display import DisplayTiming
 from indicatrix_b200.backend import (FrameScene, GpuAccumulate, GpuBackend, camera_new,
                                      environment_preset, load_library, scene_routes_to_gpu)
 
@@ -21,7 +22,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = []
-    for h in ("ix_cuda.h", "ix_dispatch.h"):
+    for h in ("ix_cuda.h", "ix_dispatch.h", "ix_display.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names += re.findall(r"\b(ix_[a-z0-9_]+)\s*\(", text)
@@ -31,7 +32,7 @@ def declared_functions():
 def test_library_exports_every_declared_symbol():
     lib = load_library()
     names = declared_functions()
-    assert len(names) >= 20
+    assert len(names) >= 30
     for n in names:
         assert hasattr(lib, n), n
 
@@ -47,8 +48,10 @@ def test_abi_struct_layout_matches_c():
         "ix_gem_metrics": abi.GemMetrics, "ix_metrics_lighting": abi.MetricsLighting,
         "ix_metrics_stone": abi.MetricsStone, "ix_metrics_pose": abi.MetricsPose,
         "ix_attribution_pixel": abi.AttributionPixel,
+        "ix_atrous_params": abi.AtrousParams, "ix_display_timing": DisplayTiming,
     }
-    src = ['#include <stdio.h>', '#include <stddef.h>', '#include "ix_cuda.h"', "int main(void){"]
+    src = ['#include <stdio.h>', '#include <stddef.h>', '#include "ix_cuda.h"', '#include "ix_display.h"',
+           "int main(void){"]
     for cname, py in checks.items():
         src.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
         for fname, _ in py._fields_:
