@@ -429,10 +429,11 @@ def main_display(args):
 
     # End to end through the public host API: H2D of the f32 sums, D2H of the RGBA8.
     e2e_ms = []
-    for k in range(max(1, args.warmup // 2) + args.steps):
+    host_rgba = np.zeros((fs.height, fs.width, 4), np.uint8)  # the caller's frame buffer, reused
+    for k in range(max(1, args.warmup // 2) + min(args.steps, 50)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        out = display.display_frame(backend, fs, spp, accum, True)
+        out = display.display_frame(backend, fs, spp, accum, True, out=host_rgba)
         if out is None:
             raise RuntimeError(f"display declined: {backend.last_lost_reason()}")
         if k >= max(1, args.warmup // 2):
@@ -465,8 +466,10 @@ def main_display(args):
             "e2e": {"value": world / (e2e_mean * 1e-3), "unit": DISPLAY_UNIT,
                     "h2d_bytes_per_step": pixels * 12, "d2h_bytes_per_step": pixels * 4, "ms_per_step": e2e_mean},
             "gpu_launches": launches,
+            # traffic: DRAM read + write bytes of one A-Trous launch (passes 1-4) from the
+            # ncu capture of this workload at full size (profiles/atrous_display_1080p.md).
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": 56.3e6,
                          "peak_source": f"{peak_kind} HBM copy bandwidth",
                          "kernel": "atrous_pass_kernel", "launch_ms": atrous_launch_ms,
                          "algorithmic_bytes_per_launch": bytes_per_launch,

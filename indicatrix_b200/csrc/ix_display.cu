@@ -9,11 +9,11 @@
 // color/gamut.rs (project_to_gamut_bounded :43-101), optics/raytracer/color.rs
 // (aces_tonemap :372).
 //
-// Layout: one thread per pixel everywhere.  The A-Trous passes read the colour as
-// float4 (one 16-byte load per tap), the guides packed as float4 (unit normal, sanitised
-// depth) and int2 (facet id, path signature); a 32 x 8 block makes every tap of a warp
-// one contiguous 32-pixel row segment, so the dilated taps stay coalesced at every
-// stride.  The last pass writes RGBA8 directly (the tone-map is fused into it), so the
+// Layout: one thread per pixel everywhere.  The A-Trous passes read the colour with the
+// pixel's sanitised depth as one float4 (one 16-byte load per tap), the facet id and path
+// signature as int2 and, unless the normals are the facets' own, the unit normal as
+// float4; a 32 x 8 block makes every tap of a warp one contiguous 32-pixel row segment,
+// so the dilated taps stay coalesced at every stride.  The last pass writes RGBA8 directly (the tone-map is fused into it), so the
 // filtered colour never goes back to HBM.
 //
 // Built twice like the transport: IX_EXACT=1 (-fmad=false; exp and pow rounded from
@@ -78,7 +78,65 @@ IX_DEV bool in_range(V3 v, float mx) {
     return v.x >= 0.0f && v.y >= 0.0f && v.z >= 0.0f && v.x <= mx && v.y <= mx && v.z <= mx;
 }
 // project_to_gamut_bounded (gamut.rs:43-101): walk the chromaticity toward the white
-// point at constant luminance in 32 steps, first in-range step wins.
+// point at constant luminance in 32 steps; the first step whose RGB is in [0, mx] wins.
+//
+// The walk is the reference's, step for step, but only over the steps that can pass.  In
+// exact arithmetic, with yp(t) > 0 on the whole walk, step t's RGB is (lum / yp(t)) M c(t)
+// with c(t) = (xp, yp, 1 - xp - yp) linear in t, so each of the six range conditions is a
+// linear inequality alpha + beta t >= 0 and the steps that can pass form one interval.
+// The bounds are computed with a margin of 1e-5 relative to the magnitudes involved
+// (the float evaluation of a step, and of the bounds' own coefficients, errs by a few
+// 1e-7 of them) and widened by a step on each side; every step outside is out of range in float arithmetic too, and the
+// steps inside are evaluated exactly as the reference does, in order.  Inputs outside
+// the analysed domain (lum <= 0, chromaticity y <= 1e-3, |x|, |y| > 8) walk all 33 steps.
+IX_DEV V3 gamut_step(uint32_t sp, float x, float y, float lum, float wx, float wy, float t) {
+    const float xp = fmaf(wx - x, t, x);
+    const float yp = fmaf(wy - y, t, y);
+    if (yp > 1e-6f) return xyz_to_linear(sp, v3((xp / yp) * lum, lum, (((1.0f - xp) - yp) / yp) * lum));
+    return xyz_to_linear(sp, v3((wx / wy) * lum, lum, (((1.0f - wx) - wy) / wy) * lum));
+}
+IX_DEV void walk_bounds(uint32_t sp, float x, float y, float lum, float wx, float wy, float mx, int* i_begin,
+                        int* i_end) {
+    *i_begin = 0;
+    *i_end = 32;
+    if (!(lum > 0.0f) || !(y > 1e-3f) || !(fabsf(x) <= 8.0f) || !(fabsf(y) <= 8.0f) || !isfinite(mx)) return;
+    const float dx = wx - x, dy = wy - y;
+    const float cbound = 2.0f + 2.0f * fmaxf(1.0f, fmaxf(fabsf(x), fabsf(y)));
+    float lo = 0.0f, hi = 1.0f;
+    const float* r = c_xyz_to_rgb[sp];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float m0 = r[3 * k], m1 = r[3 * k + 1], m2 = r[3 * k + 2];
+        // The coefficients' own float error is below 1e-6 of these magnitudes, the margin
+        // 1e-5 of them, so the half-lines below contain every step that can pass.
+        const float a = m0 * x + m1 * y + m2 * (1.0f - x - y);
+        const float bcoef = m0 * dx + m1 * dy - m2 * (dx + dy);
+        const float s = (fabsf(m0) + fabsf(m1) + fabsf(m2)) * cbound * 1e-5f;
+        // lower: a + b t >= -s ; upper: mx (y + dy t) - lum (a + b t) >= -s_up, whose
+        // margin also covers the rounding of the mx y and mx dy terms.
+        const float s_up = lum * s + (fabsf(mx * y) + fabsf(mx * dy)) * 1e-5f;
+        const float alpha[2] = {a + s, mx * y - lum * a + s_up};
+        const float beta[2] = {bcoef, mx * dy - lum * bcoef};
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            if (beta[c] > 0.0f) {
+                lo = fmaxf(lo, -alpha[c] / beta[c]);
+            } else if (beta[c] < 0.0f) {
+                hi = fminf(hi, -alpha[c] / beta[c]);
+            } else if (alpha[c] < 0.0f) {
+                lo = 2.0f;  // this condition fails at every step
+            }
+        }
+    }
+    if (!(lo <= hi)) {
+        *i_begin = 1;
+        *i_end = 0;
+        return;
+    }
+    // The bounds are within 1e-6 of the half-lines' ends; one step of slack either side.
+    *i_begin = max(0, (int)ceilf(32.0f * lo) - 1);
+    *i_end = min(32, (int)floorf(32.0f * hi) + 1);
+}
 IX_DEV V3 project_to_gamut_bounded(V3 c, uint32_t sp, float mx) {
     const float sum = (c.x + c.y) + c.z;
     if (!isfinite(sum) || sum <= 1e-6f) return v3(0.0f, 0.0f, 0.0f);
@@ -87,22 +145,14 @@ IX_DEV V3 project_to_gamut_bounded(V3 c, uint32_t sp, float mx) {
     const V3 lin = xyz_to_linear(sp, c);
     if (in_range(lin, mx)) return lin;
     const float wx = c_white_xy[sp][0], wy = c_white_xy[sp][1];
-    auto mapped = [&](float t) {
-        const float xp = fmaf(wx - x, t, x);
-        const float yp = fmaf(wy - y, t, y);
-        if (yp > 1e-6f) return v3((xp / yp) * lum, lum, (((1.0f - xp) - yp) / yp) * lum);
-        return v3((wx / wy) * lum, lum, (((1.0f - wx) - wy) / wy) * lum);
-    };
-    const V3 w = xyz_to_linear(sp, mapped(1.0f));
-    V3 resolved = v3(fmaxf(w.x, 0.0f), fmaxf(w.y, 0.0f), fmaxf(w.z, 0.0f));
-    for (uint32_t i = 0; i <= 32; ++i) {
-        const V3 cand = xyz_to_linear(sp, mapped((float)i / 32.0f));
-        if (in_range(cand, mx)) {
-            resolved = cand;
-            break;
-        }
+    int i0, i1;
+    walk_bounds(sp, x, y, lum, wx, wy, mx, &i0, &i1);
+    for (int i = i0; i <= i1; ++i) {
+        const V3 cand = gamut_step(sp, x, y, lum, wx, wy, (float)i / 32.0f);
+        if (in_range(cand, mx)) return cand;
     }
-    return resolved;
+    const V3 w = gamut_step(sp, x, y, lum, wx, wy, 1.0f);
+    return v3(fmaxf(w.x, 0.0f), fmaxf(w.y, 0.0f), fmaxf(w.z, 0.0f));
 }
 // TransferFunction::encode (space.rs:54-75).
 IX_DEV float transfer_encode(uint32_t sp, float lin) {
@@ -150,7 +200,14 @@ IX_DEV float cos_pow(float base, float power, int squarings) {
 
 // One output pixel of an A-Trous pass (atrous_pixel, pass.rs:330-378): the weights of
 // tap_contribution (:283-316) in the reference's factor order, the taps row by row.
-template <bool TONEMAP>
+//
+// Colour and depth travel together (float4 {x, y, z, sanitised depth}); the 5 taps of a
+// row are loaded before any is used (coordinates clamped into the image, the mask says
+// which count), so a thread keeps up to 15 loads in flight instead of one.  With
+// FACET_NORMALS the guides' normal is a function of the facet id (the guide pass writes
+// the plane normal), so a tap that passes the facet test has the centre's normal bit for
+// bit and its normal weight is the centre's own, computed once: the tap needs no normal.
+template <bool TONEMAP, bool FACET_NORMALS>
 __global__ void __launch_bounds__(256) atrous_pass_kernel(PassLaunch L) {
     const int x = (int)(blockIdx.x * 32u + threadIdx.x);
     const int y = (int)(blockIdx.y * 8u + threadIdx.y);
@@ -159,11 +216,17 @@ __global__ void __launch_bounds__(256) atrous_pass_kernel(PassLaunch L) {
     const size_t ci = (size_t)y * (size_t)w + (size_t)x;
     const float4 raw = L.src[ci];
     const V3 color = finite3(raw) ? v3(raw.x, raw.y, raw.z) : v3(0.0f, 0.0f, 0.0f);
+    const float cdepth = raw.w;
     const int2 cf = L.fs[ci];
     V3 out = color;
     if (cf.x >= 0) {
-        const float4 cn = L.nd[ci];
+        const float4 cn = L.nrm[ci];
         const bool c_zero = cn.x == 0.0f && cn.y == 0.0f && cn.z == 0.0f;
+        float wn_self = 1.0f;
+        if (FACET_NORMALS && !c_zero) {
+            const float c = fmaxf(clampf_((cn.x * cn.x + cn.y * cn.y) + cn.z * cn.z, -1.0f, 1.0f), 0.0f);
+            wn_self = cos_pow(c, L.normal_power, L.squarings);
+        }
         V3 sum = v3(0.0f, 0.0f, 0.0f);
         float wsum = 0.0f;
 #pragma unroll
@@ -172,32 +235,41 @@ __global__ void __launch_bounds__(256) atrous_pass_kernel(PassLaunch L) {
             if (sy < 0 || sy >= h) continue;
             const float hy = c_b3[ky];
             const size_t row = (size_t)sy * (size_t)w;
+            int2 q[5];
+            float4 t[5], qn[5];
+            bool ok[5];
 #pragma unroll
             for (int kx = 0; kx < 5; ++kx) {
                 const int sx = x + (kx - 2) * L.stride;
-                if (sx < 0 || sx >= w) continue;
-                const size_t idx = row + (size_t)sx;
-                const int2 q = L.fs[idx];
+                ok[kx] = sx >= 0 && sx < w;
+                const size_t idx = row + (size_t)min(max(sx, 0), w - 1);
+                q[kx] = L.fs[idx];
+                t[kx] = L.src[idx];
+                if (!FACET_NORMALS) qn[kx] = L.nrm[idx];
+            }
+#pragma unroll
+            for (int kx = 0; kx < 5; ++kx) {
                 // Facet identity, then the interior path signature (0 everywhere when
                 // the frame has none): hard rejections.
-                if (q.x != cf.x || q.y != cf.y) continue;
-                const float4 t = L.src[idx];
-                if (!finite3(t)) continue;
-                const float4 qn = L.nd[idx];
+                if (!ok[kx] || q[kx].x != cf.x || q[kx].y != cf.y) continue;
+                if (!finite3(t[kx])) continue;
                 float wn = 1.0f;
-                if (!c_zero && !(qn.x == 0.0f && qn.y == 0.0f && qn.z == 0.0f)) {
-                    const float c = fmaxf(clampf_((cn.x * qn.x + cn.y * qn.y) + cn.z * qn.z, -1.0f, 1.0f), 0.0f);
+                if (FACET_NORMALS) {
+                    wn = wn_self;
+                } else if (!c_zero && !(qn[kx].x == 0.0f && qn[kx].y == 0.0f && qn[kx].z == 0.0f)) {
+                    const float c = fmaxf(
+                        clampf_((cn.x * qn[kx].x + cn.y * qn[kx].y) + cn.z * qn[kx].z, -1.0f, 1.0f), 0.0f);
                     wn = cos_pow(c, L.normal_power, L.squarings);
                 }
                 if (wn == 0.0f) continue;
-                const float gap = fabsf(cn.w - qn.w);
+                const float gap = fabsf(cdepth - t[kx].w);
                 const float wd = gap == 0.0f ? 1.0f : exp_disp(gap * L.neg_inv_sigma_depth);
-                const float dx = color.x - t.x, dy = color.y - t.y, dz = color.z - t.z;
+                const float dx = color.x - t[kx].x, dy = color.y - t[kx].y, dz = color.z - t[kx].z;
                 const float dist_sq = (dx * dx + dy * dy) + dz * dz;
                 const float wc = dist_sq == 0.0f ? 1.0f : exp_disp(dist_sq * L.neg_inv_two_sigma_color_sq);
                 // kernel_w * wf * wn * wd * wc with the facet weight wf = 1.
                 const float wgt = (((hy * c_b3[kx]) * wn) * wd) * wc;
-                sum = v3(sum.x + t.x * wgt, sum.y + t.y * wgt, sum.z + t.z * wgt);
+                sum = v3(sum.x + t[kx].x * wgt, sum.y + t[kx].y * wgt, sum.z + t[kx].z * wgt);
                 wsum = wsum + wgt;
             }
         }
@@ -206,7 +278,7 @@ __global__ void __launch_bounds__(256) atrous_pass_kernel(PassLaunch L) {
     if (TONEMAP)
         L.rgba[ci] = color_encode(out * 1.0f, IX_COLOR_SPACE_SRGB);
     else
-        L.dst[ci] = make_float4(out.x, out.y, out.z, 0.0f);
+        L.dst[ci] = make_float4(out.x, out.y, out.z, cdepth);
 }
 
 __global__ void __launch_bounds__(256) tonemap_kernel(TonemapLaunch L) {
@@ -326,9 +398,9 @@ __global__ void __launch_bounds__(128) guide_kernel(GuideLaunch L) {
         }
         if (L.facet) L.facet[pix] = facet;
         if (L.sig) L.sig[pix] = sig;
-        if (L.nd) {
+        if (L.nrm) {
             const V3 u = unit_normal_or_zero(normal);
-            L.nd[pix] = make_float4(u.x, u.y, u.z, sanitize(depth));
+            L.nrm[pix] = make_float4(u.x, u.y, u.z, sanitize(depth));
         }
         if (L.fs) L.fs[pix] = make_int2(facet, (int)sig);
     }
@@ -337,14 +409,19 @@ __global__ void __launch_bounds__(128) guide_kernel(GuideLaunch L) {
 __global__ void __launch_bounds__(256) pack_kernel(PackLaunch L) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < L.pixels;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        if (L.nd) {
+        float depth;
+        if (L.depth) {
+            // Guides in the reference layout -> unit normal (w: sanitised depth), (facet, sig).
             const V3 u = unit_normal_or_zero(v3(L.normal[3 * i], L.normal[3 * i + 1], L.normal[3 * i + 2]));
-            L.nd[i] = make_float4(u.x, u.y, u.z, sanitize(L.depth[i]));
+            depth = sanitize(L.depth[i]);
+            L.nrm[i] = make_float4(u.x, u.y, u.z, depth);
             L.fs[i] = make_int2(L.facet[i], L.sig ? (int)L.sig[i] : 0);
+        } else {
+            depth = L.nrm[i].w;  // packed by the guide pass
         }
         if (L.color_out)
             L.color_out[i] = make_float4(L.color[3 * i] * L.scale, L.color[3 * i + 1] * L.scale,
-                                         L.color[3 * i + 2] * L.scale, 0.0f);
+                                         L.color[3 * i + 2] * L.scale, depth);
     }
 }
 #endif
@@ -359,10 +436,17 @@ unsigned int linear_blocks(uint64_t n) {
 cudaError_t IX_DISP_FN(launch_atrous_pass)(const PassLaunch& L, cudaStream_t s) {
     if (L.width == 0 || L.height == 0) return cudaSuccess;
     const dim3 block(32, 8), grid((L.width + 31) / 32, (L.height + 7) / 8);
-    if (L.rgba)
-        atrous_pass_kernel<true><<<grid, block, 0, s>>>(L);
-    else
-        atrous_pass_kernel<false><<<grid, block, 0, s>>>(L);
+    if (L.rgba) {
+        if (L.facet_normals)
+            atrous_pass_kernel<true, true><<<grid, block, 0, s>>>(L);
+        else
+            atrous_pass_kernel<true, false><<<grid, block, 0, s>>>(L);
+    } else {
+        if (L.facet_normals)
+            atrous_pass_kernel<false, true><<<grid, block, 0, s>>>(L);
+        else
+            atrous_pass_kernel<false, false><<<grid, block, 0, s>>>(L);
+    }
     return cudaGetLastError();
 }
 cudaError_t IX_DISP_FN(launch_tonemap)(const TonemapLaunch& L, cudaStream_t s) {

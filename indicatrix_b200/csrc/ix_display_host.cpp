@@ -12,14 +12,86 @@
 #include "ix_backend_state.h"
 #include "ix_display_launch.h"
 
+#include <atomic>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 using namespace ixh;
 
+// A few host threads that copy between pageable caller memory and the pinned staging
+// ring; `run(fn)` calls fn(t) for t = 0..size()-1 (t = 0 on the calling thread) and
+// returns when all have finished.
+class CopyPool {
+public:
+    CopyPool() {
+        const unsigned hc = std::thread::hardware_concurrency();
+        n_ = std::max(1u, std::min(8u, hc ? hc : 1u));
+        for (unsigned t = 1; t < n_; ++t) workers_.emplace_back([this, t] { loop(t); });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& w : workers_) w.join();
+    }
+    unsigned size() const { return n_; }
+    void run(const std::function<void(unsigned)>& fn) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            fn_ = &fn;
+            pending_ = n_ - 1;
+            ++generation_;
+        }
+        cv_.notify_all();
+        fn(0);
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [&] { return pending_ == 0; });
+        fn_ = nullptr;
+    }
+
+private:
+    void loop(unsigned t) {
+        uint64_t seen = 0;
+        for (;;) {
+            const std::function<void(unsigned)>* fn;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || generation_ != seen; });
+                if (stop_) return;
+                seen = generation_;
+                fn = fn_;
+            }
+            (*fn)(t);
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--pending_ == 0) done_cv_.notify_all();
+        }
+    }
+    unsigned n_ = 1;
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(unsigned)>* fn_ = nullptr;
+    unsigned pending_ = 0;
+    uint64_t generation_ = 0;
+    bool stop_ = false;
+};
+
+constexpr size_t STAGE_CHUNK = 4u << 20;  // bytes per pinned slot
+
 struct DisplayState {
+    // Pinned two-slot ring for host <-> device copies of caller buffers, and the threads
+    // that fill and drain it.
+    uint8_t* h_stage = nullptr;
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    CopyPool pool;
     float* d_planes = nullptr;
     size_t planes_cap = 0;
     // Guides in the reference layout (uploaded or computed).
@@ -32,8 +104,8 @@ struct DisplayState {
     uint32_t* d_sig = nullptr;
     size_t sig_cap = 0;
     // Packed guides and the colour ping-pong of the passes.
-    float4* d_nd = nullptr;
-    size_t nd_cap = 0;
+    float4* d_nrm = nullptr;
+    size_t nrm_cap = 0;
     int2* d_fs = nullptr;
     size_t fs_cap = 0;
     float4* d_col[2] = {nullptr, nullptr};
@@ -54,12 +126,15 @@ struct DisplayState {
 
 void display_state_free(DisplayState* d) {
     if (!d) return;
+    if (d->h_stage) cudaFreeHost(d->h_stage);
+    for (cudaEvent_t e : d->stage_ev)
+        if (e) cudaEventDestroy(e);
     cudaFree(d->d_planes);
     cudaFree(d->d_depth);
     cudaFree(d->d_normal);
     cudaFree(d->d_facet);
     cudaFree(d->d_sig);
-    cudaFree(d->d_nd);
+    cudaFree(d->d_nrm);
     cudaFree(d->d_fs);
     cudaFree(d->d_col[0]);
     cudaFree(d->d_col[1]);
@@ -81,6 +156,10 @@ DisplayState* state(ix_backend* b) {
         b->display = new DisplayState();
         for (cudaEvent_t& e : b->display->ev)
             if (cudaEventCreate(&e) != cudaSuccess) e = nullptr;
+        for (cudaEvent_t& e : b->display->stage_ev)
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) e = nullptr;
+        if (cudaMallocHost((void**)&b->display->h_stage, 2 * STAGE_CHUNK) != cudaSuccess)
+            b->display->h_stage = nullptr;
     }
     return b->display;
 }
@@ -132,7 +211,7 @@ Resolved resolve(const ix_atrous_params& p, uint32_t spp) {
 }
 
 bool alloc_frame(ix_backend* b, DisplayState* d, uint64_t n, bool guides_raw, bool xyz, bool rgba) {
-    cudaError_t e = grow_device(&d->d_nd, &d->nd_cap, n);
+    cudaError_t e = grow_device(&d->d_nrm, &d->nrm_cap, n);
     if (e == cudaSuccess) e = grow_device(&d->d_fs, &d->fs_cap, n);
     if (e == cudaSuccess) e = grow_device(&d->d_col[0], &d->col_cap[0], n);
     if (e == cudaSuccess) e = grow_device(&d->d_col[1], &d->col_cap[1], n);
@@ -154,6 +233,62 @@ cudaError_t d2h(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s) : cudaSuccess;
 }
 
+// Caller memory is pageable: it goes through the pinned ring in 4 MB chunks, the host
+// threads copying chunk k + 1 while the DMA engine moves chunk k.  Without a ring (pinned
+// allocation failed) the plain pageable copy is used.
+void parallel_copy(DisplayState* d, void* dst, const void* src, size_t bytes) {
+    const unsigned nt = d->pool.size();
+    const size_t part = (bytes + nt - 1) / nt;
+    d->pool.run([&](unsigned t) {
+        const size_t off = (size_t)t * part;
+        if (off < bytes) std::memcpy((uint8_t*)dst + off, (const uint8_t*)src + off, std::min(part, bytes - off));
+    });
+}
+cudaError_t h2d_staged(DisplayState* d, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    if (!d->h_stage || !d->stage_ev[0] || !d->stage_ev[1] || bytes < (256u << 10)) return h2d(dst, src, bytes, st);
+    for (size_t off = 0, k = 0; off < bytes; off += STAGE_CHUNK, ++k) {
+        const int slot = (int)(k & 1);
+        const size_t len = std::min(STAGE_CHUNK, bytes - off);
+        cudaError_t e = cudaEventSynchronize(d->stage_ev[slot]);  // the slot's previous DMA
+        if (e != cudaSuccess) return e;
+        uint8_t* h = d->h_stage + slot * STAGE_CHUNK;
+        parallel_copy(d, h, (const uint8_t*)src + off, len);
+        e = cudaMemcpyAsync((uint8_t*)dst + off, h, len, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaEventRecord(d->stage_ev[slot], st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+// Device -> caller memory; returns when `dst` holds the data (it waits for the stream).
+cudaError_t d2h_staged(DisplayState* d, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    if (!d->h_stage || !d->stage_ev[0] || !d->stage_ev[1] || bytes < (256u << 10)) {
+        cudaError_t e = d2h(dst, src, bytes, st);
+        return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+    }
+    const size_t chunks = (bytes + STAGE_CHUNK - 1) / STAGE_CHUNK;
+    auto issue = [&](size_t k) {
+        const int slot = (int)(k & 1);
+        const size_t off = k * STAGE_CHUNK, len = std::min(STAGE_CHUNK, bytes - off);
+        cudaError_t e = cudaEventSynchronize(d->stage_ev[slot]);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d->h_stage + slot * STAGE_CHUNK, (const uint8_t*)src + off, len,
+                                cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaEventRecord(d->stage_ev[slot], st);
+        return e;
+    };
+    cudaError_t e = issue(0);
+    for (size_t k = 0; k < chunks && e == cudaSuccess; ++k) {
+        const int slot = (int)(k & 1);
+        const size_t off = k * STAGE_CHUNK, len = std::min(STAGE_CHUNK, bytes - off);
+        e = cudaEventSynchronize(d->stage_ev[slot]);
+        if (e != cudaSuccess) break;
+        // Chunk k has landed; start chunk k + 1 into the other slot before copying out.
+        if (k + 1 < chunks) e = issue(k + 1);
+        parallel_copy(d, (uint8_t*)dst + off, d->h_stage + slot * STAGE_CHUNK, len);
+    }
+    return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+}
+
 void record(DisplayState* d, int i, cudaStream_t st) {
     if (d->ev[i]) cudaEventRecord(d->ev[i], st);
 }
@@ -163,11 +298,11 @@ float elapsed(DisplayState* d, int a, int c) {
     return 0.0f;
 }
 
-// The passes over the packed guides in d_nd / d_fs and the colour in d_col[0]; the last
+// The passes over the packed guides in d_nrm / d_fs and the colour in d_col[0]; the last
 // pass writes RGBA8 into `rgba` when it is given, else colour.  Returns the index of the
 // colour buffer holding the result (rgba == null) and counts the launches.
 int run_passes(ix_backend* b, DisplayState* d, const Resolved& r, uint32_t w, uint32_t h, uchar4* rgba,
-               uint32_t* launches, cudaError_t* err, cudaStream_t st) {
+               bool facet_normals, uint32_t* launches, cudaError_t* err, cudaStream_t st) {
     int cur = 0;
     *err = cudaSuccess;
     for (uint32_t pass = 0; pass < r.passes && *err == cudaSuccess; ++pass) {
@@ -176,8 +311,9 @@ int run_passes(ix_backend* b, DisplayState* d, const Resolved& r, uint32_t w, ui
         L.height = h;
         L.stride = 1 << pass;
         L.src = d->d_col[cur];
-        L.nd = d->d_nd;
+        L.nrm = d->d_nrm;
         L.fs = d->d_fs;
+        L.facet_normals = facet_normals ? 1 : 0;
         const bool last = pass + 1 == r.passes;
         L.dst = (last && rgba) ? nullptr : d->d_col[cur ^ 1];
         L.rgba = (last && rgba) ? rgba : nullptr;
@@ -191,7 +327,7 @@ int run_passes(ix_backend* b, DisplayState* d, const Resolved& r, uint32_t w, ui
 // The frame after packing: identity -> tone-map the average; else the passes with the
 // tone-map fused into the last.  d_col[0] holds the average.
 cudaError_t frame_after_pack(ix_backend* b, DisplayState* d, const Resolved& r, uint32_t w, uint32_t h,
-                             uint32_t* launches, cudaStream_t st) {
+                             bool facet_normals, uint32_t* launches, cudaStream_t st) {
     const uint64_t n = (uint64_t)w * h;
     if (r.identity) {
         TonemapLaunch T{n, nullptr, d->d_col[0], 1.0f, IX_COLOR_SPACE_SRGB, d->d_rgba};
@@ -199,7 +335,7 @@ cudaError_t frame_after_pack(ix_backend* b, DisplayState* d, const Resolved& r, 
         return tonemap_launch(b, T, st);
     }
     cudaError_t e;
-    run_passes(b, d, r, w, h, d->d_rgba, launches, &e, st);
+    run_passes(b, d, r, w, h, d->d_rgba, facet_normals, launches, &e, st);
     return e;
 }
 
@@ -284,11 +420,10 @@ int ix_generate_guide_buffers(ix_backend* b, uint32_t width, uint32_t height, co
                   d->d_depth, d->d_normal, d->d_facet, path_sig ? d->d_sig : nullptr, nullptr, nullptr};
     if (e == cudaSuccess) e = launch_guides_exact(G, b->stream);
     record(d, 1, b->stream);
-    if (e == cudaSuccess) e = d2h(depth, d->d_depth, 4 * n, b->stream);
-    if (e == cudaSuccess) e = d2h(normal, d->d_normal, 12 * n, b->stream);
-    if (e == cudaSuccess) e = d2h(facet_id, d->d_facet, 4 * n, b->stream);
-    if (e == cudaSuccess && path_sig) e = d2h(path_sig, d->d_sig, 4 * n, b->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess) e = d2h_staged(d, depth, d->d_depth, 4 * n, b->stream);
+    if (e == cudaSuccess) e = d2h_staged(d, normal, d->d_normal, 12 * n, b->stream);
+    if (e == cudaSuccess) e = d2h_staged(d, facet_id, d->d_facet, 4 * n, b->stream);
+    if (e == cudaSuccess && path_sig) e = d2h_staged(d, path_sig, d->d_sig, 4 * n, b->stream);
     if (fail(b, e, "guide pass")) return IX_DECLINED;
     d->pending = false;
     d->timing = ix_display_timing{elapsed(d, 0, 1), 0.0f, 0.0f, 0, 1};
@@ -316,26 +451,25 @@ int ix_atrous_denoise(ix_backend* b, const float* color, const float* depth, con
     if (!alloc_frame(b, d, n, true, true, false)) return IX_DECLINED;
     d->cached = false;
     const auto t0 = std::chrono::steady_clock::now();
-    cudaError_t e = h2d(d->d_xyz, color, 12 * n, b->stream);
-    if (e == cudaSuccess) e = h2d(d->d_depth, depth, 4 * n, b->stream);
-    if (e == cudaSuccess) e = h2d(d->d_normal, normal, 12 * n, b->stream);
-    if (e == cudaSuccess) e = h2d(d->d_facet, facet_id, 4 * n, b->stream);
-    if (e == cudaSuccess && path_sig) e = h2d(d->d_sig, path_sig, 4 * n, b->stream);
+    cudaError_t e = h2d_staged(d, d->d_xyz, color, 12 * n, b->stream);
+    if (e == cudaSuccess) e = h2d_staged(d, d->d_depth, depth, 4 * n, b->stream);
+    if (e == cudaSuccess) e = h2d_staged(d, d->d_normal, normal, 12 * n, b->stream);
+    if (e == cudaSuccess) e = h2d_staged(d, d->d_facet, facet_id, 4 * n, b->stream);
+    if (e == cudaSuccess && path_sig) e = h2d_staged(d, d->d_sig, path_sig, 4 * n, b->stream);
     record(d, 0, b->stream);
-    PackLaunch P{n, d->d_depth, d->d_normal, d->d_facet, path_sig ? d->d_sig : nullptr, d->d_nd, d->d_fs,
+    PackLaunch P{n, d->d_depth, d->d_normal, d->d_facet, path_sig ? d->d_sig : nullptr, d->d_nrm, d->d_fs,
                  d->d_xyz, 1.0f, d->d_col[0]};
     if (e == cudaSuccess) e = launch_pack_exact(P, b->stream);
     record(d, 1, b->stream);
     uint32_t launches = 1;
     int cur = 0;
-    if (e == cudaSuccess) cur = run_passes(b, d, r, width, height, nullptr, &launches, &e, b->stream);
+    if (e == cudaSuccess) cur = run_passes(b, d, r, width, height, nullptr, false, &launches, &e, b->stream);
     record(d, 2, b->stream);
     UnpackLaunch U{n, d->d_col[cur], d->d_xyz};
     if (e == cudaSuccess) e = unpack_launch(b, U, b->stream);
     ++launches;
     record(d, 3, b->stream);
-    if (e == cudaSuccess) e = d2h(out, d->d_xyz, 12 * n, b->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess) e = d2h_staged(d, out, d->d_xyz, 12 * n, b->stream);
     if (fail(b, e, "denoise")) return IX_DECLINED;
     d->pending = false;
     d->timing = ix_display_timing{0.0f, elapsed(d, 0, 1), elapsed(d, 1, 2), r.passes, launches};
@@ -357,13 +491,12 @@ static int tonemap_impl(ix_backend* b, const float* xyz, uint64_t pixels, float 
     if (e == cudaSuccess) e = grow_device(&d->d_rgba, &d->rgba_cap, pixels);
     if (fail(b, e, "tonemap buffers")) return IX_DECLINED;
     const auto t0 = std::chrono::steady_clock::now();
-    e = h2d(d->d_xyz, xyz, 12 * pixels, b->stream);
+    e = h2d_staged(d, d->d_xyz, xyz, 12 * pixels, b->stream);
     record(d, 0, b->stream);
     TonemapLaunch T{pixels, d->d_xyz, nullptr, scale, space, d->d_rgba};
     if (e == cudaSuccess) e = tonemap_launch(b, T, b->stream);
     record(d, 1, b->stream);
-    if (e == cudaSuccess) e = d2h(rgba, d->d_rgba, 4 * pixels, b->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess) e = d2h_staged(d, rgba, d->d_rgba, 4 * pixels, b->stream);
     if (fail(b, e, "tonemap")) return IX_DECLINED;
     d->pending = false;
     d->timing = ix_display_timing{0.0f, 0.0f, 0.0f, 0, 1};
@@ -406,22 +539,21 @@ int ix_denoise_and_tonemap_frame(ix_backend* b, uint32_t width, uint32_t height,
     if (!alloc_frame(b, d, n, true, true, true)) return IX_DECLINED;
     d->cached = false;
     const auto t0 = std::chrono::steady_clock::now();
-    cudaError_t e = h2d(d->d_xyz, accum, 12 * n, b->stream);
-    if (e == cudaSuccess) e = h2d(d->d_depth, depth, 4 * n, b->stream);
-    if (e == cudaSuccess) e = h2d(d->d_normal, normal, 12 * n, b->stream);
-    if (e == cudaSuccess) e = h2d(d->d_facet, facet_id, 4 * n, b->stream);
-    if (e == cudaSuccess && path_sig) e = h2d(d->d_sig, path_sig, 4 * n, b->stream);
+    cudaError_t e = h2d_staged(d, d->d_xyz, accum, 12 * n, b->stream);
+    if (e == cudaSuccess) e = h2d_staged(d, d->d_depth, depth, 4 * n, b->stream);
+    if (e == cudaSuccess) e = h2d_staged(d, d->d_normal, normal, 12 * n, b->stream);
+    if (e == cudaSuccess) e = h2d_staged(d, d->d_facet, facet_id, 4 * n, b->stream);
+    if (e == cudaSuccess && path_sig) e = h2d_staged(d, d->d_sig, path_sig, 4 * n, b->stream);
     record(d, 0, b->stream);
     const float inv = 1.0f / (float)spp;
-    PackLaunch P{n, d->d_depth, d->d_normal, d->d_facet, path_sig ? d->d_sig : nullptr, d->d_nd, d->d_fs,
+    PackLaunch P{n, d->d_depth, d->d_normal, d->d_facet, path_sig ? d->d_sig : nullptr, d->d_nrm, d->d_fs,
                  d->d_xyz, inv, d->d_col[0]};
     if (e == cudaSuccess) e = launch_pack_exact(P, b->stream);
     record(d, 1, b->stream);
     uint32_t launches = 1;
-    if (e == cudaSuccess) e = frame_after_pack(b, d, r, width, height, &launches, b->stream);
+    if (e == cudaSuccess) e = frame_after_pack(b, d, r, width, height, false, &launches, b->stream);
     record(d, 2, b->stream);
-    if (e == cudaSuccess) e = d2h(rgba, d->d_rgba, 4 * n, b->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess) e = d2h_staged(d, rgba, d->d_rgba, 4 * n, b->stream);
     if (fail(b, e, "denoise and tonemap")) return IX_DECLINED;
     d->pending = false;
     d->timing = ix_display_timing{0.0f, elapsed(d, 0, 1), elapsed(d, 1, 2), r.identity ? 0u : r.passes, launches};
@@ -469,7 +601,7 @@ static int display_frame_impl(ix_backend* b, const ix_scene* scene, uint32_t wit
         // module docs): computed once per pose, reused for every frame of it.
         e = h2d(d->d_planes, sc.planes, 16 * (size_t)sc.n_planes, st);
         GuideLaunch G{sc.camera, sc.width, sc.height, reinterpret_cast<const float4*>(d->d_planes), sc.n_planes, n_d,
-                      nullptr, nullptr, nullptr, nullptr, d->d_nd, d->d_fs};
+                      nullptr, nullptr, nullptr, nullptr, d->d_nrm, d->d_fs};
         if (e == cudaSuccess) e = launch_guides_exact(G, st);
         ++launches;
         d->cached = e == cudaSuccess;
@@ -478,7 +610,7 @@ static int display_frame_impl(ix_backend* b, const ix_scene* scene, uint32_t wit
     record(d, 1, st);
     const float* src = accum_dev;
     if (!src) {
-        if (e == cudaSuccess) e = h2d(d->d_xyz, accum_host, 12 * n, st);
+        if (e == cudaSuccess) e = h2d_staged(d, d->d_xyz, accum_host, 12 * n, st);
         src = d->d_xyz;
     }
     record(d, 2, st);
@@ -490,19 +622,18 @@ static int display_frame_impl(ix_backend* b, const ix_scene* scene, uint32_t wit
         ++launches;
     } else {
         const float inv = 1.0f / (float)spp;
-        PackLaunch P{n, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, src, inv, d->d_col[0]};
+        PackLaunch P{n, nullptr, nullptr, nullptr, nullptr, d->d_nrm, nullptr, src, inv, d->d_col[0]};
         if (e == cudaSuccess) e = launch_pack_exact(P, st);
         ++launches;
         uchar4* out = rgba_dev ? reinterpret_cast<uchar4*>(rgba_dev) : d->d_rgba;
         uchar4* keep = d->d_rgba;
         d->d_rgba = out;
-        if (e == cudaSuccess) e = frame_after_pack(b, d, r, sc.width, sc.height, &launches, st);
+        if (e == cudaSuccess) e = frame_after_pack(b, d, r, sc.width, sc.height, true, &launches, st);
         d->d_rgba = keep;
     }
     record(d, 3, st);
-    if (rgba_host && e == cudaSuccess) e = d2h(rgba_host, d->d_rgba, 4 * n, st);
     // The host form waits for its RGBA8; the device form stays asynchronous on `st`.
-    if (e == cudaSuccess && rgba_host) e = cudaStreamSynchronize(st);
+    if (rgba_host && e == cudaSuccess) e = d2h_staged(d, rgba_host, d->d_rgba, 4 * n, st);
     if (fail(b, e, "display frame")) {
         d->cached = false;
         return IX_DECLINED;

@@ -23,20 +23,21 @@ struct GuideLaunch {
     float* normal;
     int32_t* facet;
     uint32_t* sig;
-    // The A-Trous passes' packed guides: unit normal + sanitised depth, (facet, sig).
-    float4* nd;
+    // The A-Trous passes' packed guides: unit normal (w: sanitised depth), (facet, sig).
+    float4* nrm;
     int2* fs;
 };
 
-// Guides given in the reference layout -> the packed form; colour (3 floats per pixel)
-// times `scale` -> float4.  Either half may be skipped (null pointers).
+// Guides given in the reference layout (depth non-null) -> the packed form, or already
+// packed by the guide pass (depth null: nrm is read for the depth); colour (3 floats per
+// pixel) times `scale` -> float4 {x, y, z, sanitised depth} when color_out is non-null.
 struct PackLaunch {
     uint64_t pixels;
     const float* depth;
     const float* normal;
     const int32_t* facet;
     const uint32_t* sig;   // null: no signature (0 everywhere)
-    float4* nd;
+    float4* nrm;
     int2* fs;
     const float* color;    // 3 floats per pixel
     float scale;
@@ -47,9 +48,10 @@ struct PackLaunch {
 struct PassLaunch {
     uint32_t width, height;
     int stride;
-    const float4* src;
-    const float4* nd;
+    const float4* src;     // {x, y, z, sanitised depth}
+    const float4* nrm;     // unit normal
     const int2* fs;
+    int facet_normals;     // the normal is a function of the facet id (guide-pass guides)
     float neg_inv_sigma_depth;
     float neg_inv_two_sigma_color_sq;
     float normal_power;    // max(power, 0)

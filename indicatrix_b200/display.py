@@ -208,15 +208,20 @@ def denoise_and_tonemap_frame(backend: GpuBackend, frame: FirstHitSnapshot,
 
 
 def display_frame(backend: GpuBackend, scene: FrameScene, spp: int, accum: np.ndarray, with_signature: bool = False,
-                  params: Optional[AtrousParams] = None) -> Optional[np.ndarray]:
+                  params: Optional[AtrousParams] = None, out: Optional[np.ndarray] = None) -> Optional[np.ndarray]:
     """The whole display step of one accumulated frame on the device: guides of `scene`
     (cached per pose), average, denoise, tone-map.  `accum` is the frame's XYZ sums (the
-    f64 sums of try_accumulate are rounded to f32, the reference's accumulation type)."""
+    f64 sums of try_accumulate are rounded to f32, the reference's accumulation type).
+    `out` (uint8 [height, width, 4], contiguous) is written in place when given, like the
+    reference's `_into` forms; else a new array is returned."""
     if not backend.available:
         return None
     params = params if params is not None else AtrousParams.default()
     accum = _f32(accum, (scene.width * scene.height, 3))
-    out = np.zeros((scene.height, scene.width, 4), np.uint8)
+    if out is None:
+        out = np.zeros((scene.height, scene.width, 4), np.uint8)
+    elif out.dtype != np.uint8 or out.size != 4 * scene.width * scene.height or not out.flags.c_contiguous:
+        raise ValueError("out must be a contiguous uint8 buffer of width * height * 4")
     sc = scene.to_abi()
     rc = _lib().ix_display_frame(backend._h, C.byref(sc), 1 if with_signature else 0, spp, _p(accum, C.c_float),
                                  C.byref(params), _p(out, C.c_uint8))

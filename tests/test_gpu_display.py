@@ -70,6 +70,21 @@ def test_tonemap_matches_oracle_fast(backend, oracle):
         assert diff.max() <= FAST_MAX_LEVELS and np.mean(diff == 0) >= 0.9999, (space, diff.max(), np.mean(diff == 0))
 
 
+def test_tonemap_matches_oracle_exact(exact_backend, oracle):
+    """Exact build: every gamut walk takes the oracle's step (the analytic bounds of the
+    walk skip only steps that cannot pass), so a channel can differ only where pow rounds
+    differently: by 1 level at most, on almost none."""
+    rng = np.random.default_rng(11)
+    colors = (rng.random((257, 311, 3), np.float32) * np.float32(3.0)).astype(np.float32)
+    colors[::7, ::5] *= np.float32(40.0)
+    colors[::11, ::3, 1] *= np.float32(0.01)  # far out of gamut: long walks
+    for space in sorted(TONEMAP_PINS):
+        want = oracle.tonemap_to_rgba(colors, 1.0, space)
+        got = display.tonemap_accumulation(exact_backend, 311, 257, 1, colors, space)
+        diff = np.abs(got.astype(int) - want.astype(int))
+        assert diff.max() <= 1 and np.mean(diff == 0) >= 0.99999, (space, diff.max(), np.mean(diff == 0))
+
+
 def test_denoised_frame_pin_on_device(exact_backend, oracle):
     """The reference's pinned pipeline (frame_denoise.rs:232) on the device, through the
     guides-given entry and through the one-call display frame."""
