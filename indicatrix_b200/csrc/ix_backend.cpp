@@ -423,6 +423,7 @@ void ix_backend_destroy(ix_backend* b) {
     cudaFree(b->d_batch_out);
     cudaFree(b->d_finishes);
     display_state_free(b->display);
+    radiance_state_free(b->radiance);
     if (b->h_attr_map) cudaFreeHost(b->h_attr_map);
     if (b->h_sums) cudaFreeHost(b->h_sums);
     if (b->ev0) cudaEventDestroy(b->ev0);

@@ -15,6 +15,8 @@
 
 struct DisplayState;  // the display pipeline's pooled buffers (ix_display_host.cpp)
 void display_state_free(DisplayState* d);
+struct RadianceState;  // the radiance codec's device and pinned buffers (ix_radiance.cpp)
+void radiance_state_free(RadianceState* r);
 
 struct ix_backend {
     int device = 0;
@@ -72,6 +74,8 @@ struct ix_backend {
     uint64_t next_ticket = 0, serving = 0;
     // Guide buffers, colour ping-pong and output of the display pipeline.
     DisplayState* display = nullptr;
+    // Payload bytes of the radiance codec's device forms.
+    RadianceState* radiance = nullptr;
 };
 
 namespace ixh {
