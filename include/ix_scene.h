@@ -84,7 +84,9 @@ typedef struct ix_material {
     ix_absorption abs_e;                /* extraordinary absorption                   */
     float absorption_path_scale;        /* path length units per model unit           */
     float edge_rounding_radius;         /* 0 = sharp facet edges                      */
-    float scattering_sigma_s;           /* interior scattering; 0 on the CUDA path     */
+    float scattering_sigma_s;           /* Henyey-Greenstein interior scattering: sigma_s  */
+                                        /* per model unit (0 = clear)                     */
+    float scattering_g;                 /* HG asymmetry, -1 < g < 1                        */
 } ix_material;
 
 /* Lighting model ids: the reference's LightingModel::gpu_id for the two it shares

@@ -75,6 +75,7 @@ class Material(C.Structure):
         ("absorption_path_scale", C.c_float),
         ("edge_rounding_radius", C.c_float),
         ("scattering_sigma_s", C.c_float),
+        ("scattering_g", C.c_float),
     ]
 
 

@@ -456,7 +456,7 @@ int ix_scene_routes_to_gpu(const ix_scene* s) {
     if (s->n_planes > IX_MAX_PLANES || (s->n_planes && !s->planes)) return 0;
     if (s->width == 0 || s->height == 0) return 0;
     const ix_material& m = s->material;
-    if (m.scattering_sigma_s > 0.0f || m.edge_rounding_radius > 0.0f) return 0;
+    if (m.edge_rounding_radius > 0.0f) return 0;
     if (m.has_e_dispersion && m.e_dispersion.kind > IX_DISP_CAUCHY) return 0;
     const ix_environment& e = s->environment;
     if (e.model != IX_ENV_STUDIO && e.model != IX_ENV_ISO_HEMISPHERE && e.model != IX_ENV_UNIFORM) return 0;
@@ -483,6 +483,8 @@ int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metr
     // MAX_DIAGNOSTIC_PIXELS pixels accepts no sample; the frame is still traced.
     if (!attribution || n_pixels > IX_ATTRIBUTION_MAX_PIXELS)
         return accumulate_impl<double>(b, scene, sample_offset, spp, accum_xyz, cancel);
+    // The recorder does not follow interior scattering events (PathEvents::scatter).
+    if (scene->material.scattering_sigma_s > 0.0f) return IX_DECLINED;
     if (b->lost) return IX_DECLINED;
     if (!ix_scene_routes_to_gpu(scene)) return IX_DECLINED;
     if (b->limits.max_pixels && n_pixels > b->limits.max_pixels) return IX_DECLINED;

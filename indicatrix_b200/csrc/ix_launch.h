@@ -16,6 +16,7 @@ enum : uint32_t {
     SCENE_ABSORBING = 1u,   // the o-ray or e-ray absorption has a non-zero term
     SCENE_UNIAXIAL = 2u,    // uniaxial birefringence (ix_material::anisotropic)
     SCENE_PLEOCHROIC = 4u,  // the o-ray and e-ray absorption differ
+    SCENE_SCATTERING = 8u,  // Henyey-Greenstein interior scattering (scattering_sigma_s > 0)
 };
 inline bool absorption_present(const ix_absorption& a) {
     if (a.has_spline) return true;
@@ -40,11 +41,14 @@ inline uint32_t scene_flags(const ix_material& m) {
     if (absorption_present(m.abs_o) || absorption_present(m.abs_e)) f |= SCENE_ABSORBING;
     if (m.anisotropic) f |= SCENE_UNIAXIAL;
     if (!absorption_equal(m.abs_o, m.abs_e)) f |= SCENE_PLEOCHROIC;
+    if (m.scattering_sigma_s > 0.0f) f |= SCENE_SCATTERING;
     return f;
 }
 // The isotropic megakernel assumes equal o/e absorption and no birefringence; any other
 // scene runs the uniaxial instantiation of the transport.
-inline bool needs_uniaxial_kernel(uint32_t flags) { return (flags & (SCENE_UNIAXIAL | SCENE_PLEOCHROIC)) != 0; }
+inline bool needs_uniaxial_kernel(uint32_t flags) {
+    return (flags & (SCENE_UNIAXIAL | SCENE_PLEOCHROIC | SCENE_SCATTERING)) != 0;
+}
 
 // One frame-tracing launch over the pixels [pixel_begin, pixel_begin + n_pixels).
 struct TraceLaunch {

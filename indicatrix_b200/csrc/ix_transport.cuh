@@ -31,11 +31,13 @@ constexpr float R_UNPOL_SELECT_MAX = 0.98f;              // refraction/mod.rs:15
 // pointing at device memory, plus per-scene flags resolved on the host.
 struct DevScene {
     const ix_scene& s;
-    uint32_t absorbing;  // the material has any absorption term
-    uint32_t aniso;      // uniaxial birefringence
+    uint32_t absorbing;   // the material has any absorption term
+    uint32_t aniso;       // uniaxial birefringence
+    uint32_t scattering;  // Henyey-Greenstein interior scattering (uniaxial instantiation)
 };
 IX_DEV DevScene make_scene(const ix_scene& s, uint32_t flags) {
-    return DevScene{s, (flags & SCENE_ABSORBING) ? 1u : 0u, (flags & SCENE_UNIAXIAL) ? 1u : 0u};
+    return DevScene{s, (flags & SCENE_ABSORBING) ? 1u : 0u, (flags & SCENE_UNIAXIAL) ? 1u : 0u,
+                    (flags & SCENE_SCATTERING) ? 1u : 0u};
 }
 
 // The 8 lanes of one path: `mask` selects them in the warp, `c` is this lane's channel.
@@ -434,6 +436,84 @@ IX_DEV void lane_frosted_apply(LanePath& P, const FrostedScatter& f) {
     P.st = Stokes{intensity(P.st), 0.0f, 0.0f, 0.0f};
 }
 
+// ------------------------------------------------------------------------------------
+// Henyey-Greenstein interior scattering: try_scatter_step (scattering/hg.rs:256-340) with
+// maybe_scatter_or_extinguish (:21-84) and sample_henyey_greenstein_direction (:390),
+// without next-event estimation (no light-sampling technique in the modelled
+// environments) or zoning.  Runs in the uniaxial instantiation of the transport (which
+// also traces isotropic materials), so the isotropic one carries none of it.
+// ------------------------------------------------------------------------------------
+constexpr uint32_t DISTANCE_SAMPLE_STREAM = 0xA24BAED4u;  // sampling.rs:28
+constexpr uint32_t PHASE_DIR_U_STREAM = 0x9FB21C65u;      // sampling.rs:31
+constexpr uint32_t PHASE_DIR_V_STREAM = 0x1CE4E5B9u;      // sampling.rs:32
+IX_DEV float log_scatter(float x) {
+#if IX_EXACT
+    return (float)log((double)x);
+#else
+    return logf(x);
+#endif
+}
+struct ScatterResult {
+    float st_factor;  // scattered: the channel's new (unpolarised) intensity; else survival ratio
+    float pdf_factor;
+    V3 dir;           // scattered: the HG direction about the old one
+    float t_model;    // scattered: distance to the event in model units
+    int scattered;
+};
+// One channel of the segment's free-flight draw (the hero's extinction decides, through
+// lane 0 of the group; every lane takes the same branch).  Out of line and by value, like
+// frosted_scatter, so the bounce around the call compiles as it does without it.
+static __device__ __noinline__ ScatterResult scatter_or_survive(Group g, uint32_t seed, uint32_t bounce, float alpha,
+                                                                float sigma_s_model, float path_scale, float g_hg,
+                                                                float hit_t, float intensity_now, V3 forward) {
+    ScatterResult r;
+    const float sigma_s = sigma_s_model / path_scale;
+    const float sigma_t = alpha + sigma_s;
+    const float sigma_t_hero = gshfl(g, sigma_t, 0);
+    const float dist_rand = unit_draw(seed, bounce, DISTANCE_SAMPLE_STREAM);
+    const float one_minus_u = fmaxf(1.0f - dist_rand, 1e-7f);
+    const float t_free = -log_scatter(one_minus_u) / sigma_t_hero;
+    const float hit_scaled = hit_t * path_scale;
+    if (t_free < hit_scaled) {
+        const float pdf_hero = sigma_t_hero * one_minus_u;
+        const float tr = exp_lane(-sigma_t * t_free);
+        r.st_factor = intensity_now * (tr * sigma_s / pdf_hero);
+        r.pdf_factor = sigma_t * tr;
+        // sample_henyey_greenstein_direction: cos theta from u1, the azimuth (2 pi) u2
+        // about the old direction in frosted_orthonormal_basis.
+        const float u1 = unit_draw(seed, bounce, PHASE_DIR_U_STREAM);
+        const float u2 = unit_draw(seed, bounce, PHASE_DIR_V_STREAM);
+        float cos_theta;
+        if (fabsf(g_hg) < 1e-3f) {
+            cos_theta = fmaf(2.0f, -u1, 1.0f);
+        } else {
+            const float one_minus_g2 = fmaf(g_hg, -g_hg, 1.0f);
+            const float denom = fmaf(2.0f * g_hg, u1, 1.0f - g_hg);
+            const float sq = one_minus_g2 / denom;
+            cos_theta = fmaf(sq, -sq, fmaf(g_hg, g_hg, 1.0f)) / (2.0f * g_hg);
+        }
+        cos_theta = clampf_(cos_theta, -1.0f, 1.0f);
+        const float sin_theta = sqrtf(fmaxf(fmaf(cos_theta, -cos_theta, 1.0f), 0.0f));
+        float sin_p, cos_p;
+        sincosf((2.0f * 3.14159265358979323846f) * u2, &sin_p, &cos_p);
+        const V3 a = fabsf(forward.x) > 0.9f ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
+        const V3 t = normalize_or_zero(a - forward * dot(forward, a));
+        const V3 b = cross(forward, t);
+        r.dir = normalize_or_zero((t * (sin_theta * cos_p) + b * (sin_theta * sin_p)) + forward * cos_theta);
+        r.t_model = t_free / path_scale;
+        r.scattered = 1;
+        return r;
+    }
+    const float survive = exp_lane(-sigma_t * hit_scaled);
+    const float survive_hero = gshfl(g, survive, 0);
+    r.st_factor = survive / fmaxf(survive_hero, 1e-30f);
+    r.pdf_factor = survive;
+    r.dir = forward;
+    r.t_model = 0.0f;
+    r.scattered = 0;
+    return r;
+}
+
 // One iteration of the bounce loop (bounce_body.rs:361-423 and facet_event :611-707).
 // On BOUNCE_ESCAPED `esc` is this channel's escape radiance already weighted by its
 // Stokes intensity (accumulate_miss_radiance, transport/bounce.rs:40).
@@ -601,13 +681,51 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
         esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         return BOUNCE_ESCAPED;
     }
+    const V3 c_axis = load3(mat.c_axis);
+    const bool aniso = S.aniso != 0;
+    // The channel's alpha along the wave normal: the assigned eigenmode's field for a
+    // crystal, the mean over both eigen-polarisations otherwise (absorption.rs:99-197).
+    auto channel_alpha = [&](V3 k) {
+        if (aniso) {
+            const V3 e = assigned_mode_e_field(k, c_axis, P.is_e, P.n_hero, P.n_e_hero);
+            return absorption_quadratic_form(c_axis, P.alpha, P.alpha_e, e);
+        }
+        const V3 ea = ordinary_eigen_polarization(k, c_axis);
+        const V3 eb = normalize_or_zero(cross(k, ea));
+        return midpointf_(absorption_quadratic_form(c_axis, P.alpha, P.alpha_e, ea),
+                          absorption_quadratic_form(c_axis, P.alpha, P.alpha_e, eb));
+    };
+    if (S.scattering && P.inside) {
+        // The interior segment may end in a scattering event first (bounce_body.rs:408-417).
+        const ScatterResult r = scatter_or_survive(g, P.seed, bounce, S.absorbing ? channel_alpha(P.k) : 0.0f,
+                                                   mat.scattering_sigma_s, mat.absorption_path_scale,
+                                                   mat.scattering_g, hit.t, intensity(P.st), P.d);
+        P.pdf = P.pdf * r.pdf_factor;
+        if (r.scattered) {
+            P.st = Stokes{r.st_factor, 0.0f, 0.0f, 0.0f};
+            P.o = P.o + r.t_model * P.d;
+            P.d = r.dir;
+            P.k = r.dir;
+            P.has_prev = false;  // depolarised: no plane of incidence to rotate from
+            if (bounce > 4) {
+                float max_i = intensity(P.st);
+#pragma unroll
+                for (int mm = 4; mm > 0; mm >>= 1) max_i = fmaxf(max_i, gxor(g, max_i, mm));
+                const float q = clampf_(fmaxf(0.0f, max_i), 0.05f, 1.0f);
+                if (unit_draw(P.seed, bounce, RUSSIAN_ROULETTE_STREAM) > q) return BOUNCE_KILLED;
+                P.st = scale(P.st, 1.0f / q);
+                P.split = P.split / q;
+            }
+            P.bounce = bounce + 1;
+            return BOUNCE_CONTINUE;
+        }
+        P.st = scale(P.st, r.st_factor);
+    }
     P.facet = hit.facet;
     const float4 pl = planes[hit.facet];
     V3 normal = v3(pl.x, pl.y, pl.z);
     const V3 hit_point = P.o + hit.t * P.d;
     const V3 k_hat = P.k;
-    const V3 c_axis = load3(mat.c_axis);
-    const bool aniso = S.aniso != 0;
 
     // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:69), about k.
     const V3 cpn = normalize_or_zero(cross(k_hat, normal));
@@ -626,17 +744,8 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     // mean over both eigen-polarisations otherwise.
     if (P.inside) {
         normal = -normal;
-        if (S.absorbing) {
-            float alpha;
-            if (aniso) {
-                const V3 e = assigned_mode_e_field(k_hat, c_axis, P.is_e, P.n_hero, P.n_e_hero);
-                alpha = absorption_quadratic_form(c_axis, P.alpha, P.alpha_e, e);
-            } else {
-                const V3 ea = ordinary_eigen_polarization(k_hat, c_axis);
-                const V3 eb = normalize_or_zero(cross(k_hat, ea));
-                alpha = midpointf_(absorption_quadratic_form(c_axis, P.alpha, P.alpha_e, ea),
-                                   absorption_quadratic_form(c_axis, P.alpha, P.alpha_e, eb));
-            }
+        if (S.absorbing && !S.scattering) {
+            const float alpha = channel_alpha(k_hat);
             P.st = scale(P.st, exp_lane(-alpha * (hit.t * mat.absorption_path_scale)));
         }
     }

@@ -19,6 +19,15 @@ def _base(dispersion: abi.Dispersion) -> abi.Material:
     m.absorption_path_scale = 1.0
     m.edge_rounding_radius = 0.0
     m.scattering_sigma_s = 0.0
+    m.scattering_g = 0.0
+    return m
+
+
+def with_scattering(m: abi.Material, sigma_s: float, g: float) -> abi.Material:
+    """GemMaterial::with_scattering: Henyey-Greenstein interior scattering, sigma_s per
+    model unit and asymmetry g (optics/materials/mod.rs)."""
+    m.scattering_sigma_s = float(sigma_s)
+    m.scattering_g = float(g)
     return m
 
 

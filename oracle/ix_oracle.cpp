@@ -68,6 +68,7 @@ static inline F atan_(F a) { g_cnt.transc++; return F(atanf(a.v)); }
 static inline F atan2_(F a, F b) { g_cnt.transc++; return F(atan2f(a.v, b.v)); }
 static inline F acos_(F a) { g_cnt.transc++; return F(acosf(a.v)); }
 static inline F exp_(F a) { g_cnt.transc++; return F(expf(a.v)); }
+static inline F ln_(F a) { g_cnt.transc++; return F(logf(a.v)); }
 static inline F midpoint_(F a, F b) {
     g_cnt.add++; g_cnt.mul++;
     return F((float)(((double)a.v + (double)b.v) / 2.0));
@@ -84,6 +85,7 @@ static inline F atan_(F a) { return atanf(a); }
 static inline F atan2_(F a, F b) { return atan2f(a, b); }
 static inline F acos_(F a) { return acosf(a); }
 static inline F exp_(F a) { return expf(a); }
+static inline F ln_(F a) { return logf(a); }
 // f32::midpoint on x86_64: ((a as f64 + b as f64) / 2.0) as f32.
 static inline F midpoint_(F a, F b) { return (float)(((double)a + (double)b) / 2.0); }
 #endif
@@ -1692,10 +1694,10 @@ static void apply_frosted_bounce(Path& P, const Geo& g, V3 normal, uint32_t boun
     o->new_inside = !P.inside;
 }
 
-static void apply_absorption(Path& P, F path_len) {
-    const ix_material& m = P.sc->material;
+// channel_absorption_alphas_assigned (raytracer/absorption.rs): each channel's alpha
+// along the current wave normal, for the assigned mode of a uniaxial material.
+static void channel_alphas(const Path& P, F alpha[8]) {
     TensorFrame tf = tensor_frame(P.c_axis);
-    F alpha[8];
     if (!P.aniso) {
         V3 ea = ordinary_eigen_polarization(P.k, P.c_axis);
         V3 eb = normalize_or_zero(cross(P.k, ea));
@@ -1706,11 +1708,103 @@ static void apply_absorption(Path& P, F path_len) {
         V3 e_mode = assigned_mode_e_field_uniaxial(P.k, P.c_axis, P.is_e, P.n_ch[0], P.n_e_at[0]);
         for (int c = 0; c < 8; ++c) alpha[c] = quadratic_form(tf, P.alpha_ch_o[c], P.alpha_ch_e[c], e_mode);
     }
+}
+static void apply_absorption(Path& P, F path_len) {
+    const ix_material& m = P.sc->material;
+    F alpha[8];
+    channel_alphas(P, alpha);
     F scaled_len = path_len * F(m.absorption_path_scale);
     for (int c = 0; c < 8; ++c) P.stokes[c] = scale(P.stokes[c], exp_lane(-alpha[c] * scaled_len));
 }
 
 enum { TERM_ESCAPED = 0, TERM_RR = 1, TERM_CAP = 2 };
+
+// apply_russian_roulette (transport/bounce.rs:355): false when the path is killed.
+static bool russian_roulette(Path& P, uint32_t bounce) {
+    F max_i = 0.0f;
+    for (int c = 0; c < 8; ++c) max_i = max_(max_i, intensity(P.stokes[c]));
+    F q = clamp_(max_i, 0.05f, 1.0f);
+    F rr = unit_draw(P.seed, bounce, RUSSIAN_ROULETTE_STREAM);
+    if (rr > q) return false;
+    for (int c = 0; c < 8; ++c) P.stokes[c] = scale(P.stokes[c], F(1.0f) / q);
+    for (int c = 0; c < 8; ++c) P.split[c] = P.split[c] / q;
+    return true;
+}
+
+// Henyey-Greenstein interior scattering (optics/raytracer/scattering/hg.rs).
+static const uint32_t DISTANCE_SAMPLE_STREAM = 0xA24BAED4u;  // sampling.rs:28
+static const uint32_t PHASE_DIR_U_STREAM = 0x9FB21C65u;      // sampling.rs:31
+static const uint32_t PHASE_DIR_V_STREAM = 0x1CE4E5B9u;      // sampling.rs:32
+// sample_henyey_greenstein_direction (hg.rs:390).
+static V3 sample_hg_direction(F u1, F u2, F g, V3 forward) {
+    F cos_theta;
+    if (abs_(g) < F(1e-3f)) {
+        cos_theta = fma_(2.0f, -u1, 1.0f);
+    } else {
+        F one_minus_g2 = fma_(g, -g, 1.0f);
+        F denom = fma_(F(2.0f) * g, u1, F(1.0f) - g);
+        F sq = one_minus_g2 / denom;
+        cos_theta = fma_(sq, -sq, fma_(g, g, 1.0f)) / (F(2.0f) * g);
+    }
+    cos_theta = clamp_(cos_theta, -1.0f, 1.0f);
+    F sin_theta = sqrt_(max_(fma_(cos_theta, -cos_theta, 1.0f), 0.0f));
+    F phi = F(2.0f * 3.14159265358979323846f) * u2;
+    F sin_p = sin_(phi), cos_p = cos_(phi);
+    V3 t, b;
+    frosted_orthonormal_basis(forward, &t, &b);
+    return normalize_or_zero((t * (sin_theta * cos_p) + b * (sin_theta * sin_p)) + forward * cos_theta);
+}
+enum { SCATTER_NONE = 0, SCATTER_SURVIVED = 1, SCATTER_KILLED = 2 };
+// try_scatter_step (hg.rs:256-340) with maybe_scatter_or_extinguish (hg.rs:21-84), without
+// next-event estimation (no light-sampling technique in the modelled environments) and
+// without zoning: a free flight drawn with the hero's extinction either scatters inside
+// the segment -- each channel reweighted by its transmittance, depolarised, the HG lobe
+// about the old direction, roulette after bounce 4 -- or reaches the facet with every
+// channel's survival relative to the hero's.
+static int scatter_step(Path& P, F hit_t, uint32_t bounce) {
+    const ix_material& m = P.sc->material;
+    F alpha[8];
+    if (P.absorbing) {
+        channel_alphas(P, alpha);
+    } else {
+        for (int c = 0; c < 8; ++c) alpha[c] = 0.0f;
+    }
+    const F path_scale = m.absorption_path_scale;
+    const F sigma_s = F(m.scattering_sigma_s) / path_scale;
+    const F sigma_t_hero = alpha[0] + sigma_s;
+    const F dist_rand = unit_draw(P.seed, bounce, DISTANCE_SAMPLE_STREAM);
+    const F one_minus_u = max_(F(1.0f) - dist_rand, 1e-7f);
+    const F t_free = -ln_(one_minus_u) / sigma_t_hero;
+    const F hit_scaled = hit_t * path_scale;
+    if (t_free < hit_scaled) {
+        const F pdf_hero = sigma_t_hero * one_minus_u;
+        for (int c = 0; c < 8; ++c) {
+            const F sigma_t = alpha[c] + sigma_s;
+            const F tr = exp_lane(-(alpha[c] + sigma_s) * t_free);
+            const F weight = tr * sigma_s / pdf_hero;
+            P.stokes[c] = unpolarized(intensity(P.stokes[c]) * weight);
+            P.path_pdf[c] = P.path_pdf[c] * (sigma_t * tr);
+        }
+        const F u1 = unit_draw(P.seed, bounce, PHASE_DIR_U_STREAM);
+        const F u2 = unit_draw(P.seed, bounce, PHASE_DIR_V_STREAM);
+        const V3 old_dir = P.ray.dir;
+        const V3 new_dir = sample_hg_direction(u1, u2, F(m.scattering_g), old_dir);
+        const F t_model = t_free / path_scale;
+        P.ray = Ray{P.ray.origin + t_model * old_dir, new_dir};
+        P.k = new_dir;
+        P.has_prev = false;  // depolarised: no plane of incidence to rotate from
+        if (bounce > 4 && !russian_roulette(P, bounce)) return SCATTER_KILLED;
+        return SCATTER_SURVIVED;
+    }
+    F survive[8];
+    for (int c = 0; c < 8; ++c) survive[c] = exp_lane(-(alpha[c] + sigma_s) * hit_scaled);
+    const F survive_hero = survive[0];
+    for (int c = 0; c < 8; ++c) {
+        P.stokes[c] = scale(P.stokes[c], survive[c] / max_(survive_hero, 1e-30f));
+        P.path_pdf[c] = P.path_pdf[c] * survive[c];
+    }
+    return SCATTER_NONE;
+}
 
 // PathEvents::facet (transport/path_events.rs:55-79): the first facet event, the first
 // inside-to-outside transition, internal events before it and a re-entry after it.
@@ -1788,6 +1882,15 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
             }
             break;
         }
+        // The interior segment may end in a scattering event first (bounce_body.rs:408-417).
+        if (P.inside && m.scattering_sigma_s > 0.0f) {
+            const int sc_out = scatter_step(P, hit.t, bounce);
+            if (sc_out == SCATTER_KILLED) {
+                term = TERM_RR;
+                break;
+            }
+            if (sc_out == SCATTER_SURVIVED) continue;
+        }
         // facet_event (bounce_body.rs:611).
         V3 hit_point = P.ray.origin + hit.t * P.ray.dir;
         V3 normal = shading_normal_near_edge(sc->planes, sc->n_planes, hit_point, hit.facet,
@@ -1856,17 +1959,9 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
             for (int c = 0; c < 8; ++c) P.stokes[c] = scale(P.stokes[c], glare);
         }
         // apply_russian_roulette (transport/bounce.rs:355).
-        if (bounce > 4) {
-            F max_i = 0.0f;
-            for (int c = 0; c < 8; ++c) max_i = max_(max_i, intensity(P.stokes[c]));
-            F q = clamp_(max_i, 0.05f, 1.0f);
-            F rr = unit_draw(P.seed, bounce, RUSSIAN_ROULETTE_STREAM);
-            if (rr > q) {
-                term = TERM_RR;
-                break;
-            }
-            for (int c = 0; c < 8; ++c) P.stokes[c] = scale(P.stokes[c], F(1.0f) / q);
-            for (int c = 0; c < 8; ++c) P.split[c] = P.split[c] / q;
+        if (bounce > 4 && !russian_roulette(P, bounce)) {
+            term = TERM_RR;
+            break;
         }
     }
     // finish (bounce_body.rs:724).
@@ -1907,7 +2002,6 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
 static bool scene_supported(const ix_scene* sc) {
     if (!sc) return false;
     if (sc->n_planes > 0 && !sc->planes) return false;
-    if (sc->material.scattering_sigma_s > 0.0f) return false;
     return true;
 }
 

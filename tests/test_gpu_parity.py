@@ -386,9 +386,9 @@ def test_f32_accumulate_adds_into(backend):
 def test_decline_and_cancel_leave_accum_untouched(backend):
     """gpu_backend/mod.rs:122-130: a decline or a cancel never writes the accumulator."""
     fs = small_scene(8, 8)
-    scattering = materials.diamond()
-    scattering.scattering_sigma_s = 0.5  # volume scattering does not route to the GPU
-    fs.material = scattering
+    rounded = materials.diamond()
+    rounded.edge_rounding_radius = 0.01  # rounded facet edges do not route to the GPU
+    fs.material = rounded
     acc = np.full((8, 8, 3), 7.0)
     assert backend.try_accumulate_cancellable(fs, 0, 4, acc) == GpuAccumulate.DECLINED
     assert np.all(acc == 7.0)
