@@ -456,7 +456,6 @@ int ix_scene_routes_to_gpu(const ix_scene* s) {
     if (s->n_planes > IX_MAX_PLANES || (s->n_planes && !s->planes)) return 0;
     if (s->width == 0 || s->height == 0) return 0;
     const ix_material& m = s->material;
-    if (m.edge_rounding_radius > 0.0f) return 0;
     if (m.has_e_dispersion && m.e_dispersion.kind > IX_DISP_CAUCHY) return 0;
     const ix_environment& e = s->environment;
     if (e.model != IX_ENV_STUDIO && e.model != IX_ENV_ISO_HEMISPHERE && e.model != IX_ENV_UNIFORM) return 0;

@@ -17,6 +17,7 @@ enum : uint32_t {
     SCENE_UNIAXIAL = 2u,    // uniaxial birefringence (ix_material::anisotropic)
     SCENE_PLEOCHROIC = 4u,  // the o-ray and e-ray absorption differ
     SCENE_SCATTERING = 8u,  // Henyey-Greenstein interior scattering (scattering_sigma_s > 0)
+    SCENE_ROUNDED = 16u,    // rounded facet edges (edge_rounding_radius > 0)
 };
 inline bool absorption_present(const ix_absorption& a) {
     if (a.has_spline) return true;
@@ -42,12 +43,13 @@ inline uint32_t scene_flags(const ix_material& m) {
     if (m.anisotropic) f |= SCENE_UNIAXIAL;
     if (!absorption_equal(m.abs_o, m.abs_e)) f |= SCENE_PLEOCHROIC;
     if (m.scattering_sigma_s > 0.0f) f |= SCENE_SCATTERING;
+    if (m.edge_rounding_radius > 0.0f) f |= SCENE_ROUNDED;
     return f;
 }
 // The isotropic megakernel assumes equal o/e absorption and no birefringence; any other
 // scene runs the uniaxial instantiation of the transport.
 inline bool needs_uniaxial_kernel(uint32_t flags) {
-    return (flags & (SCENE_UNIAXIAL | SCENE_PLEOCHROIC | SCENE_SCATTERING)) != 0;
+    return (flags & (SCENE_UNIAXIAL | SCENE_PLEOCHROIC | SCENE_SCATTERING | SCENE_ROUNDED)) != 0;
 }
 
 // One frame-tracing launch over the pixels [pixel_begin, pixel_begin + n_pixels).

@@ -34,10 +34,11 @@ struct DevScene {
     uint32_t absorbing;   // the material has any absorption term
     uint32_t aniso;       // uniaxial birefringence
     uint32_t scattering;  // Henyey-Greenstein interior scattering (uniaxial instantiation)
+    uint32_t rounded;     // rounded facet edges (uniaxial instantiation)
 };
 IX_DEV DevScene make_scene(const ix_scene& s, uint32_t flags) {
     return DevScene{s, (flags & SCENE_ABSORBING) ? 1u : 0u, (flags & SCENE_UNIAXIAL) ? 1u : 0u,
-                    (flags & SCENE_SCATTERING) ? 1u : 0u};
+                    (flags & SCENE_SCATTERING) ? 1u : 0u, (flags & SCENE_ROUNDED) ? 1u : 0u};
 }
 
 // The 8 lanes of one path: `mask` selects them in the warp, `c` is this lane's channel.
@@ -437,6 +438,44 @@ IX_DEV void lane_frosted_apply(LanePath& P, const FrostedScatter& f) {
 }
 
 // ------------------------------------------------------------------------------------
+// shading_normal_near_edge (optics/raytracer/intersect.rs:196): within
+// `edge_rounding_radius` of another facet's plane the shading normal blends, by a
+// smoothstep of the distance, toward the bisector with the nearest plane.  The 8 lanes of
+// the group scan the planes together; the nearest is the first of the minimal distance,
+// as the reference's strict `<` keeps.  Out of line: rounded stones only.
+// ------------------------------------------------------------------------------------
+static __device__ __noinline__ V3 group_shading_normal(Group g, const float4* __restrict__ planes, int n, V3 x,
+                                                       int facet, V3 hit_normal, float radius) {
+    float best = INFINITY;
+    int best_i = 0x7FFFFFFF;
+    for (int i = g.c; i < n; i += 8) {
+        if (i == facet) continue;
+        const float4 p = planes[i];
+        const float dist = -(p.w + ((p.x * x.x + p.y * x.y) + p.z * x.z));
+        if (dist < best) {
+            best = dist;
+            best_i = i;
+        }
+    }
+#pragma unroll
+    for (int m = 4; m > 0; m >>= 1) {
+        const float ob = gxor(g, best, m);
+        const int oi = gxor(g, best_i, m);
+        if (ob < best || (ob == best && oi < best_i)) {
+            best = ob;
+            best_i = oi;
+        }
+    }
+    if (!(best < radius) || best_i == 0x7FFFFFFF) return hit_normal;
+    const float4 q = planes[best_i];
+    const V3 nearest = v3(q.x, q.y, q.z);
+    const float t = clampf_(1.0f - best / radius, 0.0f, 1.0f);
+    const float smooth_t = t * t * fmaf(2.0f, -t, 3.0f);
+    const V3 bis = normalize_or_zero(hit_normal + nearest);
+    return normalize_or_zero(hit_normal * (1.0f - smooth_t) + bis * smooth_t);
+}
+
+// ------------------------------------------------------------------------------------
 // Henyey-Greenstein interior scattering: try_scatter_step (scattering/hg.rs:256-340) with
 // maybe_scatter_or_extinguish (:21-84) and sample_henyey_greenstein_direction (:390),
 // without next-event estimation (no light-sampling technique in the modelled
@@ -725,6 +764,9 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     const float4 pl = planes[hit.facet];
     V3 normal = v3(pl.x, pl.y, pl.z);
     const V3 hit_point = P.o + hit.t * P.d;
+    if (S.rounded)
+        normal = group_shading_normal(g, planes, (int)sc.n_planes, hit_point, hit.facet, normal,
+                                      mat.edge_rounding_radius);
     const V3 k_hat = P.k;
 
     // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:69), about k.

@@ -3180,4 +3180,9 @@ int ixo_count_denoise_flops(const float* color, const float* depth, const float*
 #endif
 }
 
+void ixo_shading_normal_near_edge(const float* planes, uint32_t n_planes, const float hit_point[3], int32_t facet,
+                                  const float hit_normal[3], float radius, float out[3]) {
+    store3(out, shading_normal_near_edge(planes, n_planes, load3(hit_point), facet, load3(hit_normal), F(radius)));
+}
+
 }  // extern "C"

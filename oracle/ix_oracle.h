@@ -161,6 +161,9 @@ int ixo_count_flops(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_
 /* The display pipeline after the path (renderer/guide_pass.rs, renderer/denoise/,
  * renderer/tonemap.rs, renderer/frame_denoise.rs); threads 0 = all host threads, the
  * results do not depend on it. */
+/* shading_normal_near_edge (optics/raytracer/intersect.rs:196). */
+void ixo_shading_normal_near_edge(const float* planes, uint32_t n_planes, const float hit_point[3], int32_t facet,
+                                  const float hit_normal[3], float radius, float out[3]);
 void ixo_atrous_params_default(ix_atrous_params* p);
 /* Counting build only: the operation tally of one A-Trous denoise (paths = pixel-passes). */
 int ixo_count_denoise_flops(const float* color, const float* depth, const float* normal, const int32_t* facet_id,

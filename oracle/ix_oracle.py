@@ -156,6 +156,7 @@ def _load(name: str) -> C.CDLL:
     lib.ixo_atrous_denoise.argtypes = [f32p, f32p, f32p, i32p, u32p, C.c_uint32, C.c_uint32, C.c_uint32,
                                        P(abi.AtrousParams), f32p, C.c_int]
     lib.ixo_color_encode.argtypes = [f32p, C.c_uint32, u8p]
+    lib.ixo_shading_normal_near_edge.argtypes = [f32p, C.c_uint32, f32p, C.c_int32, f32p, C.c_float, f32p]
     lib.ixo_count_denoise_flops.restype = C.c_int
     lib.ixo_count_denoise_flops.argtypes = [f32p, f32p, f32p, i32p, u32p, C.c_uint32, C.c_uint32, C.c_uint32,
                                             P(abi.AtrousParams), P(FlopCounts)]
@@ -477,4 +478,12 @@ def count_denoise_flops(color, depth, normal, facet, sig, spp: int, params=None)
         _ptr(sig, C.c_uint32), w, h, spp, C.byref(params), C.byref(out))
     if rc != 0:
         raise RuntimeError("the counting oracle build is required")
+    return out
+
+
+def shading_normal_near_edge(planes: np.ndarray, hit_point, facet: int, hit_normal, radius: float) -> np.ndarray:
+    planes = np.ascontiguousarray(planes, np.float32)
+    out = np.zeros(3, np.float32)
+    lib().ixo_shading_normal_near_edge(_f32p(planes), planes.shape[0], _f32p(np.asarray(hit_point, np.float32)),
+                                       facet, _f32p(np.asarray(hit_normal, np.float32)), radius, _f32p(out))
     return out

@@ -386,9 +386,9 @@ def test_f32_accumulate_adds_into(backend):
 def test_decline_and_cancel_leave_accum_untouched(backend):
     """gpu_backend/mod.rs:122-130: a decline or a cancel never writes the accumulator."""
     fs = small_scene(8, 8)
-    rounded = materials.diamond()
-    rounded.edge_rounding_radius = 0.01  # rounded facet edges do not route to the GPU
-    fs.material = rounded
+    unknown = materials.diamond()
+    unknown.dispersion.kind = 7  # a dispersion model this backend does not know declines
+    fs.material = unknown
     acc = np.full((8, 8, 3), 7.0)
     assert backend.try_accumulate_cancellable(fs, 0, 4, acc) == GpuAccumulate.DECLINED
     assert np.all(acc == 7.0)

@@ -95,13 +95,13 @@ def test_routing_predicate():
     m = materials.quartz()
     m.e_dispersion.kind = 7
     assert not scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, fs.planes, m, 32, fs.environment))
-    # Interior scattering routes (isotropic and uniaxial); rounded facet edges do not.
+    # Interior scattering (isotropic and uniaxial) and rounded facet edges route.
     for m in (materials.diamond(), materials.sapphire()):
         m = materials.with_scattering(m, 0.5, 0.3)
         assert scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, fs.planes, m, 32, fs.environment))
     m = materials.diamond()
     m.edge_rounding_radius = 0.01
-    assert not scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, fs.planes, m, 32, fs.environment))
+    assert scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, fs.planes, m, 32, fs.environment))
     # Frosted facets route (apply_frosted_bounce runs on the device).
     fin = np.zeros(fs.planes.shape[0], np.uint8)
     fin[70] = 1
