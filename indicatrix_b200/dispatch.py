@@ -164,3 +164,46 @@ def distributed_accumulate(trace: Callable[[int, int], np.ndarray], pixels: int,
         for first, done, sums in chunks:
             m.add(first, done, sums)
     return m.finish()
+
+
+def distributed_accumulate_payloads(trace: Callable[[int, int], np.ndarray], width: int, height: int, start: int,
+                                    end: int, chunk: int, encoding: int = 2,
+                                    key: str = "ix_payload_cursor") -> Optional[Tuple[np.ndarray, int, int]]:
+    """The lanes' wire form of `distributed_accumulate`: every chunk's per-pixel sums go
+    over the group as a radiance payload (Vec3 f32, byte-shuffled and LZ4-compressed when
+    that is smaller; indicatrix-net radiance/payload.rs), and rank 0 checks each frame's
+    sample range against the request -- a frame outside [start, end) or one that would
+    take the cumulative count past the range is refused (RadianceError FrameOutsideRange /
+    SampleCountOverrun, radiance/mod.rs:109-117) -- then decodes and adds the frames into
+    f32 sums in ascending first-sample order with the valid-sample rule.  Returns
+    (sums [pixels, 3] f32, samples, dropped pixels) on rank 0, None elsewhere."""
+    import torch.distributed as dist
+
+    from .radiance import PayloadDecoder, PayloadEncoder, RadianceError
+
+    store = dist.distributed_c10d._get_default_store()
+    enc = PayloadEncoder(encoding)
+    mine = []
+    while True:
+        c = store_claim(store, key, start, end, chunk)
+        if c is None:
+            break
+        sums = np.ascontiguousarray(trace(c[0], c[1]), np.float64).reshape(-1)
+        p = enc.encode(sums.astype(np.float32).tobytes())
+        mine.append((c[0], c[1], int(p.encoding), p.raw_len, p.bytes))
+    gathered: List = [None] * dist.get_world_size()
+    dist.all_gather_object(gathered, mine)
+    if dist.get_rank() != 0:
+        return None
+    frames = sorted((f for chunks in gathered for f in chunks), key=lambda f: f[0])
+    acc = np.zeros((width * height, 3), np.float32)
+    dec = PayloadDecoder()
+    cumulative, dropped = 0, 0
+    for first, done, encoding_used, raw_len, wire in frames:
+        if first < start or first + done > end:
+            raise RadianceError(9)
+        if cumulative + done > end - start:
+            raise RadianceError(10)
+        dropped += dec.decode_and_add(encoding_used, raw_len, wire, width, height, acc)
+        cumulative += done
+    return acc, cumulative, dropped

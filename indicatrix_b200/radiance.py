@@ -37,7 +37,8 @@ class RadianceError(Exception):
     """RadianceError (radiance/mod.rs:68): ``code`` is the C code, ``name`` the variant."""
 
     NAMES = {1: "LengthMismatch", 3: "TooLarge", 4: "RawLenMismatch", 5: "UnsupportedEncoding",
-             6: "DecompressFailed", 7: "ShortOutput", 8: "BufferTooSmall", 16: "Declined"}
+             6: "DecompressFailed", 7: "ShortOutput", 8: "BufferTooSmall", 9: "FrameOutsideRange",
+             10: "SampleCountOverrun", 16: "Declined"}
 
     def __init__(self, code: int) -> None:
         self.code = code

@@ -153,3 +153,59 @@ def test_two_rank_gloo_sample_sharding_merges_deterministically(oracle):
         _, s64, _ = oracle.trace_frame(sc, first, min(5, 23 - first), threads=1)
         want = want + s64.reshape(-1)
     assert np.array_equal(sums.view(np.uint64), want.view(np.uint64))
+
+
+def _rank_payload_main(rank, world, port, out_path):
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    sys.path.insert(0, os.path.join(root, "oracle"))
+    import datetime
+
+    import torch.distributed as dist
+
+    import ix_oracle
+    from indicatrix_b200 import workloads
+    from indicatrix_b200.dispatch import distributed_accumulate_payloads
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    fs = workloads.round_brilliant_frame(8, 6)
+    sc = fs.to_abi()
+
+    def trace(first, count):
+        _, s64, _ = ix_oracle.trace_frame(sc, first, count, threads=1)
+        return s64
+
+    res = distributed_accumulate_payloads(trace, 8, 6, 0, 23, 5)
+    if rank == 0:
+        with open(out_path, "wb") as f:
+            pickle.dump(res, f)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_gloo_lanes_exchange_radiance_payloads(oracle):
+    """The wire form: 2 gloo ranks send their chunks as radiance payloads (f32 Vec3,
+    shuffled + LZ4 where smaller) and rank 0 decodes and adds them in sample order: the
+    f32 sums equal a single process adding the same chunks' f32 frames in that order."""
+    import torch.multiprocessing as mp
+
+    from indicatrix_b200 import workloads
+
+    port = _free_port()
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "res.pkl")
+        mp.start_processes(_rank_payload_main, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+        with open(out, "rb") as f:
+            acc, n, dropped = pickle.load(f)
+    assert n == 23 and dropped == 0
+    fs = workloads.round_brilliant_frame(8, 6)  # kept alive: the scene points into its planes
+    sc = fs.to_abi()
+    want = np.zeros((48, 3), np.float32)
+    for first in range(0, 23, 5):
+        _, s64, _ = oracle.trace_frame(sc, first, min(5, 23 - first), threads=1)
+        want = (want + s64.reshape(-1, 3).astype(np.float32)).astype(np.float32)
+    assert want.sum() > 0
+    assert np.array_equal(acc.view(np.uint32), want.view(np.uint32))
