@@ -63,7 +63,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
                                          "-prec-sqrt=false", "-ftz=true"])):
             obj = os.path.join(BUILD_DIR, f"{unit}_{variant}.o")
             jobs.append((obj, common + flags + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj]))
-    for unit in ("ix_probe", "ix_noalloc", "ix_radiance"):
+    for unit in ("ix_probe", "ix_noalloc", "ix_radiance", "ix_surrogate"):
         obj = os.path.join(BUILD_DIR, unit + ".o")
         jobs.append((obj, common + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj]))
     procs = [(obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))

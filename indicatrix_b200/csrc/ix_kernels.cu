@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_c
 
 // The trace kernel with spectral attribution: the same task loop, and each path's
 // class code and luminance recorded for the fold.  Each CTA first derives the exit
-// lighting's threshold (96 radiances and their median), which the classes are judged by.
+// lighting's threshold (96 radiances and their median), which decides the classes.
 template <int MINB, bool UNI>
 __global__ void __launch_bounds__(128, MINB)
     IX_SFX(trace_attributed_kernel)(const __grid_constant__ TraceLaunch L, const __grid_constant__ AttrLaunch A) {

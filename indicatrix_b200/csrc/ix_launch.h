@@ -157,7 +157,7 @@ cudaError_t launch_metrics_exact(const MetricsLaunch& l, cudaStream_t stream);
 cudaError_t launch_metrics_fast(const MetricsLaunch& l, cudaStream_t stream);
 
 // Spectral attribution of a trace launch (classify_path, color/metrics/attribution.rs:75):
-// the exit lighting the classes are judged by, and where each sample's class code and
+// the exit lighting that decides the classes, and where each sample's class code and
 // luminance go -- [sample][pixel] over the launch's samples [0, spp) and pixels
 // [0, n_pixels), so the fold reads them coalesced.
 struct AttrLaunch {

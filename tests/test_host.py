@@ -22,7 +22,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = []
-    for h in ("ix_cuda.h", "ix_dispatch.h", "ix_display.h", "ix_radiance.h"):
+    for h in ("ix_cuda.h", "ix_dispatch.h", "ix_display.h", "ix_radiance.h", "ix_surrogate.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names += re.findall(r"\b(ix_[a-z0-9_]+)\s*\(", text)
