@@ -120,6 +120,10 @@ class SurrogateMLP:
             _ok(_lib().ix_mlp_to_bf16(w.numel(), w.data_ptr(), layer.wb.data_ptr(), self._stream()))
             self.layers.append(layer)
         self.step = 0
+        # Per-output standardisation of the targets (set by fit): the outputs differ in
+        # scale by orders of magnitude, and the loss weighs them equally once scaled.
+        self.t_mean = np.zeros(N_OUTPUTS, np.float32)
+        self.t_std = np.ones(N_OUTPUTS, np.float32)
 
     def _stream(self) -> int:
         return self.torch.cuda.current_stream().cuda_stream
@@ -156,7 +160,7 @@ class SurrogateMLP:
         torch = self.torch
         xt = torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(self.dev)
         _, out = self._forward(self._bf16(xt), x.shape[0])
-        return out.cpu().numpy()
+        return out.cpu().numpy() * self.t_std + self.t_mean
 
     def gradients(self, x: np.ndarray, t: np.ndarray):
         """Loss and the f32 gradients [(dW, db) per layer] of one batch (no update)."""
@@ -208,6 +212,9 @@ class SurrogateMLP:
     def fit(self, x: np.ndarray, t: np.ndarray, epochs: int = 200, batch: int = 256, lr: float = 2e-3,
             seed: int = 0) -> List[float]:
         rng = np.random.default_rng(seed)
+        self.t_mean = t.mean(axis=0).astype(np.float32)
+        self.t_std = np.maximum(t.std(axis=0), 1e-6).astype(np.float32)
+        t = ((t - self.t_mean) / self.t_std).astype(np.float32)
         losses = []
         for _ in range(epochs):
             order = rng.permutation(x.shape[0])
