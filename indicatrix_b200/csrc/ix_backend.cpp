@@ -34,13 +34,6 @@ using namespace ixh;
 
 namespace {
 
-bool material_has_absorption(const ix_absorption& a) {
-    if (a.has_spline) return true;
-    for (uint32_t i = 0; i < a.n_bands && i < IX_MAX_BANDS; ++i)
-        if (a.bands[i].peak != 0.0f) return true;
-    return false;
-}
-
 uint32_t pixels_per_task(uint32_t spp) {
     // About 64 paths per warp task (16 per 8-lane group), whole pixels, at most 8: small
     // tasks keep every warp busy to the end of a launch (a single frame at 256^2 x 64 spp
