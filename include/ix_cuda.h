@@ -17,7 +17,9 @@
  *   - a sample whose XYZ has a NaN/Inf component is dropped but still counted
  *     (optics/raytracer/sampling.rs:237).
  * Per-pixel sums are formed on the device in f64 and are bit-identical for any chunking
- * and any run.
+ * and any run.  (The path-pool kernels form them exactly, in fixed point, and round
+ * once; a sample with a component of 2^62 or more is dropped and counted as a non-finite
+ * one is.)
  */
 #ifndef IX_CUDA_H
 #define IX_CUDA_H
@@ -46,10 +48,14 @@ typedef struct ix_backend_options {
     int32_t device;              /* CUDA device ordinal                                  */
     uint32_t pipeline;           /* IX_PIPELINE_*                                        */
     uint32_t precision;          /* IX_PRECISION_*                                       */
-    uint32_t threads_per_block;  /* 0 = autotuned                                        */
+    uint32_t threads_per_block;  /* CTA size of batch plans: 0 = any (autotuned), or 64,  */
+                                 /* 128 or 256 (the path-pool loop at that size); any     */
+                                 /* other value makes ix_backend_create return NULL       */
     uint64_t chunk_paths;        /* paths per launch; 0 = default (2^26)                   */
-    uint32_t kernel_variant;     /* register budget of the megakernel: 0 default (eight    */
-                                 /* CTAs per SM), 1 unconstrained, 2 six, 3 eight CTAs/SM   */
+    uint32_t kernel_variant;     /* kernel of single-scene calls: 0 default (the path-pool */
+                                 /* loop, 128 threads, 32 warps/SM budget); k = 1..6 picks  */
+                                 /* variant k - 1 (budget + 3 * shape, shapes 0-1 of      */
+                                 /* ix_batch_plan_autotune); anything else returns NULL    */
 } ix_backend_options;
 
 /* GpuWorkLimits (gpu_backend/limits.rs:6-27): a request above a limit is declined. */
@@ -91,9 +97,9 @@ void ix_set_work_limits(ix_backend* b, const ix_work_limits* limits);
 /* Rounding mode of later calls (IX_PRECISION_*). */
 void ix_set_precision(ix_backend* b, uint32_t precision);
 /* scene_routes_to_gpu (gpu_backend/mod.rs:288): 1 when this backend can trace `scene`
- * (convex, <= IX_MAX_PLANES, polished or frosted facets, no volume scattering or edge
- * rounding, an isotropic or uniaxial material with modelled dispersion, a modelled
- * environment).  The facet finishes are not read here. */
+ * (convex, <= IX_MAX_PLANES, polished or frosted facets, an isotropic or uniaxial
+ * material with modelled dispersion, a modelled environment, at most 2^32 - 1 pixels).
+ * The facet finishes are not read here. */
 int ix_scene_routes_to_gpu(const ix_scene* scene);
 /* GpuBackend::try_accumulate_geom_cancellable (backend.rs:272) with an f32 accumulator:
  * adds (float)(f64 pixel sum) into accum_xyz.  `cancel` may be NULL; it is polled
@@ -125,8 +131,17 @@ ix_batch_plan* ix_batch_plan_create(ix_backend* b, const ix_scene* scenes, uint3
 /* One persistent launch of every job on `stream` (NULL: the backend's stream); not
  * synchronised.  IX_DONE or IX_DECLINED. */
 int ix_batch_plan_run(ix_batch_plan* p, void* stream);
-/* Times each megakernel register variant `reps` times and keeps the fastest. */
+/* The autotuner (the reference picks GpuPipelineKind by hand, gpu_backend/mod.rs:347):
+ * times every kernel variant this build carries -- the static task loop and the
+ * path-pool loop at 64, 128 and 256 threads per CTA, each under three register budgets
+ * (variant = budget + 3 * shape) -- `reps` times on a strided sample of about 1/16 of
+ * the plan's work (every job represented), keeps the fastest and writes it to `chosen`.
+ * With ix_backend_options.threads_per_block set, only that CTA size is tried.
+ * Returns 0, or -1 on a device error. */
 int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen);
+/* Pins the plan's kernel variant (budget + 3 * shape, see ix_batch_plan_autotune).
+ * Returns 0, or -1 when this build or this plan cannot run it. */
+int ix_batch_plan_set_variant(ix_batch_plan* p, uint32_t variant);
 /* Copies the plan's sums to host memory (ix_batch_plan_output_size doubles). */
 int ix_batch_plan_download(ix_batch_plan* p, double* host_out);
 uint64_t ix_batch_plan_output_size(const ix_batch_plan* p);

@@ -76,6 +76,7 @@ def load_library() -> C.CDLL:
                                              C.c_uint32]
         lib.ix_batch_plan_run.argtypes = [C.c_void_p, C.c_void_p]
         lib.ix_batch_plan_autotune.argtypes = [C.c_void_p, C.c_int, P(C.c_uint32)]
+        lib.ix_batch_plan_set_variant.argtypes = [C.c_void_p, C.c_uint32]
         lib.ix_batch_plan_download.argtypes = [C.c_void_p, P(C.c_double)]
         lib.ix_batch_plan_output_size.restype = C.c_uint64
         lib.ix_batch_plan_output_size.argtypes = [C.c_void_p]
@@ -600,6 +601,10 @@ class BatchPlan:
         if self._lib.ix_batch_plan_autotune(self._h, reps, C.byref(v)) != 0:
             raise RuntimeError(f"autotune failed: {self._b.last_lost_reason()}")
         return int(v.value)
+
+    def set_variant(self, variant: int) -> bool:
+        """Pins the kernel variant (budget + 3 * shape); False when it cannot run here."""
+        return self._lib.ix_batch_plan_set_variant(self._h, int(variant)) == 0
 
     @property
     def variant(self) -> int:

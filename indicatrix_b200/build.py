@@ -57,13 +57,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
     jobs = []  # (object, command); the device units compile concurrently
     # The fused build also takes the approximate divide / square root and flushes
     # denormals; the slab scan's division stays IEEE (__fdiv_rn) in both builds.
-    for unit in ("ix_kernels", "ix_metrics", "ix_display"):
+    for unit in ("ix_kernels", "ix_pool", "ix_metrics", "ix_display"):
         for variant, flags in (("exact", ["-DIX_EXACT=1", "-fmad=false"]),
                                ("fast", ["-DIX_EXACT=0", "-fmad=true", "-prec-div=false",
                                          "-prec-sqrt=false", "-ftz=true"])):
             obj = os.path.join(BUILD_DIR, f"{unit}_{variant}.o")
             jobs.append((obj, common + flags + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj]))
-    for unit in ("ix_probe", "ix_noalloc", "ix_radiance", "ix_surrogate"):
+    for unit in ("ix_probe", "ix_fixed", "ix_noalloc", "ix_radiance", "ix_surrogate"):
         obj = os.path.join(BUILD_DIR, unit + ".o")
         jobs.append((obj, common + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj]))
     procs = [(obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))

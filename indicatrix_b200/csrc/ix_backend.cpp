@@ -46,65 +46,97 @@ uint32_t pixels_per_task(uint32_t spp) {
 // pixels each.  The reference's first launch of at most 1M paths (gpu/frame/mod.rs:
 // 355-361) keeps a display GPU's watchdog away; a compute B200 has none, and a 1M-path
 // launch cannot fill its 148 SMs (the results do not depend on the chunking).
+// Kernel variant of single-scene calls when the options name none: the path-pool loop,
+// 128 threads, the 32-warps-per-SM register budget.
+constexpr uint32_t kDefaultVariant = 2 + 3 * ix::SHAPE_POOL_128;
+
 uint64_t chunk_budget(const ix_backend* b, int launch_index) {
     (void)launch_index;
     return b->chunk_paths ? b->chunk_paths : (64ull << 20);
 }
 
 // Enqueue the trace launches for pixels [0, n_pixels) of `sc` (device planes) into
-// d_out; chunked so no single launch exceeds the path budget.  With `attr`, every launch
-// is the attributed trace kernel, followed by the fold of its records into d_map (the
-// frame's attribution map on the device).  Returns the launch count or -1 on a CUDA
-// error (b->last_error set).
+// d_out; chunked so no single launch exceeds the path budget.  A launch covers whole
+// pixels, so the sums do not depend on the chunking.  The path-pool shapes add into
+// fixed-point sums of the launch's pixels (b->d_acc) and round them into d_out after each
+// launch; a pixel's samples beyond FIXED_MAX_SAMPLES go to later launches of the same
+// pixels.  With `attr`, every launch is the attributed trace kernel (static task loop),
+// followed by the fold of its records into d_map (the frame's attribution map on the
+// device).  Returns the launch count or -1 on a CUDA error (b->last_error set).
 int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uint32_t spp,
                   double* d_out, int accumulate, cudaStream_t stream,
                   const volatile int32_t* cancel, bool* cancelled,
                   const ix::AttrLaunch* attr = nullptr, ix_attribution_pixel* d_map = nullptr) {
-    const uint32_t n_pixels = sc.width * sc.height;
+    const uint64_t n_pixels64 = (uint64_t)sc.width * sc.height;
+    if (n_pixels64 > 0xFFFFFFFFull) {
+        b->last_error = "frame has more than 2^32 - 1 pixels";
+        return -1;
+    }
+    const uint32_t n_pixels = (uint32_t)n_pixels64;
     const bool exact = b->precision == IX_PRECISION_EXACT;
     ix::TraceLaunch L;
     std::memset(&L, 0, sizeof(L));
     L.scene = sc;
     L.flags = ix::scene_flags(sc.material);
-    L.sample_offset = sample_offset;
-    L.spp = spp;
     L.pixels_per_task = pixels_per_task(spp);
-    L.accumulate = accumulate;
     L.task_counter = b->d_counter;
     L.dropped = b->d_dropped;
-    L.threads = (int)b->threads;
-    L.variant = (int)b->variant;
+    L.variant = attr ? 0 : (int)b->variant;
+    const int shape = ix::variant_shape(L.variant);
+    const bool pool = ix::shape_is_pool(shape);
+    L.threads = ix::shape_threads(shape);
     const int uni = ix::needs_uniaxial_kernel(L.flags) ? 1 : 0;
-    L.blocks = b->sm_count * (exact ? b->bps_exact[uni][b->variant] : b->bps_fast[uni][b->variant]);
+    L.blocks = b->sm_count * (exact ? b->bps_exact[uni][L.variant] : b->bps_fast[uni][L.variant]);
     if (attr) L.blocks = b->sm_count * (exact ? b->bps_attr_exact[uni] : b->bps_attr_fast[uni]);
-    if (L.blocks <= 0) L.blocks = b->sm_count > 0 ? b->sm_count : 1;
-    uint32_t begin = 0;
+    if (L.blocks <= 0) {
+        b->last_error = "kernel variant not available in this build";
+        return -1;
+    }
+    // Sample blocks: one for the static task loop, FIXED_MAX_SAMPLES at most for the pool.
+    const uint32_t block = pool ? std::min<uint32_t>(spp, ix::FIXED_MAX_SAMPLES) : spp;
     int launches = 0;
-    while (begin < n_pixels) {
-        if (cancel && *cancel) {
-            *cancelled = true;
-            return launches;
+    for (uint32_t s0 = 0; s0 < spp; s0 += block) {
+        const uint32_t sb = std::min(block, spp - s0);
+        L.sample_offset = sample_offset + s0;
+        L.spp = sb;
+        L.accumulate = s0 == 0 ? accumulate : 1;
+        uint32_t begin = 0;
+        while (begin < n_pixels) {
+            if (cancel && *cancel) {
+                *cancelled = true;
+                return launches;
+            }
+            uint64_t px = std::max<uint64_t>(1, chunk_budget(b, launches) / std::max<uint32_t>(sb, 1));
+            uint32_t n = (uint32_t)std::min<uint64_t>(px, n_pixels - begin);
+            L.pixel_begin = begin;
+            L.n_pixels = n;
+            L.out = d_out + (size_t)begin * 3;
+            if (pool) {
+                if (fail(b, grow_device(&b->d_acc, &b->acc_cap, (size_t)n * ix::FIXED_WORDS), "sums alloc")) return -1;
+                L.acc = b->d_acc;
+            }
+            if (attr) {
+                cudaError_t e = exact ? ix::launch_trace_attributed_exact(L, *attr, stream)
+                                      : ix::launch_trace_attributed_fast(L, *attr, stream);
+                if (fail(b, e, "attributed trace launch")) return -1;
+                const ix::AttrFoldLaunch F{attr->cls, attr->y, d_map + begin, n, sb};
+                e = exact ? ix::launch_attribution_fold_exact(F, stream) : ix::launch_attribution_fold_fast(F, stream);
+                if (fail(b, e, "attribution fold")) return -1;
+            } else {
+                cudaError_t e = exact ? ix::launch_trace_exact(L, stream) : ix::launch_trace_fast(L, stream);
+                if (fail(b, e, "trace launch")) return -1;
+            }
+            ++launches;
+            begin += n;
         }
-        uint64_t px = std::max<uint64_t>(1, chunk_budget(b, launches) / std::max<uint32_t>(spp, 1));
-        uint32_t n = (uint32_t)std::min<uint64_t>(px, n_pixels - begin);
-        L.pixel_begin = begin;
-        L.n_pixels = n;
-        L.out = d_out + (size_t)begin * 3;
-        if (attr) {
-            cudaError_t e = exact ? ix::launch_trace_attributed_exact(L, *attr, stream)
-                                  : ix::launch_trace_attributed_fast(L, *attr, stream);
-            if (fail(b, e, "attributed trace launch")) return -1;
-            const ix::AttrFoldLaunch F{attr->cls, attr->y, d_map + begin, n, spp};
-            e = exact ? ix::launch_attribution_fold_exact(F, stream) : ix::launch_attribution_fold_fast(F, stream);
-            if (fail(b, e, "attribution fold")) return -1;
-        } else {
-            cudaError_t e = exact ? ix::launch_trace_exact(L, stream) : ix::launch_trace_fast(L, stream);
-            if (fail(b, e, "trace launch")) return -1;
-        }
-        ++launches;
-        begin += n;
     }
     return launches;
+}
+
+// Kernels one trace launch of the backend's single-scene variant takes: the trace kernel,
+// and for the path-pool shapes the rounding of its fixed-point sums.
+uint32_t kernels_per_launch(const ix_backend* b) {
+    return ix::shape_is_pool(ix::variant_shape((int)b->variant)) ? 2u : 1u;
 }
 
 // Points a device copy of host scene `sc` at the backend's copy of its facet finishes
@@ -178,7 +210,7 @@ int accumulate_impl(ix_backend* b, const ix_scene* scene, uint32_t sample_offset
     b->timing.kernel_ms = ms;
     b->timing.reduce_ms = std::chrono::duration<float, std::milli>(t1 - t0).count();
     b->timing.paths = n_pixels * spp;
-    b->timing.launches = (uint32_t)launches;
+    b->timing.launches = (uint32_t)launches * kernels_per_launch(b);
     b->dropped = dropped;
     return IX_DONE;
 }
@@ -360,15 +392,20 @@ ix_backend* ix_backend_create(const ix_backend_options* opts) {
         (void)cudaGetLastError();
         return nullptr;
     }
+    // threads_per_block: 0 (any CTA size) or one of the sizes the path-pool shapes come in.
+    if (opts && opts->threads_per_block != 0 && opts->threads_per_block != 64 && opts->threads_per_block != 128 &&
+        opts->threads_per_block != 256)
+        return nullptr;
+    if (opts && opts->kernel_variant > (uint32_t)ix_backend::kVariants) return nullptr;
     ix_backend* b = new ix_backend();
     if (opts) {
         b->device = opts->device;
         b->pipeline = opts->pipeline;
         b->precision = opts->precision;
-        if (opts->threads_per_block) b->threads = opts->threads_per_block;
+        b->batch_threads = opts->threads_per_block;
         b->chunk_paths = opts->chunk_paths;
     }
-    if (b->device < 0 || b->device >= n || b->threads % 32 || b->threads > 128 || b->threads == 0) {
+    if (b->device < 0 || b->device >= n) {
         delete b;
         return nullptr;
     }
@@ -385,19 +422,30 @@ ix_backend* ix_backend_create(const ix_backend_options* opts) {
     }
     b->sm_count = prop.multiProcessorCount;
     b->label = prop.name;
+    static_assert(ix_backend::kVariants == ix::N_VARIANTS, "variant table size");
     for (int u = 0; u < 2; ++u)
-        for (int v = 0; v < 3; ++v) {
-            b->bps_exact[u][v] = std::max(1, ix::trace_blocks_per_sm_exact((int)b->threads, v, u, nullptr));
-            b->bps_fast[u][v] = std::max(1, ix::trace_blocks_per_sm_fast((int)b->threads, v, u, nullptr));
+        for (int v = 0; v < ix::N_VARIANTS; ++v) {
+            const int threads = ix::shape_threads(ix::variant_shape(v));
+            b->bps_exact[u][v] = ix::trace_blocks_per_sm_exact(threads, v, u, nullptr);
+            b->bps_fast[u][v] = ix::trace_blocks_per_sm_fast(threads, v, u, nullptr);
         }
     for (int u = 0; u < 2; ++u) {
         b->bps_attr_exact[u] = std::max(1, ix::trace_attributed_blocks_per_sm_exact((int)b->threads, u));
         b->bps_attr_fast[u] = std::max(1, ix::trace_attributed_blocks_per_sm_fast((int)b->threads, u));
     }
-    // Option 0 = the measured default (8 CTAs per SM); 1/2/3 = unconstrained / 6 / 8.
-    b->variant = 2;
-    if (opts && opts->kernel_variant >= 1 && opts->kernel_variant <= 3) b->variant = opts->kernel_variant - 1;
+    // Option 0 = the measured default; k >= 1 = variant k - 1 (budget + 3 * shape).
+    b->variant = kDefaultVariant;
+    if (opts && opts->kernel_variant >= 1) b->variant = opts->kernel_variant - 1;
+    if (b->bps_exact[0][b->variant] <= 0 || b->bps_fast[0][b->variant] <= 0) {
+        // Single-scene calls run only the variants both builds carry.
+        ix_backend_destroy(b);
+        return nullptr;
+    }
     b->batch_variant = b->variant;
+    if (b->batch_threads && (uint32_t)ix::shape_threads(ix::variant_shape(b->batch_variant)) != b->batch_threads)
+        b->batch_variant = b->batch_threads == 64 ? 2 + 3 * ix::SHAPE_POOL_64
+                                                  : (b->batch_threads == 256 ? 2 + 3 * ix::SHAPE_POOL_256
+                                                                             : 2 + 3 * ix::SHAPE_POOL_128);
     return b;
 }
 
@@ -415,6 +463,7 @@ void ix_backend_destroy(ix_backend* b) {
     cudaFree(b->d_attr_map);
     cudaFree(b->d_batch_out);
     cudaFree(b->d_finishes);
+    cudaFree(b->d_acc);
     display_state_free(b->display);
     radiance_state_free(b->radiance);
     if (b->h_attr_map) cudaFreeHost(b->h_attr_map);
@@ -448,6 +497,7 @@ int ix_scene_routes_to_gpu(const ix_scene* s) {
     if (!s) return 0;
     if (s->n_planes > IX_MAX_PLANES || (s->n_planes && !s->planes)) return 0;
     if (s->width == 0 || s->height == 0) return 0;
+    if ((uint64_t)s->width * s->height > 0xFFFFFFFFull) return 0;  // pixel indices are 32-bit
     const ix_material& m = s->material;
     if (m.has_e_dispersion && m.e_dispersion.kind > IX_DISP_CAUCHY) return 0;
     const ix_environment& e = s->environment;
@@ -544,7 +594,7 @@ int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metr
     b->timing.kernel_ms = ms;
     b->timing.reduce_ms = std::chrono::duration<float, std::milli>(t1 - t0).count();
     b->timing.paths = n_pixels * spp;
-    b->timing.launches = (uint32_t)launches;
+    b->timing.launches = (uint32_t)launches * 2;  // the attributed trace and its record fold
     b->dropped = dropped;
     return IX_DONE;
 }
@@ -556,8 +606,10 @@ int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metr
 // ------------------------------------------------------------------------------------
 struct ix_batch_plan {
     ix_backend* b = nullptr;
-    uint32_t n_scenes = 0, n_jobs = 0, total_tasks = 0;
+    uint32_t n_scenes = 0, n_jobs = 0, total_tasks = 0, total_chunks = 0;
     uint64_t out_doubles = 0, paths = 0;
+    bool pool_ok = true;  // every job fits the path-pool loop (spp <= FIXED_MAX_SAMPLES)
+    unsigned long long* d_acc = nullptr;  // fixed-point sums, FIXED_WORDS per pixel of every job
     ix_scene* d_scenes = nullptr;
     uint32_t* d_flags = nullptr;
     uint32_t uniaxial = 0;  // some scene needs the uniaxial transport instantiation
@@ -590,9 +642,25 @@ void plan_free_graph(ix_batch_plan* p) {
     p->graph_variant = -1;
 }
 
-cudaError_t plan_enqueue(ix_batch_plan* p, cudaStream_t st, uint32_t variant) {
+// Resident CTAs per SM of batch variant `v` for plan `p` in the backend's rounding build
+// (0: the build does not carry it, or the plan cannot run it).
+int plan_blocks_per_sm(const ix_batch_plan* p, uint32_t v) {
+    if (v >= (uint32_t)ix::N_VARIANTS) return 0;
+    const int shape = ix::variant_shape((int)v);
+    if (ix::shape_is_pool(shape) && !p->pool_ok) return 0;
+    const int threads = ix::shape_threads(shape);
+    return p->b->precision == IX_PRECISION_EXACT ? ix::batch_blocks_per_sm_exact(threads, (int)v, (int)p->uniaxial)
+                                                 : ix::batch_blocks_per_sm_fast(threads, (int)v, (int)p->uniaxial);
+}
+
+// Enqueues one launch of variant `variant` over every `stride`-th task / chunk of the plan
+// (stride 1: the whole plan) and, for the path-pool shapes, the rounding of its sums.
+cudaError_t plan_enqueue(ix_batch_plan* p, cudaStream_t st, uint32_t variant, uint32_t stride = 1) {
     ix_backend* b = p->b;
     const bool exact = b->precision == IX_PRECISION_EXACT;
+    const int bps = plan_blocks_per_sm(p, variant);
+    if (bps <= 0) return cudaErrorInvalidValue;
+    const int shape = ix::variant_shape((int)variant);
     ix::BatchLaunch L;
     std::memset(&L, 0, sizeof(L));
     L.scenes = p->d_scenes;
@@ -601,16 +669,24 @@ cudaError_t plan_enqueue(ix_batch_plan* p, cudaStream_t st, uint32_t variant) {
     L.jobs = p->d_jobs;
     L.n_jobs = p->n_jobs;
     L.total_tasks = p->total_tasks;
+    L.total_chunks = p->total_chunks;
     L.out = p->d_out;
     L.accumulate = 0;
     L.task_counter = p->d_counter;
     L.dropped = p->d_dropped;
-    L.threads = 128;
+    L.stride = std::max<uint32_t>(1, stride);
+    L.threads = ix::shape_threads(shape);
     L.variant = (int)variant;
-    int bps = exact ? ix::batch_blocks_per_sm_exact(128, (int)variant, (int)p->uniaxial)
-                    : ix::batch_blocks_per_sm_fast(128, (int)variant, (int)p->uniaxial);
-    L.blocks = b->sm_count * std::max(1, bps);
-    return exact ? ix::launch_batch_exact(L, st) : ix::launch_batch_fast(L, st);
+    L.blocks = b->sm_count * bps;
+    const uint64_t pixels = p->out_doubles / 3;
+    if (ix::shape_is_pool(shape)) {
+        L.acc = p->d_acc;
+        cudaError_t e = cudaMemsetAsync(p->d_acc, 0, pixels * ix::FIXED_WORDS * sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = exact ? ix::launch_batch_exact(L, st) : ix::launch_batch_fast(L, st);
+    if (e != cudaSuccess || !ix::shape_is_pool(shape)) return e;
+    return ix::launch_fixed_to_f64(p->d_acc, p->d_out, pixels, 0, st);
 }
 
 // ix_batch_plan_run / ix_batch_plan_download for a caller that already holds the
@@ -632,7 +708,7 @@ int plan_run_locked(ix_batch_plan* p, cudaStream_t st) {
     if (fail(b, cudaGraphLaunch(p->exec, st), "graph launch")) return IX_DECLINED;
     if (fail(b, cudaEventRecord(b->ev1, st), "event")) return IX_DECLINED;
     b->timing.paths = p->paths;
-    b->timing.launches = 1;
+    b->timing.launches = ix::shape_is_pool(ix::variant_shape((int)p->variant)) ? 2 : 1;
     return IX_DONE;
 }
 int plan_download_locked(ix_batch_plan* p, double* host_out) {
@@ -658,8 +734,9 @@ static ix_batch_plan* plan_create_locked(ix_backend* b, const ix_scene* scenes, 
     p->b = b;
     p->n_scenes = n_scenes;
     p->n_jobs = n_jobs;
-    // Job table: tasks of ~256 paths, jobs laid out back to back.
-    uint64_t task = 0, out = 0;
+    // Job table: tasks of ~64 paths (static task loop) and chunks of 32 paths (path-pool
+    // loop), jobs laid out back to back.
+    uint64_t task = 0, out = 0, chunk = 0;
     p->jobs.resize(n_jobs);
     p->job_out.resize(n_jobs);
     for (uint32_t j = 0; j < n_jobs; ++j) {
@@ -677,16 +754,28 @@ static ix_batch_plan* plan_create_locked(ix_backend* b, const ix_scene* scenes, 
         bj.task_begin = (uint32_t)task;
         bj.sample_offset = in.sample_offset;
         bj.out_offset = out;
+        const uint64_t job_paths = (uint64_t)bj.n_pixels * in.spp;
+        if ((uint64_t)sc.width * sc.height > 0xFFFFFFFFull || job_paths > 0xFFFFFFFFull - 32) {
+            delete p;
+            return nullptr;
+        }
+        bj.paths = (uint32_t)job_paths;
+        bj.chunk_begin = (uint32_t)std::min<uint64_t>(chunk, 0xFFFFFFFFull);
+        bj.acc_offset = out / 3 * ix::FIXED_WORDS;
+        if (in.spp > ix::FIXED_MAX_SAMPLES) p->pool_ok = false;
         p->job_out[j] = out;
         task += (bj.n_pixels + bj.ppt - 1) / bj.ppt;
+        chunk += (job_paths + 31) / 32;
         out += (uint64_t)bj.n_pixels * 3;
-        p->paths += (uint64_t)bj.n_pixels * in.spp;
+        p->paths += job_paths;
     }
     if (task >= 0xFFFFFFFFull) {
         delete p;
         return nullptr;
     }
+    if (chunk >= 0xFFFFFFFFull) p->pool_ok = false;
     p->total_tasks = (uint32_t)task;
+    p->total_chunks = p->pool_ok ? (uint32_t)chunk : 0;
     p->out_doubles = out;
     uint64_t plane_floats = 0;
     for (uint32_t i = 0; i < n_scenes; ++i) plane_floats += (uint64_t)scenes[i].n_planes * 4;
@@ -722,7 +811,9 @@ static ix_batch_plan* plan_create_locked(ix_backend* b, const ix_scene* scenes, 
          (pooled_out ? grow_device(&b->d_batch_out, &b->batch_out_cap, std::max<uint64_t>(out, 1))
                      : cudaMalloc((void**)&p->d_out, std::max<uint64_t>(out, 1) * sizeof(double))) == cudaSuccess &&
          cudaMalloc((void**)&p->d_counter, sizeof(uint32_t)) == cudaSuccess &&
-         cudaMalloc((void**)&p->d_dropped, sizeof(unsigned long long)) == cudaSuccess;
+         cudaMalloc((void**)&p->d_dropped, sizeof(unsigned long long)) == cudaSuccess &&
+         (!p->pool_ok || cudaMalloc((void**)&p->d_acc, std::max<uint64_t>(out / 3, 1) * ix::FIXED_WORDS *
+                                                          sizeof(unsigned long long)) == cudaSuccess);
     if (ok && pooled_out) {
         p->d_out = b->d_batch_out;
         p->out_pooled = true;
@@ -733,6 +824,7 @@ static ix_batch_plan* plan_create_locked(ix_backend* b, const ix_scene* scenes, 
          cudaMemcpy(p->d_jobs, p->jobs.data(), n_jobs * sizeof(ix::BatchJob), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemset(p->d_dropped, 0, sizeof(unsigned long long)) == cudaSuccess;
     p->variant = b->batch_variant;
+    if (ok && plan_blocks_per_sm(p, p->variant) <= 0) p->variant = ix::variant_budget((int)p->variant);
     if (!ok) {
         fail(b, cudaGetLastError(), "batch plan");
         ix_batch_plan_destroy(p);
@@ -759,17 +851,27 @@ int ix_batch_plan_run(ix_batch_plan* p, void* stream) {
 int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen) {
     if (!p || p->b->lost) return -1;
     ix_backend* b = p->b;
+    Turn turn(b);
+    if (fail(b, cudaSetDevice(b->device), "set device")) return -1;
+    // Each candidate is timed on every stride-th task / chunk of the plan: about 1/16 of
+    // its work, spread over all its jobs, and never fewer claims than the grid has warps.
+    const uint64_t units = std::max<uint64_t>(1, std::min(p->total_tasks, p->pool_ok ? p->total_chunks : p->total_tasks));
+    const uint64_t min_claims = (uint64_t)b->sm_count * 64 * 4;
+    const uint32_t stride = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(16, units / min_claims));
     float best = 1e30f;
     uint32_t best_v = p->variant;
-    for (uint32_t v = 0; v < 3; ++v) {
-        p->variant = v;
+    for (uint32_t v = 0; v < (uint32_t)ix::N_VARIANTS; ++v) {
+        if (plan_blocks_per_sm(p, v) <= 0) continue;
+        if (b->batch_threads && (uint32_t)ix::shape_threads(ix::variant_shape((int)v)) != b->batch_threads) continue;
         float total = 0.0f;
         for (int r = 0; r < std::max(1, reps) + 1; ++r) {
-            if (ix_batch_plan_run(p, nullptr) != IX_DONE) return -1;
+            if (fail(b, cudaEventRecord(b->ev0, b->stream), "event")) return -1;
+            if (fail(b, plan_enqueue(p, b->stream, v, stride), "autotune launch")) return -1;
+            if (fail(b, cudaEventRecord(b->ev1, b->stream), "event")) return -1;
             if (fail(b, cudaStreamSynchronize(b->stream), "autotune")) return -1;
             float ms = 0.0f;
             cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-            if (r > 0) total += ms;  // first run of a variant builds its graph
+            if (r > 0) total += ms;  // the first run of a candidate warms it up
         }
         if (total < best) {
             best = total;
@@ -780,6 +882,14 @@ int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen) {
     p->tuned = true;
     b->batch_variant = best_v;  // later plans of this backend start from the pick
     if (chosen) *chosen = best_v;
+    return 0;
+}
+
+int ix_batch_plan_set_variant(ix_batch_plan* p, uint32_t variant) {
+    if (!p || p->b->lost) return -1;
+    Turn turn(p->b);
+    if (plan_blocks_per_sm(p, variant) <= 0) return -1;
+    p->variant = variant;
     return 0;
 }
 
@@ -809,6 +919,7 @@ void ix_batch_plan_destroy(ix_batch_plan* p) {
     cudaFree(p->d_planes);
     cudaFree(p->d_finishes);
     if (!p->out_pooled) cudaFree(p->d_out);
+    cudaFree(p->d_acc);
     cudaFree(p->d_counter);
     cudaFree(p->d_dropped);
     (void)cudaGetLastError();
@@ -894,7 +1005,7 @@ int ix_accumulate_device(ix_backend* b, const ix_scene* scene, uint32_t sample_o
     if (launches < 0) return IX_DECLINED;
     if (fail(b, cudaEventRecord(b->ev1, st), "event")) return IX_DECLINED;
     b->timing.paths = (uint64_t)scene->width * scene->height * spp;
-    b->timing.launches = (uint32_t)launches;
+    b->timing.launches = (uint32_t)launches * kernels_per_launch(b);
     return IX_DONE;
 }
 

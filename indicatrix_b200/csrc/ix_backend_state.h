@@ -54,12 +54,19 @@ struct ix_backend {
     // A host scene's per-facet finishes, copied for the kernels.
     uint8_t* d_finishes = nullptr;
     size_t finishes_cap = 0;
+    // Fixed-point per-pixel sums of the path-pool kernels (FIXED_WORDS per pixel of a launch).
+    unsigned long long* d_acc = nullptr;
+    size_t acc_cap = 0;
     int sm_count = 0;
+    // Kernel variant (budget + 3 * shape, ix_launch.h) of single-scene calls.
     uint32_t variant = 0;
-    // Register variant new batch plans start from: the last autotuner pick (or `variant`).
+    // Variant new batch plans start from: the last autotuner pick (or `variant`).
     uint32_t batch_variant = 0;
-    // Resident CTAs per SM by [uniaxial instantiation][variant].
-    int bps_exact[2][3] = {{1, 1, 1}, {1, 1, 1}}, bps_fast[2][3] = {{1, 1, 1}, {1, 1, 1}};
+    // CTA size new batch plans are restricted to (0: any; 64, 128 or 256).
+    uint32_t batch_threads = 0;
+    // Resident CTAs per SM by [uniaxial instantiation][variant] (0: not in this build).
+    static constexpr int kVariants = 12;
+    int bps_exact[2][kVariants] = {}, bps_fast[2][kVariants] = {};
     // ... and of the attributed trace kernels by [uniaxial instantiation].
     int bps_attr_exact[2] = {1, 1}, bps_attr_fast[2] = {1, 1};
     std::string label;

@@ -332,10 +332,12 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(batch_kernel)(const __grid_c
     uint32_t cached = 0xFFFFFFFFu;
     uint32_t drops = 0;  // non-finite samples this lane dropped
     for (;;) {
-        uint32_t task = 0;
-        if (lane == 0) task = atomicAdd(L.task_counter, 1u);
-        task = __shfl_sync(0xFFFFFFFFu, task, 0);
-        if (task >= L.total_tasks) break;
+        uint32_t claim = 0;
+        if (lane == 0) claim = atomicAdd(L.task_counter, 1u);
+        claim = __shfl_sync(0xFFFFFFFFu, claim, 0);
+        const uint64_t task64 = (uint64_t)claim * L.stride;  // the claim's task
+        if (task64 >= L.total_tasks) break;
+        const uint32_t task = (uint32_t)task64;
         uint32_t lo = 0, hi = L.n_jobs;  // last job with task_begin <= task
         while (hi - lo > 1) {
             const uint32_t mid = (lo + hi) >> 1;
@@ -483,19 +485,21 @@ __global__ void IX_SFX(check_kernel)(const __grid_constant__ CheckLaunch L) {
 static bool launch_shape_ok(int threads) { return threads == 128; }
 
 cudaError_t IX_SFX(launch_trace)(const TraceLaunch& l, cudaStream_t stream) {
+    if (l.variant < 0 || l.variant >= N_VARIANTS) return cudaErrorInvalidValue;
+    if (shape_is_pool(variant_shape(l.variant))) return IX_SFX(launch_pool_trace)(l, stream);
     if (l.pixels_per_task == 0 || l.pixels_per_task > (uint32_t)TRACE_MAX_PPT) return cudaErrorInvalidValue;
     if (!launch_shape_ok(l.threads)) return cudaErrorInvalidValue;
     if (l.scene.n_planes > IX_MAX_PLANES) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     if (needs_uniaxial_kernel(l.flags)) {
-        switch (l.variant) {
+        switch (variant_budget(l.variant)) {
             case 1: IX_SFX(trace_kernel)<UNI_MINB_1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
             case 2: IX_SFX(trace_kernel)<UNI_MINB_2, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
             default: IX_SFX(trace_kernel)<1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
         }
     } else {
-        switch (l.variant) {
+        switch (variant_budget(l.variant)) {
             case 1: IX_SFX(trace_kernel)<6, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
             case 2: IX_SFX(trace_kernel)<8, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
             default: IX_SFX(trace_kernel)<1, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
@@ -532,17 +536,19 @@ cudaError_t IX_SFX(launch_attribution_fold)(const AttrFoldLaunch& l, cudaStream_
 }
 
 cudaError_t IX_SFX(launch_batch)(const BatchLaunch& l, cudaStream_t stream) {
-    if (!launch_shape_ok(l.threads) || l.n_jobs == 0) return cudaErrorInvalidValue;
+    if (l.variant < 0 || l.variant >= N_VARIANTS) return cudaErrorInvalidValue;
+    if (shape_is_pool(variant_shape(l.variant))) return IX_SFX(launch_pool_batch)(l, stream);
+    if (!launch_shape_ok(l.threads) || l.n_jobs == 0 || l.stride == 0) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     if (l.uniaxial) {
-        switch (l.variant) {
+        switch (variant_budget(l.variant)) {
             case 1: IX_SFX(batch_kernel)<UNI_MINB_1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
             case 2: IX_SFX(batch_kernel)<UNI_MINB_2, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
             default: IX_SFX(batch_kernel)<1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
         }
     } else {
-        switch (l.variant) {
+        switch (variant_budget(l.variant)) {
             case 1: IX_SFX(batch_kernel)<6, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
             case 2: IX_SFX(batch_kernel)<8, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
             default: IX_SFX(batch_kernel)<1, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
@@ -577,6 +583,10 @@ static int occupancy(K kernel, int threads) {
 
 int IX_SFX(trace_blocks_per_sm)(int threads, int variant, int uniaxial, size_t* smem_bytes) {
     if (smem_bytes) *smem_bytes = 0;
+    if (variant < 0 || variant >= N_VARIANTS) return 0;
+    if (shape_is_pool(variant_shape(variant))) return IX_SFX(pool_trace_blocks_per_sm)(variant, uniaxial);
+    if (threads != 128) return 0;
+    variant = variant_budget(variant);
     if (uniaxial) {
         if (variant == 1) return occupancy(IX_SFX(trace_kernel)<UNI_MINB_1, true>, threads);
         if (variant == 2) return occupancy(IX_SFX(trace_kernel)<UNI_MINB_2, true>, threads);
@@ -593,6 +603,10 @@ int IX_SFX(trace_attributed_blocks_per_sm)(int threads, int uniaxial) {
 }
 
 int IX_SFX(batch_blocks_per_sm)(int threads, int variant, int uniaxial) {
+    if (variant < 0 || variant >= N_VARIANTS) return 0;
+    if (shape_is_pool(variant_shape(variant))) return IX_SFX(pool_batch_blocks_per_sm)(variant, uniaxial);
+    if (threads != 128) return 0;
+    variant = variant_budget(variant);
     if (uniaxial) {
         if (variant == 1) return occupancy(IX_SFX(batch_kernel)<UNI_MINB_1, true>, threads);
         if (variant == 2) return occupancy(IX_SFX(batch_kernel)<UNI_MINB_2, true>, threads);

@@ -52,6 +52,34 @@ inline bool needs_uniaxial_kernel(uint32_t flags) {
     return (flags & (SCENE_UNIAXIAL | SCENE_PLEOCHROIC | SCENE_SCATTERING | SCENE_ROUNDED)) != 0;
 }
 
+// Launch shapes of the trace megakernels.  A shape is a task loop and a CTA size:
+//  * SHAPE_TASKS: the static task loop (a warp task is a run of whole pixels x all their
+//    samples, its paths split over the 4 groups of the warp by a fixed stride; per-pixel
+//    f64 sums folded in a fixed order), 128 threads;
+//  * SHAPE_POOL_*: the path-pool loop (a warp claims 32 paths at a time, prepares their
+//    camera samples one per lane, and each 8-lane group takes the next prepared path
+//    whenever its own finishes; samples are added into per-pixel fixed-point sums, which
+//    no order of arrival changes), 128, 64 or 256 threads.
+// A kernel variant is budget + 3 * shape, the budget being the register allocation's
+// resident-warp target (0 unconstrained, 1 and 2 the two occupancy targets of each loop).
+enum LaunchShape : int { SHAPE_TASKS = 0, SHAPE_POOL_128 = 1, SHAPE_POOL_64 = 2, SHAPE_POOL_256 = 3 };
+constexpr int N_SHAPES = 4;
+constexpr int N_BUDGETS = 3;
+constexpr int N_VARIANTS = N_SHAPES * N_BUDGETS;
+inline int variant_shape(int v) { return v / N_BUDGETS; }
+inline int variant_budget(int v) { return v % N_BUDGETS; }
+inline int shape_threads(int shape) { return shape == SHAPE_POOL_64 ? 64 : shape == SHAPE_POOL_256 ? 256 : 128; }
+inline bool shape_is_pool(int shape) { return shape != SHAPE_TASKS; }
+
+// Fixed-point per-pixel sums of the path-pool kernels: for each of X, Y and Z three 64-bit
+// words (t, a, b) holding t 2^24 + a 2^-16 + b 2^-56.  A sample adds its exact binary
+// expansion split into those digits (a and b below 2^40, so no word carries within a
+// launch of up to FIXED_MAX_SAMPLES samples per pixel); the sum is exact, whatever the
+// order the samples arrive in, and is rounded to f64 once by the conversion kernel.
+constexpr int FIXED_WORDS = 9;
+constexpr uint32_t FIXED_MAX_SAMPLES = 1u << 22;  // samples of one pixel in one launch
+constexpr float FIXED_MAX_VALUE = 4.611686018427387904e18f;  // 2^62: larger samples are dropped
+
 // One frame-tracing launch over the pixels [pixel_begin, pixel_begin + n_pixels).
 struct TraceLaunch {
     ix_scene scene;            // `planes` is a device pointer here
@@ -60,19 +88,23 @@ struct TraceLaunch {
     uint32_t n_pixels;
     uint32_t sample_offset;
     uint32_t spp;
-    uint32_t pixels_per_task;  // consecutive pixels one warp task covers
+    uint32_t pixels_per_task;  // consecutive pixels one warp task covers (SHAPE_TASKS)
     double* out;               // device, n_pixels * 3 per-pixel sums
     int accumulate;            // 1: out += sums, 0: out = sums
     uint32_t* task_counter;    // device, zeroed by the launcher
     unsigned long long* dropped;  // device, non-finite samples dropped (may be null)
+    unsigned long long* acc;   // device, n_pixels * FIXED_WORDS fixed-point sums (pool shapes)
     int blocks;                // persistent grid size
     int threads;               // threads per block (multiple of 32)
-    int variant;               // register/occupancy variant: 0 unconstrained, 1 six blocks/SM, 2 eight
+    int variant;               // budget + 3 * shape (see LaunchShape)
 };
 
 // One job of a batched launch: `n_pixels` pixels of scene `scene` x `spp` samples from
-// `sample_offset`, split into tasks of `ppt` pixels starting at global task `task_begin`;
-// its per-pixel sums go to out + out_offset.
+// `sample_offset`; the static task loop splits it into tasks of `ppt` pixels starting at
+// global task `task_begin`, the path-pool loop into chunks of 32 paths (sample-major:
+// path i is sample i / n_pixels of pixel i % n_pixels) starting at global chunk
+// `chunk_begin`.  Its per-pixel sums go to out + out_offset (3 doubles per pixel) and,
+// for the path-pool loop, its fixed-point sums to acc + acc_offset (FIXED_WORDS per pixel).
 struct BatchJob {
     uint32_t scene;
     uint32_t n_pixels;
@@ -81,23 +113,35 @@ struct BatchJob {
     uint32_t task_begin;
     uint32_t sample_offset;
     uint64_t out_offset;
+    uint32_t chunk_begin;
+    uint32_t paths;
+    uint64_t acc_offset;
 };
 
 struct BatchLaunch {
     const ix_scene* scenes;      // device array; each scene's `planes` is a device pointer
     const uint32_t* flags;       // device, scene_flags per scene
     uint32_t uniaxial;           // any scene needs the uniaxial transport
-    const BatchJob* jobs;        // device, ascending task_begin
+    const BatchJob* jobs;        // device, ascending task_begin and chunk_begin
     uint32_t n_jobs;
     uint32_t total_tasks;
+    uint32_t total_chunks;
     double* out;
     int accumulate;
     uint32_t* task_counter;
     unsigned long long* dropped;
+    unsigned long long* acc;     // device, FIXED_WORDS per pixel of every job (pool shapes)
+    uint32_t stride;             // the k-th claim takes task / chunk k * stride (1: all of them;
+                                 // the autotuner times variants on a strided sample)
     int blocks;
     int threads;
-    int variant;
+    int variant;                 // budget + 3 * shape
 };
+
+// Rounds fixed-point sums to f64 (out = sum, or out += sum with `accumulate`), one
+// thread per pixel component.
+cudaError_t launch_fixed_to_f64(const unsigned long long* acc, double* out, uint64_t n_pixels, int accumulate,
+                                cudaStream_t stream);
 
 // Per-function check kernels: evaluate one reference function per input row on the
 // device so the host can compare against the CPU oracle value by value.
@@ -191,6 +235,17 @@ cudaError_t launch_batch_exact(const BatchLaunch& l, cudaStream_t stream);
 cudaError_t launch_batch_fast(const BatchLaunch& l, cudaStream_t stream);
 int batch_blocks_per_sm_exact(int threads, int variant, int uniaxial);
 int batch_blocks_per_sm_fast(int threads, int variant, int uniaxial);
+// The path-pool kernels (ix_pool.cu), dispatched to by launch_trace_* / launch_batch_*
+// for the pool shapes.  A variant a build does not carry returns cudaErrorInvalidValue
+// (the exact build carries the 128-thread pool shape only).
+cudaError_t launch_pool_trace_exact(const TraceLaunch& l, cudaStream_t stream);
+cudaError_t launch_pool_trace_fast(const TraceLaunch& l, cudaStream_t stream);
+cudaError_t launch_pool_batch_exact(const BatchLaunch& l, cudaStream_t stream);
+cudaError_t launch_pool_batch_fast(const BatchLaunch& l, cudaStream_t stream);
+int pool_trace_blocks_per_sm_exact(int variant, int uniaxial);
+int pool_trace_blocks_per_sm_fast(int variant, int uniaxial);
+int pool_batch_blocks_per_sm_exact(int variant, int uniaxial);
+int pool_batch_blocks_per_sm_fast(int variant, int uniaxial);
 cudaError_t launch_check_exact(const CheckLaunch& l, cudaStream_t stream);
 cudaError_t launch_check_fast(const CheckLaunch& l, cudaStream_t stream);
 // Occupancy-derived resident blocks per SM for the trace kernel at `threads` per block

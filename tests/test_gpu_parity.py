@@ -452,7 +452,7 @@ def test_batch_plan_one_launch_matches_single_scene_calls(backend):
         assert backend.try_accumulate(fs, off, spp, single)
         assert np.array_equal(plan.sums(j), single)
     chosen = plan.autotune(reps=1)
-    assert chosen in (0, 1, 2)
+    assert 0 <= chosen < 12  # budget + 3 * shape: static tasks, or the path pool at 128 / 64 / 256 threads
     # The register variants are separate compilations; in the fused-rounding build their
     # multiply-add contraction may differ, so bits are compared within a variant and the
     # variants against each other statistically.
