@@ -24,6 +24,9 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#if defined(IX_ORACLE_AVX2) && !defined(IX_COUNT_FLOPS)
+#include <immintrin.h>
+#endif
 #include <cstdint>
 #include <cstring>
 #include <thread>
@@ -662,10 +665,88 @@ struct Hit {
     V3 normal;
     int facet;
 };
+#if defined(IX_ORACLE_AVX2) && !defined(IX_COUNT_FLOPS)
+// The AVX2 twin of the slab scan (simd/slab.rs:200-290, slab_scan_avx2): 8 planes per
+// block with the scalar operation order (left-associated dot products, separate
+// multiply and add, an IEEE division), the block's entering max / exiting min checked
+// against the running state, and only blocks that could change it replayed through the
+// scalar step in ascending plane order -- bit-identical to the scalar scan.  Planes are
+// read in this library's {nx, ny, nz, d} rows and transposed in registers.
+static inline float hmax8(__m256 v) {
+    __m128 m = _mm_max_ps(_mm256_castps256_ps128(v), _mm256_extractf128_ps(v, 1));
+    m = _mm_max_ps(m, _mm_movehl_ps(m, m));
+    m = _mm_max_ps(m, _mm_shuffle_ps(m, m, 0x01));
+    return _mm_cvtss_f32(m);
+}
+static inline float hmin8(__m256 v) {
+    __m128 m = _mm_min_ps(_mm256_castps256_ps128(v), _mm256_extractf128_ps(v, 1));
+    m = _mm_min_ps(m, _mm_movehl_ps(m, m));
+    m = _mm_min_ps(m, _mm_shuffle_ps(m, m, 0x01));
+    return _mm_cvtss_f32(m);
+}
+#endif
+
 static bool intersect(const float* planes, uint32_t n, const Ray& ray, Hit* hit) {
     F t_near = -1e30f, t_far = 1e30f;
     int near_idx = -1, far_idx = -1;
-    for (uint32_t i = 0; i < n; ++i) {
+    uint32_t i0 = 0;
+#if defined(IX_ORACLE_AVX2) && !defined(IX_COUNT_FLOPS)
+    {
+        const __m256 dx = _mm256_set1_ps(ray.dir.x), dy = _mm256_set1_ps(ray.dir.y), dz = _mm256_set1_ps(ray.dir.z);
+        const __m256 ox = _mm256_set1_ps(ray.origin.x), oy = _mm256_set1_ps(ray.origin.y),
+                     oz = _mm256_set1_ps(ray.origin.z);
+        const __m256 thr = _mm256_set1_ps(1e-7f), sign = _mm256_set1_ps(-0.0f), zero = _mm256_setzero_ps();
+        const __m256 neg_inf = _mm256_set1_ps(-INFINITY), pos_inf = _mm256_set1_ps(INFINITY);
+        alignas(32) float den_l[8], side_l[8], t_l[8];
+        for (; i0 + 8 <= n; i0 += 8) {
+            const float* b = planes + 4 * (size_t)i0;
+            const __m256 r0 = _mm256_insertf128_ps(_mm256_castps128_ps256(_mm_loadu_ps(b)), _mm_loadu_ps(b + 16), 1);
+            const __m256 r1 = _mm256_insertf128_ps(_mm256_castps128_ps256(_mm_loadu_ps(b + 4)), _mm_loadu_ps(b + 20), 1);
+            const __m256 r2 = _mm256_insertf128_ps(_mm256_castps128_ps256(_mm_loadu_ps(b + 8)), _mm_loadu_ps(b + 24), 1);
+            const __m256 r3 = _mm256_insertf128_ps(_mm256_castps128_ps256(_mm_loadu_ps(b + 12)), _mm_loadu_ps(b + 28), 1);
+            const __m256 t0 = _mm256_unpacklo_ps(r0, r1), t1 = _mm256_unpackhi_ps(r0, r1);
+            const __m256 t2 = _mm256_unpacklo_ps(r2, r3), t3 = _mm256_unpackhi_ps(r2, r3);
+            const __m256 nx = _mm256_shuffle_ps(t0, t2, 0x44), ny = _mm256_shuffle_ps(t0, t2, 0xEE);
+            const __m256 nz = _mm256_shuffle_ps(t1, t3, 0x44), d = _mm256_shuffle_ps(t1, t3, 0xEE);
+            const __m256 denom =
+                _mm256_add_ps(_mm256_add_ps(_mm256_mul_ps(nx, dx), _mm256_mul_ps(ny, dy)), _mm256_mul_ps(nz, dz));
+            const __m256 dot_o =
+                _mm256_add_ps(_mm256_add_ps(_mm256_mul_ps(nx, ox), _mm256_mul_ps(ny, oy)), _mm256_mul_ps(nz, oz));
+            const __m256 side = _mm256_add_ps(d, dot_o);
+            const __m256 t = _mm256_div_ps(_mm256_xor_ps(side, sign), denom);  // (-side) / denom
+            const __m256 absd = _mm256_andnot_ps(sign, denom);
+            const __m256 valid = _mm256_cmp_ps(absd, thr, _CMP_GT_OQ);
+            const __m256 par_out =
+                _mm256_and_ps(_mm256_cmp_ps(absd, thr, _CMP_LE_OQ), _mm256_cmp_ps(side, zero, _CMP_GT_OQ));
+            if (_mm256_movemask_ps(par_out) != 0) return false;  // parallel plane, origin outside
+            const __m256 entering = _mm256_and_ps(valid, _mm256_cmp_ps(denom, zero, _CMP_LT_OQ));
+            const __m256 exiting = _mm256_andnot_ps(entering, valid);
+            const float ent_max = hmax8(_mm256_blendv_ps(neg_inf, t, entering));
+            const float ex_min = hmin8(_mm256_blendv_ps(pos_inf, t, exiting));
+            if (!(ent_max > t_near || ex_min < t_far)) continue;  // the block changes nothing
+            _mm256_store_ps(den_l, denom);
+            _mm256_store_ps(side_l, side);
+            _mm256_store_ps(t_l, t);
+            for (int k = 0; k < 8; ++k) {
+                const F denom_k = den_l[k];
+                if (abs_(denom_k) > F(1e-7f)) {
+                    if (denom_k < F(0.0f)) {
+                        if (F(t_l[k]) > t_near) {
+                            t_near = t_l[k];
+                            near_idx = (int)(i0 + k);
+                        }
+                    } else if (F(t_l[k]) < t_far) {
+                        t_far = t_l[k];
+                        far_idx = (int)(i0 + k);
+                    }
+                } else if (F(side_l[k]) > F(0.0f)) {
+                    return false;
+                }
+            }
+        }
+    }
+#endif
+    for (uint32_t i = i0; i < n; ++i) {
         V3 nrm = load3(planes + 4 * i);
         F denom = dot(nrm, ray.dir);
         F side = F(planes[4 * i + 3]) + dot(nrm, ray.origin);
@@ -1709,12 +1790,46 @@ static void channel_alphas(const Path& P, F alpha[8]) {
         for (int c = 0; c < 8; ++c) alpha[c] = quadratic_form(tf, P.alpha_ch_o[c], P.alpha_ch_e[c], e_mode);
     }
 }
+#if defined(IX_ORACLE_AVX2) && !defined(IX_COUNT_FLOPS)
+// exp_f32x8 (simd/exp_poly.rs:122), the AVX2 level: exp_lane's steps on 8 lanes at once
+// (the clamp with _mm256_min/max_ps's second-operand rule, floor of x log2e + 1/2, the
+// two-constant reduction and the polynomial with fused multiply-adds, 2^n from the
+// exponent bits) -- bit-identical to exp_lane per lane.
+static void exp8(const float in[8], float out[8]) {
+    uint32_t c1bits = 0x3F318000u;
+    float c1f;
+    std::memcpy(&c1f, &c1bits, 4);
+    __m256 x = _mm256_loadu_ps(in);
+    x = _mm256_min_ps(x, _mm256_set1_ps(88.02875f));
+    x = _mm256_max_ps(x, _mm256_set1_ps(-87.33654f));
+    const __m256 n = _mm256_floor_ps(_mm256_fmadd_ps(x, _mm256_set1_ps(1.44269504088896340736f), _mm256_set1_ps(0.5f)));
+    x = _mm256_fmadd_ps(n, _mm256_set1_ps(-c1f), x);
+    x = _mm256_fmadd_ps(n, _mm256_set1_ps(2.1219444e-4f), x);
+    const __m256 z = _mm256_mul_ps(x, x);
+    __m256 p = _mm256_set1_ps(1.9875691e-4f);
+    p = _mm256_fmadd_ps(p, x, _mm256_set1_ps(1.3981999e-3f));
+    p = _mm256_fmadd_ps(p, x, _mm256_set1_ps(8.333452e-3f));
+    p = _mm256_fmadd_ps(p, x, _mm256_set1_ps(4.1665796e-2f));
+    p = _mm256_fmadd_ps(p, x, _mm256_set1_ps(1.6666665e-1f));
+    p = _mm256_fmadd_ps(p, x, _mm256_set1_ps(5.0000003e-1f));
+    p = _mm256_add_ps(_mm256_fmadd_ps(p, z, x), _mm256_set1_ps(1.0f));
+    const __m256i e = _mm256_slli_epi32(_mm256_add_epi32(_mm256_cvttps_epi32(n), _mm256_set1_epi32(127)), 23);
+    _mm256_storeu_ps(out, _mm256_mul_ps(p, _mm256_castsi256_ps(e)));
+}
+#endif
 static void apply_absorption(Path& P, F path_len) {
     const ix_material& m = P.sc->material;
     F alpha[8];
     channel_alphas(P, alpha);
     F scaled_len = path_len * F(m.absorption_path_scale);
+#if defined(IX_ORACLE_AVX2) && !defined(IX_COUNT_FLOPS)
+    float arg[8], e[8];
+    for (int c = 0; c < 8; ++c) arg[c] = -alpha[c] * scaled_len;
+    exp8(arg, e);
+    for (int c = 0; c < 8; ++c) P.stokes[c] = scale(P.stokes[c], e[c]);
+#else
     for (int c = 0; c < 8; ++c) P.stokes[c] = scale(P.stokes[c], exp_lane(-alpha[c] * scaled_len));
+#endif
 }
 
 enum { TERM_ESCAPED = 0, TERM_RR = 1, TERM_CAP = 2 };
@@ -2699,6 +2814,64 @@ void ixo_fresnel_reflect_apply(float r_s, float r_p, const float s_in[4], float 
     s_out[2] = raw(o.u);
     s_out[3] = raw(o.v);
 }
+float ixo_spectral_absorption(const ix_absorption* a, float lambda_nm) { return raw(spectral_absorption(*a, lambda_nm)); }
+
+void ixo_rotate_stokes(const float k[3], const float normal[3], const float prev_pn[3], uint32_t has_prev,
+                       const float s_in[4], float s_out[4], float cpn_out[3]) {
+    // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:69) as facet_event calls it.
+    const V3 kk = load3(k), nn = load3(normal), prev = load3(prev_pn);
+    Stokes st{s_in[0], s_in[1], s_in[2], s_in[3]};
+    const V3 cpn = normalize_or_zero(cross(kk, nn));
+    if (has_prev && length_squared(cpn) > F(1e-6f) && length_squared(prev) > F(1e-6f)) {
+        F cos_psi = clamp_(dot(prev, cpn), -1.0f, 1.0f);
+        F sin_psi = dot(cross(prev, cpn), normalize_or_zero(kk));
+        st = apply(frame_rotation(atan2_(sin_psi, cos_psi)), st);
+    }
+    s_out[0] = raw(st.i), s_out[1] = raw(st.q), s_out[2] = raw(st.u), s_out[3] = raw(st.v);
+    store3(cpn_out, cpn);
+}
+
+void ixo_fresnel_channel(float n1, float n2, float cos_i, const float s_in[4], float out[13]) {
+    // One channel of apply_partial_reflect_bounce / apply_tir_bounce (reflected Stokes,
+    // before the 1 / r_unpol selection weight) and of apply_refract_channel (transmitted
+    // Stokes, before 1 / (1 - r_unpol)), with the same geometry the bounce computes.
+    const Stokes st{s_in[0], s_in[1], s_in[2], s_in[3]};
+    const F one_m_c2 = fma_(F(cos_i), -F(cos_i), 1.0f);
+    const F sin_i = sqrt_(max_(one_m_c2, 0.0f));
+    const F eta = F(n1) / F(n2);
+    const F s2 = eta * eta * one_m_c2;
+    for (int i = 0; i < 13; ++i) out[i] = 0.0f;
+    if (s2 > F(1.0f)) {
+        const Stokes r = apply(tir_retardation(tir_phase_delta(n1, cos_i, sin_i)), st);
+        out[0] = raw(r.i), out[1] = raw(r.q), out[2] = raw(r.u), out[3] = raw(r.v);
+        out[12] = 1.0f;
+        return;
+    }
+    const F cos_t = sqrt_(max_(F(1.0f) - s2, 0.0f));
+    F r_s, r_p;
+    fresnel_rs_rp(n1, n2, cos_i, cos_t, &r_s, &r_p);
+    const Stokes r = apply(fresnel_reflection(r_s, r_p), st);
+    const F two = F(2.0f) * F(n1) * F(cos_i);
+    const F t_s = two / fma_(F(n2), cos_t, F(n1) * F(cos_i));
+    const F t_p = two / fma_(F(n1), cos_t, F(n2) * F(cos_i));
+    const Stokes t = apply(fresnel_transmission(n1, n2, cos_i, cos_t, t_s, t_p), st);
+    out[0] = raw(r.i), out[1] = raw(r.q), out[2] = raw(r.u), out[3] = raw(r.v);
+    out[4] = raw(t.i), out[5] = raw(t.q), out[6] = raw(t.u), out[7] = raw(t.v);
+    out[8] = raw(r_s), out[9] = raw(r_p), out[10] = raw(t_s), out[11] = raw(t_p);
+}
+
+float ixo_channel_alpha(const ix_material* m, const float k[3], float lambda_nm) {
+    // The non-birefringent branch of channel_absorption_alphas_assigned
+    // (raytracer/absorption.rs:197): the midpoint of the tensor's quadratic form over the
+    // two eigen-polarisations of the wave normal.
+    const V3 c_axis = load3(m->c_axis), kk = load3(k);
+    const F ao = spectral_absorption(m->abs_o, lambda_nm), ae = spectral_absorption(m->abs_e, lambda_nm);
+    const TensorFrame tf = tensor_frame(c_axis);
+    const V3 ea = ordinary_eigen_polarization(kk, c_axis);
+    const V3 eb = normalize_or_zero(cross(kk, ea));
+    return raw(midpoint_(quadratic_form(tf, ao, ae, ea), quadratic_form(tf, ao, ae, eb)));
+}
+
 int ixo_intersect(const float* planes, uint32_t n_planes, const float origin[3],
                   const float dir[3], float* t, int32_t* facet) {
     Ray r{load3(origin), load3(dir)};
@@ -2996,6 +3169,57 @@ int64_t ixo_trace_pixels(const ix_scene* scene, uint32_t pixel_begin, uint32_t p
     int64_t total = 0;
     for (auto d : dropped) total += d;
     return total;
+}
+
+int64_t ixo_trace_pixel_set(const ix_scene* scenes, uint32_t n_scenes, const uint32_t* scene_of,
+                            const uint32_t* pixel, const uint32_t* spp, uint32_t n, uint32_t sample_offset,
+                            uint32_t threads, double* sums_f64) {
+    for (uint32_t i = 0; i < n_scenes; ++i)
+        if (!scene_supported(&scenes[i])) return -1;
+    for (uint32_t k = 0; k < n; ++k)
+        if (scene_of[k] >= n_scenes || pixel[k] >= scenes[scene_of[k]].width * scenes[scene_of[k]].height) return -1;
+    if (threads == 0) threads = 1;
+    std::atomic<uint32_t> next{0};
+    std::vector<int64_t> dropped(threads, 0);
+    auto worker = [&](uint32_t t) {
+        for (;;) {
+            const uint32_t k = next.fetch_add(1, std::memory_order_relaxed);
+            if (k >= n) break;
+            const ix_scene* sc = &scenes[scene_of[k]];
+            Rot rot = pixel_rotations(pixel[k]);
+            double sd[3] = {0.0, 0.0, 0.0};
+            for (uint32_t s = 0; s < spp[k]; ++s) {
+                V3 xyz = sample_xyz(sc, pixel[k], rot, sample_offset + s, nullptr);
+                if (xyz_finite(xyz)) {
+                    sd[0] += (double)raw(xyz.x);
+                    sd[1] += (double)raw(xyz.y);
+                    sd[2] += (double)raw(xyz.z);
+                } else {
+                    dropped[t]++;
+                }
+            }
+            if (sums_f64) {
+                sums_f64[3 * (size_t)k] = sd[0];
+                sums_f64[3 * (size_t)k + 1] = sd[1];
+                sums_f64[3 * (size_t)k + 2] = sd[2];
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < threads; ++t) pool.emplace_back(worker, t);
+    worker(0);
+    for (auto& th : pool) th.join();
+    int64_t total = 0;
+    for (auto d : dropped) total += d;
+    return total;
+}
+
+int ixo_simd_build(void) {
+#if defined(IX_ORACLE_AVX2) && !defined(IX_COUNT_FLOPS)
+    return 1;
+#else
+    return 0;
+#endif
 }
 
 int ixo_trace_samples(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_end,

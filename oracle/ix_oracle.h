@@ -69,6 +69,20 @@ float ixo_exp_lane(float x);
 /* polarization.rs + refraction/tir.rs: Fresnel amplitude coefficients and TIR phase */
 float ixo_tir_phase_delta(float n1, float cos_i, float sin_i);
 void ixo_fresnel_reflect_apply(float r_s, float r_p, const float s_in[4], float s_out[4]);
+/* spectral_absorption: alpha(lambda) of one eigenmode (Gaussian bands + the spline). */
+float ixo_spectral_absorption(const ix_absorption* a, float lambda_nm);
+/* rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:69) as facet_event calls
+ * it: the new plane-of-incidence normal normalize_or_zero(k x n) and, when there is a
+ * previous one, the Stokes vector rotated by frame_rotation(psi). */
+void ixo_rotate_stokes(const float k[3], const float normal[3], const float prev_pn[3], uint32_t has_prev,
+                       const float s_in[4], float s_out[4], float cpn_out[3]);
+/* One channel's Fresnel step at (n1, n2, cos_i): out[0..3] the reflected Stokes vector
+ * (the TIR retarder past the critical angle), out[4..7] the transmitted one, out[8..11]
+ * r_s, r_p, t_s, t_p, out[12] 1 for TIR (then out[4..11] are 0). */
+void ixo_fresnel_channel(float n1, float n2, float cos_i, const float s_in[4], float out[13]);
+/* A non-birefringent material's channel alpha along wave normal k
+ * (channel_absorption_alphas_assigned, raytracer/absorption.rs:197). */
+float ixo_channel_alpha(const ix_material* m, const float k[3], float lambda_nm);
 /* simd/slab.rs:147 + intersect.rs:101: returns 1 and fills t/idx on a hit */
 int ixo_intersect(const float* planes, uint32_t n_planes, const float origin[3],
                   const float dir[3], float* t, int32_t* facet);
@@ -99,6 +113,17 @@ int64_t ixo_trace_frame(const ix_scene* scene, uint32_t sample_offset, uint32_t 
 int64_t ixo_trace_pixels(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_end,
                          uint32_t sample_offset, uint32_t spp, uint32_t threads,
                          double* sums_f64);
+/* A set of (scene, pixel) entries, each traced over samples [sample_offset,
+ * sample_offset + spp[k]) as renderer/cpu_frame.rs:45 traces them, entries claimed one at
+ * a time by `threads` host threads.  Per-entry f64 sums go to sums_f64 (3 per entry) when
+ * it is not NULL.  Returns the dropped non-finite samples, or -1 on an unsupported scene
+ * or an out-of-range entry. */
+int64_t ixo_trace_pixel_set(const ix_scene* scenes, uint32_t n_scenes, const uint32_t* scene_of,
+                            const uint32_t* pixel, const uint32_t* spp, uint32_t n, uint32_t sample_offset,
+                            uint32_t threads, double* sums_f64);
+/* 1 for the build with the AVX2 twins of the slab scan and the 8-lane exp (simd/slab.rs,
+ * simd/exp_poly.rs), 0 for the scalar build. */
+int ixo_simd_build(void);
 /* Per-sample XYZ of the pixels [pixel_begin, pixel_end) x samples, row-major
  * [pixel][sample][3], for path-level comparisons. */
 int ixo_trace_samples(const ix_scene* scene, uint32_t pixel_begin, uint32_t pixel_end,

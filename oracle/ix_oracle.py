@@ -143,6 +143,16 @@ def _load(name: str) -> C.CDLL:
     lib.ixo_attribute_pixels.argtypes = [P(abi.Scene), C.c_int32, C.c_float, C.c_float, C.c_float,
                                          C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                          C.c_void_p, P(C.c_double)]
+    lib.ixo_trace_pixel_set.restype = C.c_int64
+    lib.ixo_trace_pixel_set.argtypes = [P(abi.Scene), C.c_uint32, P(C.c_uint32), P(C.c_uint32), P(C.c_uint32),
+                                        C.c_uint32, C.c_uint32, C.c_uint32, P(C.c_double)]
+    lib.ixo_simd_build.restype = C.c_int
+    lib.ixo_spectral_absorption.restype = C.c_float
+    lib.ixo_spectral_absorption.argtypes = [P(abi.Absorption), C.c_float]
+    lib.ixo_rotate_stokes.argtypes = [f32p, f32p, f32p, C.c_uint32, f32p, f32p, f32p]
+    lib.ixo_fresnel_channel.argtypes = [C.c_float, C.c_float, C.c_float, f32p, f32p]
+    lib.ixo_channel_alpha.restype = C.c_float
+    lib.ixo_channel_alpha.argtypes = [P(abi.Material), f32p, C.c_float]
     lib.ixo_counting_build.restype = C.c_int
     lib.ixo_count_flops.restype = C.c_int
     lib.ixo_count_flops.argtypes = [P(abi.Scene), C.c_uint32, C.c_uint32, C.c_uint32,
@@ -173,6 +183,44 @@ def lib() -> C.CDLL:
 
 def counting_lib() -> C.CDLL:
     return _load("libix_oracle_count.so")
+
+
+def host_has_avx2() -> bool:
+    """True when this host's CPU reports AVX2 and FMA (the AVX2 build's instructions)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    return "avx2" in flags and "fma" in flags
+    except OSError:
+        pass
+    return False
+
+
+def simd_lib() -> C.CDLL:
+    """The AVX2 build (bit-identical to lib()) on hosts with AVX2 and FMA, else lib()."""
+    return _load("libix_oracle_avx2.so") if host_has_avx2() else lib()
+
+
+def trace_pixel_set(scenes, entries, sample_offset: int = 0, threads: int = 0, library=None, sums: bool = False):
+    """Traces (scene index, pixel, spp) entries over ``scenes`` (abi.Scene list), claimed one
+    at a time by ``threads`` host threads (0: all).  Returns (paths traced, dropped, per-entry
+    f64 sums or None)."""
+    if threads <= 0:
+        threads = os.cpu_count() or 1
+    library = library or lib()
+    arr = (abi.Scene * len(scenes))(*scenes)
+    e = np.ascontiguousarray(entries, np.uint32).reshape(-1, 3)
+    cols = [np.ascontiguousarray(e[:, i]) for i in range(3)]
+    out = np.zeros((e.shape[0], 3), np.float64) if sums else None
+    u32p = C.POINTER(C.c_uint32)
+    rc = library.ixo_trace_pixel_set(arr, len(scenes), cols[0].ctypes.data_as(u32p), cols[1].ctypes.data_as(u32p),
+                                     cols[2].ctypes.data_as(u32p), e.shape[0], sample_offset, threads,
+                                     out.ctypes.data_as(C.POINTER(C.c_double)) if sums else None)
+    if rc < 0:
+        raise ValueError("scene not supported by the oracle, or an entry out of range")
+    return int(cols[2].astype(np.uint64).sum()), int(rc), out
 
 
 def _f32p(a: np.ndarray):

@@ -301,3 +301,51 @@ def test_white_furnace_target(oracle):
         target += out * L0
     target /= 106.856
     assert np.all(np.abs(mean - target) / target < 0.02), (mean, target)
+
+
+def test_avx2_twins_bit_identical_to_the_scalar_oracle(oracle):
+    """The reference's determinism contract (simd/mod.rs:7-27; slab.rs tests): the AVX2
+    slab scan and the 8-lane exp give the scalar code's bits.  The slab scan on random
+    plane sets of 1-100 planes with planes parallel to the ray sprinkled in, and whole
+    sample sets of the benchmark's stones (absorbing and clear, all tilts), through both
+    builds."""
+    import ctypes as C
+
+    from indicatrix_b200 import workloads
+
+    if not oracle.host_has_avx2():
+        pytest.skip("host without AVX2 / FMA")
+    scalar, simd = oracle.lib(), oracle.simd_lib()
+    assert scalar.ixo_simd_build() == 0 and simd.ixo_simd_build() == 1
+    rng = np.random.default_rng(7)
+    t, f = C.c_float(), C.c_int32()
+    for count in (1, 5, 8, 9, 16, 17, 40, 100):
+        for _ in range(40):
+            d = rng.uniform(-1, 1, 3).astype(np.float32)
+            d /= max(np.linalg.norm(d), 1e-3)
+            n = rng.uniform(-1, 1, (count, 3)).astype(np.float32)
+            for i in range(3, count, 9):  # exactly parallel to the ray
+                fb = np.float32([1, 0, 0]) if abs(d[0]) < 0.9 else np.float32([0, 1, 0])
+                n[i] = np.cross(d, fb)
+            n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-3)
+            planes = np.concatenate([n, rng.uniform(-1, 1, (count, 1))], axis=1).astype(np.float32)
+            o = (rng.uniform(-1, 1, 3) * 3).astype(np.float32)
+            res = []
+            for lib in (scalar, simd):
+                hit = lib.ixo_intersect(oracle._f32p(planes), count, oracle._f32p(o.copy()), oracle._f32p(d.copy()),
+                                        C.byref(t), C.byref(f))
+                res.append((hit, np.float32(t.value).view(np.uint32) if hit else 0, f.value if hit else -1))
+            assert res[0] == res[1], (count, res)
+    stones = workloads.random_stones(64)
+    scenes, entries, keep = [], [], []
+    for i, st in enumerate(stones[:8]):
+        for tilt in (0.0, 25.0, 40.0):
+            fs = workloads.tilted_scene(st, tilt, 128, 128, 32)
+            keep.append(fs)
+            scenes.append(fs.to_abi())
+            for p in rng.integers(0, 128 * 128, 6):
+                entries.append((len(scenes) - 1, int(p), 8))
+    _, _, a = oracle.trace_pixel_set(scenes, entries, threads=4, library=scalar, sums=True)
+    _, _, b = oracle.trace_pixel_set(scenes, entries, threads=4, library=simd, sums=True)
+    assert a.sum() > 0
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
