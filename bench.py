@@ -126,19 +126,19 @@ class ClockSampler:
 # ----------------------------------------------------------------------------------
 # Workloads
 # ----------------------------------------------------------------------------------
-def frame_workload():
+def frame_workload(builder=None):
     from indicatrix_b200 import workloads
 
-    fs = workloads.round_brilliant_frame(256, 256, 32)
+    fs = workloads.round_brilliant_frame(256, 256, 32, builder=builder)
     return [(fs, 64)], {"workload": "round brilliant frame 256x256 x 64 spp", "pixels": 65536,
                         "spp": 64, "planes": int(fs.planes.shape[0]), "material": "diamond",
                         "environment": "D65 hemisphere, 20 deg head shadow", "max_depth": 32}
 
 
-def stress_workload():
+def stress_workload(builder=None):
     from indicatrix_b200 import workloads
 
-    fs = workloads.anisotropic_stress_frame(512, 512, 64)
+    fs = workloads.anisotropic_stress_frame(512, 512, 64, builder=builder)
     return [(fs, 256)], {"workload": "anisotropic stress frame 512x512 x 256 spp", "pixels": 512 * 512,
                          "spp": 256, "planes": int(fs.planes.shape[0]),
                          "material": "uniaxial corundum (n_o 1.768, n_e 1.760, Sellmeier o/e), optic axis "
@@ -147,7 +147,7 @@ def stress_workload():
                          "environment": "D65 hemisphere, 20 deg head shadow", "max_depth": 64}
 
 
-def batch_workload(n_stones: int = 64):
+def batch_workload(n_stones: int = 64, builder=None):
     from indicatrix_b200 import workloads
 
     # The first n_stones of the same seeded sequence (64 is the benchmark; fewer make the
@@ -156,55 +156,99 @@ def batch_workload(n_stones: int = 64):
     items = []
     for st in stones:
         for tilt in workloads.TILTS_DEG:
-            items.append((workloads.tilted_scene(st, tilt, 128, 128, 32), st.spp))
+            items.append((workloads.tilted_scene(st, tilt, 128, 128, 32, builder=builder), st.spp))
     paths = sum(fs.width * fs.height * spp for fs, spp in items)
     return items, {"workload": f"{n_stones} random stones x 9 tilts x 128x128, spp in {{32,64,128,256}}",
                    "stones": n_stones, "tilts": 9, "paths": paths, "max_depth": 32}
 
 
+def workload_items(args, builder=None):
+    if args.workload == "batch":
+        return batch_workload(args.stones, builder)
+    return {"frame": frame_workload, "stress": stress_workload}[args.workload](builder)
+
+
 # ----------------------------------------------------------------------------------
 # CPU baseline: the oracle on the host cores, on a bounded sample of the workload.
 # ----------------------------------------------------------------------------------
-def cpu_baseline(items, seconds: float):
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ix_oracle
 
     ix_oracle.build()
+    return ix_oracle
+
+
+def cpu_entries(items, per_item: int, seed: int):
+    """A seeded sample with the GPU step's path distribution: `per_item` pixels drawn
+    uniformly from every scene of the workload, each with all its samples (so every scene
+    contributes in proportion to its paths)."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for k, (fs, spp) in enumerate(items):
+        for p in rng.integers(0, fs.width * fs.height, per_item):
+            rows.append((k, int(p), spp))
+    return np.array(rows, np.uint32)
+
+
+def cpu_trace(ixo, scenes, entries, threads):
+    lib = ixo.simd_lib()
+    t0 = time.perf_counter()
+    paths, _, _ = ixo.trace_pixel_set(scenes, entries, 0, threads, lib)
+    return paths, time.perf_counter() - t0
+
+
+def cpu_plan(ixo, items, scenes, seconds: float, threads: int, seed: int):
+    """Pixels per scene sized from a short calibration run so that tracing the sample on
+    `threads` host threads takes about `seconds`."""
+    probe = cpu_entries(items, max(2, 1024 // len(items)), seed ^ 0x5A5A)
+    paths, dt = cpu_trace(ixo, scenes, probe, threads)
+    rate = paths / max(dt, 1e-3)
+    mean_spp = sum(spp for _, spp in items) / len(items)
+    return max(1, int(round(rate * seconds / (mean_spp * len(items)))))
+
+
+def cpu_kind(ixo):
+    if ixo.simd_lib().ixo_simd_build():
+        return ("the oracle (the reference CPU tracer restated in C++, -O3, with its AVX2 slab-scan and "
+                "8-lane exp twins)")
+    return "the oracle (the reference CPU tracer restated in C++, -O3, scalar)"
+
+
+def cpu_baseline(items, seconds: float):
+    """All-core and single-core rates of the oracle on the workload's path distribution."""
+    ixo = _oracle()
     threads = os.cpu_count() or 1
-    # Scene after scene of the workload (a spread of the batch's stones and tilts): each
-    # traced over a band of rows through the middle of the frame (where the stone is),
-    # sized from a short calibration, until about `seconds` of wall time are spent.
-    order = items[:: max(1, len(items) // 16)] or items
-    total_paths, total_dt, scenes = 0, 0.0, 0
-    for fs, spp in order:
-        remaining = seconds - total_dt
-        if remaining <= 0.05 * seconds:
-            break
-        sc = fs.to_abi()
-        n_pix = fs.width * fs.height
-        t0 = time.perf_counter()
-        probe = min(n_pix, 256)
-        p0 = max(0, n_pix // 2 - probe // 2)
-        ix_oracle.trace_pixels(sc, p0, p0 + probe, 0, spp, threads)
-        dt = max(time.perf_counter() - t0, 1e-3)
-        want = int(probe / dt * remaining)
-        start = max(0, n_pix // 2 - want // 2)
-        end = min(n_pix, start + max(want, 1))
-        t0 = time.perf_counter()
-        ix_oracle.trace_pixels(sc, start, end, 0, spp, threads)
-        total_dt += time.perf_counter() - t0
-        total_paths += (end - start) * spp
-        scenes += 1
-    return {"value": total_paths / total_dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"central pixel bands of {scenes} scene(s) of the workload = {total_paths} paths, "
-                      f"{total_dt:.1f} s, C++ oracle -O3 on {threads} host threads"}
+    scenes = [fs.to_abi() for fs, _ in items]
+    per_item = cpu_plan(ixo, items, scenes, seconds, threads, seed=101)
+    entries = cpu_entries(items, per_item, 101)
+    paths, dt = cpu_trace(ixo, scenes, entries, threads)
+    per_item1 = cpu_plan(ixo, items, scenes, max(2.0, seconds / 3.0), 1, seed=202)
+    one = cpu_entries(items, per_item1, 202)
+    p1, d1 = cpu_trace(ixo, scenes, one, 1)
+    return {"value": paths / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "single_core": p1 / d1,
+            "sample": f"{per_item} pixels drawn uniformly from each of the {len(items)} scenes of the workload, "
+                      f"all their samples ({paths} paths, {dt:.1f} s on {threads} host threads; single core: "
+                      f"{per_item1} pixels per scene, {p1} paths, {d1:.1f} s); {cpu_kind(ixo)}"}
+
+
+def loaded_native_libraries():
+    """Shared objects under this repository mapped into this process (relative paths)."""
+    names = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if line.strip() else ""
+                if path.startswith(ROOT) and path.endswith(".so"):
+                    names.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(names)
 
 
 def count_flops(items):
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import ix_oracle
-
-    ix_oracle.build()
+    ixo = _oracle()
     total_f, total_p = 0, 0
     div = sqrt = transc = 0
     step = max(1, len(items) // 8)
@@ -215,7 +259,7 @@ def count_flops(items):
         stride = max(1, n_pix // (8192 // max(1, spp // 16)))
         while math.gcd(stride, fs.width) != 1:
             stride += 1
-        c = ix_oracle.count_flops(sc, 0, n_pix, stride, 0, spp)
+        c = ixo.count_flops(sc, 0, n_pix, stride, 0, spp)
         total_f += c.flops()
         total_p += c.paths
         div, sqrt, transc = div + c.div, sqrt + c.sqrt, transc + c.transcendental
@@ -226,47 +270,45 @@ def count_flops(items):
 # ----------------------------------------------------------------------------------
 # Reference arm
 # ----------------------------------------------------------------------------------
+REFERENCE_RUN_SECONDS = 150.0  # the whole --steps K --warmup W run of the reference arm
+
+
 def run_reference(args, items, cfg):
+    """The reference's CPU implementation of the path (restated in C++, see cpu_kind) on
+    every host thread: each step traces a fresh seeded sample with the GPU step's path
+    distribution, sized so the whole run takes about REFERENCE_RUN_SECONDS.  Scenes are
+    built by the oracle's own host formulas: nothing of the CUDA library is loaded."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import ix_oracle
-
-    ix_oracle.build()
+    ixo = _oracle()
     threads = os.cpu_count() or 1
-    # Each step: a central band of 4096 pixels (where the stone is) of the next scene of
-    # the workload, all its samples.
-    order = items[:: max(1, len(items) // 16)] or items
-
-    def band(k):
-        fs, spp = order[k % len(order)]
-        n_pix = fs.width * fs.height
-        px = max(1, min(n_pix, 4096))
-        start = max(0, n_pix // 2 - px // 2)
-        return fs.to_abi(), start, start + px, spp
-
+    scenes = [fs.to_abi() for fs, _ in items]
+    per_step = REFERENCE_RUN_SECONDS / max(1, args.steps + args.warmup)
+    per_item = cpu_plan(ixo, items, scenes, per_step, threads, seed=7)
     for w in range(args.warmup):
-        sc, s0, _, spp = band(w)
-        ix_oracle.trace_pixels(sc, s0, s0 + 64, 0, spp, threads)
+        cpu_trace(ixo, scenes, cpu_entries(items, per_item, 1000 + w), threads)
     times, paths = [], 0
     for k in range(args.steps):
-        sc, s0, s1, spp = band(k)
-        t0 = time.perf_counter()
-        ix_oracle.trace_pixels(sc, s0, s1, 0, spp, threads)
-        times.append(time.perf_counter() - t0)
-        paths += (s1 - s0) * spp
+        p, dt = cpu_trace(ixo, scenes, cpu_entries(items, per_item, 2000 + k), threads)
+        times.append(dt)
+        paths += p
     value = paths / sum(times)
+    libs = loaded_native_libraries()
+    if any("libix_cuda" in n for n in libs):
+        raise RuntimeError(f"the reference arm loaded the CUDA library: {libs}")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"per step a central band of 4096 pixels x all samples of the next "
-                                   f"workload scene ({paths} paths in {args.steps} steps); the reference "
-                                   "(Rust) cannot be built here, its CPU tracer restated in C++ is timed"},
+                         "sample": f"per step {per_item} fresh pixels drawn uniformly from each of the "
+                                   f"{len(items)} scenes of the workload, all their samples ({paths} paths in "
+                                   f"{args.steps} steps); {cpu_kind(ixo)}; the reference (Rust) cannot be "
+                                   "built here"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "native_libraries": libs,
     }), flush=True)
 
 
@@ -488,20 +530,42 @@ def main_display(args):
 # ----------------------------------------------------------------------------------
 # Our arm
 # ----------------------------------------------------------------------------------
+# DRAM read + write bytes per pixel of one trace-kernel launch, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on a small case of the same kernel, and
+# how that case was taken.
+DRAM_BYTES_PER_PIXEL = {"batch": 11.75, "stress": 19.7}
+TRAFFIC_SOURCE = {
+    "batch": "ncu capture of the batch kernel on the first 4 stones x 9 tilts (589,824 pixels), "
+             "per-pixel bytes scaled to this launch's pixels",
+    "stress": "ncu capture of the stress frame kernel at 128x128 x 256 spp, per-pixel bytes scaled to "
+              "this launch's pixels",
+}
+
+
+def device_tensor(torch, ptr: int, n: int, dev):
+    """A zero-copy torch view of `n` f64 at device address `ptr` (the library's buffer)."""
+
+    class _Buf:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                    "strides": None}
+
+    return torch.as_tensor(_Buf(), device=dev)
+
 def main():
     args = parse()
     if args.workload == "display":
         main_display(args)
         return
     rank, world, local = dist_env()
-    if args.workload == "batch":
-        items, cfg = batch_workload(args.stones)
-    else:
-        items, cfg = {"frame": frame_workload, "stress": stress_workload}[args.workload]()
-    cfg["parallelism"] = f"sample-range shards x{world}" if world > 1 else "single GPU"
     if args.impl == "reference":
+        # Scenes from the oracle's host formulas (Camera::new, the lighting presets): the
+        # reference arm runs the reference's CPU path only.
+        items, cfg = workload_items(args, builder=_oracle())
+        cfg["parallelism"] = f"sample-range shards x{world}" if world > 1 else "single GPU"
         run_reference(args, items, cfg)
         return
+    items, cfg = workload_items(args)
+    cfg["parallelism"] = f"sample-range shards x{world}" if world > 1 else "single GPU"
 
     import torch
 
@@ -528,16 +592,17 @@ def main():
     # the step events are recorded on it.
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
-    sample_base = rank * 1_000_000  # disjoint absolute sample ranges per rank
+    # Disjoint absolute sample ranges per rank: rank r traces [r spp, (r + 1) spp) of every
+    # scene, so rank order is first-sample order for the fold.
     dev_items = []
     plan = None
     if args.workload == "batch":
         from indicatrix_b200.backend import BatchPlan
 
-        plan = BatchPlan(backend, [(fs, sample_base, spp) for fs, spp in items])
+        plan = BatchPlan(backend, [(fs, rank * spp, spp) for fs, spp in items])
         cfg["autotuned_variant"] = plan.autotune(reps=1)
         n_out = sum(fs.width * fs.height * 3 for fs, _ in items)
-        result = torch.empty(0)
+        result = device_tensor(torch, plan.device_output(), n_out, dev)
     else:
         for fs, spp in items:
             sc = fs.to_abi()
@@ -551,17 +616,15 @@ def main():
         if plan is not None:
             plan.run(stream.cuda_stream)
         for sc, _planes, out, spp, _fs in dev_items:
-            rc = backend.accumulate_device(sc, sample_base + 0, spp, out.data_ptr(), False,
-                                           stream.cuda_stream)
+            rc = backend.accumulate_device(sc, rank * spp, spp, out.data_ptr(), False, stream.cuda_stream)
             if rc != 0:
                 raise RuntimeError(f"device trace declined: {backend.last_lost_reason()}")
-        if world > 1 and plan is None:
-            gathered = [torch.empty_like(result) for _ in range(world)]
-            torch.distributed.all_gather(gathered, result)
-            # fold in ascending first-sample order (rank order == first-sample order)
-            acc = gathered[0].clone()
-            for g in gathered[1:]:
-                acc += g
+        if world > 1:
+            # The exchange step: every rank's per-pixel f64 sums to rank 0 (NCCL gather),
+            # folded there in first-sample order.
+            from indicatrix_b200.dispatch import gather_fold
+
+            gather_fold(result)
 
     for k in range(args.warmup):
         step(k)
@@ -589,13 +652,12 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         mean_ms = float(t.item())
     value = world * total_paths / (mean_ms * 1e-3)
+    # Kernels of this library per step: the trace launch(es), plus the rounding of the
+    # fixed-point sums after each path-pool launch.
     if plan is not None:
-        launches_per_step = 1
+        launches_per_step = 2 if plan.variant >= 3 else 1
     else:
-        launches_per_step = 0
-        for fs, spp in items:
-            n = fs.width * fs.height * spp
-            launches_per_step += 1 + (1 if n > (1 << 20) else 0)
+        launches_per_step = backend.last_timing().launches
 
     # End-to-end through the public API with host buffers (H2D scenes and planes, D2H
     # per-pixel sums): try_accumulate for the frame, try_accumulate_batch for the batch.
@@ -607,12 +669,12 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         if plan is not None:
-            batch = [GpuBatchItem(fs, sample_base, spp, acc) for (fs, spp), acc in zip(items, accs)]
+            batch = [GpuBatchItem(fs, rank * spp, spp, acc) for (fs, spp), acc in zip(items, accs)]
             if backend.try_accumulate_batch_cancellable(batch) != 0:
                 raise RuntimeError(f"e2e batch declined: {backend.last_lost_reason()}")
         else:
             for (fs, spp), acc in zip(items, accs):
-                if not backend.try_accumulate(fs, sample_base, spp, acc):
+                if not backend.try_accumulate(fs, rank * spp, spp, acc):
                     raise RuntimeError(f"e2e trace declined: {backend.last_lost_reason()}")
         t1 = time.perf_counter()
         if k >= max(1, args.warmup // 2):
@@ -630,13 +692,12 @@ def main():
         flops_per_path, flop_info = count_flops(items)
         # dominant kernel: the trace megakernel; per-launch algorithmic FLOPs / duration
         achieved = flops_per_path * total_paths / (mean_ms * 1e-3)
-        # DRAM bytes (read + write) per pixel from one ncu capture of a small case of the
-        # same kernel, scaled to a full launch by its pixels (the per-pixel f64 sums are the
-        # only DRAM traffic; planes and paths live on chip): profiles/*.md.
-        dram_bytes_per_pixel = {"batch": 11.75, "stress": 19.7}.get(args.workload)
+        # DRAM bytes (read + write) per pixel of the trace kernel, from one ncu capture of a
+        # small case of the same kernel and variant, scaled to this launch by its pixels
+        # (the per-pixel sums are the only DRAM traffic; planes and paths stay on chip).
+        dram_bytes_per_pixel = DRAM_BYTES_PER_PIXEL.get(args.workload)
         total_pixels = sum(fs.width * fs.height for fs, _ in items)
-        traffic = (dram_bytes_per_pixel * total_pixels / launches_per_step
-                   if dram_bytes_per_pixel is not None else None)
+        traffic = dram_bytes_per_pixel * total_pixels if dram_bytes_per_pixel is not None else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True,
@@ -651,6 +712,7 @@ def main():
             "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak / 1e12,
                          "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                          "traffic": traffic,
+                         "traffic_source": TRAFFIC_SOURCE.get(args.workload),
                          "peak_source": "measured by the FP32 FMA-chain probe kernel (FMA = 2 FLOP) "
                                         "in this run; MEASURED_PEAKS.json has no non-tensor FP32 figure",
                          "flops_per_path": flops_per_path, "flop_count": flop_info},

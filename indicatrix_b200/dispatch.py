@@ -129,6 +129,35 @@ class Merger:
             self._h = None
 
 
+def fold_in_order(parts):
+    """Merger::add's fold (merge/mod.rs:239) of per-rank sums that are contiguous sample
+    ranges in rank order -- rank r traced [r n, (r + 1) n) -- so rank order is ascending
+    first-sample order: left to right, each part added into the running sums.  Works on
+    numpy arrays and on torch tensors (on the device that holds them)."""
+    acc = parts[0].copy() if isinstance(parts[0], np.ndarray) else parts[0].clone()
+    for p in parts[1:]:
+        acc += p
+    return acc
+
+
+def gather_fold(sums, group=None):
+    """The one exchange step of a sharded render: every rank's per-pixel sums (a torch
+    tensor, the same shape on every rank) go to rank 0 with one gather over the process
+    group (NCCL over NVLink between GPUs, gloo on CPU), and rank 0 folds them in rank
+    order with fold_in_order.  Returns the folded sums on rank 0 and None on the others.
+    Every rank takes the same collective step."""
+    import torch
+    import torch.distributed as dist
+
+    rank = dist.get_rank(group)
+    world = dist.get_world_size(group)
+    parts = [torch.empty_like(sums) for _ in range(world)] if rank == 0 else None
+    dist.gather(sums, parts, dst=0, group=group)
+    if rank != 0:
+        return None
+    return fold_in_order(parts)
+
+
 def store_claim(store, key: str, start: int, end: int, want: int) -> Optional[Tuple[int, int]]:
     """A SampleCursor shared by every rank through a torch.distributed store: the store's
     atomic add hands out disjoint ranges of `want` samples."""

@@ -17,8 +17,8 @@ from typing import List
 
 import numpy as np
 
-from . import abi, geometry, materials
-from .backend import FrameScene, camera_new, environment_preset, PRESET_ISO_HEMISPHERE
+from . import abi, backend, geometry, materials
+from .backend import FrameScene, PRESET_ISO_HEMISPHERE
 
 FACE_UP_PITCH = np.float32(math.pi / 2.0)
 DEFAULT_FOV_DEG = 42.0
@@ -27,16 +27,32 @@ FACE_UP_DISTANCE = 1.6
 CM_PER_MODEL_UNIT = 0.65
 
 
-def iso_hemisphere(head_shadow_deg: float = 20.0) -> abi.Environment:
-    return environment_preset(PRESET_ISO_HEMISPHERE, 1.0, 0.0, 0.0, 0.0, 1.0, head_shadow_deg)
+# The host formulas that turn a pose into a camera and a lighting preset into an
+# environment (Camera::new, EnvironmentSource::Studio): by default this library's
+# (ix_camera_new / ix_environment_preset).  Any object with the same two functions --
+# camera_new(yaw, pitch, distance, fov_deg) and environment_preset(preset, exposure,
+# light_yaw, light_pitch, backdrop, surface_glare, head_shadow_deg) -- can stand in for it,
+# e.g. a CPU implementation that must not load the CUDA library.
+class _LibraryBuilder:
+    camera_new = staticmethod(backend.camera_new)
+    environment_preset = staticmethod(backend.environment_preset)
 
 
-def round_brilliant_frame(width: int = 256, height: int = 256, max_bounces: int = 32) -> FrameScene:
+LIBRARY_BUILDER = _LibraryBuilder()
+
+
+def iso_hemisphere(head_shadow_deg: float = 20.0, builder=None) -> abi.Environment:
+    b = builder or LIBRARY_BUILDER
+    return b.environment_preset(PRESET_ISO_HEMISPHERE, 1.0, 0.0, 0.0, 0.0, 1.0, head_shadow_deg)
+
+
+def round_brilliant_frame(width: int = 256, height: int = 256, max_bounces: int = 32, builder=None) -> FrameScene:
+    b = builder or LIBRARY_BUILDER
     planes = geometry.to_f32(geometry.round_brilliant())
-    cam = camera_new(0.0, float(FACE_UP_PITCH), FACE_UP_DISTANCE, DEFAULT_FOV_DEG)
+    cam = b.camera_new(0.0, float(FACE_UP_PITCH), FACE_UP_DISTANCE, DEFAULT_FOV_DEG)
     return FrameScene(camera=cam, width=width, height=height, planes=planes,
                       material=materials.diamond(), max_bounces=max_bounces,
-                      environment=iso_hemisphere())
+                      environment=iso_hemisphere(builder=b))
 
 
 @dataclass
@@ -128,24 +144,26 @@ def stress_material(seed: int = 7, tilt_deg: float = 30.0) -> abi.Material:
 
 
 def anisotropic_stress_frame(width: int = 512, height: int = 512, max_bounces: int = 64,
-                             seed: int = 7) -> FrameScene:
+                             seed: int = 7, builder=None) -> FrameScene:
     """The emerald step cut (3 crown + 3 pavilion tiers, 49 facets) in the stress
     material, face up under the D65 hemisphere with the 20-degree head shadow, max depth 64."""
+    b = builder or LIBRARY_BUILDER
     planes = geometry.to_f32(geometry.step_cut())
-    cam = camera_new(0.0, float(FACE_UP_PITCH), FACE_UP_DISTANCE, DEFAULT_FOV_DEG)
+    cam = b.camera_new(0.0, float(FACE_UP_PITCH), FACE_UP_DISTANCE, DEFAULT_FOV_DEG)
     return FrameScene(camera=cam, width=width, height=height, planes=planes,
                       material=stress_material(seed), max_bounces=max_bounces,
-                      environment=iso_hemisphere())
+                      environment=iso_hemisphere(builder=b))
 
 
 TILTS_DEG = [0.0, 5.0, 10.0, 15.0, 20.0, 25.0, 30.0, 35.0, 40.0]
 
 
 def tilted_scene(stone: StoneSpec, tilt_deg: float, width: int = 128, height: int = 128,
-                 max_bounces: int = 32) -> FrameScene:
+                 max_bounces: int = 32, builder=None) -> FrameScene:
     """The stone seen face-up with the camera tilted `tilt_deg` from the table normal."""
+    b = builder or LIBRARY_BUILDER
     pitch = float(np.float32(math.pi / 2.0 - math.radians(tilt_deg)))
-    cam = camera_new(0.0, pitch, FACE_UP_DISTANCE, DEFAULT_FOV_DEG)
+    cam = b.camera_new(0.0, pitch, FACE_UP_DISTANCE, DEFAULT_FOV_DEG)
     return FrameScene(camera=cam, width=width, height=height, planes=stone.planes,
                       material=stone.material, max_bounces=max_bounces,
-                      environment=iso_hemisphere())
+                      environment=iso_hemisphere(builder=b))

@@ -209,3 +209,67 @@ def test_two_rank_gloo_lanes_exchange_radiance_payloads(oracle):
         want = (want + s64.reshape(-1, 3).astype(np.float32)).astype(np.float32)
     assert want.sum() > 0
     assert np.array_equal(acc.view(np.uint32), want.view(np.uint32))
+
+
+def _rank_gather_main(rank, world, port, out_path):
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    sys.path.insert(0, os.path.join(root, "oracle"))
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import ix_oracle
+    from indicatrix_b200 import workloads
+    from indicatrix_b200.dispatch import gather_fold
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    # Two jobs of different spp, back to back in one buffer, as a batch plan lays them out:
+    # rank r traces samples [r spp_j, (r + 1) spp_j) of job j.
+    jobs = [(workloads.round_brilliant_frame(6, 5), 4), (workloads.round_brilliant_frame(4, 4), 7)]
+    parts = []
+    for fs, spp in jobs:
+        _, s64, _ = ix_oracle.trace_frame(fs.to_abi(), rank * spp, spp, threads=1)
+        parts.append(s64.reshape(-1))
+    mine = torch.from_numpy(np.concatenate(parts))
+    folded = gather_fold(mine)
+    if rank == 0:
+        with open(out_path, "wb") as f:
+            pickle.dump(folded.numpy(), f)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_gloo_gather_fold_equals_the_merger(oracle):
+    """The batch path's exchange step (bench.py under torchrun): each rank's per-pixel sums
+    of every job go to rank 0 in one gather and are folded in rank order; the result
+    equals Merger::add folding each job's two sample ranges in first-sample order, bit
+    for bit."""
+    import torch.multiprocessing as mp
+
+    from indicatrix_b200 import workloads
+    from indicatrix_b200.dispatch import Merger
+
+    port = _free_port()
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "res.pkl")
+        mp.start_processes(_rank_gather_main, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+        with open(out, "rb") as f:
+            got = pickle.load(f)
+    want = []
+    for (w, h), spp in (((6, 5), 4), ((4, 4), 7)):
+        fs = workloads.round_brilliant_frame(w, h)
+        m = Merger(w * h, 0)
+        for r in (1, 0):  # arrival order does not matter: the merger parks rank 1's chunk
+            _, s64, _ = oracle.trace_frame(fs.to_abi(), r * spp, spp, threads=1)
+            m.add(r * spp, spp, s64.reshape(-1))
+        sums, n = m.finish()
+        assert n == 2 * spp
+        want.append(sums)
+    want = np.concatenate(want)
+    assert want.sum() > 0
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
