@@ -1301,6 +1301,12 @@ int ix_debug_check(ix_backend* b, const ix_scene* scene, int32_t fn, uint32_t n,
                    const uint32_t* in, uint32_t in_stride, uint32_t* out, uint32_t out_stride) {
     if (!b || !scene || (n && (!in || !out))) return -1;
     if (scene->n_planes > IX_MAX_PLANES) return -1;
+    // 32-bit words each check function reads from / writes to a row (ix::CheckFn order):
+    // rows narrower than that are refused before anything reaches the device.
+    static const uint8_t kIn[] = {2, 1, 1, 1, 1, 1, 3, 7, 7, 6, 2, 2, 1, 8, 14, 7, 4};
+    static const uint8_t kOut[] = {4, 8, 1, 3, 1, 1, 1, 6, 1, 2, 4, 6, 1, 4, 7, 13, 1};
+    static_assert(sizeof(kIn) == ix::CHECK_CHANNEL_ALPHA + 1 && sizeof(kOut) == sizeof(kIn), "check table");
+    if (fn < 0 || fn >= (int32_t)sizeof(kIn) || in_stride < kIn[fn] || out_stride < kOut[fn]) return -1;
     Turn turn(b);
     if (fail(b, cudaSetDevice(b->device), "set device")) return -1;
     size_t in_words = (size_t)n * in_stride, out_words = (size_t)n * out_stride;

@@ -478,6 +478,65 @@ __global__ void IX_SFX(check_kernel)(const __grid_constant__ CheckLaunch L) {
             break;
         }
         case CHECK_ABSORPTION: put(0, spectral_absorption(S.s.material.abs_o, inf(0))); break;
+        case CHECK_STOKES_ROTATE: {
+            // The bounce's rotate_stokes_to_plane_of_incidence, as group_bounce calls it.
+            Stokes st{inf(10), inf(11), inf(12), inf(13)};
+            const V3 cpn = rotate_to_plane_of_incidence(st, in[9] != 0, v3(inf(6), inf(7), inf(8)),
+                                                        v3(inf(0), inf(1), inf(2)), v3(inf(3), inf(4), inf(5)));
+            put(0, st.i);
+            put(1, st.q);
+            put(2, st.u);
+            put(3, st.v);
+            put(4, cpn.x);
+            put(5, cpn.y);
+            put(6, cpn.z);
+            break;
+        }
+        case CHECK_FRESNEL_CHANNEL: {
+            // One channel of the bounce's reflect arm (the TIR retarder or the Fresnel
+            // reflection, lane_scalar_reflect's arithmetic) and refract arm (the
+            // transmission at the channel's own Snell angle), with the bounce's geometry.
+            const float n1 = inf(0), n2 = inf(1), cos_i = inf(2);
+            const Stokes st{inf(3), inf(4), inf(5), inf(6)};
+            const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
+            const float sin_i = sqrtf(fmaxf(one_m_c2, 0.0f));
+            const float ratio = __fdiv_rn(n1, n2);
+            const float s2k = (ratio * ratio) * one_m_c2;
+            for (int i = 0; i < 13; ++i) put(i, 0.0f);
+            LanePath P;
+            P.pdf = 1.0f;
+            P.st = st;
+            const Stokes r = lane_scalar_reflect(P, n1, n2, s2k, cos_i, sin_i);
+            put(0, r.i);
+            put(1, r.q);
+            put(2, r.u);
+            put(3, r.v);
+            if (s2k > 1.0f) {
+                put(12, 1.0f);
+                break;
+            }
+            const float cos_t_k = __fsqrt_rn(fmaxf(1.0f - s2k, 0.0f));
+            const float two = 2.0f * n1 * cos_i;
+            const float t_s = two / fmaf(n2, cos_t_k, n1 * cos_i);
+            const float t_p = two / fmaf(n1, cos_t_k, n2 * cos_i);
+            const Stokes t = fresnel_transmit_apply(st, n1, n2, cos_i, cos_t_k, t_s, t_p);
+            float rs, rp;
+            fresnel_rs_rp(n1, n2, cos_i, cos_t_k, rs, rp);
+            put(4, t.i);
+            put(5, t.q);
+            put(6, t.u);
+            put(7, t.v);
+            put(8, rs);
+            put(9, rp);
+            put(10, t_s);
+            put(11, t_p);
+            break;
+        }
+        case CHECK_CHANNEL_ALPHA: {
+            const ix_material& m = S.s.material;
+            put(0, iso_channel_alpha(m, spectral_absorption(m.abs_o, inf(3)), v3(inf(0), inf(1), inf(2))));
+            break;
+        }
         default: break;
     }
 }

@@ -160,6 +160,11 @@ enum CheckFn {
     CHECK_CAMERA_RAY = 11,    // in: pixel, sample (u32)  out: origin xyz, dir xyz
     CHECK_ABSORPTION = 12,    // in: lambda               out: alpha (abs_o)
     CHECK_TRACE_RAY = 13,     // in: origin xyz, dir xyz, seed (u32), hero  out: x, y, z, bounces
+    CHECK_STOKES_ROTATE = 14, // in: k xyz, n xyz, prev_pn xyz, has_prev (u32), I,Q,U,V
+                              // out: rotated I,Q,U,V, the new plane normal xyz
+    CHECK_FRESNEL_CHANNEL = 15,  // in: n1, n2, cos_i, I,Q,U,V  out: reflected I,Q,U,V,
+                                 // transmitted I,Q,U,V, r_s, r_p, t_s, t_p, TIR (0 / 1)
+    CHECK_CHANNEL_ALPHA = 16, // in: k xyz, lambda  out: alpha (scene material, isotropic form)
 };
 
 struct CheckLaunch {

@@ -193,6 +193,21 @@ IX_DEV Hit group_next_hit(const Group& g, const LanePath& P, const float4* __res
     return group_intersect(g, planes, n, P.o, P.d);
 }
 
+// rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:69): the new plane of
+// incidence's normal normalize_or_zero(k x n); with a previous one, the channel's Stokes
+// vector is rotated by the signed angle between the two planes about k.
+IX_DEV V3 rotate_to_plane_of_incidence(Stokes& st, bool has_prev, V3 prev_pn, V3 k_hat, V3 normal) {
+    const V3 cpn = normalize_or_zero(cross(k_hat, normal));
+    if (has_prev && length_squared(cpn) > 1e-6f && length_squared(prev_pn) > 1e-6f) {
+        float cos_psi = clampf_(dot(prev_pn, cpn), -1.0f, 1.0f);
+        float sin_psi = dot(cross(prev_pn, cpn), normalize_or_zero(k_hat));
+        float s2, c2;
+        rotation_2psi(sin_psi, cos_psi, c2, s2);
+        st = rotate(st, c2, s2);
+    }
+    return cpn;
+}
+
 // ------------------------------------------------------------------------------------
 // Path setup: PathState::new (bounce_body.rs:260-356).
 // ------------------------------------------------------------------------------------
@@ -274,8 +289,9 @@ IX_DEV float r_unpol_of(float r_s, float r_p) { return 0.5f * fmaf(r_p, r_p, r_s
 // Beer-Lambert for an isotropic material (raytracer/absorption.rs:99, :197): the channel
 // alpha is the midpoint of the absorption tensor's quadratic form over the two
 // eigen-polarisations of the wave normal.
-IX_DEV void lane_absorption(LanePath& P, const DevScene& S, V3 k_hat, float len) {
-    const ix_material& m = S.s.material;
+// The channel alpha of a non-birefringent material along wave normal k_hat (ao: its
+// spectral alpha).
+IX_DEV float iso_channel_alpha(const ix_material& m, float ao, V3 k_hat) {
     V3 raw_c = load3(m.c_axis);
     V3 c_axis = normalize_or_zero(raw_c);
     V3 ax = (fabsf(c_axis.x) > 0.9f) ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
@@ -293,10 +309,13 @@ IX_DEV void lane_absorption(LanePath& P, const DevScene& S, V3 k_hat, float len)
     V3 eb = normalize_or_zero(cross(k_hat, ea));
     float la0 = dot(a1, ea), la1 = dot(a2, ea), la2 = dot(c_axis, ea);
     float lb0 = dot(a1, eb), lb1 = dot(a2, eb), lb2 = dot(c_axis, eb);
-    float ao = P.alpha;
     float qa = (ao * (la0 * la0) + ao * (la1 * la1)) + ao * (la2 * la2);
     float qb = (ao * (lb0 * lb0) + ao * (lb1 * lb1)) + ao * (lb2 * lb2);
-    float alpha = midpointf_(qa, qb);
+    return midpointf_(qa, qb);
+}
+IX_DEV void lane_absorption(LanePath& P, const DevScene& S, V3 k_hat, float len) {
+    const ix_material& m = S.s.material;
+    const float alpha = iso_channel_alpha(m, P.alpha, k_hat);
     P.st = scale(P.st, exp_lane(-alpha * (len * m.absorption_path_scale)));
 }
 
@@ -572,15 +591,7 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
     const V3 hit_point = P.o + hit.t * P.d;
     const V3 k_hat = P.d;  // isotropic: wave normal == ray direction
 
-    // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:69).
-    const V3 cpn = normalize_or_zero(cross(k_hat, normal));
-    if (P.has_prev && length_squared(cpn) > 1e-6f && length_squared(P.prev_pn) > 1e-6f) {
-        float cos_psi = clampf_(dot(P.prev_pn, cpn), -1.0f, 1.0f);
-        float sin_psi = dot(cross(P.prev_pn, cpn), normalize_or_zero(k_hat));
-        float s2, c2;
-        rotation_2psi(sin_psi, cos_psi, c2, s2);
-        P.st = rotate(P.st, c2, s2);
-    }
+    const V3 cpn = rotate_to_plane_of_incidence(P.st, P.has_prev, P.prev_pn, k_hat, normal);
     P.has_prev = true;
     P.prev_pn = cpn;
 
@@ -769,15 +780,8 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
                                       mat.edge_rounding_radius);
     const V3 k_hat = P.k;
 
-    // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:69), about k.
-    const V3 cpn = normalize_or_zero(cross(k_hat, normal));
-    if (P.has_prev && length_squared(cpn) > 1e-6f && length_squared(P.prev_pn) > 1e-6f) {
-        float cos_psi = clampf_(dot(P.prev_pn, cpn), -1.0f, 1.0f);
-        float sin_psi = dot(cross(P.prev_pn, cpn), normalize_or_zero(k_hat));
-        float s2, c2;
-        rotation_2psi(sin_psi, cos_psi, c2, s2);
-        P.st = rotate(P.st, c2, s2);
-    }
+    // rotate_stokes_to_plane_of_incidence, about the wave normal k.
+    const V3 cpn = rotate_to_plane_of_incidence(P.st, P.has_prev, P.prev_pn, k_hat, normal);
     P.has_prev = true;
     P.prev_pn = cpn;
 
