@@ -13,7 +13,9 @@
  *     when it returns IX_DONE;
  *   - IX_DECLINED leaves `accum_xyz` untouched and means "trace the full spp on the
  *     CPU"; device errors are reported as a decline and mark the backend lost;
- *   - IX_CANCELLED leaves `accum_xyz` untouched;
+ *   - IX_CANCELLED leaves `accum_xyz` untouched; `cancel` (may be NULL) is the caller's
+ *     one-byte flag -- a Rust AtomicBool through AtomicBool::as_ptr -- read as nonzero =
+ *     cancelled, polled between launches;
  *   - a sample whose XYZ has a NaN/Inf component is dropped but still counted
  *     (optics/raytracer/sampling.rs:237).
  * Per-pixel sums are formed on the device in f64 and are bit-identical for any chunking
@@ -101,18 +103,28 @@ void ix_set_precision(ix_backend* b, uint32_t precision);
  * material with modelled dispersion, a modelled environment, at most 2^32 - 1 pixels).
  * The facet finishes are not read here. */
 int ix_scene_routes_to_gpu(const ix_scene* scene);
+/* scene_routes_to_gpu_with_tools (gpu_backend/tool_routing.rs:81): ix_scene_routes_to_gpu
+ * with the stone's concave tools; this backend traces convex stones only, so any tool
+ * (ntools > 0) declines. */
+int ix_scene_routes_to_gpu_with_tools(const ix_scene* scene, const ix_tool* tools, uint32_t ntools);
 /* GpuBackend::try_accumulate_geom_cancellable (backend.rs:272) with an f32 accumulator:
- * adds (float)(f64 pixel sum) into accum_xyz.  `cancel` may be NULL; it is polled
- * between chunks. */
-int ix_accumulate(ix_backend* b, const ix_scene* scene, uint32_t sample_offset, uint32_t spp,
-                  float* accum_xyz, const volatile int32_t* cancel);
+ * adds (float)(f64 pixel sum) into accum_xyz.  `tools` / `ntools` are the stone's concave
+ * tools (`tools: &[ToolPrimitive]`): ntools > 0 is declined (see ix_tool).  `cancel` may
+ * be NULL; it is polled between chunks. */
+int ix_accumulate(ix_backend* b, const ix_scene* scene, const ix_tool* tools, uint32_t ntools,
+                  uint32_t sample_offset, uint32_t spp, float* accum_xyz, const volatile uint8_t* cancel);
 /* The same with an f64 accumulator (no rounding of the pixel sums). */
-int ix_accumulate_f64(ix_backend* b, const ix_scene* scene, uint32_t sample_offset,
-                      uint32_t spp, double* accum_xyz, const volatile int32_t* cancel);
-/* GpuBackend::try_accumulate_batch_cancellable (backend.rs:451): every item traced,
- * each item's status written to item->status; returns IX_DONE when all items are done. */
-int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items,
-                        const volatile int32_t* cancel);
+int ix_accumulate_f64(ix_backend* b, const ix_scene* scene, const ix_tool* tools, uint32_t ntools,
+                      uint32_t sample_offset, uint32_t spp, double* accum_xyz, const volatile uint8_t* cancel);
+/* GpuBackend::try_accumulate_batch_cancellable (backend.rs:451): every routable item
+ * traced in one persistent launch; each item's outcome is written to item->status and,
+ * when `on_done` is not NULL, reported as on_done(user, index, status) -- the reference's
+ * `on_done: &mut dyn FnMut(usize, GpuAccumulate)` -- once per item, in index order,
+ * after that item's accumulator is final (items that are not traced first, before any
+ * tracing).  Returns IX_DONE when all items are done. */
+typedef void (*ix_batch_done_fn)(void* user, uint32_t index, int32_t status);
+int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items, const volatile uint8_t* cancel,
+                        ix_batch_done_fn on_done, void* user);
 /* Batched plans (the reference's batch path, backend.rs:451, as ONE persistent launch
  * over many stones and tilts, replayed from a CUDA graph).  A job is a whole frame of
  * scene `scene` over samples [sample_offset, sample_offset + spp).  Scenes, planes and
@@ -178,7 +190,11 @@ int ix_accumulate_device(ix_backend* b, const ix_scene* scene, uint32_t sample_o
  *     calls whose work overlaps on the GPU (different streams, or other threads) race:
  *     serialise them on one stream;
  *   - the work is enqueued on `stream` (NULL: the legacy default stream) and not
- *     synchronised.
+ *     synchronised;
+ *   - dropped samples are not reported: a sample with a non-finite component is left
+ *     out of the sums as everywhere else, and counted only inside the shared array,
+ *     which no call reads back (a caller that needs the count uses
+ *     ix_accumulate_device and ix_last_dropped).
  * Returns IX_DONE, IX_DECLINED (the scene does not route to the GPU) or an
  * IX_NOALLOC_ERR_* code. */
 #define IX_NOALLOC_MAX_LAUNCHES 64
@@ -296,7 +312,7 @@ int ix_evaluate_axis_profiles(ix_backend* b, const float* planes, uint32_t n_pla
  * lighting preset the backend does not model. */
 int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metrics_lighting* lighting,
                              uint32_t sample_offset, uint32_t spp, double* accum_xyz,
-                             ix_attribution_pixel* attribution, const volatile int32_t* cancel);
+                             ix_attribution_pixel* attribution, const volatile uint8_t* cancel);
 
 /* Per-function check kernels (the GPU equivalence harness's Tier-1/Tier-2 units,
  * renderer/gpu/ulp.rs): evaluates function `fn` (ix::CheckFn numbering) for `n` input

@@ -39,8 +39,19 @@ int ix_sample_cursor_fully_claimed(const ix_sample_cursor* c);
 enum { IX_MERGE_OK = 0, IX_MERGE_WRONG_LENGTH = -1, IX_MERGE_OVERLAP = -2,
        IX_MERGE_BUDGET = -3 };
 typedef struct ix_merger ix_merger;
-/* Merger::new(pixels, first_sample) with a parked-memory budget in bytes (0 = none). */
+/* Merger::new(pixels, first_sample) with a parked-memory budget of its own in bytes
+ * (0 = none). */
 ix_merger* ix_merger_new(uint64_t pixels, uint32_t first_sample, uint64_t parked_budget_bytes);
+/* A byte budget shared by several mergers (ParkedBudget, merge/mod.rs:72-80): each parked
+ * chunk reserves pixels * 24 bytes from it and releases them when the chunk folds, when
+ * ix_merger_finish runs, or when its merger is freed with the chunk still parked.
+ * Thread-safe; free it after every merger that uses it. */
+typedef struct ix_parked_budget ix_parked_budget;
+ix_parked_budget* ix_parked_budget_new(uint64_t bytes);
+void ix_parked_budget_free(ix_parked_budget* b);
+uint64_t ix_parked_budget_used(ix_parked_budget* b);
+/* Merger::new(pixels, first_sample).with_parked_budget(budget) (merge/mod.rs:190). */
+ix_merger* ix_merger_new_shared(uint64_t pixels, uint32_t first_sample, ix_parked_budget* budget);
 void ix_merger_free(ix_merger* m);
 /* Merger::add (merge/mod.rs:239): chunk [first_sample, first_sample + done) with its
  * per-pixel sums (`len` doubles = pixels * 3).  *total (may be NULL) receives the

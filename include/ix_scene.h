@@ -131,6 +131,22 @@ typedef struct ix_scene {
     ix_environment environment;
 } ix_scene;
 
+/* A concave tool volume subtracted from the stone (ToolPrimitive,
+ * crates/indicatrix/src/geometry/tool.rs:112-131), field for field: the same 80-byte
+ * record (the reference aligns it to 16 bytes): kind 0 ball, 1 capped cylinder, 2 cone
+ * frustum, 3 bicone; sweep_kind 0 none, 1 along the axis, 2 across it.  This backend
+ * traces convex stones only: a call that passes tools is declined (the reference's GPU
+ * path declines what it cannot trace; the caller traces such a stone on the CPU). */
+typedef struct ix_tool {
+    uint32_t kind;
+    uint32_t sweep_kind;
+    uint32_t pad[2];           /* zero                                                  */
+    float origin[4];           /* centre xyz; w = radius at the centre                  */
+    float axis[4];             /* unit axis xyz; w = half-length along it (0: a ball)   */
+    float profile[4];          /* radius at -half_length, at +half_length, half-stroke, 0 */
+    float sweep_dir[4];        /* unit sweep direction (sweep_kind 2), w = 0            */
+} ix_tool;
+
 #ifdef __cplusplus
 }
 #endif

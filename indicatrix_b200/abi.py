@@ -134,6 +134,24 @@ class WorkLimits(C.Structure):
     ]
 
 
+class Tool(C.Structure):
+    """ix_tool: a concave tool volume (ToolPrimitive, geometry/tool.rs:112), 80 bytes."""
+
+    _fields_ = [
+        ("kind", C.c_uint32),
+        ("sweep_kind", C.c_uint32),
+        ("pad", C.c_uint32 * 2),
+        ("origin", C.c_float * 4),
+        ("axis", C.c_float * 4),
+        ("profile", C.c_float * 4),
+        ("sweep_dir", C.c_float * 4),
+    ]
+
+
+# ix_batch_done_fn: on_done(user, index, status).
+BATCH_DONE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32, C.c_int32)
+
+
 class BatchItem(C.Structure):
     """One stone of a batched launch (GpuBatchItem, gpu_backend/mod.rs:246)."""
 

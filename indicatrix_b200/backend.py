@@ -57,11 +57,13 @@ def load_library() -> C.CDLL:
         lib.ix_set_work_limits.argtypes = [C.c_void_p, P(abi.WorkLimits)]
         lib.ix_set_precision.argtypes = [C.c_void_p, C.c_uint32]
         lib.ix_scene_routes_to_gpu.argtypes = [P(abi.Scene)]
-        lib.ix_accumulate.argtypes = [C.c_void_p, P(abi.Scene), C.c_uint32, C.c_uint32,
-                                      P(C.c_float), P(C.c_int32)]
-        lib.ix_accumulate_f64.argtypes = [C.c_void_p, P(abi.Scene), C.c_uint32, C.c_uint32,
-                                          P(C.c_double), P(C.c_int32)]
-        lib.ix_accumulate_batch.argtypes = [C.c_void_p, P(abi.BatchItem), C.c_uint32, P(C.c_int32)]
+        lib.ix_scene_routes_to_gpu_with_tools.argtypes = [P(abi.Scene), P(abi.Tool), C.c_uint32]
+        lib.ix_accumulate.argtypes = [C.c_void_p, P(abi.Scene), P(abi.Tool), C.c_uint32, C.c_uint32, C.c_uint32,
+                                      P(C.c_float), P(C.c_uint8)]
+        lib.ix_accumulate_f64.argtypes = [C.c_void_p, P(abi.Scene), P(abi.Tool), C.c_uint32, C.c_uint32,
+                                          C.c_uint32, P(C.c_double), P(C.c_uint8)]
+        lib.ix_accumulate_batch.argtypes = [C.c_void_p, P(abi.BatchItem), C.c_uint32, P(C.c_uint8),
+                                            abi.BATCH_DONE_FN, C.c_void_p]
         lib.ix_accumulate_device.argtypes = [C.c_void_p, P(abi.Scene), C.c_uint32, C.c_uint32,
                                              C.c_void_p, C.c_int, C.c_void_p]
         lib.ix_is_lost.argtypes = [C.c_void_p]
@@ -107,7 +109,7 @@ def load_library() -> C.CDLL:
                                                   P(C.c_float), C.c_uint32, P(abi.MetricsLighting),
                                                   P(C.c_float)]
         lib.ix_accumulate_attributed.argtypes = [C.c_void_p, P(abi.Scene), P(abi.MetricsLighting), C.c_uint32,
-                                                 C.c_uint32, P(C.c_double), C.c_void_p, P(C.c_int32)]
+                                                 C.c_uint32, P(C.c_double), C.c_void_p, P(C.c_uint8)]
         _lib = lib
         return lib
 
@@ -137,10 +139,10 @@ class GpuWorkLimits:
 
 
 class CancelFlag:
-    """An ``AtomicBool``-like cancel word the library polls between chunks."""
+    """An ``AtomicBool``-like one-byte cancel flag the library polls between chunks."""
 
     def __init__(self) -> None:
-        self._word = C.c_int32(0)
+        self._word = C.c_uint8(0)
 
     def set(self) -> None:
         self._word.value = 1
@@ -228,6 +230,13 @@ def environment_uniform(radiance: float) -> abi.Environment:
 def scene_routes_to_gpu(scene: FrameScene) -> bool:
     """scene_routes_to_gpu (gpu_backend/mod.rs:288)."""
     return bool(load_library().ix_scene_routes_to_gpu(C.byref(scene.to_abi())))
+
+
+def scene_routes_to_gpu_with_tools(scene: FrameScene, tools: Sequence[abi.Tool]) -> bool:
+    """scene_routes_to_gpu_with_tools (gpu_backend/tool_routing.rs:81): any concave tool
+    declines (this backend traces convex stones)."""
+    tarr = (abi.Tool * len(tools))(*tools) if tools else None
+    return bool(load_library().ix_scene_routes_to_gpu_with_tools(C.byref(scene.to_abi()), tarr, len(tools)))
 
 
 @dataclass
@@ -358,20 +367,22 @@ class GpuBackend:
             raise ValueError("accum must be a contiguous width*height*3 array")
 
     def try_accumulate_cancellable(self, scene: FrameScene, sample_offset: int, spp: int,
-                                   accum: np.ndarray,
-                                   cancel: Optional[CancelFlag] = None) -> GpuAccumulate:
+                                   accum: np.ndarray, cancel: Optional[CancelFlag] = None,
+                                   tools: Sequence[abi.Tool] = ()) -> GpuAccumulate:
         """try_accumulate_geom_cancellable (backend.rs:272).  ``accum`` is float32 or
-        float64 and is added into only on DONE."""
+        float64 and is added into only on DONE; ``tools`` are the stone's concave tools
+        (a stone with any is declined: this backend traces convex stones)."""
         self._check_accum(scene, accum)
         if not self._h:
             return GpuAccumulate.DECLINED
         sc = scene.to_abi()
         cp = cancel.pointer() if cancel is not None else None
+        tarr = (abi.Tool * len(tools))(*tools) if tools else None
         if accum.dtype == np.float32:
-            rc = self._lib.ix_accumulate(self._h, C.byref(sc), sample_offset, spp,
+            rc = self._lib.ix_accumulate(self._h, C.byref(sc), tarr, len(tools), sample_offset, spp,
                                          accum.ctypes.data_as(C.POINTER(C.c_float)), cp)
         elif accum.dtype == np.float64:
-            rc = self._lib.ix_accumulate_f64(self._h, C.byref(sc), sample_offset, spp,
+            rc = self._lib.ix_accumulate_f64(self._h, C.byref(sc), tarr, len(tools), sample_offset, spp,
                                              accum.ctypes.data_as(C.POINTER(C.c_double)), cp)
         else:
             raise TypeError("accum must be float32 or float64")
@@ -413,7 +424,8 @@ class GpuBackend:
                                          on_done: Optional[Callable[[int, GpuAccumulate], None]] = None
                                          ) -> GpuAccumulate:
         """try_accumulate_batch_cancellable (backend.rs:451): each item's outcome is
-        reported through ``on_done(index, outcome)``."""
+        reported through ``on_done(index, outcome)`` by the library, once per item, as soon
+        as that item is final."""
         if not self._h:
             for i in range(len(items)):
                 if on_done:
@@ -433,10 +445,8 @@ class GpuBackend:
             arr[i].accum_xyz = it.accum.ctypes.data_as(C.POINTER(C.c_double))
             arr[i].status = abi.IX_DECLINED
         cp = cancel.pointer() if cancel is not None else None
-        rc = self._lib.ix_accumulate_batch(self._h, arr, len(items), cp)
-        if on_done:
-            for i in range(len(items)):
-                on_done(i, GpuAccumulate(arr[i].status))
+        cb = abi.BATCH_DONE_FN(lambda _u, i, st: on_done(int(i), GpuAccumulate(st))) if on_done else None
+        rc = self._lib.ix_accumulate_batch(self._h, arr, len(items), cp, cb, None)
         return GpuAccumulate(rc)
 
     def accumulate_device(self, scene_abi: abi.Scene, sample_offset: int, spp: int,

@@ -65,7 +65,7 @@ uint64_t chunk_budget(const ix_backend* b, int launch_index) {
 // device).  Returns the launch count or -1 on a CUDA error (b->last_error set).
 int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uint32_t spp,
                   double* d_out, int accumulate, cudaStream_t stream,
-                  const volatile int32_t* cancel, bool* cancelled,
+                  const volatile uint8_t* cancel, bool* cancelled,
                   const ix::AttrLaunch* attr = nullptr, ix_attribution_pixel* d_map = nullptr) {
     const uint64_t n_pixels64 = (uint64_t)sc.width * sc.height;
     if (n_pixels64 > 0xFFFFFFFFull) {
@@ -157,7 +157,7 @@ bool upload_finishes(ix_backend* b, ix_scene& sc, cudaStream_t st) {
 
 template <typename AccT>
 int accumulate_impl(ix_backend* b, const ix_scene* scene, uint32_t sample_offset, uint32_t spp,
-                    AccT* accum, const volatile int32_t* cancel) {
+                    AccT* accum, const volatile uint8_t* cancel) {
     if (!b || !scene || !accum) return IX_DECLINED;
     if (b->lost) return IX_DECLINED;
     if (!ix_scene_routes_to_gpu(scene)) return IX_DECLINED;
@@ -506,19 +506,26 @@ int ix_scene_routes_to_gpu(const ix_scene* s) {
     return 1;
 }
 
-int ix_accumulate(ix_backend* b, const ix_scene* scene, uint32_t sample_offset, uint32_t spp,
-                  float* accum_xyz, const volatile int32_t* cancel) {
+int ix_scene_routes_to_gpu_with_tools(const ix_scene* scene, const ix_tool* tools, uint32_t ntools) {
+    (void)tools;
+    return ntools == 0 ? ix_scene_routes_to_gpu(scene) : 0;
+}
+
+int ix_accumulate(ix_backend* b, const ix_scene* scene, const ix_tool* tools, uint32_t ntools,
+                  uint32_t sample_offset, uint32_t spp, float* accum_xyz, const volatile uint8_t* cancel) {
+    if (!ix_scene_routes_to_gpu_with_tools(scene, tools, ntools)) return IX_DECLINED;
     return accumulate_impl<float>(b, scene, sample_offset, spp, accum_xyz, cancel);
 }
 
-int ix_accumulate_f64(ix_backend* b, const ix_scene* scene, uint32_t sample_offset,
-                      uint32_t spp, double* accum_xyz, const volatile int32_t* cancel) {
+int ix_accumulate_f64(ix_backend* b, const ix_scene* scene, const ix_tool* tools, uint32_t ntools,
+                      uint32_t sample_offset, uint32_t spp, double* accum_xyz, const volatile uint8_t* cancel) {
+    if (!ix_scene_routes_to_gpu_with_tools(scene, tools, ntools)) return IX_DECLINED;
     return accumulate_impl<double>(b, scene, sample_offset, spp, accum_xyz, cancel);
 }
 
 int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metrics_lighting* lighting,
                              uint32_t sample_offset, uint32_t spp, double* accum_xyz,
-                             ix_attribution_pixel* attribution, const volatile int32_t* cancel) {
+                             ix_attribution_pixel* attribution, const volatile uint8_t* cancel) {
     if (!b || !scene || !accum_xyz || !lighting) return IX_DECLINED;
     const uint64_t n_pixels = (uint64_t)scene->width * scene->height;
     // AttributionMap::checked (attribution_map.rs:201): a map of more than
@@ -926,12 +933,19 @@ void ix_batch_plan_destroy(ix_batch_plan* p) {
     delete p;
 }
 
-int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items,
-                        const volatile int32_t* cancel) {
+int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items, const volatile uint8_t* cancel,
+                        ix_batch_done_fn on_done, void* user) {
     if (!b || (!items && n_items)) return IX_DECLINED;
     if (n_items == 0) return IX_DONE;
+    // on_done (backend.rs:451): once per item, in index order, after its outcome is final.
+    auto report = [&](uint32_t i) {
+        if (on_done) on_done(user, i, items[i].status);
+    };
     if (cancel && *cancel) {
-        for (uint32_t j = 0; j < n_items; ++j) items[j].status = IX_CANCELLED;
+        for (uint32_t j = 0; j < n_items; ++j) {
+            items[j].status = IX_CANCELLED;
+            report(j);
+        }
         return IX_CANCELLED;
     }
     // Items the CUDA path cannot trace are declined individually; the rest run in one
@@ -950,15 +964,32 @@ int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items,
         scenes.push_back(*items[i].scene);
         which.push_back(i);
     }
+    {
+        // Items that will not be traced (declined, or nothing to trace) are final now.
+        size_t k = 0;
+        for (uint32_t i = 0; i < n_items; ++i) {
+            if (k < which.size() && which[k] == i) {
+                ++k;
+                continue;
+            }
+            report(i);
+        }
+    }
     if (!jobs.empty()) {
-        if (b->lost) return IX_DECLINED;
+        if (b->lost) {
+            for (uint32_t k : which) report(k);
+            return IX_DECLINED;
+        }
         // One turn for the whole call: the plan's sums sit in the backend's pooled device
         // buffer and come back through its pinned staging buffer, which no other call may
         // touch meanwhile.
         Turn turn(b);
         ix_batch_plan* p = plan_create_locked(b, scenes.data(), (uint32_t)scenes.size(), jobs.data(),
                                               (uint32_t)jobs.size(), true);
-        if (!p) return IX_DECLINED;
+        if (!p) {
+            for (uint32_t k : which) report(k);
+            return IX_DECLINED;
+        }
         bool ok = !fail(b, grow_pinned(&b->h_sums, &b->hsums_cap, (size_t)p->out_doubles), "host alloc") &&
                   plan_run_locked(p, b->stream) == IX_DONE && plan_download_locked(p, b->h_sums) == 0;
         if (ok && !(cancel && *cancel)) {
@@ -982,6 +1013,7 @@ int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items,
         }
         ix_batch_plan_destroy(p);
     }
+    for (uint32_t k : which) report(k);
     int overall = IX_DONE;
     for (uint32_t i = 0; i < n_items; ++i)
         if (items[i].status != IX_DONE) {

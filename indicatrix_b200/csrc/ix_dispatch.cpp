@@ -21,6 +21,23 @@ struct ix_sample_cursor {
     std::deque<std::pair<uint32_t, uint32_t>> requeued;
 };
 
+// A byte budget several mergers park against (ParkedBudget, merge/mod.rs:72-80): reserve
+// refuses past the cap, release returns bytes; thread-safe.
+struct ix_parked_budget {
+    std::mutex mu;
+    uint64_t cap, used = 0;
+    bool reserve(uint64_t bytes) {
+        std::lock_guard<std::mutex> lk(mu);
+        if (used + bytes > cap) return false;
+        used += bytes;
+        return true;
+    }
+    void release(uint64_t bytes) {
+        std::lock_guard<std::mutex> lk(mu);
+        used -= bytes < used ? bytes : used;
+    }
+};
+
 struct ix_merger {
     struct Parked {
         uint32_t done;
@@ -29,7 +46,10 @@ struct ix_merger {
     mutable std::mutex mu;
     uint64_t pixels;
     uint32_t first_sample;
-    uint64_t budget, reserved = 0;
+    // The budget parked chunks are charged against: the merger's own (ix_merger_new with a
+    // nonzero size), a shared one (ix_merger_new_shared), or none.
+    ix_parked_budget* budget = nullptr;
+    bool owns_budget = false;
     std::vector<double> merged;
     uint32_t merged_count = 0, parked_count = 0;
     uint32_t frontier;
@@ -117,16 +137,45 @@ int ix_sample_cursor_fully_claimed(const ix_sample_cursor* c) {
     return (c->next >= c->end && c->requeued.empty()) ? 1 : 0;
 }
 
+ix_parked_budget* ix_parked_budget_new(uint64_t bytes) {
+    ix_parked_budget* b = new ix_parked_budget();
+    b->cap = bytes;
+    return b;
+}
+
+void ix_parked_budget_free(ix_parked_budget* b) { delete b; }
+
+uint64_t ix_parked_budget_used(ix_parked_budget* b) {
+    if (!b) return 0;
+    std::lock_guard<std::mutex> lk(b->mu);
+    return b->used;
+}
+
 ix_merger* ix_merger_new(uint64_t pixels, uint32_t first_sample, uint64_t parked_budget_bytes) {
     ix_merger* m = new ix_merger();
     m->pixels = pixels;
     m->first_sample = first_sample;
     m->frontier = first_sample;
-    m->budget = parked_budget_bytes;
+    if (parked_budget_bytes) {
+        m->budget = ix_parked_budget_new(parked_budget_bytes);
+        m->owns_budget = true;
+    }
     return m;
 }
 
-void ix_merger_free(ix_merger* m) { delete m; }
+ix_merger* ix_merger_new_shared(uint64_t pixels, uint32_t first_sample, ix_parked_budget* budget) {
+    ix_merger* m = ix_merger_new(pixels, first_sample, 0);
+    m->budget = budget;
+    return m;
+}
+
+void ix_merger_free(ix_merger* m) {
+    if (!m) return;
+    // A merger dropped with chunks still parked returns their charge (merge/tests.rs:172).
+    if (m->budget && !m->parked.empty()) m->budget->release(m->parked.size() * m->pixels * 3 * sizeof(double));
+    if (m->owns_budget) delete m->budget;
+    delete m;
+}
 
 int ix_merger_add(ix_merger* m, uint32_t first_sample, uint32_t done, const double* sums, uint64_t len,
                   uint32_t* total) {
@@ -157,15 +206,15 @@ int ix_merger_add(ix_merger* m, uint32_t first_sample, uint32_t done, const doub
     const size_t after = m->parked.size();
     const uint64_t chunk_bytes = m->pixels * 3 * sizeof(double);
     if (m->budget) {
+        // Only a chunk that stays parked needs budget; folded chunks release theirs.
         if (after > before) {
-            if (m->reserved + chunk_bytes > m->budget) {
+            if (!m->budget->reserve(chunk_bytes)) {
                 m->parked.erase(first_sample);
                 m->parked_count -= done;
                 return IX_MERGE_BUDGET;
             }
-            m->reserved += chunk_bytes;
         } else if (after < before) {
-            m->reserved -= chunk_bytes * (before - after);
+            m->budget->release(chunk_bytes * (before - after));
         }
     }
     m->dropped_pixels += dropped;
@@ -204,9 +253,9 @@ uint32_t ix_merger_finish(ix_merger* m, double* dst, uint64_t len) {
         add_assign(m->merged, kv.second.sum);
         m->merged_count += kv.second.done;
     }
+    if (m->budget && !m->parked.empty()) m->budget->release(m->parked.size() * m->pixels * 3 * sizeof(double));
     m->parked.clear();
     m->parked_count = 0;
-    m->reserved = 0;
     if (m->merged.empty()) m->merged.assign(len, 0.0);
     std::memcpy(dst, m->merged.data(), len * sizeof(double));
     return m->merged_count;

@@ -33,6 +33,13 @@ def _lib():
         lib.ix_sample_cursor_fully_claimed.argtypes = [C.c_void_p]
         lib.ix_merger_new.restype = C.c_void_p
         lib.ix_merger_new.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64]
+        lib.ix_merger_new_shared.restype = C.c_void_p
+        lib.ix_merger_new_shared.argtypes = [C.c_uint64, C.c_uint32, C.c_void_p]
+        lib.ix_parked_budget_new.restype = C.c_void_p
+        lib.ix_parked_budget_new.argtypes = [C.c_uint64]
+        lib.ix_parked_budget_free.argtypes = [C.c_void_p]
+        lib.ix_parked_budget_used.restype = C.c_uint64
+        lib.ix_parked_budget_used.argtypes = [C.c_void_p]
         lib.ix_merger_free.argtypes = [C.c_void_p]
         lib.ix_merger_add.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, P(C.c_double), C.c_uint64,
                                       P(C.c_uint32)]
@@ -82,14 +89,37 @@ class SampleCursor:
             self._h = None
 
 
+class ParkedBudget:
+    """A byte budget several mergers park against (ParkedBudget, merge/mod.rs:72)."""
+
+    def __init__(self, bytes_: int):
+        self._lib = _lib()
+        self._h = self._lib.ix_parked_budget_new(bytes_)
+
+    @property
+    def used(self) -> int:
+        return int(self._lib.ix_parked_budget_used(self._h))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.ix_parked_budget_free(self._h)
+            self._h = None
+
+
 class Merger:
     """Merger (merge/mod.rs:155): left fold of chunk sums in ascending first-sample
-    order; chunks ahead of the frontier are parked."""
+    order; chunks ahead of the frontier are parked, charged against an own byte budget
+    (``parked_budget_bytes``) or a shared ``ParkedBudget``."""
 
-    def __init__(self, pixels: int, first_sample: int = 0, parked_budget_bytes: int = 0):
+    def __init__(self, pixels: int, first_sample: int = 0, parked_budget_bytes: int = 0,
+                 shared_budget: Optional["ParkedBudget"] = None):
         self._lib = _lib()
         self.pixels = pixels
-        self._h = self._lib.ix_merger_new(pixels, first_sample, parked_budget_bytes)
+        self._budget = shared_budget  # kept alive while this merger uses it
+        if shared_budget is not None:
+            self._h = self._lib.ix_merger_new_shared(pixels, first_sample, shared_budget._h)
+        else:
+            self._h = self._lib.ix_merger_new(pixels, first_sample, parked_budget_bytes)
 
     def add(self, first_sample: int, done: int, sums: np.ndarray) -> int:
         s = np.ascontiguousarray(sums, np.float64).reshape(-1)

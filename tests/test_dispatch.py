@@ -92,6 +92,35 @@ def test_merger_parked_budget_refuses_instead_of_growing():
     assert m.frontier == 6
 
 
+def test_mergers_share_one_parked_budget():
+    """Merger::with_parked_budget (merge/mod.rs:190) with one budget shared by two mergers,
+    as merge/tests.rs:140-230 exercises it: a chunk that must park past the shared cap is
+    refused and not counted; filling the gap at the frontier folds the backlog and releases
+    its charge; finishing and freeing release exactly what is still parked, once."""
+    from indicatrix_b200.dispatch import ParkedBudget
+
+    def chunk(v):
+        return np.full(2 * 3, v)
+
+    budget = ParkedBudget(2 * 2 * 3 * 8)  # two 2-pixel chunks of f64 sums
+    a = Merger(2, 0, shared_budget=budget)
+    b = Merger(2, 0, shared_budget=budget)
+    assert a.add(2, 1, chunk(1.0)) == 1 and budget.used == 48
+    assert b.add(2, 1, chunk(1.0)) == 1 and budget.used == 96
+    with pytest.raises(MergeError):
+        b.add(4, 1, chunk(1.0))  # a third parked chunk: over the shared cap
+    assert b.total == 1
+    assert a.add(0, 2, chunk(1.0)) == 3 and budget.used == 48  # a's backlog folds
+    assert b.add(4, 1, chunk(1.0)) == 2 and budget.used == 96  # room again
+    sums, n = b.finish()
+    assert n == 2 and budget.used == 0  # b's two parked chunks released once (a has none)
+    del b
+    assert budget.used == 0
+    assert a.add(5, 1, chunk(2.0)) == 4 and budget.used == 48  # parks past a's frontier 3
+    del a  # freed with that chunk still parked: its charge returns
+    assert budget.used == 0
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))

@@ -14,8 +14,9 @@ import pytest
 
 from indicatrix_b200 import abi, geometry, materials, workloads
 from indicatrix_b200.display import DisplayTiming
-from indicatrix_b200.backend import (FrameScene, GpuAccumulate, GpuBackend, camera_new,
-                                     environment_preset, load_library, scene_routes_to_gpu)
+from indicatrix_b200.backend import (CancelFlag, FrameScene, GpuAccumulate, GpuBackend, camera_new,
+                                     environment_preset, load_library, scene_routes_to_gpu,
+                                     scene_routes_to_gpu_with_tools)
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -49,6 +50,7 @@ def test_abi_struct_layout_matches_c():
         "ix_metrics_stone": abi.MetricsStone, "ix_metrics_pose": abi.MetricsPose,
         "ix_attribution_pixel": abi.AttributionPixel,
         "ix_atrous_params": abi.AtrousParams, "ix_display_timing": DisplayTiming,
+        "ix_tool": abi.Tool,
     }
     src = ['#include <stdio.h>', '#include <stddef.h>', '#include "ix_cuda.h"', '#include "ix_display.h"',
            "int main(void){"]
@@ -107,6 +109,10 @@ def test_routing_predicate():
     fin[70] = 1
     assert scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, fs.planes, materials.diamond(), 32,
                                           fs.environment, fin))
+    huge = FrameScene(fs.camera, 65536, 65536, fs.planes, materials.diamond(), 32, fs.environment)
+    assert not scene_routes_to_gpu(huge)  # 2^32 pixels: beyond 32-bit pixel indices
+    assert scene_routes_to_gpu(FrameScene(fs.camera, 65535, 65537, fs.planes, materials.diamond(), 32,
+                                          fs.environment))
     too_many = np.zeros((129, 4), np.float32)
     too_many[:, 1] = 1.0
     assert not scene_routes_to_gpu(FrameScene(fs.camera, 8, 8, too_many, materials.diamond(), 32,
@@ -149,3 +155,33 @@ def test_step_cut_and_random_stones():
         assert st.spp in (32, 64, 128, 256)
         assert bool(st.material.abs_o.has_spline) == (i % 2 == 1)
         assert geometry.face_planes(st.planes.astype(np.float64)).all()
+
+
+def test_tools_decline_and_the_abi_forms_of_cancel_and_on_done():
+    """The boundary's argument forms: an ix_tool is the reference's 80-byte ToolPrimitive
+    and any tool declines routing (tool_routing.rs:81; convex stones only here); the cancel
+    flag is one byte, as a Rust AtomicBool; a CTA size other than 0 / 64 / 128 / 256 and an
+    unknown kernel variant are refused at create time (no device is needed to see that);
+    on_done reports every item of a declined batch."""
+    assert C.sizeof(abi.Tool) == 80
+    fs = workloads.round_brilliant_frame(8, 8)
+    assert scene_routes_to_gpu_with_tools(fs, [])
+    ball = abi.Tool()
+    ball.kind = 0
+    ball.origin[:] = [0.0, 0.3, 0.0, 0.05]
+    assert not scene_routes_to_gpu_with_tools(fs, [ball])
+    flag = CancelFlag()
+    assert C.sizeof(flag._word) == 1 and not flag.is_set()
+    flag.set()
+    assert flag.is_set() and flag.pointer().contents.value == 1
+    lib = load_library()
+    for tpb, variant in ((96, 0), (512, 0), (0, 13)):
+        opts = abi.BackendOptions(0, 0, 0, tpb, 0, variant)
+        assert not lib.ix_backend_create(C.byref(opts))
+    from indicatrix_b200.backend import GpuBatchItem
+
+    seen = []
+    items = [GpuBatchItem(fs, 0, 4, np.zeros((8, 8, 3))) for _ in range(3)]
+    assert GpuBackend.disabled().try_accumulate_batch_cancellable(
+        items, None, lambda i, r: seen.append((i, r))) == GpuAccumulate.DECLINED
+    assert seen == [(i, GpuAccumulate.DECLINED) for i in range(3)]
