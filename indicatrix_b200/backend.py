@@ -445,7 +445,9 @@ class GpuBackend:
             arr[i].accum_xyz = it.accum.ctypes.data_as(C.POINTER(C.c_double))
             arr[i].status = abi.IX_DECLINED
         cp = cancel.pointer() if cancel is not None else None
-        cb = abi.BATCH_DONE_FN(lambda _u, i, st: on_done(int(i), GpuAccumulate(st))) if on_done else None
+        # A NULL callback is a null function pointer of the callback's type.
+        cb = (abi.BATCH_DONE_FN(lambda _u, i, st: on_done(int(i), GpuAccumulate(st))) if on_done
+              else C.cast(None, abi.BATCH_DONE_FN))
         rc = self._lib.ix_accumulate_batch(self._h, arr, len(items), cp, cb, None)
         return GpuAccumulate(rc)
 

@@ -63,7 +63,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
                                          "-prec-sqrt=false", "-ftz=true"])):
             obj = os.path.join(BUILD_DIR, f"{unit}_{variant}.o")
             jobs.append((obj, common + flags + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj]))
-    for unit in ("ix_probe", "ix_fixed", "ix_noalloc", "ix_radiance", "ix_surrogate"):
+    for unit in ("ix_probe", "ix_fixed", "ix_noalloc", "ix_radiance", "ix_surrogate", "ix_umma", "ix_image_metrics"):
         obj = os.path.join(BUILD_DIR, unit + ".o")
         jobs.append((obj, common + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj]))
     procs = [(obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
@@ -78,7 +78,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if errors:
         raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
     cuda_inc = os.path.join(_cuda_home(nvcc), "include")
-    for unit in ("ix_backend", "ix_dispatch", "ix_display_host", "ix_radiance_host"):
+    for unit in ("ix_backend", "ix_dispatch", "ix_display_host", "ix_radiance_host", "ix_design"):
         host_obj = os.path.join(BUILD_DIR, unit + ".o")
         cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
                f"-I{INCLUDE}", f"-I{cuda_inc}", "-c", os.path.join(CSRC, unit + ".cpp"), "-o", host_obj]

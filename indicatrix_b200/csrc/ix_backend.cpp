@@ -12,6 +12,7 @@
 
 #include "../../include/ix_cuda.h"
 #include "../../include/ix_cie_tables.h"
+#include "../../include/ix_design.h"
 #include "ix_backend_state.h"
 #include "ix_launch.h"
 
@@ -1375,3 +1376,79 @@ int ix_debug_check(ix_backend* b, const ix_scene* scene, int32_t fn, uint32_t n,
 }
 
 }  // extern "C"
+
+// ---- design batches (include/ix_design.h) --------------------------------------------
+extern "C" int ix_evaluate_designs(ix_backend* b, const ix_design* designs, uint32_t n, const ix_design_view* view,
+                                   float* out) {
+    if (!b || !designs || !view || !view->cameras || !out || n == 0 || view->n_views == 0 || view->spp < 2 ||
+        view->width == 0 || view->height == 0 || b->lost)
+        return IX_DECLINED;
+    // One scene per design and view; two jobs per scene, over the two halves of the
+    // sample range, for the split-half metrics.
+    const uint64_t n_scenes = (uint64_t)n * view->n_views, n_jobs = 2 * n_scenes;
+    const uint32_t spp_a = view->spp / 2, spp_b = view->spp - spp_a;
+    if (n_jobs > (1u << 24) || (uint64_t)view->sample_offset + view->spp > 0xFFFFFFFFull) {
+        b->last_error = "too many designs x views in one call";
+        return IX_DECLINED;
+    }
+    const uint32_t girdle = view->girdle_segments ? view->girdle_segments : 64;
+    const uint32_t count = ix_design_planes(&designs[0], girdle, nullptr, 0);
+    if (count == 0) {
+        b->last_error = "design out of its domain";
+        return IX_DECLINED;
+    }
+    std::vector<float> planes((size_t)n * count * 4);
+    std::vector<ix_scene> scenes(n_scenes);
+    std::vector<ix_batch_job> jobs(n_jobs);
+    for (uint32_t i = 0; i < n; ++i) {
+        ix_material mat;
+        float* pl = planes.data() + (size_t)i * count * 4;
+        if (ix_design_planes(&designs[i], girdle, pl, count) != count || ix_design_material(&designs[i], &mat) != 0) {
+            b->last_error = "design out of its domain";
+            return IX_DECLINED;
+        }
+        for (uint32_t v = 0; v < view->n_views; ++v) {
+            const uint64_t j = (uint64_t)i * view->n_views + v;
+            ix_scene& sc = scenes[j];
+            std::memset(&sc, 0, sizeof(sc));
+            sc.camera = view->cameras[v];
+            sc.width = view->width;
+            sc.height = view->height;
+            sc.planes = pl;
+            sc.n_planes = count;
+            sc.material = mat;
+            sc.max_bounces = view->max_bounces;
+            sc.environment = view->environment;
+            jobs[2 * j] = ix_batch_job{(uint32_t)j, view->sample_offset, spp_a};
+            jobs[2 * j + 1] = ix_batch_job{(uint32_t)j, view->sample_offset + spp_a, spp_b};
+        }
+    }
+    for (uint64_t j = 0; j < n_scenes; ++j)
+        if (!ix_scene_routes_to_gpu(&scenes[j])) {
+            b->last_error = "design scene does not route to the GPU";
+            return IX_DECLINED;
+        }
+    Turn turn(b);
+    ix_batch_plan* p =
+        plan_create_locked(b, scenes.data(), (uint32_t)n_scenes, jobs.data(), (uint32_t)n_jobs, true);
+    if (!p) return IX_DECLINED;
+    int rc = IX_DONE;
+    float* d_metrics = nullptr;
+    if (fail(b, cudaMalloc((void**)&d_metrics, n_scenes * 3 * sizeof(float)), "metrics buffer") ||
+        fail(b, cudaEventRecord(b->ev0, b->stream), "event") ||
+        fail(b, plan_enqueue(p, b->stream, p->variant), "design batch launch") ||
+        fail(b, ix::launch_image_metrics(p->d_scenes, p->d_jobs, (uint32_t)n_scenes, p->d_out, d_metrics, b->stream),
+             "image metrics") ||
+        fail(b, cudaEventRecord(b->ev1, b->stream), "event") ||
+        fail(b, cudaMemcpyAsync(out, d_metrics, n_scenes * 3 * sizeof(float), cudaMemcpyDeviceToHost, b->stream),
+             "metrics download") ||
+        fail(b, cudaStreamSynchronize(b->stream), "design batch"))
+        rc = IX_DECLINED;
+    if (rc == IX_DONE) {
+        b->timing.paths = p->paths;
+        b->timing.launches = (ix::shape_is_pool(ix::variant_shape((int)p->variant)) ? 2u : 1u) + 1u;
+    }
+    cudaFree(d_metrics);
+    ix_batch_plan_destroy(p);
+    return rc;
+}

@@ -142,6 +142,11 @@ struct BatchLaunch {
 // thread per pixel component.
 cudaError_t launch_fixed_to_f64(const unsigned long long* acc, double* out, uint64_t n_pixels, int accumulate,
                                 cudaStream_t stream);
+// Brilliance, fire and scintillation of every view (`sums`: the batch's f64 per-pixel
+// sums; jobs 2v and 2v + 1 are view v's two half-sample renders, at their out_offset)
+// into out[3 * v] (ix_design.h).
+cudaError_t launch_image_metrics(const ix_scene* scenes, const BatchJob* jobs, uint32_t n_views, const double* sums,
+                                 float* out, cudaStream_t stream);
 
 // Per-function check kernels: evaluate one reference function per input row on the
 // device so the host can compare against the CPU oracle value by value.

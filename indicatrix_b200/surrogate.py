@@ -1,50 +1,87 @@
-"""Learned surrogate for design search: an MLP from a round brilliant's design parameters
-(table %, crown and pavilion angles, refractive index, dispersion) to its tilt-resolved
-brilliance / fire / scintillation, trained on metrics this library computes on the GPU
-(``GpuBackend.evaluate_metrics_batch``, the reference's evaluate_gem_optical_metrics),
-with forward, backward and Adam on the library's own kernels (``include/ix_surrogate.h``:
-BF16 tensor-core GEMM with FP32 accumulation).  ``screened_search`` ranks many candidate
-designs with the network and re-evaluates only the best with the metrics kernel.
+"""Learned surrogate for design search over 12-parameter round brilliants.
 
-No reference counterpart (the reference optimizes on the analytic metrics directly).
-torch provides device memory and the stream; every arithmetic step runs in the library.
+* ``evaluate_designs`` renders designs with the batched path tracer and measures their
+  brilliance / fire / scintillation at 9 tilts (``include/ix_design.h``: one persistent
+  launch over designs x tilts, image metrics reduced on the device).
+* ``SurrogateMLP`` is the 12 -> 256 -> 256 -> 256 -> 27 SiLU network, BF16 weights and
+  activations with FP32 accumulation: forward, backward and Adam run on the library's
+  kernels (``include/ix_surrogate.h``: tcgen05 GEMMs with fused bias / SiLU epilogues).
+* ``SurrogateEnsemble`` trains several members from different seeds; their disagreement
+  on a candidate's score decides whether the tracer must score it instead.
+* ``screened_search`` is the evolutionary search in which the ensemble scores every
+  candidate, candidates it disagrees on fall back to the tracer, and the tracer re-renders
+  the best of each generation; ``traced_search`` is the same search scored by the tracer
+  alone, the baseline it is measured against.
+
+No reference counterpart: the reference's cut optimiser scores candidates with its
+analytic metrics (crates/indicatrix-cut-core/src/optimize/mod.rs:1-80).  torch provides
+device memory and the stream; every arithmetic step runs in the library.
 """
 from __future__ import annotations
 
 import ctypes as C
 import math
-from dataclasses import dataclass
+import time
+from dataclasses import dataclass, field
 from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
-from . import geometry, materials
-from .backend import GpuBackend, MetricsLighting, load_library
+from . import abi
+from .backend import GpuBackend, camera_new, environment_preset, load_library, PRESET_ISO_HEMISPHERE
 
-TILTS_DEG = [0.0, 5.0, 10.0, 15.0, 20.0, 25.0, 30.0, 35.0, 40.0]
-N_FEATURES = 5
-N_OUTPUTS = 3 * len(TILTS_DEG)  # brilliance, fire, scintillation at each tilt
-# Design space: table %, crown deg, pavilion deg, n_d, dispersion (Cauchy B in um^2).
-LOWER = np.array([45.0, 25.0, 37.0, 1.5, 0.002], np.float64)
-UPPER = np.array([70.0, 45.0, 45.0, 2.5, 0.02], np.float64)
+PARAM_NAMES = ("crown_deg", "pavilion_deg", "star_offset_deg", "upper_half_offset_deg", "lower_half_offset_deg",
+               "table_pct", "girdle_pct", "n_d", "dispersion", "absorb_peak", "absorb_center_nm", "absorb_width_nm")
+N_FEATURES = len(PARAM_NAMES)
+# The design box: the batched workload's cut and material ranges (crown 25-45 deg,
+# pavilion 37-45 deg, table 45-70 %, n_D 1.45-2.60, n_F - n_C 0.01-0.07, absorption
+# 0-5 /cm) and the facet offsets and girdle of common round brilliants.
+LOWER = np.array([25.0, 37.0, -16.0, 3.0, 0.5, 45.0, 1.0, 1.45, 0.01, 0.0, 420.0, 20.0], np.float64)
+UPPER = np.array([45.0, 45.0, -8.0, 10.0, 3.0, 70.0, 4.0, 2.60, 0.07, 5.0, 680.0, 120.0], np.float64)
+TILTS_DEG = (0.0, 5.0, 10.0, 15.0, 20.0, 25.0, 30.0, 35.0, 40.0)
+METRICS = ("brilliance", "fire", "scintillation")
+N_OUTPUTS = len(METRICS) * len(TILTS_DEG)  # output k = metric k // 9 at tilt k % 9
+DIMS = (N_FEATURES, 256, 256, 256, N_OUTPUTS)
+FACE_UP_DISTANCE = 1.6
+FOV_DEG = 42.0
 
 _bound = False
+
+
+class DesignView(C.Structure):
+    """ix_design_view (include/ix_design.h)."""
+    _fields_ = [
+        ("cameras", C.POINTER(abi.Camera)),
+        ("n_views", C.c_uint32),
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("spp", C.c_uint32),
+        ("sample_offset", C.c_uint32),
+        ("max_bounces", C.c_uint32),
+        ("girdle_segments", C.c_uint32),
+        ("environment", abi.Environment),
+    ]
 
 
 def _lib() -> C.CDLL:
     global _bound
     lib = load_library()
     if not _bound:
-        vp, f32p = C.c_void_p, C.POINTER(C.c_float)
+        vp = C.c_void_p
         u32, u64, f32 = C.c_uint32, C.c_uint64, C.c_float
         lib.ix_mlp_gemm_bf16.argtypes = [C.c_int, C.c_int, u32, u32, u32, vp, u32, vp, u32, vp, u32, vp]
-        lib.ix_mlp_bias_act.argtypes = [u32, u32, vp, vp, C.c_int, vp, vp, vp, vp]
+        lib.ix_mlp_linear.argtypes = [u32, u32, u32, vp, u32, vp, vp, C.c_int, vp, vp, vp, vp]
+        lib.ix_mlp_backward_silu.argtypes = [u32, u32, u32, vp, vp, vp, vp, vp, vp]
+        lib.ix_mlp_status.argtypes = [C.c_int]
+        lib.ix_mlp_status.restype = u32
         lib.ix_mlp_mse_grad.argtypes = [u32, u32, vp, vp, vp, vp, vp, vp]
-        lib.ix_mlp_relu_backward.argtypes = [u64, vp, vp, vp, vp, vp]
         lib.ix_mlp_bias_grad.argtypes = [u32, u32, vp, vp, vp]
         lib.ix_mlp_adam.argtypes = [u64, vp, vp, vp, vp, vp, f32, f32, f32, f32, u32, vp]
         lib.ix_mlp_to_bf16.argtypes = [u64, vp, vp, vp]
-        del f32p
+        lib.ix_design_planes.argtypes = [vp, u32, vp, u32]
+        lib.ix_design_planes.restype = u32
+        lib.ix_design_material.argtypes = [vp, C.POINTER(abi.Material)]
+        lib.ix_evaluate_designs.argtypes = [vp, vp, u32, C.POINTER(DesignView), vp]
         _bound = True
     return lib
 
@@ -54,43 +91,105 @@ def _ok(rc: int) -> None:
         raise RuntimeError("surrogate kernel launch failed")
 
 
-# ---- designs and their metrics --------------------------------------------------------
+# ---- designs and their traced metrics --------------------------------------------------
 def sample_designs(n: int, seed: int) -> np.ndarray:
-    """n designs uniform over the design box, [n, 5]."""
+    """n designs uniform over the design box, [n, 12] float64."""
     rng = np.random.default_rng(seed)
     return LOWER + (UPPER - LOWER) * rng.random((n, N_FEATURES))
 
 
 def normalize(designs: np.ndarray) -> np.ndarray:
+    """The network's input: each parameter mapped from its range to [-1, 1]."""
     return ((designs - LOWER) / (UPPER - LOWER) * 2.0 - 1.0).astype(np.float32)
 
 
-def design_stone(d: np.ndarray) -> Tuple[np.ndarray, object]:
-    planes = geometry.to_f32(geometry.round_brilliant(geometry.RoundBrilliantParams(
-        table_pct=float(d[0]), crown_deg=float(d[1]), pavilion_deg=float(d[2]))))
-    return planes, materials.cauchy(float(d[3]), float(d[4]), 0.0)
+def _design_rows(designs: np.ndarray) -> np.ndarray:
+    d = np.ascontiguousarray(np.asarray(designs, np.float64).reshape(-1, N_FEATURES), np.float32)
+    return d
 
 
-def evaluate_designs(backend: GpuBackend, designs: np.ndarray,
-                     lighting: Optional[MetricsLighting] = None) -> np.ndarray:
-    """The metrics kernel's brilliance, fire and scintillation of every design at every
-    tilt in one launch: [n, 27] (brilliance % / 100, fire, scintillation % / 100)."""
-    lighting = lighting if lighting is not None else MetricsLighting(10, 0.85, 0.95)
-    stones = [design_stone(d) for d in designs]
-    poses = [(i, 0.0, math.radians(90.0 - t)) for i in range(len(designs)) for t in TILTS_DEG]
-    m = backend.evaluate_metrics_batch(stones, poses, lighting, True)
-    if m is None:
-        raise RuntimeError(f"metrics declined: {backend.last_lost_reason()}")
-    m = m.reshape(len(designs), len(TILTS_DEG), 5)
-    # GemOpticalMetrics order: brilliance %, fire index, scintillation %, windowing %, extinction %.
-    out = np.concatenate([m[:, :, 0] / 100.0, m[:, :, 1], m[:, :, 2] / 100.0], axis=1)
-    return out.astype(np.float32)
+def design_planes(design: np.ndarray, girdle_segments: int = 64) -> np.ndarray:
+    """The design's f32 half-spaces [k, 4] (ix_design_planes)."""
+    row = _design_rows(design)
+    lib = _lib()
+    k = lib.ix_design_planes(row.ctypes.data, girdle_segments, None, 0)
+    if k == 0:
+        raise ValueError("design out of its domain")
+    out = np.zeros((k, 4), np.float32)
+    lib.ix_design_planes(row.ctypes.data, girdle_segments, out.ctypes.data, k)
+    return out
+
+
+def design_material(design: np.ndarray) -> abi.Material:
+    m = abi.Material()
+    if _lib().ix_design_material(_design_rows(design).ctypes.data, C.byref(m)) != 0:
+        raise ValueError("design out of its domain")
+    return m
+
+
+@dataclass
+class RenderSpec:
+    """How designs are traced: image size, samples per pixel, first sample, depth, the
+    tilts (camera pitch from the table normal) and the girdle's segment count."""
+    width: int = 32
+    height: int = 32
+    spp: int = 32
+    sample_offset: int = 0
+    max_bounces: int = 32
+    girdle_segments: int = 64
+    tilts_deg: Tuple[float, ...] = TILTS_DEG
+
+    def paths_per_design(self) -> int:
+        return self.width * self.height * self.spp * len(self.tilts_deg)
+
+
+def _view(spec: RenderSpec):
+    cams = (abi.Camera * len(spec.tilts_deg))()
+    for i, t in enumerate(spec.tilts_deg):
+        pitch = float(np.float32(math.pi / 2.0 - math.radians(t)))
+        cams[i] = camera_new(0.0, pitch, FACE_UP_DISTANCE, FOV_DEG)
+    env = environment_preset(PRESET_ISO_HEMISPHERE, 1.0, 0.0, 0.0, 0.0, 1.0, 20.0)
+    view = DesignView(C.cast(cams, C.POINTER(abi.Camera)), len(spec.tilts_deg), spec.width, spec.height, spec.spp,
+                      spec.sample_offset, spec.max_bounces, spec.girdle_segments, env)
+    return view, cams
+
+
+def evaluate_designs(backend: GpuBackend, designs: np.ndarray, spec: RenderSpec = RenderSpec(),
+                     max_per_call: int = 4096) -> np.ndarray:
+    """Traced metrics of every design, [n, 27]: brilliance at the 9 tilts, then fire, then
+    scintillation (ix_evaluate_designs, one batched launch per `max_per_call` designs)."""
+    if not backend.available:
+        raise RuntimeError("no CUDA backend")
+    rows = _design_rows(designs)
+    n, t = rows.shape[0], len(spec.tilts_deg)
+    out = np.zeros((n, t, 3), np.float32)
+    view, cams = _view(spec)
+    lib = _lib()
+    for a in range(0, n, max_per_call):
+        b = min(n, a + max_per_call)
+        rc = lib.ix_evaluate_designs(backend._h, rows[a:].ctypes.data, b - a, C.byref(view),
+                                     out[a:].ctypes.data)
+        if rc != abi.IX_DONE:
+            raise RuntimeError(f"design batch declined: {backend.last_lost_reason()}")
+    del cams
+    return np.ascontiguousarray(out.transpose(0, 2, 1).reshape(n, N_OUTPUTS))
+
+
+def tilt_means(metrics: np.ndarray) -> np.ndarray:
+    """[n, 3]: each metric averaged over the tilts."""
+    return metrics.reshape(metrics.shape[0], len(METRICS), -1).mean(axis=2)
+
+
+def score(metrics: np.ndarray, scales: np.ndarray) -> np.ndarray:
+    """A design's search score: the sum over the three metrics of its tilt-averaged value
+    divided by that metric's scale (the training set's mean), so each counts alike."""
+    return (tilt_means(metrics) / scales).sum(axis=1)
 
 
 # ---- the network ----------------------------------------------------------------------
 @dataclass
 class Layer:
-    w: object   # f32 [in, out] master weights (torch)
+    w: object   # f32 [out, in] master weights (torch)
     wb: object  # bf16 copy
     b: object   # f32 [out]
     mw: object
@@ -100,142 +199,283 @@ class Layer:
 
 
 class SurrogateMLP:
-    """[5] -> hidden -> hidden -> [27], ReLU, MSE, Adam; BF16 GEMMs with FP32 accumulation
-    on the library's tensor-core kernel, FP32 master weights."""
+    """12 -> 256 -> 256 -> 256 -> 27 with SiLU between layers, MSE on standardised targets,
+    Adam; BF16 GEMMs with FP32 accumulation on the tcgen05 kernels, FP32 master weights."""
 
-    def __init__(self, hidden: int = 128, seed: int = 0, device: str = "cuda") -> None:
+    def __init__(self, dims: Sequence[int] = DIMS, seed: int = 0, device: str = "cuda") -> None:
         import torch
 
         self.torch = torch
         self.dev = torch.device(device)
+        self.dims = tuple(int(d) for d in dims)
         g = np.random.default_rng(seed)
-        dims = [N_FEATURES, hidden, hidden, N_OUTPUTS]
         self.layers: List[Layer] = []
-        for fan_in, fan_out in zip(dims[:-1], dims[1:]):
-            w = torch.from_numpy((g.standard_normal((fan_in, fan_out)) * math.sqrt(2.0 / fan_in)).astype(np.float32))
-            w = w.to(self.dev)
+        for fan_in, fan_out in zip(self.dims[:-1], self.dims[1:]):
+            w = (g.standard_normal((fan_out, fan_in)) / math.sqrt(fan_in)).astype(np.float32)
+            w = torch.from_numpy(w).to(self.dev)
             z = lambda *s: torch.zeros(*s, dtype=torch.float32, device=self.dev)  # noqa: E731
-            layer = Layer(w, torch.empty(fan_in, fan_out, dtype=torch.bfloat16, device=self.dev), z(fan_out),
-                          z(fan_in, fan_out), z(fan_in, fan_out), z(fan_out), z(fan_out))
+            layer = Layer(w, torch.empty(fan_out, fan_in, dtype=torch.bfloat16, device=self.dev), z(fan_out),
+                          z(fan_out, fan_in), z(fan_out, fan_in), z(fan_out), z(fan_out))
             _ok(_lib().ix_mlp_to_bf16(w.numel(), w.data_ptr(), layer.wb.data_ptr(), self._stream()))
             self.layers.append(layer)
         self.step = 0
-        # Per-output standardisation of the targets (set by fit): the outputs differ in
-        # scale by orders of magnitude, and the loss weighs them equally once scaled.
-        self.t_mean = np.zeros(N_OUTPUTS, np.float32)
-        self.t_std = np.ones(N_OUTPUTS, np.float32)
+        # Per-output standardisation of the targets (set by fit).
+        self.t_mean = np.zeros(self.dims[-1], np.float32)
+        self.t_std = np.ones(self.dims[-1], np.float32)
 
     def _stream(self) -> int:
         return self.torch.cuda.current_stream().cuda_stream
 
-    def _bf16(self, x):
-        xb = self.torch.empty(x.shape, dtype=self.torch.bfloat16, device=self.dev)
-        _ok(_lib().ix_mlp_to_bf16(x.numel(), x.data_ptr(), xb.data_ptr(), self._stream()))
+    def to_device_bf16(self, x: np.ndarray):
+        torch = self.torch
+        xt = torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(self.dev)
+        xb = torch.empty(xt.shape, dtype=torch.bfloat16, device=self.dev)
+        _ok(_lib().ix_mlp_to_bf16(xt.numel(), xt.data_ptr(), xb.data_ptr(), self._stream()))
         return xb
 
-    def _forward(self, xb, m: int):
-        """Returns per layer (input bf16, pre-activation z) and the f32 output."""
+    def forward_device(self, xb, keep: bool = False):
+        """xb: bf16 [m, 12] on the device.  Returns the f32 output [m, 27] (standardised)
+        and, with keep, per layer (bf16 input, f32 pre-activation)."""
         torch, lib, s = self.torch, _lib(), self._stream()
+        m = xb.shape[0]
         acts = []
         h = xb
         out = None
         for li, L in enumerate(self.layers):
-            k, n = L.w.shape
-            acc = torch.empty(m, n, dtype=torch.float32, device=self.dev)
-            _ok(lib.ix_mlp_gemm_bf16(0, 0, m, n, k, h.data_ptr(), k, L.wb.data_ptr(), n, acc.data_ptr(), n, s))
-            last = li == len(self.layers) - 1
-            z = torch.empty_like(acc)
-            if last:
-                out = torch.empty_like(acc)
-                _ok(lib.ix_mlp_bias_act(m, n, acc.data_ptr(), L.b.data_ptr(), 0, z.data_ptr(), out.data_ptr(), None, s))
-                acts.append((h, z))
+            n, k = L.w.shape
+            if li == len(self.layers) - 1:
+                out = torch.empty(m, n, dtype=torch.float32, device=self.dev)
+                _ok(lib.ix_mlp_linear(m, n, k, h.data_ptr(), k, L.wb.data_ptr(), L.b.data_ptr(), 0, None,
+                                      out.data_ptr(), None, s))
+                acts.append((h, None))
             else:
+                z = torch.empty(m, n, dtype=torch.float32, device=self.dev) if keep else None
                 hb = torch.empty(m, n, dtype=torch.bfloat16, device=self.dev)
-                _ok(lib.ix_mlp_bias_act(m, n, acc.data_ptr(), L.b.data_ptr(), 1, z.data_ptr(), None, hb.data_ptr(), s))
+                _ok(lib.ix_mlp_linear(m, n, k, h.data_ptr(), k, L.wb.data_ptr(), L.b.data_ptr(), 1,
+                                      z.data_ptr() if keep else None, None, hb.data_ptr(), s))
                 acts.append((h, z))
                 h = hb
-        return acts, out
+        return out, acts
 
     def predict(self, x: np.ndarray) -> np.ndarray:
-        torch = self.torch
-        xt = torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(self.dev)
-        _, out = self._forward(self._bf16(xt), x.shape[0])
+        """Metrics [m, 27] of normalised designs x [m, 12]."""
+        out, _ = self.forward_device(self.to_device_bf16(x))
         return out.cpu().numpy() * self.t_std + self.t_mean
 
     def gradients(self, x: np.ndarray, t: np.ndarray):
-        """Loss and the f32 gradients [(dW, db) per layer] of one batch (no update)."""
+        """Loss and the f32 gradients [(dW [out, in], db)] of one batch (no update); t are
+        the targets as the network sees them (standardised)."""
+        return self._gradients_device(self.to_device_bf16(x),
+                                      self.torch.from_numpy(np.ascontiguousarray(t, np.float32)).to(self.dev))
+
+    def _gradients_device(self, xb, tt):
         torch, lib, s = self.torch, _lib(), self._stream()
-        m = x.shape[0]
-        xt = torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(self.dev)
-        tt = torch.from_numpy(np.ascontiguousarray(t, np.float32)).to(self.dev)
-        acts, out = self._forward(self._bf16(xt), m)
+        m = xb.shape[0]
+        out, acts = self.forward_device(xb, keep=True)
         loss = torch.zeros(1, dtype=torch.float32, device=self.dev)
-        dy = torch.empty_like(out)
-        dyb = torch.empty(out.shape, dtype=torch.bfloat16, device=self.dev)
-        _ok(lib.ix_mlp_mse_grad(m, out.shape[1], out.data_ptr(), tt.data_ptr(), dy.data_ptr(), dyb.data_ptr(),
+        d_f32 = torch.empty_like(out)
+        d_b16 = torch.empty(out.shape, dtype=torch.bfloat16, device=self.dev)
+        _ok(lib.ix_mlp_mse_grad(m, out.shape[1], out.data_ptr(), tt.data_ptr(), d_f32.data_ptr(), d_b16.data_ptr(),
                                 loss.data_ptr(), s))
         grads = [None] * len(self.layers)
-        d_f32, d_b16 = dy, dyb
         for li in range(len(self.layers) - 1, -1, -1):
             L = self.layers[li]
-            h_in, _z = acts[li]
-            k, n = L.w.shape
-            dw = torch.empty(k, n, dtype=torch.float32, device=self.dev)
-            # dW = h_in^T dZ  (h_in: m x k, dZ: m x n)
-            _ok(lib.ix_mlp_gemm_bf16(1, 0, k, n, m, h_in.data_ptr(), k, d_b16.data_ptr(), n, dw.data_ptr(), n, s))
+            h_in = acts[li][0]
+            n, k = L.w.shape
+            # dW = dZ^T h_in: (n x m) (m x k).
+            dw = torch.empty(n, k, dtype=torch.float32, device=self.dev)
+            _ok(lib.ix_mlp_gemm_bf16(1, 0, n, k, m, d_b16.data_ptr(), n, h_in.data_ptr(), k, dw.data_ptr(), k, s))
             db = torch.empty(n, dtype=torch.float32, device=self.dev)
             _ok(lib.ix_mlp_bias_grad(m, n, d_f32.data_ptr(), db.data_ptr(), s))
             grads[li] = (dw, db)
             if li > 0:
-                # dH_prev = dZ W^T, then through the previous layer's ReLU.
-                dh = torch.empty(m, k, dtype=torch.float32, device=self.dev)
-                _ok(lib.ix_mlp_gemm_bf16(0, 1, m, k, n, d_b16.data_ptr(), n, L.wb.data_ptr(), n, dh.data_ptr(), k, s))
+                # dZ_prev = (dZ W) * silu'(z_prev), fused in the GEMM's epilogue.
                 z_prev = acts[li - 1][1]
-                dz = torch.empty_like(dh)
+                dz = torch.empty(m, k, dtype=torch.float32, device=self.dev)
                 dzb = torch.empty(m, k, dtype=torch.bfloat16, device=self.dev)
-                _ok(lib.ix_mlp_relu_backward(dh.numel(), dh.data_ptr(), z_prev.data_ptr(), dz.data_ptr(), dzb.data_ptr(),
-                                             s))
+                _ok(lib.ix_mlp_backward_silu(m, k, n, d_b16.data_ptr(), L.wb.data_ptr(), z_prev.data_ptr(),
+                                             dz.data_ptr(), dzb.data_ptr(), s))
                 d_f32, d_b16 = dz, dzb
-        return float(loss.item()), grads
+        return loss, grads
 
-    def train_step(self, x: np.ndarray, t: np.ndarray, lr: float = 2e-3) -> float:
+    def _adam(self, grads, lr: float) -> None:
         lib, s = _lib(), self._stream()
-        loss, grads = self.gradients(x, t)
         self.step += 1
         for L, (dw, db) in zip(self.layers, grads):
             _ok(lib.ix_mlp_adam(L.w.numel(), L.w.data_ptr(), L.wb.data_ptr(), dw.data_ptr(), L.mw.data_ptr(),
                                 L.vw.data_ptr(), lr, 0.9, 0.999, 1e-8, self.step, s))
             _ok(lib.ix_mlp_adam(L.b.numel(), L.b.data_ptr(), None, db.data_ptr(), L.mb.data_ptr(), L.vb.data_ptr(),
                                 lr, 0.9, 0.999, 1e-8, self.step, s))
-        return loss
 
-    def fit(self, x: np.ndarray, t: np.ndarray, epochs: int = 200, batch: int = 256, lr: float = 2e-3,
-            seed: int = 0) -> List[float]:
-        rng = np.random.default_rng(seed)
+    def train_step(self, x: np.ndarray, t: np.ndarray, lr: float = 1e-3) -> float:
+        loss, grads = self.gradients(x, t)
+        self._adam(grads, lr)
+        return float(loss.item())
+
+    def fit(self, x: np.ndarray, t: np.ndarray, epochs: int = 200, batch: int = 4096, lr: float = 1e-3,
+            seed: int = 0, lr_final: Optional[float] = None) -> List[float]:
+        """Adam on standardised targets; the data stays on the device and each epoch
+        visits it in a fresh order.  lr decays geometrically to lr_final (default lr / 20)
+        over the epochs.  Returns the mean loss of each epoch."""
+        torch = self.torch
         self.t_mean = t.mean(axis=0).astype(np.float32)
         self.t_std = np.maximum(t.std(axis=0), 1e-6).astype(np.float32)
-        t = ((t - self.t_mean) / self.t_std).astype(np.float32)
+        ts = ((t - self.t_mean) / self.t_std).astype(np.float32)
+        xb_all = self.to_device_bf16(x)
+        t_all = torch.from_numpy(ts).to(self.dev)
+        n = x.shape[0]
+        g = torch.Generator(device="cpu")
+        g.manual_seed(seed)
+        lr_final = lr / 20.0 if lr_final is None else lr_final
+        decay = (lr_final / lr) ** (1.0 / max(1, epochs - 1))
         losses = []
-        for _ in range(epochs):
-            order = rng.permutation(x.shape[0])
-            ep = []
-            for i in range(0, x.shape[0], batch):
+        for ep in range(epochs):
+            order = torch.randperm(n, generator=g).to(self.dev)
+            total = torch.zeros((), dtype=torch.float32, device=self.dev)
+            steps = 0
+            for i in range(0, n, batch):
                 idx = order[i:i + batch]
-                ep.append(self.train_step(x[idx], t[idx], lr))
-            losses.append(float(np.mean(ep)))
+                loss, grads = self._gradients_device(xb_all[idx].contiguous(), t_all[idx].contiguous())
+                self._adam(grads, lr * decay ** ep)
+                total += loss[0]
+                steps += 1
+            losses.append(float(total.item()) / steps)
         return losses
 
 
-def score(metrics: np.ndarray) -> np.ndarray:
-    """A design's search score: mean over tilts of brilliance + fire + scintillation."""
-    return metrics.reshape(metrics.shape[0], 3, len(TILTS_DEG)).mean(axis=2).sum(axis=1)
+class SurrogateEnsemble:
+    """`members` networks of the same shape from different seeds, trained on the same data
+    in different orders; the spread of their scores is the disagreement."""
+
+    def __init__(self, members: int = 4, seed: int = 0, dims: Sequence[int] = DIMS) -> None:
+        self.nets = [SurrogateMLP(dims, seed=seed + 1000 * i) for i in range(members)]
+
+    def fit(self, x: np.ndarray, t: np.ndarray, **kw) -> List[List[float]]:
+        seed = kw.pop("seed", 0)
+        return [net.fit(x, t, seed=seed + i, **kw) for i, net in enumerate(self.nets)]
+
+    def predict_members(self, x: np.ndarray) -> np.ndarray:
+        """[members, m, 27]; one bf16 upload shared by all members."""
+        xb = self.nets[0].to_device_bf16(x)
+        outs = [net.forward_device(xb)[0] for net in self.nets]
+        return np.stack([o.cpu().numpy() * net.t_std + net.t_mean for o, net in zip(outs, self.nets)])
+
+    def predict(self, x: np.ndarray) -> np.ndarray:
+        return self.predict_members(x).mean(axis=0)
+
+    def score(self, x: np.ndarray, scales: np.ndarray) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """(mean metrics [m, 27], mean score [m], disagreement [m]): the members' score
+        standard deviation relative to their mean score."""
+        pm = self.predict_members(x)
+        per = np.stack([score(p, scales) for p in pm])
+        mean = per.mean(axis=0)
+        return pm.mean(axis=0), mean, per.std(axis=0) / np.maximum(np.abs(mean), 1e-12)
 
 
-def screened_search(backend: GpuBackend, net: SurrogateMLP, candidates: np.ndarray, keep: int):
-    """Rank `candidates` with the network, re-evaluate the best `keep` with the metrics
-    kernel, return (designs, metrics) of the survivors in descending true score."""
-    pred = net.predict(normalize(candidates))
-    best = np.argsort(-score(pred))[:keep]
-    true = evaluate_designs(backend, candidates[best])
-    order = np.argsort(-score(true))
-    return candidates[best][order], true[order]
+# ---- design search --------------------------------------------------------------------
+@dataclass
+class SearchConfig:
+    population: int = 4096
+    generations: int = 50
+    elite: int = 64          # designs per generation the tracer re-renders / keeps
+    sigma: float = 0.05      # mutation step, fraction of each parameter's range
+    fallback: float = 0.02   # ensemble disagreement above which the tracer scores a design
+    seed: int = 0
+
+
+@dataclass
+class SearchResult:
+    best_design: np.ndarray
+    best_metrics: np.ndarray       # traced at the search's fidelity
+    best_score: float
+    history: List[float] = field(default_factory=list)  # best traced score after each generation
+    evaluations: int = 0           # candidates scored (by the network or the tracer)
+    traced: int = 0                # designs the tracer rendered
+    fallbacks: int = 0             # candidates the tracer scored because the ensemble disagreed
+    seconds: float = 0.0           # wall time of the generations, device work synchronised
+
+    @property
+    def evals_per_s(self) -> float:
+        return self.evaluations / self.seconds if self.seconds > 0 else 0.0
+
+
+def _offspring(rng: np.random.Generator, parents: np.ndarray, n: int, sigma: float) -> np.ndarray:
+    """n children of the parents: uniform crossover of two random parents, a Gaussian step
+    of sigma x range per parameter, clipped to the box; the parents come first."""
+    k = parents.shape[0]
+    a = parents[rng.integers(0, k, n)]
+    b = parents[rng.integers(0, k, n)]
+    mask = rng.random(a.shape) < 0.5
+    child = np.where(mask, a, b) + rng.standard_normal(a.shape) * sigma * (UPPER - LOWER)
+    child = np.clip(child, LOWER, UPPER)
+    child[:min(k, n)] = parents[:min(k, n)]
+    return child
+
+
+def traced_search(backend: GpuBackend, scales: np.ndarray, cfg: SearchConfig = SearchConfig(),
+                  spec: RenderSpec = RenderSpec()) -> SearchResult:
+    """Evolutionary search in which the tracer scores every candidate."""
+    rng = np.random.default_rng(cfg.seed)
+    pop = sample_designs(cfg.population, cfg.seed)
+    best = None
+    res = SearchResult(np.zeros(N_FEATURES), np.zeros(N_OUTPUTS), -np.inf)
+    t0 = time.perf_counter()
+    for _ in range(cfg.generations):
+        m = evaluate_designs(backend, pop, spec)
+        s = score(m, scales)
+        order = np.argsort(-s)[:cfg.elite]
+        if best is None or s[order[0]] > best:
+            best = float(s[order[0]])
+            res.best_design, res.best_metrics, res.best_score = pop[order[0]].copy(), m[order[0]].copy(), best
+        res.history.append(best)
+        res.evaluations += len(pop)
+        res.traced += len(pop)
+        pop = _offspring(rng, pop[order], cfg.population, cfg.sigma)
+    res.seconds = time.perf_counter() - t0
+    return res
+
+
+def screened_search(backend: GpuBackend, ensemble: SurrogateEnsemble, scales: np.ndarray,
+                    cfg: SearchConfig = SearchConfig(), spec: RenderSpec = RenderSpec()) -> SearchResult:
+    """Evolutionary search in which the ensemble scores every candidate; candidates whose
+    ensemble disagreement exceeds cfg.fallback are scored by the tracer instead, and the
+    best cfg.elite of each generation are re-rendered by the tracer, whose scores rank the
+    parents of the next generation."""
+    rng = np.random.default_rng(cfg.seed)
+    pop = sample_designs(cfg.population, cfg.seed)
+    best = None
+    res = SearchResult(np.zeros(N_FEATURES), np.zeros(N_OUTPUTS), -np.inf)
+    t0 = time.perf_counter()
+    for _ in range(cfg.generations):
+        _, s, dis = ensemble.score(normalize(pop), scales)
+        fb = np.flatnonzero(dis > cfg.fallback)
+        traced = {}
+        if fb.size:
+            m_fb = evaluate_designs(backend, pop[fb], spec)
+            s[fb] = score(m_fb, scales)
+            traced.update({int(i): m_fb[j] for j, i in enumerate(fb)})
+        top = np.argsort(-s)[:cfg.elite]
+        redo = np.array([i for i in top if int(i) not in traced], np.int64)
+        if redo.size:
+            m_re = evaluate_designs(backend, pop[redo], spec)
+            traced.update({int(i): m_re[j] for j, i in enumerate(redo)})
+        m_top = np.stack([traced[int(i)] for i in top])
+        s_top = score(m_top, scales)
+        order = np.argsort(-s_top)
+        if best is None or s_top[order[0]] > best:
+            best = float(s_top[order[0]])
+            i = top[order[0]]
+            res.best_design, res.best_metrics, res.best_score = pop[i].copy(), m_top[order[0]].copy(), best
+        res.history.append(best)
+        res.evaluations += len(pop)
+        res.traced += fb.size + redo.size
+        res.fallbacks += fb.size
+        pop = _offspring(rng, pop[top[order]], cfg.population, cfg.sigma)
+    res.seconds = time.perf_counter() - t0
+    return res
+
+
+def relative_error(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """|a - b| / |b| per tilt-averaged metric ([3]) of one design's metrics [27]."""
+    ta, tb = tilt_means(a.reshape(1, -1))[0], tilt_means(b.reshape(1, -1))[0]
+    return np.abs(ta - tb) / np.maximum(np.abs(tb), 1e-12)

@@ -15,21 +15,34 @@ def bf16(x: np.ndarray) -> np.ndarray:
     return r.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+def _logistic(z):
+    return 1.0 / (1.0 + np.exp(-z))
+
+
+def silu(z):
+    return z * _logistic(z)
+
+
+def silu_grad(z):
+    s = _logistic(z)
+    return s * (1.0 + z * (1.0 - s))
+
+
 def forward(ws, bs, x):
-    """ws, bs: per layer weights [in, out] and biases; ReLU between layers.  Returns
-    (per layer (bf16 input, pre-activation), output)."""
+    """ws, bs: per layer weights [out, in] and biases; SiLU between layers, none after the
+    last.  Returns (per layer (bf16 input, pre-activation), output)."""
     acts = []
     h = bf16(x)
     for i, (w, b) in enumerate(zip(ws, bs)):
-        z = h @ bf16(w) + np.asarray(b, np.float64)
+        z = h @ bf16(w).T + np.asarray(b, np.float64)
         acts.append((h, z))
         if i < len(ws) - 1:
-            h = bf16(np.maximum(z, 0.0))
+            h = bf16(silu(z))
     return acts, z
 
 
 def gradients(ws, bs, x, t):
-    """MSE loss and [(dW, db)] per layer."""
+    """MSE loss and [(dW, db)] per layer (dW [out, in])."""
     acts, y = forward(ws, bs, x)
     m, n = y.shape
     d = y - np.asarray(t, np.float64)
@@ -39,8 +52,8 @@ def gradients(ws, bs, x, t):
     for i in range(len(ws) - 1, -1, -1):
         h_in, _ = acts[i]
         dzb = bf16(dz)
-        grads[i] = (h_in.T @ dzb, dz.sum(axis=0))
+        grads[i] = (dzb.T @ h_in, dz.sum(axis=0))
         if i > 0:
-            dh = dzb @ bf16(ws[i]).T
-            dz = np.where(acts[i - 1][1] > 0.0, dh, 0.0)
+            dh = dzb @ bf16(ws[i])
+            dz = dh * silu_grad(acts[i - 1][1])
     return loss, grads

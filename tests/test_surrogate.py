@@ -1,18 +1,20 @@
 """The surrogate MLP's FP64 restatement (oracle/mlp_oracle.py), checked by central finite
 differences so it can serve as the device gradients' checker; and the design-space helpers
-of indicatrix_b200/surrogate.py (no GPU)."""
+of indicatrix_b200/surrogate.py and include/ix_design.h that run on the host (no GPU)."""
+import math
+
 import numpy as np
 
 import mlp_oracle as mo
-from indicatrix_b200 import surrogate
+from indicatrix_b200 import abi, geometry, surrogate
 
 
 def test_oracle_gradients_match_finite_differences():
     rng = np.random.default_rng(3)
-    dims = [5, 16, 16, 27]
-    ws = [rng.standard_normal((a, b)) * 0.5 for a, b in zip(dims[:-1], dims[1:])]
+    dims = [12, 16, 16, 27]
+    ws = [rng.standard_normal((b, a)) * 0.5 for a, b in zip(dims[:-1], dims[1:])]
     bs = [rng.standard_normal(b) * 0.1 for b in dims[1:]]
-    x = rng.standard_normal((12, 5))
+    x = rng.standard_normal((12, 12))
     t = rng.standard_normal((12, 27))
     # Without bf16 rounding the restatement is exact backprop: compare to differences.
     orig = mo.bf16
@@ -21,7 +23,7 @@ def test_oracle_gradients_match_finite_differences():
         _, grads = mo.gradients(ws, bs, x, t)
         eps = 1e-6
         for li in range(3):
-            for (i, j) in [(0, 0), (1, 2), (3, 4)]:
+            for (i, j) in [(0, 0), (1, 2), (3, 4), (15, 11)]:
                 if i >= ws[li].shape[0] or j >= ws[li].shape[1]:
                     continue
                 wp = [w.copy() for w in ws]
@@ -40,6 +42,12 @@ def test_oracle_gradients_match_finite_differences():
         mo.bf16 = orig
 
 
+def test_silu_derivative_matches_differences():
+    z = np.linspace(-8.0, 8.0, 101)
+    num = (mo.silu(z + 1e-6) - mo.silu(z - 1e-6)) / 2e-6
+    assert np.max(np.abs(num - mo.silu_grad(z))) < 1e-8
+
+
 def test_bf16_rounding_is_round_to_nearest_even():
     vals = np.array([1.0, 1.00390625, 1.01171875, 3.0e-5, -2.5, 65504.0], np.float32)
     r = mo.bf16(vals)
@@ -48,8 +56,68 @@ def test_bf16_rounding_is_round_to_nearest_even():
 
 def test_design_box_and_normalisation():
     d = surrogate.sample_designs(100, 1)
+    assert d.shape == (100, 12)
     assert np.all(d >= surrogate.LOWER) and np.all(d <= surrogate.UPPER)
     z = surrogate.normalize(d)
     assert z.dtype == np.float32 and np.all(np.abs(z) <= 1.0)
-    planes, disp = surrogate.design_stone(d[0])
-    assert planes.shape[0] <= 128 and planes.shape[1] == 4
+    assert len(surrogate.PARAM_NAMES) == 12 and surrogate.N_OUTPUTS == 27
+    assert surrogate.DIMS == (12, 256, 256, 256, 27)
+
+
+def test_design_planes_match_the_python_builder():
+    """ix_design_planes (host C++) gives the planes of geometry.round_brilliant for the same
+    parameters, to an f32 ulp (the two evaluate the same double formulas)."""
+    for row in surrogate.sample_designs(20, 5):
+        got = surrogate.design_planes(row, 64)
+        p = geometry.RoundBrilliantParams(
+            table_pct=float(np.float32(row[5])), crown_deg=float(np.float32(row[0])),
+            pavilion_deg=float(np.float32(row[1])), girdle_pct=float(np.float32(row[6])),
+            star_offset_deg=float(np.float32(row[2])), upper_half_offset_deg=float(np.float32(row[3])),
+            lower_half_offset_deg=float(np.float32(row[4])))
+        want = geometry.to_f32(geometry.round_brilliant(p))
+        assert got.shape == want.shape == (121, 4)
+        assert np.all(np.abs(got - want) <= 2.0 * np.spacing(np.abs(want).astype(np.float32)) + 1e-12)
+
+
+def test_design_planes_reject_out_of_domain():
+    row = surrogate.sample_designs(1, 2)[0].copy()
+    row[0] = 95.0  # crown angle past vertical
+    lib = surrogate._lib()
+    r = np.ascontiguousarray(row, np.float32)
+    assert lib.ix_design_planes(r.ctypes.data, 64, None, 0) == 0
+    row = surrogate.sample_designs(1, 2)[0].copy()
+    row[7] = math.nan
+    r = np.ascontiguousarray(row, np.float32)
+    assert lib.ix_design_planes(r.ctypes.data, 64, None, 0) == 0
+
+
+def test_design_material_is_cauchy_through_nd_and_dispersion():
+    row = surrogate.sample_designs(1, 3)[0].copy()
+    row[9] = 2.0
+    m = surrogate.design_material(row)
+    assert m.dispersion.kind == abi.DISP_CAUCHY
+    A, B = m.dispersion.b[0], m.dispersion.b[1]
+    n = lambda l_um: A + B / (l_um * l_um)  # noqa: E731
+    assert abs(n(0.5893) - np.float32(row[7])) < 1e-5
+    assert abs((n(0.4861) - n(0.6563)) - np.float32(row[8])) < 1e-5
+    assert m.abs_o.n_bands == 1 and m.abs_e.n_bands == 1
+    assert abs(m.abs_o.bands[0].peak - 2.0) < 1e-6 and m.abs_o.bands[0].shape == abi.BAND_GAUSS_WAVELENGTH
+    row[9] = 0.0
+    assert surrogate.design_material(row).abs_o.n_bands == 0
+
+
+def test_offspring_stay_in_the_box_and_keep_parents():
+    rng = np.random.default_rng(0)
+    parents = surrogate.sample_designs(8, 4)
+    kids = surrogate._offspring(rng, parents, 100, 0.3)
+    assert kids.shape == (100, 12)
+    assert np.all(kids >= surrogate.LOWER) and np.all(kids <= surrogate.UPPER)
+    assert np.array_equal(kids[:8], parents)
+
+
+def test_score_weighs_metrics_by_scale():
+    m = np.zeros((2, 27))
+    m[0, :9] = 2.0   # brilliance
+    m[1, 9:18] = 1.0  # fire
+    s = surrogate.score(m, np.array([2.0, 0.5, 1.0]))
+    assert np.allclose(s, [1.0, 2.0])
