@@ -29,6 +29,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 
 using namespace ixh;
@@ -863,27 +864,48 @@ int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen) {
     if (fail(b, cudaSetDevice(b->device), "set device")) return -1;
     // Each candidate is timed on every stride-th task / chunk of the plan: about 1/16 of
     // its work, spread over all its jobs, and never fewer claims than the grid has warps.
+    // The sample ranks the candidates; the best kFinalists then run the whole plan once
+    // each and the fastest of those is kept (a strided sample changes the job mix each warp
+    // sees, which can reorder candidates a few percent apart).
     const uint64_t units = std::max<uint64_t>(1, std::min(p->total_tasks, p->pool_ok ? p->total_chunks : p->total_tasks));
     const uint64_t min_claims = (uint64_t)b->sm_count * 64 * 4;
     const uint32_t stride = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(16, units / min_claims));
-    float best = 1e30f;
-    uint32_t best_v = p->variant;
+    auto time_variant = [&](uint32_t v, uint32_t st, float* ms) -> bool {
+        if (fail(b, cudaEventRecord(b->ev0, b->stream), "event")) return false;
+        if (fail(b, plan_enqueue(p, b->stream, v, st), "autotune launch")) return false;
+        if (fail(b, cudaEventRecord(b->ev1, b->stream), "event")) return false;
+        if (fail(b, cudaStreamSynchronize(b->stream), "autotune")) return false;
+        *ms = 0.0f;
+        cudaEventElapsedTime(ms, b->ev0, b->ev1);
+        return true;
+    };
+    std::vector<std::pair<float, uint32_t>> ranked;
     for (uint32_t v = 0; v < (uint32_t)ix::N_VARIANTS; ++v) {
         if (plan_blocks_per_sm(p, v) <= 0) continue;
         if (b->batch_threads && (uint32_t)ix::shape_threads(ix::variant_shape((int)v)) != b->batch_threads) continue;
         float total = 0.0f;
         for (int r = 0; r < std::max(1, reps) + 1; ++r) {
-            if (fail(b, cudaEventRecord(b->ev0, b->stream), "event")) return -1;
-            if (fail(b, plan_enqueue(p, b->stream, v, stride), "autotune launch")) return -1;
-            if (fail(b, cudaEventRecord(b->ev1, b->stream), "event")) return -1;
-            if (fail(b, cudaStreamSynchronize(b->stream), "autotune")) return -1;
             float ms = 0.0f;
-            cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+            if (!time_variant(v, stride, &ms)) return -1;
             if (r > 0) total += ms;  // the first run of a candidate warms it up
         }
-        if (total < best) {
-            best = total;
-            best_v = v;
+        ranked.emplace_back(total, v);
+    }
+    uint32_t best_v = p->variant;
+    if (!ranked.empty()) {
+        std::sort(ranked.begin(), ranked.end());
+        best_v = ranked[0].second;
+        constexpr size_t kFinalists = 3;
+        if (stride > 1 && ranked.size() > 1) {
+            float best = 1e30f;
+            for (size_t i = 0; i < std::min(kFinalists, ranked.size()); ++i) {
+                float ms = 0.0f;
+                if (!time_variant(ranked[i].second, 1, &ms)) return -1;
+                if (ms < best) {
+                    best = ms;
+                    best_v = ranked[i].second;
+                }
+            }
         }
     }
     p->variant = best_v;

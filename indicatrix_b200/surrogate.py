@@ -46,6 +46,8 @@ FACE_UP_DISTANCE = 1.6
 FOV_DEG = 42.0
 
 _bound = False
+# Kernel launches this module has enqueued (the bench's launch count).
+launches = 0
 
 
 class DesignView(C.Structure):
@@ -171,6 +173,8 @@ def evaluate_designs(backend: GpuBackend, designs: np.ndarray, spec: RenderSpec 
                                      out[a:].ctypes.data)
         if rc != abi.IX_DONE:
             raise RuntimeError(f"design batch declined: {backend.last_lost_reason()}")
+        global launches
+        launches += int(backend.last_timing().launches)
     del cams
     return np.ascontiguousarray(out.transpose(0, 2, 1).reshape(n, N_OUTPUTS))
 
@@ -227,6 +231,8 @@ class SurrogateMLP:
         return self.torch.cuda.current_stream().cuda_stream
 
     def to_device_bf16(self, x: np.ndarray):
+        global launches
+        launches += 1
         torch = self.torch
         xt = torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(self.dev)
         xb = torch.empty(xt.shape, dtype=torch.bfloat16, device=self.dev)
@@ -236,11 +242,13 @@ class SurrogateMLP:
     def forward_device(self, xb, keep: bool = False):
         """xb: bf16 [m, 12] on the device.  Returns the f32 output [m, 27] (standardised)
         and, with keep, per layer (bf16 input, f32 pre-activation)."""
+        global launches
         torch, lib, s = self.torch, _lib(), self._stream()
         m = xb.shape[0]
         acts = []
         h = xb
         out = None
+        launches += len(self.layers)
         for li, L in enumerate(self.layers):
             n, k = L.w.shape
             if li == len(self.layers) - 1:

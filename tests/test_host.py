@@ -14,6 +14,7 @@ import pytest
 
 from indicatrix_b200 import abi, geometry, materials, workloads
 from indicatrix_b200.display import DisplayTiming
+from indicatrix_b200.surrogate import DesignView
 from indicatrix_b200.backend import (CancelFlag, FrameScene, GpuAccumulate, GpuBackend, camera_new,
                                      environment_preset, load_library, scene_routes_to_gpu,
                                      scene_routes_to_gpu_with_tools)
@@ -23,7 +24,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = []
-    for h in ("ix_cuda.h", "ix_dispatch.h", "ix_display.h", "ix_radiance.h", "ix_surrogate.h"):
+    for h in sorted(f for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names += re.findall(r"\b(ix_[a-z0-9_]+)\s*\(", text)
@@ -50,10 +51,10 @@ def test_abi_struct_layout_matches_c():
         "ix_metrics_stone": abi.MetricsStone, "ix_metrics_pose": abi.MetricsPose,
         "ix_attribution_pixel": abi.AttributionPixel,
         "ix_atrous_params": abi.AtrousParams, "ix_display_timing": DisplayTiming,
-        "ix_tool": abi.Tool,
+        "ix_tool": abi.Tool, "ix_design_view": DesignView,
     }
     src = ['#include <stdio.h>', '#include <stddef.h>', '#include "ix_cuda.h"', '#include "ix_display.h"',
-           "int main(void){"]
+           '#include "ix_design.h"', "int main(void){", 'printf("ix_design %zu\\n", sizeof(ix_design));']
     for cname, py in checks.items():
         src.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
         for fname, _ in py._fields_:
@@ -66,6 +67,7 @@ def test_abi_struct_layout_matches_c():
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
         out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
     got = dict(line.split() for line in out if line)
+    assert int(got["ix_design"]) == 4 * 12  # 12 f32 parameters, passed as float rows
     for cname, py in checks.items():
         assert int(got[cname]) == C.sizeof(py), cname
         for fname, _ in py._fields_:
