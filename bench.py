@@ -60,11 +60,15 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--stones", type=int, default=64,
                     help="batch workload: the first N of the 64 seeded stones (profiling small case)")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="batch workload: pin the kernel variant (budget + 3 * shape) instead of autotuning")
     ap.add_argument("--designs", type=int, default=16384, help="surrogate workload: training designs")
     ap.add_argument("--population", type=int, default=4096, help="surrogate workload: candidates per generation")
     ap.add_argument("--generations", type=int, default=50, help="surrogate workload: search generations")
     ap.add_argument("--epochs", type=int, default=300, help="surrogate workload: training epochs per member")
     ap.add_argument("--members", type=int, default=4, help="surrogate workload: ensemble members")
+    ap.add_argument("--gemm-only", action="store_true",
+                    help="surrogate workload: time the fused linear layer's GEMM shapes only (profiling case)")
     return ap.parse_args()
 
 
@@ -597,6 +601,17 @@ def main_surrogate(args):
     from indicatrix_b200 import surrogate as S
     from indicatrix_b200.backend import GpuBackend
 
+    if args.gemm_only:
+        peak, peak_kind = tensor_peak()
+        rows = []
+        for m, n, k in [(4096, 256, 256), (65536, 256, 256), (4096, 27, 256), (4096, 256, 12)]:
+            ms = time_gemm(torch, m, n, k, reps=max(1, args.steps))
+            tf = 2 * m * n * k / (ms * 1e-3) / 1e12
+            rows.append({"shape": [m, n, k], "launch_ms": ms, "tflops": tf, "frac": tf / peak})
+        print(json.dumps({"workload": "surrogate GEMM layers (fused bias + SiLU epilogue)", "peak": peak,
+                          "peak_source": f"{peak_kind} cuBLAS bf16 burst", "layers": rows}), flush=True)
+        return
+
     backend = GpuBackend.acquire(device=local)
     if not backend.available:
         raise RuntimeError("libix_cuda.so could not create a backend")
@@ -769,7 +784,12 @@ def main():
         from indicatrix_b200.backend import BatchPlan
 
         plan = BatchPlan(backend, [(fs, rank * spp, spp) for fs, spp in items])
-        cfg["autotuned_variant"] = plan.autotune(reps=1)
+        if args.variant >= 0:
+            if not plan.set_variant(args.variant):
+                raise RuntimeError(f"kernel variant {args.variant} is not available in this build")
+            cfg["pinned_variant"] = args.variant
+        else:
+            cfg["autotuned_variant"] = plan.autotune(reps=1)
         n_out = sum(fs.width * fs.height * 3 for fs, _ in items)
         result = device_tensor(torch, plan.device_output(), n_out, dev)
     else:

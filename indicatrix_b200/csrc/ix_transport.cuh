@@ -387,7 +387,7 @@ IX_DEV void group_narrow_compat(const Group& g, LanePath& P, int status, V3 dir_
 // with its reflectance folded into the channel pdf.
 IX_DEV Stokes lane_scalar_reflect(LanePath& P, float n1k, float n2k, float s2k, float cos_i, float sin_i) {
     if (s2k > 1.0f) return tir_retard(P.st, n1k, cos_i, sin_i);
-    const float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
+    const float cos_t_k = __fsqrt_rn(fmaxf(1.0f - s2k, 0.0f));
     float rs, rp;
     fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, rs, rp);
     P.pdf = P.pdf * clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
@@ -626,6 +626,16 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
         reflect = unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM) < r_unpol;
     }
     const bool frosted = facet_frosted(S, hit.facet);
+    // The channel's own Snell geometry and Fresnel amplitudes at its index, which the
+    // reflect and refract arms below both use: formed once here, before the arms split
+    // the warp's groups, instead of once in each arm.
+    const float ratio = __fdiv_rn(n1k, n2k);
+    const float s2k = (ratio * ratio) * one_m_c2;
+    const bool lane_tir = s2k > 1.0f;
+    const float cos_t_k = lane_tir ? 0.0f : __fsqrt_rn(fmaxf(1.0f - s2k, 0.0f));
+    float rs = 1.0f, rp = 1.0f;
+    if (!lane_tir) fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, rs, rp);
+    const float r_k = clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
     V3 new_dir;
     bool new_inside = P.inside;
     if (frosted) {
@@ -637,17 +647,12 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
         // apply_tir_bounce (tir.rs:98-116) / apply_partial_reflect_bounce
         // (reflect_refract.rs:33): the channel's TIR retarder or Fresnel reflection; a
         // partial reflection divides by the selection probability (TIR scales by 1).
-        const float etak = __fdiv_rn(n1k, n2k);
-        const float s2k = etak * etak * one_m_c2;
         Stokes s;
-        if (s2k > 1.0f) {
+        if (lane_tir) {
             s = tir_retard(P.st, n1k, cos_i, sin_i);
         } else {
-            float cos_t_k = sqrtf(fmaxf(1.0f - s2k, 0.0f));
-            float rs, rp;
-            fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, rs, rp);
             s = fresnel_reflect_apply(P.st, rs, rp);
-            P.pdf = P.pdf * clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+            P.pdf = P.pdf * r_k;
         }
         P.st = scale(s, tir ? 1.0f : 1.0f / r_unpol);
         new_dir = k_hat - 2.0f * dot(k_hat, normal) * normal;
@@ -659,17 +664,14 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
         // The directions entering the match test take IEEE divide / sqrt (normalize_dir).
         const float cos_t_dir = __fsqrt_rn(fmaxf(1.0f - sin2_t_dir, 0.0f));
         const V3 final_refr = normalize_dir(eta * k_hat + fmaf(eta, cos_i, -cos_t_dir) * normal);
-        const float ratio = __fdiv_rn(n1k, n2k);
-        const float s2k = (ratio * ratio) * one_m_c2;
         int status = 0;  // 0 channel TIR, 1 direction matches the hero, 2 diverges
         V3 dir_k = v3(0.0f, 0.0f, 0.0f);
         float t_intensity = 0.0f;
         const Stokes original = P.st;
-        if (s2k > 1.0f) {
+        if (lane_tir) {
             P.st = scale(P.st, 0.0f);
             P.pdf = 0.0f;
         } else {
-            const float cos_t_k = __fsqrt_rn(fmaxf(1.0f - s2k, 0.0f));
             dir_k = normalize_dir(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
             status = dot(dir_k, final_refr) >= DIRECTION_MATCH_COS_TOL ? 1 : 2;
             const float two = 2.0f * n1k * cos_i;
@@ -678,9 +680,7 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
             const Stokes transmitted =
                 scale(fresnel_transmit_apply(original, n1k, n2k, cos_i, cos_t_k, t_s, t_p),
                       1.0f / (1.0f - r_unpol));
-            float rs, rp;
-            fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, rs, rp);
-            P.pdf = P.pdf * (1.0f - clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX));
+            P.pdf = P.pdf * (1.0f - r_k);
             // apply_channel_chromatic_termination (reflect_refract.rs:444): a diverging
             // channel's radiance is zeroed (its pdf keeps accumulating).
             P.st = status == 1 ? transmitted : scale(original, 0.0f);

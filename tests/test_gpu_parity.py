@@ -465,3 +465,31 @@ def test_batch_plan_one_launch_matches_single_scene_calls(backend):
     assert np.array_equal(plan.download(), a)
     assert abs(a.sum() - first.sum()) <= 2e-2 * first.sum()
     plan.close()
+
+
+def test_every_batch_variant_in_the_exact_build(exact_backend):
+    """Every kernel variant the exact build carries (the static task loop under each
+    register budget, the path-pool loop) traces the same batch: the pool's fixed-point sums
+    are order-independent and exact, so every pool variant gives the same bits; the task
+    loop's ascending-order f64 sums agree with them to f64 rounding."""
+    from indicatrix_b200.backend import BatchPlan
+
+    stones = workloads.random_stones(3, seed=8)
+    jobs = [(workloads.tilted_scene(st, tilt, 20, 16), 3, 24) for st in stones for tilt in (0.0, 30.0)]
+    plan = BatchPlan(exact_backend, jobs)
+    by_shape = {}
+    ran = []
+    for v in range(12):
+        if not plan.set_variant(v):
+            continue
+        plan.run()
+        out = plan.download().copy()
+        ran.append(v)
+        by_shape.setdefault(v // 3 == 0, []).append(out)
+    assert 0 in ran and any(v >= 3 for v in ran), ran
+    for outs in by_shape.values():
+        for o in outs[1:]:
+            assert np.array_equal(o.view(np.uint64), outs[0].view(np.uint64))
+    tasks, pool = by_shape[True][0], by_shape[False][0]
+    assert np.all(np.abs(tasks - pool) <= 1e-12 * np.maximum(np.abs(pool), 1e-300))
+    plan.close()

@@ -116,10 +116,14 @@ def test_backward_silu_epilogue():
                                                  torch.from_numpy(zp).cuda().data_ptr(), dz.data_ptr(),
                                                  dzb.data_ptr(), _stream()) == 0
     g = mo.bf16(dzn) @ mo.bf16(w)
-    want = g * mo.silu_grad(zp.astype(np.float64))
-    scale = (np.abs(mo.bf16(dzn)) @ np.abs(mo.bf16(w))) * np.abs(mo.silu_grad(zp.astype(np.float64))) + 1e-30
+    sg = mo.silu_grad(zp.astype(np.float64))
+    want = g * sg
+    ab = np.abs(mo.bf16(dzn)) @ np.abs(mo.bf16(w))
     got = dz.cpu().numpy()
-    assert np.max(np.abs(got - want) / (scale + 1e-6 * np.abs(want))) <= 1e-5
+    # The GEMM's accumulation error scaled by |silu'|, plus the fast logistic's absolute
+    # error in silu' (a few 1e-7; silu' crosses zero near z = -1.28) times |dz_next W|.
+    bound = _tol(k) * ab * np.abs(sg) + 2e-6 * ab
+    assert np.all(np.abs(got - want) <= bound), np.max(np.abs(got - want) / bound)
     assert np.array_equal(dzb.float().cpu().numpy(), mo.bf16(got).astype(np.float32))
 
 
