@@ -5,10 +5,12 @@
 // extra) over a range of K: BF16 operands, FP32 accumulation in tensor memory.
 //   * all 128 threads stage 64-wide K slices of A and B into shared memory in the
 //     tensor cores' K-major, unswizzled canonical layout (8-row x 16-byte core matrices),
-//     zero-filling past the matrix edges, two stages deep;
+//     zero-filling past the matrix edges, STAGES slices deep: rows contiguous along K go
+//     by 16-byte cp.async (in flight while earlier slices multiply), transposed views
+//     element by element;
 //   * one thread issues the slice's four tcgen05.mma (M 128, N NT, K 16 each) with shared
 //     memory descriptors and commits them to the stage's mbarrier, which the threads wait
-//     on before they overwrite that stage, so staging slice i + 1 overlaps slice i's MMAs;
+//     on before they refill that stage;
 //   * the accumulator lives in TMEM (NT columns, allocated by warp 0); after the last
 //     commit every warp reads its 32 lanes (tile rows) with tcgen05.ld and applies the
 //     fused epilogue: store, bias + SiLU (forward), or the SiLU derivative (backward).
@@ -30,6 +32,7 @@ namespace {
 constexpr int TM = 128;        // rows of a tile (the MMA's M)
 constexpr int BK = 64;         // K per stage: four MMAs of K 16
 constexpr int THREADS = 128;
+constexpr int STAGES = 3;      // K slices in shared memory at once
 constexpr uint32_t WAIT_LIMIT = 1u << 24;  // mbarrier polls before a wait gives up
 constexpr int SM_COUNT = 148;
 
@@ -121,21 +124,19 @@ __device__ void stage_tile(uint8_t* stage, const __nv_bfloat16* g, int64_t rs, i
     if (vec) {
         // 16-byte vectors along K (ks == 1, rows 16-byte aligned); consecutive threads
         // take consecutive rows of one 8-wide K chunk.
+        // cp.async with a source size: bytes past it (the matrix's edge) are zero-filled;
+        // a chunk wholly outside reads nothing (size 0, from the operand's base address).
         for (uint32_t idx = tid; idx < (uint32_t)R * (BK / 8); idx += THREADS) {
             const uint32_t r = idx % R, kc = idx / R;
             const uint32_t gr = r0 + r, gk = k0 + kc * 8;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            const __nv_bfloat16* p = g;
+            uint32_t bytes = 0;
             if (gr < rows && gk < k_end) {
-                const __nv_bfloat16* p = g + (int64_t)gr * rs + gk;
-                if (gk + 8 <= k_end) {
-                    v = __ldg(reinterpret_cast<const uint4*>(p));
-                } else {
-                    uint32_t e[8];
-                    for (uint32_t j = 0; j < 8; ++j) e[j] = (gk + j < k_end) ? __bfloat16_as_ushort(p[j]) : 0u;
-                    v = make_uint4(e[0] | (e[1] << 16), e[2] | (e[3] << 16), e[4] | (e[5] << 16), e[6] | (e[7] << 16));
-                }
+                p = g + (int64_t)gr * rs + gk;
+                bytes = 2u * min(8u, k_end - gk);
             }
-            *reinterpret_cast<uint4*>(stage + (kc * (R / 8) + r / 8) * 128 + (r % 8) * 16) = v;
+            const uint32_t dst = smem_u32(stage + (kc * (R / 8) + r / 8) * 128 + (r % 8) * 16);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(p), "r"(bytes) : "memory");
         }
     } else {
         // Element by element; consecutive threads take consecutive rows (coalesced when
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(THREADS) umma_gemm_kernel(const __grid_constan
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int A_STAGE = TM * BK * 2;
     constexpr int B_STAGE = NT * BK * 2;
-    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ __align__(8) uint64_t s_bar[STAGES];
     __shared__ uint32_t s_taddr;
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     const uint32_t r0 = blockIdx.x * TM, c0 = blockIdx.y * NT;
@@ -170,8 +171,7 @@ __global__ void __launch_bounds__(THREADS) umma_gemm_kernel(const __grid_constan
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        mbar_init(&s_bar[0], 1);
-        mbar_init(&s_bar[1], 1);
+        for (int i = 0; i < STAGES; ++i) mbar_init(&s_bar[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -181,29 +181,31 @@ __global__ void __launch_bounds__(THREADS) umma_gemm_kernel(const __grid_constan
 
     const uint32_t n_k = (k_end + BK - 1 - k_begin) / BK;  // k_end > k_begin (host)
     constexpr uint32_t IDESC = instr_desc(NT);
+    auto a_slot = [&](uint32_t slot) { return smem + slot * A_STAGE; };
+    auto b_slot = [&](uint32_t slot) { return smem + STAGES * A_STAGE + slot * B_STAGE; };
+    auto load = [&](uint32_t slice) {
+        const uint32_t slot = slice % STAGES, k0 = k_begin + slice * BK;
+        stage_tile<TM>(a_slot(slot), P.a, P.a_rs, P.a_ks, r0, P.m, k0, k_end, a_vec);
+        stage_tile<NT>(b_slot(slot), P.b, P.b_rs, P.b_ks, c0, P.n, k0, k_end, b_vec);
+    };
+    // Prologue: slices 0 .. STAGES - 2 in flight.  Every iteration commits one cp.async
+    // group (possibly empty), so "all but the newest STAGES - 2 groups done" always means
+    // "the slice about to be multiplied has landed".
+#pragma unroll
+    for (uint32_t i = 0; i < (uint32_t)STAGES - 1; ++i) {
+        if (i < n_k) load(i);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     bool ok = true;
     for (uint32_t it = 0; it < n_k; ++it) {
-        const uint32_t s = it & 1u;
-        uint8_t* a_st = smem + s * A_STAGE;
-        uint8_t* b_st = smem + 2 * A_STAGE + s * B_STAGE;
-        // The MMAs that read this stage two slices ago must be done before it is refilled;
-        // the CTA decides together, so every thread leaves the loop at the same slice.
-        if (it >= 2) {
-            const bool w = mbar_wait(&s_bar[s], ((it - 2) >> 1) & 1u);
-            if (__syncthreads_or(!w)) {
-                ok = false;
-                break;
-            }
-        }
-        const uint32_t k0 = k_begin + it * BK;
-        stage_tile<TM>(a_st, P.a, P.a_rs, P.a_ks, r0, P.m, k0, k_end, a_vec);
-        stage_tile<NT>(b_st, P.b, P.b_rs, P.b_ks, c0, P.n, k0, k_end, b_vec);
-        // Make the generic-proxy stores visible to the tensor cores' async proxy.
+        const uint32_t slot = it % STAGES;
+        asm volatile("cp.async.wait_group %0;" ::"n"(STAGES - 2) : "memory");
+        // Make this thread's shared-memory writes visible to the tensor cores' async proxy.
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t a_base = smem_u32(a_st), b_base = smem_u32(b_st);
+            const uint32_t a_base = smem_u32(a_slot(slot)), b_base = smem_u32(b_slot(slot));
 #pragma unroll
             for (int kk = 0; kk < BK / 16; ++kk) {
                 const uint64_t da = smem_desc(a_base + kk * 2 * (TM / 8) * 128, (TM / 8) * 128, 128);
@@ -216,17 +218,34 @@ __global__ void __launch_bounds__(THREADS) umma_gemm_kernel(const __grid_constan
                     "l"(da), "l"(db), "r"(IDESC), "r"(accumulate));
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&s_bar[s]))
+                             smem_u32(&s_bar[slot]))
                          : "memory");
         }
+        // Refill the slot slice it - 1 used with slice it + STAGES - 1, once the MMAs that
+        // read it are done; the CTA decides together, so every thread leaves the loop at
+        // the same slice.
+        const uint32_t next = it + STAGES - 1;
+        if (next < n_k) {
+            if (it >= 1) {
+                const uint32_t prev = it - 1;
+                const bool w = mbar_wait(&s_bar[prev % STAGES], (prev / STAGES) & 1u);
+                if (__syncthreads_or(!w)) {
+                    ok = false;
+                    break;
+                }
+            }
+            load(next);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     // The last commit tracks every MMA issued before it.
     const uint32_t last = n_k - 1;
-    if (ok) ok = !__syncthreads_or(!mbar_wait(&s_bar[last & 1u], (last >> 1) & 1u));
+    if (ok) ok = !__syncthreads_or(!mbar_wait(&s_bar[last % STAGES], (last / STAGES) & 1u));
     if (!ok) {
         if (tid == 0) atomicOr(P.status, 1u);
         // A last bounded chance for the tensor cores to drain before TMEM is freed.
-        (void)mbar_wait(&s_bar[last & 1u], (last >> 1) & 1u);
+        (void)mbar_wait(&s_bar[last % STAGES], (last / STAGES) & 1u);
     } else {
         tc_fence_after();
         // Epilogue: warp w owns TMEM lanes (tile rows) 32w .. 32w + 31; each tcgen05.ld
@@ -280,7 +299,7 @@ __global__ void __launch_bounds__(256) split_sum_kernel(const float* __restrict_
 
 template <int NT>
 cudaError_t launch_nt(const GemmParams& p, uint32_t splits, cudaStream_t st) {
-    const int smem = 2 * (TM + NT) * BK * 2;
+    const int smem = STAGES * (TM + NT) * BK * 2;
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [&] {

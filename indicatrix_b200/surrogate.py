@@ -421,15 +421,18 @@ def _offspring(rng: np.random.Generator, parents: np.ndarray, n: int, sigma: flo
 
 
 def traced_search(backend: GpuBackend, scales: np.ndarray, cfg: SearchConfig = SearchConfig(),
-                  spec: RenderSpec = RenderSpec()) -> SearchResult:
-    """Evolutionary search in which the tracer scores every candidate."""
+                  spec: RenderSpec = RenderSpec(), evaluate=None) -> SearchResult:
+    """Evolutionary search in which the tracer scores every candidate.  `evaluate` (designs
+    -> metrics [n, 27]) defaults to evaluate_designs on `backend` with `spec`."""
+    if evaluate is None:
+        evaluate = lambda d: evaluate_designs(backend, d, spec)  # noqa: E731
     rng = np.random.default_rng(cfg.seed)
     pop = sample_designs(cfg.population, cfg.seed)
     best = None
     res = SearchResult(np.zeros(N_FEATURES), np.zeros(N_OUTPUTS), -np.inf)
     t0 = time.perf_counter()
     for _ in range(cfg.generations):
-        m = evaluate_designs(backend, pop, spec)
+        m = evaluate(pop)
         s = score(m, scales)
         order = np.argsort(-s)[:cfg.elite]
         if best is None or s[order[0]] > best:
@@ -444,11 +447,14 @@ def traced_search(backend: GpuBackend, scales: np.ndarray, cfg: SearchConfig = S
 
 
 def screened_search(backend: GpuBackend, ensemble: SurrogateEnsemble, scales: np.ndarray,
-                    cfg: SearchConfig = SearchConfig(), spec: RenderSpec = RenderSpec()) -> SearchResult:
+                    cfg: SearchConfig = SearchConfig(), spec: RenderSpec = RenderSpec(),
+                    evaluate=None) -> SearchResult:
     """Evolutionary search in which the ensemble scores every candidate; candidates whose
     ensemble disagreement exceeds cfg.fallback are scored by the tracer instead, and the
     best cfg.elite of each generation are re-rendered by the tracer, whose scores rank the
-    parents of the next generation."""
+    parents of the next generation.  `evaluate` as for traced_search."""
+    if evaluate is None:
+        evaluate = lambda d: evaluate_designs(backend, d, spec)  # noqa: E731
     rng = np.random.default_rng(cfg.seed)
     pop = sample_designs(cfg.population, cfg.seed)
     best = None
@@ -459,13 +465,13 @@ def screened_search(backend: GpuBackend, ensemble: SurrogateEnsemble, scales: np
         fb = np.flatnonzero(dis > cfg.fallback)
         traced = {}
         if fb.size:
-            m_fb = evaluate_designs(backend, pop[fb], spec)
+            m_fb = evaluate(pop[fb])
             s[fb] = score(m_fb, scales)
             traced.update({int(i): m_fb[j] for j, i in enumerate(fb)})
         top = np.argsort(-s)[:cfg.elite]
         redo = np.array([i for i in top if int(i) not in traced], np.int64)
         if redo.size:
-            m_re = evaluate_designs(backend, pop[redo], spec)
+            m_re = evaluate(pop[redo])
             traced.update({int(i): m_re[j] for j, i in enumerate(redo)})
         m_top = np.stack([traced[int(i)] for i in top])
         s_top = score(m_top, scales)

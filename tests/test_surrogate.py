@@ -121,3 +121,68 @@ def test_score_weighs_metrics_by_scale():
     m[1, 9:18] = 1.0  # fire
     s = surrogate.score(m, np.array([2.0, 0.5, 1.0]))
     assert np.allclose(s, [1.0, 2.0])
+
+
+def _analytic_metrics(d):
+    """A smooth stand-in for the tracer on the design box: [n, 27], maximal at the box's
+    centre in every normalised parameter."""
+    z = surrogate.normalize(d).astype(np.float64)
+    base = 1.0 - 0.1 * (z ** 2).sum(axis=1)
+    tilt = np.linspace(1.0, 0.8, 9)
+    return np.concatenate([np.outer(base, tilt), 0.1 * np.outer(base, tilt), 0.5 * np.outer(base, tilt)], axis=1)
+
+
+class _FakeEnsemble:
+    """Members that agree except on designs with a large first parameter."""
+
+    def __init__(self, noise):
+        self.noise = noise
+
+    def score(self, x, scales):
+        d = surrogate.LOWER + (np.asarray(x, np.float64) + 1.0) / 2.0 * (surrogate.UPPER - surrogate.LOWER)
+        m = _analytic_metrics(d)
+        s = surrogate.score(m, scales)
+        dis = np.where(x[:, 0] > 0.8, self.noise, 0.0)
+        return m, s, dis
+
+
+def test_traced_search_improves_and_counts_every_candidate():
+    calls = []
+
+    def evaluate(d):
+        calls.append(len(d))
+        return _analytic_metrics(d)
+
+    scales = np.array([1.0, 0.1, 0.5])
+    cfg = surrogate.SearchConfig(population=256, generations=6, elite=16, seed=3)
+    r = surrogate.traced_search(None, scales, cfg, evaluate=evaluate)
+    assert r.evaluations == 256 * 6 and r.traced == 256 * 6 and calls == [256] * 6
+    assert all(b >= a for a, b in zip(r.history, r.history[1:]))  # elitist: never worse
+    assert r.history[-1] > r.history[0]
+    assert np.all(r.best_design >= surrogate.LOWER) and np.all(r.best_design <= surrogate.UPPER)
+
+
+def test_screened_search_falls_back_on_disagreement_and_retraces_the_elite():
+    traced = []
+
+    def evaluate(d):
+        traced.append(np.array(d))
+        return _analytic_metrics(d)
+
+    scales = np.array([1.0, 0.1, 0.5])
+    cfg = surrogate.SearchConfig(population=256, generations=4, elite=16, fallback=0.02, seed=5)
+    r = surrogate.screened_search(None, _FakeEnsemble(0.05), scales, cfg, evaluate=evaluate)
+    assert r.evaluations == 256 * 4
+    # Every candidate over the disagreement bar went to the tracer, and the elite of each
+    # generation was re-rendered (those already traced as fallbacks are not traced twice).
+    assert r.fallbacks > 0 and r.traced == sum(len(t) for t in traced)
+    assert r.traced <= r.fallbacks + 16 * 4
+    for t in traced:
+        assert len(t) > 0
+    # With members that always agree nothing falls back and only the elite is traced.
+    traced.clear()
+    r2 = surrogate.screened_search(None, _FakeEnsemble(0.0), scales, cfg, evaluate=evaluate)
+    assert r2.fallbacks == 0 and r2.traced == 16 * 4
+    assert r2.history[-1] >= r2.history[0]
+    # The best design's reported metrics are traced ones.
+    assert np.allclose(r2.best_metrics, _analytic_metrics(r2.best_design[None])[0])
