@@ -10,13 +10,13 @@
  * two renders over disjoint halves a, b of the sample range, and reduces each view on the
  * device to three image metrics over the stone's pixels:
  *   brilliance     mean luminance Y (the environment's radiance is the unit);
- *   fire           luminance-weighted RMS chroma, sqrt(sum Y c_a . c_b / sum Y), with c a
- *                  pixel's xy chromaticity offset from the equal-energy white (1/3, 1/3)
- *                  in one half;
+ *   fire           RMS chromaticity offset from the equal-energy white, each pixel
+ *                  weighted by S^2 (S = X + Y + Z): sqrt(sum N_a . N_b / sum S_a S_b) with
+ *                  N = (X - S / 3, Y - S / 3) of one half;
  *   scintillation  spatial coefficient of variation of Y, sqrt(cov(Y_a, Y_b)) / mean Y.
  * Products of independent halves keep per-pixel sampling noise out of the two
- * second-moment metrics (one render's |c|^2 or var(Y) would grow with it), so they
- * converge with spp without a noise bias.  The stone's pixels are those whose primary ray
+ * second-moment metrics (one render's |N|^2 or var(Y) would grow with it), and no
+ * per-pixel ratio is formed, so they converge with spp without a noise bias.  The stone's pixels are those whose primary ray
  * through the pixel centre enters the stone's half-space set.  These are measurements on the tracer's renders; they stand in
  * for, and are not, the reference's analytic metric estimators
  * (crates/indicatrix/src/color/metrics/evaluate.rs:158).

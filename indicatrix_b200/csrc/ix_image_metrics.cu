@@ -33,13 +33,15 @@ __device__ bool ray_enters(const float4* __restrict__ planes, uint32_t n, float3
 }
 
 // Per view, jobs 2v and 2v + 1 are two renders of one scene over disjoint sample ranges
-// (halves a and b).  With Y the luminance of both halves together,
+// (halves a and b, each as its per-sample mean).  With S = X + Y + Z, N = (X - S / 3,
+// Y - S / 3) the pixel's chromaticity offset from the equal-energy white in unnormalised
+// form, and Y the luminance of both halves together,
 //   brilliance    = mean Y over the stone's pixels;
-//   fire          = sqrt(sum Y c_a . c_b / sum Y), c the pixel's chromaticity offset
-//                   (x - 1/3, y - 1/3) in one half: the product of independent halves has
-//                   the noise-free chroma^2 as its expectation, so per-pixel noise does
-//                   not inflate it as |c|^2 of one render would;
-//   scintillation = sqrt(cov(Y_a, Y_b)) / mean Y, the spatial covariance of the halves,
+//   fire          = sqrt(sum N_a . N_b / sum S_a S_b): the RMS of the chromaticity offset
+//                   |N| / S over the stone, each pixel weighted by S^2.  Products of
+//                   independent halves have the noise-free |N|^2 and S^2 as expectations
+//                   and no per-pixel ratio is formed, so per-pixel noise biases neither;
+//   scintillation = sqrt(cov(Y_a, Y_b)) / mean Y: the spatial covariance of the halves,
 //                   which per-pixel noise leaves unbiased, over the mean.
 __global__ void __launch_bounds__(THREADS) image_metrics_kernel(const ix_scene* __restrict__ scenes,
                                                                 const BatchJob* __restrict__ jobs,
@@ -54,8 +56,8 @@ __global__ void __launch_bounds__(THREADS) image_metrics_kernel(const ix_scene* 
     const double inv_ab = 1.0 / ((double)ja.spp + (double)jb.spp);
     const double* pa = sums + ja.out_offset;
     const double* pb = sums + jb.out_offset;
-    // count, sum Y, sum Ya, sum Yb, sum Ya Yb, sum Y (c_a . c_b)
-    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    // count, sum Y, sum Ya, sum Yb, sum Ya Yb, sum N_a . N_b, sum S_a S_b
+    double acc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     for (uint32_t i = threadIdx.x; i < ja.n_pixels; i += THREADS) {
         const uint32_t y = i / sc.width, x = i - y * sc.width;
         // The pinhole ray through the pixel centre (the camera model of the transport).
@@ -68,32 +70,31 @@ __global__ void __launch_bounds__(THREADS) image_metrics_kernel(const ix_scene* 
         const float3 o = make_float3(c.origin[0], c.origin[1], c.origin[2]);
         if (!ray_enters(reinterpret_cast<const float4*>(sc.planes), sc.n_planes, o, d)) continue;
         const uint64_t k = 3 * (uint64_t)i;
-        const double Xa = pa[k], Ya = pa[k + 1], Za = pa[k + 2];
-        const double Xb = pb[k], Yb = pb[k + 1], Zb = pb[k + 2];
-        const double Y = (Ya + Yb) * inv_ab;
+        const double Y = (pa[k + 1] + pb[k + 1]) * inv_ab;
+        const double Xa = pa[k] * inv_a, Ya = pa[k + 1] * inv_a, Za = pa[k + 2] * inv_a;
+        const double Xb = pb[k] * inv_b, Yb = pb[k + 1] * inv_b, Zb = pb[k + 2] * inv_b;
         const double sa = Xa + Ya + Za, sb = Xb + Yb + Zb;
-        double cc = 0.0;
-        if (sa > 0.0 && sb > 0.0)
-            cc = (Xa / sa - 1.0 / 3.0) * (Xb / sb - 1.0 / 3.0) + (Ya / sa - 1.0 / 3.0) * (Yb / sb - 1.0 / 3.0);
+        const double nxa = Xa - sa / 3.0, nya = Ya - sa / 3.0, nxb = Xb - sb / 3.0, nyb = Yb - sb / 3.0;
         acc[0] += 1.0;
         acc[1] += Y;
-        acc[2] += Ya * inv_a;
-        acc[3] += Yb * inv_b;
-        acc[4] += (Ya * inv_a) * (Yb * inv_b);
-        acc[5] += Y * cc;
+        acc[2] += Ya;
+        acc[3] += Yb;
+        acc[4] += Ya * Yb;
+        acc[5] += nxa * nxb + nya * nyb;
+        acc[6] += sa * sb;
     }
     // Fixed-order reduction: warps by shuffle, then one thread over the warps' partials.
-    __shared__ double part[THREADS / 32][6];
-    for (int q = 0; q < 6; ++q) {
+    __shared__ double part[THREADS / 32][7];
+    for (int q = 0; q < 7; ++q) {
         double val = acc[q];
         for (int off = 16; off > 0; off >>= 1) val += __shfl_down_sync(0xFFFFFFFFu, val, off);
         if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5][q] = val;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        double t[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int wi = 0; wi < THREADS / 32; ++wi)
-            for (int q = 0; q < 6; ++q) t[q] += part[wi][q];
+            for (int q = 0; q < 7; ++q) t[q] += part[wi][q];
         float* o = out + 3 * (uint64_t)blockIdx.x;
         if (t[0] <= 0.0 || t[1] <= 0.0) {
             o[0] = o[1] = o[2] = 0.0f;
@@ -102,7 +103,7 @@ __global__ void __launch_bounds__(THREADS) image_metrics_kernel(const ix_scene* 
         const double n = t[0], mean = t[1] / n;
         const double cov = t[4] / n - (t[2] / n) * (t[3] / n);
         o[0] = (float)mean;
-        o[1] = (float)sqrt(fmax(t[5] / t[1], 0.0));
+        o[1] = t[6] > 0.0 ? (float)sqrt(fmax(t[5] / t[6], 0.0)) : 0.0f;
         o[2] = (float)(sqrt(fmax(cov, 0.0)) / mean);
     }
 }
