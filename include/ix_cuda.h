@@ -147,8 +147,9 @@ int ix_batch_plan_run(ix_batch_plan* p, void* stream);
  * times every kernel variant this build carries -- the static task loop and the
  * path-pool loop at 64, 128 and 256 threads per CTA, each under three register budgets
  * (variant = budget + 3 * shape) -- `reps` times on a strided sample of about 1/16 of
- * the plan's work (every job represented), then runs the three fastest on the whole plan
- * once each, keeps the fastest of those and writes it to `chosen`.
+ * the plan's work (every job represented), then runs the two fastest and the fastest of
+ * each loop (static tasks, path pool) on the whole plan once each, keeps the fastest of
+ * those and writes it to `chosen`.
  * With ix_backend_options.threads_per_block set, only that CTA size is tried.
  * Returns 0, or -1 on a device error. */
 int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen);

@@ -895,15 +895,28 @@ int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen) {
     if (!ranked.empty()) {
         std::sort(ranked.begin(), ranked.end());
         best_v = ranked[0].second;
-        constexpr size_t kFinalists = 3;
         if (stride > 1 && ranked.size() > 1) {
+            // Finalists: the two best of the sample, and the best of each loop (static
+            // tasks, path pool) -- the sample favours neither loop reliably.
+            std::vector<uint32_t> finalists;
+            auto add = [&](uint32_t v) {
+                if (std::find(finalists.begin(), finalists.end(), v) == finalists.end()) finalists.push_back(v);
+            };
+            add(ranked[0].second);
+            add(ranked[1].second);
+            for (bool pool : {false, true})
+                for (const auto& r : ranked)
+                    if (ix::shape_is_pool(ix::variant_shape((int)r.second)) == pool) {
+                        add(r.second);
+                        break;
+                    }
             float best = 1e30f;
-            for (size_t i = 0; i < std::min(kFinalists, ranked.size()); ++i) {
+            for (uint32_t v : finalists) {
                 float ms = 0.0f;
-                if (!time_variant(ranked[i].second, 1, &ms)) return -1;
+                if (!time_variant(v, 1, &ms)) return -1;
                 if (ms < best) {
                     best = ms;
-                    best_v = ranked[i].second;
+                    best_v = v;
                 }
             }
         }

@@ -40,8 +40,13 @@ IX_DEV V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
 IX_DEV V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
 IX_DEV V3 operator*(float s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
 IX_DEV float dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+// glam's cross product, each product rounded before the subtraction in both builds (no
+// multiply-add contraction): parallel inputs then give exactly the zero vector, as on the
+// CPU, which the plane-of-incidence and basis code test for (a contracted product leaves
+// the rounding residual of the other, a nonzero vector in an arbitrary direction).
 IX_DEV V3 cross(V3 a, V3 b) {
-    return v3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+    return v3(__fmul_rn(a.y, b.z) - __fmul_rn(b.y, a.z), __fmul_rn(a.z, b.x) - __fmul_rn(b.z, a.x),
+              __fmul_rn(a.x, b.y) - __fmul_rn(b.x, a.y));
 }
 IX_DEV float length_squared(V3 a) { return dot(a, a); }
 // glam normalize: v * (1 / sqrt(dot(v, v))), IEEE divide and sqrt.
@@ -120,20 +125,31 @@ IX_DEV Stokes fresnel_transmit_apply(const Stokes& s, float n1, float n2, float 
 }
 // MuellerMatrix::tir_retardation (polarization.rs:184):
 // cols (1,0,0,0), (0,1,0,0), (0,0,cd,-sd), (0,0,sd,cd).
+// sin and cos of an f32 angle, each rounded to f32 from a double evaluation: the
+// correctly rounded values in all but the rarest cases, which is what a correctly
+// rounding host libm returns.
+IX_DEV void sincos_f32_rounded(float x, float* s, float* c) {
+    double sd, cd;
+    sincos((double)x, &sd, &cd);
+    *s = (float)sd;
+    *c = (float)cd;
+}
 IX_DEV Stokes tir_retard_apply(const Stokes& s, float delta) {
     float sd, cd;
-    sincosf(delta, &sd, &cd);
+    sincos_f32_rounded(delta, &sd, &cd);
     return Stokes{s.i, s.q, cd * s.u + sd * s.v, (-sd) * s.u + cd * s.v};
 }
 // cos 2psi and sin 2psi of the frame-rotation angle psi = atan2(s, c)
 // (raytracer/absorption.rs:47, polarization.rs:138).  The exact build forms psi and its
-// sincos as the reference does; the fast build uses the double-angle identities
+// sincos as the reference does, each step rounded to f32 from double as a correctly
+// rounding libm would; the fast build uses the double-angle identities
 // cos 2psi = (c^2 - s^2) / (c^2 + s^2), sin 2psi = 2cs / (c^2 + s^2), which need no
 // transcendental (and give psi = 0 for c = s = 0, as atan2 does).
 IX_DEV void rotation_2psi(float sin_psi, float cos_psi, float& c2, float& s2) {
 #if IX_EXACT
-    const float psi = atan2f(sin_psi, cos_psi);
-    sincosf(2.0f * psi, &s2, &c2);
+    // psi and sin / cos of 2 psi, each rounded to f32 from double (see sincos_f32_rounded).
+    const float psi = (float)atan2((double)sin_psi, (double)cos_psi);
+    sincos_f32_rounded(2.0f * psi, &s2, &c2);
 #else
     const float nn = fmaf(cos_psi, cos_psi, sin_psi * sin_psi);
     if (nn > 0.0f) {

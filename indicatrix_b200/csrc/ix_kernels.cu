@@ -499,7 +499,7 @@ __global__ void IX_SFX(check_kernel)(const __grid_constant__ CheckLaunch L) {
             const float n1 = inf(0), n2 = inf(1), cos_i = inf(2);
             const Stokes st{inf(3), inf(4), inf(5), inf(6)};
             const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
-            const float sin_i = sqrtf(fmaxf(one_m_c2, 0.0f));
+            const float sin_i = __fsqrt_rn(fmaxf(one_m_c2, 0.0f));
             const float ratio = __fdiv_rn(n1, n2);
             const float s2k = (ratio * ratio) * one_m_c2;
             for (int i = 0; i < 13; ++i) put(i, 0.0f);

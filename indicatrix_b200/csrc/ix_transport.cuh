@@ -259,12 +259,16 @@ IX_DEV void group_init(const Group& g, LanePath& P, const DevScene& S, uint32_t 
 // Per-channel physics.
 // ------------------------------------------------------------------------------------
 // tir_phase_delta (refraction/tir.rs:33).
+// IEEE square root and division in both builds: near the critical angle the radicand
+// n^2 sin^2 - 1 cancels, and an approximate square root or quotient there moves the
+// retarder by far more than its budget.
 IX_DEV float tir_tan_half(float n1k, float cos_i, float sin_i) {
-    return (cos_i * sqrtf(fmaxf(fmaf(n1k * n1k * sin_i, sin_i, -1.0f), 0.0f))) /
-           fmaxf(n1k * sin_i * sin_i, 1e-6f);
+    return __fdiv_rn(cos_i * __fsqrt_rn(fmaxf(fmaf(n1k * n1k * sin_i, sin_i, -1.0f), 0.0f)),
+                     fmaxf(n1k * sin_i * sin_i, 1e-6f));
 }
 IX_DEV float tir_phase_delta(float n1k, float cos_i, float sin_i) {
-    return 2.0f * atanf(tir_tan_half(n1k, cos_i, sin_i));
+    // atan rounded to f32 from double, as a correctly rounding libm's atanf.
+    return 2.0f * (float)atan((double)tir_tan_half(n1k, cos_i, sin_i));
 }
 // The channel's TIR retarder (tir.rs:98-116, polarization.rs:184).  The fast build forms
 // cos(delta) and sin(delta) of delta = 2 atan(t) without a transcendental:
@@ -604,7 +608,7 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
     // compute_bounce_refraction_geometry (refraction/geometry.rs:306), isotropic.
     const float cos_i = clampf_(dot(-k_hat, normal), 0.0f, 1.0f);
     const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
-    const float sin_i = sqrtf(fmaxf(one_m_c2, 0.0f));
+    const float sin_i = __fsqrt_rn(fmaxf(one_m_c2, 0.0f));  // IEEE: the TIR retarder is ill-conditioned in it
     const float n1 = P.inside ? P.n_hero : 1.0f;
     const float n2 = P.inside ? 1.0f : P.n_hero;
     const float eta = __fdiv_rn(n1, n2);  // IEEE: it decides TIR and the hero's direction
@@ -799,7 +803,7 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     // compute_bounce_refraction_geometry (refraction/geometry.rs:306).
     const float cos_i = clampf_(dot(-k_hat, normal), 0.0f, 1.0f);
     const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
-    const float sin_i = sqrtf(fmaxf(one_m_c2, 0.0f));
+    const float sin_i = __fsqrt_rn(fmaxf(one_m_c2, 0.0f));  // IEEE: the TIR retarder is ill-conditioned in it
     float n_eff = P.n, n_eff_hero = P.n_hero;
     if (aniso) {
         // theta_c_for_bounce (geometry.rs:75): two fixed-point steps on entry.

@@ -90,10 +90,11 @@ def test_frame_map_matches_oracle(exact_backend, oracle):
 
 def test_attributed_sums_equal_plain_sums(backend, exact_backend):
     """The recorder only observes: the attributed call's XYZ sums are the plain call's.
-    Exact build: bit for bit, against every register variant of the plain kernel.  Fast
-    build: bit for bit against the plain kernel of the same register budget (6 CTAs/SM);
-    the compiler contracts multiply-adds differently under the 8-CTA budget, so against
-    that variant the sums agree as two fast-build renders do."""
+    Exact build: bit for bit, against every register variant of the static task loop (the
+    loop the attributed kernel runs).  Fast build: the attributed and plain kernels are
+    separate compilations whose multiply-add contraction may differ, so their sums agree as
+    two fast-build renders of the same samples do (the median pixel within 1e-5, the
+    frame's total within 2e-3: a path whose branch draw flips moves one pixel)."""
     fs = workloads.round_brilliant_frame(40, 32, max_bounces=32)
     _, acc = gpu_map(exact_backend, fs, ISO, 5, 24)
     for variant in (1, 2, 3):
@@ -103,14 +104,11 @@ def test_attributed_sums_equal_plain_sums(backend, exact_backend):
         assert np.array_equal(acc.view(np.uint64), plain.view(np.uint64)), variant
         b.close()
     _, acc = gpu_map(backend, fs, ISO, 5, 24)
-    same_budget = GpuBackend.acquire(precision=abi.PRECISION_FAST, kernel_variant=2)
-    plain = np.zeros((32, 40, 3))
-    assert same_budget.try_accumulate(fs, 5, 24, plain)
-    same_budget.close()
-    assert np.array_equal(acc.view(np.uint64), plain.view(np.uint64))
     default = np.zeros((32, 40, 3))
     assert backend.try_accumulate(fs, 5, 24, default)
-    assert abs(acc.sum() - default.sum()) <= 0.01 * default.sum()
+    rel = np.abs(acc - default) / np.maximum(np.abs(default), 1e-12)
+    assert np.median(rel[default > 0]) <= 1e-5
+    assert abs(acc.sum() - default.sum()) <= 2e-3 * default.sum()
 
 
 def test_chunking_and_sample_split_do_not_change_the_map(oracle):

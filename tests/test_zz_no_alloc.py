@@ -68,8 +68,8 @@ def test_noalloc_entry_rejects_requests_beyond_its_scratch():
                                                  C.c_void_p, C.c_int, C.c_void_p]
     fs = workloads.round_brilliant_frame(8, 8)
     sc, planes = _device_scene(torch, fs)
-    sc.width = 65536
-    sc.height = 65536  # 2^32 pixels x 2 spp: beyond 64 launches of 2^26 paths
+    sc.width = 65535
+    sc.height = 65535  # under 2^32 pixels (larger frames do not route), x 2 spp: beyond 64 launches of 2^26 paths
     out = torch.zeros(3, dtype=torch.float64, device="cuda")
     rc = lib.ix_accumulate_device_noalloc(C.byref(sc), 0, 2, C.c_void_p(out.data_ptr()), 0, None)
     assert rc == IX_NOALLOC_ERR_TOO_LARGE
