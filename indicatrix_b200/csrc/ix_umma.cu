@@ -12,8 +12,9 @@
 //     memory descriptors and commits them to the stage's mbarrier, which the threads wait
 //     on before they refill that stage;
 //   * the accumulator lives in TMEM (NT columns, allocated by warp 0); after the last
-//     commit every warp reads its 32 lanes (tile rows) with tcgen05.ld and applies the
-//     fused epilogue: store, bias + SiLU (forward), or the SiLU derivative (backward).
+//     commit every warp reads its 32 lanes (tile rows) with tcgen05.ld, transposes them
+//     through shared memory and applies the fused epilogue with coalesced stores: store,
+//     bias + SiLU (forward), or the SiLU derivative (backward).
 // Tall-K products with few output tiles (weight gradients: K = the batch) split K over
 // blockIdx.z into f32 partials that a second kernel sums in split order, so results do
 // not depend on scheduling.
@@ -249,9 +250,11 @@ __global__ void __launch_bounds__(THREADS) umma_gemm_kernel(const __grid_constan
     } else {
         tc_fence_after();
         // Epilogue: warp w owns TMEM lanes (tile rows) 32w .. 32w + 31; each tcgen05.ld
-        // gives a thread 8 consecutive columns of its row.
-        const uint32_t row = r0 + warp * 32 + lane;
-        float* out_f32 = P.out_f32 ? P.out_f32 + (size_t)blockIdx.z * P.m * P.ldo : nullptr;
+        // gives a thread 8 consecutive columns of its row.  The warp's 32 x NT block goes
+        // through shared memory (the operand stages are free now; rows padded by one word,
+        // so both passes are conflict-free) and leaves row by row with the lanes on
+        // consecutive columns: every store and every z_prev / bias load is coalesced.
+        float* stage = reinterpret_cast<float*>(smem) + warp * 32 * (NT + 1);
         for (int cc = 0; cc < NT; cc += 8) {
             uint32_t v[8];
             const uint32_t src = taddr + ((warp * 32u) << 16) + (uint32_t)cc;
@@ -260,12 +263,18 @@ __global__ void __launch_bounds__(THREADS) umma_gemm_kernel(const __grid_constan
                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
                 : "r"(src));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row >= P.m) continue;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const uint32_t col = c0 + cc + j;
+            for (int j = 0; j < 8; ++j) stage[lane * (NT + 1) + cc + j] = __uint_as_float(v[j]);
+        }
+        __syncwarp();
+        float* out_f32 = P.out_f32 ? P.out_f32 + (size_t)blockIdx.z * P.m * P.ldo : nullptr;
+        for (int r = 0; r < 32; ++r) {
+            const uint32_t row = r0 + warp * 32 + r;
+            if (row >= P.m) break;
+            for (int c = lane; c < NT; c += 32) {
+                const uint32_t col = c0 + c;
                 if (col >= P.n) break;
-                float x = __uint_as_float(v[j]);
+                float x = stage[r * (NT + 1) + c];
                 const size_t o = (size_t)row * P.ldo + col;
                 if (P.epi == EPI_BIAS_ACT) {
                     if (P.bias) x += P.bias[col];
@@ -299,7 +308,9 @@ __global__ void __launch_bounds__(256) split_sum_kernel(const float* __restrict_
 
 template <int NT>
 cudaError_t launch_nt(const GemmParams& p, uint32_t splits, cudaStream_t st) {
-    const int smem = STAGES * (TM + NT) * BK * 2;
+    // The operand stages, reused by the epilogue's 4 x 32 x (NT + 1) f32 staging.
+    constexpr int stage_bytes = STAGES * (TM + NT) * BK * 2, epi_bytes = 4 * 32 * (NT + 1) * 4;
+    const int smem = stage_bytes > epi_bytes ? stage_bytes : epi_bytes;
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [&] {
