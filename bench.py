@@ -615,7 +615,7 @@ def main_surrogate(args):
     backend = GpuBackend.acquire(device=local)
     if not backend.available:
         raise RuntimeError("libix_cuda.so could not create a backend")
-    spec = S.RenderSpec(width=32, height=32, spp=32)
+    spec = S.RenderSpec(width=32, height=32, spp=64)
     final_spec = S.RenderSpec(width=32, height=32, spp=1024, sample_offset=1 << 21)
     t0 = time.perf_counter()
     train = S.sample_designs(args.designs, 2)
@@ -665,8 +665,8 @@ def main_surrogate(args):
                    "population": args.population, "generations": gens, "retraced_per_generation": 64,
                    "fallback_disagreement": 0.02, "ensemble_members": args.members,
                    "network": "12-256-256-256-27 SiLU, BF16 weights/activations, FP32 accumulation",
-                   "search_render": "32x32, 32 spp, 9 tilts 0-40 deg (split-half image metrics)",
-                   "training_set": f"{args.designs} designs at 32x32, 32 spp, 9 tilts; Adam lr 1e-3 -> 5e-5, "
+                   "search_render": "32x32, 64 spp, 9 tilts 0-40 deg (split-half image metrics)",
+                   "training_set": f"{args.designs} designs at 32x32, 64 spp, 9 tilts; Adam lr 1e-3 -> 5e-5, "
                                    f"batch 4096, {args.epochs} epochs per member",
                    "final_render": "32x32, 1024 spp, 9 tilts, a disjoint sample range",
                    "scale_note": "config 4/5 name 200k designs at 64x64 64 spp and re-renders at 256x256 "
@@ -714,10 +714,10 @@ def main_surrogate(args):
 # DRAM read + write bytes per pixel of one trace-kernel launch, measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on a small case of the same kernel, and
 # how that case was taken.
-DRAM_BYTES_PER_PIXEL = {"batch": 11.75, "stress": 19.7}
+DRAM_BYTES_PER_PIXEL = {"batch": 124.6, "stress": 19.7}
 TRAFFIC_SOURCE = {
-    "batch": "ncu capture of the batch kernel on the first 4 stones x 9 tilts (589,824 pixels), "
-             "per-pixel bytes scaled to this launch's pixels",
+    "batch": "ncu --set full capture of the task-loop batch kernel (32-warp budget) on the first 4 stones x "
+             "9 tilts (589,824 pixels), per-pixel bytes scaled to this launch's pixels",
     "stress": "ncu capture of the stress frame kernel at 128x128 x 256 spp, per-pixel bytes scaled to "
               "this launch's pixels",
 }

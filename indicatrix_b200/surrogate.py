@@ -407,57 +407,71 @@ class SearchResult:
         return self.evaluations / self.seconds if self.seconds > 0 else 0.0
 
 
-def _offspring(rng: np.random.Generator, parents: np.ndarray, n: int, sigma: float) -> np.ndarray:
+def _offspring(rng: np.random.Generator, parents: np.ndarray, n: int, sigma: float,
+               keep_parents: bool = True) -> np.ndarray:
     """n children of the parents: uniform crossover of two random parents, a Gaussian step
-    of sigma x range per parameter, clipped to the box; the parents come first."""
+    of sigma x range per parameter, clipped to the box; with keep_parents the parents
+    come first."""
     k = parents.shape[0]
     a = parents[rng.integers(0, k, n)]
     b = parents[rng.integers(0, k, n)]
     mask = rng.random(a.shape) < 0.5
     child = np.where(mask, a, b) + rng.standard_normal(a.shape) * sigma * (UPPER - LOWER)
     child = np.clip(child, LOWER, UPPER)
-    child[:min(k, n)] = parents[:min(k, n)]
+    if keep_parents:
+        child[:min(k, n)] = parents[:min(k, n)]
     return child
+
+
+def _next_elite(elite_d, elite_m, new_d, new_m, scales, k):
+    """The best k of the current elite and the newly traced designs, by traced score."""
+    if elite_d is not None:
+        new_d = np.concatenate([elite_d, new_d])
+        new_m = np.concatenate([elite_m, new_m])
+    order = np.argsort(-score(new_m, scales), kind="stable")[:k]
+    return new_d[order], new_m[order]
 
 
 def traced_search(backend: GpuBackend, scales: np.ndarray, cfg: SearchConfig = SearchConfig(),
                   spec: RenderSpec = RenderSpec(), evaluate=None) -> SearchResult:
-    """Evolutionary search in which the tracer scores every candidate.  `evaluate` (designs
-    -> metrics [n, 27]) defaults to evaluate_designs on `backend` with `spec`."""
+    """Evolutionary search in which the tracer scores every candidate: each generation
+    traces `population` children of the elite, and the elite becomes the best cfg.elite
+    of itself and the children by traced score.  `evaluate` (designs -> metrics [n, 27])
+    defaults to evaluate_designs on `backend` with `spec`."""
     if evaluate is None:
         evaluate = lambda d: evaluate_designs(backend, d, spec)  # noqa: E731
     rng = np.random.default_rng(cfg.seed)
     pop = sample_designs(cfg.population, cfg.seed)
-    best = None
+    elite_d = elite_m = None
     res = SearchResult(np.zeros(N_FEATURES), np.zeros(N_OUTPUTS), -np.inf)
     t0 = time.perf_counter()
     for _ in range(cfg.generations):
         m = evaluate(pop)
-        s = score(m, scales)
-        order = np.argsort(-s)[:cfg.elite]
-        if best is None or s[order[0]] > best:
-            best = float(s[order[0]])
-            res.best_design, res.best_metrics, res.best_score = pop[order[0]].copy(), m[order[0]].copy(), best
-        res.history.append(best)
+        elite_d, elite_m = _next_elite(elite_d, elite_m, pop, m, scales, cfg.elite)
         res.evaluations += len(pop)
         res.traced += len(pop)
-        pop = _offspring(rng, pop[order], cfg.population, cfg.sigma)
+        res.history.append(float(score(elite_m[:1], scales)[0]))
+        pop = _offspring(rng, elite_d, cfg.population, cfg.sigma, keep_parents=False)
     res.seconds = time.perf_counter() - t0
+    res.best_design, res.best_metrics, res.best_score = elite_d[0].copy(), elite_m[0].copy(), res.history[-1]
     return res
 
 
 def screened_search(backend: GpuBackend, ensemble: SurrogateEnsemble, scales: np.ndarray,
                     cfg: SearchConfig = SearchConfig(), spec: RenderSpec = RenderSpec(),
                     evaluate=None) -> SearchResult:
-    """Evolutionary search in which the ensemble scores every candidate; candidates whose
-    ensemble disagreement exceeds cfg.fallback are scored by the tracer instead, and the
-    best cfg.elite of each generation are re-rendered by the tracer, whose scores rank the
-    parents of the next generation.  `evaluate` as for traced_search."""
+    """Evolutionary search in which the ensemble scores every candidate.  Each generation
+    scores `population` children of the elite with the ensemble; children whose ensemble
+    disagreement exceeds cfg.fallback are scored by the tracer instead, the best
+    cfg.elite children by that score are rendered by the tracer, and the elite becomes the
+    best cfg.elite of itself and every traced child by traced score -- so every reported
+    metric is a traced one and the elite never gets worse.  `evaluate` as for
+    traced_search."""
     if evaluate is None:
         evaluate = lambda d: evaluate_designs(backend, d, spec)  # noqa: E731
     rng = np.random.default_rng(cfg.seed)
     pop = sample_designs(cfg.population, cfg.seed)
-    best = None
+    elite_d = elite_m = None
     res = SearchResult(np.zeros(N_FEATURES), np.zeros(N_OUTPUTS), -np.inf)
     t0 = time.perf_counter()
     for _ in range(cfg.generations):
@@ -468,24 +482,21 @@ def screened_search(backend: GpuBackend, ensemble: SurrogateEnsemble, scales: np
             m_fb = evaluate(pop[fb])
             s[fb] = score(m_fb, scales)
             traced.update({int(i): m_fb[j] for j, i in enumerate(fb)})
-        top = np.argsort(-s)[:cfg.elite]
+        top = np.argsort(-s, kind="stable")[:cfg.elite]
         redo = np.array([i for i in top if int(i) not in traced], np.int64)
         if redo.size:
             m_re = evaluate(pop[redo])
             traced.update({int(i): m_re[j] for j, i in enumerate(redo)})
-        m_top = np.stack([traced[int(i)] for i in top])
-        s_top = score(m_top, scales)
-        order = np.argsort(-s_top)
-        if best is None or s_top[order[0]] > best:
-            best = float(s_top[order[0]])
-            i = top[order[0]]
-            res.best_design, res.best_metrics, res.best_score = pop[i].copy(), m_top[order[0]].copy(), best
-        res.history.append(best)
+        idx = np.array(sorted(traced), np.int64)
+        elite_d, elite_m = _next_elite(elite_d, elite_m, pop[idx], np.stack([traced[int(i)] for i in idx]),
+                                       scales, cfg.elite)
         res.evaluations += len(pop)
         res.traced += fb.size + redo.size
         res.fallbacks += fb.size
-        pop = _offspring(rng, pop[top[order]], cfg.population, cfg.sigma)
+        res.history.append(float(score(elite_m[:1], scales)[0]))
+        pop = _offspring(rng, elite_d, cfg.population, cfg.sigma, keep_parents=False)
     res.seconds = time.perf_counter() - t0
+    res.best_design, res.best_metrics, res.best_score = elite_d[0].copy(), elite_m[0].copy(), res.history[-1]
     return res
 
 

@@ -184,3 +184,36 @@ def test_split_half_metrics_converge_without_noise_bias(backend):
     rel = (tl - th) / th
     # Mean relative deviation per metric across designs: no systematic offset.
     assert np.all(np.abs(rel.mean(axis=0)) < 0.03), rel.mean(axis=0)
+
+
+def test_surrogate_screened_search_against_tracer_only_search(backend):
+    """Config 5 at reduced scale: the 4-member ensemble, trained on traced designs, screens
+    an evolutionary search (population 4096, top 64 re-traced per generation, tracer
+    fallback above 2 % ensemble disagreement) against the same search scored by the tracer
+    alone, both timed the same way (host designs in, host metrics out).  The screened
+    search must deliver >= 20x the design evaluations per second, its final design's
+    metrics must be within 1 % of that design's 1024-spp render, and its final design must
+    score within 3 % of the tracer-only search's."""
+    spec = surrogate.RenderSpec(width=32, height=32, spp=64)
+    train = surrogate.sample_designs(8192, 31)
+    y = surrogate.evaluate_designs(backend, train, spec)
+    scales = surrogate.tilt_means(y).mean(axis=0)
+    ens = surrogate.SurrogateEnsemble(4, seed=3)
+    ens.fit(surrogate.normalize(train), y, epochs=200, batch=4096, lr=1e-3)
+    hold = surrogate.sample_designs(256, 32)
+    y_hold = surrogate.evaluate_designs(backend, hold, surrogate.RenderSpec(spp=1024, sample_offset=1 << 20))
+    _, s_hold, dis = ens.score(surrogate.normalize(hold), scales)
+    s_true = surrogate.score(y_hold, scales)
+    assert np.median(np.abs(s_hold - s_true) / s_true) < 0.05
+    assert np.mean(dis > 0.02) < 0.05
+    cfg = surrogate.SearchConfig(population=4096, generations=6, elite=64, fallback=0.02, seed=7)
+    screened = surrogate.screened_search(backend, ens, scales, cfg, spec)
+    traced = surrogate.traced_search(backend, scales, cfg, spec)
+    assert screened.evaluations == traced.evaluations == 4096 * 6
+    assert screened.evals_per_s >= 20.0 * traced.evals_per_s, (screened.evals_per_s, traced.evals_per_s)
+    final = surrogate.evaluate_designs(backend, np.stack([screened.best_design, traced.best_design]),
+                                       surrogate.RenderSpec(spp=1024, sample_offset=1 << 21))
+    err = surrogate.relative_error(screened.best_metrics, final[0])
+    assert np.all(err <= 0.01), err
+    f = surrogate.score(final, scales)
+    assert f[0] >= 0.97 * f[1], f
