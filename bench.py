@@ -61,7 +61,8 @@ def parse():
     ap.add_argument("--stones", type=int, default=64,
                     help="batch workload: the first N of the 64 seeded stones (profiling small case)")
     ap.add_argument("--variant", type=int, default=-1,
-                    help="batch workload: pin the kernel variant (budget + 3 * shape) instead of autotuning")
+                    help="pin the kernel variant (budget + 3 * shape): the batch plan's instead of "
+                         "autotuning, the frame's instead of the backend's default")
     ap.add_argument("--designs", type=int, default=16384, help="surrogate workload: training designs")
     ap.add_argument("--population", type=int, default=4096, help="surrogate workload: candidates per generation")
     ap.add_argument("--generations", type=int, default=50, help="surrogate workload: search generations")
@@ -765,7 +766,10 @@ def main():
     from indicatrix_b200.backend import GpuBackend
 
     precision = abi.PRECISION_EXACT if args.precision == "exact" else abi.PRECISION_FAST
-    backend = GpuBackend.acquire(device=local, precision=precision)
+    # Frames: a pinned kernel variant goes to the backend (0 = its default per scene);
+    # the batch plan pins or autotunes its own below.
+    frame_variant = args.variant + 1 if (args.variant >= 0 and args.workload != "batch") else 0
+    backend = GpuBackend.acquire(device=local, precision=precision, kernel_variant=frame_variant)
     if not backend.available:
         raise RuntimeError("libix_cuda.so could not create a backend")
 

@@ -92,7 +92,9 @@ ix_backend* ix_backend_create(const ix_backend_options* opts);
 void ix_backend_destroy(ix_backend* b);
 /* GpuBackend::adapter_label (backend.rs:165): device name, NUL-terminated. */
 int ix_backend_label(const ix_backend* b, char* buf, size_t len);
-/* GpuBackend::set_pipeline_kind (backend.rs:165). */
+/* GpuBackend::set_pipeline_kind (backend.rs:165).  Only the megakernel pipeline is built:
+ * IX_PIPELINE_WAVEFRONT is accepted and every call still runs the megakernel (the batch
+ * autotuner chooses among its loops, CTA sizes and register budgets instead). */
 void ix_set_pipeline_kind(ix_backend* b, uint32_t kind);
 /* GpuBackend::set_work_limits (gpu_backend/limits.rs:75). */
 void ix_set_work_limits(ix_backend* b, const ix_work_limits* limits);

@@ -350,6 +350,22 @@ class SurrogateMLP:
             losses.append(float(total.item()) / steps)
         return losses
 
+    def refine(self, x: np.ndarray, t: np.ndarray, steps: int = 10, batch: int = 256, lr: float = 2e-4,
+               seed: int = 0) -> None:
+        """A few Adam steps on (x, t) under the standardisation fit() set, the moments
+        carried on: a search feeds it the designs it has traced, so the network sharpens
+        where the search is going."""
+        torch = self.torch
+        ts = ((t - self.t_mean) / self.t_std).astype(np.float32)
+        xb_all = self.to_device_bf16(x)
+        t_all = torch.from_numpy(ts).to(self.dev)
+        n = x.shape[0]
+        rng = np.random.default_rng(seed)
+        for _ in range(steps):
+            idx = torch.from_numpy(rng.integers(0, n, min(batch, n))).to(self.dev)
+            _, grads = self._gradients_device(xb_all[idx].contiguous(), t_all[idx].contiguous())
+            self._adam(grads, lr)
+
 
 class SurrogateEnsemble:
     """`members` networks of the same shape from different seeds, trained on the same data
@@ -361,6 +377,10 @@ class SurrogateEnsemble:
     def fit(self, x: np.ndarray, t: np.ndarray, **kw) -> List[List[float]]:
         seed = kw.pop("seed", 0)
         return [net.fit(x, t, seed=seed + i, **kw) for i, net in enumerate(self.nets)]
+
+    def refine(self, x: np.ndarray, t: np.ndarray, steps: int = 10, seed: int = 0) -> None:
+        for i, net in enumerate(self.nets):
+            net.refine(x, t, steps=steps, seed=seed + i)
 
     def predict_members(self, x: np.ndarray) -> np.ndarray:
         """[members, m, 27]; one bf16 upload shared by all members."""
@@ -388,6 +408,7 @@ class SearchConfig:
     elite: int = 64          # designs per generation the tracer re-renders / keeps
     sigma: float = 0.05      # mutation step, fraction of each parameter's range
     fallback: float = 0.02   # ensemble disagreement above which the tracer scores a design
+    refine_steps: int = 10   # screened search: Adam steps per member on the traced designs, per generation
     seed: int = 0
 
 
@@ -465,13 +486,16 @@ def screened_search(backend: GpuBackend, ensemble: SurrogateEnsemble, scales: np
     disagreement exceeds cfg.fallback are scored by the tracer instead, the best
     cfg.elite children by that score are rendered by the tracer, and the elite becomes the
     best cfg.elite of itself and every traced child by traced score -- so every reported
-    metric is a traced one and the elite never gets worse.  `evaluate` as for
-    traced_search."""
+    metric is a traced one and the elite never gets worse.  After each generation every
+    member takes cfg.refine_steps Adam steps on all the designs this search has traced
+    (the tracer's renders are the surrogate's training data: where the search goes, the
+    network sharpens).  `evaluate` as for traced_search."""
     if evaluate is None:
         evaluate = lambda d: evaluate_designs(backend, d, spec)  # noqa: E731
     rng = np.random.default_rng(cfg.seed)
     pop = sample_designs(cfg.population, cfg.seed)
     elite_d = elite_m = None
+    seen_d, seen_m = [], []
     res = SearchResult(np.zeros(N_FEATURES), np.zeros(N_OUTPUTS), -np.inf)
     t0 = time.perf_counter()
     for _ in range(cfg.generations):
@@ -488,8 +512,13 @@ def screened_search(backend: GpuBackend, ensemble: SurrogateEnsemble, scales: np
             m_re = evaluate(pop[redo])
             traced.update({int(i): m_re[j] for j, i in enumerate(redo)})
         idx = np.array(sorted(traced), np.int64)
-        elite_d, elite_m = _next_elite(elite_d, elite_m, pop[idx], np.stack([traced[int(i)] for i in idx]),
-                                       scales, cfg.elite)
+        new_m = np.stack([traced[int(i)] for i in idx])
+        elite_d, elite_m = _next_elite(elite_d, elite_m, pop[idx], new_m, scales, cfg.elite)
+        if cfg.refine_steps > 0 and hasattr(ensemble, "refine"):
+            seen_d.append(pop[idx])
+            seen_m.append(new_m)
+            ensemble.refine(normalize(np.concatenate(seen_d)), np.concatenate(seen_m), steps=cfg.refine_steps,
+                            seed=cfg.seed + len(seen_d))
         res.evaluations += len(pop)
         res.traced += fb.size + redo.size
         res.fallbacks += fb.size
