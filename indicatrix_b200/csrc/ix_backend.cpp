@@ -51,6 +51,10 @@ uint32_t pixels_per_task(uint32_t spp) {
 // Kernel variant of single-scene calls when the options name none: the path-pool loop,
 // 128 threads, the 32-warps-per-SM register budget.
 constexpr uint32_t kDefaultVariant = 2 + 3 * ix::SHAPE_POOL_128;
+// Scenes that need the uniaxial transport default to the static task loop with the
+// 16-warp budget: measured fastest for it (the pool loop's larger body costs the bigger
+// uniaxial kernel more instruction fetch than it saves).
+constexpr uint32_t kDefaultUniaxialVariant = 2 + 3 * ix::SHAPE_TASKS;
 
 uint64_t chunk_budget(const ix_backend* b, int launch_index) {
     (void)launch_index;
@@ -65,6 +69,13 @@ uint64_t chunk_budget(const ix_backend* b, int launch_index) {
 // pixels.  With `attr`, every launch is the attributed trace kernel (static task loop),
 // followed by the fold of its records into d_map (the frame's attribution map on the
 // device).  Returns the launch count or -1 on a CUDA error (b->last_error set).
+// The single-scene kernel variant for a scene with transport flags `flags`: the one the
+// options pinned, else the backend's default for its transport.
+uint32_t frame_variant(const ix_backend* b, uint32_t flags) {
+    if (b->variant_pinned) return b->variant;
+    return ix::needs_uniaxial_kernel(flags) ? kDefaultUniaxialVariant : b->variant;
+}
+
 int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uint32_t spp,
                   double* d_out, int accumulate, cudaStream_t stream,
                   const volatile uint8_t* cancel, bool* cancelled,
@@ -83,7 +94,7 @@ int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uin
     L.pixels_per_task = pixels_per_task(spp);
     L.task_counter = b->d_counter;
     L.dropped = b->d_dropped;
-    L.variant = attr ? 0 : (int)b->variant;
+    L.variant = attr ? 0 : (int)frame_variant(b, L.flags);
     const int shape = ix::variant_shape(L.variant);
     const bool pool = ix::shape_is_pool(shape);
     L.threads = ix::shape_threads(shape);
@@ -135,10 +146,10 @@ int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uin
     return launches;
 }
 
-// Kernels one trace launch of the backend's single-scene variant takes: the trace kernel,
-// and for the path-pool shapes the rounding of its fixed-point sums.
-uint32_t kernels_per_launch(const ix_backend* b) {
-    return ix::shape_is_pool(ix::variant_shape((int)b->variant)) ? 2u : 1u;
+// Kernels one trace launch of a scene's single-scene variant takes: the trace kernel, and
+// for the path-pool shapes the rounding of its fixed-point sums.
+uint32_t kernels_per_launch(const ix_backend* b, const ix_scene& sc) {
+    return ix::shape_is_pool(ix::variant_shape((int)frame_variant(b, ix::scene_flags(sc.material)))) ? 2u : 1u;
 }
 
 // Points a device copy of host scene `sc` at the backend's copy of its facet finishes
@@ -212,7 +223,7 @@ int accumulate_impl(ix_backend* b, const ix_scene* scene, uint32_t sample_offset
     b->timing.kernel_ms = ms;
     b->timing.reduce_ms = std::chrono::duration<float, std::milli>(t1 - t0).count();
     b->timing.paths = n_pixels * spp;
-    b->timing.launches = (uint32_t)launches * kernels_per_launch(b);
+    b->timing.launches = (uint32_t)launches * kernels_per_launch(b, sc);
     b->dropped = dropped;
     return IX_DONE;
 }
@@ -437,7 +448,10 @@ ix_backend* ix_backend_create(const ix_backend_options* opts) {
     }
     // Option 0 = the measured default; k >= 1 = variant k - 1 (budget + 3 * shape).
     b->variant = kDefaultVariant;
-    if (opts && opts->kernel_variant >= 1) b->variant = opts->kernel_variant - 1;
+    if (opts && opts->kernel_variant >= 1) {
+        b->variant = opts->kernel_variant - 1;
+        b->variant_pinned = true;
+    }
     if (b->bps_exact[0][b->variant] <= 0 || b->bps_fast[0][b->variant] <= 0) {
         // Single-scene calls run only the variants both builds carry.
         ix_backend_destroy(b);
@@ -1073,7 +1087,7 @@ int ix_accumulate_device(ix_backend* b, const ix_scene* scene, uint32_t sample_o
     if (launches < 0) return IX_DECLINED;
     if (fail(b, cudaEventRecord(b->ev1, st), "event")) return IX_DECLINED;
     b->timing.paths = (uint64_t)scene->width * scene->height * spp;
-    b->timing.launches = (uint32_t)launches * kernels_per_launch(b);
+    b->timing.launches = (uint32_t)launches * kernels_per_launch(b, *scene);
     return IX_DONE;
 }
 

@@ -60,6 +60,7 @@ struct ix_backend {
     int sm_count = 0;
     // Kernel variant (budget + 3 * shape, ix_launch.h) of single-scene calls.
     uint32_t variant = 0;
+    bool variant_pinned = false;  // ix_backend_options.kernel_variant chose it
     // Variant new batch plans start from: the last autotuner pick (or `variant`).
     uint32_t batch_variant = 0;
     // CTA size new batch plans are restricted to (0: any; 64, 128 or 256).

@@ -40,11 +40,15 @@ IX_DEV V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
 IX_DEV V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
 IX_DEV V3 operator*(float s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
 IX_DEV float dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
-// glam's cross product, each product rounded before the subtraction in both builds (no
-// multiply-add contraction): parallel inputs then give exactly the zero vector, as on the
-// CPU, which the plane-of-incidence and basis code test for (a contracted product leaves
-// the rounding residual of the other, a nonzero vector in an arbitrary direction).
 IX_DEV V3 cross(V3 a, V3 b) {
+    return v3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+// glam's cross product with each product rounded before the subtraction in both builds
+// (no multiply-add contraction): parallel inputs give exactly the zero vector, as on the
+// CPU.  For the sites that normalise a cross product or test its length for a degenerate
+// frame (a contracted product leaves the other's rounding residual: a nonzero vector in
+// an arbitrary direction).
+IX_DEV V3 cross_rn(V3 a, V3 b) {
     return v3(__fmul_rn(a.y, b.z) - __fmul_rn(b.y, a.z), __fmul_rn(a.z, b.x) - __fmul_rn(b.z, a.x),
               __fmul_rn(a.x, b.y) - __fmul_rn(b.x, a.y));
 }

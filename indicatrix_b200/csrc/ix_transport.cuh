@@ -197,7 +197,9 @@ IX_DEV Hit group_next_hit(const Group& g, const LanePath& P, const float4* __res
 // incidence's normal normalize_or_zero(k x n); with a previous one, the channel's Stokes
 // vector is rotated by the signed angle between the two planes about k.
 IX_DEV V3 rotate_to_plane_of_incidence(Stokes& st, bool has_prev, V3 prev_pn, V3 k_hat, V3 normal) {
-    const V3 cpn = normalize_or_zero(cross(k_hat, normal));
+    // Uncontracted: at normal incidence k x n is exactly zero and the plane stays undefined
+    // (no rotation), as on the CPU.
+    const V3 cpn = normalize_or_zero(cross_rn(k_hat, normal));
     if (has_prev && length_squared(cpn) > 1e-6f && length_squared(prev_pn) > 1e-6f) {
         float cos_psi = clampf_(dot(prev_pn, cpn), -1.0f, 1.0f);
         float sin_psi = dot(cross(prev_pn, cpn), normalize_or_zero(k_hat));

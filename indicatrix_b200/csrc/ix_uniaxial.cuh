@@ -195,7 +195,7 @@ IX_DEV UFrame uframe_build(V3 k, V3 normal, V3 c, float cos_i, float sin_i) {
         V3 fb = (fabsf(f.zhat.x) < 0.9f) ? v3(1.0f, 0.0f, 0.0f) : v3(0.0f, 1.0f, 0.0f);
         f.that = normalize_or_zero(fb - f.zhat * dot(f.zhat, fb));
     }
-    V3 s = normalize_or_zero(cross(k, normal));
+    V3 s = normalize_or_zero(cross_rn(k, normal));  // uncontracted: exactly zero at normal incidence
     f.s_axis = (length_squared(s) > 1e-8f) ? s : normalize_or_zero(cross(f.zhat, f.that));
     f.cos_i = cos_i;
     f.sin_i = sin_i;
