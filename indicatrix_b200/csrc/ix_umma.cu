@@ -1,9 +1,9 @@
 // ix_umma.cu -- the learned surrogate's GEMMs on the 5th-generation tensor cores.
 //
-// One CTA computes a 128 x NT tile of C = A B^T (A: m x k, B: n x k, both read through
+// One 256-thread CTA computes a 128 x NT tile of C = A B^T (A: m x k, B: n x k, both read through
 // arbitrary row / column strides, so any transpose of the caller's buffers costs nothing
 // extra) over a range of K: BF16 operands, FP32 accumulation in tensor memory.
-//   * all 128 threads stage 64-wide K slices of A and B into shared memory in the
+//   * all 256 threads stage 64-wide K slices of A and B into shared memory in the
 //     tensor cores' K-major, unswizzled canonical layout (8-row x 16-byte core matrices),
 //     zero-filling past the matrix edges, STAGES slices deep: rows contiguous along K go
 //     by 16-byte cp.async (in flight while earlier slices multiply), transposed views
@@ -12,8 +12,9 @@
 //     memory descriptors and commits them to the stage's mbarrier, which the threads wait
 //     on before they refill that stage;
 //   * the accumulator lives in TMEM (NT columns, allocated by warp 0); after the last
-//     commit every warp reads its 32 lanes (tile rows) with tcgen05.ld, transposes them
-//     through shared memory and applies the fused epilogue with coalesced stores: store,
+//     commit each warp reads its lane quadrant's rows (half of the columns) with tcgen05.ld,
+//     transposes them through shared memory and applies the fused epilogue with coalesced
+//     stores: store,
 //     bias + SiLU (forward), or the SiLU derivative (backward).
 // Tall-K products with few output tiles (weight gradients: K = the batch) split K over
 // blockIdx.z into f32 partials that a second kernel sums in split order, so results do
@@ -32,7 +33,7 @@ namespace {
 
 constexpr int TM = 128;        // rows of a tile (the MMA's M)
 constexpr int BK = 64;         // K per stage: four MMAs of K 16
-constexpr int THREADS = 128;
+constexpr int THREADS = 256;      // 8 warps: staging and epilogue split over them
 constexpr int STAGES = 3;      // K slices in shared memory at once
 constexpr uint32_t WAIT_LIMIT = 1u << 24;  // mbarrier polls before a wait gives up
 constexpr int SM_COUNT = 148;
@@ -249,32 +250,35 @@ __global__ void __launch_bounds__(THREADS) umma_gemm_kernel(const __grid_constan
         (void)mbar_wait(&s_bar[last % STAGES], (last / STAGES) & 1u);
     } else {
         tc_fence_after();
-        // Epilogue: warp w owns TMEM lanes (tile rows) 32w .. 32w + 31; each tcgen05.ld
-        // gives a thread 8 consecutive columns of its row.  The warp's 32 x NT block goes
-        // through shared memory (the operand stages are free now; rows padded by one word,
-        // so both passes are conflict-free) and leaves row by row with the lanes on
-        // consecutive columns: every store and every z_prev / bias load is coalesced.
-        float* stage = reinterpret_cast<float*>(smem) + warp * 32 * (NT + 1);
-        for (int cc = 0; cc < NT; cc += 8) {
+        // Epilogue: warp w reads TMEM lane quadrant w % 4 (tile rows 32 (w % 4) ..) and
+        // column half w / 4; each tcgen05.ld gives a thread 8 consecutive columns of its
+        // row.  The warp's 32 x NT/2 block goes through shared memory (the operand stages
+        // are free now; rows padded by one word, so both passes are conflict-free) and
+        // leaves row by row with the lanes on consecutive columns: every store and every
+        // z_prev / bias load is coalesced.
+        constexpr int HW = NT / 2;
+        const uint32_t quad = warp & 3u, half = warp >> 2;
+        float* stage = reinterpret_cast<float*>(smem) + warp * 32 * (HW + 1);
+        for (int cc = 0; cc < HW; cc += 8) {
             uint32_t v[8];
-            const uint32_t src = taddr + ((warp * 32u) << 16) + (uint32_t)cc;
+            const uint32_t src = taddr + ((quad * 32u) << 16) + half * HW + (uint32_t)cc;
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
                 : "r"(src));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int j = 0; j < 8; ++j) stage[lane * (NT + 1) + cc + j] = __uint_as_float(v[j]);
+            for (int j = 0; j < 8; ++j) stage[lane * (HW + 1) + cc + j] = __uint_as_float(v[j]);
         }
         __syncwarp();
         float* out_f32 = P.out_f32 ? P.out_f32 + (size_t)blockIdx.z * P.m * P.ldo : nullptr;
         for (int r = 0; r < 32; ++r) {
-            const uint32_t row = r0 + warp * 32 + r;
+            const uint32_t row = r0 + quad * 32 + r;
             if (row >= P.m) break;
-            for (int c = lane; c < NT; c += 32) {
-                const uint32_t col = c0 + c;
+            for (int c = lane; c < HW; c += 32) {
+                const uint32_t col = c0 + half * HW + c;
                 if (col >= P.n) break;
-                float x = stage[r * (NT + 1) + c];
+                float x = stage[r * (HW + 1) + c];
                 const size_t o = (size_t)row * P.ldo + col;
                 if (P.epi == EPI_BIAS_ACT) {
                     if (P.bias) x += P.bias[col];
@@ -308,8 +312,8 @@ __global__ void __launch_bounds__(256) split_sum_kernel(const float* __restrict_
 
 template <int NT>
 cudaError_t launch_nt(const GemmParams& p, uint32_t splits, cudaStream_t st) {
-    // The operand stages, reused by the epilogue's 4 x 32 x (NT + 1) f32 staging.
-    constexpr int stage_bytes = STAGES * (TM + NT) * BK * 2, epi_bytes = 4 * 32 * (NT + 1) * 4;
+    // The operand stages, reused by the epilogue's 8 warps x 32 x (NT / 2 + 1) f32 staging.
+    constexpr int stage_bytes = STAGES * (TM + NT) * BK * 2, epi_bytes = (THREADS / 32) * 32 * (NT / 2 + 1) * 4;
     const int smem = stage_bytes > epi_bytes ? stage_bytes : epi_bytes;
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
@@ -357,10 +361,10 @@ int run(GemmParams p, void* stream) {
     }
     p.status = static_cast<unsigned int*>(st_ptr);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    // Tile width: the narrowest of 32 / 64 / 128 / 256 that covers n, halved (down to 64)
-    // while the grid would leave SMs idle.
+    // Tile width: the narrowest of 32 / 64 / 128 / 256 that covers n, halved (down to 32)
+    // while the grid would give fewer than two CTAs per SM.
     int nt = p.n <= 32 ? 32 : p.n <= 64 ? 64 : p.n <= 128 ? 128 : 256;
-    while (nt > 64 && tiles(p.m, TM) * tiles(p.n, nt) < (uint32_t)SM_COUNT) nt >>= 1;
+    while (nt > 32 && tiles(p.m, TM) * tiles(p.n, nt) < 2u * SM_COUNT) nt >>= 1;
     // Split K when the output has few tiles and K is long (store epilogue only).
     uint32_t splits = 1;
     const uint32_t n_tiles = tiles(p.m, TM) * tiles(p.n, nt);
