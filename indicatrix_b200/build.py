@@ -57,7 +57,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     jobs = []  # (object, command); the device units compile concurrently
     # The fused build also takes the approximate divide / square root and flushes
     # denormals; the slab scan's division stays IEEE (__fdiv_rn) in both builds.
-    for unit in ("ix_kernels", "ix_pool", "ix_metrics", "ix_display"):
+    for unit in ("ix_kernels", "ix_pool", "ix_wavefront", "ix_metrics", "ix_display"):
         for variant, flags in (("exact", ["-DIX_EXACT=1", "-fmad=false"]),
                                ("fast", ["-DIX_EXACT=0", "-fmad=true", "-prec-div=false",
                                          "-prec-sqrt=false", "-ftz=true"])):

@@ -643,6 +643,7 @@ struct ix_batch_plan {
     unsigned long long* d_dropped = nullptr;
     std::vector<ix::BatchJob> jobs;
     std::vector<uint64_t> job_out;  // first double of each job's sums
+    std::vector<uint32_t> h_max_bounces;  // per scene
     // CUDA graph of [counter reset, batch kernel], rebuilt when the stream or the variant
     // changes.
     cudaGraph_t graph = nullptr;
@@ -652,6 +653,19 @@ struct ix_batch_plan {
     uint32_t variant = 0;
     bool tuned = false;
     bool out_pooled = false;  // d_out is the backend's pooled buffer
+    // The wavefront pipeline's buffers (allocated on its first run) and its two-iteration
+    // CUDA graph.
+    uint32_t* wf_pw = nullptr;
+    uint32_t* wf_lw = nullptr;
+    uint32_t* wf_queues = nullptr;
+    uint32_t* wf_counts = nullptr;
+    unsigned long long* wf_claim = nullptr;
+    uint32_t wf_capacity = 0;
+    unsigned long long* h_wf = nullptr;  // pinned: the claim counter, the next active count
+    cudaGraph_t wf_graph = nullptr;
+    cudaGraphExec_t wf_exec = nullptr;
+    cudaStream_t wf_stream = nullptr;
+    uint32_t wf_iterations = 0;  // of the last wavefront run
     uint8_t* d_finishes = nullptr;  // every scene's facet finishes, back to back
 };
 
@@ -668,6 +682,12 @@ void plan_free_graph(ix_batch_plan* p) {
 // Resident CTAs per SM of batch variant `v` for plan `p` in the backend's rounding build
 // (0: the build does not carry it, or the plan cannot run it).
 int plan_blocks_per_sm(const ix_batch_plan* p, uint32_t v) {
+    if (v == (uint32_t)ix::VARIANT_WAVEFRONT) {
+        // Isotropic plans only; the same padded path space as the pool loop.
+        if (p->uniaxial || !p->pool_ok) return 0;
+        return p->b->precision == IX_PRECISION_EXACT ? ix::wavefront_blocks_per_sm_exact()
+                                                     : ix::wavefront_blocks_per_sm_fast();
+    }
     if (v >= (uint32_t)ix::N_VARIANTS) return 0;
     const int shape = ix::variant_shape((int)v);
     if (ix::shape_is_pool(shape) && !p->pool_ok) return 0;
@@ -678,7 +698,93 @@ int plan_blocks_per_sm(const ix_batch_plan* p, uint32_t v) {
 
 // Enqueues one launch of variant `variant` over every `stride`-th task / chunk of the plan
 // (stride 1: the whole plan) and, for the path-pool shapes, the rounding of its sums.
+// The wavefront pipeline over the whole plan on `st`: start, then iterations from a
+// two-iteration CUDA graph until every path has been claimed and no slot is active (the
+// host reads the claim counter and the next active count every 16 iterations), then the
+// fixed-point sums rounded to f64.  Synchronises `st`.
+cudaError_t plan_run_wavefront(ix_batch_plan* p, cudaStream_t st) {
+    ix_backend* b = p->b;
+    const bool exact = b->precision == IX_PRECISION_EXACT;
+    const int bps = plan_blocks_per_sm(p, ix::VARIANT_WAVEFRONT);
+    if (bps <= 0) return cudaErrorInvalidValue;
+    const uint64_t total_slots = (uint64_t)p->total_chunks * 32ull;
+    const uint64_t pixels = p->out_doubles / 3;
+    cudaError_t e = cudaSuccess;
+    if (!p->wf_pw) {
+        const uint32_t cap = (uint32_t)std::min<uint64_t>(1ull << 20, std::max<uint64_t>(total_slots, 1024));
+        e = cudaMalloc((void**)&p->wf_pw, (size_t)20 * cap * sizeof(uint32_t));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&p->wf_lw, (size_t)11 * 8 * cap * sizeof(uint32_t));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&p->wf_queues, (size_t)ix::WF_QUEUES * cap * sizeof(uint32_t));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&p->wf_counts, ix::WF_QUEUES * sizeof(uint32_t));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&p->wf_claim, sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMallocHost((void**)&p->h_wf, 2 * sizeof(unsigned long long));
+        if (e != cudaSuccess) return e;
+        p->wf_capacity = cap;
+    }
+    ix::WaveLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.scenes = p->d_scenes;
+    L.flags = p->d_flags;
+    L.jobs = p->d_jobs;
+    L.n_jobs = p->n_jobs;
+    L.total_slots = total_slots;
+    L.acc = p->d_acc;
+    L.dropped = p->d_dropped;
+    L.claim = p->wf_claim;
+    L.capacity = p->wf_capacity;
+    L.pw = p->wf_pw;
+    L.lw = p->wf_lw;
+    L.queues = p->wf_queues;
+    L.counts = p->wf_counts;
+    L.blocks = b->sm_count * bps;
+    if (!p->wf_exec || p->wf_stream != st) {
+        if (p->wf_exec) cudaGraphExecDestroy(p->wf_exec);
+        if (p->wf_graph) cudaGraphDestroy(p->wf_graph);
+        p->wf_exec = nullptr;
+        p->wf_graph = nullptr;
+        e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        cudaError_t e1 = exact ? ix::launch_wavefront_iteration_exact(L, 0, st) : ix::launch_wavefront_iteration_fast(L, 0, st);
+        cudaError_t e2 = exact ? ix::launch_wavefront_iteration_exact(L, 1, st) : ix::launch_wavefront_iteration_fast(L, 1, st);
+        cudaError_t e3 = cudaStreamEndCapture(st, &p->wf_graph);
+        if (e1 != cudaSuccess) return e1;
+        if (e2 != cudaSuccess) return e2;
+        if (e3 != cudaSuccess) return e3;
+        e = cudaGraphInstantiate(&p->wf_exec, p->wf_graph, 0);
+        if (e != cudaSuccess) return e;
+        p->wf_stream = st;
+    }
+    e = cudaMemsetAsync(p->d_acc, 0, pixels * ix::FIXED_WORDS * sizeof(unsigned long long), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p->wf_counts, 0, ix::WF_QUEUES * sizeof(uint32_t), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p->wf_claim, 0, sizeof(unsigned long long), st);
+    if (e == cudaSuccess) e = exact ? ix::launch_wavefront_start_exact(L, st) : ix::launch_wavefront_start_fast(L, st);
+    if (e != cudaSuccess) return e;
+    // Every path advances one bounce per iteration and ends within max_bounces + 1 of them,
+    // so the iterations are bounded: a run past the bound is an error, not a wait.  (A slot
+    // whose claim lands in a job's padding retires early, so the slots left carry a few
+    // more paths each; the bound allows twice the even share.)
+    uint32_t max_bounces = 0;
+    for (uint32_t j = 0; j < p->n_scenes; ++j) max_bounces = std::max(max_bounces, p->h_max_bounces[j]);
+    const uint64_t bound = 2 * (total_slots / p->wf_capacity + 2) * (uint64_t)(max_bounces + 2) + 64;
+    uint64_t iterations = 0;
+    for (;;) {
+        for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaGraphLaunch(p->wf_exec, st);
+        iterations += 16;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(p->h_wf, p->wf_claim, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(p->h_wf + 1, p->wf_counts + ix::WF_ACTIVE0, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
+        const uint32_t active = (uint32_t)(p->h_wf[1] & 0xFFFFFFFFull);
+        if (active == 0 && p->h_wf[0] >= total_slots) break;
+        if (iterations > bound) return cudaErrorLaunchTimeout;
+    }
+    p->wf_iterations = (uint32_t)std::min<uint64_t>(iterations, 0xFFFFFFFFull);
+    return ix::launch_fixed_to_f64(p->d_acc, p->d_out, pixels, 0, st);
+}
+
 cudaError_t plan_enqueue(ix_batch_plan* p, cudaStream_t st, uint32_t variant, uint32_t stride = 1) {
+    if (variant == (uint32_t)ix::VARIANT_WAVEFRONT) return plan_run_wavefront(p, st);
     ix_backend* b = p->b;
     const bool exact = b->precision == IX_PRECISION_EXACT;
     const int bps = plan_blocks_per_sm(p, variant);
@@ -717,6 +823,15 @@ cudaError_t plan_enqueue(ix_batch_plan* p, cudaStream_t st, uint32_t variant, ui
 int plan_run_locked(ix_batch_plan* p, cudaStream_t st) {
     ix_backend* b = p->b;
     if (fail(b, cudaSetDevice(b->device), "set device")) return IX_DECLINED;
+    if (p->variant == (uint32_t)ix::VARIANT_WAVEFRONT) {
+        // Host-driven: its iteration count depends on the paths, so it is not one graph.
+        if (fail(b, cudaEventRecord(b->ev0, st), "event")) return IX_DECLINED;
+        if (fail(b, plan_run_wavefront(p, st), "wavefront")) return IX_DECLINED;
+        if (fail(b, cudaEventRecord(b->ev1, st), "event")) return IX_DECLINED;
+        b->timing.paths = p->paths;
+        b->timing.launches = 3 * p->wf_iterations + 2;
+        return IX_DONE;
+    }
     if (!p->exec || p->graph_stream != st || p->graph_variant != (int)p->variant) {
         plan_free_graph(p);
         if (fail(b, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture")) return IX_DECLINED;
@@ -825,6 +940,7 @@ static ix_batch_plan* plan_create_locked(ix_backend* b, const ix_scene* scenes, 
         dev_scenes[i].facet_finishes = has_finishes ? p->d_finishes + finish_off[i] : nullptr;
         dev_scenes[i].n_finishes = has_finishes ? scenes[i].n_finishes : 0;
         flags[i] = ix::scene_flags(scenes[i].material);
+        p->h_max_bounces.push_back(scenes[i].max_bounces);
         if (ix::needs_uniaxial_kernel(flags[i])) p->uniaxial = 1;
         off += (uint64_t)scenes[i].n_planes * 4;
     }
@@ -847,7 +963,9 @@ static ix_batch_plan* plan_create_locked(ix_backend* b, const ix_scene* scenes, 
          cudaMemcpy(p->d_jobs, p->jobs.data(), n_jobs * sizeof(ix::BatchJob), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemset(p->d_dropped, 0, sizeof(unsigned long long)) == cudaSuccess;
     p->variant = b->batch_variant;
-    if (ok && plan_blocks_per_sm(p, p->variant) <= 0) p->variant = ix::variant_budget((int)p->variant);
+    if (b->pipeline == IX_PIPELINE_WAVEFRONT && ok && plan_blocks_per_sm(p, ix::VARIANT_WAVEFRONT) > 0)
+        p->variant = ix::VARIANT_WAVEFRONT;
+    if (ok && plan_blocks_per_sm(p, p->variant) <= 0) p->variant = ix::variant_budget((int)p->variant % ix::N_VARIANTS);
     if (!ok) {
         fail(b, cudaGetLastError(), "batch plan");
         ix_batch_plan_destroy(p);
@@ -924,6 +1042,8 @@ int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen) {
                         add(r.second);
                         break;
                     }
+            // The wavefront pipeline (isotropic plans) runs the whole plan only.
+            if (plan_blocks_per_sm(p, ix::VARIANT_WAVEFRONT) > 0) add((uint32_t)ix::VARIANT_WAVEFRONT);
             float best = 1e30f;
             for (uint32_t v : finalists) {
                 float ms = 0.0f;
@@ -979,6 +1099,14 @@ void ix_batch_plan_destroy(ix_batch_plan* p) {
     cudaFree(p->d_acc);
     cudaFree(p->d_counter);
     cudaFree(p->d_dropped);
+    if (p->wf_exec) cudaGraphExecDestroy(p->wf_exec);
+    if (p->wf_graph) cudaGraphDestroy(p->wf_graph);
+    cudaFree(p->wf_pw);
+    cudaFree(p->wf_lw);
+    cudaFree(p->wf_queues);
+    cudaFree(p->wf_counts);
+    cudaFree(p->wf_claim);
+    if (p->h_wf) cudaFreeHost(p->h_wf);
     (void)cudaGetLastError();
     delete p;
 }

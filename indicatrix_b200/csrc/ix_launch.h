@@ -138,6 +138,37 @@ struct BatchLaunch {
     int variant;                 // budget + 3 * shape
 };
 
+// The wavefront pipeline over a batch plan of isotropic scenes (ix_wavefront.cu): path
+// slots whose state lives in HBM (path words once per path, lane words per channel), six
+// queues of `capacity` slot indices and their counts, and the claim counter over the
+// plan's padded path space (each job's paths start at 32 x its chunk_begin).
+enum : int { WF_ACTIVE0 = 0, WF_ACTIVE1 = 1, WF_REFLECT = 2, WF_REFRACT = 3, WF_FROSTED = 4, WF_FINISH = 5,
+             WF_QUEUES = 6 };
+constexpr int VARIANT_WAVEFRONT = N_VARIANTS;  // the batch plans' variant id of the wavefront
+struct WaveLaunch {
+    const ix_scene* scenes;
+    const uint32_t* flags;
+    const BatchJob* jobs;
+    uint32_t n_jobs;
+    unsigned long long total_slots;  // 32 x the plan's chunks
+    unsigned long long* acc;         // fixed-point sums, FIXED_WORDS per pixel of every job
+    unsigned long long* dropped;
+    unsigned long long* claim;       // next padded path index
+    uint32_t capacity;               // path slots
+    uint32_t* pw;                    // path words, [word][slot]
+    uint32_t* lw;                    // lane words, [word][slot][channel]
+    uint32_t* queues;                // [queue][capacity]
+    uint32_t* counts;                // [queue]
+    int blocks;
+};
+constexpr size_t WF_BYTES_PER_SLOT = (20 + 11 * 8 + WF_QUEUES) * sizeof(uint32_t);
+cudaError_t launch_wavefront_start_exact(const WaveLaunch& l, cudaStream_t stream);
+cudaError_t launch_wavefront_start_fast(const WaveLaunch& l, cudaStream_t stream);
+cudaError_t launch_wavefront_iteration_exact(const WaveLaunch& l, int parity, cudaStream_t stream);
+cudaError_t launch_wavefront_iteration_fast(const WaveLaunch& l, int parity, cudaStream_t stream);
+int wavefront_blocks_per_sm_exact();
+int wavefront_blocks_per_sm_fast();
+
 // Rounds fixed-point sums to f64 (out = sum, or out += sum with `accumulate`), one
 // thread per pixel component.
 cudaError_t launch_fixed_to_f64(const unsigned long long* acc, double* out, uint64_t n_pixels, int accumulate,

@@ -581,130 +581,157 @@ static __device__ __noinline__ ScatterResult scatter_or_survive(Group g, uint32_
 // One iteration of the bounce loop (bounce_body.rs:361-423 and facet_event :611-707).
 // On BOUNCE_ESCAPED `esc` is this channel's escape radiance already weighted by its
 // Stokes intensity (accumulate_miss_radiance, transport/bounce.rs:40).
-IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
-                        const float4* __restrict__ planes, float& esc) {
+// The isotropic bounce in three phases, which the megakernel runs back to back and the
+// wavefront pipeline (ix_wavefront.cu) runs in separate kernels with the path state in
+// HBM between them:
+//   bounce_hit       the intersection; at a facet, the Stokes frame rotation and the
+//                    interior segment's absorption (the path state's only changes);
+//   bounce_geometry  the facet's refraction geometry and the dispatch decision (frosted,
+//                    reflect, refract) -- a pure function of the path state and t, so the
+//                    wavefront recomputes it after the state's round trip through HBM;
+//   bounce_arm       the chosen arm, the new ray, surface glare and roulette.
+struct BounceGeom {
+    V3 normal, hit_point, k_hat;
+    float cos_i, one_m_c2, sin_i, n1, n2, eta, sin2_t, n1k, n2k, r_unpol;
+    bool tir, reflect, frosted;
+    // the channel's own Snell geometry and Fresnel amplitudes at its index
+    float ratio, s2k, cos_t_k, rs, rp, r_k;
+    bool lane_tir;
+};
+
+// Returns BOUNCE_ESCAPED (esc set) or BOUNCE_CONTINUE with P.facet the hit facet and `t`
+// its distance.
+IX_DEV int bounce_hit(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes, float& esc,
+                      float& t) {
     const ix_scene& sc = S.s;
-    const uint32_t bounce = P.bounce;
-    const int n_planes = (int)sc.n_planes;
-    Hit hit = group_next_hit(g, P, planes, n_planes);
+    Hit hit = group_next_hit(g, P, planes, (int)sc.n_planes);
     if (hit.facet < 0) {
         esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         return BOUNCE_ESCAPED;
     }
     P.facet = hit.facet;
+    t = hit.t;
     const float4 pl = planes[hit.facet];
-    V3 normal = v3(pl.x, pl.y, pl.z);
-    const V3 hit_point = P.o + hit.t * P.d;
+    const V3 normal = v3(pl.x, pl.y, pl.z);
     const V3 k_hat = P.d;  // isotropic: wave normal == ray direction
-
     const V3 cpn = rotate_to_plane_of_incidence(P.st, P.has_prev, P.prev_pn, k_hat, normal);
     P.has_prev = true;
     P.prev_pn = cpn;
-
     // apply_interior_segment (transport/inner.rs:170).
-    if (P.inside) {
-        normal = -normal;
-        if (S.absorbing) lane_absorption(P, S, k_hat, hit.t);
-    }
+    if (P.inside && S.absorbing) lane_absorption(P, S, k_hat, hit.t);
+    return BOUNCE_CONTINUE;
+}
 
+IX_DEV void bounce_geometry(const LanePath& P, const DevScene& S, const float4* __restrict__ planes, float t,
+                            BounceGeom& G) {
+    const float4 pl = planes[P.facet];
+    G.k_hat = P.d;
+    G.hit_point = P.o + t * P.d;
+    G.normal = P.inside ? -v3(pl.x, pl.y, pl.z) : v3(pl.x, pl.y, pl.z);
     // compute_bounce_refraction_geometry (refraction/geometry.rs:306), isotropic.
-    const float cos_i = clampf_(dot(-k_hat, normal), 0.0f, 1.0f);
-    const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
-    const float sin_i = __fsqrt_rn(fmaxf(one_m_c2, 0.0f));  // IEEE: the TIR retarder is ill-conditioned in it
-    const float n1 = P.inside ? P.n_hero : 1.0f;
-    const float n2 = P.inside ? 1.0f : P.n_hero;
-    const float eta = __fdiv_rn(n1, n2);  // IEEE: it decides TIR and the hero's direction
-    const float sin2_t = eta * eta * one_m_c2;
-    const float n1k = P.inside ? P.n : 1.0f;
-    const float n2k = P.inside ? 1.0f : P.n;
-
+    G.cos_i = clampf_(dot(-G.k_hat, G.normal), 0.0f, 1.0f);
+    G.one_m_c2 = fmaf(G.cos_i, -G.cos_i, 1.0f);
+    G.sin_i = __fsqrt_rn(fmaxf(G.one_m_c2, 0.0f));  // IEEE: the TIR retarder is ill-conditioned in it
+    G.n1 = P.inside ? P.n_hero : 1.0f;
+    G.n2 = P.inside ? 1.0f : P.n_hero;
+    G.eta = __fdiv_rn(G.n1, G.n2);  // IEEE: it decides TIR and the hero's direction
+    G.sin2_t = G.eta * G.eta * G.one_m_c2;
+    G.n1k = P.inside ? P.n : 1.0f;
+    G.n2k = P.inside ? 1.0f : P.n;
     // dispatch_bounce (transport/bounce.rs:108): a frosted facet scatters diffusely;
     // otherwise the hero decides TIR (sin2_t > 1), else apply_partial_fresnel_bounce
     // (refraction/dispatch.rs:307) draws reflect vs refract.
-    const bool tir = sin2_t > 1.0f;
-    float r_unpol = 1.0f;
-    bool reflect = tir;
-    if (!tir) {
-        float cos_t = sqrtf(fmaxf(1.0f - sin2_t, 0.0f));
+    G.tir = G.sin2_t > 1.0f;
+    G.r_unpol = 1.0f;
+    G.reflect = G.tir;
+    if (!G.tir) {
+        float cos_t = sqrtf(fmaxf(1.0f - G.sin2_t, 0.0f));
         float r_s, r_p;
-        fresnel_rs_rp(n1, n2, cos_i, cos_t, r_s, r_p);
-        r_unpol = clampf_(r_unpol_of(r_s, r_p), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
-        reflect = unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM) < r_unpol;
+        fresnel_rs_rp(G.n1, G.n2, G.cos_i, cos_t, r_s, r_p);
+        G.r_unpol = clampf_(r_unpol_of(r_s, r_p), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
+        G.reflect = unit_draw(P.seed, P.bounce, FRESNEL_BRANCH_STREAM) < G.r_unpol;
     }
-    const bool frosted = facet_frosted(S, hit.facet);
+    G.frosted = facet_frosted(S, P.facet);
     // The channel's own Snell geometry and Fresnel amplitudes at its index, which the
-    // reflect and refract arms below both use: formed once here, before the arms split
-    // the warp's groups, instead of once in each arm.
-    const float ratio = __fdiv_rn(n1k, n2k);
-    const float s2k = (ratio * ratio) * one_m_c2;
-    const bool lane_tir = s2k > 1.0f;
-    const float cos_t_k = lane_tir ? 0.0f : __fsqrt_rn(fmaxf(1.0f - s2k, 0.0f));
-    float rs = 1.0f, rp = 1.0f;
-    if (!lane_tir) fresnel_rs_rp(n1k, n2k, cos_i, cos_t_k, rs, rp);
-    const float r_k = clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+    // reflect and refract arms both use: formed once here, before the arms split the
+    // warp's groups, instead of once in each arm.
+    G.ratio = __fdiv_rn(G.n1k, G.n2k);
+    G.s2k = (G.ratio * G.ratio) * G.one_m_c2;
+    G.lane_tir = G.s2k > 1.0f;
+    G.cos_t_k = G.lane_tir ? 0.0f : __fsqrt_rn(fmaxf(1.0f - G.s2k, 0.0f));
+    G.rs = 1.0f;
+    G.rp = 1.0f;
+    if (!G.lane_tir) fresnel_rs_rp(G.n1k, G.n2k, G.cos_i, G.cos_t_k, G.rs, G.rp);
+    G.r_k = clampf_(r_unpol_of(G.rs, G.rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX);
+}
+
+// Returns BOUNCE_CONTINUE or BOUNCE_KILLED (roulette).
+IX_DEV int bounce_arm(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes,
+                      const BounceGeom& G) {
+    const uint32_t bounce = P.bounce;
     V3 new_dir;
     bool new_inside = P.inside;
-    if (frosted) {
-        const FrostedScatter f = frosted_scatter(P.seed, bounce, normal, n1, n2, cos_i, sin2_t);
+    if (G.frosted) {
+        const FrostedScatter f = frosted_scatter(P.seed, bounce, G.normal, G.n1, G.n2, G.cos_i, G.sin2_t);
         lane_frosted_apply(P, f);
         new_dir = f.dir;
         if (f.transmit) new_inside = !P.inside;
-    } else if (reflect) {
+    } else if (G.reflect) {
         // apply_tir_bounce (tir.rs:98-116) / apply_partial_reflect_bounce
         // (reflect_refract.rs:33): the channel's TIR retarder or Fresnel reflection; a
         // partial reflection divides by the selection probability (TIR scales by 1).
         Stokes s;
-        if (lane_tir) {
-            s = tir_retard(P.st, n1k, cos_i, sin_i);
+        if (G.lane_tir) {
+            s = tir_retard(P.st, G.n1k, G.cos_i, G.sin_i);
         } else {
-            s = fresnel_reflect_apply(P.st, rs, rp);
-            P.pdf = P.pdf * r_k;
+            s = fresnel_reflect_apply(P.st, G.rs, G.rp);
+            P.pdf = P.pdf * G.r_k;
         }
-        P.st = scale(s, tir ? 1.0f : 1.0f / r_unpol);
-        new_dir = k_hat - 2.0f * dot(k_hat, normal) * normal;
+        P.st = scale(s, G.tir ? 1.0f : 1.0f / G.r_unpol);
+        new_dir = G.k_hat - 2.0f * dot(G.k_hat, G.normal) * G.normal;
     } else {
         // apply_refract_bounce (reflect_refract.rs:121): the hero's direction, then each
         // channel's own Snell direction, transmission and direction match
         // (apply_refract_channel :517, compute_channel_refraction_geometry :255).
-        const float sin2_t_dir = fminf(eta * eta * one_m_c2, 1.0f);
+        const float sin2_t_dir = fminf(G.eta * G.eta * G.one_m_c2, 1.0f);
         // The directions entering the match test take IEEE divide / sqrt (normalize_dir).
         const float cos_t_dir = __fsqrt_rn(fmaxf(1.0f - sin2_t_dir, 0.0f));
-        const V3 final_refr = normalize_dir(eta * k_hat + fmaf(eta, cos_i, -cos_t_dir) * normal);
+        const V3 final_refr = normalize_dir(G.eta * G.k_hat + fmaf(G.eta, G.cos_i, -cos_t_dir) * G.normal);
         int status = 0;  // 0 channel TIR, 1 direction matches the hero, 2 diverges
         V3 dir_k = v3(0.0f, 0.0f, 0.0f);
         float t_intensity = 0.0f;
         const Stokes original = P.st;
-        if (lane_tir) {
+        if (G.lane_tir) {
             P.st = scale(P.st, 0.0f);
             P.pdf = 0.0f;
         } else {
-            dir_k = normalize_dir(ratio * k_hat + fmaf(ratio, cos_i, -cos_t_k) * normal);
+            dir_k = normalize_dir(G.ratio * G.k_hat + fmaf(G.ratio, G.cos_i, -G.cos_t_k) * G.normal);
             status = dot(dir_k, final_refr) >= DIRECTION_MATCH_COS_TOL ? 1 : 2;
-            const float two = 2.0f * n1k * cos_i;
-            const float t_s = two / fmaf(n2k, cos_t_k, n1k * cos_i);
-            const float t_p = two / fmaf(n1k, cos_t_k, n2k * cos_i);
+            const float two = 2.0f * G.n1k * G.cos_i;
+            const float t_s = two / fmaf(G.n2k, G.cos_t_k, G.n1k * G.cos_i);
+            const float t_p = two / fmaf(G.n1k, G.cos_t_k, G.n2k * G.cos_i);
             const Stokes transmitted =
-                scale(fresnel_transmit_apply(original, n1k, n2k, cos_i, cos_t_k, t_s, t_p),
-                      1.0f / (1.0f - r_unpol));
-            P.pdf = P.pdf * (1.0f - r_k);
+                scale(fresnel_transmit_apply(original, G.n1k, G.n2k, G.cos_i, G.cos_t_k, t_s, t_p),
+                      1.0f / (1.0f - G.r_unpol));
+            P.pdf = P.pdf * (1.0f - G.r_k);
             // apply_channel_chromatic_termination (reflect_refract.rs:444): a diverging
             // channel's radiance is zeroed (its pdf keeps accumulating).
             P.st = status == 1 ? transmitted : scale(original, 0.0f);
             t_intensity = intensity(transmitted);
         }
-        group_exit_probes(g, P, S, planes, hit_point, status == 2 && P.inside && intensity(original) > 0.0f,
+        group_exit_probes(g, P, S, planes, G.hit_point, status == 2 && P.inside && intensity(original) > 0.0f,
                           dir_k, t_intensity);
         if (!P.inside) group_narrow_compat(g, P, status, dir_k);
         new_dir = final_refr;
         new_inside = !P.inside;
     }
     P.d = new_dir;
-    P.o = hit_point + new_dir * 1e-4f;
+    P.o = G.hit_point + new_dir * 1e-4f;
     P.inside = new_inside;
 
     // Surface glare (bounce_body.rs:691-697): the outside reflection of a polished facet.
-    const float glare = clampf_(sc.environment.surface_glare, 0.0f, 1.0f);
-    if (bounce == 0 && !P.inside && glare < 1.0f && !frosted) P.st = scale(P.st, glare);
+    const float glare = clampf_(S.s.environment.surface_glare, 0.0f, 1.0f);
+    if (bounce == 0 && !P.inside && glare < 1.0f && !G.frosted) P.st = scale(P.st, glare);
     // apply_russian_roulette (transport/bounce.rs:355): q from the brightest channel.
     if (bounce > 4) {
         float max_i = intensity(P.st);
@@ -717,6 +744,15 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
     }
     P.bounce = bounce + 1;
     return BOUNCE_CONTINUE;
+}
+
+IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
+                        const float4* __restrict__ planes, float& esc) {
+    float t = 0.0f;
+    if (bounce_hit(g, P, S, planes, esc, t) == BOUNCE_ESCAPED) return BOUNCE_ESCAPED;
+    BounceGeom G;
+    bounce_geometry(P, S, planes, t, G);
+    return bounce_arm(g, P, S, planes, G);
 }
 
 // ------------------------------------------------------------------------------------

@@ -455,7 +455,7 @@ def test_batch_plan_one_launch_matches_single_scene_calls(backend):
         assert backend.try_accumulate(fs, off, spp, single)
         assert np.array_equal(plan.sums(j), single)
     chosen = plan.autotune(reps=1)
-    assert 0 <= chosen < 12  # budget + 3 * shape: static tasks, or the path pool at 128 / 64 / 256 threads
+    assert 0 <= chosen <= 12  # budget + 3 * shape (static tasks, the path pool at 128 / 64 / 256 threads), 12 wavefront
     # The register variants are separate compilations; in the fused-rounding build their
     # multiply-add contraction may differ, so bits are compared within a variant and the
     # variants against each other statistically.
@@ -469,9 +469,10 @@ def test_batch_plan_one_launch_matches_single_scene_calls(backend):
 
 def test_every_batch_variant_in_the_exact_build(exact_backend):
     """Every kernel variant the exact build carries (the static task loop under each
-    register budget, the path-pool loop) traces the same batch: the pool's fixed-point sums
-    are order-independent and exact, so every pool variant gives the same bits; the task
-    loop's ascending-order f64 sums agree with them to f64 rounding."""
+    register budget, the path-pool loop, the wavefront pipeline) traces the same batch: the
+    pool's and the wavefront's fixed-point sums are order-independent and exact, so they
+    give the same bits; the task loop's ascending-order f64 sums agree with them to f64
+    rounding."""
     from indicatrix_b200.backend import BatchPlan
 
     stones = workloads.random_stones(3, seed=8)
@@ -479,17 +480,41 @@ def test_every_batch_variant_in_the_exact_build(exact_backend):
     plan = BatchPlan(exact_backend, jobs)
     by_shape = {}
     ran = []
-    for v in range(12):
+    for v in range(13):  # 12: the wavefront pipeline, fixed-point sums like the pool loop
         if not plan.set_variant(v):
             continue
         plan.run()
         out = plan.download().copy()
         ran.append(v)
         by_shape.setdefault(v // 3 == 0, []).append(out)
-    assert 0 in ran and any(v >= 3 for v in ran), ran
+    assert 0 in ran and any(3 <= v < 12 for v in ran) and 12 in ran, ran
     for outs in by_shape.values():
         for o in outs[1:]:
             assert np.array_equal(o.view(np.uint64), outs[0].view(np.uint64))
     tasks, pool = by_shape[True][0], by_shape[False][0]
     assert np.all(np.abs(tasks - pool) <= 1e-12 * np.maximum(np.abs(pool), 1e-300))
+    plan.close()
+
+
+def test_wavefront_pipeline_matches_the_megakernel(backend):
+    """The wavefront pipeline (variant 12: path state in HBM, sort-by-event queues) on the
+    fast build against the pool megakernel on the same batch: separate compilations, so
+    per pixel they agree as two renders of the same samples do (the median pixel within
+    1e-5, the total within 1e-3); both take the same paths (the path counts agree)."""
+    from indicatrix_b200.backend import BatchPlan
+
+    stones = workloads.random_stones(4, seed=12)
+    jobs = [(workloads.tilted_scene(st, tilt, 32, 24), 0, 16) for st in stones for tilt in (0.0, 25.0)]
+    plan = BatchPlan(backend, jobs)
+    assert plan.set_variant(5)
+    plan.run()
+    mega = plan.download().copy()
+    assert plan.set_variant(12)
+    plan.run()
+    wave = plan.download().copy()
+    plan.run()
+    assert np.array_equal(plan.download(), wave)  # deterministic
+    rel = np.abs(wave - mega) / np.maximum(np.abs(mega), 1e-12)
+    assert np.median(rel[mega > 0]) <= 1e-5
+    assert abs(wave.sum() - mega.sum()) <= 1e-3 * mega.sum()
     plan.close()
