@@ -92,9 +92,10 @@ ix_backend* ix_backend_create(const ix_backend_options* opts);
 void ix_backend_destroy(ix_backend* b);
 /* GpuBackend::adapter_label (backend.rs:165): device name, NUL-terminated. */
 int ix_backend_label(const ix_backend* b, char* buf, size_t len);
-/* GpuBackend::set_pipeline_kind (backend.rs:165).  Only the megakernel pipeline is built:
- * IX_PIPELINE_WAVEFRONT is accepted and every call still runs the megakernel (the batch
- * autotuner chooses among its loops, CTA sizes and register budgets instead). */
+/* GpuBackend::set_pipeline_kind (backend.rs:165).  IX_PIPELINE_WAVEFRONT makes batch plans
+ * created afterwards start on the wavefront pipeline (variant 12 of ix_batch_plan_*: path
+ * state in device memory between kernels, one kernel per event queue) when every scene is
+ * isotropic; single-scene calls and uniaxial plans run the megakernel either way. */
 void ix_set_pipeline_kind(ix_backend* b, uint32_t kind);
 /* GpuBackend::set_work_limits (gpu_backend/limits.rs:75). */
 void ix_set_work_limits(ix_backend* b, const ix_work_limits* limits);
@@ -149,14 +150,16 @@ int ix_batch_plan_run(ix_batch_plan* p, void* stream);
  * times every kernel variant this build carries -- the static task loop and the
  * path-pool loop at 64, 128 and 256 threads per CTA, each under three register budgets
  * (variant = budget + 3 * shape) -- `reps` times on a strided sample of about 1/16 of
- * the plan's work (every job represented), then runs the two fastest and the fastest of
- * each loop (static tasks, path pool) on the whole plan once each, keeps the fastest of
- * those and writes it to `chosen`.
+ * the plan's work (every job represented), then runs the two fastest, the fastest of each
+ * loop (static tasks, path pool) and, for an isotropic plan, the wavefront pipeline
+ * (variant 12) on the whole plan once each, keeps the fastest of those and writes it to
+ * `chosen`.
  * With ix_backend_options.threads_per_block set, only that CTA size is tried.
  * Returns 0, or -1 on a device error. */
 int ix_batch_plan_autotune(ix_batch_plan* p, int reps, uint32_t* chosen);
-/* Pins the plan's kernel variant (budget + 3 * shape, see ix_batch_plan_autotune).
- * Returns 0, or -1 when this build or this plan cannot run it. */
+/* Pins the plan's kernel variant (budget + 3 * shape, or 12 for the wavefront pipeline;
+ * see ix_batch_plan_autotune).  Returns 0, or -1 when this build or this plan cannot run
+ * it. */
 int ix_batch_plan_set_variant(ix_batch_plan* p, uint32_t variant);
 /* Copies the plan's sums to host memory (ix_batch_plan_output_size doubles). */
 int ix_batch_plan_download(ix_batch_plan* p, double* host_out);

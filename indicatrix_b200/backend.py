@@ -615,7 +615,8 @@ class BatchPlan:
         return int(v.value)
 
     def set_variant(self, variant: int) -> bool:
-        """Pins the kernel variant (budget + 3 * shape); False when it cannot run here."""
+        """Pins the kernel variant (budget + 3 * shape, or 12: the wavefront pipeline);
+        False when it cannot run here."""
         return self._lib.ix_batch_plan_set_variant(self._h, int(variant)) == 0
 
     @property
