@@ -712,7 +712,7 @@ cudaError_t plan_run_wavefront(ix_batch_plan* p, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
     if (!p->wf_pw) {
         const uint32_t cap = (uint32_t)std::min<uint64_t>(1ull << 20, std::max<uint64_t>(total_slots, 1024));
-        e = cudaMalloc((void**)&p->wf_pw, (size_t)20 * cap * sizeof(uint32_t));
+        e = cudaMalloc((void**)&p->wf_pw, (size_t)32 * cap * sizeof(uint32_t));  // one 128-byte line per slot
         if (e == cudaSuccess) e = cudaMalloc((void**)&p->wf_lw, (size_t)11 * 8 * cap * sizeof(uint32_t));
         if (e == cudaSuccess) e = cudaMalloc((void**)&p->wf_queues, (size_t)ix::WF_QUEUES * cap * sizeof(uint32_t));
         if (e == cudaSuccess) e = cudaMalloc((void**)&p->wf_counts, ix::WF_QUEUES * sizeof(uint32_t));

@@ -155,13 +155,12 @@ struct WaveLaunch {
     unsigned long long* dropped;
     unsigned long long* claim;       // next padded path index
     uint32_t capacity;               // path slots
-    uint32_t* pw;                    // path words, [word][slot]
+    uint32_t* pw;                    // path words, [slot][32] (20 used)
     uint32_t* lw;                    // lane words, [word][slot][channel]
     uint32_t* queues;                // [queue][capacity]
     uint32_t* counts;                // [queue]
     int blocks;
 };
-constexpr size_t WF_BYTES_PER_SLOT = (20 + 11 * 8 + WF_QUEUES) * sizeof(uint32_t);
 cudaError_t launch_wavefront_start_exact(const WaveLaunch& l, cudaStream_t stream);
 cudaError_t launch_wavefront_start_fast(const WaveLaunch& l, cudaStream_t stream);
 cudaError_t launch_wavefront_iteration_exact(const WaveLaunch& l, int parity, cudaStream_t stream);

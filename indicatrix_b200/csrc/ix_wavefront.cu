@@ -51,7 +51,11 @@ struct Slot {
     bool escaped;
 };
 
-IX_DEV uint32_t* pw_at(const WaveLaunch& L, uint32_t w, uint32_t slot) { return L.pw + (size_t)w * L.capacity + slot; }
+// A slot's path words share one 128-byte line ([slot][32]): the group's loads of them all
+// hit the line its first load brought in.  Lane words are [word][slot][channel]: a group
+// reads or writes each word as one 32-byte sector.
+constexpr uint32_t PW_STRIDE = 32;
+IX_DEV uint32_t* pw_at(const WaveLaunch& L, uint32_t w, uint32_t slot) { return L.pw + (size_t)slot * PW_STRIDE + w; }
 IX_DEV uint32_t* lw_at(const WaveLaunch& L, uint32_t w, uint32_t slot, int c) {
     return L.lw + (size_t)w * L.capacity * 8 + (size_t)slot * 8 + c;
 }
