@@ -656,7 +656,6 @@ struct ix_batch_plan {
     // The wavefront pipeline's buffers (allocated on its first run) and its two-iteration
     // CUDA graph.
     uint32_t* wf_pw = nullptr;
-    uint32_t* wf_lw = nullptr;
     uint32_t* wf_queues = nullptr;
     uint32_t* wf_counts = nullptr;
     unsigned long long* wf_claim = nullptr;
@@ -712,8 +711,8 @@ cudaError_t plan_run_wavefront(ix_batch_plan* p, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
     if (!p->wf_pw) {
         const uint32_t cap = (uint32_t)std::min<uint64_t>(1ull << 20, std::max<uint64_t>(total_slots, 1024));
-        e = cudaMalloc((void**)&p->wf_pw, (size_t)32 * cap * sizeof(uint32_t));  // one 128-byte line per slot
-        if (e == cudaSuccess) e = cudaMalloc((void**)&p->wf_lw, (size_t)11 * 8 * cap * sizeof(uint32_t));
+        // One 512-byte state record per slot (path words, then lane words).
+        e = cudaMalloc((void**)&p->wf_pw, (size_t)128 * cap * sizeof(uint32_t));
         if (e == cudaSuccess) e = cudaMalloc((void**)&p->wf_queues, (size_t)ix::WF_QUEUES * cap * sizeof(uint32_t));
         if (e == cudaSuccess) e = cudaMalloc((void**)&p->wf_counts, ix::WF_QUEUES * sizeof(uint32_t));
         if (e == cudaSuccess) e = cudaMalloc((void**)&p->wf_claim, sizeof(unsigned long long));
@@ -733,7 +732,6 @@ cudaError_t plan_run_wavefront(ix_batch_plan* p, cudaStream_t st) {
     L.claim = p->wf_claim;
     L.capacity = p->wf_capacity;
     L.pw = p->wf_pw;
-    L.lw = p->wf_lw;
     L.queues = p->wf_queues;
     L.counts = p->wf_counts;
     L.blocks = b->sm_count * bps;
@@ -1102,7 +1100,6 @@ void ix_batch_plan_destroy(ix_batch_plan* p) {
     if (p->wf_exec) cudaGraphExecDestroy(p->wf_exec);
     if (p->wf_graph) cudaGraphDestroy(p->wf_graph);
     cudaFree(p->wf_pw);
-    cudaFree(p->wf_lw);
     cudaFree(p->wf_queues);
     cudaFree(p->wf_counts);
     cudaFree(p->wf_claim);

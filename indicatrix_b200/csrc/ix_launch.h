@@ -139,7 +139,8 @@ struct BatchLaunch {
 };
 
 // The wavefront pipeline over a batch plan of isotropic scenes (ix_wavefront.cu): path
-// slots whose state lives in HBM (path words once per path, lane words per channel), six
+// slots whose state lives in HBM (one record per slot: path words once per path, lane
+// words per channel), six
 // queues of `capacity` slot indices and their counts, and the claim counter over the
 // plan's padded path space (each job's paths start at 32 x its chunk_begin).
 enum : int { WF_ACTIVE0 = 0, WF_ACTIVE1 = 1, WF_REFLECT = 2, WF_REFRACT = 3, WF_FROSTED = 4, WF_FINISH = 5,
@@ -155,8 +156,7 @@ struct WaveLaunch {
     unsigned long long* dropped;
     unsigned long long* claim;       // next padded path index
     uint32_t capacity;               // path slots
-    uint32_t* pw;                    // path words, [slot][32] (20 used)
-    uint32_t* lw;                    // lane words, [word][slot][channel]
+    uint32_t* pw;                    // state records, [slot][128]: path words, then lane words
     uint32_t* queues;                // [queue][capacity]
     uint32_t* counts;                // [queue]
     int blocks;

@@ -51,13 +51,15 @@ struct Slot {
     bool escaped;
 };
 
-// A slot's path words share one 128-byte line ([slot][32]): the group's loads of them all
-// hit the line its first load brought in.  Lane words are [word][slot][channel]: a group
-// reads or writes each word as one 32-byte sector.
-constexpr uint32_t PW_STRIDE = 32;
-IX_DEV uint32_t* pw_at(const WaveLaunch& L, uint32_t w, uint32_t slot) { return L.pw + (size_t)slot * PW_STRIDE + w; }
+// A slot's state is one contiguous 512-byte record: its path words in the first 128 bytes
+// and, from word 32 on, its lane words channel-minor (lane word w of channel c at
+// 32 + 8 w + c), so a group reads or writes each lane word as one 32-byte sector of the
+// same record and a path's state occupies 4 whole lines of DRAM.
+constexpr uint32_t SLOT_WORDS = 128;
+constexpr uint32_t LW_BASE = 32;
+IX_DEV uint32_t* pw_at(const WaveLaunch& L, uint32_t w, uint32_t slot) { return L.pw + (size_t)slot * SLOT_WORDS + w; }
 IX_DEV uint32_t* lw_at(const WaveLaunch& L, uint32_t w, uint32_t slot, int c) {
-    return L.lw + (size_t)w * L.capacity * 8 + (size_t)slot * 8 + c;
+    return L.pw + (size_t)slot * SLOT_WORDS + LW_BASE + w * 8 + c;
 }
 IX_DEV float ldf(const uint32_t* p) { return __uint_as_float(__ldcg(p)); }
 
@@ -210,7 +212,7 @@ __global__ void __launch_bounds__(WF_THREADS) IX_SFX(wf_start_kernel)(const __gr
 }
 
 // Active queue `parity` -> event queues.
-__global__ void __launch_bounds__(WF_THREADS) IX_SFX(wf_intersect_kernel)(const __grid_constant__ WaveLaunch L,
+__global__ void __launch_bounds__(WF_THREADS, 4) IX_SFX(wf_intersect_kernel)(const __grid_constant__ WaveLaunch L,
                                                                           int parity) {
     const Group g = make_group();
     const bool leader = g.c == 0;
@@ -341,7 +343,7 @@ int IX_SFX(wavefront_blocks_per_sm)() {
 }
 
 cudaError_t IX_SFX(launch_wavefront_start)(const WaveLaunch& l, cudaStream_t stream) {
-    if (!l.acc || !l.claim || !l.pw || !l.lw || !l.queues || !l.counts || l.capacity == 0 || l.blocks <= 0)
+    if (!l.acc || !l.claim || !l.pw || !l.queues || !l.counts || l.capacity == 0 || l.blocks <= 0)
         return cudaErrorInvalidValue;
     IX_SFX(wf_start_kernel)<<<l.blocks, WF_THREADS, 0, stream>>>(l);
     return cudaGetLastError();
