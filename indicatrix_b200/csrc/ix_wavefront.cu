@@ -51,82 +51,109 @@ struct Slot {
     bool escaped;
 };
 
-// A slot's state is one contiguous 512-byte record: its path words in the first 128 bytes
-// and, from word 32 on, its lane words channel-minor (lane word w of channel c at
-// 32 + 8 w + c), so a group reads or writes each lane word as one 32-byte sector of the
-// same record and a path's state occupies 4 whole lines of DRAM.
+// A slot's state is one contiguous 512-byte record: its 20 path words (padded to 32) and
+// then, per channel c, its 11 lane words (padded to 12) at 32 + 12 c.  A group moves the
+// path words as broadcast 16-byte loads and each lane its own lane words as three 16-byte
+// loads, so a path's state is 4 whole DRAM lines and a handful of vector instructions.
 constexpr uint32_t SLOT_WORDS = 128;
-constexpr uint32_t LW_BASE = 32;
-IX_DEV uint32_t* pw_at(const WaveLaunch& L, uint32_t w, uint32_t slot) { return L.pw + (size_t)slot * SLOT_WORDS + w; }
-IX_DEV uint32_t* lw_at(const WaveLaunch& L, uint32_t w, uint32_t slot, int c) {
-    return L.pw + (size_t)slot * SLOT_WORDS + LW_BASE + w * 8 + c;
+constexpr uint32_t LW_BASE = 32, LW_STRIDE = 12;
+
+IX_DEV const uint4* rec4(const WaveLaunch& L, uint32_t slot, uint32_t word) {
+    return reinterpret_cast<const uint4*>(L.pw + (size_t)slot * SLOT_WORDS + word);
 }
-IX_DEV float ldf(const uint32_t* p) { return __uint_as_float(__ldcg(p)); }
+IX_DEV uint4* rec4w(const WaveLaunch& L, uint32_t slot, uint32_t word) {
+    return reinterpret_cast<uint4*>(L.pw + (size_t)slot * SLOT_WORDS + word);
+}
 
 IX_DEV void wf_load(const WaveLaunch& L, uint32_t slot, const Group& g, LanePath& P, Slot& s) {
-    P.seed = __ldcg(pw_at(L, PW_SEED, slot));
-    P.bounce = __ldcg(pw_at(L, PW_BOUNCE, slot));
-    P.o = v3(ldf(pw_at(L, PW_O, slot)), ldf(pw_at(L, PW_O + 1, slot)), ldf(pw_at(L, PW_O + 2, slot)));
-    P.d = v3(ldf(pw_at(L, PW_D, slot)), ldf(pw_at(L, PW_D + 1, slot)), ldf(pw_at(L, PW_D + 2, slot)));
-    P.prev_pn = v3(ldf(pw_at(L, PW_PREV, slot)), ldf(pw_at(L, PW_PREV + 1, slot)), ldf(pw_at(L, PW_PREV + 2, slot)));
-    P.observer = v3(ldf(pw_at(L, PW_OBS, slot)), ldf(pw_at(L, PW_OBS + 1, slot)), ldf(pw_at(L, PW_OBS + 2, slot)));
-    P.n_hero = ldf(pw_at(L, PW_NHERO, slot));
-    const uint32_t flags = __ldcg(pw_at(L, PW_FLAGS, slot));
+    uint32_t w[24];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const uint4 v = __ldcg(rec4(L, slot, 4 * k));
+        w[4 * k] = v.x;
+        w[4 * k + 1] = v.y;
+        w[4 * k + 2] = v.z;
+        w[4 * k + 3] = v.w;
+    }
+    const float* f = reinterpret_cast<const float*>(w);
+    P.seed = w[PW_SEED];
+    P.bounce = w[PW_BOUNCE];
+    P.o = v3(f[PW_O], f[PW_O + 1], f[PW_O + 2]);
+    P.d = v3(f[PW_D], f[PW_D + 1], f[PW_D + 2]);
+    P.prev_pn = v3(f[PW_PREV], f[PW_PREV + 1], f[PW_PREV + 2]);
+    P.observer = v3(f[PW_OBS], f[PW_OBS + 1], f[PW_OBS + 2]);
+    P.n_hero = f[PW_NHERO];
+    const uint32_t flags = w[PW_FLAGS];
     P.inside = (flags & FLAG_INSIDE) != 0;
     P.has_prev = (flags & FLAG_HAS_PREV) != 0;
     s.escaped = (flags & FLAG_ESCAPED) != 0;
-    P.facet = (int)__ldcg(pw_at(L, PW_FACET, slot));
-    s.job = __ldcg(pw_at(L, PW_JOB, slot));
-    s.row = __ldcg(pw_at(L, PW_ROW, slot));
-    s.t = ldf(pw_at(L, PW_T, slot));
-    P.lambda = ldf(lw_at(L, LW_LAMBDA, slot, g.c));
-    P.n = ldf(lw_at(L, LW_N, slot, g.c));
-    P.alpha = ldf(lw_at(L, LW_ALPHA, slot, g.c));
-    P.st = Stokes{ldf(lw_at(L, LW_ST, slot, g.c)), ldf(lw_at(L, LW_ST + 1, slot, g.c)),
-                  ldf(lw_at(L, LW_ST + 2, slot, g.c)), ldf(lw_at(L, LW_ST + 3, slot, g.c))};
-    P.pdf = ldf(lw_at(L, LW_PDF, slot, g.c));
-    P.split = ldf(lw_at(L, LW_SPLIT, slot, g.c));
-    P.compat = __ldcg(lw_at(L, LW_COMPAT, slot, g.c));
-    s.esc = ldf(lw_at(L, LW_ESC, slot, g.c));
+    P.facet = (int)w[PW_FACET];
+    s.job = w[PW_JOB];
+    s.row = w[PW_ROW];
+    s.t = f[PW_T];
+    uint32_t l[12];
+    const uint32_t base = LW_BASE + LW_STRIDE * (uint32_t)g.c;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const uint4 v = __ldcg(rec4(L, slot, base + 4 * k));
+        l[4 * k] = v.x;
+        l[4 * k + 1] = v.y;
+        l[4 * k + 2] = v.z;
+        l[4 * k + 3] = v.w;
+    }
+    const float* lf = reinterpret_cast<const float*>(l);
+    P.lambda = lf[LW_LAMBDA];
+    P.n = lf[LW_N];
+    P.alpha = lf[LW_ALPHA];
+    P.st = Stokes{lf[LW_ST], lf[LW_ST + 1], lf[LW_ST + 2], lf[LW_ST + 3]};
+    P.pdf = lf[LW_PDF];
+    P.split = lf[LW_SPLIT];
+    P.compat = l[LW_COMPAT];
+    s.esc = lf[LW_ESC];
 }
-
-IX_DEV void stf(uint32_t* p, float v) { __stcg(p, __float_as_uint(v)); }
 
 IX_DEV void wf_store(const WaveLaunch& L, uint32_t slot, const Group& g, const LanePath& P, const Slot& s) {
     if (g.c == 0) {
-        __stcg(pw_at(L, PW_SEED, slot), P.seed);
-        __stcg(pw_at(L, PW_BOUNCE, slot), P.bounce);
-        stf(pw_at(L, PW_O, slot), P.o.x);
-        stf(pw_at(L, PW_O + 1, slot), P.o.y);
-        stf(pw_at(L, PW_O + 2, slot), P.o.z);
-        stf(pw_at(L, PW_D, slot), P.d.x);
-        stf(pw_at(L, PW_D + 1, slot), P.d.y);
-        stf(pw_at(L, PW_D + 2, slot), P.d.z);
-        stf(pw_at(L, PW_PREV, slot), P.prev_pn.x);
-        stf(pw_at(L, PW_PREV + 1, slot), P.prev_pn.y);
-        stf(pw_at(L, PW_PREV + 2, slot), P.prev_pn.z);
-        stf(pw_at(L, PW_OBS, slot), P.observer.x);
-        stf(pw_at(L, PW_OBS + 1, slot), P.observer.y);
-        stf(pw_at(L, PW_OBS + 2, slot), P.observer.z);
-        stf(pw_at(L, PW_NHERO, slot), P.n_hero);
-        __stcg(pw_at(L, PW_FLAGS, slot), (P.inside ? FLAG_INSIDE : 0u) | (P.has_prev ? FLAG_HAS_PREV : 0u) |
-                                             (s.escaped ? FLAG_ESCAPED : 0u));
-        __stcg(pw_at(L, PW_FACET, slot), (uint32_t)P.facet);
-        __stcg(pw_at(L, PW_JOB, slot), s.job);
-        __stcg(pw_at(L, PW_ROW, slot), s.row);
-        stf(pw_at(L, PW_T, slot), s.t);
+        uint32_t w[20];
+        w[PW_SEED] = P.seed;
+        w[PW_BOUNCE] = P.bounce;
+        w[PW_O] = __float_as_uint(P.o.x);
+        w[PW_O + 1] = __float_as_uint(P.o.y);
+        w[PW_O + 2] = __float_as_uint(P.o.z);
+        w[PW_D] = __float_as_uint(P.d.x);
+        w[PW_D + 1] = __float_as_uint(P.d.y);
+        w[PW_D + 2] = __float_as_uint(P.d.z);
+        w[PW_PREV] = __float_as_uint(P.prev_pn.x);
+        w[PW_PREV + 1] = __float_as_uint(P.prev_pn.y);
+        w[PW_PREV + 2] = __float_as_uint(P.prev_pn.z);
+        w[PW_OBS] = __float_as_uint(P.observer.x);
+        w[PW_OBS + 1] = __float_as_uint(P.observer.y);
+        w[PW_OBS + 2] = __float_as_uint(P.observer.z);
+        w[PW_NHERO] = __float_as_uint(P.n_hero);
+        w[PW_FLAGS] = (P.inside ? FLAG_INSIDE : 0u) | (P.has_prev ? FLAG_HAS_PREV : 0u) | (s.escaped ? FLAG_ESCAPED : 0u);
+        w[PW_FACET] = (uint32_t)P.facet;
+        w[PW_JOB] = s.job;
+        w[PW_ROW] = s.row;
+        w[PW_T] = __float_as_uint(s.t);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) __stcg(rec4w(L, slot, 4 * k), make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]));
     }
-    stf(lw_at(L, LW_LAMBDA, slot, g.c), P.lambda);
-    stf(lw_at(L, LW_N, slot, g.c), P.n);
-    stf(lw_at(L, LW_ALPHA, slot, g.c), P.alpha);
-    stf(lw_at(L, LW_ST, slot, g.c), P.st.i);
-    stf(lw_at(L, LW_ST + 1, slot, g.c), P.st.q);
-    stf(lw_at(L, LW_ST + 2, slot, g.c), P.st.u);
-    stf(lw_at(L, LW_ST + 3, slot, g.c), P.st.v);
-    stf(lw_at(L, LW_PDF, slot, g.c), P.pdf);
-    stf(lw_at(L, LW_SPLIT, slot, g.c), P.split);
-    __stcg(lw_at(L, LW_COMPAT, slot, g.c), P.compat);
-    stf(lw_at(L, LW_ESC, slot, g.c), s.esc);
+    uint32_t l[12];
+    l[LW_LAMBDA] = __float_as_uint(P.lambda);
+    l[LW_N] = __float_as_uint(P.n);
+    l[LW_ALPHA] = __float_as_uint(P.alpha);
+    l[LW_ST] = __float_as_uint(P.st.i);
+    l[LW_ST + 1] = __float_as_uint(P.st.q);
+    l[LW_ST + 2] = __float_as_uint(P.st.u);
+    l[LW_ST + 3] = __float_as_uint(P.st.v);
+    l[LW_PDF] = __float_as_uint(P.pdf);
+    l[LW_SPLIT] = __float_as_uint(P.split);
+    l[LW_COMPAT] = P.compat;
+    l[LW_ESC] = __float_as_uint(s.esc);
+    l[11] = 0u;
+    const uint32_t base = LW_BASE + LW_STRIDE * (uint32_t)g.c;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) __stcg(rec4w(L, slot, base + 4 * k), make_uint4(l[4 * k], l[4 * k + 1], l[4 * k + 2], l[4 * k + 3]));
 }
 
 // Block-wide append: group leaders with a destination queue (dest >= 0) append `slot`;
@@ -255,7 +282,7 @@ __global__ void __launch_bounds__(WF_THREADS, 4) IX_SFX(wf_intersect_kernel)(con
 
 // The event queues (reflect, refract, frosted, virtually concatenated) -> next active queue
 // or finish.
-__global__ void __launch_bounds__(WF_THREADS) IX_SFX(wf_arm_kernel)(const __grid_constant__ WaveLaunch L, int parity) {
+__global__ void __launch_bounds__(WF_THREADS, 3) IX_SFX(wf_arm_kernel)(const __grid_constant__ WaveLaunch L, int parity) {
     const Group g = make_group();
     const bool leader = g.c == 0;
     const uint32_t gi = threadIdx.x >> 3;
