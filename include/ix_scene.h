@@ -87,6 +87,17 @@ typedef struct ix_material {
     float scattering_sigma_s;           /* Henyey-Greenstein interior scattering: sigma_s  */
                                         /* per model unit (0 = clear)                     */
     float scattering_g;                 /* HG asymmetry, -1 < g < 1                        */
+    /* Biaxial indicatrix (GemMaterial::biaxial_indicatrix, materials/optics.rs:16): when
+     * `biaxial` != 0, n_beta = dispersion(lambda), n_alpha = n_beta -
+     * biaxial_delta_beta_alpha, n_gamma = n_alpha + birefringence_delta, with the gamma
+     * axis along c_axis (BiaxialIndicatrix::from_gamma_axis, birefringence/biaxial.rs:58).
+     * A biaxial material must also be `anisotropic`.  abs_o / abs_beta / abs_e are the
+     * alpha / beta / gamma ray absorption (AbsorptionTensor::biaxial, absorption.rs:338);
+     * without abs_beta the beta axis takes the alpha-ray value (the uniaxial tensor). */
+    uint32_t biaxial;
+    float biaxial_delta_beta_alpha;
+    uint32_t has_abs_beta;
+    ix_absorption abs_beta;
 } ix_material;
 
 /* Lighting model ids: the reference's LightingModel::gpu_id for the two it shares

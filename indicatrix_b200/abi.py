@@ -76,6 +76,10 @@ class Material(C.Structure):
         ("edge_rounding_radius", C.c_float),
         ("scattering_sigma_s", C.c_float),
         ("scattering_g", C.c_float),
+        ("biaxial", C.c_uint32),
+        ("biaxial_delta_beta_alpha", C.c_float),
+        ("has_abs_beta", C.c_uint32),
+        ("abs_beta", Absorption),
     ]
 
 

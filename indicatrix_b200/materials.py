@@ -136,3 +136,62 @@ def rutile(c_axis=(0.0, 1.0, 0.0)) -> abi.Material:
     return uniaxial(sellmeier3([3.039851, 1.873149, 0.0], [0.0803, 0.0, 0.0]), 0.2957, c_axis,
                     o_bands=band, e_bands=band,
                     e_dispersion=sellmeier3([3.940688, 2.256312, 0.0], [0.0843, 0.0, 0.0]))
+
+
+def biaxial(dispersion: abi.Dispersion, delta: float, delta_beta_alpha: float, c_axis=(0.0, 1.0, 0.0),
+            alpha_bands=(), beta_bands=None, gamma_bands=()) -> abi.Material:
+    """A biaxial material (GemMaterial with biaxial_delta_beta_alpha set,
+    materials/optics.rs:16): n_beta from the dispersion, n_alpha = n_beta - delta_beta_alpha,
+    n_gamma = n_alpha + delta, gamma axis along c_axis; alpha / beta / gamma ray absorption
+    (AbsorptionTensor::biaxial, optics/absorption.rs:338).  Without beta bands the beta axis
+    absorbs as the alpha ray (AbsorptionTensor::isotropic / uniaxial carry no beta_ray)."""
+    m = uniaxial(dispersion, delta, c_axis, o_bands=alpha_bands, e_bands=gamma_bands)
+    m.biaxial = 1
+    m.biaxial_delta_beta_alpha = float(delta_beta_alpha)
+    if beta_bands is not None:
+        m.has_abs_beta = 1
+        _set_bands(m.abs_beta, list(beta_bands))
+    return m
+
+
+def alexandrite(c_axis=(0.0, 1.0, 0.0)) -> abi.Material:
+    """Alexandrite (materials/zircon_through_topaz.rs:108-195): three-term Sellmeier,
+    birefringence 0.0076, n_beta - n_alpha 0.001951, trichroic Cr3+ wavelength bands."""
+    w = wavelength_band
+    return biaxial(sellmeier3([0.78522, 1.21202, 16.81], [0.0, 0.01262, 1000.0]), 0.0076, 0.001951, c_axis,
+                   alpha_bands=[w(565.0, 40.0, 1.9), w(420.0, 32.0, 1.8)],
+                   beta_bands=[w(560.0, 40.0, 0.65), w(422.0, 32.0, 3.5)],
+                   gamma_bands=[w(595.0, 40.0, 3.1), w(430.0, 32.0, 1.5)])
+
+
+def topaz(c_axis=(0.0, 1.0, 0.0)) -> abi.Material:
+    """Topaz (materials/zircon_through_topaz.rs:230-257): Cauchy, birefringence 0.008,
+    n_beta - n_alpha 0.0024, one isotropic wavelength band (no beta ray)."""
+    band = [wavelength_band(620.0, 70.0, 1.6)]
+    return biaxial(cauchy(1.614872, 0.004273), 0.0080, 0.0024, c_axis, alpha_bands=band, gamma_bands=band)
+
+
+def tanzanite(c_axis=(0.0, 1.0, 0.0)) -> abi.Material:
+    """Tanzanite (materials/tanzanite_through_cubic_zirconia.rs:13-40, :66-160): Cauchy,
+    birefringence 0.013, n_beta - n_alpha 0.0025, trichroic V3+ energy bands."""
+    e = energy_band
+    return biaxial(cauchy(1.674589, 0.009123), 0.0130, 0.0025, c_axis,
+                   alpha_bands=[e(350.0, 5083.0, 4.81), e(505.0, 5500.0, 2.11), e(577.0, 3037.0, 2.36),
+                                e(751.0, 2191.0, 0.326)],
+                   beta_bands=[e(340.0, 5683.0, 12.2), e(565.0, 5493.0, 2.1), e(610.0, 1526.0, 0.873),
+                               e(771.0, 2423.0, 2.26)],
+                   gamma_bands=[e(385.0, 2560.0, 9.86), e(440.0, 3095.0, 0.508), e(538.0, 3664.0, 1.35),
+                                e(612.0, 2209.0, 1.73), e(742.0, 2551.0, 1.33)])
+
+
+def peridot(c_axis=(0.0, 1.0, 0.0)) -> abi.Material:
+    """Peridot (materials/peridot_through_benitoite.rs:13-95): Cauchy, birefringence 0.036,
+    n_beta - n_alpha 0.015, trichroic Fe2+ energy bands."""
+    e = energy_band
+    return biaxial(cauchy(1.636549, 0.006062), 0.036, 0.0150, c_axis,
+                   alpha_bands=[e(345.0, 10096.0, 5.38), e(455.0, 1410.0, 0.53), e(490.0, 2160.0, 0.44),
+                                e(637.0, 1724.0, 0.80), e(840.0, 3276.0, 4.76), e(1000.0, 2534.0, 35.2)],
+                   beta_bands=[e(341.0, 12000.0, 6.78), e(465.0, 2526.0, 1.07), e(500.0, 3000.0, 0.47),
+                               e(635.0, 2500.0, 1.33), e(840.0, 4000.0, 4.25), e(1000.0, 2401.0, 35.2)],
+                   gamma_bands=[e(376.0, 3317.0, 4.77), e(440.0, 2933.0, 2.24), e(500.0, 3000.0, 0.79),
+                                e(627.0, 2500.0, 0.77), e(840.0, 4000.0, 2.34), e(1000.0, 3663.0, 12.7)])

@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #if defined(IX_ORACLE_AVX2) && !defined(IX_COUNT_FLOPS)
 #include <immintrin.h>
@@ -909,6 +910,172 @@ static F quadratic_form(const TensorFrame& f, F ao, F ae, V3 e) {
     F l0 = dot(f.a1, e), l1 = dot(f.a2, e), l2 = dot(f.c, e);
     return (ao * (l0 * l0) + ao * (l1 * l1)) + ae * (l2 * l2);
 }
+// AbsorptionTensor3::biaxial(alpha, beta, gamma, gamma_axis).quadratic_form
+// (absorption_tensor.rs:28, :39): the same frame, beta along a2.
+static F quadratic_form3(const TensorFrame& f, F ao, F ab, F ae, V3 e) {
+    F l0 = dot(f.a1, e), l1 = dot(f.a2, e), l2 = dot(f.c, e);
+    return (ao * (l0 * l0) + ab * (l1 * l1)) + ae * (l2 * l2);
+}
+
+// ------------------------------------------------------------------------------------
+// Biaxial indicatrix (birefringence/biaxial.rs, helpers.rs).  The principal frame is the
+// tensor frame of the gamma axis (from_gamma_axis, biaxial.rs:58): columns a1, a2, g.
+// ------------------------------------------------------------------------------------
+struct Indicatrix {
+    F na, nb, ng;     // n_alpha <= n_beta <= n_gamma
+    TensorFrame ax;   // a1 (alpha), a2 (beta), c (gamma)
+};
+// GemMaterial::biaxial_indicatrix (materials/optics.rs:16) at an already evaluated n_beta.
+static Indicatrix make_indicatrix(const ix_material& m, F n_beta, const TensorFrame& ax) {
+    Indicatrix I;
+    I.nb = n_beta;
+    I.na = n_beta - F(m.biaxial_delta_beta_alpha);
+    I.ng = I.na + F(m.birefringence_delta);
+    I.ax = ax;
+    return I;
+}
+// axes.transpose() * v and axes * v (glam Mat3, column order).
+static inline V3 to_local(const TensorFrame& f, V3 v) { return v3(dot(f.a1, v), dot(f.a2, v), dot(f.c, v)); }
+static inline V3 to_world(const TensorFrame& f, V3 l) { return (f.a1 * l.x + f.a2 * l.y) + f.c * l.z; }
+// cross_fma / dot_fma (helpers.rs:42, :52).
+static inline V3 cross_fma(V3 a, V3 b) {
+    return v3(fma_(a.y, b.z, -(a.z * b.y)), fma_(a.z, b.x, -(a.x * b.z)), fma_(a.x, b.y, -(a.y * b.x)));
+}
+static inline F dot_fma(V3 a, V3 b) { return fma_(a.x, b.x, fma_(a.y, b.y, a.z * b.z)); }
+// canonicalize_eigenvector_sign (helpers.rs:27).
+static inline V3 canonical_sign(V3 v) {
+    F ax = abs_(v.x), ay = abs_(v.y), az = abs_(v.z);
+    F largest = (ax >= ay && ax >= az) ? v.x : (ay >= az ? v.y : v.z);
+    return largest < F(0.0f) ? -v : v;
+}
+// indices_are_degenerate (biaxial.rs:176): |a - b| <= sqrt(f32::EPSILON) max(|a|, |b|, 1).
+static inline bool indices_degenerate(F a, F b) {
+    F scale = max_(max_(abs_(a), abs_(b)), 1.0f);
+    return abs_(a - b) <= F(std::sqrt(FLT_EPSILON)) * scale;
+}
+// uniaxial_wave_indices (biaxial.rs:160).
+static void uniaxial_wave_indices(V3 k, V3 c, F n_o, F n_e, F* n_slow, F* n_fast) {
+    F theta = acos_(abs_(clamp_(dot(k, c), -1.0f, 1.0f)));
+    F n_eff = effective_extraordinary_index(n_o, n_e, theta);
+    *n_slow = max_(n_o, n_eff);
+    *n_fast = min_(n_o, n_eff);
+}
+// BiaxialIndicatrix::wave_indices (biaxial.rs:105): Fresnel's equation of the wave
+// normals as a quadratic in x = 1/n^2, with the degenerate closed forms first.
+static void wave_indices(const Indicatrix& I, V3 wave_normal, F* n_slow, F* n_fast) {
+    V3 k = normalize_or_zero(wave_normal);
+    bool ab = indices_degenerate(I.na, I.nb), bg = indices_degenerate(I.nb, I.ng);
+    if (ab && bg) {
+        F n = ((I.na + I.nb) + I.ng) / F(3.0f);
+        *n_slow = n;
+        *n_fast = n;
+        return;
+    }
+    if (ab) return uniaxial_wave_indices(k, I.ax.c, midpoint_(I.na, I.nb), I.ng, n_slow, n_fast);
+    if (bg) return uniaxial_wave_indices(k, I.ax.a1, midpoint_(I.nb, I.ng), I.na, n_slow, n_fast);
+    V3 l = to_local(I.ax, k);
+    F a2 = l.x * l.x, b2 = l.y * l.y, g2 = l.z * l.z;
+    F b1 = F(1.0f) / (I.na * I.na), b2c = F(1.0f) / (I.nb * I.nb), b3 = F(1.0f) / (I.ng * I.ng);
+    F big_b = fma_(a2, b2c + b3, fma_(b2, b1 + b3, g2 * (b1 + b2c)));
+    F big_c = fma_(a2, b2c * b3, fma_(b2, b1 * b3, (g2 * b1) * b2c));
+    F disc = sqrt_(max_(fma_(big_b, big_b, F(-4.0f) * big_c), 0.0f));
+    F x_lo = F(0.5f) * (big_b - disc);
+    F x_hi = midpoint_(big_b, disc);
+    *n_slow = F(1.0f) / sqrt_(max_(x_lo, 1e-12f));
+    *n_fast = F(1.0f) / sqrt_(max_(x_hi, 1e-12f));
+}
+// precise_root_near (biaxial.rs:288): the root of the same quadratic nearest x, from the
+// cancellation-free form of the discriminant.
+static F precise_root_near(V3 l, const F b[3], F x) {
+    F a = l.x * l.x, bb = l.y * l.y, cc = l.z * l.z;
+    F big_b = fma_(a, b[1] + b[2], fma_(bb, b[0] + b[2], cc * (b[0] + b[1])));
+    F xd = b[0] - b[1], yd = b[2] - b[0];
+    F a_plus_c = a + cc, a_plus_bb = a + bb;
+    F two_a_minus_bc = F(2.0f) * fma_(bb, -cc, a);
+    F disc_sq = fma_(a_plus_c * a_plus_c, xd * xd, fma_(a_plus_bb * a_plus_bb, yd * yd, (two_a_minus_bc * xd) * yd));
+    F disc = sqrt_(max_(disc_sq, 0.0f));
+    F x_lo = F(0.5f) * (big_b - disc);
+    F x_hi = midpoint_(big_b, disc);
+    return abs_(x - x_lo) <= abs_(x - x_hi) ? x_lo : x_hi;
+}
+// eigenvector_world (biaxial.rs:243): the null direction of Gamma - x I as the
+// sign-aligned sum of its three row-pair cross products.
+static V3 eigenvector_world(const Indicatrix& I, V3 l, const F b[3], F x_in, V3 k_hat) {
+    F x = precise_root_near(l, b, x_in);
+    F s = fma_(b[0], l.x * l.x, fma_(b[1], l.y * l.y, (b[2] * l.z) * l.z));
+    F m00 = fma_(l.x * l.x, fma_(F(2.0f), -b[0], s), b[0] - x);
+    F m11 = fma_(l.y * l.y, fma_(F(2.0f), -b[1], s), b[1] - x);
+    F m22 = fma_(l.z * l.z, fma_(F(2.0f), -b[2], s), b[2] - x);
+    F m01 = (l.x * l.y) * ((s - b[0]) - b[1]);
+    F m02 = (l.x * l.z) * ((s - b[0]) - b[2]);
+    F m12 = (l.y * l.z) * ((s - b[1]) - b[2]);
+    V3 r0 = v3(m00, m01, m02), r1 = v3(m01, m11, m12), r2 = v3(m02, m12, m22);
+    V3 c01 = cross_fma(r0, r1), c02 = cross_fma(r0, r2), c12 = cross_fma(r1, r2);
+    F s02 = dot_fma(c01, c02) < F(0.0f) ? F(-1.0f) : F(1.0f);
+    F s12 = dot_fma(c01, c12) < F(0.0f) ? F(-1.0f) : F(1.0f);
+    V3 vl = (c01 + c02 * s02) + c12 * s12;
+    V3 vw = to_world(I.ax, vl);
+    if (length_squared(vw) > F(1e-12f)) return normalize(canonical_sign(vw));
+    V3 t;
+    stable_orthonormal_basis(k_hat, &t, nullptr);
+    return t;
+}
+// eigen_polarizations (biaxial.rs:197): the D direction of the slow (want_slow) or fast mode.
+static V3 eigen_polarization(const Indicatrix& I, V3 wave_normal, bool want_slow) {
+    V3 k = normalize_or_zero(wave_normal);
+    V3 l = to_local(I.ax, k);
+    F b[3] = {F(1.0f) / (I.na * I.na), F(1.0f) / (I.nb * I.nb), F(1.0f) / (I.ng * I.ng)};
+    F ns, nf;
+    wave_indices(I, wave_normal, &ns, &nf);
+    F n = want_slow ? ns : nf;
+    return eigenvector_world(I, l, b, F(1.0f) / (n * n), k);
+}
+// d_to_e_direction (biaxial.rs:322).
+static V3 d_to_e_direction(const Indicatrix& I, V3 d) {
+    V3 dl = to_local(I.ax, d);
+    V3 el = v3(dl.x / (I.na * I.na), dl.y / (I.nb * I.nb), dl.z / (I.ng * I.ng));
+    return normalize_or_zero(to_world(I.ax, el));
+}
+// poynting_direction (biaxial.rs:468).
+static V3 poynting_direction(V3 wave_normal, V3 e_field) {
+    V3 k = normalize_or_zero(wave_normal);
+    V3 e = normalize_or_zero(e_field);
+    V3 perp = k - e * dot(e, k);
+    F len2 = length_squared(perp);
+    if (len2 > F(1e-10f)) {
+        F len = sqrt_(len2);
+        return v3(perp.x / len, perp.y / len, perp.z / len);
+    }
+    return k;
+}
+// mode_poynting_dir (biaxial.rs:420) and assigned_mode_e_field (biaxial.rs:438): mode B
+// (is_extraordinary) is the slow D eigenvector, mode A the fast one.
+static V3 mode_poynting_dir(const Indicatrix& I, V3 wave_normal, bool want_slow) {
+    V3 e = d_to_e_direction(I, eigen_polarization(I, wave_normal, want_slow));
+    return poynting_direction(wave_normal, e);
+}
+static V3 assigned_mode_e_field_biaxial(const Indicatrix& I, V3 wave_normal, bool is_e) {
+    return d_to_e_direction(I, eigen_polarization(I, wave_normal, is_e));
+}
+// resolve_entry_mode (biaxial.rs:370): two fixed-point steps of Snell's law against the
+// mode's own direction-dependent index, seeded with n_seed.
+static F resolve_entry_mode(const Indicatrix& I, V3 incident, V3 normal, F cos_i, F n_seed, bool want_slow,
+                            V3* wave_dir_out) {
+    F n_guess = n_seed;
+    V3 wave_dir = incident;
+    for (int it = 0; it < 2; ++it) {
+        F eta = F(1.0f) / n_guess;
+        F s2 = eta * eta * fma_(cos_i, -cos_i, 1.0f);
+        if (s2 > F(1.0f)) break;
+        F ct = sqrt_(max_(F(1.0f) - s2, 0.0f));
+        wave_dir = normalize(eta * incident + fma_(eta, cos_i, -ct) * normal);
+        F ns, nf;
+        wave_indices(I, wave_dir, &ns, &nf);
+        n_guess = want_slow ? ns : nf;
+    }
+    *wave_dir_out = wave_dir;
+    return n_guess;
+}
 
 // ------------------------------------------------------------------------------------
 // Closed-form uniaxial interface solves (raytracer/uniaxial_fresnel/*.rs, after Lekner,
@@ -1254,8 +1421,11 @@ struct Path {
     F n_e_at[8];   // extraordinary_index_at per channel (uniaxial only)
     F alpha_ch_o[8];
     F alpha_ch_e[8];
+    F alpha_ch_b[8];  // beta-ray absorption (biaxial only; the alpha-ray value without abs_beta)
     bool absorbing;
     bool aniso;
+    bool biaxial;     // biaxial indicatrix (cache.hero_indicatrix.is_some())
+    TensorFrame ax;   // principal / absorption frame of the optic (gamma) axis
     bool is_e;  // the eigenmode assigned at the last entry (or by internal coupling)
     V3 c_axis;  // the material's optic axis as stored (RayMaterialContext::c_axis)
     Stokes stokes[8];
@@ -1317,7 +1487,15 @@ struct Geo {
     F n1_ch[8], n2_ch[8], sin2_t_ch[8];
     bool has_frame;
     UFrame frame;
+    // Biaxial material: mode A (fast root at the mode-A wave normal) and mode B (slow root
+    // at the mode-B wave normal) indices per channel (geometry.rs:255).
+    bool is_biaxial;
+    F n_biax_a_ch[8], n_biax_b_ch[8];
 };
+// The hero channel's (channel 0's) and channel c's indicatrix.
+static Indicatrix channel_indicatrix(const Path& P, int c) {
+    return make_indicatrix(P.sc->material, P.n_ch[c], P.ax);
+}
 
 // theta_c_for_bounce (refraction/geometry.rs:75), uniaxial only.
 static F theta_c_for_bounce(const Path& P, V3 normal, V3 k, F cos_i) {
@@ -1354,10 +1532,35 @@ static Geo compute_geo(const Path& P, V3 normal) {
     }
     g.n_o_hero = P.n_ch[0];
     g.n_e_hero = g.n_o_hero + F(P.sc->material.birefringence_delta);
-    // n_medium_ch: the ordinary indices while inside in the ordinary mode, else n_eff.
+    g.is_biaxial = P.biaxial;
+    if (P.biaxial) {
+        // hero_biaxial_wave_dirs + per_channel_biaxial_indices (geometry.rs:220-285): the
+        // hero's indicatrix resolves each mode's wave normal on entry (the tracked wave
+        // normal inside); every channel evaluates its own indicatrix there.
+        const Indicatrix hero = channel_indicatrix(P, 0);
+        V3 dir_a = k, dir_b = k;
+        if (!P.inside) {
+            resolve_entry_mode(hero, k, normal, g.cos_i, P.n_ch[0], false, &dir_a);
+            resolve_entry_mode(hero, k, normal, g.cos_i, P.n_ch[0], true, &dir_b);
+        }
+        for (int c = 0; c < 8; ++c) {
+            const Indicatrix ic = channel_indicatrix(P, c);
+            F ns, nf;
+            wave_indices(ic, dir_a, &ns, &nf);
+            g.n_biax_a_ch[c] = nf;
+            wave_indices(ic, dir_b, &ns, &nf);
+            g.n_biax_b_ch[c] = ns;
+        }
+    }
+    // n_medium_ch: mode A (the ordinary indices for a uniaxial material) while inside in
+    // that mode, else mode B (n_eff).
     const bool ordinary_medium = P.aniso && P.inside && !P.is_e;
     F n_med[8];
-    for (int c = 0; c < 8; ++c) n_med[c] = ordinary_medium ? P.n_ch[c] : n_eff[c];
+    for (int c = 0; c < 8; ++c) {
+        const F mode_a = P.biaxial ? g.n_biax_a_ch[c] : P.n_ch[c];
+        const F mode_b = P.biaxial ? g.n_biax_b_ch[c] : n_eff[c];
+        n_med[c] = ordinary_medium ? mode_a : mode_b;
+    }
     g.n1 = P.inside ? n_med[0] : F(1.0f);
     g.n2 = P.inside ? F(1.0f) : n_med[0];
     F eta = g.n1 / g.n2;
@@ -1368,14 +1571,16 @@ static Geo compute_geo(const Path& P, V3 normal) {
         F etak = g.n1_ch[c] / g.n2_ch[c];
         g.sin2_t_ch[c] = etak * etak * fma_(g.cos_i, -g.cos_i, 1.0f);
     }
-    g.has_frame = P.aniso;
-    if (P.aniso) g.frame = uframe_build(k, normal, P.c_axis, g.cos_i, g.sin_i);
+    g.has_frame = P.aniso && !P.biaxial;
+    if (g.has_frame) g.frame = uframe_build(k, normal, P.c_axis, g.cos_i, g.sin_i);
     return g;
 }
 
-// poynting_dir_for_mode (refraction/geometry.rs:440).
+// poynting_dir_for_mode (refraction/geometry.rs:440): both biaxial modes walk off.
 static V3 poynting_dir_for_mode(const Path& P, const Geo& g, V3 k, bool inside, bool is_e) {
-    if (!inside || !P.aniso || !is_e) return k;
+    if (!inside || !P.aniso) return k;
+    if (g.is_biaxial) return mode_poynting_dir(channel_indicatrix(P, 0), k, is_e);
+    if (!is_e) return k;
     return extraordinary_poynting_dir(k, P.c_axis, g.n_o_hero, g.n_e_hero);
 }
 
@@ -1449,18 +1654,27 @@ static void apply_partial_reflect(Path& P, const Geo& g, F r_unpol) {
 static void apply_refract_bounce(Path& P, const Geo& g, F r_unpol, V3 k, V3 normal, V3 hit_point,
                                  bool use_e, bool has_az, F az_c, F az_s, Outcome* o) {
     const bool entering = !P.inside && P.aniso;
+    const bool biaxial_entry = entering && g.is_biaxial;
     const F cos_i = g.cos_i;
-    F n2_hero_dir = (entering && !use_e) ? g.n_o_hero : g.n2;
-    V3 refr = snell_dir(g.n1 / n2_hero_dir, cos_i, k, normal);
-    V3 final_refr = (entering && use_e) ? extraordinary_poynting_dir(refr, P.c_axis, g.n_o_hero, g.n_e_hero)
-                                        : refr;
+    V3 refr, final_refr;
+    if (biaxial_entry) {
+        // The selected mode's own index and walk-off (reflect_refract.rs:160-180).
+        F n2_hero_dir = use_e ? g.n_biax_b_ch[0] : g.n_biax_a_ch[0];
+        refr = snell_dir(g.n1 / n2_hero_dir, cos_i, k, normal);
+        final_refr = mode_poynting_dir(channel_indicatrix(P, 0), refr, use_e);
+    } else {
+        F n2_hero_dir = (entering && !use_e) ? g.n_o_hero : g.n2;
+        refr = snell_dir(g.n1 / n2_hero_dir, cos_i, k, normal);
+        final_refr = (entering && use_e) ? extraordinary_poynting_dir(refr, P.c_axis, g.n_o_hero, g.n_e_hero)
+                                         : refr;
+    }
     V3 dirs[8];
     bool have_dir[8];
     bool hero_match[8];
     for (int c = 0; c < 8; ++c) {
         Stokes original = P.stokes[c];
         F n1k = g.n1_ch[c];
-        F n2k = (entering && !use_e) ? P.n_ch[c] : g.n2_ch[c];
+        F n2k = (entering && !use_e) ? (g.is_biaxial ? g.n_biax_a_ch[c] : P.n_ch[c]) : g.n2_ch[c];
         F ratio = n1k / n2k;
         F sin2_t_k = (ratio * ratio) * fma_(cos_i, -cos_i, 1.0f);
         if (sin2_t_k > F(1.0f)) {
@@ -1473,7 +1687,8 @@ static void apply_refract_bounce(Path& P, const Geo& g, F r_unpol, V3 k, V3 norm
         F cos_t_k = sqrt_(max_(F(1.0f) - sin2_t_k, 0.0f));
         F eta_k = n1k / n2k;
         V3 refr_k = normalize(eta_k * k + fma_(eta_k, cos_i, -cos_t_k) * normal);
-        V3 final_k = (entering && use_e)
+        V3 final_k = biaxial_entry ? mode_poynting_dir(channel_indicatrix(P, c), refr_k, use_e)
+                     : (entering && use_e)
                          ? extraordinary_poynting_dir(refr_k, P.c_axis, P.n_ch[c],
                                                       P.n_ch[c] + F(P.sc->material.birefringence_delta))
                          : refr_k;
@@ -1520,14 +1735,16 @@ static void apply_scalar_fresnel(Path& P, const Geo& g, V3 k, V3 normal, V3 cpn,
     const bool entering = !P.inside && P.aniso;
     // resolve_entry_mode_selection (dispatch.rs:162).
     F p_o = 0.5f, cos2 = 0.0f, sin2 = 0.0f;
-    bool has_sel = entering && entry_eigenmode_selection(P.c_axis, cpn, k, P.stokes[0], &p_o, &cos2, &sin2);
+    // A biaxial material has no ordinary eigenmode to weigh: 50 / 50 (dispatch.rs:176).
+    bool has_sel = entering && !g.is_biaxial &&
+                   entry_eigenmode_selection(P.c_axis, cpn, k, P.stokes[0], &p_o, &cos2, &sin2);
     if (!has_sel) p_o = 0.5f;
     F msr = unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM);
     bool use_e = entering ? (msr < F(1.0f) - p_o) : P.is_e;
     F az_c = use_e ? -cos2 : cos2;
     F az_s = use_e ? -sin2 : sin2;
     // compute_entry_reflect_probability (dispatch.rs:230).
-    bool ord_sel = entering && !use_e;
+    bool ord_sel = entering && !g.is_biaxial && !use_e;
     F n2 = ord_sel ? g.n_o_hero : g.n2;
     F sin2_t = g.sin2_t;
     if (ord_sel) {
@@ -1779,6 +1996,14 @@ static void apply_frosted_bounce(Path& P, const Geo& g, V3 normal, uint32_t boun
 // along the current wave normal, for the assigned mode of a uniaxial material.
 static void channel_alphas(const Path& P, F alpha[8]) {
     TensorFrame tf = tensor_frame(P.c_axis);
+    if (P.biaxial) {
+        // The hero indicatrix's assigned-mode field against each channel's biaxial
+        // tensor (absorption.rs:227-242, wavelength_cache.rs:44-52).
+        V3 e_mode = assigned_mode_e_field_biaxial(channel_indicatrix(P, 0), P.k, P.is_e);
+        for (int c = 0; c < 8; ++c)
+            alpha[c] = quadratic_form3(tf, P.alpha_ch_o[c], P.alpha_ch_b[c], P.alpha_ch_e[c], e_mode);
+        return;
+    }
     if (!P.aniso) {
         V3 ea = ordinary_eigen_polarization(P.k, P.c_axis);
         V3 eb = normalize_or_zero(cross(P.k, ea));
@@ -1957,13 +2182,18 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
     const ix_material& m = sc->material;
     P.absorbing = absorption_present(m.abs_o) || absorption_present(m.abs_e);
     P.aniso = m.anisotropic != 0;
+    P.biaxial = m.biaxial != 0;
+    if (P.biaxial && m.has_abs_beta) P.absorbing = P.absorbing || absorption_present(m.abs_beta);
     P.is_e = false;
     P.c_axis = load3(m.c_axis);
+    P.ax = tensor_frame(P.c_axis);
     for (int c = 0; c < 8; ++c) {
         P.n_ch[c] = dispersion_eval(m.dispersion, P.lambdas[c]);
         P.n_e_at[c] = P.aniso ? extraordinary_index_at(m, P.lambdas[c], P.n_ch[c]) : P.n_ch[c];
         P.alpha_ch_o[c] = P.absorbing ? spectral_absorption(m.abs_o, P.lambdas[c]) : F(0.0f);
         P.alpha_ch_e[c] = P.absorbing ? spectral_absorption(m.abs_e, P.lambdas[c]) : F(0.0f);
+        P.alpha_ch_b[c] = (P.absorbing && P.biaxial && m.has_abs_beta) ? spectral_absorption(m.abs_beta, P.lambdas[c])
+                                                                       : P.alpha_ch_o[c];
         P.stokes[c] = unpolarized(1.0f);
         P.radiance[c] = 0.0f;
         P.path_pdf[c] = 1.0f;
@@ -2063,7 +2293,7 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
             F p_o = 0.5f;
             if (o.has_p_o) {
                 p_o = o.p_o;
-            } else {
+            } else if (!P.biaxial) {
                 F po, c2, s2;
                 if (entry_eigenmode_selection(P.c_axis, cpn, P.k, P.stokes[0], &po, &c2, &s2)) p_o = po;
             }
@@ -2860,6 +3090,35 @@ void ixo_fresnel_channel(float n1, float n2, float cos_i, const float s_in[4], f
     out[8] = raw(r_s), out[9] = raw(r_p), out[10] = raw(t_s), out[11] = raw(t_p);
 }
 
+// The biaxial indicatrix of `m` at lambda (its own channel) evaluated at wave normal k:
+// out[0..1] wave_indices (slow, fast); out[2..7] eigen_polarizations (slow xyz, fast xyz);
+// out[8..13] mode_poynting_dir (slow, fast); out[14..21] resolve_entry_mode against
+// `normal` at cos_i seeded with n_beta (slow n, dir xyz, fast n, dir xyz); out[22..23]
+// the assigned-mode alpha of the biaxial tensor (mode B, mode A).
+void ixo_biaxial_bundle(const ix_material* m, const float k[3], const float normal[3], float cos_i,
+                        float lambda_nm, float out[24]) {
+    const V3 kk = load3(k), nn = load3(normal);
+    const F n_beta = dispersion_eval(m->dispersion, lambda_nm);
+    const TensorFrame ax = tensor_frame(load3(m->c_axis));
+    const Indicatrix I = make_indicatrix(*m, n_beta, ax);
+    F ns, nf;
+    wave_indices(I, kk, &ns, &nf);
+    out[0] = raw(ns);
+    out[1] = raw(nf);
+    store3(out + 2, eigen_polarization(I, kk, true));
+    store3(out + 5, eigen_polarization(I, kk, false));
+    store3(out + 8, mode_poynting_dir(I, kk, true));
+    store3(out + 11, mode_poynting_dir(I, kk, false));
+    V3 d;
+    out[14] = raw(resolve_entry_mode(I, kk, nn, cos_i, n_beta, true, &d));
+    store3(out + 15, d);
+    out[18] = raw(resolve_entry_mode(I, kk, nn, cos_i, n_beta, false, &d));
+    store3(out + 19, d);
+    const F ao = spectral_absorption(m->abs_o, lambda_nm), ae = spectral_absorption(m->abs_e, lambda_nm);
+    const F ab = m->has_abs_beta ? spectral_absorption(m->abs_beta, lambda_nm) : ao;
+    out[22] = raw(quadratic_form3(ax, ao, ab, ae, assigned_mode_e_field_biaxial(I, kk, true)));
+    out[23] = raw(quadratic_form3(ax, ao, ab, ae, assigned_mode_e_field_biaxial(I, kk, false)));
+}
 float ixo_channel_alpha(const ix_material* m, const float k[3], float lambda_nm) {
     // The non-birefringent branch of channel_absorption_alphas_assigned
     // (raytracer/absorption.rs:197): the midpoint of the tensor's quadratic form over the
