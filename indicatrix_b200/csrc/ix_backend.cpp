@@ -98,7 +98,7 @@ int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uin
     const int shape = ix::variant_shape(L.variant);
     const bool pool = ix::shape_is_pool(shape);
     L.threads = ix::shape_threads(shape);
-    const int uni = ix::needs_uniaxial_kernel(L.flags) ? 1 : 0;
+    const int uni = ix::transport_class(L.flags);
     L.blocks = b->sm_count * (exact ? b->bps_exact[uni][L.variant] : b->bps_fast[uni][L.variant]);
     if (attr) L.blocks = b->sm_count * (exact ? b->bps_attr_exact[uni] : b->bps_attr_fast[uni]);
     if (L.blocks <= 0) {
@@ -436,13 +436,14 @@ ix_backend* ix_backend_create(const ix_backend_options* opts) {
     b->sm_count = prop.multiProcessorCount;
     b->label = prop.name;
     static_assert(ix_backend::kVariants == ix::N_VARIANTS, "variant table size");
-    for (int u = 0; u < 2; ++u)
+    static_assert(ix_backend::kClasses == ix::N_TRANSPORT_CLASSES, "transport table size");
+    for (int u = 0; u < ix::N_TRANSPORT_CLASSES; ++u)
         for (int v = 0; v < ix::N_VARIANTS; ++v) {
             const int threads = ix::shape_threads(ix::variant_shape(v));
             b->bps_exact[u][v] = ix::trace_blocks_per_sm_exact(threads, v, u, nullptr);
             b->bps_fast[u][v] = ix::trace_blocks_per_sm_fast(threads, v, u, nullptr);
         }
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < ix::N_TRANSPORT_CLASSES; ++u) {
         b->bps_attr_exact[u] = std::max(1, ix::trace_attributed_blocks_per_sm_exact((int)b->threads, u));
         b->bps_attr_fast[u] = std::max(1, ix::trace_attributed_blocks_per_sm_fast((int)b->threads, u));
     }
@@ -519,6 +520,10 @@ int ix_scene_routes_to_gpu(const ix_scene* s) {
     const ix_environment& e = s->environment;
     if (e.model != IX_ENV_STUDIO && e.model != IX_ENV_ISO_HEMISPHERE && e.model != IX_ENV_UNIFORM) return 0;
     if (m.dispersion.kind > IX_DISP_CAUCHY) return 0;
+    // A biaxial indicatrix is traced as the anisotropic transport's biaxial arm; an
+    // isotropic material carrying one (the reference's eigen-polarisation mean of the
+    // isotropic absorption branch over a biaxial indicatrix) is not built.
+    if (m.biaxial && !m.anisotropic) return 0;
     return 1;
 }
 
@@ -635,7 +640,7 @@ struct ix_batch_plan {
     unsigned long long* d_acc = nullptr;  // fixed-point sums, FIXED_WORDS per pixel of every job
     ix_scene* d_scenes = nullptr;
     uint32_t* d_flags = nullptr;
-    uint32_t uniaxial = 0;  // some scene needs the uniaxial transport instantiation
+    uint32_t uniaxial = 0;  // transport instantiation (ix::TransportClass): the largest of the scenes'
     ix::BatchJob* d_jobs = nullptr;
     float* d_planes = nullptr;
     double* d_out = nullptr;
@@ -939,7 +944,7 @@ static ix_batch_plan* plan_create_locked(ix_backend* b, const ix_scene* scenes, 
         dev_scenes[i].n_finishes = has_finishes ? scenes[i].n_finishes : 0;
         flags[i] = ix::scene_flags(scenes[i].material);
         p->h_max_bounces.push_back(scenes[i].max_bounces);
-        if (ix::needs_uniaxial_kernel(flags[i])) p->uniaxial = 1;
+        p->uniaxial = std::max(p->uniaxial, (uint32_t)ix::transport_class(flags[i]));
         off += (uint64_t)scenes[i].n_planes * 4;
     }
     ok = ok && cudaMalloc((void**)&p->d_scenes, n_scenes * sizeof(ix_scene)) == cudaSuccess &&
@@ -1510,9 +1515,9 @@ int ix_debug_check(ix_backend* b, const ix_scene* scene, int32_t fn, uint32_t n,
     if (scene->n_planes > IX_MAX_PLANES) return -1;
     // 32-bit words each check function reads from / writes to a row (ix::CheckFn order):
     // rows narrower than that are refused before anything reaches the device.
-    static const uint8_t kIn[] = {2, 1, 1, 1, 1, 1, 3, 7, 7, 6, 2, 2, 1, 8, 14, 7, 4};
-    static const uint8_t kOut[] = {4, 8, 1, 3, 1, 1, 1, 6, 1, 2, 4, 6, 1, 4, 7, 13, 1};
-    static_assert(sizeof(kIn) == ix::CHECK_CHANNEL_ALPHA + 1 && sizeof(kOut) == sizeof(kIn), "check table");
+    static const uint8_t kIn[] = {2, 1, 1, 1, 1, 1, 3, 7, 7, 6, 2, 2, 1, 8, 14, 7, 4, 9};
+    static const uint8_t kOut[] = {4, 8, 1, 3, 1, 1, 1, 6, 1, 2, 4, 6, 1, 4, 7, 13, 1, 24};
+    static_assert(sizeof(kIn) == ix::CHECK_BIAXIAL + 1 && sizeof(kOut) == sizeof(kIn), "check table");
     if (fn < 0 || fn >= (int32_t)sizeof(kIn) || in_stride < kIn[fn] || out_stride < kOut[fn]) return -1;
     Turn turn(b);
     if (fail(b, cudaSetDevice(b->device), "set device")) return -1;

@@ -65,11 +65,12 @@ struct ix_backend {
     uint32_t batch_variant = 0;
     // CTA size new batch plans are restricted to (0: any; 64, 128 or 256).
     uint32_t batch_threads = 0;
-    // Resident CTAs per SM by [uniaxial instantiation][variant] (0: not in this build).
-    static constexpr int kVariants = 12;
-    int bps_exact[2][kVariants] = {}, bps_fast[2][kVariants] = {};
-    // ... and of the attributed trace kernels by [uniaxial instantiation].
-    int bps_attr_exact[2] = {1, 1}, bps_attr_fast[2] = {1, 1};
+    // Resident CTAs per SM by [transport instantiation (ix::TransportClass)][variant]
+    // (0: not in this build).
+    static constexpr int kVariants = 12, kClasses = 3;
+    int bps_exact[kClasses][kVariants] = {}, bps_fast[kClasses][kVariants] = {};
+    // ... and of the attributed trace kernels by [transport instantiation].
+    int bps_attr_exact[kClasses] = {1, 1, 1}, bps_attr_fast[kClasses] = {1, 1, 1};
     std::string label;
     // State.
     bool lost = false;

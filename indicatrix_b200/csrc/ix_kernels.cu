@@ -96,10 +96,10 @@ IX_DEV uint32_t classify_path(uint32_t ev, V3 exit_dir, V3 observer, const ExitS
 
 // One warp task: pixels [pixel0, pixel0 + npix) x samples [sample_offset, +spp), written
 // to out[0 .. 3 npix).  Returns the number of non-finite samples this lane dropped.
-// UNI selects the transport instantiation (isotropic megakernel, or the uniaxial one);
+// UNI selects the transport instantiation (TransportClass);
 // ATTR adds the event record of each path and writes its class and luminance to `at`
 // (the traced arithmetic is the same: the record only reads the path state).
-template <bool UNI, bool ATTR = false>
+template <int UNI, bool ATTR = false>
 IX_DEV uint32_t trace_task(const Group& g, const DevScene& S, const float4* __restrict__ planes,
                            uint32_t pixel0, uint32_t npix, uint32_t spp, uint32_t sample_offset,
                            WarpScratch& ws, double* out, int accumulate, const AttrTask* at = nullptr) {
@@ -229,7 +229,7 @@ IX_DEV uint32_t trace_task(const Group& g, const DevScene& S, const float4* __re
 
 // Single scene: MINB is the resident CTAs per SM the register allocation must allow
 // (1 = unconstrained).
-template <int MINB, bool UNI>
+template <int MINB, int UNI>
 __global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_constant__ TraceLaunch L) {
     __shared__ float4 s_planes[IX_MAX_PLANES];
     __shared__ WarpScratch s_scratch[WARPS_PER_CTA];
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(trace_kernel)(const __grid_c
 // The trace kernel with spectral attribution: the same task loop, and each path's
 // class code and luminance recorded for the fold.  Each CTA first derives the exit
 // lighting's threshold (96 radiances and their median), which decides the classes.
-template <int MINB, bool UNI>
+template <int MINB, int UNI>
 __global__ void __launch_bounds__(128, MINB)
     IX_SFX(trace_attributed_kernel)(const __grid_constant__ TraceLaunch L, const __grid_constant__ AttrLaunch A) {
     __shared__ float4 s_planes[IX_MAX_PLANES];
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(128) IX_SFX(attribution_fold_kernel)(const __g
 // Many scenes in one persistent launch (BatchLaunch): the task space is the
 // concatenation of every job's tasks; a warp finds its job by binary search over the
 // jobs' first-task offsets and reloads its plane slot only when the job's scene changes.
-template <int MINB, bool UNI>
+template <int MINB, int UNI>
 __global__ void __launch_bounds__(128, MINB) IX_SFX(batch_kernel)(const __grid_constant__ BatchLaunch L) {
     __shared__ float4 s_planes[WARPS_PER_CTA][IX_MAX_PLANES];
     __shared__ WarpScratch s_scratch[WARPS_PER_CTA];
@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(128, MINB) IX_SFX(batch_kernel)(const __grid_c
 
 // Per-path checks: each 8-lane group traces one input row, exactly as the megakernel
 // traces a path.
-template <bool UNI>
+template <int UNI>
 __global__ void __launch_bounds__(128) IX_SFX(check_trace_kernel)(const __grid_constant__ CheckLaunch L) {
     __shared__ float4 s_planes[IX_MAX_PLANES];
     const float4* gplanes = reinterpret_cast<const float4*>(L.scene.planes);
@@ -537,8 +537,64 @@ __global__ void IX_SFX(check_kernel)(const __grid_constant__ CheckLaunch L) {
             put(0, iso_channel_alpha(m, spectral_absorption(m.abs_o, inf(3)), v3(inf(0), inf(1), inf(2))));
             break;
         }
+        case CHECK_BIAXIAL: {
+            const ix_material& m = S.s.material;
+            const V3 k = v3(inf(0), inf(1), inf(2)), nn = v3(inf(3), inf(4), inf(5));
+            const float cos_i = inf(6), lambda = inf(7), n_beta = inf(8);
+            const BiaxFrame F = biax_frame(load3(m.c_axis));
+            const Indicatrix I = make_indicatrix(m, n_beta);
+            float ns, nf;
+            wave_indices(I, F, k, ns, nf);
+            put(0, ns);
+            put(1, nf);
+            auto put3 = [&](int i, V3 v) { put(i, v.x); put(i + 1, v.y); put(i + 2, v.z); };
+            put3(2, eigen_polarization(I, F, k, true));
+            put3(5, eigen_polarization(I, F, k, false));
+            put3(8, mode_poynting_dir(I, F, k, true));
+            put3(11, mode_poynting_dir(I, F, k, false));
+            V3 d;
+            put(14, resolve_entry_mode(I, F, k, nn, cos_i, n_beta, true, d));
+            put3(15, d);
+            put(18, resolve_entry_mode(I, F, k, nn, cos_i, n_beta, false, d));
+            put3(19, d);
+            const float ao = spectral_absorption(m.abs_o, lambda), ae = spectral_absorption(m.abs_e, lambda);
+            const float ab = m.has_abs_beta ? spectral_absorption(m.abs_beta, lambda) : ao;
+            put(22, biaxial_quadratic_form(F, ao, ab, ae, assigned_mode_e_field_biaxial(I, F, k, true)));
+            put(23, biaxial_quadratic_form(F, ao, ab, ae, assigned_mode_e_field_biaxial(I, F, k, false)));
+            break;
+        }
         default: break;
     }
+}
+
+// The static task loop's kernels by (transport class, register budget): budgets 1 and 2
+// are the occupancy targets of each transport (6 / 8 CTAs per SM isotropic, UNI_MINB_1 /
+// UNI_MINB_2 for the uniaxial instantiations), 0 unconstrained.
+template <int UNI>
+struct TaskLoop {
+    static constexpr int minb(int budget) {
+        return budget == 1 ? (UNI ? UNI_MINB_1 : 6) : budget == 2 ? (UNI ? UNI_MINB_2 : 8) : 1;
+    }
+    using TraceFn = void (*)(const TraceLaunch);
+    using BatchFn = void (*)(const BatchLaunch);
+    static TraceFn trace(int budget) {
+        switch (budget) {
+            case 1: return IX_SFX(trace_kernel)<minb(1), UNI>;
+            case 2: return IX_SFX(trace_kernel)<minb(2), UNI>;
+            default: return IX_SFX(trace_kernel)<1, UNI>;
+        }
+    }
+    static BatchFn batch(int budget) {
+        switch (budget) {
+            case 1: return IX_SFX(batch_kernel)<minb(1), UNI>;
+            case 2: return IX_SFX(batch_kernel)<minb(2), UNI>;
+            default: return IX_SFX(batch_kernel)<1, UNI>;
+        }
+    }
+};
+template <typename L>
+static void start_task_loop(void (*kernel)(const L), const L& l, cudaStream_t stream) {
+    kernel<<<l.blocks, l.threads, 0, stream>>>(l);
 }
 
 static bool launch_shape_ok(int threads) { return threads == 128; }
@@ -551,18 +607,10 @@ cudaError_t IX_SFX(launch_trace)(const TraceLaunch& l, cudaStream_t stream) {
     if (l.scene.n_planes > IX_MAX_PLANES) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
-    if (needs_uniaxial_kernel(l.flags)) {
-        switch (variant_budget(l.variant)) {
-            case 1: IX_SFX(trace_kernel)<UNI_MINB_1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
-            case 2: IX_SFX(trace_kernel)<UNI_MINB_2, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
-            default: IX_SFX(trace_kernel)<1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
-        }
-    } else {
-        switch (variant_budget(l.variant)) {
-            case 1: IX_SFX(trace_kernel)<6, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
-            case 2: IX_SFX(trace_kernel)<8, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
-            default: IX_SFX(trace_kernel)<1, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
-        }
+    switch (transport_class(l.flags)) {
+        case TRANSPORT_BIAXIAL: start_task_loop(TaskLoop<TRANSPORT_BIAXIAL>::trace(variant_budget(l.variant)), l, stream); break;
+        case TRANSPORT_UNIAXIAL: start_task_loop(TaskLoop<TRANSPORT_UNIAXIAL>::trace(variant_budget(l.variant)), l, stream); break;
+        default: start_task_loop(TaskLoop<TRANSPORT_ISOTROPIC>::trace(variant_budget(l.variant)), l, stream); break;
     }
     return cudaGetLastError();
 }
@@ -578,10 +626,17 @@ cudaError_t IX_SFX(launch_trace_attributed)(const TraceLaunch& l, const AttrLaun
     if (l.scene.n_planes > IX_MAX_PLANES || !a.cls || !a.y) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
-    if (needs_uniaxial_kernel(l.flags))
-        IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, true><<<l.blocks, l.threads, 0, stream>>>(l, a);
-    else
-        IX_SFX(trace_attributed_kernel)<ATTR_MINB_ISO, false><<<l.blocks, l.threads, 0, stream>>>(l, a);
+    switch (transport_class(l.flags)) {
+        case TRANSPORT_BIAXIAL:
+            IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, TRANSPORT_BIAXIAL><<<l.blocks, l.threads, 0, stream>>>(l, a);
+            break;
+        case TRANSPORT_UNIAXIAL:
+            IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, TRANSPORT_UNIAXIAL><<<l.blocks, l.threads, 0, stream>>>(l, a);
+            break;
+        default:
+            IX_SFX(trace_attributed_kernel)<ATTR_MINB_ISO, TRANSPORT_ISOTROPIC><<<l.blocks, l.threads, 0, stream>>>(l, a);
+            break;
+    }
     return cudaGetLastError();
 }
 
@@ -600,18 +655,10 @@ cudaError_t IX_SFX(launch_batch)(const BatchLaunch& l, cudaStream_t stream) {
     if (!launch_shape_ok(l.threads) || l.n_jobs == 0 || l.stride == 0) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
-    if (l.uniaxial) {
-        switch (variant_budget(l.variant)) {
-            case 1: IX_SFX(batch_kernel)<UNI_MINB_1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
-            case 2: IX_SFX(batch_kernel)<UNI_MINB_2, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
-            default: IX_SFX(batch_kernel)<1, true><<<l.blocks, l.threads, 0, stream>>>(l); break;
-        }
-    } else {
-        switch (variant_budget(l.variant)) {
-            case 1: IX_SFX(batch_kernel)<6, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
-            case 2: IX_SFX(batch_kernel)<8, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
-            default: IX_SFX(batch_kernel)<1, false><<<l.blocks, l.threads, 0, stream>>>(l); break;
-        }
+    switch (l.uniaxial) {
+        case TRANSPORT_BIAXIAL: start_task_loop(TaskLoop<TRANSPORT_BIAXIAL>::batch(variant_budget(l.variant)), l, stream); break;
+        case TRANSPORT_UNIAXIAL: start_task_loop(TaskLoop<TRANSPORT_UNIAXIAL>::batch(variant_budget(l.variant)), l, stream); break;
+        default: start_task_loop(TaskLoop<TRANSPORT_ISOTROPIC>::batch(variant_budget(l.variant)), l, stream); break;
     }
     return cudaGetLastError();
 }
@@ -622,10 +669,11 @@ cudaError_t IX_SFX(launch_check)(const CheckLaunch& l, cudaStream_t stream) {
     const int threads = 128;
     if (l.fn == CHECK_TRACE || l.fn == CHECK_TRACE_RAY) {
         const int blocks = (int)((l.n * 8ull + threads - 1) / threads);
-        if (needs_uniaxial_kernel(l.flags))
-            IX_SFX(check_trace_kernel)<true><<<blocks, threads, 0, stream>>>(l);
-        else
-            IX_SFX(check_trace_kernel)<false><<<blocks, threads, 0, stream>>>(l);
+        switch (transport_class(l.flags)) {
+            case TRANSPORT_BIAXIAL: IX_SFX(check_trace_kernel)<TRANSPORT_BIAXIAL><<<blocks, threads, 0, stream>>>(l); break;
+            case TRANSPORT_UNIAXIAL: IX_SFX(check_trace_kernel)<TRANSPORT_UNIAXIAL><<<blocks, threads, 0, stream>>>(l); break;
+            default: IX_SFX(check_trace_kernel)<TRANSPORT_ISOTROPIC><<<blocks, threads, 0, stream>>>(l); break;
+        }
     } else {
         const int blocks = (int)((l.n + threads - 1) / threads);
         IX_SFX(check_kernel)<<<blocks, threads, 0, stream>>>(l);
@@ -645,35 +693,33 @@ int IX_SFX(trace_blocks_per_sm)(int threads, int variant, int uniaxial, size_t* 
     if (variant < 0 || variant >= N_VARIANTS) return 0;
     if (shape_is_pool(variant_shape(variant))) return IX_SFX(pool_trace_blocks_per_sm)(variant, uniaxial);
     if (threads != 128) return 0;
-    variant = variant_budget(variant);
-    if (uniaxial) {
-        if (variant == 1) return occupancy(IX_SFX(trace_kernel)<UNI_MINB_1, true>, threads);
-        if (variant == 2) return occupancy(IX_SFX(trace_kernel)<UNI_MINB_2, true>, threads);
-        return occupancy(IX_SFX(trace_kernel)<1, true>, threads);
+    const int budget = variant_budget(variant);
+    switch (uniaxial) {
+        case TRANSPORT_BIAXIAL: return occupancy(TaskLoop<TRANSPORT_BIAXIAL>::trace(budget), threads);
+        case TRANSPORT_UNIAXIAL: return occupancy(TaskLoop<TRANSPORT_UNIAXIAL>::trace(budget), threads);
+        default: return occupancy(TaskLoop<TRANSPORT_ISOTROPIC>::trace(budget), threads);
     }
-    if (variant == 1) return occupancy(IX_SFX(trace_kernel)<6, false>, threads);
-    if (variant == 2) return occupancy(IX_SFX(trace_kernel)<8, false>, threads);
-    return occupancy(IX_SFX(trace_kernel)<1, false>, threads);
 }
 
 int IX_SFX(trace_attributed_blocks_per_sm)(int threads, int uniaxial) {
-    if (uniaxial) return occupancy(IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, true>, threads);
-    return occupancy(IX_SFX(trace_attributed_kernel)<ATTR_MINB_ISO, false>, threads);
+    switch (uniaxial) {
+        case TRANSPORT_BIAXIAL: return occupancy(IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, TRANSPORT_BIAXIAL>, threads);
+        case TRANSPORT_UNIAXIAL:
+            return occupancy(IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, TRANSPORT_UNIAXIAL>, threads);
+        default: return occupancy(IX_SFX(trace_attributed_kernel)<ATTR_MINB_ISO, TRANSPORT_ISOTROPIC>, threads);
+    }
 }
 
 int IX_SFX(batch_blocks_per_sm)(int threads, int variant, int uniaxial) {
     if (variant < 0 || variant >= N_VARIANTS) return 0;
     if (shape_is_pool(variant_shape(variant))) return IX_SFX(pool_batch_blocks_per_sm)(variant, uniaxial);
     if (threads != 128) return 0;
-    variant = variant_budget(variant);
-    if (uniaxial) {
-        if (variant == 1) return occupancy(IX_SFX(batch_kernel)<UNI_MINB_1, true>, threads);
-        if (variant == 2) return occupancy(IX_SFX(batch_kernel)<UNI_MINB_2, true>, threads);
-        return occupancy(IX_SFX(batch_kernel)<1, true>, threads);
+    const int budget = variant_budget(variant);
+    switch (uniaxial) {
+        case TRANSPORT_BIAXIAL: return occupancy(TaskLoop<TRANSPORT_BIAXIAL>::batch(budget), threads);
+        case TRANSPORT_UNIAXIAL: return occupancy(TaskLoop<TRANSPORT_UNIAXIAL>::batch(budget), threads);
+        default: return occupancy(TaskLoop<TRANSPORT_ISOTROPIC>::batch(budget), threads);
     }
-    if (variant == 1) return occupancy(IX_SFX(batch_kernel)<6, false>, threads);
-    if (variant == 2) return occupancy(IX_SFX(batch_kernel)<8, false>, threads);
-    return occupancy(IX_SFX(batch_kernel)<1, false>, threads);
 }
 
 }  // namespace ix

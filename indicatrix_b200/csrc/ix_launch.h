@@ -18,6 +18,7 @@ enum : uint32_t {
     SCENE_PLEOCHROIC = 4u,  // the o-ray and e-ray absorption differ
     SCENE_SCATTERING = 8u,  // Henyey-Greenstein interior scattering (scattering_sigma_s > 0)
     SCENE_ROUNDED = 16u,    // rounded facet edges (edge_rounding_radius > 0)
+    SCENE_BIAXIAL = 32u,    // biaxial indicatrix (ix_material::biaxial, with anisotropic)
 };
 inline bool absorption_present(const ix_absorption& a) {
     if (a.has_spline) return true;
@@ -40,7 +41,9 @@ inline bool absorption_equal(const ix_absorption& a, const ix_absorption& b) {
 inline uint32_t scene_flags(const ix_material& m) {
     uint32_t f = 0;
     if (absorption_present(m.abs_o) || absorption_present(m.abs_e)) f |= SCENE_ABSORBING;
+    if (m.biaxial && m.has_abs_beta && absorption_present(m.abs_beta)) f |= SCENE_ABSORBING;
     if (m.anisotropic) f |= SCENE_UNIAXIAL;
+    if (m.anisotropic && m.biaxial) f |= SCENE_BIAXIAL;
     if (!absorption_equal(m.abs_o, m.abs_e)) f |= SCENE_PLEOCHROIC;
     if (m.scattering_sigma_s > 0.0f) f |= SCENE_SCATTERING;
     if (m.edge_rounding_radius > 0.0f) f |= SCENE_ROUNDED;
@@ -49,7 +52,16 @@ inline uint32_t scene_flags(const ix_material& m) {
 // The isotropic megakernel assumes equal o/e absorption and no birefringence; any other
 // scene runs the uniaxial instantiation of the transport.
 inline bool needs_uniaxial_kernel(uint32_t flags) {
-    return (flags & (SCENE_UNIAXIAL | SCENE_PLEOCHROIC | SCENE_SCATTERING | SCENE_ROUNDED)) != 0;
+    return (flags & (SCENE_UNIAXIAL | SCENE_PLEOCHROIC | SCENE_SCATTERING | SCENE_ROUNDED | SCENE_BIAXIAL)) != 0;
+}
+// The transport instantiation a scene needs: the isotropic megakernel, the uniaxial one,
+// or the uniaxial one with the biaxial bounce (which serves uniaxial and isotropic scenes
+// too, so a batch takes the largest of its scenes' classes).
+enum TransportClass : int { TRANSPORT_ISOTROPIC = 0, TRANSPORT_UNIAXIAL = 1, TRANSPORT_BIAXIAL = 2 };
+constexpr int N_TRANSPORT_CLASSES = 3;
+inline int transport_class(uint32_t flags) {
+    if (flags & SCENE_BIAXIAL) return TRANSPORT_BIAXIAL;
+    return needs_uniaxial_kernel(flags) ? TRANSPORT_UNIAXIAL : TRANSPORT_ISOTROPIC;
 }
 
 // Launch shapes of the trace megakernels.  A shape is a task loop and a CTA size:
@@ -121,7 +133,7 @@ struct BatchJob {
 struct BatchLaunch {
     const ix_scene* scenes;      // device array; each scene's `planes` is a device pointer
     const uint32_t* flags;       // device, scene_flags per scene
-    uint32_t uniaxial;           // any scene needs the uniaxial transport
+    uint32_t uniaxial;           // the plan's transport class (TransportClass): the largest of its scenes'
     const BatchJob* jobs;        // device, ascending task_begin and chunk_begin
     uint32_t n_jobs;
     uint32_t total_tasks;
@@ -200,6 +212,12 @@ enum CheckFn {
     CHECK_FRESNEL_CHANNEL = 15,  // in: n1, n2, cos_i, I,Q,U,V  out: reflected I,Q,U,V,
                                  // transmitted I,Q,U,V, r_s, r_p, t_s, t_p, TIR (0 / 1)
     CHECK_CHANNEL_ALPHA = 16, // in: k xyz, lambda  out: alpha (scene material, isotropic form)
+    CHECK_BIAXIAL = 17,       // in: k xyz, normal xyz, cos_i, lambda, n_beta  out: the scene
+                              // material's biaxial indicatrix at n_beta (its absorption at
+                              // lambda): wave_indices (slow, fast), eigen D
+                              // (slow xyz, fast xyz), mode_poynting_dir (slow, fast),
+                              // resolve_entry_mode (slow n, dir xyz, fast n, dir xyz), assigned-
+                              // mode alpha of the trichroic tensor (mode B, mode A)
 };
 
 struct CheckLaunch {
@@ -288,8 +306,8 @@ int pool_batch_blocks_per_sm_exact(int variant, int uniaxial);
 int pool_batch_blocks_per_sm_fast(int variant, int uniaxial);
 cudaError_t launch_check_exact(const CheckLaunch& l, cudaStream_t stream);
 cudaError_t launch_check_fast(const CheckLaunch& l, cudaStream_t stream);
-// Occupancy-derived resident blocks per SM for the trace kernel at `threads` per block
-// (the uniaxial instantiation when `uniaxial` != 0).
+// Occupancy-derived resident blocks per SM for the trace kernel at `threads` per block.
+// In these `uniaxial` is the transport class (TransportClass) of the instantiation.
 int trace_blocks_per_sm_exact(int threads, int variant, int uniaxial, size_t* smem_bytes);
 int trace_blocks_per_sm_fast(int threads, int variant, int uniaxial, size_t* smem_bytes);
 // FP32 FMA-pipe throughput probe (ix_probe.cu): best FLOP/s of `reps` timed runs.

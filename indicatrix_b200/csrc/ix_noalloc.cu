@@ -37,7 +37,7 @@ struct DeviceSetup {
     bool ready = false;
     uint32_t* scratch = nullptr;  // device address of g_noalloc_scratch
     int sm_count = 0;
-    int blocks_per_sm[2] = {0, 0};  // isotropic / uniaxial transport instantiation
+    int blocks_per_sm[ix::N_TRANSPORT_CLASSES] = {0, 0, 0};  // by transport instantiation (TransportClass)
 };
 DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mu;
@@ -61,7 +61,8 @@ int setup_device(int dev, DeviceSetup** out) {
         }
         s.scratch = static_cast<uint32_t*>(p);
         s.sm_count = sms;
-        for (int u = 0; u < 2; ++u) s.blocks_per_sm[u] = std::max(1, ix::trace_blocks_per_sm_fast(128, 2, u, nullptr));
+        for (int u = 0; u < ix::N_TRANSPORT_CLASSES; ++u)
+            s.blocks_per_sm[u] = std::max(1, ix::trace_blocks_per_sm_fast(128, 2, u, nullptr));
         s.ready = true;
     }
     *out = &s;
@@ -107,7 +108,7 @@ extern "C" int ix_accumulate_device_noalloc(const ix_scene* scene, uint32_t samp
     L.dropped = reinterpret_cast<unsigned long long*>(s->scratch + kMaxLaunches);
     L.threads = 128;
     L.variant = 2;
-    L.blocks = s->sm_count * s->blocks_per_sm[ix::needs_uniaxial_kernel(L.flags) ? 1 : 0];
+    L.blocks = s->sm_count * s->blocks_per_sm[ix::transport_class(L.flags)];
     uint64_t begin = 0;
     for (int k = 0; begin < n_pixels; ++k) {
         const uint32_t n = (uint32_t)std::min<uint64_t>(px_per_launch, n_pixels - begin);

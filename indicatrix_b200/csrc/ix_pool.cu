@@ -96,7 +96,7 @@ IX_DEV uint32_t pool_fill(WarpPool& wp, const PoolJob& J, uint32_t chunk, uint32
 // belongs to and returns its index; `load_planes(job)` returns the job's planes (called
 // with the warp converged and its groups idle).  The k-th claim on `counter` takes chunk
 // k * stride while that is below total_chunks.  Returns the samples this lane dropped.
-template <bool UNI, class JobOf, class LoadPlanes>
+template <int UNI, class JobOf, class LoadPlanes>
 IX_DEV uint32_t pool_loop(const Group& g, uint32_t* counter, uint32_t total_chunks, uint32_t stride, WarpPool& wp,
                           JobOf job_of, LoadPlanes load_planes) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -179,11 +179,11 @@ IX_DEV uint32_t pool_loop(const Group& g, uint32_t* counter, uint32_t total_chun
 }
 
 // Resident-warp targets of the register budgets 1 and 2 (isotropic / uniaxial transport).
-template <bool UNI>
+template <int UNI>
 constexpr int budget_warps(int budget) {
     return budget == 0 ? 0 : (UNI ? (budget == 1 ? 12 : 16) : (budget == 1 ? 24 : 32));
 }
-template <int WARPS, bool UNI>
+template <int WARPS, int UNI>
 constexpr int budget_minb(int budget) {
     return budget_warps<UNI>(budget) == 0 ? 1
                                           : (budget_warps<UNI>(budget) / WARPS > 0 ? budget_warps<UNI>(budget) / WARPS : 1);
@@ -192,7 +192,7 @@ constexpr int budget_minb(int budget) {
 }  // namespace
 
 // Single scene: the launch's pixels x samples; the planes are shared by the whole CTA.
-template <int WARPS, int MINB, bool UNI>
+template <int WARPS, int MINB, int UNI>
 __global__ void __launch_bounds__(WARPS * 32, MINB) IX_SFX(pool_trace_kernel)(const __grid_constant__ TraceLaunch L) {
     __shared__ float4 s_planes[IX_MAX_PLANES];
     __shared__ WarpPool s_pool[WARPS];
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) IX_SFX(pool_trace_kernel)(co
 // Many scenes in one persistent launch: the chunk space is the concatenation of every
 // job's chunks; a warp finds a chunk's job by binary search over the jobs' first chunks
 // and keeps the planes of its current job's scene in its own shared-memory slot.
-template <int WARPS, int MINB, bool UNI>
+template <int WARPS, int MINB, int UNI>
 __global__ void __launch_bounds__(WARPS * 32, MINB) IX_SFX(pool_batch_kernel)(const __grid_constant__ BatchLaunch L) {
     __shared__ float4 s_planes[WARPS][IX_MAX_PLANES];
     __shared__ WarpPool s_pool[WARPS];
@@ -280,7 +280,7 @@ namespace {
 
 // Kernel of (shape, budget, transport) for the single-scene and the batched loop.  The
 // exact build carries the 128-thread shape only, the single-scene loop that shape only.
-template <int WARPS, bool UNI>
+template <int WARPS, int UNI>
 struct PoolKernels {
     static void* trace(int budget) {
         switch (budget) {
@@ -298,7 +298,7 @@ struct PoolKernels {
     }
 };
 
-template <bool UNI>
+template <int UNI>
 void* pick(bool batch, int variant) {
     const int shape = variant_shape(variant), budget = variant_budget(variant);
     if (shape == SHAPE_POOL_128) return batch ? PoolKernels<4, UNI>::batch(budget) : PoolKernels<4, UNI>::trace(budget);
@@ -308,9 +308,13 @@ void* pick(bool batch, int variant) {
 #endif
     return nullptr;
 }
-void* pick_kernel(bool batch, int variant, bool uni) {
+void* pick_kernel(bool batch, int variant, int transport) {
     if (variant < 0 || variant >= N_VARIANTS) return nullptr;
-    return uni ? pick<true>(batch, variant) : pick<false>(batch, variant);
+    switch (transport) {
+        case TRANSPORT_BIAXIAL: return pick<TRANSPORT_BIAXIAL>(batch, variant);
+        case TRANSPORT_UNIAXIAL: return pick<TRANSPORT_UNIAXIAL>(batch, variant);
+        default: return pick<TRANSPORT_ISOTROPIC>(batch, variant);
+    }
 }
 
 int blocks_per_sm(void* k, int variant) {
@@ -325,7 +329,7 @@ int blocks_per_sm(void* k, int variant) {
 }  // namespace
 
 cudaError_t IX_SFX(launch_pool_trace)(const TraceLaunch& l, cudaStream_t stream) {
-    void* k = pick_kernel(false, l.variant, needs_uniaxial_kernel(l.flags));
+    void* k = pick_kernel(false, l.variant, transport_class(l.flags));
     if (!k || !l.acc || l.threads != shape_threads(variant_shape(l.variant))) return cudaErrorInvalidValue;
     if (l.scene.n_planes > IX_MAX_PLANES || l.spp > FIXED_MAX_SAMPLES) return cudaErrorInvalidValue;
     if ((uint64_t)l.n_pixels * l.spp > 0xFFFFFFFFull - POOL_CHUNK) return cudaErrorInvalidValue;
@@ -340,7 +344,7 @@ cudaError_t IX_SFX(launch_pool_trace)(const TraceLaunch& l, cudaStream_t stream)
 }
 
 cudaError_t IX_SFX(launch_pool_batch)(const BatchLaunch& l, cudaStream_t stream) {
-    void* k = pick_kernel(true, l.variant, l.uniaxial != 0);
+    void* k = pick_kernel(true, l.variant, (int)l.uniaxial);
     if (!k || !l.acc || l.n_jobs == 0 || l.stride == 0 || l.threads != shape_threads(variant_shape(l.variant)))
         return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
@@ -350,10 +354,10 @@ cudaError_t IX_SFX(launch_pool_batch)(const BatchLaunch& l, cudaStream_t stream)
 }
 
 int IX_SFX(pool_trace_blocks_per_sm)(int variant, int uniaxial) {
-    return blocks_per_sm(pick_kernel(false, variant, uniaxial != 0), variant);
+    return blocks_per_sm(pick_kernel(false, variant, uniaxial), variant);
 }
 int IX_SFX(pool_batch_blocks_per_sm)(int variant, int uniaxial) {
-    return blocks_per_sm(pick_kernel(true, variant, uniaxial != 0), variant);
+    return blocks_per_sm(pick_kernel(true, variant, uniaxial), variant);
 }
 
 }  // namespace ix

@@ -18,6 +18,7 @@
 #include "ix_device.cuh"
 #include "ix_launch.h"
 #include "ix_uniaxial.cuh"
+#include "ix_biaxial.cuh"
 
 namespace ix {
 
@@ -35,10 +36,12 @@ struct DevScene {
     uint32_t aniso;       // uniaxial birefringence
     uint32_t scattering;  // Henyey-Greenstein interior scattering (uniaxial instantiation)
     uint32_t rounded;     // rounded facet edges (uniaxial instantiation)
+    uint32_t biaxial;     // biaxial indicatrix (uniaxial instantiation)
 };
 IX_DEV DevScene make_scene(const ix_scene& s, uint32_t flags) {
     return DevScene{s, (flags & SCENE_ABSORBING) ? 1u : 0u, (flags & SCENE_UNIAXIAL) ? 1u : 0u,
-                    (flags & SCENE_SCATTERING) ? 1u : 0u, (flags & SCENE_ROUNDED) ? 1u : 0u};
+                    (flags & SCENE_SCATTERING) ? 1u : 0u, (flags & SCENE_ROUNDED) ? 1u : 0u,
+                    (flags & SCENE_BIAXIAL) ? 1u : 0u};
 }
 
 // The 8 lanes of one path: `mask` selects them in the warp, `c` is this lane's channel.
@@ -77,9 +80,10 @@ struct LanePath {
     // Uniaxial transport only (the isotropic kernels never touch these).
     V3 k;              // wave normal; the ray direction `d` is the Poynting direction
     bool is_e;         // eigenmode assigned at the last entry or internal coupling
-    float n_e;         // extraordinary_index_at for channel c
+    float n_e;         // extraordinary_index_at for channel c; for a biaxial material the
+                       // channel's beta-ray absorption (biaxial paths use no e index)
     float n_e_hero;    // channel 0's
-    float alpha_e;     // e-ray absorption of channel c
+    float alpha_e;     // e-ray (gamma-ray) absorption of channel c
 };
 
 // ------------------------------------------------------------------------------------
@@ -213,7 +217,7 @@ IX_DEV V3 rotate_to_plane_of_incidence(Stokes& st, bool has_prev, V3 prev_pn, V3
 // ------------------------------------------------------------------------------------
 // Path setup: PathState::new (bounce_body.rs:260-356).
 // ------------------------------------------------------------------------------------
-template <bool UNI>
+template <int UNI>
 IX_DEV void group_init_ray(const Group& g, LanePath& P, const DevScene& S, Ray r, uint32_t seed,
                            float hero_rand) {
     const ix_scene& sc = S.s;
@@ -242,11 +246,16 @@ IX_DEV void group_init_ray(const Group& g, LanePath& P, const DevScene& S, Ray r
         P.n_e = S.aniso ? extraordinary_index_at(sc.material, P.lambda, P.n) : P.n;
         P.n_e_hero = gshfl(g, P.n_e, 0);
         P.alpha_e = S.absorbing ? spectral_absorption(sc.material.abs_e, P.lambda) : 0.0f;
+        if constexpr (UNI == TRANSPORT_BIAXIAL) {
+            if (S.biaxial)  // the beta-ray alpha; the alpha ray's without beta bands (wavelength_cache.rs:37-52)
+                P.n_e = (S.absorbing && sc.material.has_abs_beta) ? spectral_absorption(sc.material.abs_beta, P.lambda)
+                                                                  : P.alpha;
+        }
     }
 }
 
 // One (pixel, absolute sample) as renderer/cpu_frame.rs:45-70 traces it.
-template <bool UNI>
+template <int UNI>
 IX_DEV void group_init(const Group& g, LanePath& P, const DevScene& S, uint32_t pixel,
                        uint32_t sample) {
     const ix_scene& sc = S.s;
@@ -1130,12 +1139,251 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     return BOUNCE_CONTINUE;
 }
 
-template <bool UNI>
+// ------------------------------------------------------------------------------------
+// One bounce of a path in a biaxial crystal (transport/bounce.rs:108-160 with the
+// biaxial arms of refraction/geometry.rs:220-400, dispatch.rs:162-300,
+// reflect_refract.rs:121-330 and absorption.rs:227): no closed-form uniaxial solve, so
+// every interface takes the scalar-Fresnel path; the two eigenmodes ("mode A", the fast
+// root, and "mode B", the slow root, in the is_e slot) take their indices from each
+// channel's own indicatrix at the hero's wave normal (resolved per mode by a two-step
+// fixed point on entry), the entry split is 50 / 50, both modes walk off, and the
+// trichroic tensor absorbs along the assigned mode's field.  Out of line and by value:
+// the uniaxial bounce, and every kernel that inlines it, compiles as it does without it.
+// ------------------------------------------------------------------------------------
+struct BiaxialStep {
+    LanePath P;
+    float esc;
+    int result;
+};
+static __device__ __noinline__ BiaxialStep group_bounce_biaxial(Group g, LanePath P, DevScene S,
+                                                                 const float4* __restrict__ planes) {
+    BiaxialStep out{P, 0.0f, BOUNCE_CONTINUE};
+    const ix_scene& sc = S.s;
+    const ix_material& mat = sc.material;
+    const uint32_t bounce = P.bounce;
+    Hit hit = group_next_hit(g, P, planes, (int)sc.n_planes);
+    if (hit.facet < 0) {
+        out.esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
+        out.P = P;
+        out.result = BOUNCE_ESCAPED;
+        return out;
+    }
+    const BiaxFrame F = biax_frame(load3(mat.c_axis));
+    const Indicatrix hero = make_indicatrix(mat, P.n_hero), own = make_indicatrix(mat, P.n);
+    // channel_absorption_alphas_assigned (absorption.rs:227): the hero indicatrix's
+    // assigned-mode field against this channel's (alpha, beta, gamma) tensor; n_e holds
+    // the beta-ray alpha.
+    auto channel_alpha = [&](V3 k) {
+        const V3 e = assigned_mode_e_field_biaxial(hero, F, k, P.is_e);
+        return biaxial_quadratic_form(F, P.alpha, P.n_e, P.alpha_e, e);
+    };
+    if (S.scattering && P.inside) {
+        const ScatterResult r = scatter_or_survive(g, P.seed, bounce, S.absorbing ? channel_alpha(P.k) : 0.0f,
+                                                   mat.scattering_sigma_s, mat.absorption_path_scale,
+                                                   mat.scattering_g, hit.t, intensity(P.st), P.d);
+        P.pdf = P.pdf * r.pdf_factor;
+        if (r.scattered) {
+            P.st = Stokes{r.st_factor, 0.0f, 0.0f, 0.0f};
+            P.o = P.o + r.t_model * P.d;
+            P.d = r.dir;
+            P.k = r.dir;
+            P.has_prev = false;
+            if (bounce > 4) {
+                float max_i = intensity(P.st);
+#pragma unroll
+                for (int mm = 4; mm > 0; mm >>= 1) max_i = fmaxf(max_i, gxor(g, max_i, mm));
+                const float q = clampf_(fmaxf(0.0f, max_i), 0.05f, 1.0f);
+                if (unit_draw(P.seed, bounce, RUSSIAN_ROULETTE_STREAM) > q) {
+                    out.P = P;
+                    out.result = BOUNCE_KILLED;
+                    return out;
+                }
+                P.st = scale(P.st, 1.0f / q);
+                P.split = P.split / q;
+            }
+            P.bounce = bounce + 1;
+            out.P = P;
+            return out;
+        }
+        P.st = scale(P.st, r.st_factor);
+    }
+    P.facet = hit.facet;
+    const float4 pl = planes[hit.facet];
+    V3 normal = v3(pl.x, pl.y, pl.z);
+    const V3 hit_point = P.o + hit.t * P.d;
+    if (S.rounded)
+        normal = group_shading_normal(g, planes, (int)sc.n_planes, hit_point, hit.facet, normal,
+                                      mat.edge_rounding_radius);
+    const V3 k_hat = P.k;
+    const V3 cpn = rotate_to_plane_of_incidence(P.st, P.has_prev, P.prev_pn, k_hat, normal);
+    P.has_prev = true;
+    P.prev_pn = cpn;
+    if (P.inside) {
+        normal = -normal;
+        if (S.absorbing && !S.scattering)
+            P.st = scale(P.st, exp_lane(-channel_alpha(k_hat) * (hit.t * mat.absorption_path_scale)));
+    }
+
+    // compute_bounce_refraction_geometry's biaxial arm (geometry.rs:306-400).
+    const float cos_i = clampf_(dot(-k_hat, normal), 0.0f, 1.0f);
+    const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
+    const float sin_i = __fsqrt_rn(fmaxf(one_m_c2, 0.0f));
+    const bool inside0 = P.inside;
+    V3 dir_a = k_hat, dir_b = k_hat;
+    if (!inside0) {
+        resolve_entry_mode(hero, F, k_hat, normal, cos_i, P.n_hero, false, dir_a);
+        resolve_entry_mode(hero, F, k_hat, normal, cos_i, P.n_hero, true, dir_b);
+    }
+    float ns, nf;
+    wave_indices(own, F, dir_a, ns, nf);
+    const float n_a = nf;
+    wave_indices(own, F, dir_b, ns, nf);
+    const float n_b = ns;
+    const float n_a_hero = gshfl(g, n_a, 0), n_b_hero = gshfl(g, n_b, 0);
+    const bool mode_a_medium = inside0 && !P.is_e;
+    const float n_med = mode_a_medium ? n_a : n_b;
+    const float n_med_hero = mode_a_medium ? n_a_hero : n_b_hero;
+    const float n1 = inside0 ? n_med_hero : 1.0f;
+    const float n2 = inside0 ? 1.0f : n_med_hero;
+    const float eta = __fdiv_rn(n1, n2);
+    const float sin2_t = eta * eta * one_m_c2;
+    const float n1k = inside0 ? n_med : 1.0f;
+    const float n2k = inside0 ? 1.0f : n_med;
+    const float etak = __fdiv_rn(n1k, n2k);
+    const float s2k = etak * etak * one_m_c2;
+
+    V3 new_k, new_s;
+    bool new_inside = inside0;
+    int update = -1;
+    int status = 0;
+    bool narrow = false, want_probe = false;
+    V3 dir_k = v3(0.0f, 0.0f, 0.0f);
+    float t_int = 0.0f;
+    const bool frosted = facet_frosted(S, hit.facet);
+    if (frosted) {
+        const FrostedScatter f = frosted_scatter(P.seed, bounce, normal, n1, n2, cos_i, sin2_t);
+        lane_frosted_apply(P, f);
+        new_k = new_s = f.dir;
+        if (f.transmit) {
+            new_inside = !inside0;
+            if (!inside0) update = unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f ? 1 : 0;
+        }
+    } else if (sin2_t > 1.0f) {
+        // apply_tir_bounce's scalar arm (tir.rs:98-116); the reflected wave normal's mode
+        // walks off (poynting_dir_for_mode, geometry.rs:440).
+        P.st = lane_scalar_reflect(P, n1k, n2k, s2k, cos_i, sin_i);
+        new_k = k_hat - 2.0f * dot(k_hat, normal) * normal;
+        new_s = mode_poynting_dir(hero, F, new_k, P.is_e);
+    } else {
+        // apply_partial_fresnel_bounce (dispatch.rs:162-300): 50 / 50 at an entry.
+        const bool entering = !inside0;
+        const bool use_e = entering ? unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f : P.is_e;
+        float r_s, r_p;
+        fresnel_rs_rp(n1, n2, cos_i, sqrtf(fmaxf(1.0f - sin2_t, 0.0f)), r_s, r_p);
+        const float r_unpol = clampf_(r_unpol_of(r_s, r_p), R_UNPOL_SELECT_MIN, R_UNPOL_SELECT_MAX);
+        if (unit_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM) < r_unpol) {
+            P.st = scale(lane_scalar_reflect(P, n1k, n2k, s2k, cos_i, sin_i), 1.0f / r_unpol);
+            new_k = k_hat - 2.0f * dot(k_hat, normal) * normal;
+            new_s = inside0 ? mode_poynting_dir(hero, F, new_k, P.is_e) : new_k;
+        } else {
+            // apply_refract_bounce (reflect_refract.rs:121-200): on entry the selected
+            // mode's own index and walk-off, per channel its own indicatrix.
+            // The hero's direction and each channel's own are formed by one correctly
+            // rounded routine, so the hero lane's channel direction is the hero direction
+            // bit for bit: the eigen-direction amplifies any difference near an optic
+            // axis, and the hero must never fail its own match test (geometry.rs:366).
+            auto refract_rn = [&](float eta, float& cos_t) {
+                const float s2 = fminf(mul_(mul_(eta, eta), one_m_c2), 1.0f);
+                cos_t = __fsqrt_rn(fmaxf(sub_(1.0f, s2), 0.0f));
+                return normalize_(vadd_(vmul_(k_hat, eta), vmul_(normal, fmaf(eta, cos_i, -cos_t))));
+            };
+            const float n2_dir = entering ? (use_e ? n_b_hero : n_a_hero) : n2;
+            float c_dir;
+            const V3 refr = refract_rn(div_(n1, n2_dir), c_dir);
+            const V3 final_refr = entering ? mode_poynting_dir(hero, F, refr, use_e) : refr;
+            const float n2k_r = (entering && !use_e) ? n_a : n2k;
+            const float ratio = div_(n1k, n2k_r);
+            const float s2r = mul_(mul_(ratio, ratio), one_m_c2);
+            const Stokes original = P.st;
+            if (s2r > 1.0f) {
+                P.st = scale(P.st, 0.0f);
+                P.pdf = 0.0f;
+            } else {
+                float cos_t_k;
+                const V3 refr_k = refract_rn(ratio, cos_t_k);
+                dir_k = entering ? mode_poynting_dir(own, F, refr_k, use_e) : refr_k;
+                status = dot(dir_k, final_refr) >= DIRECTION_MATCH_COS_TOL ? 1 : 2;
+                const float two = 2.0f * n1k * cos_i;
+                const float t_s = two / fmaf(n2k_r, cos_t_k, n1k * cos_i);
+                const float t_p = two / fmaf(n1k, cos_t_k, n2k_r * cos_i);
+                const Stokes transmitted =
+                    scale(fresnel_transmit_apply(original, n1k, n2k_r, cos_i, cos_t_k, t_s, t_p),
+                          1.0f / (1.0f - r_unpol));
+                float rs, rp;
+                fresnel_rs_rp(n1k, n2k_r, cos_i, cos_t_k, rs, rp);
+                P.pdf = P.pdf * (1.0f - clampf_(r_unpol_of(rs, rp), R_UNPOL_PDF_MIN, R_UNPOL_PDF_MAX));
+                P.st = status == 1 ? transmitted : scale(original, 0.0f);
+                t_int = intensity(transmitted);
+                want_probe = status == 2 && inside0 && intensity(original) > 0.0f;
+            }
+            narrow = entering;
+            new_k = refr;
+            new_s = final_refr;
+            new_inside = !inside0;
+            update = entering ? (use_e ? 1 : 0) : -1;
+        }
+    }
+    group_exit_probes(g, P, S, planes, hit_point, want_probe, dir_k, t_int);
+    if (narrow) group_narrow_compat(g, P, status, dir_k);
+
+    const bool was_internal_reflection = inside0 && update < 0 && new_inside == inside0;
+    P.d = new_s;
+    P.o = hit_point + new_s * 1e-4f;
+    P.k = new_k;
+    P.inside = new_inside;
+    if (update >= 0) P.is_e = update != 0;
+    // maybe_apply_internal_mode_coupling (transport/bounce.rs:441-470): a blanket 50 / 50.
+    if (was_internal_reflection) P.is_e = unit_draw(P.seed, bounce, MODE_COUPLING_STREAM) >= 0.5f;
+
+    const float glare = clampf_(sc.environment.surface_glare, 0.0f, 1.0f);
+    if (bounce == 0 && !P.inside && glare < 1.0f && !frosted) P.st = scale(P.st, glare);
+    if (bounce > 4) {
+        float max_i = intensity(P.st);
+#pragma unroll
+        for (int m = 4; m > 0; m >>= 1) max_i = fmaxf(max_i, gxor(g, max_i, m));
+        const float q = clampf_(fmaxf(0.0f, max_i), 0.05f, 1.0f);
+        if (unit_draw(P.seed, bounce, RUSSIAN_ROULETTE_STREAM) > q) {
+            out.P = P;
+            out.result = BOUNCE_KILLED;
+            return out;
+        }
+        P.st = scale(P.st, 1.0f / q);
+        P.split = P.split / q;
+    }
+    P.bounce = bounce + 1;
+    out.P = P;
+    return out;
+}
+
+// UNI is the transport instantiation (transport_class): TRANSPORT_ISOTROPIC the isotropic
+// megakernel, TRANSPORT_UNIAXIAL the uniaxial bounce, TRANSPORT_BIAXIAL the uniaxial bounce
+// plus the out-of-line biaxial one (kept out of the uniaxial kernels, whose register
+// allocation the call site would change).
+template <int UNI>
 IX_DEV int group_step(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes, float& esc) {
-    if constexpr (UNI)
+    if constexpr (UNI == TRANSPORT_BIAXIAL) {
+        if (S.biaxial) {
+            const BiaxialStep r = group_bounce_biaxial(g, P, S, planes);
+            P = r.P;
+            esc = r.esc;
+            return r.result;
+        }
         return group_bounce_uniaxial(g, P, S, planes, esc);
-    else
+    } else if constexpr (UNI == TRANSPORT_UNIAXIAL) {
+        return group_bounce_uniaxial(g, P, S, planes, esc);
+    } else {
         return group_bounce(g, P, S, planes, esc);
+    }
 }
 
 // finish (bounce_body.rs:724-764): commit the exit splits of an escaped path, integrate
@@ -1187,7 +1435,7 @@ IX_DEV V3 group_finish(const Group& g, const LanePath& P, const DevScene& S, boo
 }
 
 // A whole path by one group (the check kernels' per-path entry).
-template <bool UNI>
+template <int UNI>
 IX_DEV V3 group_trace(const Group& g, LanePath& P, const DevScene& S, const float4* planes,
                       uint32_t* iterations) {
     float esc = 0.0f;

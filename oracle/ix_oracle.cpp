@@ -3090,15 +3090,15 @@ void ixo_fresnel_channel(float n1, float n2, float cos_i, const float s_in[4], f
     out[8] = raw(r_s), out[9] = raw(r_p), out[10] = raw(t_s), out[11] = raw(t_p);
 }
 
-// The biaxial indicatrix of `m` at lambda (its own channel) evaluated at wave normal k:
+// The biaxial indicatrix of `m` at n_beta (its absorption at lambda) evaluated at wave normal k:
 // out[0..1] wave_indices (slow, fast); out[2..7] eigen_polarizations (slow xyz, fast xyz);
 // out[8..13] mode_poynting_dir (slow, fast); out[14..21] resolve_entry_mode against
 // `normal` at cos_i seeded with n_beta (slow n, dir xyz, fast n, dir xyz); out[22..23]
 // the assigned-mode alpha of the biaxial tensor (mode B, mode A).
 void ixo_biaxial_bundle(const ix_material* m, const float k[3], const float normal[3], float cos_i,
-                        float lambda_nm, float out[24]) {
+                        float lambda_nm, float n_beta_in, float out[24]) {
     const V3 kk = load3(k), nn = load3(normal);
-    const F n_beta = dispersion_eval(m->dispersion, lambda_nm);
+    const F n_beta = n_beta_in;
     const TensorFrame ax = tensor_frame(load3(m->c_axis));
     const Indicatrix I = make_indicatrix(*m, n_beta, ax);
     F ns, nf;

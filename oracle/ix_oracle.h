@@ -84,7 +84,7 @@ void ixo_fresnel_channel(float n1, float n2, float cos_i, const float s_in[4], f
  * (channel_absorption_alphas_assigned, raytracer/absorption.rs:197). */
 float ixo_channel_alpha(const ix_material* m, const float k[3], float lambda_nm);
 void ixo_biaxial_bundle(const ix_material* m, const float k[3], const float normal[3], float cos_i,
-                        float lambda_nm, float out[24]);
+                        float lambda_nm, float n_beta, float out[24]);
 /* simd/slab.rs:147 + intersect.rs:101: returns 1 and fills t/idx on a hit */
 int ixo_intersect(const float* planes, uint32_t n_planes, const float origin[3],
                   const float dir[3], float* t, int32_t* facet);

@@ -154,7 +154,7 @@ def _load(name: str) -> C.CDLL:
     lib.ixo_channel_alpha.restype = C.c_float
     lib.ixo_channel_alpha.argtypes = [P(abi.Material), f32p, C.c_float]
     lib.ixo_biaxial_bundle.restype = None
-    lib.ixo_biaxial_bundle.argtypes = [P(abi.Material), f32p, f32p, C.c_float, C.c_float, f32p]
+    lib.ixo_biaxial_bundle.argtypes = [P(abi.Material), f32p, f32p, C.c_float, C.c_float, C.c_float, f32p]
     lib.ixo_counting_build.restype = C.c_int
     lib.ixo_count_flops.restype = C.c_int
     lib.ixo_count_flops.argtypes = [P(abi.Scene), C.c_uint32, C.c_uint32, C.c_uint32,
