@@ -133,16 +133,25 @@ def test_biaxial_frame_sums_match_oracle(exact_backend, oracle):
 def test_biaxial_tier3_fast_build(backend, oracle, name):
     """Tier 3 on the benched build: a batch plan (one persistent launch, the kernel the
     frame and batch benchmarks time) traces samples [0, 500) of a 48 x 48 biaxial frame,
-    the oracle samples [500, 1000); the reference's pass rule on X, Y and Z."""
+    the oracle samples [500, 1000); the reference's pass rule on X, Y and Z.  Each side's
+    standard error is its own sample variance (z_stats.rs:11-80): the device's from the
+    per-path check kernel over the same samples, whose per-pixel means the plan's sums
+    reproduce.  (A bright, heavy-tailed stone such as Alexandrite needs this: one side's
+    variance taken for both understates the error wherever that side missed a rare bright
+    sample, and the rule then flags ~30 pixels of 2304.)"""
     W, H, N = TIER3_W, TIER3_H, TIER3_SPP
     fs = frame_with(getattr(materials, name)(), W, H)
     plan = BatchPlan(backend, [(fs, 0, N)])
     plan.run()
     mg = plan.sums(0).reshape(-1, 3) / N
     plan.close()
+    xyz_g, _ = trace_paths(backend, fs, np.repeat(np.arange(W * H), N), np.tile(np.arange(N), W * H))
+    g = xyz_g.astype(np.float64).reshape(W * H, N, 3)
+    sg = g.var(axis=1, ddof=1) / N
+    assert np.allclose(mg, g.mean(axis=1), rtol=1e-3, atol=1e-6)
     mo, so = oracle_moments(oracle, fs.to_abi(), W * H, N, N)
     for c, axis in enumerate("XYZ"):
-        z = z_components(mo[:, c], so[:, c], mg[:, c], so[:, c])
+        z = z_components(mo[:, c], so[:, c], mg[:, c], sg[:, c])
         ok, count, cluster = passes_z_criteria(z, W, H)
         assert ok, (name, axis, count, cluster)
 
