@@ -102,18 +102,31 @@ void ix_set_work_limits(ix_backend* b, const ix_work_limits* limits);
 /* Rounding mode of later calls (IX_PRECISION_*). */
 void ix_set_precision(ix_backend* b, uint32_t precision);
 /* scene_routes_to_gpu (gpu_backend/mod.rs:288): 1 when this backend can trace `scene`
- * (convex, <= IX_MAX_PLANES, polished or frosted facets, an isotropic or uniaxial
- * material with modelled dispersion, a modelled environment, at most 2^32 - 1 pixels).
+ * (<= IX_MAX_PLANES planes carved by <= IX_MAX_TOOLS valid tools, polished or frosted
+ * facets, an isotropic, uniaxial or biaxial material with modelled dispersion, a modelled
+ * environment, at most 2^32 - 1 pixels).
  * The facet finishes are not read here. */
 int ix_scene_routes_to_gpu(const ix_scene* scene);
 /* scene_routes_to_gpu_with_tools (gpu_backend/tool_routing.rs:81): ix_scene_routes_to_gpu
- * with the stone's concave tools; this backend traces convex stones only, so any tool
- * (ntools > 0) declines. */
+ * of the stone carved by `tools` (when ntools > 0; else the scene's own tools): at most
+ * IX_MAX_TOOLS, each passing ix_tool_validate. */
 int ix_scene_routes_to_gpu_with_tools(const ix_scene* scene, const ix_tool* tools, uint32_t ntools);
+/* ToolPrimitive::validate (geometry/tool.rs:360): IX_TOOL_OK, or the first failed check
+ * (ToolPrimitiveError, tool.rs:133). */
+enum {
+    IX_TOOL_OK = 0,
+    IX_TOOL_NON_FINITE = 1,
+    IX_TOOL_NON_POSITIVE_RADIUS = 2,
+    IX_TOOL_AXIS_NOT_UNIT = 3,
+    IX_TOOL_UNKNOWN_KIND = 4,
+    IX_TOOL_UNKNOWN_SWEEP = 5,
+    IX_TOOL_PADDING_NOT_ZERO = 6
+};
+int ix_tool_validate(const ix_tool* tool);
 /* GpuBackend::try_accumulate_geom_cancellable (backend.rs:272) with an f32 accumulator:
  * adds (float)(f64 pixel sum) into accum_xyz.  `tools` / `ntools` are the stone's concave
- * tools (`tools: &[ToolPrimitive]`): ntools > 0 is declined (see ix_tool).  `cancel` may
- * be NULL; it is polled between chunks. */
+ * tools (`tools: &[ToolPrimitive]`, tool k facet id n_planes + k); with ntools = 0 the
+ * scene's own `tools` apply.  `cancel` may be NULL; it is polled between chunks. */
 int ix_accumulate(ix_backend* b, const ix_scene* scene, const ix_tool* tools, uint32_t ntools,
                   uint32_t sample_offset, uint32_t spp, float* accum_xyz, const volatile uint8_t* cancel);
 /* The same with an f64 accumulator (no rounding of the pixel sums). */
@@ -170,7 +183,7 @@ uint32_t ix_batch_plan_variant(const ix_batch_plan* p);
 uint64_t ix_batch_plan_job_offset(const ix_batch_plan* p, uint32_t job);
 void ix_batch_plan_destroy(ix_batch_plan* p);
 /* Device-resident form for callers that keep the scene and the sums in GPU memory:
- * `scene->planes`, `scene->facet_finishes` (if any) and `d_accum_xyz` are device
+ * `scene->planes`, `scene->facet_finishes` and `scene->tools` (if any) and `d_accum_xyz` are device
  * pointers; the launch is enqueued on `stream` (a cudaStream_t, or NULL for the
  * backend's own stream) and not synchronised.
  * `accumulate` = 1 adds into d_accum_xyz, 0 overwrites it. */
@@ -180,7 +193,7 @@ int ix_accumulate_device(ix_backend* b, const ix_scene* scene, uint32_t sample_o
  *
  * For callers that cannot call cudaMalloc (a host whose own pool or arena owns all
  * device memory, a sandboxed plug-in, a runtime with a fixed memory budget): they pass
- * a scene whose `planes` (and `facet_finishes`, if any) are device pointers and a device
+ * a scene whose `planes` (and `facet_finishes` and `tools`, if any) are device pointers and a device
  * output `d_accum_xyz`
  * (width * height * 3 doubles, added into when `accumulate` is 1, overwritten when 0),
  * and the call needs no backend object and makes no cudaMalloc, cudaFree or other

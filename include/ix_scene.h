@@ -125,6 +125,8 @@ typedef struct ix_environment {
     float uniform_radiance;     /* IX_ENV_UNIFORM dome radiance                         */
 } ix_environment;
 
+struct ix_tool;
+
 /* The scene.  `planes` is n_planes x {nx, ny, nz, d} with the convention n.x + d <= 0
  * inside (geometry/plane.rs:34-41).  `facet_finishes` may be NULL (all polished); entry
  * i is facet i's FacetFinish (0 Polished, nonzero Frosted), facets past n_finishes are
@@ -140,14 +142,20 @@ typedef struct ix_scene {
     ix_material material;
     uint32_t max_bounces;
     ix_environment environment;
+    /* Concave tools carved out of the stone (StoneGeometry::tools, geometry/tool.rs:173):
+     * NULL / 0 for a convex stone.  Tool k has facet id n_planes + k.  The accumulate
+     * entries take their `tools` / `ntools` arguments instead when ntools > 0. */
+    const struct ix_tool* tools;
+    uint32_t n_tools;
 } ix_scene;
 
 /* A concave tool volume subtracted from the stone (ToolPrimitive,
  * crates/indicatrix/src/geometry/tool.rs:112-131), field for field: the same 80-byte
  * record (the reference aligns it to 16 bytes): kind 0 ball, 1 capped cylinder, 2 cone
- * frustum, 3 bicone; sweep_kind 0 none, 1 along the axis, 2 across it.  This backend
- * traces convex stones only: a call that passes tools is declined (the reference's GPU
- * path declines what it cannot trace; the caller traces such a stone on the CPU). */
+ * frustum, 3 bicone; sweep_kind 0 none, 1 along the axis, 2 across it.  At most
+ * IX_MAX_TOOLS per stone (GPU_MAX_TOOL_PRIMITIVES, tool/pack.rs:51); a tool that fails
+ * ToolPrimitive::validate (tool.rs:360) makes the scene decline. */
+#define IX_MAX_TOOLS 128
 typedef struct ix_tool {
     uint32_t kind;
     uint32_t sweep_kind;

@@ -14,6 +14,7 @@ MAX_PLANES = 128
 MAX_BANDS = 8
 SPLINE_KNOTS = 16
 RING_LIGHTS = 16
+MAX_TOOLS = 128
 
 DISP_SELLMEIER1, DISP_SELLMEIER3, DISP_CAUCHY = 0, 1, 2
 BAND_GAUSS_WAVELENGTH, BAND_GAUSS_ENERGY = 0, 1
@@ -104,6 +105,20 @@ class Environment(C.Structure):
     ]
 
 
+class Tool(C.Structure):
+    """ix_tool: a concave tool volume (ToolPrimitive, geometry/tool.rs:112), 80 bytes."""
+
+    _fields_ = [
+        ("kind", C.c_uint32),
+        ("sweep_kind", C.c_uint32),
+        ("pad", C.c_uint32 * 2),
+        ("origin", C.c_float * 4),
+        ("axis", C.c_float * 4),
+        ("profile", C.c_float * 4),
+        ("sweep_dir", C.c_float * 4),
+    ]
+
+
 class Scene(C.Structure):
     _fields_ = [
         ("camera", Camera),
@@ -116,6 +131,8 @@ class Scene(C.Structure):
         ("material", Material),
         ("max_bounces", C.c_uint32),
         ("environment", Environment),
+        ("tools", C.POINTER(Tool)),
+        ("n_tools", C.c_uint32),
     ]
 
 
@@ -135,20 +152,6 @@ class WorkLimits(C.Structure):
         ("max_pixels", C.c_uint64),
         ("max_paths_per_call", C.c_uint64),
         ("max_spp", C.c_uint32),
-    ]
-
-
-class Tool(C.Structure):
-    """ix_tool: a concave tool volume (ToolPrimitive, geometry/tool.rs:112), 80 bytes."""
-
-    _fields_ = [
-        ("kind", C.c_uint32),
-        ("sweep_kind", C.c_uint32),
-        ("pad", C.c_uint32 * 2),
-        ("origin", C.c_float * 4),
-        ("axis", C.c_float * 4),
-        ("profile", C.c_float * 4),
-        ("sweep_dir", C.c_float * 4),
     ]
 
 

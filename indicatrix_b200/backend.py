@@ -58,6 +58,8 @@ def load_library() -> C.CDLL:
         lib.ix_set_precision.argtypes = [C.c_void_p, C.c_uint32]
         lib.ix_scene_routes_to_gpu.argtypes = [P(abi.Scene)]
         lib.ix_scene_routes_to_gpu_with_tools.argtypes = [P(abi.Scene), P(abi.Tool), C.c_uint32]
+        lib.ix_tool_validate.argtypes = [P(abi.Tool)]
+        lib.ix_tool_validate.restype = C.c_int
         lib.ix_accumulate.argtypes = [C.c_void_p, P(abi.Scene), P(abi.Tool), C.c_uint32, C.c_uint32, C.c_uint32,
                                       P(C.c_float), P(C.c_uint8)]
         lib.ix_accumulate_f64.argtypes = [C.c_void_p, P(abi.Scene), P(abi.Tool), C.c_uint32, C.c_uint32,
@@ -171,6 +173,7 @@ class FrameScene:
     max_bounces: int
     environment: abi.Environment
     facet_finishes: Optional[np.ndarray] = None
+    tools: Optional[Sequence[abi.Tool]] = None  # concave tools; tool k is facet n_planes + k
     _keep: list = field(default_factory=list, repr=False)
 
     def to_abi(self) -> abi.Scene:
@@ -189,6 +192,11 @@ class FrameScene:
         sc.material = self.material
         sc.max_bounces = int(self.max_bounces)
         sc.environment = self.environment
+        if self.tools:
+            arr = (abi.Tool * len(self.tools))(*self.tools)
+            sc.tools = C.cast(arr, C.POINTER(abi.Tool))
+            sc.n_tools = len(self.tools)
+            self._keep.append(arr)
         self._keep.append(planes)
         return sc
 
@@ -237,6 +245,16 @@ def scene_routes_to_gpu_with_tools(scene: FrameScene, tools: Sequence[abi.Tool])
     declines (this backend traces convex stones)."""
     tarr = (abi.Tool * len(tools))(*tools) if tools else None
     return bool(load_library().ix_scene_routes_to_gpu_with_tools(C.byref(scene.to_abi()), tarr, len(tools)))
+
+
+# ToolPrimitiveError (geometry/tool.rs:133) as ix_tool_validate returns it.
+TOOL_ERRORS = {0: None, 1: "NonFinite", 2: "NonPositiveRadius", 3: "AxisNotUnit", 4: "UnknownKind",
+               5: "UnknownSweep", 6: "PaddingNotZero"}
+
+
+def tool_validate(tool: abi.Tool) -> Optional[str]:
+    """ToolPrimitive::validate (geometry/tool.rs:360): None, or the first failed check."""
+    return TOOL_ERRORS[int(load_library().ix_tool_validate(C.byref(tool)))]
 
 
 @dataclass
@@ -371,7 +389,7 @@ class GpuBackend:
                                    tools: Sequence[abi.Tool] = ()) -> GpuAccumulate:
         """try_accumulate_geom_cancellable (backend.rs:272).  ``accum`` is float32 or
         float64 and is added into only on DONE; ``tools`` are the stone's concave tools
-        (a stone with any is declined: this backend traces convex stones)."""
+        (tool k is facet n_planes + k; when empty, the scene's own ``tools`` apply)."""
         self._check_accum(scene, accum)
         if not self._h:
             return GpuAccumulate.DECLINED

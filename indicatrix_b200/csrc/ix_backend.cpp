@@ -90,7 +90,7 @@ int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uin
     ix::TraceLaunch L;
     std::memset(&L, 0, sizeof(L));
     L.scene = sc;
-    L.flags = ix::scene_flags(sc.material);
+    L.flags = ix::scene_flags(sc);
     L.pixels_per_task = pixels_per_task(spp);
     L.task_counter = b->d_counter;
     L.dropped = b->d_dropped;
@@ -149,7 +149,7 @@ int enqueue_frame(ix_backend* b, const ix_scene& sc, uint32_t sample_offset, uin
 // Kernels one trace launch of a scene's single-scene variant takes: the trace kernel, and
 // for the path-pool shapes the rounding of its fixed-point sums.
 uint32_t kernels_per_launch(const ix_backend* b, const ix_scene& sc) {
-    return ix::shape_is_pool(ix::variant_shape((int)frame_variant(b, ix::scene_flags(sc.material)))) ? 2u : 1u;
+    return ix::shape_is_pool(ix::variant_shape((int)frame_variant(b, ix::scene_flags(sc)))) ? 2u : 1u;
 }
 
 // Points a device copy of host scene `sc` at the backend's copy of its facet finishes
@@ -165,6 +165,20 @@ bool upload_finishes(ix_backend* b, ix_scene& sc, cudaStream_t st) {
              "finishes upload"))
         return false;
     sc.facet_finishes = b->d_finishes;
+    return true;
+}
+// ... and at the backend's copy of its concave tools (none: a convex stone).
+bool upload_tools(ix_backend* b, ix_scene& sc, cudaStream_t st) {
+    if (!sc.tools || sc.n_tools == 0) {
+        sc.tools = nullptr;
+        sc.n_tools = 0;
+        return true;
+    }
+    if (fail(b, grow_device(&b->d_tools, &b->tools_cap, (size_t)sc.n_tools), "tools alloc") ||
+        fail(b, cudaMemcpyAsync(b->d_tools, sc.tools, sc.n_tools * sizeof(ix_tool), cudaMemcpyHostToDevice, st),
+             "tools upload"))
+        return false;
+    sc.tools = b->d_tools;
     return true;
 }
 
@@ -196,7 +210,7 @@ int accumulate_impl(ix_backend* b, const ix_scene* scene, uint32_t sample_offset
         return IX_DECLINED;
     ix_scene sc = *scene;
     sc.planes = b->d_planes;
-    if (!upload_finishes(b, sc, b->stream)) return IX_DECLINED;
+    if (!upload_finishes(b, sc, b->stream) || !upload_tools(b, sc, b->stream)) return IX_DECLINED;
     bool cancelled = false;
     if (fail(b, cudaEventRecord(b->ev0, b->stream), "event")) return IX_DECLINED;
     int launches = enqueue_frame(b, sc, sample_offset, spp, b->d_sums, 0, b->stream, cancel, &cancelled);
@@ -480,6 +494,7 @@ void ix_backend_destroy(ix_backend* b) {
     cudaFree(b->d_attr_map);
     cudaFree(b->d_batch_out);
     cudaFree(b->d_finishes);
+    cudaFree(b->d_tools);
     cudaFree(b->d_acc);
     display_state_free(b->display);
     radiance_state_free(b->radiance);
@@ -524,24 +539,74 @@ int ix_scene_routes_to_gpu(const ix_scene* s) {
     // isotropic material carrying one (the reference's eigen-polarisation mean of the
     // isotropic absorption branch over a biaxial indicatrix) is not built.
     if (m.biaxial && !m.anisotropic) return 0;
+    // Concave tools (tool_routing.rs:81): at most IX_MAX_TOOLS, each one valid.
+    if (s->n_tools > IX_MAX_TOOLS || (s->n_tools && !s->tools)) return 0;
+    for (uint32_t k = 0; k < s->n_tools; ++k)
+        if (ix_tool_validate(&s->tools[k]) != IX_TOOL_OK) return 0;
     return 1;
 }
 
+int ix_tool_validate(const ix_tool* t) {
+    // ToolPrimitive::validate (geometry/tool.rs:360), its checks in its order.
+    if (!t) return IX_TOOL_NON_FINITE;
+    for (int i = 0; i < 4; ++i)
+        if (!std::isfinite(t->origin[i]) || !std::isfinite(t->axis[i]) || !std::isfinite(t->profile[i]) ||
+            !std::isfinite(t->sweep_dir[i]))
+            return IX_TOOL_NON_FINITE;
+    if (t->kind > 3u) return IX_TOOL_UNKNOWN_KIND;
+    if (t->sweep_kind > 2u) return IX_TOOL_UNKNOWN_SWEEP;
+    if (t->pad[0] || t->pad[1] || t->profile[3] != 0.0f || t->sweep_dir[3] != 0.0f) return IX_TOOL_PADDING_NOT_ZERO;
+    const float radii[3] = {t->origin[3], t->profile[0], t->profile[1]};
+    const float hl = t->axis[3], stroke = t->profile[2];
+    bool neg = false, all_nonpos = true;
+    for (float r : radii) {
+        neg = neg || r < 0.0f;
+        all_nonpos = all_nonpos && r <= 0.0f;
+    }
+    const bool ball = t->kind == 0u;
+    if (neg || all_nonpos || hl < 0.0f || (!ball && hl <= 0.0f) || (ball && hl != 0.0f) || stroke < 0.0f)
+        return IX_TOOL_NON_POSITIVE_RADIUS;
+    // Vec3::length: the square root of the left-to-right dot product, in f32.
+    auto length = [](const float* v) {
+        const float d = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
+        return std::sqrt(d);
+    };
+    if (std::fabs(length(t->axis) - 1.0f) > 1e-4f) return IX_TOOL_AXIS_NOT_UNIT;
+    if (t->sweep_kind == 2u) {
+        const float dd = (t->sweep_dir[0] * t->axis[0] + t->sweep_dir[1] * t->axis[1]) + t->sweep_dir[2] * t->axis[2];
+        if (std::fabs(length(t->sweep_dir) - 1.0f) > 1e-4f || std::fabs(dd) > 1e-4f) return IX_TOOL_AXIS_NOT_UNIT;
+    }
+    return IX_TOOL_OK;
+}
+
+// The scene with the call's tools when it passes any (ntools > 0), else the scene's own.
+static ix_scene with_tools(const ix_scene* scene, const ix_tool* tools, uint32_t ntools) {
+    ix_scene s = *scene;
+    if (ntools) {
+        s.tools = tools;
+        s.n_tools = ntools;
+    }
+    return s;
+}
+
 int ix_scene_routes_to_gpu_with_tools(const ix_scene* scene, const ix_tool* tools, uint32_t ntools) {
-    (void)tools;
-    return ntools == 0 ? ix_scene_routes_to_gpu(scene) : 0;
+    if (!scene) return 0;
+    const ix_scene s = with_tools(scene, tools, ntools);
+    return ix_scene_routes_to_gpu(&s);
 }
 
 int ix_accumulate(ix_backend* b, const ix_scene* scene, const ix_tool* tools, uint32_t ntools,
                   uint32_t sample_offset, uint32_t spp, float* accum_xyz, const volatile uint8_t* cancel) {
     if (!ix_scene_routes_to_gpu_with_tools(scene, tools, ntools)) return IX_DECLINED;
-    return accumulate_impl<float>(b, scene, sample_offset, spp, accum_xyz, cancel);
+    const ix_scene s = with_tools(scene, tools, ntools);
+    return accumulate_impl<float>(b, &s, sample_offset, spp, accum_xyz, cancel);
 }
 
 int ix_accumulate_f64(ix_backend* b, const ix_scene* scene, const ix_tool* tools, uint32_t ntools,
                       uint32_t sample_offset, uint32_t spp, double* accum_xyz, const volatile uint8_t* cancel) {
     if (!ix_scene_routes_to_gpu_with_tools(scene, tools, ntools)) return IX_DECLINED;
-    return accumulate_impl<double>(b, scene, sample_offset, spp, accum_xyz, cancel);
+    const ix_scene s = with_tools(scene, tools, ntools);
+    return accumulate_impl<double>(b, &s, sample_offset, spp, accum_xyz, cancel);
 }
 
 int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metrics_lighting* lighting,
@@ -590,7 +655,7 @@ int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metr
         return IX_DECLINED;
     ix_scene sc = *scene;
     sc.planes = b->d_planes;
-    if (!upload_finishes(b, sc, b->stream)) return IX_DECLINED;
+    if (!upload_finishes(b, sc, b->stream) || !upload_tools(b, sc, b->stream)) return IX_DECLINED;
     A.cls = b->d_attr_cls;
     A.y = b->d_attr_y;
     bool cancelled = false;
@@ -671,6 +736,7 @@ struct ix_batch_plan {
     cudaStream_t wf_stream = nullptr;
     uint32_t wf_iterations = 0;  // of the last wavefront run
     uint8_t* d_finishes = nullptr;  // every scene's facet finishes, back to back
+    ix_tool* d_tools = nullptr;     // every scene's concave tools, back to back
 };
 
 namespace {
@@ -931,18 +997,31 @@ static ix_batch_plan* plan_create_locked(ix_backend* b, const ix_scene* scenes, 
             finishes.insert(finishes.end(), scenes[i].facet_finishes,
                             scenes[i].facet_finishes + scenes[i].n_finishes);
         }
+    std::vector<ix_tool> tools;
+    std::vector<size_t> tool_off(n_scenes, 0);
+    for (uint32_t i = 0; i < n_scenes; ++i)
+        if (scenes[i].tools && scenes[i].n_tools) {
+            tool_off[i] = tools.size();
+            tools.insert(tools.end(), scenes[i].tools, scenes[i].tools + scenes[i].n_tools);
+        }
     uint64_t off = 0;
     bool ok = cudaMalloc((void**)&p->d_planes, planes.size() * sizeof(float)) == cudaSuccess;
     ok = ok && (finishes.empty() || (cudaMalloc((void**)&p->d_finishes, finishes.size()) == cudaSuccess &&
                                      cudaMemcpy(p->d_finishes, finishes.data(), finishes.size(),
                                                 cudaMemcpyHostToDevice) == cudaSuccess));
+    ok = ok && (tools.empty() || (cudaMalloc((void**)&p->d_tools, tools.size() * sizeof(ix_tool)) == cudaSuccess &&
+                                  cudaMemcpy(p->d_tools, tools.data(), tools.size() * sizeof(ix_tool),
+                                             cudaMemcpyHostToDevice) == cudaSuccess));
     for (uint32_t i = 0; ok && i < n_scenes; ++i) {
         std::memcpy(planes.data() + off, scenes[i].planes, (size_t)scenes[i].n_planes * 16);
         dev_scenes[i].planes = p->d_planes + off;
         const bool has_finishes = scenes[i].facet_finishes && scenes[i].n_finishes;
         dev_scenes[i].facet_finishes = has_finishes ? p->d_finishes + finish_off[i] : nullptr;
         dev_scenes[i].n_finishes = has_finishes ? scenes[i].n_finishes : 0;
-        flags[i] = ix::scene_flags(scenes[i].material);
+        const bool has_tools = scenes[i].tools && scenes[i].n_tools;
+        dev_scenes[i].tools = has_tools ? p->d_tools + tool_off[i] : nullptr;
+        dev_scenes[i].n_tools = has_tools ? scenes[i].n_tools : 0;
+        flags[i] = ix::scene_flags(dev_scenes[i]);
         p->h_max_bounces.push_back(scenes[i].max_bounces);
         p->uniaxial = std::max(p->uniaxial, (uint32_t)ix::transport_class(flags[i]));
         off += (uint64_t)scenes[i].n_planes * 4;
@@ -1098,6 +1177,7 @@ void ix_batch_plan_destroy(ix_batch_plan* p) {
     cudaFree(p->d_jobs);
     cudaFree(p->d_planes);
     cudaFree(p->d_finishes);
+    cudaFree(p->d_tools);
     if (!p->out_pooled) cudaFree(p->d_out);
     cudaFree(p->d_acc);
     cudaFree(p->d_counter);
@@ -1536,8 +1616,8 @@ int ix_debug_check(ix_backend* b, const ix_scene* scene, int32_t fn, uint32_t n,
     std::memset(&L, 0, sizeof(L));
     L.scene = *scene;
     L.scene.planes = b->d_planes;
-    if (!upload_finishes(b, L.scene, b->stream)) return -1;
-    L.flags = ix::scene_flags(scene->material);
+    if (!upload_finishes(b, L.scene, b->stream) || !upload_tools(b, L.scene, b->stream)) return -1;
+    L.flags = ix::scene_flags(*scene);
     L.fn = fn;
     L.n = n;
     L.in_stride = in_stride;

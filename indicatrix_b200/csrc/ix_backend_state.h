@@ -54,6 +54,8 @@ struct ix_backend {
     // A host scene's per-facet finishes, copied for the kernels.
     uint8_t* d_finishes = nullptr;
     size_t finishes_cap = 0;
+    ix_tool* d_tools = nullptr;  // the call's concave tools
+    size_t tools_cap = 0;
     // Fixed-point per-pixel sums of the path-pool kernels (FIXED_WORDS per pixel of a launch).
     unsigned long long* d_acc = nullptr;
     size_t acc_cap = 0;

@@ -608,7 +608,7 @@ cudaError_t IX_SFX(launch_trace)(const TraceLaunch& l, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     switch (transport_class(l.flags)) {
-        case TRANSPORT_BIAXIAL: start_task_loop(TaskLoop<TRANSPORT_BIAXIAL>::trace(variant_budget(l.variant)), l, stream); break;
+        case TRANSPORT_EXTENDED: start_task_loop(TaskLoop<TRANSPORT_EXTENDED>::trace(variant_budget(l.variant)), l, stream); break;
         case TRANSPORT_UNIAXIAL: start_task_loop(TaskLoop<TRANSPORT_UNIAXIAL>::trace(variant_budget(l.variant)), l, stream); break;
         default: start_task_loop(TaskLoop<TRANSPORT_ISOTROPIC>::trace(variant_budget(l.variant)), l, stream); break;
     }
@@ -627,8 +627,8 @@ cudaError_t IX_SFX(launch_trace_attributed)(const TraceLaunch& l, const AttrLaun
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     switch (transport_class(l.flags)) {
-        case TRANSPORT_BIAXIAL:
-            IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, TRANSPORT_BIAXIAL><<<l.blocks, l.threads, 0, stream>>>(l, a);
+        case TRANSPORT_EXTENDED:
+            IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, TRANSPORT_EXTENDED><<<l.blocks, l.threads, 0, stream>>>(l, a);
             break;
         case TRANSPORT_UNIAXIAL:
             IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, TRANSPORT_UNIAXIAL><<<l.blocks, l.threads, 0, stream>>>(l, a);
@@ -656,7 +656,7 @@ cudaError_t IX_SFX(launch_batch)(const BatchLaunch& l, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(l.task_counter, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     switch (l.uniaxial) {
-        case TRANSPORT_BIAXIAL: start_task_loop(TaskLoop<TRANSPORT_BIAXIAL>::batch(variant_budget(l.variant)), l, stream); break;
+        case TRANSPORT_EXTENDED: start_task_loop(TaskLoop<TRANSPORT_EXTENDED>::batch(variant_budget(l.variant)), l, stream); break;
         case TRANSPORT_UNIAXIAL: start_task_loop(TaskLoop<TRANSPORT_UNIAXIAL>::batch(variant_budget(l.variant)), l, stream); break;
         default: start_task_loop(TaskLoop<TRANSPORT_ISOTROPIC>::batch(variant_budget(l.variant)), l, stream); break;
     }
@@ -670,7 +670,7 @@ cudaError_t IX_SFX(launch_check)(const CheckLaunch& l, cudaStream_t stream) {
     if (l.fn == CHECK_TRACE || l.fn == CHECK_TRACE_RAY) {
         const int blocks = (int)((l.n * 8ull + threads - 1) / threads);
         switch (transport_class(l.flags)) {
-            case TRANSPORT_BIAXIAL: IX_SFX(check_trace_kernel)<TRANSPORT_BIAXIAL><<<blocks, threads, 0, stream>>>(l); break;
+            case TRANSPORT_EXTENDED: IX_SFX(check_trace_kernel)<TRANSPORT_EXTENDED><<<blocks, threads, 0, stream>>>(l); break;
             case TRANSPORT_UNIAXIAL: IX_SFX(check_trace_kernel)<TRANSPORT_UNIAXIAL><<<blocks, threads, 0, stream>>>(l); break;
             default: IX_SFX(check_trace_kernel)<TRANSPORT_ISOTROPIC><<<blocks, threads, 0, stream>>>(l); break;
         }
@@ -695,7 +695,7 @@ int IX_SFX(trace_blocks_per_sm)(int threads, int variant, int uniaxial, size_t* 
     if (threads != 128) return 0;
     const int budget = variant_budget(variant);
     switch (uniaxial) {
-        case TRANSPORT_BIAXIAL: return occupancy(TaskLoop<TRANSPORT_BIAXIAL>::trace(budget), threads);
+        case TRANSPORT_EXTENDED: return occupancy(TaskLoop<TRANSPORT_EXTENDED>::trace(budget), threads);
         case TRANSPORT_UNIAXIAL: return occupancy(TaskLoop<TRANSPORT_UNIAXIAL>::trace(budget), threads);
         default: return occupancy(TaskLoop<TRANSPORT_ISOTROPIC>::trace(budget), threads);
     }
@@ -703,7 +703,7 @@ int IX_SFX(trace_blocks_per_sm)(int threads, int variant, int uniaxial, size_t* 
 
 int IX_SFX(trace_attributed_blocks_per_sm)(int threads, int uniaxial) {
     switch (uniaxial) {
-        case TRANSPORT_BIAXIAL: return occupancy(IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, TRANSPORT_BIAXIAL>, threads);
+        case TRANSPORT_EXTENDED: return occupancy(IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, TRANSPORT_EXTENDED>, threads);
         case TRANSPORT_UNIAXIAL:
             return occupancy(IX_SFX(trace_attributed_kernel)<ATTR_MINB_UNI, TRANSPORT_UNIAXIAL>, threads);
         default: return occupancy(IX_SFX(trace_attributed_kernel)<ATTR_MINB_ISO, TRANSPORT_ISOTROPIC>, threads);
@@ -716,7 +716,7 @@ int IX_SFX(batch_blocks_per_sm)(int threads, int variant, int uniaxial) {
     if (threads != 128) return 0;
     const int budget = variant_budget(variant);
     switch (uniaxial) {
-        case TRANSPORT_BIAXIAL: return occupancy(TaskLoop<TRANSPORT_BIAXIAL>::batch(budget), threads);
+        case TRANSPORT_EXTENDED: return occupancy(TaskLoop<TRANSPORT_EXTENDED>::batch(budget), threads);
         case TRANSPORT_UNIAXIAL: return occupancy(TaskLoop<TRANSPORT_UNIAXIAL>::batch(budget), threads);
         default: return occupancy(TaskLoop<TRANSPORT_ISOTROPIC>::batch(budget), threads);
     }

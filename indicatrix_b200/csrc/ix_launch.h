@@ -19,6 +19,7 @@ enum : uint32_t {
     SCENE_SCATTERING = 8u,  // Henyey-Greenstein interior scattering (scattering_sigma_s > 0)
     SCENE_ROUNDED = 16u,    // rounded facet edges (edge_rounding_radius > 0)
     SCENE_BIAXIAL = 32u,    // biaxial indicatrix (ix_material::biaxial, with anisotropic)
+    SCENE_CONCAVE = 64u,    // concave tools carved out of the stone (ix_scene::n_tools > 0)
 };
 inline bool absorption_present(const ix_absorption& a) {
     if (a.has_spline) return true;
@@ -52,15 +53,21 @@ inline uint32_t scene_flags(const ix_material& m) {
 // The isotropic megakernel assumes equal o/e absorption and no birefringence; any other
 // scene runs the uniaxial instantiation of the transport.
 inline bool needs_uniaxial_kernel(uint32_t flags) {
-    return (flags & (SCENE_UNIAXIAL | SCENE_PLEOCHROIC | SCENE_SCATTERING | SCENE_ROUNDED | SCENE_BIAXIAL)) != 0;
+    return (flags & (SCENE_UNIAXIAL | SCENE_PLEOCHROIC | SCENE_SCATTERING | SCENE_ROUNDED | SCENE_BIAXIAL |
+                     SCENE_CONCAVE)) != 0;
+}
+// The scene's flags: its material's, and whether tools carve it.
+inline uint32_t scene_flags(const ix_scene& s) {
+    return scene_flags(s.material) | (s.n_tools ? SCENE_CONCAVE : 0u);
 }
 // The transport instantiation a scene needs: the isotropic megakernel, the uniaxial one,
-// or the uniaxial one with the biaxial bounce (which serves uniaxial and isotropic scenes
-// too, so a batch takes the largest of its scenes' classes).
-enum TransportClass : int { TRANSPORT_ISOTROPIC = 0, TRANSPORT_UNIAXIAL = 1, TRANSPORT_BIAXIAL = 2 };
+// or the extended one -- the uniaxial bounce plus the out-of-line biaxial bounce and the
+// carved-stone intersection -- which serves every scene, so a batch takes the largest of
+// its scenes' classes.
+enum TransportClass : int { TRANSPORT_ISOTROPIC = 0, TRANSPORT_UNIAXIAL = 1, TRANSPORT_EXTENDED = 2 };
 constexpr int N_TRANSPORT_CLASSES = 3;
 inline int transport_class(uint32_t flags) {
-    if (flags & SCENE_BIAXIAL) return TRANSPORT_BIAXIAL;
+    if (flags & (SCENE_BIAXIAL | SCENE_CONCAVE)) return TRANSPORT_EXTENDED;
     return needs_uniaxial_kernel(flags) ? TRANSPORT_UNIAXIAL : TRANSPORT_ISOTROPIC;
 }
 
@@ -95,7 +102,7 @@ constexpr float FIXED_MAX_VALUE = 4.611686018427387904e18f;  // 2^62: larger sam
 // One frame-tracing launch over the pixels [pixel_begin, pixel_begin + n_pixels).
 struct TraceLaunch {
     ix_scene scene;            // `planes` is a device pointer here
-    uint32_t flags;            // scene_flags(scene.material)
+    uint32_t flags;            // scene_flags(scene)
     uint32_t pixel_begin;
     uint32_t n_pixels;
     uint32_t sample_offset;
@@ -222,7 +229,7 @@ enum CheckFn {
 
 struct CheckLaunch {
     ix_scene scene;    // device planes
-    uint32_t flags;    // scene_flags(scene.material)
+    uint32_t flags;    // scene_flags(scene)
     int fn;
     uint32_t n;
     uint32_t in_stride;   // 32-bit words per input row

@@ -99,7 +99,7 @@ extern "C" int ix_accumulate_device_noalloc(const ix_scene* scene, uint32_t samp
     ix::TraceLaunch L;
     std::memset(&L, 0, sizeof(L));
     L.scene = *scene;  // planes and facet finishes in device memory, as ix_accumulate_device
-    L.flags = ix::scene_flags(scene->material);
+    L.flags = ix::scene_flags(*scene);
     L.sample_offset = sample_offset;
     L.spp = spp;
     uint32_t ppt = 256u / spp;

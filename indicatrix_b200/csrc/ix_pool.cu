@@ -311,7 +311,7 @@ void* pick(bool batch, int variant) {
 void* pick_kernel(bool batch, int variant, int transport) {
     if (variant < 0 || variant >= N_VARIANTS) return nullptr;
     switch (transport) {
-        case TRANSPORT_BIAXIAL: return pick<TRANSPORT_BIAXIAL>(batch, variant);
+        case TRANSPORT_EXTENDED: return pick<TRANSPORT_EXTENDED>(batch, variant);
         case TRANSPORT_UNIAXIAL: return pick<TRANSPORT_UNIAXIAL>(batch, variant);
         default: return pick<TRANSPORT_ISOTROPIC>(batch, variant);
     }

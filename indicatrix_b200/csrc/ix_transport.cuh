@@ -19,6 +19,7 @@
 #include "ix_launch.h"
 #include "ix_uniaxial.cuh"
 #include "ix_biaxial.cuh"
+#include "ix_tools.cuh"
 
 namespace ix {
 
@@ -36,12 +37,13 @@ struct DevScene {
     uint32_t aniso;       // uniaxial birefringence
     uint32_t scattering;  // Henyey-Greenstein interior scattering (uniaxial instantiation)
     uint32_t rounded;     // rounded facet edges (uniaxial instantiation)
-    uint32_t biaxial;     // biaxial indicatrix (uniaxial instantiation)
+    uint32_t biaxial;     // biaxial indicatrix (extended instantiation)
+    uint32_t concave;     // concave tools carve the stone (extended instantiation)
 };
 IX_DEV DevScene make_scene(const ix_scene& s, uint32_t flags) {
     return DevScene{s, (flags & SCENE_ABSORBING) ? 1u : 0u, (flags & SCENE_UNIAXIAL) ? 1u : 0u,
                     (flags & SCENE_SCATTERING) ? 1u : 0u, (flags & SCENE_ROUNDED) ? 1u : 0u,
-                    (flags & SCENE_BIAXIAL) ? 1u : 0u};
+                    (flags & SCENE_BIAXIAL) ? 1u : 0u, (flags & SCENE_CONCAVE) ? 1u : 0u};
 }
 
 // The 8 lanes of one path: `mask` selects them in the warp, `c` is this lane's channel.
@@ -101,7 +103,14 @@ struct LanePath {
 //    that half-space for good, the scan's t_far ends at most at this plane's negative t,
 //    and it reports a miss -- returned at once, as for a parallel plane outside.
 // ------------------------------------------------------------------------------------
-IX_DEV Hit group_intersect(const Group& g, const float4* __restrict__ planes, int n, V3 o, V3 d) {
+// The scan itself: the entering planes' largest t and the first plane attaining it, the
+// exiting planes' smallest t and its plane; false when the ray misses at once (a parallel
+// plane or a receding plane the origin is outside of).
+struct Slab {
+    float t_near, t_far;
+    int near_idx, far_idx;
+};
+IX_DEV bool group_slab(const Group& g, const float4* __restrict__ planes, int n, V3 o, V3 d, Slab& out) {
     float t_near = -1e30f, t_far = 1e30f;
     int near_idx = -1, far_idx = -1;
     int outside = 0;
@@ -152,18 +161,142 @@ IX_DEV Hit group_intersect(const Group& g, const float4* __restrict__ planes, in
             far_idx = fi;
         }
     }
+    out.t_near = t_near;
+    out.t_far = t_far;
+    out.near_idx = near_idx;
+    out.far_idx = far_idx;
+    return !outside;
+}
+IX_DEV Hit group_intersect(const Group& g, const float4* __restrict__ planes, int n, V3 o, V3 d) {
     Hit h;
     h.facet = -1;
     h.t = 0.0f;
-    if (outside || t_near > t_far) return h;
-    if (t_near > 1e-4f) {
-        h.t = t_near;
-        h.facet = near_idx >= 0 ? near_idx : 0;
-    } else if (t_far > 1e-4f) {
-        h.t = t_far;
-        h.facet = far_idx >= 0 ? far_idx : 0;
+    Slab s;
+    if (!group_slab(g, planes, n, o, d, s) || s.t_near > s.t_far) return h;
+    if (s.t_near > 1e-4f) {
+        h.t = s.t_near;
+        h.facet = s.near_idx >= 0 ? s.near_idx : 0;
+    } else if (s.t_far > 1e-4f) {
+        h.t = s.t_far;
+        h.facet = s.far_idx >= 0 ? s.far_idx : 0;
     }
     return h;
+}
+
+// ------------------------------------------------------------------------------------
+// A stone carved by concave tools (intersect_stone.rs:62-170, carve): the slab and every
+// tool's interval are boundary events; walked in (t, event) order -- f32::total_cmp, then
+// slab entry, slab exit, tool k's entry, tool k's exit -- the ray is in the material while
+// it is inside the slab and inside no tool, and the hit is the first change of that state
+// past the 1e-4 restart epsilon.  Lane c takes tools c, c + 8, ...; each step of the walk
+// is the group's smallest event past the previous one.  Out of line and by value: only
+// the extended instantiation calls it, and only for a carved stone.
+// ------------------------------------------------------------------------------------
+struct CarvedHit {
+    float t;
+    int facet;  // -1: a miss; tool k is facet n_planes + k
+    V3 normal;  // the boundary's outward normal (a tool's points into the cavity)
+    int entering;
+};
+// The event's 64-bit sort key: total_cmp's order of t (its bits, negatives' magnitude
+// bits flipped, as an unsigned offset) above the event id.
+IX_DEV unsigned long long event_key(float t, uint32_t id) {
+    const int32_t b = __float_as_int(t);
+    const uint32_t ord = (uint32_t)(b ^ (int32_t)(((uint32_t)(b >> 31)) >> 1)) ^ 0x80000000u;
+    return ((unsigned long long)ord << 32) | id;
+}
+IX_DEV float event_t(unsigned long long key) {
+    const int32_t ord = (int32_t)((uint32_t)(key >> 32) ^ 0x80000000u);
+    return __int_as_float(ord ^ (int32_t)(((uint32_t)(ord >> 31)) >> 1));
+}
+static __device__ __noinline__ CarvedHit group_carved_hit(Group g, const float4* __restrict__ planes, int n_planes,
+                                                          const ix_tool* __restrict__ tools, int n_tools, V3 o,
+                                                          V3 d) {
+    constexpr int PER_LANE = IX_MAX_TOOLS / 8;
+    CarvedHit out{0.0f, -1, v3(0.0f, 0.0f, 0.0f), 0};
+    Slab s;
+    if (!group_slab(g, planes, n_planes, o, d, s) || s.t_near > s.t_far) return out;
+    float lo[PER_LANE], hi[PER_LANE];
+    uint32_t valid = 0;
+#pragma unroll 1
+    for (int i = 0; i < PER_LANE; ++i) {
+        const int k = g.c + 8 * i;
+        if (k < n_tools && tool_ray_interval(tools[k], o, d, lo[i], hi[i])) valid |= 1u << i;
+    }
+    unsigned long long prev = 0ull;
+    bool first = true;
+    int plane_depth = 0, tool_depth = 0;
+    bool inside = false;
+#pragma unroll 1
+    for (int step = 0; step < 2 + 2 * IX_MAX_TOOLS; ++step) {
+        unsigned long long best = ~0ull;
+        auto consider = [&](float t, uint32_t id) {
+            const unsigned long long e = event_key(t, id);
+            if ((first || e > prev) && e < best) best = e;
+        };
+        if (g.c == 0) {
+            consider(s.t_near, 0u);
+            consider(s.t_far, 1u);
+        }
+#pragma unroll 1
+        for (int i = 0; i < PER_LANE; ++i)
+            if ((valid >> i) & 1u) {
+                const uint32_t k = (uint32_t)(g.c + 8 * i);
+                consider(lo[i], 2u + 2u * k);
+                consider(hi[i], 3u + 2u * k);
+            }
+#pragma unroll
+        for (int m = 4; m > 0; m >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(g.mask, best, m, 8);
+            best = other < best ? other : best;
+        }
+        if (best == ~0ull) break;
+        prev = best;
+        first = false;
+        const uint32_t id = (uint32_t)(best & 0xFFFFFFFFull);
+        const float t = event_t(best);
+        if (id == 0u)
+            ++plane_depth;
+        else if (id == 1u)
+            --plane_depth;
+        else if ((id & 1u) == 0u)
+            ++tool_depth;
+        else
+            --tool_depth;
+        const bool now_inside = plane_depth > 0 && tool_depth <= 0;
+        if (now_inside == inside) continue;
+        inside = now_inside;
+        if (t <= 1e-4f) continue;
+        out.t = t;
+        out.entering = now_inside ? 1 : 0;
+        if (id <= 1u) {
+            const int idx = id == 0u ? s.near_idx : s.far_idx;
+            out.facet = idx >= 0 ? idx : 0;
+            out.normal = idx >= 0 ? v3(planes[idx].x, planes[idx].y, planes[idx].z) : v3(0.0f, 0.0f, 0.0f);
+        } else {
+            const int ti = (int)((id - 2u) >> 1);
+            out.facet = n_planes + ti;
+            out.normal = vneg_(tool_outward_normal(tools[ti], vadd_(o, vmul_(d, t))));
+        }
+        return out;
+    }
+    return out;
+}
+// shading_normal_for_hit's carved arm (transport/inner.rs:54): a tool facet keeps its
+// normal, and a plane facet rounds its edges only where no tool lies within the rounding
+// radius along the facet's frosted basis.
+static __device__ __noinline__ int carved_near_tool(V3 hit_point, V3 normal, float radius,
+                                                    const ix_tool* __restrict__ tools, int n_tools) {
+    const V3 u = stable_basis_t_(normal), v = cross_(normal, u);
+    const V3 dirs[4] = {u, vneg_(u), v, vneg_(v)};
+#pragma unroll 1
+    for (int j = 0; j < 4; ++j) {
+        const V3 probe = vadd_(hit_point, vmul_(dirs[j], radius));
+#pragma unroll 1
+        for (int k = 0; k < n_tools; ++k)
+            if (tool_contains(tools[k], probe)) return 1;
+    }
+    return 0;
 }
 
 // The exit-split probes' copy of the scan, out of line (probes are rare next to bounces).
@@ -246,7 +379,7 @@ IX_DEV void group_init_ray(const Group& g, LanePath& P, const DevScene& S, Ray r
         P.n_e = S.aniso ? extraordinary_index_at(sc.material, P.lambda, P.n) : P.n;
         P.n_e_hero = gshfl(g, P.n_e, 0);
         P.alpha_e = S.absorbing ? spectral_absorption(sc.material.abs_e, P.lambda) : 0.0f;
-        if constexpr (UNI == TRANSPORT_BIAXIAL) {
+        if constexpr (UNI == TRANSPORT_EXTENDED) {
             if (S.biaxial)  // the beta-ray alpha; the alpha ray's without beta bands (wavelength_cache.rs:37-52)
                 P.n_e = (S.absorbing && sc.material.has_abs_beta) ? spectral_absorption(sc.material.abs_beta, P.lambda)
                                                                   : P.alpha;
@@ -363,6 +496,24 @@ IX_DEV void group_exit_probes(const Group& g, LanePath& P, const DevScene& S, co
         probes &= probes - 1;
         const V3 dj = v3(gshfl(g, dir_k.x, j), gshfl(g, dir_k.y, j), gshfl(g, dir_k.z, j));
         const Hit ph = probe_intersect(g, planes, (int)S.s.n_planes, hit_point + dj * 1e-4f, dj);
+        if (ph.facet < 0 && g.c == j) {
+            const float e = lane_environment(S.s.environment, dj, P.observer, P.lambda);
+            P.split = fmaf(fmaxf(t_intensity, 0.0f), e, P.split);
+        }
+    }
+}
+
+// The exit probes of a carved stone: no shortcut (a probe may meet the stone again across
+// a cavity), each probe through the carved intersection (exit_split.rs:140).
+IX_DEV void group_exit_probes_carved(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes,
+                                     V3 hit_point, bool want_probe, V3 dir_k, float t_intensity) {
+    unsigned probes = (__ballot_sync(g.mask, want_probe) >> (threadIdx.x & 24u)) & 0xFFu;
+    while (probes) {
+        const int j = __ffs(probes) - 1;
+        probes &= probes - 1;
+        const V3 dj = v3(gshfl(g, dir_k.x, j), gshfl(g, dir_k.y, j), gshfl(g, dir_k.z, j));
+        const CarvedHit ph = group_carved_hit(g, planes, (int)S.s.n_planes, S.s.tools, (int)S.s.n_tools,
+                                              hit_point + dj * 1e-4f, dj);
         if (ph.facet < 0 && g.c == j) {
             const float e = lane_environment(S.s.environment, dj, P.observer, P.lambda);
             P.split = fmaf(fmaxf(t_intensity, 0.0f), e, P.split);
@@ -772,12 +923,72 @@ IX_DEV int group_bounce(const Group& g, LanePath& P, const DevScene& S,
 // reflect probability and the eigenmode draw; every lane solves its own channel.
 // The path carries the wave normal `k` beside the (walked-off) ray direction `d`.
 // ------------------------------------------------------------------------------------
+// A carved stone's hit (extended instantiation): the intersection's own normal, and the
+// medium the ray is in taken from the intersection (bounce_body.rs:391-397: the 1e-4
+// restart may have stepped over a second boundary, a tool's rim on a facet).
+struct BounceHit {
+    Hit hit;
+    V3 normal;  // carved only
+    int carved;
+};
+template <int UNI>
+IX_DEV BounceHit bounce_next_hit(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes) {
+    BounceHit b;
+    b.carved = 0;
+    if constexpr (UNI == TRANSPORT_EXTENDED) {
+        if (S.concave) {
+            const CarvedHit ch = group_carved_hit(g, planes, (int)S.s.n_planes, S.s.tools, (int)S.s.n_tools, P.o, P.d);
+            b.hit.t = ch.t;
+            b.hit.facet = ch.facet;
+            b.normal = ch.normal;
+            b.carved = 1;
+            if (ch.facet >= 0) P.inside = ch.entering == 0;
+            return b;
+        }
+    }
+    b.hit = group_next_hit(g, P, planes, (int)S.s.n_planes);
+    return b;
+}
+// The geometric normal at the hit: the carved intersection's, else the facet plane's.
+IX_DEV V3 bounce_hit_normal(const BounceHit& bh, const float4* __restrict__ planes) {
+    if (bh.carved) return bh.normal;
+    const float4 pl = planes[bh.hit.facet];
+    return v3(pl.x, pl.y, pl.z);
+}
+// The shading normal at a hit: rounded edges (shading_normal_near_edge), on a carved
+// stone only away from its tools.
+template <int UNI>
+IX_DEV V3 bounce_shading_normal(const Group& g, const DevScene& S, const float4* __restrict__ planes,
+                                const BounceHit& bh, V3 hit_point, V3 normal) {
+    if (!S.rounded) return normal;
+    const float radius = S.s.material.edge_rounding_radius;
+    if constexpr (UNI == TRANSPORT_EXTENDED) {
+        if (bh.carved && ((uint32_t)bh.hit.facet >= S.s.n_planes ||
+                          carved_near_tool(hit_point, normal, radius, S.s.tools, (int)S.s.n_tools)))
+            return normal;
+    }
+    return group_shading_normal(g, planes, (int)S.s.n_planes, hit_point, bh.hit.facet, normal, radius);
+}
+template <int UNI>
+IX_DEV void bounce_exit_probes(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes,
+                               const BounceHit& bh, V3 hit_point, bool want_probe, V3 dir_k, float t_int) {
+    if constexpr (UNI == TRANSPORT_EXTENDED) {
+        if (bh.carved) {
+            group_exit_probes_carved(g, P, S, planes, hit_point, want_probe, dir_k, t_int);
+            return;
+        }
+    }
+    group_exit_probes(g, P, S, planes, hit_point, want_probe, dir_k, t_int);
+}
+
+template <int UNI>
 IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
                                  const float4* __restrict__ planes, float& esc) {
     const ix_scene& sc = S.s;
     const ix_material& mat = sc.material;
     const uint32_t bounce = P.bounce;
-    Hit hit = group_next_hit(g, P, planes, (int)sc.n_planes);
+    const BounceHit bh = bounce_next_hit<UNI>(g, P, S, planes);
+    const Hit hit = bh.hit;
     if (hit.facet < 0) {
         esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         return BOUNCE_ESCAPED;
@@ -823,12 +1034,8 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
         P.st = scale(P.st, r.st_factor);
     }
     P.facet = hit.facet;
-    const float4 pl = planes[hit.facet];
-    V3 normal = v3(pl.x, pl.y, pl.z);
     const V3 hit_point = P.o + hit.t * P.d;
-    if (S.rounded)
-        normal = group_shading_normal(g, planes, (int)sc.n_planes, hit_point, hit.facet, normal,
-                                      mat.edge_rounding_radius);
+    V3 normal = bounce_shading_normal<UNI>(g, S, planes, bh, hit_point, bounce_hit_normal(bh, planes));
     const V3 k_hat = P.k;
 
     // rotate_stokes_to_plane_of_incidence, about the wave normal k.
@@ -1100,7 +1307,7 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
             update = entering ? (use_e ? 1 : 0) : -1;
         }
     }
-    group_exit_probes(g, P, S, planes, hit_point, want_probe, dir_k, t_int);
+    bounce_exit_probes<UNI>(g, P, S, planes, bh, hit_point, want_probe, dir_k, t_int);
     if (narrow) group_narrow_compat(g, P, status, dir_k);
 
     const bool was_internal_reflection = inside0 && update < 0 && new_inside == inside0;
@@ -1161,7 +1368,8 @@ static __device__ __noinline__ BiaxialStep group_bounce_biaxial(Group g, LanePat
     const ix_scene& sc = S.s;
     const ix_material& mat = sc.material;
     const uint32_t bounce = P.bounce;
-    Hit hit = group_next_hit(g, P, planes, (int)sc.n_planes);
+    const BounceHit bh = bounce_next_hit<TRANSPORT_EXTENDED>(g, P, S, planes);
+    const Hit hit = bh.hit;
     if (hit.facet < 0) {
         out.esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         out.P = P;
@@ -1208,12 +1416,8 @@ static __device__ __noinline__ BiaxialStep group_bounce_biaxial(Group g, LanePat
         P.st = scale(P.st, r.st_factor);
     }
     P.facet = hit.facet;
-    const float4 pl = planes[hit.facet];
-    V3 normal = v3(pl.x, pl.y, pl.z);
     const V3 hit_point = P.o + hit.t * P.d;
-    if (S.rounded)
-        normal = group_shading_normal(g, planes, (int)sc.n_planes, hit_point, hit.facet, normal,
-                                      mat.edge_rounding_radius);
+    V3 normal = bounce_shading_normal<TRANSPORT_EXTENDED>(g, S, planes, bh, hit_point, bounce_hit_normal(bh, planes));
     const V3 k_hat = P.k;
     const V3 cpn = rotate_to_plane_of_incidence(P.st, P.has_prev, P.prev_pn, k_hat, normal);
     P.has_prev = true;
@@ -1333,7 +1537,7 @@ static __device__ __noinline__ BiaxialStep group_bounce_biaxial(Group g, LanePat
             update = entering ? (use_e ? 1 : 0) : -1;
         }
     }
-    group_exit_probes(g, P, S, planes, hit_point, want_probe, dir_k, t_int);
+    bounce_exit_probes<TRANSPORT_EXTENDED>(g, P, S, planes, bh, hit_point, want_probe, dir_k, t_int);
     if (narrow) group_narrow_compat(g, P, status, dir_k);
 
     const bool was_internal_reflection = inside0 && update < 0 && new_inside == inside0;
@@ -1366,21 +1570,21 @@ static __device__ __noinline__ BiaxialStep group_bounce_biaxial(Group g, LanePat
 }
 
 // UNI is the transport instantiation (transport_class): TRANSPORT_ISOTROPIC the isotropic
-// megakernel, TRANSPORT_UNIAXIAL the uniaxial bounce, TRANSPORT_BIAXIAL the uniaxial bounce
+// megakernel, TRANSPORT_UNIAXIAL the uniaxial bounce, TRANSPORT_EXTENDED the uniaxial bounce
 // plus the out-of-line biaxial one (kept out of the uniaxial kernels, whose register
 // allocation the call site would change).
 template <int UNI>
 IX_DEV int group_step(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes, float& esc) {
-    if constexpr (UNI == TRANSPORT_BIAXIAL) {
+    if constexpr (UNI == TRANSPORT_EXTENDED) {
         if (S.biaxial) {
             const BiaxialStep r = group_bounce_biaxial(g, P, S, planes);
             P = r.P;
             esc = r.esc;
             return r.result;
         }
-        return group_bounce_uniaxial(g, P, S, planes, esc);
+        return group_bounce_uniaxial<UNI>(g, P, S, planes, esc);
     } else if constexpr (UNI == TRANSPORT_UNIAXIAL) {
-        return group_bounce_uniaxial(g, P, S, planes, esc);
+        return group_bounce_uniaxial<UNI>(g, P, S, planes, esc);
     } else {
         return group_bounce(g, P, S, planes, esc);
     }

@@ -226,3 +226,66 @@ def bounding_radius(planes: np.ndarray) -> float:
     if np.any(inside):
         best = float(np.max(np.linalg.norm(verts[inside], axis=1)))
     return best
+
+
+# ------------------------------------------------------------------------------------
+# Concave tools (ToolPrimitive, crates/indicatrix/src/geometry/tool.rs:233-340): the
+# constructors fill the 80-byte record in f32 as the reference does.
+# ------------------------------------------------------------------------------------
+TOOL_BALL, TOOL_CYLINDER, TOOL_FRUSTUM, TOOL_BICONE = 0, 1, 2, 3
+SWEEP_NONE, SWEEP_ALONG_AXIS, SWEEP_ACROSS_AXIS = 0, 1, 2
+
+
+def _tool(kind, centre, axis, rim, half_length, r):
+    from . import abi
+    t = abi.Tool()
+    t.kind = kind
+    t.sweep_kind = SWEEP_NONE
+    t.origin[:] = [float(np.float32(x)) for x in centre] + [float(np.float32(rim))]
+    t.axis[:] = [float(np.float32(x)) for x in axis] + [float(np.float32(half_length))]
+    t.profile[:] = [float(np.float32(r[0])), float(np.float32(r[1])), 0.0, 0.0]
+    t.sweep_dir[:] = [0.0, 0.0, 0.0, 0.0]
+    return t
+
+
+def tool_ball(centre, radius: float):
+    """ToolPrimitive::ball: a spherical dimple."""
+    return _tool(TOOL_BALL, centre, (0.0, 0.0, 1.0), radius, 0.0, (radius, radius))
+
+
+def tool_cylinder(centre, axis, radius: float, half_length: float):
+    """ToolPrimitive::cylinder: a capped cylinder along the unit axis."""
+    return _tool(TOOL_CYLINDER, centre, axis, radius, half_length, (radius, radius))
+
+
+def tool_frustum(centre, axis, r_neg: float, r_pos: float, half_length: float):
+    """ToolPrimitive::frustum: radius r_neg at -half_length, r_pos at +half_length; the
+    rim is their f32 mean 0.5 * (r_neg + r_pos)."""
+    rim = np.float32(0.5) * (np.float32(r_neg) + np.float32(r_pos))
+    return _tool(TOOL_FRUSTUM, centre, axis, rim, half_length, (r_neg, r_pos))
+
+
+def tool_bicone(centre, axis, rim_radius: float, half_length: float):
+    """ToolPrimitive::bicone: two cones meeting at the rim, apexes on the axis."""
+    return _tool(TOOL_BICONE, centre, axis, rim_radius, half_length, (0.0, 0.0))
+
+
+def with_sweep(tool, sweep: int, half_stroke: float, direction=(0.0, 0.0, 0.0)):
+    """ToolPrimitive::with_sweep: the tool reciprocates +-half_stroke along its axis
+    (SWEEP_ALONG_AXIS) or along `direction` across it (SWEEP_ACROSS_AXIS)."""
+    tool.sweep_kind = int(sweep)
+    tool.profile[2] = float(np.float32(half_stroke))
+    if sweep == SWEEP_ACROSS_AXIS:
+        tool.sweep_dir[:] = [float(np.float32(x)) for x in direction] + [0.0]
+    else:
+        tool.sweep_dir[:] = [0.0, 0.0, 0.0, 0.0]
+    return tool
+
+
+def any_orthonormal_vector(n):
+    """glam Vec3::any_orthonormal_vector (Duff et al., JCGT 2017) in f32."""
+    n = np.asarray(n, np.float32)
+    sign = np.float32(-1.0) if math.copysign(1.0, float(n[2])) < 0 else np.float32(1.0)
+    a = np.float32(-1.0) / (sign + n[2])
+    b = (n[0] * n[1]) * a
+    return np.array([b, sign + (n[1] * n[1]) * a, -n[1]], np.float32)

@@ -687,7 +687,11 @@ static inline float hmin8(__m256 v) {
 }
 #endif
 
-static bool intersect(const float* planes, uint32_t n, const Ray& ray, Hit* hit) {
+// The slab scan proper (simd/slab.rs slab_scan): the entering planes' largest t and the
+// first plane attaining it, the exiting planes' smallest t and its plane; false for a
+// parallel plane the origin is outside of.
+static bool slab_scan_raw(const float* planes, uint32_t n, const Ray& ray, F* tn_out, int* ni_out, F* tf_out,
+                          int* fi_out) {
     F t_near = -1e30f, t_far = 1e30f;
     int near_idx = -1, far_idx = -1;
     uint32_t i0 = 0;
@@ -766,6 +770,19 @@ static bool intersect(const float* planes, uint32_t n, const Ray& ray, Hit* hit)
             return false;
         }
     }
+    *tn_out = t_near;
+    *ni_out = near_idx;
+    *tf_out = t_far;
+    *fi_out = far_idx;
+    return true;
+}
+
+// intersect_polyhedron (intersect.rs:101-127): the slab, then the first boundary past
+// the 1e-4 restart epsilon.
+static bool intersect(const float* planes, uint32_t n, const Ray& ray, Hit* hit) {
+    F t_near, t_far;
+    int near_idx, far_idx;
+    if (!slab_scan_raw(planes, n, ray, &t_near, &near_idx, &t_far, &far_idx)) return false;
     if (t_near > t_far) return false;
     if (t_near > F(1e-4f)) {
         hit->t = t_near;
@@ -780,6 +797,400 @@ static bool intersect(const float* planes, uint32_t n, const Ray& ray, Hit* hit)
         return true;
     }
     return false;
+}
+
+// ------------------------------------------------------------------------------------
+// Concave tools (geometry/tool.rs, geometry/tool/interval.rs) and the carved stone
+// (optics/raytracer/intersect_stone.rs): each tool is the convex hull interval of the
+// pieces it decomposes into (balls, frusta, and the wedges of an across-axis sweep); the
+// stone is the slab minus the tools, walked in sorted boundary order.
+// ------------------------------------------------------------------------------------
+enum { TOOL_BALL = 0, TOOL_CYLINDER = 1, TOOL_FRUSTUM = 2, TOOL_BICONE = 3 };
+enum { SWEEP_NONE = 0, SWEEP_ALONG = 1, SWEEP_ACROSS = 2 };
+enum { PIECE_BALL = 0, PIECE_FRUSTUM = 1, PIECE_WEDGE = 2 };
+struct Piece {
+    int kind;
+    V3 c, a, d;
+    F r, hl, s, r0, r1;
+};
+static Piece ball_piece(V3 c, F r) {
+    Piece p{};
+    p.kind = PIECE_BALL;
+    p.c = c;
+    p.r = r;
+    return p;
+}
+static Piece frustum_piece(V3 c, V3 a, F hl, F r0, F r1) {
+    Piece p{};
+    p.kind = PIECE_FRUSTUM;
+    p.c = c;
+    p.a = a;
+    p.hl = hl;
+    p.r0 = r0;
+    p.r1 = r1;
+    return p;
+}
+static inline V3 tool_vec(const float* v) { return v3(v[0], v[1], v[2]); }
+// ToolPrimitive::pieces (tool.rs:470): at most 6.
+static int tool_pieces(const ix_tool& t, Piece out[6]) {
+    if (t.kind > TOOL_BICONE || t.sweep_kind > SWEEP_ACROSS) return 0;
+    const V3 c = tool_vec(t.origin), a = tool_vec(t.axis);
+    const F stroke = t.profile[2];
+    const bool swept = t.sweep_kind != SWEEP_NONE && stroke > F(0.0f);
+    int n = 0;
+    if (t.kind == TOOL_BALL) {
+        const F r = t.origin[3];
+        if (swept) {
+            const V3 dir = t.sweep_kind == SWEEP_ALONG ? a : tool_vec(t.sweep_dir);
+            out[n++] = ball_piece(c - dir * stroke, r);
+            out[n++] = ball_piece(c + dir * stroke, r);
+            out[n++] = frustum_piece(c, dir, stroke, r, r);
+        } else {
+            out[n++] = ball_piece(c, r);
+        }
+        return n;
+    }
+    // segments (tool.rs:430): (z_lo, z_hi, r_lo, r_hi) along the axis, and the peak.
+    const F hl = t.axis[3], rim = t.origin[3], rn = t.profile[0], rp = t.profile[1];
+    F seg[2][4];
+    int ns = 1;
+    F peak_z, peak_r;
+    if (t.kind == TOOL_CYLINDER) {
+        seg[0][0] = -hl; seg[0][1] = hl; seg[0][2] = rim; seg[0][3] = rim;
+        peak_z = hl;
+        peak_r = rim;
+    } else if (t.kind == TOOL_FRUSTUM) {
+        seg[0][0] = -hl; seg[0][1] = hl; seg[0][2] = rn; seg[0][3] = rp;
+        peak_z = rp >= rn ? hl : -hl;
+        peak_r = rp >= rn ? rp : rn;
+    } else {
+        seg[0][0] = -hl; seg[0][1] = 0.0f; seg[0][2] = rn; seg[0][3] = rim;
+        seg[1][0] = 0.0f; seg[1][1] = hl; seg[1][2] = rim; seg[1][3] = rp;
+        ns = 2;
+        peak_z = 0.0f;
+        peak_r = rim;
+    }
+    auto seg_piece = [&](const F* sg, V3 shift) {
+        return frustum_piece((c + a * (F(0.5f) * (sg[0] + sg[1]))) + shift, a, F(0.5f) * (sg[1] - sg[0]), sg[2], sg[3]);
+    };
+    for (int i = 0; i < ns; ++i) {
+        const F* sg = seg[i];
+        if (!swept) {
+            out[n++] = seg_piece(sg, v3(0.0f, 0.0f, 0.0f));
+        } else if (t.sweep_kind == SWEEP_ALONG) {
+            out[n++] = seg_piece(sg, sg[3] >= sg[2] ? (-a) * stroke : a * stroke);
+        } else {
+            const V3 dir = tool_vec(t.sweep_dir);
+            out[n++] = seg_piece(sg, (-dir) * stroke);
+            out[n++] = seg_piece(sg, dir * stroke);
+            Piece w{};
+            w.kind = PIECE_WEDGE;
+            w.c = c + a * (F(0.5f) * (sg[0] + sg[1]));
+            w.a = a;
+            w.d = dir;
+            w.hl = F(0.5f) * (sg[1] - sg[0]);
+            w.s = stroke;
+            w.r0 = sg[2];
+            w.r1 = sg[3];
+            out[n++] = w;
+        }
+    }
+    if (swept && t.sweep_kind == SWEEP_ALONG) out[n++] = frustum_piece(c + a * peak_z, a, stroke, peak_r, peak_r);
+    return n;
+}
+// quadratic_roots (interval.rs:8): a t^2 + 2 b t + c = 0, the stable form.
+static bool quadratic_roots(F a, F b, F c, F* lo, F* hi) {
+    const F disc = fma_(b, b, -(a * c));
+    if (disc <= F(1e-7f) * fma_(b, b, abs_(a * c))) return false;
+    const F sq = sqrt_(disc);
+    const F q = -(b + F(std::copysign(raw(sq), raw(b))));
+    const F r1 = q / a, r2 = c / q;
+    *lo = r1 <= r2 ? r1 : r2;
+    *hi = r1 <= r2 ? r2 : r1;
+    return true;
+}
+static bool ball_interval(const Ray& ray, V3 c, F r, F* lo, F* hi) {
+    const V3 o = ray.origin - c;
+    return quadratic_roots(dot(ray.dir, ray.dir), dot(o, ray.dir), fma_(r, -r, dot(o, o)), lo, hi);
+}
+static bool cap_range(F z0, F dz, F hl, F* s0, F* s1) {
+    if (abs_(dz) > F(1e-7f)) {
+        const F t1 = (-hl - z0) / dz, t2 = (hl - z0) / dz;
+        *s0 = t1 <= t2 ? t1 : t2;
+        *s1 = t1 <= t2 ? t2 : t1;
+        return true;
+    }
+    if (abs_(z0) <= hl) {
+        *s0 = -1e30f;
+        *s1 = 1e30f;
+        return true;
+    }
+    return false;
+}
+static bool clip_range(F lo, F hi, F s0, F s1, F* l, F* h) {
+    *l = max_(lo, s0);
+    *h = min_(hi, s1);
+    return *l <= *h;
+}
+// frustum_interval (interval.rs:52): the cone's quadratic clipped to the caps.
+static bool frustum_interval(const Ray& ray, V3 c, V3 a, F hl, F r0, F r1, F* lo_out, F* hi_out) {
+    const V3 o = ray.origin - c;
+    const F z0 = dot(o, a), dz = dot(ray.dir, a);
+    F s0, s1;
+    if (!cap_range(z0, dz, hl, &s0, &s1)) return false;
+    const F rm = F(0.5f) * (r0 + r1);
+    const F k = (r1 - r0) / (F(2.0f) * hl);
+    const V3 p = o - a * z0, q = ray.dir - a * dz;
+    const F rz0 = fma_(k, z0, rm);
+    const F rate = k * dz;
+    const F qa = fma_(rate, -rate, dot(q, q));
+    const F qb = fma_(-rate, rz0, dot(p, q));
+    const F qc = fma_(rz0, -rz0, dot(p, p));
+    if (abs_(qa) <= F(1e-7f)) {
+        if (abs_(qb) <= F(1e-7f)) {
+            if (!(qc <= F(0.0f))) return false;
+            *lo_out = s0;
+            *hi_out = s1;
+            return true;
+        }
+        const F t = -qc / (F(2.0f) * qb);
+        return qb > F(0.0f) ? clip_range(-1e30f, t, s0, s1, lo_out, hi_out)
+                            : clip_range(t, 1e30f, s0, s1, lo_out, hi_out);
+    }
+    F lo, hi;
+    if (!quadratic_roots(qa, qb, qc, &lo, &hi)) return false;
+    if (qa > F(0.0f)) return clip_range(lo, hi, s0, s1, lo_out, hi_out);
+    F xl, xh, yl, yh;
+    const bool x = clip_range(-1e30f, lo, s0, s1, &xl, &xh);
+    const bool y = clip_range(hi, 1e30f, s0, s1, &yl, &yh);
+    if (x && y) {
+        *lo_out = min_(xl, yl);
+        *hi_out = max_(xh, yh);
+        return true;
+    }
+    if (x) {
+        *lo_out = xl;
+        *hi_out = xh;
+        return true;
+    }
+    if (y) {
+        *lo_out = yl;
+        *hi_out = yh;
+        return true;
+    }
+    return false;
+}
+// wedge_interval (interval.rs:112): a slab of six planes.
+static bool wedge_interval(const Ray& ray, V3 c, V3 a, V3 d, F hl, F s, F r0, F r1, F* lo, F* hi) {
+    const V3 w = cross(a, d);
+    const F k = (r1 - r0) / (F(2.0f) * hl);
+    const F rm = F(0.5f) * (r0 + r1);
+    const V3 fn[6] = {a, -a, d, -d, w - a * k, (-w) - a * k};
+    const F fe[6] = {-hl, -hl, -s, -s, -rm, -rm};
+    const V3 o = ray.origin - c;
+    F t_near = -1e30f, t_far = 1e30f;
+    for (int i = 0; i < 6; ++i) {
+        const F denom = dot(fn[i], ray.dir);
+        const F side = dot(fn[i], o) + fe[i];
+        if (abs_(denom) > F(1e-7f)) {
+            const F t = -side / denom;
+            if (denom < F(0.0f))
+                t_near = max_(t_near, t);
+            else
+                t_far = min_(t_far, t);
+        } else if (side > F(0.0f)) {
+            return false;
+        }
+    }
+    if (!(t_near <= t_far)) return false;
+    *lo = t_near;
+    *hi = t_far;
+    return true;
+}
+static bool piece_interval(const Piece& pc, const Ray& ray, F* lo, F* hi) {
+    if (pc.kind == PIECE_BALL) return ball_interval(ray, pc.c, pc.r, lo, hi);
+    if (pc.kind == PIECE_FRUSTUM) return frustum_interval(ray, pc.c, pc.a, pc.hl, pc.r0, pc.r1, lo, hi);
+    return wedge_interval(ray, pc.c, pc.a, pc.d, pc.hl, pc.s, pc.r0, pc.r1, lo, hi);
+}
+// Vec3::any_orthonormal_vector (glam; Duff et al., "Building an Orthonormal Basis,
+// Revisited", JCGT 2017).
+static V3 any_orthonormal_vector(V3 n) {
+    const F sign = std::signbit(raw(n.z)) ? F(-1.0f) : F(1.0f);
+    const F a = F(-1.0f) / (sign + n.z);
+    const F b = (n.x * n.y) * a;
+    return v3(b, sign + (n.y * n.y) * a, -n.y);
+}
+// Piece::sd_normal (tool.rs:228): signed distance and outward normal.
+static F piece_sd_normal(const Piece& pc, V3 p, V3* n_out) {
+    if (pc.kind == PIECE_BALL) {
+        const V3 q = p - pc.c;
+        const F len = sqrt_(dot(q, q));
+        *n_out = len > F(1e-12f) ? v3(q.x / len, q.y / len, q.z / len) : v3(0.0f, 0.0f, 1.0f);
+        return len - pc.r;
+    }
+    if (pc.kind == PIECE_FRUSTUM) {
+        const V3 q = p - pc.c;
+        const F z = dot(q, pc.a);
+        const V3 perp = q - pc.a * z;
+        const F rho = sqrt_(dot(perp, perp));
+        const V3 rho_hat = rho > F(1e-12f) ? v3(perp.x / rho, perp.y / rho, perp.z / rho) : any_orthonormal_vector(pc.a);
+        const F cap_sd = z >= F(0.0f) ? z - pc.hl : -z - pc.hl;
+        const V3 cap_n = z >= F(0.0f) ? pc.a : -pc.a;
+        const F dr = pc.r1 - pc.r0;
+        const F len = sqrt_(fma_(F(4.0f) * pc.hl, pc.hl, dr * dr));
+        const F rm = F(0.5f) * (pc.r0 + pc.r1);
+        const F side_sd = fma_(z, -dr, ((rho - rm) * F(2.0f)) * pc.hl) / len;
+        const V3 side_n = rho_hat * ((F(2.0f) * pc.hl) / len) - pc.a * (dr / len);
+        if (side_sd > cap_sd) {
+            *n_out = side_n;
+            return side_sd;
+        }
+        *n_out = cap_n;
+        return cap_sd;
+    }
+    const V3 q = p - pc.c;
+    const V3 w = cross(pc.a, pc.d);
+    const F z = dot(q, pc.a), x = dot(q, pc.d), y = dot(q, w);
+    const F k = (pc.r1 - pc.r0) / (F(2.0f) * pc.hl);
+    const F rm = F(0.5f) * (pc.r0 + pc.r1);
+    const F kappa = F(1.0f) / sqrt_(fma_(k, k, 1.0f));
+    F best = z >= F(0.0f) ? z - pc.hl : -z - pc.hl;
+    V3 best_n = z >= F(0.0f) ? pc.a : -pc.a;
+    const F along = x >= F(0.0f) ? x - pc.s : -x - pc.s;
+    if (along > best) {
+        best = along;
+        best_n = x >= F(0.0f) ? pc.d : -pc.d;
+    }
+    const F sp = ((y - rm) - k * z) * kappa;
+    if (sp > best) {
+        best = sp;
+        best_n = (w - pc.a * k) * kappa;
+    }
+    const F sn = ((-y - rm) - k * z) * kappa;
+    if (sn > best) {
+        best = sn;
+        best_n = ((-w) - pc.a * k) * kappa;
+    }
+    *n_out = best_n;
+    return best;
+}
+// ToolPrimitive::ray_interval (tool.rs:580): the hull of the pieces' intervals.
+static bool tool_ray_interval(const ix_tool& t, const Ray& ray, F* lo, F* hi) {
+    Piece ps[6];
+    const int n = tool_pieces(t, ps);
+    bool any = false;
+    for (int i = 0; i < n; ++i) {
+        F c, d;
+        if (!piece_interval(ps[i], ray, &c, &d)) continue;
+        if (!any) {
+            *lo = c;
+            *hi = d;
+            any = true;
+        } else {
+            *lo = min_(*lo, c);
+            *hi = max_(*hi, d);
+        }
+    }
+    return any;
+}
+// outward_normal (tool.rs:560): the normal of the piece whose surface is nearest.
+static V3 tool_outward_normal(const ix_tool& t, V3 p) {
+    Piece ps[6];
+    const int n = tool_pieces(t, ps);
+    if (n == 0) return v3(0.0f, 0.0f, 1.0f);
+    F best = INFINITY;
+    V3 best_n = v3(0.0f, 0.0f, 1.0f);
+    for (int i = 0; i < n; ++i) {
+        V3 nn;
+        const F sd = piece_sd_normal(ps[i], p, &nn);
+        if (abs_(sd) < best) {
+            best = abs_(sd);
+            best_n = nn;
+        }
+    }
+    return best_n;
+}
+// contains (tool.rs:545).
+static bool tool_contains(const ix_tool& t, V3 p) {
+    Piece ps[6];
+    const int n = tool_pieces(t, ps);
+    for (int i = 0; i < n; ++i) {
+        V3 nn;
+        if (piece_sd_normal(ps[i], p, &nn) <= F(0.0f)) return true;
+    }
+    return false;
+}
+// f32::total_cmp's key: the bits, negatives' magnitude bits flipped, compared signed.
+static inline int32_t total_order_key(F t) {
+    int32_t b;
+    const float f = raw(t);
+    std::memcpy(&b, &f, 4);
+    return b ^ (int32_t)(((uint32_t)(b >> 31)) >> 1);
+}
+// carve + intersect_stone_soa_side (intersect_stone.rs:62-170): the first boundary past
+// 1e-4 where the ray's in-material state changes; *entering is the state after it.
+static bool intersect_carved(const float* planes, uint32_t n_planes, const ix_tool* tools, uint32_t n_tools,
+                             const Ray& ray, Hit* hit, bool* entering) {
+    F t_near, t_far;
+    int near_idx, far_idx;
+    if (!slab_scan_raw(planes, n_planes, ray, &t_near, &near_idx, &t_far, &far_idx)) return false;
+    if (t_near > t_far) return false;
+    struct Ev {
+        F t;
+        uint32_t key;
+    };
+    std::vector<Ev> ev;
+    ev.reserve(2 * n_tools + 2);
+    ev.push_back({t_near, 0u});
+    ev.push_back({t_far, 1u});
+    for (uint32_t k = 0; k < n_tools && k < IX_MAX_TOOLS; ++k) {
+        F c, d;
+        if (tool_ray_interval(tools[k], ray, &c, &d)) {
+            ev.push_back({c, 2u + 2u * k});
+            ev.push_back({d, 3u + 2u * k});
+        }
+    }
+    std::sort(ev.begin(), ev.end(), [](const Ev& x, const Ev& y) {
+        const int32_t a = total_order_key(x.t), b = total_order_key(y.t);
+        return a != b ? a < b : x.key < y.key;
+    });
+    int plane_depth = 0, tool_depth = 0;
+    bool inside = false;
+    for (const Ev& e : ev) {
+        if (e.key == 0)
+            ++plane_depth;
+        else if (e.key == 1)
+            --plane_depth;
+        else if (e.key % 2 == 0)
+            ++tool_depth;
+        else
+            --tool_depth;
+        const bool now_inside = plane_depth > 0 && tool_depth <= 0;
+        if (now_inside == inside) continue;
+        inside = now_inside;
+        if (e.t <= F(1e-4f)) continue;
+        hit->t = e.t;
+        if (e.key <= 1) {
+            const int idx = e.key == 0 ? near_idx : far_idx;
+            hit->normal = idx >= 0 ? load3(planes + 4 * idx) : v3(0.0f, 0.0f, 0.0f);
+            hit->facet = idx >= 0 ? idx : 0;
+        } else {
+            const uint32_t ti = (e.key - 2u) / 2u;
+            const V3 point = ray.origin + ray.dir * e.t;
+            hit->normal = -tool_outward_normal(tools[ti], point);
+            hit->facet = (int)(n_planes + ti);
+        }
+        *entering = now_inside;
+        return true;
+    }
+    return false;
+}
+// intersect_stone_soa (intersect_stone.rs:136) for a scene: the slab alone for a convex
+// stone.  *carved tells whether *entering was set.
+static bool intersect_scene(const ix_scene* sc, const Ray& ray, Hit* hit, bool* carved, bool* entering) {
+    *carved = sc->n_tools > 0 && sc->tools;
+    if (!*carved) return intersect(sc->planes, sc->n_planes, ray, hit);
+    return intersect_carved(sc->planes, sc->n_planes, sc->tools, sc->n_tools, ray, hit, entering);
 }
 
 // shading_normal_near_edge (intersect.rs:196).
@@ -1447,7 +1858,8 @@ struct Path {
 static void try_split_exit_channel(Path& P, V3 hit_point, int k, V3 dir_k, F transmitted_i) {
     Ray probe{hit_point + dir_k * F(1e-4f), dir_k};
     Hit h;
-    if (intersect(P.sc->planes, P.sc->n_planes, probe, &h)) return;
+    bool carved, entering;
+    if (intersect_scene(P.sc, probe, &h, &carved, &entering)) return;
     F env = environment_channel(P.sc->environment, dir_k, P.lambdas[k], P.observer);
     P.split[k] = fma_(max_(transmitted_i, 0.0f) * F(1.0f), env, P.split[k]);
     P.splits++;
@@ -1937,6 +2349,24 @@ static void frosted_orthonormal_basis(V3 n, V3* t, V3* b) {
     *t = normalize_or_zero(a - n * dot(n, a));
     *b = cross(n, *t);
 }
+// shading_normal_for_hit (transport/inner.rs:54): a carved stone rounds a plane facet's
+// edges only away from the tools (four probes a rounding radius out along the facet's
+// frosted basis); a tool facet keeps its own normal.
+static V3 shading_normal_for_hit(const ix_scene* sc, V3 hit_point, int facet, V3 hit_normal, F radius) {
+    const bool carved = sc->n_tools > 0 && sc->tools;
+    if (!carved || radius <= F(0.0f))
+        return shading_normal_near_edge(sc->planes, sc->n_planes, hit_point, facet, hit_normal, radius);
+    if ((uint32_t)facet >= sc->n_planes) return hit_normal;
+    V3 u, v;
+    frosted_orthonormal_basis(hit_normal, &u, &v);
+    const V3 dirs[4] = {u, -u, v, -v};
+    for (const V3& dir : dirs) {
+        const V3 probe = hit_point + dir * radius;
+        for (uint32_t k = 0; k < sc->n_tools; ++k)
+            if (tool_contains(sc->tools[k], probe)) return hit_normal;
+    }
+    return shading_normal_near_edge(sc->planes, sc->n_planes, hit_point, facet, hit_normal, radius);
+}
 // cosine_weighted_hemisphere (frosted.rs:34): (2 pi) u2 as the angle, glam's left-to-right
 // sum of the three scaled basis vectors.
 static V3 cosine_weighted_hemisphere(F u1, F u2, V3 n) {
@@ -2213,7 +2643,8 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
     for (bounce = 0; bounce < sc->max_bounces; ++bounce) {
         iterations = bounce + 1;
         Hit hit;
-        if (!intersect(sc->planes, sc->n_planes, P.ray, &hit)) {
+        bool carved = false, entering = false;
+        if (!intersect_scene(sc, P.ray, &hit, &carved, &entering)) {
             // handle_miss (bounce_body/miss.rs:33) + accumulate_miss_radiance (bounce.rs:40).
             F env[8];
             environment_channels(sc->environment, P.ray.dir, P.lambdas, P.observer, env);
@@ -2227,6 +2658,9 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
             }
             break;
         }
+        // A carved stone's hit tells which medium the ray is in (bounce_body.rs:391-397):
+        // the restart may have stepped over a second boundary within 1e-4.
+        if (carved) P.inside = !entering;
         // The interior segment may end in a scattering event first (bounce_body.rs:408-417).
         if (P.inside && m.scattering_sigma_s > 0.0f) {
             const int sc_out = scatter_step(P, hit.t, bounce);
@@ -2238,8 +2672,7 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
         }
         // facet_event (bounce_body.rs:611).
         V3 hit_point = P.ray.origin + hit.t * P.ray.dir;
-        V3 normal = shading_normal_near_edge(sc->planes, sc->n_planes, hit_point, hit.facet,
-                                             hit.normal, m.edge_rounding_radius);
+        V3 normal = shading_normal_for_hit(sc, hit_point, hit.facet, hit.normal, m.edge_rounding_radius);
         // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:69).
         V3 cpn = normalize_or_zero(cross(P.k, normal));
         if (P.has_prev && length_squared(cpn) > F(1e-6f) && length_squared(P.prev_pn) > F(1e-6f)) {
@@ -3118,6 +3551,48 @@ void ixo_biaxial_bundle(const ix_material* m, const float k[3], const float norm
     const F ab = m->has_abs_beta ? spectral_absorption(m->abs_beta, lambda_nm) : ao;
     out[22] = raw(quadratic_form3(ax, ao, ab, ae, assigned_mode_e_field_biaxial(I, kk, true)));
     out[23] = raw(quadratic_form3(ax, ao, ab, ae, assigned_mode_e_field_biaxial(I, kk, false)));
+}
+// A tool's ray interval (ToolPrimitive::ray_interval): 1 and out = (t_lo, t_hi), or 0.
+int ixo_tool_ray_interval(const ix_tool* t, const float origin[3], const float dir[3], float out[2]) {
+    F lo, hi;
+    if (!tool_ray_interval(*t, Ray{load3(origin), load3(dir)}, &lo, &hi)) return 0;
+    out[0] = raw(lo);
+    out[1] = raw(hi);
+    return 1;
+}
+int ixo_tool_contains(const ix_tool* t, const float p[3]) { return tool_contains(*t, load3(p)) ? 1 : 0; }
+// The distance to the nearest piece surface (boundary_gap, tool.rs:550).
+float ixo_tool_boundary_gap(const ix_tool* t, const float p[3]) {
+    Piece ps[6];
+    const int n = tool_pieces(*t, ps);
+    F best = INFINITY;
+    for (int i = 0; i < n; ++i) {
+        V3 nn;
+        best = min_(best, abs_(piece_sd_normal(ps[i], load3(p), &nn)));
+    }
+    return n ? raw(best) : 0.0f;
+}
+void ixo_tool_outward_normal(const ix_tool* t, const float p[3], float out[3]) {
+    store3(out, tool_outward_normal(*t, load3(p)));
+}
+// intersect_stone_soa_side: returns 1 on a hit (t, normal, facet, and for a carved
+// stone entering 0 / 1, else -1 in *entering), 0 on a miss.
+int ixo_intersect_stone(const float* planes, uint32_t n_planes, const ix_tool* tools, uint32_t n_tools,
+                        const float origin[3], const float dir[3], float* t, float normal[3], int32_t* facet,
+                        int32_t* entering) {
+    ix_scene sc{};
+    sc.planes = planes;
+    sc.n_planes = n_planes;
+    sc.tools = tools;
+    sc.n_tools = n_tools;
+    Hit h;
+    bool carved = false, ent = false;
+    if (!intersect_scene(&sc, Ray{load3(origin), load3(dir)}, &h, &carved, &ent)) return 0;
+    *t = raw(h.t);
+    store3(normal, h.normal);
+    *facet = h.facet;
+    *entering = carved ? (ent ? 1 : 0) : -1;
+    return 1;
 }
 float ixo_channel_alpha(const ix_material* m, const float k[3], float lambda_nm) {
     // The non-birefringent branch of channel_absorption_alphas_assigned

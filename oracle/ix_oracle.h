@@ -83,6 +83,13 @@ void ixo_fresnel_channel(float n1, float n2, float cos_i, const float s_in[4], f
 /* A non-birefringent material's channel alpha along wave normal k
  * (channel_absorption_alphas_assigned, raytracer/absorption.rs:197). */
 float ixo_channel_alpha(const ix_material* m, const float k[3], float lambda_nm);
+int ixo_tool_ray_interval(const ix_tool* t, const float origin[3], const float dir[3], float out[2]);
+int ixo_tool_contains(const ix_tool* t, const float p[3]);
+float ixo_tool_boundary_gap(const ix_tool* t, const float p[3]);
+void ixo_tool_outward_normal(const ix_tool* t, const float p[3], float out[3]);
+int ixo_intersect_stone(const float* planes, uint32_t n_planes, const ix_tool* tools, uint32_t n_tools,
+                        const float origin[3], const float dir[3], float* t, float normal[3], int32_t* facet,
+                        int32_t* entering);
 void ixo_biaxial_bundle(const ix_material* m, const float k[3], const float normal[3], float cos_i,
                         float lambda_nm, float n_beta, float out[24]);
 /* simd/slab.rs:147 + intersect.rs:101: returns 1 and fills t/idx on a hit */

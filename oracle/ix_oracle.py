@@ -153,6 +153,17 @@ def _load(name: str) -> C.CDLL:
     lib.ixo_fresnel_channel.argtypes = [C.c_float, C.c_float, C.c_float, f32p, f32p]
     lib.ixo_channel_alpha.restype = C.c_float
     lib.ixo_channel_alpha.argtypes = [P(abi.Material), f32p, C.c_float]
+    lib.ixo_tool_ray_interval.restype = C.c_int
+    lib.ixo_tool_ray_interval.argtypes = [P(abi.Tool), f32p, f32p, f32p]
+    lib.ixo_tool_contains.restype = C.c_int
+    lib.ixo_tool_contains.argtypes = [P(abi.Tool), f32p]
+    lib.ixo_tool_boundary_gap.restype = C.c_float
+    lib.ixo_tool_boundary_gap.argtypes = [P(abi.Tool), f32p]
+    lib.ixo_tool_outward_normal.restype = None
+    lib.ixo_tool_outward_normal.argtypes = [P(abi.Tool), f32p, f32p]
+    lib.ixo_intersect_stone.restype = C.c_int
+    lib.ixo_intersect_stone.argtypes = [f32p, C.c_uint32, P(abi.Tool), C.c_uint32, f32p, f32p, f32p, f32p,
+                                        P(C.c_int32), P(C.c_int32)]
     lib.ixo_biaxial_bundle.restype = None
     lib.ixo_biaxial_bundle.argtypes = [P(abi.Material), f32p, f32p, C.c_float, C.c_float, C.c_float, f32p]
     lib.ixo_counting_build.restype = C.c_int

@@ -159,9 +159,10 @@ def test_step_cut_and_random_stones():
         assert geometry.face_planes(st.planes.astype(np.float64)).all()
 
 
-def test_tools_decline_and_the_abi_forms_of_cancel_and_on_done():
-    """The boundary's argument forms: an ix_tool is the reference's 80-byte ToolPrimitive
-    and any tool declines routing (tool_routing.rs:81; convex stones only here); the cancel
+def test_tools_route_and_the_abi_forms_of_cancel_and_on_done():
+    """The boundary's argument forms: an ix_tool is the reference's 80-byte ToolPrimitive;
+    a valid tool routes and one failing ToolPrimitive::validate declines (here a ball
+    record with a zero axis, tool_routing.rs:81); the cancel
     flag is one byte, as a Rust AtomicBool; a CTA size other than 0 / 64 / 128 / 256 and an
     unknown kernel variant are refused at create time (no device is needed to see that);
     on_done reports every item of a declined batch."""
@@ -172,6 +173,7 @@ def test_tools_decline_and_the_abi_forms_of_cancel_and_on_done():
     ball.kind = 0
     ball.origin[:] = [0.0, 0.3, 0.0, 0.05]
     assert not scene_routes_to_gpu_with_tools(fs, [ball])
+    assert scene_routes_to_gpu_with_tools(fs, [geometry.tool_ball((0.0, 0.3, 0.0), 0.05)])
     flag = CancelFlag()
     assert C.sizeof(flag._word) == 1 and not flag.is_set()
     flag.set()
