@@ -100,11 +100,21 @@ typedef struct ix_material {
     ix_absorption abs_beta;
 } ix_material;
 
-/* Lighting model ids: the reference's LightingModel::gpu_id for the two it shares
- * (environment/mod.rs:218-229) plus a uniform furnace dome. */
-enum { IX_ENV_STUDIO = 0, IX_ENV_ISO_HEMISPHERE = 1, IX_ENV_UNIFORM = 100 };
-/* Illuminant spectral power (environment/spectral.rs:89-113). */
-enum { IX_SPEC_D65 = 0, IX_SPEC_BLACKBODY = 1, IX_SPEC_FLAT = 2 };
+/* Lighting model ids: the reference's LightingModel::gpu_id (environment/mod.rs:281-289)
+ * plus a uniform furnace dome. */
+enum {
+    IX_ENV_STUDIO = 0,
+    IX_ENV_ISO_HEMISPHERE = 1,
+    IX_ENV_LIGHT_TENT = 2,
+    IX_ENV_DAYLIGHT_DOME = 3,
+    IX_ENV_ASET = 4,
+    IX_ENV_DAYLIGHT_SUN = 5,
+    IX_ENV_UNIFORM = 100
+};
+/* Illuminant spectral power (environment/spectral.rs:89-145): D65, a normalised blackbody,
+ * flat, a Gaussian line (the UV lamps), and the wavelength itself (the ASET view's zone
+ * bands read it, rig.rs:580). */
+enum { IX_SPEC_D65 = 0, IX_SPEC_BLACKBODY = 1, IX_SPEC_FLAT = 2, IX_SPEC_GAUSSIAN = 3, IX_SPEC_WAVELENGTH = 4 };
 
 typedef struct ix_environment {
     uint32_t model;
@@ -123,6 +133,11 @@ typedef struct ix_environment {
     uint32_t white_balance;     /* apply the Bradford von Kries round trip at finish     */
     float wb_lms[3];            /* LMS scale of the white balance                       */
     float uniform_radiance;     /* IX_ENV_UNIFORM dome radiance                         */
+    /* TentParams (environment/mod.rs:185) of the IX_ENV_LIGHT_TENT presets. */
+    float tent_walls, tent_cards, tent_spark, tent_ground, tent_flat;
+    float sun_factor;           /* IX_ENV_DAYLIGHT_SUN: SUN_RADIANCE x horizon_blend(key_dir) */
+    float line_centre_nm;       /* IX_SPEC_GAUSSIAN: line centre and sigma                  */
+    float line_sigma_nm;
 } ix_environment;
 
 struct ix_tool;

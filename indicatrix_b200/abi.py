@@ -19,7 +19,8 @@ MAX_TOOLS = 128
 DISP_SELLMEIER1, DISP_SELLMEIER3, DISP_CAUCHY = 0, 1, 2
 BAND_GAUSS_WAVELENGTH, BAND_GAUSS_ENERGY = 0, 1
 ENV_STUDIO, ENV_ISO_HEMISPHERE, ENV_UNIFORM = 0, 1, 100
-SPEC_D65, SPEC_BLACKBODY, SPEC_FLAT = 0, 1, 2
+ENV_LIGHT_TENT, ENV_DAYLIGHT_DOME, ENV_ASET, ENV_DAYLIGHT_SUN = 2, 3, 4, 5
+SPEC_D65, SPEC_BLACKBODY, SPEC_FLAT, SPEC_GAUSSIAN, SPEC_WAVELENGTH = 0, 1, 2, 3, 4
 
 # GpuAccumulate (gpu_backend/mod.rs:308-326) plus the internal error the C ABI maps to
 # a decline.
@@ -102,6 +103,14 @@ class Environment(C.Structure):
         ("white_balance", C.c_uint32),
         ("wb_lms", C.c_float * 3),
         ("uniform_radiance", C.c_float),
+        ("tent_walls", C.c_float),
+        ("tent_cards", C.c_float),
+        ("tent_spark", C.c_float),
+        ("tent_ground", C.c_float),
+        ("tent_flat", C.c_float),
+        ("sun_factor", C.c_float),
+        ("line_centre_nm", C.c_float),
+        ("line_sigma_nm", C.c_float),
     ]
 
 

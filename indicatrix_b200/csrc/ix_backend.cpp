@@ -533,7 +533,18 @@ int ix_scene_routes_to_gpu(const ix_scene* s) {
     const ix_material& m = s->material;
     if (m.has_e_dispersion && m.e_dispersion.kind > IX_DISP_CAUCHY) return 0;
     const ix_environment& e = s->environment;
-    if (e.model != IX_ENV_STUDIO && e.model != IX_ENV_ISO_HEMISPHERE && e.model != IX_ENV_UNIFORM) return 0;
+    if (e.model > IX_ENV_DAYLIGHT_SUN && e.model != IX_ENV_UNIFORM) return 0;
+    // The UV lamps are fluorescence sources; their scenes never reach the GPU
+    // (gpu_backend/mod.rs:288-298).
+    if (e.spectrum == IX_SPEC_GAUSSIAN) return 0;
+    // DaylightSun enables next-event estimation at frosted facets and scattering events
+    // (environment_supports_nee, environment/nee.rs:60), which this path does not carry:
+    // such scenes decline; a polished, clear stone takes no light sample and is traced.
+    if (e.model == IX_ENV_DAYLIGHT_SUN) {
+        if (m.scattering_sigma_s > 0.0f) return 0;
+        for (uint32_t i = 0; s->facet_finishes && i < s->n_finishes; ++i)
+            if (s->facet_finishes[i]) return 0;
+    }
     if (m.dispersion.kind > IX_DISP_CAUCHY) return 0;
     // A biaxial indicatrix is traced as the anisotropic transport's biaxial arm; an
     // isotropic material carrying one (the reference's eigen-polarisation mean of the
@@ -1366,23 +1377,47 @@ int ix_environment_preset(int32_t preset, float exposure, float light_yaw, float
                           ix_environment* out) {
     if (!out) return -1;
     std::memset(out, 0, sizeof(*out));
-    float temp_k, spot;
-    bool d65;
+    // LightingPreset::params / model / uses_d65 / uv_line (environment/mod.rs:318-560).
+    float temp_k = 6500.0f, spot = 1.0f;
+    float tent[5] = {1.0f, 1.0f, 1.0f, 0.02f, 0.0f};  // walls, cards, spark, ground, flat
+    bool d65 = true, uv = false;
+    float uv_centre = 0.0f, uv_fwhm = 0.0f;
     uint32_t model;
     switch (preset) {
-        case 1: model = IX_ENV_ISO_HEMISPHERE; temp_k = 6500.0f; spot = 1.0f; d65 = true; break;
-        case 7: model = IX_ENV_STUDIO; temp_k = 6500.0f; spot = 1.0f; d65 = true; break;
-        case 8: model = IX_ENV_STUDIO; temp_k = 3200.0f; spot = 1.2f; d65 = false; break;
-        case 9: model = IX_ENV_STUDIO; temp_k = 2856.0f; spot = 1.2f; d65 = false; break;
-        case 10: model = IX_ENV_STUDIO; temp_k = 5000.0f; spot = 1.6f; d65 = false; break;
-        case 11: model = IX_ENV_STUDIO; temp_k = 6000.0f; spot = 2.4f; d65 = false; break;
+        case 0: model = IX_ENV_LIGHT_TENT; temp_k = 5000.0f; d65 = false; break;        // LightTent
+        case 1: model = IX_ENV_ISO_HEMISPHERE; break;                                    // IsoHemisphere
+        case 2: model = IX_ENV_LIGHT_TENT; spot = 0.0f; tent[0] = 5.0f; tent[1] = 0.0f;  // WhiteTray
+                tent[2] = 0.0f; tent[3] = 0.8f; tent[4] = 1.0f; break;
+        case 3: model = IX_ENV_LIGHT_TENT; tent[0] = 3.0f; tent[1] = 0.0f; tent[3] = 0.05f; break;  // ShopLights
+        case 4: model = IX_ENV_LIGHT_TENT; tent[0] = 0.4f; tent[1] = 0.0f; tent[2] = 0.0f;          // WindowDaylight
+                tent[3] = 0.03f; break;
+        case 5: model = IX_ENV_DAYLIGHT_DOME; break;                                     // DaylightDome
+        case 6: model = IX_ENV_DAYLIGHT_SUN; break;                                      // DaylightSun
+        case 7: model = IX_ENV_STUDIO; break;                                            // Daylight
+        case 8: model = IX_ENV_STUDIO; temp_k = 3200.0f; spot = 1.2f; d65 = false; break;  // Incandescent
+        case 9: model = IX_ENV_STUDIO; temp_k = 2856.0f; spot = 1.2f; d65 = false; break;  // IlluminantA
+        case 10: model = IX_ENV_STUDIO; temp_k = 5000.0f; spot = 1.6f; d65 = false; break;  // RingLights
+        case 11: model = IX_ENV_STUDIO; temp_k = 6000.0f; spot = 2.4f; d65 = false; break;  // DarkSpotlight
+        case 12: model = IX_ENV_ASET; break;                                             // Aset
+        case 13: model = IX_ENV_STUDIO; d65 = false; uv = true; uv_centre = 365.0f; uv_fwhm = 10.0f; break;
+        case 14: model = IX_ENV_STUDIO; d65 = false; uv = true; uv_centre = 395.0f; uv_fwhm = 12.0f; break;
         default: return -1;
     }
     out->model = model;
-    out->spectrum = d65 ? IX_SPEC_D65 : IX_SPEC_BLACKBODY;
+    out->spectrum = model == IX_ENV_ASET ? IX_SPEC_WAVELENGTH : uv ? IX_SPEC_GAUSSIAN : d65 ? IX_SPEC_D65
+                                                                                              : IX_SPEC_BLACKBODY;
+    if (uv) {
+        out->line_centre_nm = uv_centre;
+        out->line_sigma_nm = uv_fwhm / (2.0f * std::sqrt(2.0f * 0.6931472f));  // fwhm / (2 sqrt(2 ln 2))
+    }
+    out->tent_walls = tent[0];
+    out->tent_cards = tent[1];
+    out->tent_spark = tent[2];
+    out->tent_ground = tent[3];
+    out->tent_flat = tent[4];
     out->exposure = exposure;
     out->spot_mult = spot;
-    out->ambient_fill = 1;
+    out->ambient_fill = uv ? 0 : 1;
     out->backdrop = backdrop;
     out->surface_glare = (surface_glare >= 1.0f || std::isnan(surface_glare)) ? 1.0f
                          : (surface_glare > 0.0f ? surface_glare : 0.0f);
@@ -1419,7 +1454,15 @@ int ix_environment_preset(int32_t preset, float exposure, float light_yaw, float
         float a = std::fma((float)i, step, light_yaw);
         hstore(out->ring_dirs[i], hnormalize(h3(std::sin(a) * 0.75f, sp * 0.8f, std::cos(a) * 0.75f)));
     }
-    if (!d65) {
+    // sun_radiance_factor (sun.rs:25): SUN_RADIANCE x horizon_blend(key_dir).
+    {
+        const float y = out->key_dir[1];
+        float t = (y - -0.05f) / (0.05f - -0.05f);
+        t = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
+        out->sun_factor = 40000.0f * (t * t * std::fma(-2.0f, t, 3.0f));
+    }
+    // uses_white_balance (mod.rs:553): neither D65 nor a UV lamp nor the ASET view.
+    if (!d65 && !uv && model != IX_ENV_ASET) {
         out->white_balance = 1;
         hstore(out->wb_lms, white_balance(temp_k));
     } else {

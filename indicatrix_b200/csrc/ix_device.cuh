@@ -454,6 +454,16 @@ IX_DEV float spectral_power(const ix_environment& env, float lambda_nm) {
     if (env.spectrum == IX_SPEC_BLACKBODY) return blackbody(env.bb_t_k, env.bb_denom_560, lambda_nm);
     return 1.0f;
 }
+// ... with the UV lamps' line and the ASET view's wavelength input (spectral.rs:137,
+// rig.rs:165): the extended lookup's.
+IX_DEV float spectral_power_ext(const ix_environment& env, float lambda_nm) {
+    if (env.spectrum == IX_SPEC_GAUSSIAN) {
+        const float z = (lambda_nm - env.line_centre_nm) / env.line_sigma_nm;
+        return expf((-0.5f * z) * z);
+    }
+    if (env.spectrum == IX_SPEC_WAVELENGTH) return lambda_nm;
+    return spectral_power(env, lambda_nm);
+}
 
 // ------------------------------------------------------------------------------------
 // Environment (environment/rig.rs:67-377): the direction-only lighting, then the
@@ -470,6 +480,62 @@ struct Lighting {
     int ring_len;  // ring emitters lit for this direction (at most 4 overlap)
     bool has_softbox, has_fill, has_ground;
 };
+// The tent, dome, sun and ASET constants (rig.rs:67-85, :120-135, sun.rs:10-20).
+constexpr float TENT_KEY_OUTER_COS = 0.7660444f, TENT_KEY_INNER_COS = 0.9396926f;
+constexpr float SPARK_OUTER_COS = 0.9961947f, SPARK_INNER_COS = 0.9993908f;
+constexpr float CARD_OUTER_COS = 0.898794f, CARD_INNER_COS = 0.9612617f;
+constexpr float ASET_SIGMA_NM = 8.493218f;
+constexpr float ASET_EDGE_45_LO = 0.6871068f, ASET_EDGE_45_HI = 0.7271068f;
+constexpr float ASET_EDGE_75_LO = 0.9459258f, ASET_EDGE_75_HI = 0.9859258f;
+constexpr float SUN_DISC_COS = 0.9999889f;
+IX_DEV float aset_band(float lambda_nm, float centre_nm) {
+    const float z = (lambda_nm - centre_nm) / ASET_SIGMA_NM;
+    return expf((-0.5f * z) * z);
+}
+// The scaled and banded models other than the iso-hemisphere (rig.rs:254-310, :439-500):
+// returns the Scaled factor for the tent, dome and sun; for the ASET view the three zone
+// weights and the tray's ground in *bands (the radiance is banded at lookup time).
+IX_DEV float other_model_lighting(const ix_environment& env, V3 d, V3 observer, float* bands) {
+    const float tray = env.backdrop;
+    const float horizon = smoothstep_(-0.05f, 0.05f, d.y);
+    const float vis = 1.0f - smoothstep_(env.shadow_cos[0], env.shadow_cos[1], dot(d, observer));
+    auto lit_ground = [&](float own) {
+        return tray > 0.0f ? ((1.0f - horizon) * vis) * tray : own * (1.0f - horizon);
+    };
+    if (env.model == IX_ENV_LIGHT_TENT) {
+        float walls = fmaf(0.08f, fmaxf(d.y, 0.0f), 0.14f) * env.tent_walls;
+        if (env.tent_flat > 0.0f) walls = fmaf(0.18f * env.tent_walls, env.tent_flat, walls * (1.0f - env.tent_flat));
+        float card = 0.0f;
+#pragma unroll
+        for (int slot = 4; slot <= 12; slot += 4)
+            card = fmaxf(card, smoothstep_(CARD_OUTER_COS, CARD_INNER_COS, dot(d, load3(env.ring_dirs[slot]))));
+        walls = walls * fmaf(card * env.tent_cards, -0.9f, 1.0f);
+        const float key = smoothstep_(TENT_KEY_OUTER_COS, TENT_KEY_INNER_COS, dot(d, load3(env.key_dir))) *
+                          (1.4f * env.spot_mult);
+        const float spark = (smoothstep_(SPARK_OUTER_COS, SPARK_INNER_COS, dot(d, load3(env.fill_dir))) *
+                             (5.0f * env.spot_mult)) * env.tent_spark;
+        return ((walls + key) + spark) * (horizon * vis) + lit_ground(env.tent_ground);
+    }
+    if (env.model == IX_ENV_ASET) {
+        const float s45 = smoothstep_(ASET_EDGE_45_LO, ASET_EDGE_45_HI, d.y);
+        const float s75 = smoothstep_(ASET_EDGE_75_LO, ASET_EDGE_75_HI, d.y);
+        bands[0] = (s45 * (1.0f - s75)) * horizon;
+        bands[1] = (1.0f - s45) * horizon;
+        bands[2] = s75 * horizon;
+        bands[3] = tray > 0.0f ? (1.0f - horizon) * tray : 0.0f;
+        return 0.0f;
+    }
+    // DaylightDome and DaylightSun: the sky, its aureole about the sun, and the sun's disc.
+    const float sun_dot = dot(d, load3(env.key_dir));
+    const float sky = fmaf(0.08f, 1.0f - fmaxf(d.y, 0.0f), 0.10f);
+    const float glow = fmaxf(sun_dot, 0.0f);
+    const float glow2 = glow * glow;
+    const float glow4 = glow2 * glow2;
+    const float aureole = (glow4 * glow4) * 0.30f;
+    const float sum = (sky + aureole) * (horizon * vis) + lit_ground(0.04f);
+    if (env.model == IX_ENV_DAYLIGHT_DOME) return sum;
+    return sum + (sun_dot >= SUN_DISC_COS ? env.sun_factor : 0.0f);
+}
 IX_DEV Lighting direction_lighting(const ix_environment& env, V3 dir, V3 observer) {
     Lighting L;
     L.factor = 0.0f;
@@ -485,6 +551,7 @@ IX_DEV Lighting direction_lighting(const ix_environment& env, V3 dir, V3 observe
         L.factor = (tray > 0.0f) ? fmaf((1.0f - horizon) * vis, tray, horizon * vis) : horizon * vis;
         return L;
     }
+
     float exposure = env.exposure;
     float spot = env.spot_mult;
     L.bg = env.ambient_fill ? fmaxf(fmaf(0.012f, fmaf(d.y, 0.5f, 0.5f), 0.015f), 0.005f) * exposure
@@ -522,6 +589,26 @@ IX_DEV float lighting_radiance(const Lighting& L, const ix_environment& env, flo
     for (int i = 0; i < L.ring_len; ++i) r = fmaf(L.ring[i], spec, r);
     if (L.has_ground) return fmaf(L.horizon, r, L.ground * spec);
     return r;
+}
+
+// The escape radiance for every lighting model (sample_studio_environment_channels,
+// rig.rs:701): the studio rig, iso-hemisphere and uniform dome as direction_lighting /
+// lighting_radiance form them, the tent, dome, sun and ASET models beside them.  Only the
+// extended transport instantiation calls it, so the other instantiations' escape lookup
+// (and, through the interprocedural register allocation, their kernels) is unchanged.
+IX_DEV float environment_radiance_ext(const ix_environment& env, V3 dir, V3 observer, float lambda) {
+    const float spec = spectral_power_ext(env, lambda);
+    if (env.model == IX_ENV_STUDIO || env.model == IX_ENV_ISO_HEMISPHERE || env.model == IX_ENV_UNIFORM)
+        return lighting_radiance(direction_lighting(env, dir, observer), env, spec);
+    float bands[4];
+    const float factor = other_model_lighting(env, normalize(dir), observer, bands);
+    if (env.model != IX_ENV_ASET) return factor * (spec * env.exposure);
+    // DirectionLighting::Banded (rig.rs:140): `spec` is the wavelength.
+    const float r = (bands[0] * aset_band(spec, 610.0f)) * 8.0f;
+    const float g = (bands[1] * aset_band(spec, 540.0f)) * 5.0f;
+    const float b = (bands[2] * aset_band(spec, 460.0f)) * 16.0f;
+    const float zones = ((r + g) + b) * env.exposure;
+    return bands[3] > 0.0f ? fmaf(bands[3] * d65(spec), env.exposure, zones) : zones;
 }
 
 // ExitLighting (color/metrics/lighting.rs:137-209) and returned_or_reason

@@ -452,9 +452,8 @@ __global__ void IX_SFX(check_kernel)(const __grid_constant__ CheckLaunch L) {
             break;
         }
         case CHECK_ENV: {
-            const ix_environment& env = S.s.environment;
-            Lighting Lg = direction_lighting(env, v3(inf(0), inf(1), inf(2)), v3(inf(4), inf(5), inf(6)));
-            put(0, lighting_radiance(Lg, env, spectral_power(env, inf(3))));
+            put(0, environment_radiance_ext(S.s.environment, v3(inf(0), inf(1), inf(2)), v3(inf(4), inf(5), inf(6)),
+                                            inf(3)));
             break;
         }
         case CHECK_INTERSECT: {

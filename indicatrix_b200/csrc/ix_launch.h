@@ -20,6 +20,7 @@ enum : uint32_t {
     SCENE_ROUNDED = 16u,    // rounded facet edges (edge_rounding_radius > 0)
     SCENE_BIAXIAL = 32u,    // biaxial indicatrix (ix_material::biaxial, with anisotropic)
     SCENE_CONCAVE = 64u,    // concave tools carved out of the stone (ix_scene::n_tools > 0)
+    SCENE_ENV_EXTENDED = 128u,  // a lighting model past the studio rig and iso-hemisphere
 };
 inline bool absorption_present(const ix_absorption& a) {
     if (a.has_spline) return true;
@@ -54,20 +55,23 @@ inline uint32_t scene_flags(const ix_material& m) {
 // scene runs the uniaxial instantiation of the transport.
 inline bool needs_uniaxial_kernel(uint32_t flags) {
     return (flags & (SCENE_UNIAXIAL | SCENE_PLEOCHROIC | SCENE_SCATTERING | SCENE_ROUNDED | SCENE_BIAXIAL |
-                     SCENE_CONCAVE)) != 0;
+                     SCENE_CONCAVE | SCENE_ENV_EXTENDED)) != 0;
 }
 // The scene's flags: its material's, and whether tools carve it.
 inline uint32_t scene_flags(const ix_scene& s) {
-    return scene_flags(s.material) | (s.n_tools ? SCENE_CONCAVE : 0u);
+    const uint32_t m = s.environment.model;
+    const bool env_ext = (m != IX_ENV_STUDIO && m != IX_ENV_ISO_HEMISPHERE && m != IX_ENV_UNIFORM) ||
+                         s.environment.spectrum > IX_SPEC_FLAT;
+    return scene_flags(s.material) | (s.n_tools ? SCENE_CONCAVE : 0u) | (env_ext ? SCENE_ENV_EXTENDED : 0u);
 }
 // The transport instantiation a scene needs: the isotropic megakernel, the uniaxial one,
-// or the extended one -- the uniaxial bounce plus the out-of-line biaxial bounce and the
-// carved-stone intersection -- which serves every scene, so a batch takes the largest of
-// its scenes' classes.
+// or the extended one -- the uniaxial bounce plus the out-of-line biaxial bounce, the
+// carved-stone intersection and every lighting model -- which serves every scene, so a
+// batch takes the largest of its scenes' classes.
 enum TransportClass : int { TRANSPORT_ISOTROPIC = 0, TRANSPORT_UNIAXIAL = 1, TRANSPORT_EXTENDED = 2 };
 constexpr int N_TRANSPORT_CLASSES = 3;
 inline int transport_class(uint32_t flags) {
-    if (flags & (SCENE_BIAXIAL | SCENE_CONCAVE)) return TRANSPORT_EXTENDED;
+    if (flags & (SCENE_BIAXIAL | SCENE_CONCAVE | SCENE_ENV_EXTENDED)) return TRANSPORT_EXTENDED;
     return needs_uniaxial_kernel(flags) ? TRANSPORT_UNIAXIAL : TRANSPORT_ISOTROPIC;
 }
 

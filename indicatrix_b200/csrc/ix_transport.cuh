@@ -475,19 +475,33 @@ static __device__ __noinline__ float lane_environment(const ix_environment& env,
     Lighting L = direction_lighting(env, dir, observer);
     return lighting_radiance(L, env, spectral_power(env, lambda));
 }
+// Every lighting model's escape radiance (environment_radiance_ext), out of line, for
+// the extended instantiation only.
+static __device__ __noinline__ float lane_environment_ext(const ix_environment& env, V3 dir, V3 observer,
+                                                         float lambda) {
+    return environment_radiance_ext(env, dir, observer, lambda);
+}
+template <int UNI>
+IX_DEV float lane_env(const ix_environment& env, V3 dir, V3 observer, float lambda) {
+    if constexpr (UNI == TRANSPORT_EXTENDED)
+        return lane_environment_ext(env, dir, observer, lambda);
+    else
+        return lane_environment(env, dir, observer, lambda);
+}
 
 enum BounceResult { BOUNCE_CONTINUE = 0, BOUNCE_ESCAPED = 1, BOUNCE_KILLED = 2 };
 
 // try_split_exit_channel (refraction/exit_split.rs:128): at an exit, each diverging live
 // channel probes its own refracted direction `dir_k`; the group scans each probe
 // together and the probing lane adds its transmitted intensity times the radiance found.
+template <int UNI = TRANSPORT_ISOTROPIC>
 IX_DEV void group_exit_probes(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes,
                               V3 hit_point, bool want_probe, V3 dir_k, float t_intensity) {
     // A probe leaving through the exit facet itself cannot meet the stone: its channel
     // goes straight to the environment, every such lane at once.
     const bool clear = want_probe && leaves_stone_through(planes, P.facet, hit_point + dir_k * 1e-4f, dir_k);
     if (clear) {
-        const float e = lane_environment(S.s.environment, dir_k, P.observer, P.lambda);
+        const float e = lane_env<UNI>(S.s.environment, dir_k, P.observer, P.lambda);
         P.split = fmaf(fmaxf(t_intensity, 0.0f), e, P.split);
     }
     unsigned probes = (__ballot_sync(g.mask, want_probe && !clear) >> (threadIdx.x & 24u)) & 0xFFu;
@@ -497,7 +511,7 @@ IX_DEV void group_exit_probes(const Group& g, LanePath& P, const DevScene& S, co
         const V3 dj = v3(gshfl(g, dir_k.x, j), gshfl(g, dir_k.y, j), gshfl(g, dir_k.z, j));
         const Hit ph = probe_intersect(g, planes, (int)S.s.n_planes, hit_point + dj * 1e-4f, dj);
         if (ph.facet < 0 && g.c == j) {
-            const float e = lane_environment(S.s.environment, dj, P.observer, P.lambda);
+            const float e = lane_env<UNI>(S.s.environment, dj, P.observer, P.lambda);
             P.split = fmaf(fmaxf(t_intensity, 0.0f), e, P.split);
         }
     }
@@ -515,7 +529,7 @@ IX_DEV void group_exit_probes_carved(const Group& g, LanePath& P, const DevScene
         const CarvedHit ph = group_carved_hit(g, planes, (int)S.s.n_planes, S.s.tools, (int)S.s.n_tools,
                                               hit_point + dj * 1e-4f, dj);
         if (ph.facet < 0 && g.c == j) {
-            const float e = lane_environment(S.s.environment, dj, P.observer, P.lambda);
+            const float e = lane_env<TRANSPORT_EXTENDED>(S.s.environment, dj, P.observer, P.lambda);
             P.split = fmaf(fmaxf(t_intensity, 0.0f), e, P.split);
         }
     }
@@ -978,7 +992,7 @@ IX_DEV void bounce_exit_probes(const Group& g, LanePath& P, const DevScene& S, c
             return;
         }
     }
-    group_exit_probes(g, P, S, planes, hit_point, want_probe, dir_k, t_int);
+    group_exit_probes<UNI>(g, P, S, planes, hit_point, want_probe, dir_k, t_int);
 }
 
 template <int UNI>
@@ -990,7 +1004,7 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     const BounceHit bh = bounce_next_hit<UNI>(g, P, S, planes);
     const Hit hit = bh.hit;
     if (hit.facet < 0) {
-        esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
+        esc = fmaf(intensity(P.st), lane_env<UNI>(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         return BOUNCE_ESCAPED;
     }
     const V3 c_axis = load3(mat.c_axis);
@@ -1371,7 +1385,7 @@ static __device__ __noinline__ BiaxialStep group_bounce_biaxial(Group g, LanePat
     const BounceHit bh = bounce_next_hit<TRANSPORT_EXTENDED>(g, P, S, planes);
     const Hit hit = bh.hit;
     if (hit.facet < 0) {
-        out.esc = fmaf(intensity(P.st), lane_environment(sc.environment, P.d, P.observer, P.lambda), 0.0f);
+        out.esc = fmaf(intensity(P.st), lane_env<TRANSPORT_EXTENDED>(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         out.P = P;
         out.result = BOUNCE_ESCAPED;
         return out;

@@ -571,14 +571,30 @@ static F spectral_power(const ix_environment& env, F lambda_nm) {
     switch (env.spectrum) {
         case IX_SPEC_D65: return d65(lambda_nm);
         case IX_SPEC_BLACKBODY: return blackbody(env.bb_t_k, env.bb_denom_560, lambda_nm);
+        case IX_SPEC_GAUSSIAN: {  // IlluminantSpectrum::Gaussian (spectral.rs:137)
+            const F z = (lambda_nm - F(env.line_centre_nm)) / F(env.line_sigma_nm);
+            return exp_((F(-0.5f) * z) * z);
+        }
+        case IX_SPEC_WAVELENGTH: return lambda_nm;  // aset_spec_input (rig.rs:165)
         default: return 1.0f;
     }
 }
+// The tent, dome and ASET constants (rig.rs:67-85, :120-135, sun.rs:10-20).
+constexpr float TENT_KEY_OUTER_COS = 0.7660444f, TENT_KEY_INNER_COS = 0.9396926f;
+constexpr float SPARK_OUTER_COS = 0.9961947f, SPARK_INNER_COS = 0.9993908f;
+constexpr float CARD_OUTER_COS = 0.898794f, CARD_INNER_COS = 0.9612617f;
+constexpr int CARD_RING_SLOTS[3] = {4, 8, 12};
+constexpr float ASET_SIGMA_NM = 8.493218f;
+constexpr float ASET_EDGE_45_LO = 0.6871068f, ASET_EDGE_45_HI = 0.7271068f;
+constexpr float ASET_EDGE_75_LO = 0.9459258f, ASET_EDGE_75_HI = 0.9859258f;
+constexpr float SUN_DISC_COS = 0.9999889f;
+constexpr float SUN_RADIANCE = 40000.0f;
 // The direction-only part of the lighting (rig.rs:67-96, 157-170, 320-377), reduced to
 // how radiance(spec_power) is formed from it.
 struct Lighting {
-    int kind;  // 0 scaled, 1 rig, 2 uniform
+    int kind;  // 0 scaled, 1 rig, 2 uniform, 3 banded (ASET)
     F factor;
+    F red, green, blue, tray_ground;  // banded
     F bg, softbox, fill;
     bool has_softbox, has_fill;
     F ring[IX_RING_LIGHTS];
@@ -604,6 +620,62 @@ static Lighting direction_lighting(const ix_environment& env, V3 dir, V3 observe
             L.factor = fma_((F(1.0f) - horizon) * vis, tray, horizon * vis);
         else
             L.factor = horizon * vis;
+        return L;
+    }
+    // lit_ground (rig.rs:230): the tray below the horizon, else the model's own ground.
+    auto lit_ground = [&](F horizon, F vis, F own) {
+        return tray > F(0.0f) ? ((F(1.0f) - horizon) * vis) * tray : own * (F(1.0f) - horizon);
+    };
+    if (env.model == IX_ENV_LIGHT_TENT) {
+        // light_tent_lighting (rig.rs:254).
+        const F horizon = smoothstep(-0.05f, 0.05f, d.y);
+        F walls = fma_(0.08f, max_(d.y, 0.0f), 0.14f) * F(env.tent_walls);
+        if (F(env.tent_flat) > F(0.0f))
+            walls = fma_(F(0.18f) * F(env.tent_walls), env.tent_flat, walls * (F(1.0f) - F(env.tent_flat)));
+        F card = 0.0f;
+        for (int slot : CARD_RING_SLOTS)
+            card = max_(card, smoothstep(CARD_OUTER_COS, CARD_INNER_COS, dot(d, load3(env.ring_dirs[slot]))));
+        walls = walls * fma_(card * F(env.tent_cards), -0.9f, 1.0f);
+        const F key = smoothstep(TENT_KEY_OUTER_COS, TENT_KEY_INNER_COS, dot(d, load3(env.key_dir))) *
+                      (F(1.4f) * F(env.spot_mult));
+        const F spark = (smoothstep(SPARK_OUTER_COS, SPARK_INNER_COS, dot(d, load3(env.fill_dir))) *
+                         (F(5.0f) * F(env.spot_mult))) * F(env.tent_spark);
+        const F vis = F(1.0f) - smoothstep(env.shadow_cos[0], env.shadow_cos[1], dot(d, observer));
+        const F above = ((walls + key) + spark) * (horizon * vis);
+        L.factor = above + lit_ground(horizon, vis, env.tent_ground);
+        return L;
+    }
+    if (env.model == IX_ENV_DAYLIGHT_DOME || env.model == IX_ENV_DAYLIGHT_SUN) {
+        // daylight_dome_lighting (rig.rs:297) and daylight_sun_radiance (rig.rs:466): the
+        // sky, its aureole about the sun, and for DaylightSun the 0.27 degree disc.
+        const F horizon = smoothstep(-0.05f, 0.05f, d.y);
+        const F sun_dot = dot(d, load3(env.key_dir));
+        const F sky = fma_(0.08f, F(1.0f) - max_(d.y, 0.0f), 0.10f);
+        const F glow = max_(sun_dot, 0.0f);
+        const F glow2 = glow * glow;
+        const F glow4 = glow2 * glow2;
+        const F aureole = (glow4 * glow4) * F(0.30f);
+        const F vis = F(1.0f) - smoothstep(env.shadow_cos[0], env.shadow_cos[1], dot(d, observer));
+        const F above = (sky + aureole) * (horizon * vis);
+        const F ground = lit_ground(horizon, vis, 0.04f);
+        if (env.model == IX_ENV_DAYLIGHT_DOME) {
+            L.factor = above + ground;
+        } else {
+            const F sun = sun_dot >= F(SUN_DISC_COS) ? F(env.sun_factor) : F(0.0f);
+            L.factor = (above + ground) + sun;
+        }
+        return L;
+    }
+    if (env.model == IX_ENV_ASET) {
+        // aset_radiance (rig.rs:439): three elevation zones, banded at radiance time.
+        const F horizon = smoothstep(-0.05f, 0.05f, d.y);
+        const F s45 = smoothstep(ASET_EDGE_45_LO, ASET_EDGE_45_HI, d.y);
+        const F s75 = smoothstep(ASET_EDGE_75_LO, ASET_EDGE_75_HI, d.y);
+        L.kind = 3;
+        L.red = (s45 * (F(1.0f) - s75)) * horizon;
+        L.green = (F(1.0f) - s45) * horizon;
+        L.blue = s75 * horizon;
+        L.tray_ground = tray > F(0.0f) ? (F(1.0f) - horizon) * tray : F(0.0f);
         return L;
     }
     // Studio rig (rig.rs:320-377).
@@ -638,9 +710,22 @@ static Lighting direction_lighting(const ix_environment& env, V3 dir, V3 observe
     return L;
 }
 // DirectionLighting::radiance (rig.rs:112-155).
+static F aset_band(F lambda_nm, F centre_nm) {
+    const F z = (lambda_nm - centre_nm) / F(ASET_SIGMA_NM);
+    return exp_((F(-0.5f) * z) * z);
+}
 static F lighting_radiance(const Lighting& L, const ix_environment& env, F spec) {
     if (L.kind == 2) return F(env.uniform_radiance) * spec;
     if (L.kind == 0) return L.factor * (spec * F(env.exposure));
+    if (L.kind == 3) {
+        // DirectionLighting::Banded (rig.rs:140): `spec` is the wavelength.
+        const F r = (L.red * aset_band(spec, 610.0f)) * F(8.0f);
+        const F g = (L.green * aset_band(spec, 540.0f)) * F(5.0f);
+        const F b = (L.blue * aset_band(spec, 460.0f)) * F(16.0f);
+        const F zones = ((r + g) + b) * F(env.exposure);
+        if (L.tray_ground > F(0.0f)) return fma_(L.tray_ground * d65(spec), env.exposure, zones);
+        return zones;
+    }
     F r = L.bg * spec;
     if (L.has_softbox) r = fma_(L.softbox, spec, r);
     if (L.has_fill) r = fma_(L.fill, spec, r);
@@ -3623,23 +3708,49 @@ int ixo_environment_preset(int32_t preset, float exposure, float light_yaw, floa
                            float backdrop, float surface_glare, float head_shadow_deg,
                            ix_environment* out) {
     std::memset(out, 0, sizeof(*out));
-    float temp_k, spot;
-    bool d65_spec;
+    // LightingPreset::params / model / uses_d65 / uv_line (environment/mod.rs:318-560).
+    float temp_k = 6500.0f, spot = 1.0f;
+    float tent[5] = {1.0f, 1.0f, 1.0f, 0.02f, 0.0f};  // walls, cards, spark, ground, flat
+    bool d65_spec = true, uv = false;
+    float uv_centre = 0.0f, uv_fwhm = 0.0f;
     uint32_t model;
     switch (preset) {
-        case 1: model = IX_ENV_ISO_HEMISPHERE; temp_k = 6500.0f; spot = 1.0f; d65_spec = true; break;
-        case 7: model = IX_ENV_STUDIO; temp_k = 6500.0f; spot = 1.0f; d65_spec = true; break;
+        case 0: model = IX_ENV_LIGHT_TENT; temp_k = 5000.0f; d65_spec = false; break;
+        case 1: model = IX_ENV_ISO_HEMISPHERE; break;
+        case 2: model = IX_ENV_LIGHT_TENT; spot = 0.0f; tent[0] = 5.0f; tent[1] = 0.0f; tent[2] = 0.0f;
+                tent[3] = 0.8f; tent[4] = 1.0f; break;
+        case 3: model = IX_ENV_LIGHT_TENT; tent[0] = 3.0f; tent[1] = 0.0f; tent[3] = 0.05f; break;
+        case 4: model = IX_ENV_LIGHT_TENT; tent[0] = 0.4f; tent[1] = 0.0f; tent[2] = 0.0f; tent[3] = 0.03f; break;
+        case 5: model = IX_ENV_DAYLIGHT_DOME; break;
+        case 6: model = IX_ENV_DAYLIGHT_SUN; break;
+        case 7: model = IX_ENV_STUDIO; break;
         case 8: model = IX_ENV_STUDIO; temp_k = 3200.0f; spot = 1.2f; d65_spec = false; break;
         case 9: model = IX_ENV_STUDIO; temp_k = 2856.0f; spot = 1.2f; d65_spec = false; break;
         case 10: model = IX_ENV_STUDIO; temp_k = 5000.0f; spot = 1.6f; d65_spec = false; break;
         case 11: model = IX_ENV_STUDIO; temp_k = 6000.0f; spot = 2.4f; d65_spec = false; break;
+        case 12: model = IX_ENV_ASET; break;
+        case 13: model = IX_ENV_STUDIO; d65_spec = false; uv = true; uv_centre = 365.0f; uv_fwhm = 10.0f; break;
+        case 14: model = IX_ENV_STUDIO; d65_spec = false; uv = true; uv_centre = 395.0f; uv_fwhm = 12.0f; break;
         default: return -1;
     }
     out->model = model;
-    out->spectrum = d65_spec ? IX_SPEC_D65 : IX_SPEC_BLACKBODY;
+    out->spectrum = model == IX_ENV_ASET ? IX_SPEC_WAVELENGTH
+                    : uv                 ? IX_SPEC_GAUSSIAN
+                    : d65_spec           ? IX_SPEC_D65
+                                         : IX_SPEC_BLACKBODY;
+    if (uv) {
+        out->line_centre_nm = uv_centre;
+        // fwhm / (2 sqrt(2 ln 2)) in f32 (mod.rs:560).
+        out->line_sigma_nm = uv_fwhm / (2.0f * std::sqrt(2.0f * 0.6931472f));
+    }
+    out->tent_walls = tent[0];
+    out->tent_cards = tent[1];
+    out->tent_spark = tent[2];
+    out->tent_ground = tent[3];
+    out->tent_flat = tent[4];
     out->exposure = exposure;
     out->spot_mult = spot;
-    out->ambient_fill = 1;
+    out->ambient_fill = uv ? 0 : 1;
     out->backdrop = backdrop;
     // clamp_surface_glare (environment/source.rs:170).
     out->surface_glare = (surface_glare >= 1.0f || std::isnan(surface_glare)) ? 1.0f
@@ -3680,8 +3791,11 @@ int ixo_environment_preset(int32_t preset, float exposure, float light_yaw, floa
         store3(out->ring_dirs[i],
                normalize(v3(sin_(angle) * F(0.75f), sin_pitch * F(0.8f), cos_(angle) * F(0.75f))));
     }
-    // illuminant_white_balance (color.rs:328): identity unless the preset uses one.
-    if (!d65_spec) {
+    // sun_radiance_factor (sun.rs:25): the disc's radiance, faded below the horizon.
+    out->sun_factor = raw(F(SUN_RADIANCE) * smoothstep(-0.05f, 0.05f, F(out->key_dir[1])));
+    // illuminant_white_balance (color.rs:328): identity unless the preset uses one
+    // (uses_white_balance, mod.rs:553: neither D65 nor a UV lamp nor the ASET view).
+    if (!d65_spec && !uv && model != IX_ENV_ASET) {
         out->white_balance = 1;
         store3(out->wb_lms, illuminant_white_balance(temp_k));
     } else {
