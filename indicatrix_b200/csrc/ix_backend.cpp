@@ -537,14 +537,10 @@ int ix_scene_routes_to_gpu(const ix_scene* s) {
     // The UV lamps are fluorescence sources; their scenes never reach the GPU
     // (gpu_backend/mod.rs:288-298).
     if (e.spectrum == IX_SPEC_GAUSSIAN) return 0;
-    // DaylightSun enables next-event estimation at frosted facets and scattering events
-    // (environment_supports_nee, environment/nee.rs:60), which this path does not carry:
-    // such scenes decline; a polished, clear stone takes no light sample and is traced.
-    if (e.model == IX_ENV_DAYLIGHT_SUN) {
-        if (m.scattering_sigma_s > 0.0f) return 0;
-        for (uint32_t i = 0; s->facet_finishes && i < s->n_finishes; ++i)
-            if (s->facet_finishes[i]) return 0;
-    }
+    // DaylightSun enables next-event estimation (environment_supports_nee,
+    // environment/nee.rs:60): the frosted facets' light samples are traced; those of
+    // Henyey-Greenstein scattering events are not, so a scattering stone declines.
+    if (e.model == IX_ENV_DAYLIGHT_SUN && m.scattering_sigma_s > 0.0f) return 0;
     if (m.dispersion.kind > IX_DISP_CAUCHY) return 0;
     // A biaxial indicatrix is traced as the anisotropic transport's biaxial arm; an
     // isotropic material carrying one (the reference's eigen-polarisation mean of the

@@ -175,7 +175,7 @@ IX_DEV uint32_t trace_task(const Group& g, const DevScene& S, const float4* __re
         }
         if (r == BOUNCE_CONTINUE && P.bounce < max_bounces) continue;
         // The path finished (escaped, roulette, or reached the bounce cap).
-        const V3 xyz = group_finish(g, P, S, r == BOUNCE_ESCAPED, esc);
+        const V3 xyz = group_finish<UNI>(g, P, S, r == BOUNCE_ESCAPED, esc);
         if constexpr (ATTR) {
             if (g.c == 0) {
                 const size_t rec = (size_t)(q - cur_j * spp) * at->stride + at->pixel0 + cur_j;

@@ -171,7 +171,7 @@ IX_DEV uint32_t pool_loop(const Group& g, uint32_t* counter, uint32_t total_chun
         const int r = capped ? (int)BOUNCE_KILLED : group_step<UNI>(g, P, S, planes, esc);
         if (r == BOUNCE_CONTINUE && P.bounce < max_bounces) continue;
         // The path finished (escaped, roulette, or reached the bounce cap).
-        const V3 xyz = group_finish(g, P, S, r == BOUNCE_ESCAPED, esc);
+        const V3 xyz = group_finish<UNI>(g, P, S, r == BOUNCE_ESCAPED, esc);
         drops += add_sample_fixed(g, J.acc + (size_t)row * FIXED_WORDS, xyz);
         busy = false;
     }

@@ -86,6 +86,12 @@ struct LanePath {
                        // channel's beta-ray absorption (biaxial paths use no e index)
     float n_e_hero;    // channel 0's
     float alpha_e;     // e-ray (gamma-ray) absorption of channel c
+    // Extended transport under the DaylightSun model only: the radiance next-event
+    // estimation deposited so far, and the BSDF pdf of the last frosted light-sampled
+    // bounce's continuation (pending_light_mis, bounce_body.rs:202), read by the next escape.
+    float nee_rad;
+    float carry_pdf;
+    bool has_carry;
 };
 
 // ------------------------------------------------------------------------------------
@@ -380,6 +386,9 @@ IX_DEV void group_init_ray(const Group& g, LanePath& P, const DevScene& S, Ray r
         P.n_e_hero = gshfl(g, P.n_e, 0);
         P.alpha_e = S.absorbing ? spectral_absorption(sc.material.abs_e, P.lambda) : 0.0f;
         if constexpr (UNI == TRANSPORT_EXTENDED) {
+            P.nee_rad = 0.0f;
+            P.carry_pdf = 0.0f;
+            P.has_carry = false;
             if (S.biaxial)  // the beta-ray alpha; the alpha ray's without beta bands (wavelength_cache.rs:37-52)
                 P.n_e = (S.absorbing && sc.material.has_abs_beta) ? spectral_absorption(sc.material.abs_beta, P.lambda)
                                                                   : P.alpha;
@@ -575,10 +584,10 @@ IX_DEV Stokes lane_scalar_reflect(LanePath& P, float n1k, float n2k, float s2k, 
 }
 
 // ------------------------------------------------------------------------------------
-// Frosted (bruted) facets: apply_frosted_bounce (optics/raytracer/scattering/frosted.rs:289)
-// without next-event estimation, which the reference enables only for an HDR map or the
-// DaylightSun model (environment_supports_nee, environment/nee.rs:60), neither of which
-// this path carries.
+// Frosted (bruted) facets: apply_frosted_bounce (optics/raytracer/scattering/frosted.rs:289).
+// Next-event estimation, which the reference enables for an HDR map or the DaylightSun
+// model (environment_supports_nee, environment/nee.rs:60), runs under DaylightSun in the
+// extended transport instantiation (frosted_sun_nee below); HDR maps are not carried.
 // ------------------------------------------------------------------------------------
 constexpr uint32_t FROSTED_DIR_U_STREAM = 0x27D4EB2Fu;  // sampling.rs:24
 constexpr uint32_t FROSTED_DIR_V_STREAM = 0x165667B1u;  // sampling.rs:25
@@ -634,6 +643,79 @@ static __device__ __noinline__ FrostedScatter frosted_scatter(uint32_t seed, uin
 IX_DEV void lane_frosted_apply(LanePath& P, const FrostedScatter& f) {
     P.pdf = P.pdf * f.pdf_factor;
     P.st = Stokes{intensity(P.st), 0.0f, 0.0f, 0.0f};
+}
+
+// nee_contribution_frosted_exterior (scattering/frosted.rs:98) under DaylightSun: one
+// direction drawn uniformly over the sun's disc (sun_cone_direction, environment/sun.rs:70,
+// with 1 - cos kept exact), rejected behind the facet and, on a carved stone, when a shadow
+// probe from 1e-4 along it meets the stone; weighted by the balance heuristic against the
+// Lambertian cos / pi density the diffuse draw has there.  Returns the channel's deposit,
+// (I * common) * (sun factor * (spd * exposure)), or 0.  The 8 lanes share the direction
+// and every decision (the hit point, normal and draws are the path's), so the group enters
+// the shadow probe together.  Out of line: the extended instantiation's frosted arms only.
+constexpr uint32_t FROSTED_NEE_ENV_DIR_U_STREAM = 0x6A09E667u;  // sampling.rs:52
+constexpr uint32_t FROSTED_NEE_ENV_DIR_V_STREAM = 0xBB67AE85u;  // sampling.rs:53
+constexpr float SUN_ONE_MINUS_COS = 1.1086464e-5f;              // 186 x 2^-24, sun.rs:55
+constexpr float SUN_SOLID_ANGLE = 6.965831e-5f;                 // 2 pi x SUN_ONE_MINUS_COS, sun.rs:57
+IX_DEV V3 sun_cone_direction(V3 key, float u0, float u1) {
+    const float one_minus_cos = u0 * SUN_ONE_MINUS_COS;
+    const float cos_t = 1.0f - one_minus_cos;
+    const float sin_t = sqrtf(fmaxf(one_minus_cos * (2.0f - one_minus_cos), 0.0f));
+    float sin_p, cos_p;
+    sincosf((2.0f * 3.14159265358979323846f) * u1, &sin_p, &cos_p);
+    const V3 a = fabsf(key.x) > 0.9f ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
+    const V3 t = normalize_or_zero(a - key * dot(key, a));
+    const V3 b = cross(key, t);
+    return normalize_or_zero((t * (sin_t * cos_p) + b * (sin_t * sin_p)) + key * cos_t);
+}
+// balance_heuristic (scattering/mod.rs:102).
+IX_DEV float balance_heuristic(float a, float b) {
+    const float denom = a + b;
+    return denom > 1e-12f ? a / denom : 0.0f;
+}
+// environment_nee_pdf (environment/nee.rs:144) for the sun: uniform over its disc.
+IX_DEV float sun_nee_pdf(const ix_environment& env, V3 dir) {
+    return dot(dir, load3(env.key_dir)) >= SUN_DISC_COS ? 1.0f / SUN_SOLID_ANGLE : 0.0f;
+}
+static __device__ __noinline__ float frosted_sun_nee(Group g, DevScene S, const float4* __restrict__ planes,
+                                                     uint32_t seed, uint32_t bounce, V3 origin, V3 ext_normal,
+                                                     float lambda, float intensity_now) {
+    const ix_environment& env = S.s.environment;
+    const float u0 = unit_draw(seed, bounce, FROSTED_NEE_ENV_DIR_U_STREAM);
+    const float u1 = unit_draw(seed, bounce, FROSTED_NEE_ENV_DIR_V_STREAM);
+    const V3 dir = sun_cone_direction(load3(env.key_dir), u0, u1);
+    const float pdf = 1.0f / SUN_SOLID_ANGLE;
+    const float cos_light = dot(dir, ext_normal);
+    if (cos_light <= 0.0f) return 0.0f;
+    if (S.concave) {
+        const CarvedHit h = group_carved_hit(g, planes, (int)S.s.n_planes, S.s.tools, (int)S.s.n_tools,
+                                             origin + dir * 1e-4f, dir);
+        if (h.facet >= 0) return 0.0f;
+    }
+    const float brdf_pdf = cos_light / 3.14159265358979323846f;
+    const float mis = balance_heuristic(pdf, brdf_pdf);
+    if (mis <= 0.0f) return 0.0f;
+    const float common = (brdf_pdf * mis) / pdf;
+    const float env_k = env.sun_factor * (spectral_power_ext(env, lambda) * env.exposure);
+    return (intensity_now * common) * env_k;
+}
+// The exterior-side frosted events (the reflect of an outside hit, the transmit of an
+// inside one; apply_frosted_bounce's NEE eligibility) under DaylightSun: the deposit and
+// the carry the next escape weighs itself with.  `normal` faces the incident side.
+IX_DEV void frosted_exterior_event(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes,
+                                   const FrostedScatter& f, bool inside0, V3 normal, V3 hit_point, uint32_t bounce) {
+    if (S.s.environment.model != IX_ENV_DAYLIGHT_SUN || (f.transmit ? !inside0 : inside0)) return;
+    const V3 ext_normal = f.transmit ? -normal : normal;
+    P.nee_rad = frosted_sun_nee(g, S, planes, P.seed, bounce, hit_point, ext_normal, P.lambda, intensity(P.st)) +
+                P.nee_rad;
+    P.has_carry = true;
+    P.carry_pdf = dot(f.dir, ext_normal) / 3.14159265358979323846f;
+}
+// The escape of the extended instantiation: the carried balance weight against the sun's
+// light samples (handle_miss, bounce_body/miss.rs:40), folded onto the deposits so far.
+IX_DEV float escape_with_carry(const LanePath& P, const ix_environment& env, float radiance) {
+    const float mis = P.has_carry ? balance_heuristic(P.carry_pdf, sun_nee_pdf(env, P.d)) : 1.0f;
+    return fmaf(intensity(P.st) * mis, radiance, P.nee_rad);
 }
 
 // ------------------------------------------------------------------------------------
@@ -700,7 +782,10 @@ struct ScatterResult {
 };
 // One channel of the segment's free-flight draw (the hero's extinction decides, through
 // lane 0 of the group; every lane takes the same branch).  Out of line and by value, like
-// frosted_scatter, so the bounce around the call compiles as it does without it.
+// frosted_scatter, so the bounce around the call compiles as it does without it; one copy
+// per transport instantiation (UNI), so the extended one's callers leave the uniaxial
+// kernels' copy, and its register allocation, alone.
+template <int UNI>
 static __device__ __noinline__ ScatterResult scatter_or_survive(Group g, uint32_t seed, uint32_t bounce, float alpha,
                                                                 float sigma_s_model, float path_scale, float g_hg,
                                                                 float hit_t, float intensity_now, V3 forward) {
@@ -1004,9 +1089,14 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     const BounceHit bh = bounce_next_hit<UNI>(g, P, S, planes);
     const Hit hit = bh.hit;
     if (hit.facet < 0) {
-        esc = fmaf(intensity(P.st), lane_env<UNI>(sc.environment, P.d, P.observer, P.lambda), 0.0f);
+        if constexpr (UNI == TRANSPORT_EXTENDED)
+            esc = escape_with_carry(P, sc.environment, lane_env<UNI>(sc.environment, P.d, P.observer, P.lambda));
+        else
+            esc = fmaf(intensity(P.st), lane_env<UNI>(sc.environment, P.d, P.observer, P.lambda), 0.0f);
         return BOUNCE_ESCAPED;
     }
+    // pending_light_mis.take() (bounce_body.rs:372): only this iteration's escape reads it.
+    if constexpr (UNI == TRANSPORT_EXTENDED) P.has_carry = false;
     const V3 c_axis = load3(mat.c_axis);
     const bool aniso = S.aniso != 0;
     // The channel's alpha along the wave normal: the assigned eigenmode's field for a
@@ -1023,7 +1113,7 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
     };
     if (S.scattering && P.inside) {
         // The interior segment may end in a scattering event first (bounce_body.rs:408-417).
-        const ScatterResult r = scatter_or_survive(g, P.seed, bounce, S.absorbing ? channel_alpha(P.k) : 0.0f,
+        const ScatterResult r = scatter_or_survive<UNI>(g, P.seed, bounce, S.absorbing ? channel_alpha(P.k) : 0.0f,
                                                    mat.scattering_sigma_s, mat.absorption_path_scale,
                                                    mat.scattering_g, hit.t, intensity(P.st), P.d);
         P.pdf = P.pdf * r.pdf_factor;
@@ -1134,6 +1224,8 @@ IX_DEV int group_bounce_uniaxial(const Group& g, LanePath& P, const DevScene& S,
             new_inside = !inside0;
             if (!inside0 && aniso) update = unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f ? 1 : 0;
         }
+        if constexpr (UNI == TRANSPORT_EXTENDED)
+            frosted_exterior_event(g, P, S, planes, f, inside0, normal, hit_point, bounce);
     } else if (sin2_t > 1.0f) {
         // apply_tir_bounce (tir.rs:41): forced reflection.
         if (nondeg) {
@@ -1385,11 +1477,13 @@ static __device__ __noinline__ BiaxialStep group_bounce_biaxial(Group g, LanePat
     const BounceHit bh = bounce_next_hit<TRANSPORT_EXTENDED>(g, P, S, planes);
     const Hit hit = bh.hit;
     if (hit.facet < 0) {
-        out.esc = fmaf(intensity(P.st), lane_env<TRANSPORT_EXTENDED>(sc.environment, P.d, P.observer, P.lambda), 0.0f);
+        out.esc = escape_with_carry(P, sc.environment,
+                                    lane_env<TRANSPORT_EXTENDED>(sc.environment, P.d, P.observer, P.lambda));
         out.P = P;
         out.result = BOUNCE_ESCAPED;
         return out;
     }
+    P.has_carry = false;  // pending_light_mis.take() (bounce_body.rs:372)
     const BiaxFrame F = biax_frame(load3(mat.c_axis));
     const Indicatrix hero = make_indicatrix(mat, P.n_hero), own = make_indicatrix(mat, P.n);
     // channel_absorption_alphas_assigned (absorption.rs:227): the hero indicatrix's
@@ -1400,7 +1494,8 @@ static __device__ __noinline__ BiaxialStep group_bounce_biaxial(Group g, LanePat
         return biaxial_quadratic_form(F, P.alpha, P.n_e, P.alpha_e, e);
     };
     if (S.scattering && P.inside) {
-        const ScatterResult r = scatter_or_survive(g, P.seed, bounce, S.absorbing ? channel_alpha(P.k) : 0.0f,
+        const ScatterResult r =
+            scatter_or_survive<TRANSPORT_EXTENDED>(g, P.seed, bounce, S.absorbing ? channel_alpha(P.k) : 0.0f,
                                                    mat.scattering_sigma_s, mat.absorption_path_scale,
                                                    mat.scattering_g, hit.t, intensity(P.st), P.d);
         P.pdf = P.pdf * r.pdf_factor;
@@ -1486,6 +1581,7 @@ static __device__ __noinline__ BiaxialStep group_bounce_biaxial(Group g, LanePat
             new_inside = !inside0;
             if (!inside0) update = unit_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f ? 1 : 0;
         }
+        frosted_exterior_event(g, P, S, planes, f, inside0, normal, hit_point, bounce);
     } else if (sin2_t > 1.0f) {
         // apply_tir_bounce's scalar arm (tir.rs:98-116); the reflected wave normal's mode
         // walks off (poynting_dir_for_mode, geometry.rs:440).
@@ -1583,20 +1679,30 @@ static __device__ __noinline__ BiaxialStep group_bounce_biaxial(Group g, LanePat
     return out;
 }
 
+// The extended instantiation's uniaxial bounce, out of line and by value like the biaxial
+// one: every kernel (task loop, pool, per-path check) then runs the same compiled bounce, so
+// the fast build's multiply-add contraction, and with it each path's result, is the same
+// whichever kernel traces the path.
+static __device__ __noinline__ BiaxialStep group_bounce_extended(Group g, LanePath P, DevScene S,
+                                                                  const float4* __restrict__ planes) {
+    BiaxialStep out{P, 0.0f, BOUNCE_CONTINUE};
+    out.result = group_bounce_uniaxial<TRANSPORT_EXTENDED>(g, P, S, planes, out.esc);
+    out.P = P;
+    return out;
+}
+
 // UNI is the transport instantiation (transport_class): TRANSPORT_ISOTROPIC the isotropic
-// megakernel, TRANSPORT_UNIAXIAL the uniaxial bounce, TRANSPORT_EXTENDED the uniaxial bounce
-// plus the out-of-line biaxial one (kept out of the uniaxial kernels, whose register
-// allocation the call site would change).
+// megakernel, TRANSPORT_UNIAXIAL the uniaxial bounce, TRANSPORT_EXTENDED the out-of-line
+// uniaxial and biaxial bounces (kept out of the uniaxial kernels, whose register allocation
+// the call sites would change).
 template <int UNI>
 IX_DEV int group_step(const Group& g, LanePath& P, const DevScene& S, const float4* __restrict__ planes, float& esc) {
     if constexpr (UNI == TRANSPORT_EXTENDED) {
-        if (S.biaxial) {
-            const BiaxialStep r = group_bounce_biaxial(g, P, S, planes);
-            P = r.P;
-            esc = r.esc;
-            return r.result;
-        }
-        return group_bounce_uniaxial<UNI>(g, P, S, planes, esc);
+        const BiaxialStep r =
+            S.biaxial ? group_bounce_biaxial(g, P, S, planes) : group_bounce_extended(g, P, S, planes);
+        P = r.P;
+        esc = r.esc;
+        return r.result;
     } else if constexpr (UNI == TRANSPORT_UNIAXIAL) {
         return group_bounce_uniaxial<UNI>(g, P, S, planes, esc);
     } else {
@@ -1608,6 +1714,9 @@ IX_DEV int group_step(const Group& g, LanePath& P, const DevScene& S, const floa
 // each channel over its MIS family (optics/raytracer/color.rs:145), apply the Bradford
 // round trip for studio environments (color.rs:252) and floor at zero.  Every lane of
 // the group returns the path's XYZ.
+// `esc` is the escape radiance (with the extended instantiation's next-event deposits
+// folded in); a path that did not escape keeps only those deposits.
+template <int UNI = TRANSPORT_ISOTROPIC>
 IX_DEV V3 group_finish(const Group& g, const LanePath& P, const DevScene& S, bool escaped, float esc) {
     // family pdf: the sum, in ascending channel order, over this channel's family.
     float family = 0.0f;
@@ -1622,7 +1731,11 @@ IX_DEV V3 group_finish(const Group& g, const LanePath& P, const DevScene& S, boo
         }
     }
     const float w = (family <= 1e-12f) ? 1.0f : (8.0f * pdf0) / family;
-    const float rad = escaped ? esc + P.split : 0.0f;
+    float rad;
+    if constexpr (UNI == TRANSPORT_EXTENDED)
+        rad = escaped ? esc + P.split : P.nee_rad;
+    else
+        rad = escaped ? esc + P.split : 0.0f;
     const float s = (rad * w) * (50.0f / 106.856f);
     const V3 c = cmf(P.lambda);
     const float cx = c.x * s, cy = c.y * s, cz = c.z * s;
@@ -1665,7 +1778,7 @@ IX_DEV V3 group_trace(const Group& g, LanePath& P, const DevScene& S, const floa
         if (r != BOUNCE_CONTINUE) break;
     }
     if (iterations) *iterations = it;
-    return group_finish(g, P, S, r == BOUNCE_ESCAPED, esc);
+    return group_finish<UNI>(g, P, S, r == BOUNCE_ESCAPED, esc);
 }
 
 }  // namespace ix

@@ -231,6 +231,8 @@ static inline uint32_t reverse_bits(uint32_t v) {
 // `(x as f32) / 4_294_967_295.0`: the literal rounds to 2^32 in f32.
 static inline F unit_from_hash(uint32_t h) { return fromu(h) / F(4294967296.0f); }
 // unit_draw (transport/inner/bounce_body.rs:71-73), the per-bounce stream draw.
+constexpr uint32_t FROSTED_NEE_ENV_DIR_U_STREAM = 0x6A09E667u;  // sampling.rs:52
+constexpr uint32_t FROSTED_NEE_ENV_DIR_V_STREAM = 0xBB67AE85u;  // sampling.rs:53
 static inline F unit_draw(uint32_t seed, uint32_t bounce, uint32_t stream) {
     return unit_from_hash(hash_u32(seed ^ hash_u32(bounce ^ stream)));
 }
@@ -589,6 +591,8 @@ constexpr float ASET_EDGE_45_LO = 0.6871068f, ASET_EDGE_45_HI = 0.7271068f;
 constexpr float ASET_EDGE_75_LO = 0.9459258f, ASET_EDGE_75_HI = 0.9859258f;
 constexpr float SUN_DISC_COS = 0.9999889f;
 constexpr float SUN_RADIANCE = 40000.0f;
+constexpr float SUN_ONE_MINUS_COS = 1.1086464e-5f;  // 186 x 2^-24
+constexpr float SUN_SOLID_ANGLE = 6.965831e-5f;
 // The direction-only part of the lighting (rig.rs:67-96, 157-170, 320-377), reduced to
 // how radiance(spec_power) is formed from it.
 struct Lighting {
@@ -1921,6 +1925,8 @@ struct Path {
     bool absorbing;
     bool aniso;
     bool biaxial;     // biaxial indicatrix (cache.hero_indicatrix.is_some())
+    bool has_carry;   // pending_light_mis: the BSDF pdf of the last light-sampled bounce's
+    F carry_pdf;      // continuation, consumed by the next escape (bounce_body.rs:372)
     TensorFrame ax;   // principal / absorption frame of the optic (gamma) axis
     bool is_e;  // the eigenmode assigned at the last entry (or by internal coupling)
     V3 c_axis;  // the material's optic axis as stored (RayMaterialContext::c_axis)
@@ -2422,9 +2428,10 @@ static void apply_uniaxial_internal(Path& P, const Geo& g, V3 k, V3 normal, V3 h
 
 // apply_absorption (raytracer/absorption.rs:99-197): the mean over the two eigenmodes
 // for an isotropic material, the assigned eigenmode's field for a uniaxial one.
-// Frosted facets (optics/raytracer/scattering/frosted.rs, scattering/mod.rs:110) without
-// next-event estimation, which the modelled environments do not enable
-// (environment_supports_nee, environment/nee.rs:60: DaylightSun and HDR maps only).
+// Frosted facets (optics/raytracer/scattering/frosted.rs, scattering/mod.rs:110), with
+// next-event estimation toward the sun under DaylightSun, the one modelled environment
+// that enables it (environment_supports_nee, environment/nee.rs:60; HDR maps are not
+// modelled).
 static const uint32_t FROSTED_DIR_U_STREAM = 0x27D4EB2Fu;  // sampling.rs:24
 static const uint32_t FROSTED_DIR_V_STREAM = 0x165667B1u;  // sampling.rs:25
 
@@ -2467,7 +2474,57 @@ static V3 cosine_weighted_hemisphere(F u1, F u2, V3 n) {
 // (always reflection past the hero's critical angle); every channel is depolarised and
 // its path pdf takes the chosen branch's probability.  An anisotropic entry draws its
 // eigenmode with probability one half.
-static void apply_frosted_bounce(Path& P, const Geo& g, V3 normal, uint32_t bounce, Outcome* o) {
+// sun_cone_direction (environment/sun.rs:70): a direction uniform in the sun's cone.
+static V3 sun_cone_direction(V3 key, F u0, F u1) {
+    const F one_minus_cos = u0 * F(SUN_ONE_MINUS_COS);
+    const F cos_t = F(1.0f) - one_minus_cos;
+    const F sin_t = sqrt_(max_(one_minus_cos * (F(2.0f) - one_minus_cos), 0.0f));
+    const F phi = F(2.0f * 3.14159265358979323846f) * u1;
+    const F sin_p = sin_(phi), cos_p = cos_(phi);
+    const V3 a = abs_(key.x) > F(0.9f) ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
+    const V3 t = normalize_or_zero(a - key * dot(key, a));
+    const V3 b = cross(key, t);
+    return normalize_or_zero((t * (sin_t * cos_p) + b * (sin_t * sin_p)) + key * cos_t);
+}
+// balance_heuristic (scattering/mod.rs:102).
+static F balance_heuristic(F a, F b) {
+    const F denom = a + b;
+    return denom > F(1e-12f) ? a / denom : F(0.0f);
+}
+// environment_nee_pdf (environment/nee.rs:144) for DaylightSun: uniform over the disc.
+static F sun_nee_pdf(const ix_environment& env, V3 dir) {
+    return dot(dir, load3(env.key_dir)) >= F(SUN_DISC_COS) ? F(1.0f) / F(SUN_SOLID_ANGLE) : F(0.0f);
+}
+// nee_contribution_frosted_exterior (scattering/frosted.rs:98) for the DaylightSun sky:
+// one sun-cone light sample, a shadow probe on a carved stone, the balance heuristic
+// against the Lambertian cos / pi density, deposited into every channel's radiance.
+static void frosted_sun_nee(Path& P, V3 origin, V3 ext_normal, uint32_t bounce) {
+    const ix_environment& env = P.sc->environment;
+    const F u0 = unit_draw(P.seed, bounce, FROSTED_NEE_ENV_DIR_U_STREAM);
+    const F u1 = unit_draw(P.seed, bounce, FROSTED_NEE_ENV_DIR_V_STREAM);
+    const V3 dir = sun_cone_direction(load3(env.key_dir), u0, u1);
+    const F pdf = F(1.0f) / F(SUN_SOLID_ANGLE);
+    const F cos_light = dot(dir, ext_normal);
+    if (cos_light <= F(0.0f)) return;
+    if (P.sc->n_tools && P.sc->tools) {
+        Hit h;
+        bool carved, entering;
+        if (intersect_scene(P.sc, Ray{origin + dir * F(1e-4f), dir}, &h, &carved, &entering)) return;
+    }
+    const F brdf_pdf = cos_light / F(3.14159265358979323846f);
+    const F mis = balance_heuristic(pdf, brdf_pdf);
+    if (mis <= F(0.0f)) return;
+    const F common = (brdf_pdf * mis) / pdf;
+    for (int c = 0; c < 8; ++c) {
+        // EnvNeeSample::radiance (environment/nee.rs:47): geometry x (spd x exposure).
+        const F env_k = F(env.sun_factor) * (spectral_power(env, P.lambdas[c]) * F(env.exposure));
+        P.radiance[c] = ((intensity(P.stokes[c]) * common) * env_k) + P.radiance[c];
+    }
+}
+static void apply_frosted_bounce(Path& P, const Geo& g, V3 normal, V3 hit_point, uint32_t bounce, Outcome* o) {
+    // NEE is on under DaylightSun (environment_supports_nee, nee.rs:60); the reflect of an
+    // outside hit and the transmit of an inside one are the exterior-side events.
+    const bool nee = P.sc->environment.model == IX_ENV_DAYLIGHT_SUN;
     const F u1 = unit_draw(P.seed, bounce, FROSTED_DIR_U_STREAM);
     const F u2 = unit_draw(P.seed, bounce, FROSTED_DIR_V_STREAM);
     o->update = -1;
@@ -2491,6 +2548,11 @@ static void apply_frosted_bounce(Path& P, const Geo& g, V3 normal, uint32_t boun
             P.stokes[c] = unpolarized(intensity(P.stokes[c]));
             P.path_pdf[c] = P.path_pdf[c] * r_unpol;
         }
+        if (nee && !P.inside) {
+            frosted_sun_nee(P, hit_point, normal, bounce);
+            P.has_carry = true;
+            P.carry_pdf = dot(d, normal) / F(3.14159265358979323846f);
+        }
         o->new_k = o->new_s = d;
         o->new_inside = P.inside;
         return;
@@ -2502,6 +2564,11 @@ static void apply_frosted_bounce(Path& P, const Geo& g, V3 normal, uint32_t boun
     for (int c = 0; c < 8; ++c) {
         P.stokes[c] = unpolarized(intensity(P.stokes[c]));
         P.path_pdf[c] = P.path_pdf[c] * t_unpol;
+    }
+    if (nee && P.inside) {
+        frosted_sun_nee(P, hit_point, -normal, bounce);
+        P.has_carry = true;
+        P.carry_pdf = dot(d, -normal) / F(3.14159265358979323846f);
     }
     o->new_k = o->new_s = d;
     o->new_inside = !P.inside;
@@ -2717,6 +2784,8 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
     }
     P.ray = initial;
     P.k = initial.dir;
+    P.has_carry = false;
+    P.carry_pdf = 0.0f;
     P.inside = false;
     P.has_prev = false;
     P.escaped = false;
@@ -2729,12 +2798,17 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
         iterations = bounce + 1;
         Hit hit;
         bool carved = false, entering = false;
+        // pending_light_mis.take() (bounce_body.rs:372): only this iteration's escape reads it.
+        const bool had_carry = P.has_carry;
+        const F carry_pdf = P.carry_pdf;
+        P.has_carry = false;
         if (!intersect_scene(sc, P.ray, &hit, &carved, &entering)) {
             // handle_miss (bounce_body/miss.rs:33) + accumulate_miss_radiance (bounce.rs:40).
+            const F mis = had_carry ? balance_heuristic(carry_pdf, sun_nee_pdf(sc->environment, P.ray.dir)) : F(1.0f);
             F env[8];
             environment_channels(sc->environment, P.ray.dir, P.lambdas, P.observer, env);
             for (int c = 0; c < 8; ++c)
-                P.radiance[c] = fma_(intensity(P.stokes[c]) * F(1.0f), env[c], P.radiance[c]);
+                P.radiance[c] = fma_(intensity(P.stokes[c]) * mis, env[c], P.radiance[c]);
             P.escaped = true;
             term = TERM_ESCAPED;
             if (ev) {  // PathEvents::miss (path_events.rs:88)
@@ -2785,7 +2859,7 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
         const bool frosted =
             sc->facet_finishes && (uint32_t)hit.facet < sc->n_finishes && sc->facet_finishes[hit.facet] != 0;
         if (frosted) {
-            apply_frosted_bounce(P, g, normal, bounce, &o);
+            apply_frosted_bounce(P, g, normal, hit_point, bounce, &o);
         } else if (g.sin2_t > F(1.0f)) {
             apply_tir_bounce(P, g, P.k, normal, &o);
         } else {
@@ -3678,6 +3752,31 @@ int ixo_intersect_stone(const float* planes, uint32_t n_planes, const ix_tool* t
     *facet = h.facet;
     *entering = carved ? (ent ? 1 : 0) : -1;
     return 1;
+}
+// sample_environment_for_nee under DaylightSun (environment/nee.rs:81): the disc draw
+// for (u0, u1) into dir, returning its pdf.
+float ixo_sun_nee_sample(const ix_environment* env, float u0, float u1, float dir[3]) {
+    store3(dir, sun_cone_direction(load3(env->key_dir), u0, u1));
+    return raw(F(1.0f) / F(SUN_SOLID_ANGLE));
+}
+// environment_nee_pdf under DaylightSun (environment/nee.rs:144).
+float ixo_sun_nee_pdf(const ix_environment* env, const float dir[3]) { return raw(sun_nee_pdf(*env, load3(dir))); }
+float ixo_balance_heuristic(float a, float b) { return raw(balance_heuristic(a, b)); }
+// nee_contribution_frosted_exterior (scattering/frosted.rs:98) under the scene's
+// DaylightSun: the deposit of one event at `origin` into radiance[8], the channels at
+// lambdas[8] with unpolarised intensities[8].
+void ixo_frosted_sun_nee(const ix_scene* sc, const float origin[3], const float ext_normal[3], uint32_t seed,
+                         uint32_t bounce, const float lambdas[8], const float intensities[8], float radiance[8]) {
+    Path P{};
+    P.sc = sc;
+    P.seed = seed;
+    for (int c = 0; c < 8; ++c) {
+        P.lambdas[c] = lambdas[c];
+        P.stokes[c] = Stokes{F(intensities[c]), F(0.0f), F(0.0f), F(0.0f)};
+        P.radiance[c] = radiance[c];
+    }
+    frosted_sun_nee(P, load3(origin), load3(ext_normal), bounce);
+    for (int c = 0; c < 8; ++c) radiance[c] = raw(P.radiance[c]);
 }
 float ixo_channel_alpha(const ix_material* m, const float k[3], float lambda_nm) {
     // The non-birefringent branch of channel_absorption_alphas_assigned

@@ -92,6 +92,13 @@ int ixo_intersect_stone(const float* planes, uint32_t n_planes, const ix_tool* t
                         int32_t* entering);
 void ixo_biaxial_bundle(const ix_material* m, const float k[3], const float normal[3], float cos_i,
                         float lambda_nm, float n_beta, float out[24]);
+/* DaylightSun next-event estimation (environment/nee.rs:81,144; scattering/mod.rs:102;
+ * scattering/frosted.rs:98). */
+float ixo_sun_nee_sample(const ix_environment* env, float u0, float u1, float dir[3]);
+float ixo_sun_nee_pdf(const ix_environment* env, const float dir[3]);
+float ixo_balance_heuristic(float a, float b);
+void ixo_frosted_sun_nee(const ix_scene* sc, const float origin[3], const float ext_normal[3], uint32_t seed,
+                         uint32_t bounce, const float lambdas[8], const float intensities[8], float radiance[8]);
 /* simd/slab.rs:147 + intersect.rs:101: returns 1 and fills t/idx on a hit */
 int ixo_intersect(const float* planes, uint32_t n_planes, const float origin[3],
                   const float dir[3], float* t, int32_t* facet);

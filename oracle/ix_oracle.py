@@ -164,6 +164,14 @@ def _load(name: str) -> C.CDLL:
     lib.ixo_intersect_stone.restype = C.c_int
     lib.ixo_intersect_stone.argtypes = [f32p, C.c_uint32, P(abi.Tool), C.c_uint32, f32p, f32p, f32p, f32p,
                                         P(C.c_int32), P(C.c_int32)]
+    lib.ixo_sun_nee_sample.restype = C.c_float
+    lib.ixo_sun_nee_sample.argtypes = [P(abi.Environment), C.c_float, C.c_float, f32p]
+    lib.ixo_sun_nee_pdf.restype = C.c_float
+    lib.ixo_sun_nee_pdf.argtypes = [P(abi.Environment), f32p]
+    lib.ixo_balance_heuristic.restype = C.c_float
+    lib.ixo_balance_heuristic.argtypes = [C.c_float, C.c_float]
+    lib.ixo_frosted_sun_nee.restype = None
+    lib.ixo_frosted_sun_nee.argtypes = [P(abi.Scene), f32p, f32p, C.c_uint32, C.c_uint32, f32p, f32p, f32p]
     lib.ixo_biaxial_bundle.restype = None
     lib.ixo_biaxial_bundle.argtypes = [P(abi.Material), f32p, f32p, C.c_float, C.c_float, C.c_float, f32p]
     lib.ixo_counting_build.restype = C.c_int

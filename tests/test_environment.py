@@ -6,8 +6,8 @@ each of the 15 presets under two light poses, the observer off and on and three
 head-shadow sizes, over 48 directions (above, inside and below the horizon band) at 450,
 550 and 650 nm.  The oracle's lookup reproduces every row bit for bit; the product host
 code builds each preset's environment record bit-identical to the oracle's; the routing
-predicate takes every model the path traces and declines the UV lamps and the light
-samples DaylightSun would need.
+predicate takes every model the path traces and declines the UV lamps and, under
+DaylightSun, a scattering stone (whose light samples are not traced).
 """
 import ctypes as C
 import json
@@ -98,8 +98,8 @@ def test_host_environment_records_match_oracle(oracle):
 
 def test_routing_of_the_lighting_models():
     """Every lighting model of the reference routes; a UV lamp (fluorescence source,
-    gpu_backend/mod.rs:288-298) declines; DaylightSun declines a frosted or scattering
-    stone (it would take light samples there) and routes a polished, clear one."""
+    gpu_backend/mod.rs:288-298) declines; DaylightSun routes a polished or frosted stone
+    (the frosted facets' light samples are traced) and declines a scattering one."""
     from indicatrix_b200.backend import environment_preset, scene_routes_to_gpu
     fs = workloads.round_brilliant_frame(8, 8)
     for preset in range(13):
@@ -113,7 +113,7 @@ def test_routing_of_the_lighting_models():
     fs.facet_finishes = fin
     assert scene_routes_to_gpu(fs)
     fin[40] = 1
-    assert not scene_routes_to_gpu(fs)
+    assert scene_routes_to_gpu(fs)
     fs.facet_finishes = None
     fs.material = materials.with_scattering(materials.diamond(), 1.0, 0.3)
     assert not scene_routes_to_gpu(fs)
