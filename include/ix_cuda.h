@@ -104,9 +104,8 @@ void ix_set_precision(ix_backend* b, uint32_t precision);
 /* scene_routes_to_gpu (gpu_backend/mod.rs:288): 1 when this backend can trace `scene`
  * (<= IX_MAX_PLANES planes carved by <= IX_MAX_TOOLS valid tools, polished or frosted
  * facets, an isotropic, uniaxial or biaxial material with modelled dispersion, a lighting
- * model of the reference's six (not a UV lamp's line spectrum; under DaylightSun, which
- * takes light samples at frosted facets and scattering events, no interior scattering),
- * at most 2^32 - 1 pixels). */
+ * model of the reference's six (not a UV lamp's line spectrum), at most 2^32 - 1
+ * pixels). */
 int ix_scene_routes_to_gpu(const ix_scene* scene);
 /* scene_routes_to_gpu_with_tools (gpu_backend/tool_routing.rs:81): ix_scene_routes_to_gpu
  * of the stone carved by `tools` (when ntools > 0; else the scene's own tools): at most

@@ -538,9 +538,11 @@ int ix_scene_routes_to_gpu(const ix_scene* s) {
     // (gpu_backend/mod.rs:288-298).
     if (e.spectrum == IX_SPEC_GAUSSIAN) return 0;
     // DaylightSun enables next-event estimation (environment_supports_nee,
-    // environment/nee.rs:60): the frosted facets' light samples are traced; those of
-    // Henyey-Greenstein scattering events are not, so a scattering stone declines.
-    if (e.model == IX_ENV_DAYLIGHT_SUN && m.scattering_sigma_s > 0.0f) return 0;
+    // environment/nee.rs:60): the frosted facets' light samples are traced; a
+    // Henyey-Greenstein event takes none under an analytic sun and carries no weight
+    // (nee_contribution_hg_scatter and phase_pdf_for_mis are HDR-map only,
+    // scattering/hg_nee.rs:165, hg.rs:573), so a scattering stone traces as it does
+    // under any other model.
     if (m.dispersion.kind > IX_DISP_CAUCHY) return 0;
     // A biaxial indicatrix is traced as the anisotropic transport's biaxial arm; an
     // isotropic material carrying one (the reference's eigen-polarisation mean of the

@@ -6,8 +6,7 @@ each of the 15 presets under two light poses, the observer off and on and three
 head-shadow sizes, over 48 directions (above, inside and below the horizon band) at 450,
 550 and 650 nm.  The oracle's lookup reproduces every row bit for bit; the product host
 code builds each preset's environment record bit-identical to the oracle's; the routing
-predicate takes every model the path traces and declines the UV lamps and, under
-DaylightSun, a scattering stone (whose light samples are not traced).
+predicate takes every model the path traces and declines the UV lamps.
 """
 import ctypes as C
 import json
@@ -98,8 +97,9 @@ def test_host_environment_records_match_oracle(oracle):
 
 def test_routing_of_the_lighting_models():
     """Every lighting model of the reference routes; a UV lamp (fluorescence source,
-    gpu_backend/mod.rs:288-298) declines; DaylightSun routes a polished or frosted stone
-    (the frosted facets' light samples are traced) and declines a scattering one."""
+    gpu_backend/mod.rs:288-298) declines; DaylightSun routes polished, frosted and
+    scattering stones (the frosted facets' light samples are traced; a scattering event
+    takes none under the analytic sun, scattering/hg_nee.rs:165)."""
     from indicatrix_b200.backend import environment_preset, scene_routes_to_gpu
     fs = workloads.round_brilliant_frame(8, 8)
     for preset in range(13):
@@ -116,4 +116,4 @@ def test_routing_of_the_lighting_models():
     assert scene_routes_to_gpu(fs)
     fs.facet_finishes = None
     fs.material = materials.with_scattering(materials.diamond(), 1.0, 0.3)
-    assert not scene_routes_to_gpu(fs)
+    assert scene_routes_to_gpu(fs)

@@ -3,10 +3,11 @@ the CPU oracle through the C ABI (nee_contribution_frosted_exterior,
 scattering/frosted.rs:98; the escape's balance weight, bounce_body/miss.rs:40).
 
 The round brilliant with a bruted girdle and a frosted table under a low sun: per path in
-the exact build for isotropic, uniaxial and biaxial materials and a carved stone (whose
-light samples are shadow-probed); paths cut at the bounce cap keep their light samples
-(at one bounce a stone pixel is lit by next-event estimation alone); frame sums through
-the accumulate entry; Tier 3 of the benched build.  As in test_gpu_frosted, the diffuse
+the exact build for isotropic, uniaxial and biaxial materials, a carved stone (whose
+light samples are shadow-probed) and scattering stones (whose Henyey-Greenstein events
+take no light sample under the analytic sun); paths cut at the bounce cap keep their
+light samples (at one bounce a stone pixel is lit by next-event estimation alone); frame
+sums through the accumulate entry; Tier 3 of the benched build.  As in test_gpu_frosted, the diffuse
 lobe's and the disc draw's sin/cos round a few ULP apart between the device and the host
 libm, so the per-path bars are the frosted ones.
 """
@@ -28,6 +29,10 @@ CASES = {
     "sapphire_tilted": lambda: materials.sapphire((0.0, 0.8, 0.6)),
     "tanzanite": lambda: materials.tanzanite((0.3, 0.8, 0.52)),
     "carved_diamond": lambda: materials.diamond(),
+    # A Henyey-Greenstein event takes no light sample under the analytic sun
+    # (scattering/hg_nee.rs:165); the frosted facets of the scattering stone still do.
+    "scattering_diamond": lambda: materials.with_scattering(materials.diamond(), 0.5, 0.3),
+    "scattering_sapphire": lambda: materials.with_scattering(materials.sapphire((0.0, 0.8, 0.6)), 0.5, 0.3),
 }
 
 
@@ -88,13 +93,13 @@ def test_sun_nee_frame_sums(exact_backend, oracle):
     assert abs(acc.sum() - s64.sum()) / s64.sum() < 1e-2
 
 
-@pytest.mark.parametrize("name", ["diamond", "carved_diamond"])
+@pytest.mark.parametrize("name", ["diamond", "carved_diamond", "scattering_diamond"])
 def test_sun_nee_tier3_fast_build(backend, oracle, name):
     """Tier 3 on the benched build: the batch plan's means over samples [0, 500) against
     the oracle's [500, 1000), each side's own variance."""
     W, H, N = TIER3_W, TIER3_H, TIER3_SPP
     tools = carved_round_brilliant_tools() if name.startswith("carved") else None
-    fs = sun_scene(oracle, materials.diamond(), W, H, tools=tools)
+    fs = sun_scene(oracle, CASES[name](), W, H, tools=tools)
     plan = BatchPlan(backend, [(fs, 0, N)])
     plan.run()
     mg = plan.sums(0).reshape(-1, 3) / N

@@ -6,8 +6,8 @@ angle, with the constant pdf the independent lookup also returns (zero outside);
 balance weights of the two techniques sum to one and together conserve a Lambertian
 reflector's energy; one frosted-exterior deposit equals the analytic direct-light value
 (cos / pi) x solid angle x L_sun(lambda) and a surface facing away gets none.  Beside
-them: the shadow probe of a carved stone, and the routing, which now traces a frosted
-stone under the sun and still declines a scattering one.
+them: the shadow probe of a carved stone, and the routing, which traces frosted and
+scattering stones under the sun.
 """
 import ctypes as C
 import math
@@ -137,8 +137,9 @@ def test_carved_stone_shadow_probe(oracle):
 
 
 def test_routing_under_the_sun():
-    """DaylightSun routes a frosted stone (its light samples are traced) and declines a
-    scattering one (the Henyey-Greenstein events' light samples are not)."""
+    """DaylightSun routes a frosted stone (its light samples are traced), carved or not,
+    and a scattering one (a Henyey-Greenstein event takes no light sample under the
+    analytic sun, scattering/hg_nee.rs:165)."""
     from indicatrix_b200.backend import environment_preset, scene_routes_to_gpu
     fs = workloads.round_brilliant_frame(8, 8)
     fs.environment = environment_preset(6, 1.0, 0.5, 0.8)
@@ -149,4 +150,4 @@ def test_routing_under_the_sun():
     fs.tools = [geometry.tool_ball((0.0, 0.32, 0.0), 0.22)]
     assert scene_routes_to_gpu(fs)
     fs.material = materials.with_scattering(materials.diamond(), 1.0, 0.3)
-    assert not scene_routes_to_gpu(fs)
+    assert scene_routes_to_gpu(fs)
