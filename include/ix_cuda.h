@@ -262,8 +262,8 @@ typedef struct ix_gem_metrics {
 
 /* The lighting a call scores against: a LightingPreset index (as ix_environment_preset),
  * the rig's light yaw / pitch and the environment's head-shadow size in degrees
- * (16 = the default).  The scorer models the studio rigs and the iso-hemisphere
- * (presets 1 and 7-11); a call with any other preset declines. */
+ * (16 = the default).  Every preset scores (the ASET view as the iso-hemisphere,
+ * color/metrics/lighting.rs:125); an unknown preset declines. */
 typedef struct ix_metrics_lighting {
     int32_t preset;
     float light_yaw;

@@ -388,17 +388,21 @@ float metrics_head_shadow_cos(bool studio, float deg) {
 // ExitLighting::new (lighting.rs:137) for a lighting preset: the preset at exposure 1, no
 // tray and the default head-shadow edges, its spectral power at 550 nm, the threshold
 // factor over the median hemisphere radiance, the observer cone and the 96 hemisphere
-// probe directions (hemisphere_direction, lighting.rs:74).  False for a preset the scorer
-// does not model: it scores under the studio rigs and the iso-hemisphere (the direction
-// lighting of those two models); the tent, dome, sun, ASET and UV-lamp presets decline.
+// probe directions (hemisphere_direction, lighting.rs:74).  Every preset scores: the ASET
+// view as the iso-hemisphere (scoring_preset, lighting.rs:125); a UV lamp's line spectrum
+// at 550 nm.  False for an unknown preset.
 bool exit_lighting_setup(const ix_metrics_lighting& lighting, ix_environment* env, float* spec, float* factor,
                          float* head_shadow_cos, float dirs[96][3]) {
-    if (ix_environment_preset(lighting.preset, 1.0f, lighting.light_yaw, lighting.light_pitch, 0.0f, 1.0f, 16.0f,
-                              env) != 0)
+    const int32_t scoring = lighting.preset == 12 ? 1 : lighting.preset;
+    if (ix_environment_preset(scoring, 1.0f, lighting.light_yaw, lighting.light_pitch, 0.0f, 1.0f, 16.0f, env) != 0)
         return false;
-    if (env->model != IX_ENV_STUDIO && env->model != IX_ENV_ISO_HEMISPHERE) return false;
     const bool studio = env->model == IX_ENV_STUDIO;
-    *spec = env->spectrum == IX_SPEC_D65 ? d65_host(550.0f) : blackbody(env->bb_t_k, env->bb_denom_560, 550.0f);
+    if (env->spectrum == IX_SPEC_GAUSSIAN) {
+        const float z = (550.0f - env->line_centre_nm) / env->line_sigma_nm;
+        *spec = std::exp((-0.5f * z) * z);
+    } else {
+        *spec = env->spectrum == IX_SPEC_D65 ? d65_host(550.0f) : blackbody(env->bb_t_k, env->bb_denom_560, 550.0f);
+    }
     *factor = studio ? 4.0f : 0.5f;
     *head_shadow_cos = metrics_head_shadow_cos(studio, lighting.head_shadow_deg);
     for (int i = 0; i < 96; ++i) {

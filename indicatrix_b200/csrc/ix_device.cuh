@@ -611,16 +611,41 @@ IX_DEV float environment_radiance_ext(const ix_environment& env, V3 dir, V3 obse
     return bands[3] > 0.0f ? fmaf(bands[3] * d65(spec), env.exposure, zones) : zones;
 }
 
+// RadianceSource::radiance (color/metrics/lighting.rs:93) of the models past the studio rig
+// and the iso-hemisphere (tent, dome, sun): the extended lookup at 550 nm with no observer.
+// Out of line: the kernels that may meet either kind of model call it from a branch.
+static __device__ __noinline__ float exit_radiance_ext(const ix_environment& env, V3 dir) {
+    return environment_radiance_ext(env, dir, v3(0.0f, 0.0f, 0.0f), 550.0f);
+}
+// The scoring radiance along `dir`: the rig's direction lighting at the host's 550 nm
+// power `spec` (SCORE_RIG: the studio rigs and the iso-hemisphere), the extended lookup
+// (SCORE_EXT: every other model), or either by the environment's model (SCORE_ANY).  The
+// metrics kernel is built for the first two, so the rig's instantiation compiles as it
+// does without the extended lookup.
+enum ScoreKind { SCORE_RIG = 0, SCORE_EXT = 1, SCORE_ANY = 2 };
+__host__ __device__ __forceinline__ bool rig_scored(const ix_environment& env) {
+    return env.model == IX_ENV_STUDIO || env.model == IX_ENV_ISO_HEMISPHERE;
+}
+template <int SCORE>
+IX_DEV float exit_radiance(const ix_environment& env, float spec, V3 dir) {
+    if constexpr (SCORE == SCORE_EXT) {
+        return exit_radiance_ext(env, dir);
+    } else {
+        if constexpr (SCORE == SCORE_ANY)
+            if (!rig_scored(env)) return exit_radiance_ext(env, dir);
+        return lighting_radiance(direction_lighting(env, dir, v3(0.0f, 0.0f, 0.0f)), env, spec);
+    }
+}
+
 // ExitLighting (color/metrics/lighting.rs:137-209) and returned_or_reason
 // (visibility.rs:55): the metrics' verdict on a direction leaving the stone.  `env` is the
 // scoring environment (the preset at exposure 1, no tray), `spec` its 550 nm power.
-struct ExitScorer {
+template <int SCORE>
+struct ExitScorerT {
     const ix_environment& env;
     float spec, threshold, head_shadow_cos;
     // is_illuminated (lighting.rs:207): the scoring light's radiance along `dir`.
-    IX_DEV bool lit(V3 dir) const {
-        return lighting_radiance(direction_lighting(env, dir, v3(0.0f, 0.0f, 0.0f)), env, spec) > threshold;
-    }
+    IX_DEV bool lit(V3 dir) const { return exit_radiance<SCORE>(env, spec, dir) > threshold; }
     // Exits closer to the eye than the head-shadow cone are lost to the observer.
     IX_DEV bool shadowed(V3 exit_dir, V3 observer) const { return dot(exit_dir, observer) > head_shadow_cos; }
     // ray_is_visibly_returned (visibility.rs:78) for an observer at -forward.
@@ -629,16 +654,18 @@ struct ExitScorer {
         return lit(exit_dir);
     }
 };
+using ExitScorer = ExitScorerT<SCORE_ANY>;
 
 // ambient_level (lighting.rs:101) scaled by SOURCE_OVER_AMBIENT or
 // UNIFORM_FRACTION_OF_AMBIENT (`factor`) and floored at the least positive normal
 // (lighting.rs:186): the median of the radiances along the 96 hemisphere directions.
 // Block-wide: every thread of the block calls it; `s_rad` is 96 floats of shared memory.
+template <int SCORE>
 IX_DEV float exit_lighting_threshold(const ix_environment& env, float spec, float factor, const float (*dirs)[3],
                                      float* s_rad, float* s_threshold) {
     for (int i = threadIdx.x; i < 96; i += blockDim.x) {
         const V3 d = v3(dirs[i][0], dirs[i][1], dirs[i][2]);
-        s_rad[i] = lighting_radiance(direction_lighting(env, d, v3(0.0f, 0.0f, 0.0f)), env, spec);
+        s_rad[i] = exit_radiance<SCORE>(env, spec, d);
     }
     __syncthreads();
     if (threadIdx.x == 0) {

@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(128, MINB)
     const float4* gplanes = reinterpret_cast<const float4*>(L.scene.planes);
     for (uint32_t i = threadIdx.x; i < L.scene.n_planes; i += blockDim.x) s_planes[i] = gplanes[i];
     // Its barriers also publish the plane cache.
-    const float threshold = exit_lighting_threshold(A.env, A.spec, A.factor, A.dirs, s_rad, &s_threshold);
+    const float threshold = exit_lighting_threshold<SCORE_ANY>(A.env, A.spec, A.factor, A.dirs, s_rad, &s_threshold);
     const ExitScorer scorer{A.env, A.spec, threshold, A.head_shadow_cos};
     const DevScene S = make_scene(L.scene, L.flags);
     const Group g = make_group();

@@ -127,6 +127,9 @@ IX_DEV V3 basis_vec(const MetricsPoseDev& p, int k, int which) {
 
 }  // namespace
 
+// SCORE: SCORE_RIG for the studio rigs and the iso-hemisphere, SCORE_EXT for every other
+// lighting model (the launch picks by the scoring environment's model).
+template <int SCORE>
 __global__ void __launch_bounds__(METRICS_THREADS) IX_SFX(metrics_kernel)(const __grid_constant__ MetricsLaunch L) {
     __shared__ float4 s_planes[IX_MAX_PLANES];
     __shared__ float s_rad[96];
@@ -137,8 +140,8 @@ __global__ void __launch_bounds__(METRICS_THREADS) IX_SFX(metrics_kernel)(const 
     const int n = (int)stone.n_planes;
     for (int i = threadIdx.x; i < n; i += blockDim.x) s_planes[i] = L.planes[stone.plane_offset + i];
     // The exit-lighting threshold; its barriers also publish the plane cache.
-    const float threshold = exit_lighting_threshold(L.env, L.spec, L.factor, L.dirs, s_rad, &s_threshold);
-    const ExitScorer sc{L.env, L.spec, threshold, L.head_shadow_cos};
+    const float threshold = exit_lighting_threshold<SCORE>(L.env, L.spec, L.factor, L.dirs, s_rad, &s_threshold);
+    const ExitScorerT<SCORE> sc{L.env, L.spec, threshold, L.head_shadow_cos};
     const float nd = fmaxf(dispersion_eval(stone.dispersion, 589.3f), 1.1f);
     const float n_f = fmaxf(dispersion_eval(stone.dispersion, 486.1f), 1.001f);
     const float n_c = fmaxf(dispersion_eval(stone.dispersion, 656.3f), 1.001f);
@@ -260,7 +263,10 @@ __global__ void __launch_bounds__(METRICS_THREADS) IX_SFX(metrics_kernel)(const 
 
 cudaError_t IX_SFX(launch_metrics)(const MetricsLaunch& l, cudaStream_t stream) {
     if (l.n_poses == 0) return cudaSuccess;
-    IX_SFX(metrics_kernel)<<<l.n_poses, METRICS_THREADS, 0, stream>>>(l);
+    if (rig_scored(l.env))
+        IX_SFX(metrics_kernel)<SCORE_RIG><<<l.n_poses, METRICS_THREADS, 0, stream>>>(l);
+    else
+        IX_SFX(metrics_kernel)<SCORE_EXT><<<l.n_poses, METRICS_THREADS, 0, stream>>>(l);
     return cudaGetLastError();
 }
 

@@ -3032,7 +3032,9 @@ static V3 hemisphere_direction(int index) {
 }
 static bool metric_lighting(int32_t preset, float light_yaw, float light_pitch, float head_shadow_deg,
                             MetricLighting* out) {
-    if (ixo_environment_preset(preset, 1.0f, light_yaw, light_pitch, 0.0f, 1.0f, 16.0f, &out->env) != 0)
+    // scoring_preset (lighting.rs:125): the ASET view scores as the iso-hemisphere.
+    if (ixo_environment_preset(preset == 12 ? 1 : preset, 1.0f, light_yaw, light_pitch, 0.0f, 1.0f, 16.0f,
+                               &out->env) != 0)
         return false;
     const bool studio = out->env.model == IX_ENV_STUDIO;
     out->spec = spectral_power(out->env, 550.0f);

@@ -149,6 +149,19 @@ def test_studio_lighting_classes(exact_backend, oracle):
         assert np.sum(want == cls) > 0, cls
 
 
+@pytest.mark.parametrize("preset", [0, 6], ids=["tent", "sun"])
+def test_lit_model_classes(exact_backend, oracle, preset):
+    """Under the tent and the sun (scored by the 0.5 x ambient rule of every model past the
+    studio rig, color/metrics/lighting.rs:186) the per-sample classes match the oracle."""
+    from indicatrix_b200.backend import environment_preset
+
+    fs = workloads.round_brilliant_frame(40, 40, max_bounces=32)
+    fs.environment = environment_preset(preset, 1.0, 0.85, 0.95, 0.0, 1.0, 16.0)
+    light = MetricsLighting(preset=preset, light_yaw=0.85, light_pitch=0.95, head_shadow_deg=16.0)
+    got, want, _, _ = per_sample(exact_backend, oracle, fs, light, 4)
+    assert np.mean(got == want) >= 0.999, np.mean(got == want)
+
+
 def test_cancel_decline_and_no_map(backend):
     """A cancelled or declined call writes neither the sums nor the map; a frame traced
     with an empty map (invalid size) still gets its sums."""
@@ -160,7 +173,7 @@ def test_cancel_decline_and_no_map(backend):
     flag.set()
     assert backend.try_accumulate_attributed(fs, ISO, 0, 4, acc, m, flag) == GpuAccumulate.CANCELLED
     assert np.all(acc == 3.0) and np.all(m.pixels["samples"] == 9)
-    bad = MetricsLighting(preset=12, light_yaw=0.0, light_pitch=0.0, head_shadow_deg=16.0)  # Aset
+    bad = MetricsLighting(preset=15, light_yaw=0.0, light_pitch=0.0, head_shadow_deg=16.0)  # no such preset
     assert backend.try_accumulate_attributed(fs, bad, 0, 4, acc, m) == GpuAccumulate.DECLINED
     assert np.all(acc == 3.0) and np.all(m.pixels["samples"] == 9)
     empty = AttributionMap(0, 0)

@@ -44,8 +44,11 @@ def metric_cases():
 
 
 @pytest.mark.parametrize("lighting", [MetricsLighting(10, 0.85, 0.95), MetricsLighting(1, 0.0, 0.0, 16.0),
-                                      MetricsLighting(1, 0.0, 0.0, 30.0), MetricsLighting(8, 2.1, 0.4)],
-                         ids=["ring", "iso16", "iso30", "incandescent"])
+                                      MetricsLighting(1, 0.0, 0.0, 30.0), MetricsLighting(8, 2.1, 0.4),
+                                      MetricsLighting(0, 0.85, 0.95), MetricsLighting(3, 0.4, 1.0, 20.0),
+                                      MetricsLighting(5, 0.85, 0.95), MetricsLighting(6, 0.4, 0.9),
+                                      MetricsLighting(13, 0.85, 0.95)],
+                         ids=["ring", "iso16", "iso30", "incandescent", "tent", "shop", "dome", "sun", "uv365"])
 def test_metrics_batch_matches_oracle(exact_backend, backend, oracle, lighting):
     """Many stones x poses in one launch: exact build identical to the oracle except the
     fire index (a few ULP); fused build within a few classified rays."""
@@ -132,3 +135,13 @@ def test_all_axes_profiles_match_oracle(exact_backend, backend, oracle):
             f = np.array([fast[a].brilliance[s], fast[a].extinction[s], fast[a].windowing[s]])
             w3 = np.array([want[0], want[4], want[3]])
             assert np.all(np.abs(f - w3) <= np.maximum(1.5, 0.02 * np.abs(w3))), (a, job, f, want)
+
+
+def test_aset_scores_as_the_iso_hemisphere(exact_backend):
+    """scoring_preset (color/metrics/lighting.rs:125): the ASET view is a false-colour
+    diagnostic, scored as the grading standard, so switching to it never moves the numbers."""
+    stones, poses = metric_cases()
+    args = [(p, m.dispersion) for p, m in stones]
+    aset = exact_backend.evaluate_metrics_batch(args, poses, MetricsLighting(12, 0.3, 0.7, 20.0))
+    iso = exact_backend.evaluate_metrics_batch(args, poses, MetricsLighting(1, 0.3, 0.7, 20.0))
+    assert np.array_equal(np.asarray(aset), np.asarray(iso))
