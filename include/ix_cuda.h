@@ -329,8 +329,10 @@ int ix_evaluate_axis_profiles(ix_backend* b, const float* planes, uint32_t n_pla
  * (renderer/attribution_map.rs:105), in ascending sample order.  `attribution` is
  * caller-owned, width * height records, updated only when the call returns IX_DONE.  A
  * frame of more than IX_ATTRIBUTION_MAX_PIXELS pixels (or a NULL map) is traced without
- * attribution (AttributionMap::checked, attribution_map.rs:201).  IX_DECLINED also for a
- * lighting preset the backend does not model. */
+ * attribution (AttributionMap::checked, attribution_map.rs:201).  A scattering stone's
+ * records also count the hits whose path scattered; a path ended by its scattering
+ * event's roulette (ScatterAbsorbed) takes the roulette's class.  IX_DECLINED also for an
+ * unknown lighting preset. */
 int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metrics_lighting* lighting,
                              uint32_t sample_offset, uint32_t spp, double* accum_xyz,
                              ix_attribution_pixel* attribution, const volatile uint8_t* cancel);

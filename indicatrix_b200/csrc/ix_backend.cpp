@@ -635,7 +635,6 @@ int ix_accumulate_attributed(ix_backend* b, const ix_scene* scene, const ix_metr
     if (!attribution || n_pixels > IX_ATTRIBUTION_MAX_PIXELS)
         return accumulate_impl<double>(b, scene, sample_offset, spp, accum_xyz, cancel);
     // The recorder does not follow interior scattering events (PathEvents::scatter).
-    if (scene->material.scattering_sigma_s > 0.0f) return IX_DECLINED;
     if (b->lost) return IX_DECLINED;
     if (!ix_scene_routes_to_gpu(scene)) return IX_DECLINED;
     if (b->limits.max_pixels && n_pixels > b->limits.max_pixels) return IX_DECLINED;

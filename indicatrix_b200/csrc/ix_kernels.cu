@@ -64,6 +64,7 @@ enum : uint32_t {
     EV_WINDOWED = 8u,   // ... through a facet whose outward normal has y < -0.05
     EV_ROULETTE = 16u,  // the loop stopped by Russian roulette
     EV_ESCAPED = 32u,   // the loop stopped because the ray met no facet
+    EV_SCATTERED = 64u, // a Henyey-Greenstein scattering event happened
 };
 
 // Where a task's attribution records go: record (s, pixel0 + j) of the launch is at
@@ -161,9 +162,14 @@ IX_DEV uint32_t trace_task(const Group& g, const DevScene& S, const float4* __re
         const bool inside_before = P.inside;
         const int r = capped ? (int)BOUNCE_KILLED : group_step<UNI>(g, P, S, planes, esc);
         if constexpr (ATTR) {
+            // A scattering step (the only step that leaves no plane of incidence behind)
+            // records PathEvents::scatter (path_events.rs:96), no facet event; one ended by
+            // its roulette is ScatterAbsorbed, which takes the roulette's class slot.
+            const bool scatter_step = !capped && r != BOUNCE_ESCAPED && !P.has_prev;
+            if (scatter_step) ev |= EV_SCATTERED;
             // record_facet (bounce_body.rs:680) runs after every facet dispatch, before
             // the roulette that may end the path; a miss records no facet event.
-            if (!capped && r != BOUNCE_ESCAPED) {
+            if (!capped && r != BOUNCE_ESCAPED && !scatter_step) {
                 if (!(ev & EV_FACET)) ev |= EV_FACET | (P.inside ? EV_ENTERED : 0u);
                 if (inside_before && !P.inside && !(ev & EV_EXITED)) {
                     ev |= EV_EXITED | (planes[P.facet].y < -0.05f ? EV_WINDOWED : 0u);
@@ -179,7 +185,9 @@ IX_DEV uint32_t trace_task(const Group& g, const DevScene& S, const float4* __re
         if constexpr (ATTR) {
             if (g.c == 0) {
                 const size_t rec = (size_t)(q - cur_j * spp) * at->stride + at->pixel0 + cur_j;
-                at->cls[rec] = (uint8_t)classify_path(ev, exit_dir, P.observer, *at->scorer);
+                const uint32_t cls = classify_path(ev, exit_dir, P.observer, *at->scorer);
+                // A hit's record carries the scattered flag in bit 6 (the classes are 0-8).
+                at->cls[rec] = (uint8_t)(cls | ((cls != IX_CLASS_MISS && (ev & EV_SCATTERED)) ? 0x40u : 0u));
                 at->y[rec] = xyz.y;
             }
         }
@@ -300,11 +308,14 @@ __global__ void __launch_bounds__(128) IX_SFX(attribution_fold_kernel)(const __g
     auto sat = [](uint32_t v) { return v == 0xFFFFFFFFu ? v : v + 1u; };
     for (uint32_t s = 0; s < L.spp; ++s) {
         const size_t rec = (size_t)s * L.n_pixels + p;
-        const uint32_t c = L.cls[rec];
+        const uint32_t raw = L.cls[rec];
+        const bool scattered = raw != IX_CLASS_MISS && (raw & 0x40u);
+        const uint32_t c = raw == IX_CLASS_MISS ? raw : (raw & 0x3Fu);
         const float y = L.y[rec];
         a.samples = sat(a.samples);
         if (c >= IX_ATTRIBUTION_CLASSES) continue;
         a.hits = sat(a.hits);
+        if (scattered) a.scattered = a.scattered + 1u;  // a plain add, as the reference's
         const bool finite = isfinite(y);
 #pragma unroll
         for (uint32_t k = 0; k < IX_ATTRIBUTION_CLASSES; ++k) {

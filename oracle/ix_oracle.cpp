@@ -2639,7 +2639,7 @@ static void apply_absorption(Path& P, F path_len) {
 #endif
 }
 
-enum { TERM_ESCAPED = 0, TERM_RR = 1, TERM_CAP = 2 };
+enum { TERM_ESCAPED = 0, TERM_RR = 1, TERM_CAP = 2, TERM_SCATTER_ABSORBED = 3 };
 
 // apply_russian_roulette (transport/bounce.rs:355): false when the path is killed.
 static bool russian_roulette(Path& P, uint32_t bounce) {
@@ -2823,8 +2823,9 @@ static V3 trace_path(const ix_scene* sc, Ray initial, uint32_t seed, F hero_rand
         // The interior segment may end in a scattering event first (bounce_body.rs:408-417).
         if (P.inside && m.scattering_sigma_s > 0.0f) {
             const int sc_out = scatter_step(P, hit.t, bounce);
+            if (ev && sc_out != SCATTER_NONE) ev->scattered = 1;  // PathEvents::scatter (path_events.rs:96)
             if (sc_out == SCATTER_KILLED) {
-                term = TERM_RR;
+                term = TERM_SCATTER_ABSORBED;  // bounce_body.rs:527
                 break;
             }
             if (sc_out == SCATTER_SURVIVED) continue;
@@ -3266,7 +3267,7 @@ static uint32_t classify_events(const ixo_path_events& ev, V3 observer, const Me
     if (ev.exit_facet < 0) {
         // unexited_reason (attribution.rs:57): roulette, the bounce cap, or an escape
         // without an exit event (the analytical map's "no intersection").
-        if (ev.termination == TERM_RR) return IX_CLASS_KILLED;
+        if (ev.termination == TERM_RR || ev.termination == TERM_SCATTER_ABSORBED) return IX_CLASS_KILLED;
         if (ev.termination == TERM_CAP) return IX_CLASS_BUDGET;
         return IX_CLASS_NO_INTERSECTION;
     }
@@ -3987,7 +3988,7 @@ int64_t ixo_attribute_pixels(const ix_scene* scene, int32_t preset, float light_
                 V3 xyz = sample_xyz(scene, pixel, rot, sample_offset + s, nullptr, &ev, &cam_dir);
                 // The observer is the reverse of the camera ray (attribution_tests.rs:129).
                 const uint32_t cls = classify_events(ev, -cam_dir, L);
-                attribution_add(&ap, cls, 0, 0, raw(xyz.y));
+                attribution_add(&ap, cls, ev.scattered, 0, raw(xyz.y));
                 if (xyz_finite(xyz)) {
                     sd[0] += (double)raw(xyz.x);
                     sd[1] += (double)raw(xyz.y);

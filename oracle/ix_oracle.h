@@ -41,6 +41,7 @@ typedef struct ixo_path_events {
     uint32_t termination;        /* ixo_path_info numbering                              */
     uint32_t has_escaped_dir;
     float escaped_dir[3];
+    uint32_t scattered;          /* a Henyey-Greenstein scattering event happened         */
 } ixo_path_events;
 typedef struct ixo_flop_counts {
     uint64_t add, mul, fma, div, sqrt, transcendental, paths;

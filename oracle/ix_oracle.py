@@ -41,10 +41,11 @@ class PathEvents(C.Structure):
         ("termination", C.c_uint32),
         ("has_escaped_dir", C.c_uint32),
         ("escaped_dir", C.c_float * 3),
+        ("scattered", C.c_uint32),
     ]
 
 
-TERM_ESCAPED, TERM_RR, TERM_CAP = 0, 1, 2
+TERM_ESCAPED, TERM_RR, TERM_CAP, TERM_SCATTER_ABSORBED = 0, 1, 2, 3
 
 
 class FlopCounts(C.Structure):

@@ -186,6 +186,29 @@ def test_a_convex_stone_never_reenters_and_rarely_loses_a_path_after_entry(oracl
     assert lost * 50 <= entered, (lost, entered)
 
 
+def test_roulette_and_scatter_are_reasons(oracle):
+    """russian_roulette_and_scatter_are_reasons (attribution_tests.rs:201): a scattering,
+    absorbing corundum (sigma_s 3, g 0.5; the sapphire builder stands in for the built-in
+    ruby) at a 64-bounce budget scatters, ends paths by roulette and by scattering
+    absorption, and labels every entered path that never exited by its termination."""
+    mat = materials.with_scattering(materials.sapphire(), 3.0, 0.5)
+    sc, _keep = srb_scene(oracle, mat, PRESET_ISO_HEMISPHERE, max_bounces=64)
+    roulette = absorbed = scattered = 0
+    expected = {oracle.TERM_RR: abi.CLASS_KILLED, oracle.TERM_SCATTER_ABSORBED: abi.CLASS_KILLED,
+                oracle.TERM_CAP: abi.CLASS_BUDGET}
+    for i in range(3000):
+        o, d = ray_for(oracle, i)
+        seed, hero = seed_and_hero(oracle, i)
+        _, ev = oracle.trace_ray_events(sc, o, d, seed, hero)
+        scattered += ev.scattered
+        roulette += ev.termination == oracle.TERM_RR
+        absorbed += ev.termination == oracle.TERM_SCATTER_ABSORBED
+        if ev.exit_facet < 0 and ev.first_facet >= 0 and ev.first_entered:
+            cls = oracle.classify_path(ev, -d, PRESET_ISO_HEMISPHERE, YAW, PITCH)
+            assert cls == expected.get(ev.termination, abi.CLASS_NO_INTERSECTION), i
+    assert scattered > 0 and absorbed > 0 and roulette > 0, (scattered, absorbed, roulette)
+
+
 def test_a_missing_ray_records_only_the_escape(oracle):
     """attribution_tests.rs:150."""
     sc, _keep = srb_scene(oracle, materials.diamond(), PRESET_ISO_HEMISPHERE)

@@ -9,7 +9,7 @@ device folds (f32 sums in ascending sample order) with the oracle's.
 import numpy as np
 import pytest
 
-from indicatrix_b200 import abi, workloads
+from indicatrix_b200 import abi, materials, workloads
 from indicatrix_b200.attribution import AttributionMap
 from indicatrix_b200.backend import CancelFlag, GpuAccumulate, GpuBackend, MetricsLighting
 
@@ -160,6 +160,26 @@ def test_lit_model_classes(exact_backend, oracle, preset):
     light = MetricsLighting(preset=preset, light_yaw=0.85, light_pitch=0.95, head_shadow_deg=16.0)
     got, want, _, _ = per_sample(exact_backend, oracle, fs, light, 4)
     assert np.mean(got == want) >= 0.999, np.mean(got == want)
+
+
+def test_scattering_stone_classes_and_counts(exact_backend, oracle):
+    """A scattering corundum (sigma_s 3, g 0.5, 64 bounces): per-sample classes match the
+    oracle (roulette after a scattering event is ScatterAbsorbed, the roulette's slot), and
+    the map's per-pixel count of hits whose path scattered equals the oracle's."""
+    from indicatrix_b200.backend import environment_preset
+
+    fs = workloads.round_brilliant_frame(32, 32, max_bounces=64)
+    fs.material = materials.with_scattering(materials.sapphire(), 3.0, 0.5)
+    fs.environment = environment_preset(1, 1.0, 0.0, 0.0, 0.0, 1.0, 20.0)
+    got, want, _, _ = per_sample(exact_backend, oracle, fs, ISO, 4)
+    assert np.mean(got == want) >= 0.99, np.mean(got == want)
+    assert np.sum(want == abi.CLASS_KILLED) > 0
+    n = fs.width * fs.height
+    g, _ = gpu_map(exact_backend, fs, ISO, 0, 8)
+    o, _, _ = oracle.attribute_pixels(fs.to_abi(), ISO.to_abi(), 0, n, 0, 8)
+    assert g["scattered"].sum() > 0
+    assert np.mean(g["scattered"] == o["scattered"]) >= 0.99
+    assert np.all(g["scattered"] <= g["hits"])
 
 
 def test_cancel_decline_and_no_map(backend):
