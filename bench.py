@@ -9,6 +9,9 @@ One "step" is one pass of the hot path over one batch of synthetic input:
 * ``--workload stress``: the anisotropic stress frame, 512x512 x 256 spp (67,108,864
   paths) of a uniaxial pleochroic emerald-cut stone with its optic axis tilted 30
   degrees, depth 64.
+* ``--workload sun``: the extended transport on a 256x256, 64 spp round brilliant with its
+  table and girdle frosted and a dimple ground into the table, under the DaylightSun
+  model (frosted next-event estimation toward the sun's disc), depth 32.
 * ``--workload display``: the display step after the path on a 1920x1080 frame of 16 spp
   XYZ sums (the reference's denoise bench: round brilliant at (0.60, 0.45, 2.4, 42 deg),
   path signature at n_d 1.76, seeded noise in [0, 2) per channel): average, 5 A-Trous
@@ -54,7 +57,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["frame", "batch", "stress", "display", "surrogate"])
+    ap.add_argument("--workload", default="batch", choices=["frame", "batch", "stress", "sun", "display", "surrogate"])
     ap.add_argument("--precision", default="fast", choices=["fast", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -157,6 +160,17 @@ def stress_workload(builder=None):
                          "environment": "D65 hemisphere, 20 deg head shadow", "max_depth": 64}
 
 
+def sun_workload(builder=None):
+    from indicatrix_b200 import workloads
+
+    fs = workloads.carved_sun_frame(256, 256, 32, builder=builder)
+    return [(fs, 64)], {"workload": "carved frosted round brilliant under the sun 256x256 x 64 spp",
+                        "pixels": 65536, "spp": 64, "planes": int(fs.planes.shape[0]), "material": "diamond",
+                        "stone": "table and girdle frosted, a 0.11 ball dimple in the table",
+                        "environment": "DaylightSun, light yaw 0.4 pitch 0.5, frosted next-event estimation",
+                        "max_depth": 32}
+
+
 def batch_workload(n_stones: int = 64, builder=None):
     from indicatrix_b200 import workloads
 
@@ -175,7 +189,7 @@ def batch_workload(n_stones: int = 64, builder=None):
 def workload_items(args, builder=None):
     if args.workload == "batch":
         return batch_workload(args.stones, builder)
-    return {"frame": frame_workload, "stress": stress_workload}[args.workload](builder)
+    return {"frame": frame_workload, "stress": stress_workload, "sun": sun_workload}[args.workload](builder)
 
 
 # ----------------------------------------------------------------------------------
@@ -797,12 +811,25 @@ def main():
         n_out = sum(fs.width * fs.height * 3 for fs, _ in items)
         result = device_tensor(torch, plan.device_output(), n_out, dev)
     else:
+        from indicatrix_b200 import abi
+
         for fs, spp in items:
             sc = fs.to_abi()
+            # Every array of the scene goes to the device: the device entry reads no host memory.
             planes = torch.from_numpy(np.ascontiguousarray(fs.planes, np.float32)).to(dev)
             sc.planes = C.cast(C.c_void_p(planes.data_ptr()), C.POINTER(C.c_float))
+            keep = [planes]
+            if fs.facet_finishes is not None:
+                fin = torch.from_numpy(np.ascontiguousarray(fs.facet_finishes, np.uint8)).to(dev)
+                sc.facet_finishes = C.cast(C.c_void_p(fin.data_ptr()), C.POINTER(C.c_uint8))
+                keep.append(fin)
+            if fs.tools:
+                raw = np.frombuffer(bytes((abi.Tool * len(fs.tools))(*fs.tools)), np.uint8).copy()
+                tools = torch.from_numpy(raw).to(dev)
+                sc.tools = C.cast(C.c_void_p(tools.data_ptr()), C.POINTER(abi.Tool))
+                keep.append(tools)
             out = torch.zeros(fs.width * fs.height * 3, dtype=torch.float64, device=dev)
-            dev_items.append((sc, planes, out, spp, fs))
+            dev_items.append((sc, keep, out, spp, fs))
         result = dev_items[0][2]
 
     def step(k):

@@ -184,8 +184,10 @@ uint64_t ix_batch_plan_job_offset(const ix_batch_plan* p, uint32_t job);
 void ix_batch_plan_destroy(ix_batch_plan* p);
 /* Device-resident form for callers that keep the scene and the sums in GPU memory:
  * `scene->planes`, `scene->facet_finishes` and `scene->tools` (if any) and `d_accum_xyz` are device
- * pointers; the launch is enqueued on `stream` (a cudaStream_t, or NULL for the
- * backend's own stream) and not synchronised.
+ * pointers (IX_DECLINED for one that is not device or managed memory; the tools are
+ * counted but not read on the host, so the caller validates them with ix_tool_validate);
+ * the launch is enqueued on `stream` (a cudaStream_t, or NULL for the backend's own
+ * stream) and not synchronised.
  * `accumulate` = 1 adds into d_accum_xyz, 0 overwrites it. */
 int ix_accumulate_device(ix_backend* b, const ix_scene* scene, uint32_t sample_offset,
                          uint32_t spp, double* d_accum_xyz, int accumulate, void* stream);

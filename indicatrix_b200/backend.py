@@ -472,8 +472,9 @@ class GpuBackend:
     def accumulate_device(self, scene_abi: abi.Scene, sample_offset: int, spp: int,
                           d_accum_ptr: int, accumulate: bool = True,
                           stream_ptr: Optional[int] = None) -> GpuAccumulate:
-        """Device-resident form: ``scene_abi.planes`` and ``d_accum_ptr`` are device
-        pointers; the launch is enqueued on ``stream_ptr`` and not synchronised."""
+        """Device-resident form: ``scene_abi.planes``, its finishes and tools (if any) and
+        ``d_accum_ptr`` are device pointers (a host array declines); the launch is
+        enqueued on ``stream_ptr`` and not synchronised."""
         if not self._h:
             return GpuAccumulate.DECLINED
         rc = self._lib.ix_accumulate_device(self._h, C.byref(scene_abi), sample_offset, spp,

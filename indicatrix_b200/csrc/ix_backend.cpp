@@ -1298,10 +1298,25 @@ int ix_accumulate_batch(ix_backend* b, ix_batch_item* items, uint32_t n_items, c
     return overall;
 }
 
+// Whether the device can read `p` (device or managed memory); a null array is fine.
+static bool device_readable(const void* p) {
+    if (!p) return true;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
 int ix_accumulate_device(ix_backend* b, const ix_scene* scene, uint32_t sample_offset,
                          uint32_t spp, double* d_accum_xyz, int accumulate, void* stream) {
     if (!b || !scene || !d_accum_xyz) return IX_DECLINED;
-    if (b->lost || !ix_scene_routes_to_gpu(scene)) return IX_DECLINED;
+    if (b->lost || !ix::routes_device_scene(scene)) return IX_DECLINED;
+    // A host array here would fault the kernel: decline it instead.
+    if (!device_readable(scene->planes) || !device_readable(scene->facet_finishes) ||
+        !device_readable(scene->tools) || !device_readable(d_accum_xyz))
+        return IX_DECLINED;
     if ((uint64_t)scene->width * scene->height == 0 || spp == 0) return IX_DONE;
     Turn turn(b);
     cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/ix_attribution.h"
+#include "../../include/ix_cuda.h"
 #include "../../include/ix_scene.h"
 
 namespace ix {
@@ -323,5 +324,17 @@ int trace_blocks_per_sm_exact(int threads, int variant, int uniaxial, size_t* sm
 int trace_blocks_per_sm_fast(int threads, int variant, int uniaxial, size_t* smem_bytes);
 // FP32 FMA-pipe throughput probe (ix_probe.cu): best FLOP/s of `reps` timed runs.
 cudaError_t fp32_probe(int sm_count, int reps, cudaStream_t stream, double* flops);
+
+// ix_scene_routes_to_gpu for a scene whose arrays live in device memory (the device
+// entries): the tools are counted but not read on the host -- the caller validates them
+// with ix_tool_validate before uploading them.
+inline int routes_device_scene(const ix_scene* s) {
+    if (!s) return 0;
+    if (s->n_tools > IX_MAX_TOOLS || (s->n_tools && !s->tools)) return 0;
+    ix_scene copy = *s;
+    copy.tools = nullptr;
+    copy.n_tools = 0;
+    return ix_scene_routes_to_gpu(&copy);
+}
 
 }  // namespace ix

@@ -75,7 +75,7 @@ extern "C" int ix_accumulate_device_noalloc(const ix_scene* scene, uint32_t samp
                                             uint32_t spp, double* d_accum_xyz, int accumulate,
                                             void* stream) {
     if (!scene || !d_accum_xyz) return IX_NOALLOC_ERR_ARGS;
-    if (!ix_scene_routes_to_gpu(scene)) return IX_DECLINED;
+    if (!ix::routes_device_scene(scene)) return IX_DECLINED;
     const uint64_t n_pixels = (uint64_t)scene->width * scene->height;
     if (n_pixels == 0 || spp == 0) return IX_DONE;
     // Every launch needs its own counter slot: reject what would need more launches than

@@ -55,6 +55,25 @@ def round_brilliant_frame(width: int = 256, height: int = 256, max_bounces: int 
                       environment=iso_hemisphere(builder=b))
 
 
+def carved_sun_frame(width: int = 256, height: int = 256, max_bounces: int = 32, builder=None) -> FrameScene:
+    """The round brilliant with its table and girdle frosted and a spherical dimple (radius
+    0.11) ground into the table, under the DaylightSun model at light yaw 0.4, pitch 0.5,
+    seen from 0.6 rad above the girdle plane: every feature of the extended transport at
+    once (the carved-stone intersection, frosted facets with next-event estimation toward
+    the sun's disc, the extended environment lookup)."""
+    b = builder or LIBRARY_BUILDER
+    planes = geometry.to_f32(geometry.round_brilliant())
+    ny = planes[:, 1]
+    finishes = ((np.abs(ny) < 0.05) | (ny > 0.99)).astype(np.uint8)
+    table_y = float(-planes[int(np.argmax(ny)), 3])
+    cam = b.camera_new(0.4, 0.6, FACE_UP_DISTANCE, DEFAULT_FOV_DEG)
+    fs = FrameScene(camera=cam, width=width, height=height, planes=planes, material=materials.diamond(),
+                    max_bounces=max_bounces, environment=b.environment_preset(6, 1.0, 0.4, 0.5, 0.0, 1.0, 16.0),
+                    facet_finishes=finishes)
+    fs.tools = [geometry.tool_ball((0.0, table_y, 0.0), 0.11)]
+    return fs
+
+
 @dataclass
 class StoneSpec:
     planes: np.ndarray

@@ -112,3 +112,32 @@ def test_sun_nee_tier3_fast_build(backend, oracle, name):
         z = z_components(mo[:, c], so[:, c], mg[:, c], g[:, :, c].var(axis=1, ddof=1) / N)
         ok, count, cluster = passes_z_criteria(z, W, H)
         assert ok, (name, axis, count, cluster)
+
+
+def test_device_entry_reads_device_arrays_only(exact_backend):
+    """ix_accumulate_device on the carved, frosted stone under the sun: a scene whose
+    finishes and tools are still host arrays declines before any launch; with every
+    array in device memory it returns the host entry's sums."""
+    import ctypes as C
+
+    import torch
+
+    from indicatrix_b200 import abi, workloads
+
+    fs = workloads.carved_sun_frame(24, 20)
+    n = fs.width * fs.height * 3
+    out = torch.zeros(n, dtype=torch.float64, device="cuda")
+    sc = fs.to_abi()
+    planes = torch.from_numpy(np.ascontiguousarray(fs.planes, np.float32)).cuda()
+    sc.planes = C.cast(C.c_void_p(planes.data_ptr()), C.POINTER(C.c_float))
+    assert exact_backend.accumulate_device(sc, 0, 8, out.data_ptr()) != 0
+    fin = torch.from_numpy(np.ascontiguousarray(fs.facet_finishes, np.uint8)).cuda()
+    sc.facet_finishes = C.cast(C.c_void_p(fin.data_ptr()), C.POINTER(C.c_uint8))
+    raw = np.frombuffer(bytes((abi.Tool * len(fs.tools))(*fs.tools)), np.uint8).copy()
+    tools = torch.from_numpy(raw).cuda()
+    sc.tools = C.cast(C.c_void_p(tools.data_ptr()), C.POINTER(abi.Tool))
+    assert exact_backend.accumulate_device(sc, 0, 8, out.data_ptr()) == 0
+    torch.cuda.synchronize()
+    acc = np.zeros((fs.height, fs.width, 3))
+    assert exact_backend.try_accumulate(fs, 0, 8, acc)
+    assert np.allclose(out.cpu().numpy().reshape(acc.shape), acc, rtol=1e-12, atol=1e-12)
